@@ -1,0 +1,850 @@
+// CPU oracle for the SeqPairBatch alignment path -- TEST INFRASTRUCTURE ONLY.
+//
+// A plain restatement of the reference's scalar algorithms (michalsta/nwgrad,
+// src/nwgrad/cpp/nwgrad/aligner.hpp), written from reading them, used by the test suite,
+// __graft_entry__.smoke() and bench.py's CPU-baseline leg as the checker.  The product
+// (nwgrad_b200) never links or calls this file.
+//
+//   Viterbi, affine, Pointers codes ........ aligner.hpp:3955-4071 (viterbi_affine_ptr_impl)
+//   Viterbi, linear, Pointers codes ........ aligner.hpp:3756-3860 (viterbi_linear_ptr_impl)
+//   Local end cell (first row-major max) ... aligner.hpp:5975-5984 (local_row_best_)
+//   affine walk + hard gradient ............ aligner.hpp:2985-3056, 3177-3230
+//   linear walk + hard gradient ............ aligner.hpp:2852-2900 (walk_linear_impl), 3886-3925
+//   guide_j and its gap interpolation ...... aligner.hpp:3155-3160, 2734-2749
+//   tracks: per-row sets, column-0 border by runs of equal extends ... aligner.hpp:1919-2007
+//   banded rows (guide band) ............... aligner.hpp:2644-2700 (jlo/jhi/border_rows)
+//   soft (log space) forward/backward ...... aligner.hpp:6231-6330 (linear), 6362-6524 (affine)
+//   soft temperature: theta/T, log Z * T ... aligner.hpp:6594-6626
+//   blocked weighted sum of gradients ...... batch_engine.hpp:1788-1827
+//
+// Arithmetic follows the reference expression for expression (same association, same
+// >= tie-breaks, parameters cast to T once), compiled with -ffp-contract=off, so hard
+// results are bit-exact with the reference's float32 / float64 scalar path.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <vector>
+
+namespace {
+
+enum { kOpenA = 0, kExtendA = 1, kOpenB = 2, kExtendB = 3 };
+enum Tbl : uint8_t { TM = 0, TX = 1, TY = 2 };
+
+struct Model {
+    int gm;            // 0 linear, 1 affine
+    int am;            // 0 global, 1 local
+    int N, K;
+    const double* mat;   // K*N*N
+    const double* gaps;  // K*4
+};
+
+template <class T> inline T ninf() { return -std::numeric_limits<T>::infinity(); }
+// std::max semantics (first argument kept on ties): (a < b) ? b : a.
+template <class T> inline T mx(T a, T b) { return (a < b) ? b : a; }
+template <class T> inline T mx3(T a, T b, T c) { return mx(mx(a, b), c); }
+
+// One pair's per-row parameters in T (aligner.hpp:1919-2007).  Untracked: the plain
+// casts of set 0, and the closed-form borders.
+template <class T>
+struct Rows {
+    int m = 0;
+    bool tracked = false;
+    std::vector<uint32_t> rs;                 // substitution row of DP row i (index i-1)
+    std::vector<T> goa, gea, gob, geb, bx0;   // size m+1
+    std::vector<uint16_t> trk, gtrk;          // sets (tracked)
+};
+
+template <class T, bool Linear>
+void setup_rows(Rows<T>& R, const Model& M, const uint8_t* a, int m,
+                const uint16_t* track, const uint16_t* gtrack, bool tracked) {
+    R.m = m; R.tracked = tracked;
+    R.rs.resize(m); R.goa.assign(m + 1, T(0)); R.gea.assign(m + 1, T(0));
+    R.gob.assign(m + 1, T(0)); R.geb.assign(m + 1, T(0)); R.bx0.assign(m + 1, T(0));
+    R.trk.assign(m, 0); R.gtrk.assign(m + 1, 0);
+    if (track) for (int i = 0; i < m; ++i) R.trk[i] = track[i];
+    if (gtrack) for (int i = 0; i <= m; ++i) R.gtrk[i] = gtrack[i];
+    else {
+        R.gtrk[0] = m ? R.trk[0] : 0;
+        for (int i = 1; i <= m; ++i) R.gtrk[i] = R.trk[i - 1];
+    }
+    for (int i = 0; i < m; ++i) R.rs[i] = uint32_t(R.trk[i]) * uint32_t(M.N) + a[i];
+    auto gap = [&](int k, int f) { return M.gaps[4 * k + f]; };
+    for (int i = 0; i <= m; ++i) {
+        R.goa[i] = static_cast<T>(gap(R.gtrk[i], kOpenA));
+        R.gea[i] = static_cast<T>(gap(R.gtrk[i], kExtendA));
+    }
+    for (int i = 1; i <= m; ++i) {
+        R.gob[i] = static_cast<T>(gap(R.trk[i - 1], kOpenB));
+        R.geb[i] = static_cast<T>(gap(R.trk[i - 1], kExtendB));
+    }
+    if (!tracked) {
+        // untracked closed forms (aligner.hpp:6015-6021, 3714-3715)
+        const T go_b = static_cast<T>(gap(0, kOpenB)), ge_b = static_cast<T>(gap(0, kExtendB));
+        for (int i = 1; i <= m; ++i)
+            R.bx0[i] = Linear ? -static_cast<T>(i) * ge_b : -(go_b + static_cast<T>(i) * ge_b);
+        return;
+    }
+    // tracked: runs of bitwise-equal extends (aligner.hpp:1986-2006)
+    T csum = T(0);
+    int s = 1;
+    for (int i = 1; i <= m; ++i) {
+        if (i > 1 && std::memcmp(&R.geb[i], &R.geb[i - 1], sizeof(T)) != 0) {
+            csum = (s == 1) ? static_cast<T>(i - 1) * R.geb[i - 1]
+                            : csum + static_cast<T>(i - s) * R.geb[i - 1];
+            s = i;
+        }
+        const T ge = R.geb[i];
+        if (Linear) {
+            R.bx0[i] = (s == 1) ? -static_cast<T>(i) * ge : -(csum + static_cast<T>(i - s + 1) * ge);
+        } else {
+            const T go = R.gob[1];
+            R.bx0[i] = (s == 1) ? -(go + static_cast<T>(i) * ge)
+                                : -(go + (csum + static_cast<T>(i - s + 1) * ge));
+        }
+    }
+}
+
+// Guide band helpers (aligner.hpp:2644-2700).  band < 0: the full DP.
+struct Band {
+    int band = -1;
+    const int32_t* g = nullptr;
+    int m = 0, n = 0;
+    bool global = true;
+    bool full() const { return band < 0; }
+    int jlo(int i) const { return full() ? 1 : std::max(1, g[i] - band); }
+    int jhi(int i) const {
+        if (full()) return n;
+        if (global && i == m) return n;
+        int hi = g[i] + band;
+        if (i < m) hi = std::max(hi, g[i + 1] - 1 + band);
+        return std::min(n, hi);
+    }
+    int jlo0(int i) const { return full() ? 0 : std::max(0, g[i] - band); }
+    int jhi0(int i) const { return jhi(i); }
+    int border_rows() const {
+        if (full()) return m;
+        int bi = 0;
+        while (bi < m && g[bi + 1] <= band) ++bi;
+        return bi;
+    }
+    int border_cols() const { return full() ? n : jhi(0); }
+};
+
+void fill_guide_gaps(std::vector<int32_t>& gj) {   // aligner.hpp:2734-2749
+    const int n = static_cast<int>(gj.size());
+    int lo = 0;
+    while (lo < n) {
+        if (gj[lo] < 0) { ++lo; continue; }
+        int hi = lo + 1;
+        while (hi < n && gj[hi] < 0) ++hi;
+        if (hi == n) { for (int k = lo + 1; k < n; ++k) gj[k] = gj[lo]; break; }
+        for (int k = lo + 1; k < hi; ++k) gj[k] = gj[lo] + (gj[hi] - gj[lo]) * (k - lo) / (hi - lo);
+        lo = hi;
+    }
+}
+
+// Output of one hard alignment.
+struct HardOut {
+    double score = 0;
+    double* grad = nullptr;      // K*N*N + 4*K, accumulated (caller zeroes)
+    int32_t* guide = nullptr;    // m+1
+    uint8_t* moves = nullptr;    // walk order (end -> start): 0 M, 1 X (gap in B), 2 Y (gap in A)
+    int64_t nmoves = 0;
+    int32_t end_i = 0, end_j = 0, start_i = 0, start_j = 0;
+};
+
+template <class T>
+struct GradSink {
+    const Model& M; const Rows<T>& R; const uint8_t* a; const uint8_t* b; HardOut& o;
+    std::vector<int32_t>* gj;
+    int64_t cap;
+    void move(uint8_t k) { if (o.moves && o.nmoves < cap) o.moves[o.nmoves] = k; ++o.nmoves; }
+    double& gap(int i, int f) {
+        const int set = (f == kOpenA || f == kExtendA) ? R.gtrk[i] : R.trk[i - 1];
+        return o.grad[size_t(M.K) * M.N * M.N + 4 * size_t(set) + f];
+    }
+    void emit(Tbl s, int i, int j, bool open) {   // aligner.hpp:3203-3226
+        move(static_cast<uint8_t>(s));
+        if (s == TM) {
+            if (o.grad) o.grad[size_t(R.rs[i - 1]) * M.N + b[j - 1]] += 1.0;
+            if (gj) (*gj)[i - 1] = j - 1;
+        } else if (s == TX) {
+            if (o.grad) { gap(i, kExtendB) -= 1.0; if (open) gap(i, kOpenB) -= 1.0; }
+            if (gj) (*gj)[i - 1] = j;
+        } else {
+            if (o.grad) { gap(i, kExtendA) -= 1.0; if (open) gap(i, kOpenA) -= 1.0; }
+        }
+    }
+};
+
+// ── Affine Viterbi with Pointers codes (full DP) ──────────────────────────────
+// D[i*(n+1)+j] = M | X << 2 | Y << 4.  Returns the end cell and state.
+template <class T>
+void affine_fill(const Model& M, const Rows<T>& R, const uint8_t* b, int m, int n,
+                 const T* matT, std::vector<uint8_t>& D, T& score, int& bi, int& bj, Tbl& bt) {
+    const bool local = M.am == 1;
+    const size_t st = size_t(n) + 1;
+    D.assign(size_t(m + 1) * st, 0);
+    std::vector<T> pM(st), pX(st), pY(st), cM(st), cX(st), cY(st);
+    auto pick = [](T vm, T vx, T vy) -> uint8_t {
+        const uint8_t kxy = vx >= vy ? 1 : 2;
+        return vm >= mx(vx, vy) ? uint8_t(0) : kxy;
+    };
+    const T go_a0 = R.goa[0], ge_a0 = R.gea[0];
+    for (int j = 0; j <= n; ++j) {
+        if (local) { pM[j] = 0; pX[j] = ninf<T>(); pY[j] = ninf<T>(); }
+        else {
+            pM[j] = (j == 0) ? T(0) : ninf<T>();
+            pX[j] = ninf<T>();
+            pY[j] = (j == 0) ? ninf<T>() : -(go_a0 + static_cast<T>(j) * ge_a0);
+        }
+        D[j] = (j <= 1 || local) ? 3 : (3 | 2 << 4);
+    }
+    bi = 0; bj = 0; bt = TM;
+    T best_local = T(0);
+    for (int i = 1; i <= m; ++i) {
+        const T go_a = R.goa[i], ge_a = R.gea[i], go_b = R.gob[i], ge_b = R.geb[i];
+        const T* srow = matT + size_t(R.rs[i - 1]) * M.N;
+        uint8_t* d = D.data() + size_t(i) * st;
+        if (local) { cM[0] = 0; cX[0] = ninf<T>(); }
+        else { cM[0] = ninf<T>(); cX[0] = R.bx0[i]; }
+        cY[0] = ninf<T>();
+        d[0] = (i <= 1) ? 3 : (3 | 1 << 2);
+        T rowmax = T(0);
+        for (int j = 1; j <= n; ++j) {
+            const T dgM = pM[j - 1], dgX = pX[j - 1], dgY = pY[j - 1];
+            T m_val = mx3(dgM, dgX, dgY) + srow[b[j - 1]];
+            uint8_t km = pick(dgM, dgX, dgY);
+            const T ux = (pM[j] - go_b) - ge_b, vx = pX[j] - ge_b, wx = (pY[j] - go_b) - ge_b;
+            const T x_val = mx3(ux, vx, wx);
+            const uint8_t kx = pick(ux, vx, wx);
+            const T uy = (cM[j - 1] - go_a) - ge_a, vy = (cX[j - 1] - go_a) - ge_a, wy = cY[j - 1] - ge_a;
+            const T y_val = mx3(uy, vy, wy);
+            const uint8_t ky = pick(uy, vy, wy);
+            if (local) {
+                m_val = mx(m_val, T(0));
+                rowmax = mx(rowmax, mx3(m_val, x_val, y_val));
+                km = uint8_t(km | (3u * unsigned(m_val <= T(0))));
+            }
+            cM[j] = m_val; cX[j] = x_val; cY[j] = y_val;
+            d[j] = uint8_t(km | kx << 2 | ky << 4);
+        }
+        if (local && rowmax > best_local) {
+            int j = 1;
+            while (!(mx3(cM[j], cX[j], cY[j]) == rowmax)) ++j;
+            best_local = rowmax; bi = i; bj = j;
+            const T vm = cM[j], vx = cX[j], vy = cY[j];
+            bt = (vm >= vx && vm >= vy) ? TM : (vx >= vy ? TX : TY);
+        }
+        std::swap(pM, cM); std::swap(pX, cX); std::swap(pY, cY);
+    }
+    if (!local) {
+        const T vm = pM[n], vx = pX[n], vy = pY[n];
+        score = mx3(vm, vx, vy);
+        bi = m; bj = n;
+        bt = (vm >= vx && vm >= vy) ? TM : (vx >= vy ? TX : TY);
+    } else {
+        score = best_local;
+    }
+}
+
+template <class T>
+void affine_walk(const Model& M, const std::vector<uint8_t>& D, int n, int bi, int bj, Tbl bt,
+                 GradSink<T>& sink) {
+    const bool local = M.am == 1;
+    const size_t st = size_t(n) + 1;
+    auto from_code = [](unsigned c) { return c == 1 ? TX : (c == 2 ? TY : TM); };
+    int i = bi, j = bj;
+    Tbl tbl = bt;
+    while (true) {
+        if (i == 0 && j == 0) break;
+        unsigned c = 0;
+        if (local) {
+            c = D[size_t(i) * st + j];
+            if (tbl == TM && (c & 3) == 3) break;
+        } else {
+            if (i == 0) { for (; j > 0; --j) sink.emit(TY, 0, j, j == 1); break; }
+            if (j == 0) { for (; i > 0; --i) sink.emit(TX, i, 0, i == 1); break; }
+            c = D[size_t(i) * st + j];
+        }
+        if (i == 0) tbl = TY;
+        else if (j == 0) tbl = TX;
+        Tbl prev;
+        if (tbl == TM) {
+            prev = from_code(c & 3);
+            sink.emit(TM, i, j, false);
+            --i; --j;
+        } else if (tbl == TX) {
+            prev = from_code((c >> 2) & 3);
+            sink.emit(TX, i, j, prev != TX);
+            --i;
+        } else {
+            prev = from_code(c >> 4);
+            sink.emit(TY, i, j, prev != TY);
+            --j;
+        }
+        tbl = prev;
+    }
+    sink.o.start_i = i; sink.o.start_j = j;
+}
+
+// ── Linear Viterbi with Pointers codes (full DP) ──────────────────────────────
+// Codes: 0 diagonal, 1 up (gap in B), 2 left (gap in A), 3 stop.
+template <class T>
+void linear_fill(const Model& M, const Rows<T>& R, const uint8_t* b, int m, int n,
+                 const T* matT, std::vector<uint8_t>& D, T& score, int& bi, int& bj) {
+    const bool local = M.am == 1;
+    const size_t st = size_t(n) + 1;
+    D.assign(size_t(m + 1) * st, 0);
+    std::vector<T> prev(st), cur(st);
+    const T ge_a0 = R.gea[0];
+    prev[0] = T(0); D[0] = 3;
+    for (int j = 1; j <= n; ++j) {
+        prev[j] = local ? T(0) : -static_cast<T>(j) * ge_a0;
+        D[j] = local ? 3 : 2;
+    }
+    bi = 0; bj = 0;
+    T best_local = T(0);
+    for (int i = 1; i <= m; ++i) {
+        uint8_t* d = D.data() + size_t(i) * st;
+        const T* prow = matT + size_t(R.rs[i - 1]) * M.N;
+        const T ge_a = R.gea[i], ge_b = R.geb[i];
+        cur[0] = local ? T(0) : R.bx0[i];
+        d[0] = local ? 3 : 1;
+        for (int j = 1; j <= n; ++j) {
+            const T d0 = prev[j - 1] + prow[b[j - 1]];
+            const T u = prev[j] - ge_b;
+            cur[j] = mx(d0, u);
+            d[j] = uint8_t(d0 < u);
+        }
+        T left = cur[0];
+        for (int j = 1; j <= n; ++j) {
+            const T t = cur[j], l = left - ge_a;
+            T v = mx(t, l);
+            const int tl = t < l;
+            uint8_t c = uint8_t(d[j] + tl * (2 - d[j]));
+            if (local) {
+                v = mx(v, T(0));
+                c = uint8_t(c | (3u * unsigned(v <= T(0))));
+                if (v > best_local) { best_local = v; bi = i; bj = j; }
+            }
+            cur[j] = v; d[j] = c;
+            left = v;
+        }
+        std::swap(prev, cur);
+    }
+    score = local ? best_local : prev[n];
+    if (!local) { bi = m; bj = n; }
+}
+
+template <class T>
+void linear_walk(const std::vector<uint8_t>& D, int n, int bi, int bj, GradSink<T>& sink) {
+    const size_t st = size_t(n) + 1;
+    int i = bi, j = bj;
+    while (true) {
+        if (i == 0 && j == 0) break;
+        const int k = D[size_t(i) * st + j];
+        if (k == 3) break;
+        // linear moves: gap fields are extends only (aligner.hpp:3886-3925)
+        if (k == 0) { sink.emit(TM, i, j, false); --i; --j; }
+        else if (k == 1) {
+            sink.move(1);
+            if (sink.o.grad) sink.gap(i, kExtendB) -= 1.0;
+            if (sink.gj) (*sink.gj)[i - 1] = j;
+            --i;
+        } else {
+            sink.move(2);
+            if (sink.o.grad) sink.gap(i, kExtendA) -= 1.0;
+            --j;
+        }
+    }
+    sink.o.start_i = i; sink.o.start_j = j;
+}
+
+// ── Banded Viterbi (GuideBanded), score tables + re-derived walk ─────────────
+// Affine: aligner.hpp:5991-6098 (the band restricts j to [jlo(i), jhi(i)], cells outside
+// the band are -inf); walk re-derives predecessors from the tables (walk_affine_impl with
+// Ptr = false).  Linear: viterbi_linear_impl + walk_linear_impl (H equality walk).
+template <class T>
+void banded_affine(const Model& M, const Rows<T>& R, const uint8_t* b, int m, int n,
+                   const T* matT, const Band& B, GradSink<T>& sink, T& score) {
+    const bool local = M.am == 1;
+    const size_t st = size_t(n) + 1;
+    std::vector<T> VM(size_t(m + 1) * st, ninf<T>()), VX(VM), VY(VM);
+    auto at = [&](std::vector<T>& v, int i, int j) -> T& { return v[size_t(i) * st + j]; };
+    if (!local) {
+        at(VM, 0, 0) = T(0);
+        const int bi = B.border_rows(), bj = B.border_cols();
+        for (int i = 1; i <= bi; ++i) at(VX, i, 0) = R.bx0[i];
+        for (int j = 1; j <= bj; ++j) at(VY, 0, j) = -(R.goa[0] + static_cast<T>(j) * R.gea[0]);
+    } else {
+        for (int i = 0; i <= m; ++i) at(VM, i, 0) = T(0);
+        for (int j = 0; j <= n; ++j) at(VM, 0, j) = T(0);
+    }
+    int bi = 0, bj = 0; Tbl bt = TM;
+    T best_local = T(0);
+    for (int i = 1; i <= m; ++i) {
+        const T go_a = R.goa[i], ge_a = R.gea[i], go_b = R.gob[i], ge_b = R.geb[i];
+        const T* srow = matT + size_t(R.rs[i - 1]) * M.N;
+        const int j0 = B.jlo(i), j1 = B.jhi(i);
+        if (j0 > j1) continue;
+        T lM = at(VM, i, j0 - 1), lX = at(VX, i, j0 - 1), lY = at(VY, i, j0 - 1);
+        T rowmax = T(0);
+        for (int j = j0; j <= j1; ++j) {
+            const T diag = mx3(at(VM, i - 1, j - 1), at(VX, i - 1, j - 1), at(VY, i - 1, j - 1));
+            T m_val = diag + srow[b[j - 1]];
+            const T x_val = mx(((mx(at(VM, i - 1, j), at(VY, i - 1, j)) - go_b) - ge_b), at(VX, i - 1, j) - ge_b);
+            const T y_val = mx(((mx(lM, lX) - go_a) - ge_a), lY - ge_a);
+            if (local) { m_val = mx(m_val, T(0)); rowmax = mx(rowmax, mx3(m_val, x_val, y_val)); }
+            at(VM, i, j) = m_val; at(VX, i, j) = x_val; at(VY, i, j) = y_val;
+            lM = m_val; lX = x_val; lY = y_val;
+        }
+        if (local && rowmax > best_local) {
+            int j = j0;
+            while (!(mx3(at(VM, i, j), at(VX, i, j), at(VY, i, j)) == rowmax)) ++j;
+            best_local = rowmax; bi = i; bj = j;
+            const T vm = at(VM, i, j), vx = at(VX, i, j), vy = at(VY, i, j);
+            bt = (vm >= vx && vm >= vy) ? TM : (vx >= vy ? TX : TY);
+        }
+    }
+    if (!local) {
+        const T vm = at(VM, m, n), vx = at(VX, m, n), vy = at(VY, m, n);
+        score = mx3(vm, vx, vy);
+        bi = m; bj = n;
+        bt = (vm >= vx && vm >= vy) ? TM : (vx >= vy ? TX : TY);
+    } else score = best_local;
+    sink.o.end_i = bi; sink.o.end_j = bj;
+    if (sink.gj) { auto& gj = *sink.gj; gj.assign(m + 1, -1); gj[0] = 0; gj[m] = n; gj[bi] = bj; }
+    // walk, re-deriving predecessors (aligner.hpp:2985-3056, Ptr = false)
+    auto argmax = [](T vm, T vx, T vy) { if (vm >= vx && vm >= vy) return TM; return vx >= vy ? TX : TY; };
+    int i = bi, j = bj;
+    Tbl tbl = bt;
+    while (true) {
+        if (i == 0 && j == 0) break;
+        if (local) {
+            if (tbl == TM && at(VM, i, j) <= T(0)) break;
+        } else {
+            if (i == 0) { for (; j > 0; --j) sink.emit(TY, 0, j, j == 1); break; }
+            if (j == 0) { for (; i > 0; --i) sink.emit(TX, i, 0, i == 1); break; }
+        }
+        if (i == 0) tbl = TY;
+        else if (j == 0) tbl = TX;
+        Tbl prev;
+        if (tbl == TM) {
+            prev = argmax(at(VM, i - 1, j - 1), at(VX, i - 1, j - 1), at(VY, i - 1, j - 1));
+            sink.emit(TM, i, j, false); --i; --j;
+        } else if (tbl == TX) {
+            const T go_b = R.gob[i], ge_b = R.geb[i];
+            prev = argmax((at(VM, i - 1, j) - go_b) - ge_b, at(VX, i - 1, j) - ge_b, (at(VY, i - 1, j) - go_b) - ge_b);
+            sink.emit(TX, i, j, prev != TX); --i;
+        } else {
+            const T go_a = R.goa[i], ge_a = R.gea[i];
+            prev = argmax((at(VM, i, j - 1) - go_a) - ge_a, (at(VX, i, j - 1) - go_a) - ge_a, at(VY, i, j - 1) - ge_a);
+            sink.emit(TY, i, j, prev != TY); --j;
+        }
+        tbl = prev;
+    }
+    sink.o.start_i = i; sink.o.start_j = j;
+}
+
+template <class T>
+void banded_linear(const Model& M, const Rows<T>& R, const uint8_t* b, int m, int n,
+                   const T* matT, const Band& B, GradSink<T>& sink, T& score) {
+    const bool local = M.am == 1;
+    const size_t st = size_t(n) + 1;
+    std::vector<T> H(size_t(m + 1) * st, ninf<T>());
+    auto at = [&](int i, int j) -> T& { return H[size_t(i) * st + j]; };
+    // viterbi_linear_impl's banded_fill: -inf over the band's row spans (here everywhere).
+    if (!local) {
+        at(0, 0) = T(0);
+        const int bi = B.border_rows(), bj = B.border_cols();
+        for (int i = 1; i <= bi; ++i) at(i, 0) = R.bx0[i];
+        for (int j = 1; j <= bj; ++j) at(0, j) = -static_cast<T>(j) * R.gea[0];
+    } else {
+        for (int i = 0; i <= m; ++i) at(i, 0) = T(0);
+        for (int j = 0; j <= n; ++j) at(0, j) = T(0);
+    }
+    int bi = 0, bj = 0;
+    T best_local = T(0);
+    for (int i = 1; i <= m; ++i) {
+        const T ge_b = R.geb[i], ge_a = R.gea[i];
+        const T* srow = matT + size_t(R.rs[i - 1]) * M.N;
+        const int j0 = B.jlo(i), j1 = B.jhi(i);
+        T rowmax = T(0);
+        for (int j = j0; j <= j1; ++j) {
+            T v = mx3(at(i - 1, j - 1) + srow[b[j - 1]], at(i - 1, j) - ge_b, at(i, j - 1) - ge_a);
+            if (local) { v = mx(v, T(0)); rowmax = mx(rowmax, v); }
+            at(i, j) = v;
+        }
+        if (local && rowmax > best_local) {
+            int j = j0;
+            while (!(at(i, j) == rowmax)) ++j;
+            best_local = rowmax; bi = i; bj = j;
+        }
+    }
+    score = local ? best_local : at(m, n);
+    if (!local) { bi = m; bj = n; }
+    sink.o.end_i = bi; sink.o.end_j = bj;
+    if (sink.gj) {
+        auto& gj = *sink.gj; gj.assign(m + 1, -1); gj[0] = 0; gj[m] = n;
+        gj[local ? bi : m] = local ? bj : n;
+    }
+    int i = bi, j = bj;
+    while (true) {
+        if (i == 0 && j == 0) break;
+        if (local && at(i, j) <= T(0)) break;
+        int k;
+        if (i > 0 && j > 0 && at(i, j) == at(i - 1, j - 1) + matT[size_t(R.rs[i - 1]) * M.N + b[j - 1]]) k = 0;
+        else if (i > 0 && (j == 0 || at(i, j) == at(i - 1, j) - R.geb[i])) k = 1;
+        else k = 2;
+        if (k == 0) { sink.emit(TM, i, j, false); --i; --j; }
+        else if (k == 1) {
+            sink.move(1);
+            if (sink.o.grad) sink.gap(i, kExtendB) -= 1.0;
+            if (sink.gj) (*sink.gj)[i - 1] = j;
+            --i;
+        } else {
+            sink.move(2);
+            if (sink.o.grad) sink.gap(i, kExtendA) -= 1.0;
+            --j;
+        }
+    }
+    sink.o.start_i = i; sink.o.start_j = j;
+}
+
+template <class T>
+int hard_one(const Model& M, const uint8_t* a, int m, const uint8_t* b, int n,
+             const uint16_t* track, const uint16_t* gtrack, bool tracked,
+             const int32_t* guide_in, int band, HardOut& o, int64_t moves_cap) {
+    const bool linear = M.gm == 0;
+    Rows<T> R;
+    if (linear) setup_rows<T, true>(R, M, a, m, track, gtrack, tracked);
+    else        setup_rows<T, false>(R, M, a, m, track, gtrack, tracked);
+    std::vector<T> matT(size_t(M.K) * M.N * M.N);
+    for (size_t k = 0; k < matT.size(); ++k) matT[k] = static_cast<T>(M.mat[k]);
+    std::vector<int32_t> gj;
+    GradSink<T> sink{M, R, a, b, o, o.guide ? &gj : nullptr, moves_cap};
+    T score = T(0);
+    if (band >= 0) {
+        Band B; B.band = band; B.g = guide_in; B.m = m; B.n = n; B.global = M.am == 0;
+        if (linear) banded_linear<T>(M, R, b, m, n, matT.data(), B, sink, score);
+        else        banded_affine<T>(M, R, b, m, n, matT.data(), B, sink, score);
+    } else {
+        std::vector<uint8_t> D;
+        int bi, bj;
+        if (linear) {
+            linear_fill<T>(M, R, b, m, n, matT.data(), D, score, bi, bj);
+            o.end_i = bi; o.end_j = bj;
+            if (o.guide) {
+                gj.assign(m + 1, -1); gj[0] = 0; gj[m] = n;
+                if (M.am == 0) gj[m] = n; else gj[bi] = bj;
+            }
+            linear_walk<T>(D, n, bi, bj, sink);
+        } else {
+            Tbl bt;
+            affine_fill<T>(M, R, b, m, n, matT.data(), D, score, bi, bj, bt);
+            o.end_i = bi; o.end_j = bj;
+            if (o.guide) { gj.assign(m + 1, -1); gj[0] = 0; gj[m] = n; gj[bi] = bj; }
+            affine_walk<T>(M, D, n, bi, bj, bt, sink);
+        }
+    }
+    o.score = static_cast<double>(score);
+    if (o.guide) {
+        fill_guide_gaps(gj);
+        std::memcpy(o.guide, gj.data(), sizeof(int32_t) * (m + 1));
+    }
+    return 0;
+}
+
+// ── Soft, log space, double (aligner.hpp:6231-6524) ──────────────────────────
+inline double lse2(double a, double b) {
+    const double NI = -std::numeric_limits<double>::infinity();
+    if (a == NI) return b;
+    if (b == NI) return a;
+    if (a > b) return a + std::log1p(std::exp(b - a));
+    return b + std::log1p(std::exp(a - b));
+}
+inline double lse3(double a, double b, double c) { return lse2(lse2(a, b), c); }
+
+// Per-row double parameters of theta/T.
+struct DRows {
+    std::vector<double> goa, gea, gob, geb, bx0;
+    std::vector<uint32_t> rs;
+    std::vector<uint16_t> trk, gtrk;
+};
+
+void setup_drows(DRows& R, const Model& M, const uint8_t* a, int m, const uint16_t* track,
+                 const uint16_t* gtrack, double invT, bool linear) {
+    R.trk.assign(m, 0); R.gtrk.assign(m + 1, 0); R.rs.resize(m);
+    if (track) for (int i = 0; i < m; ++i) R.trk[i] = track[i];
+    if (gtrack) for (int i = 0; i <= m; ++i) R.gtrk[i] = gtrack[i];
+    else { R.gtrk[0] = m ? R.trk[0] : 0; for (int i = 1; i <= m; ++i) R.gtrk[i] = R.trk[i - 1]; }
+    for (int i = 0; i < m; ++i) R.rs[i] = uint32_t(R.trk[i]) * uint32_t(M.N) + a[i];
+    R.goa.assign(m + 1, 0); R.gea.assign(m + 1, 0); R.gob.assign(m + 1, 0); R.geb.assign(m + 1, 0);
+    R.bx0.assign(m + 1, 0);
+    for (int i = 0; i <= m; ++i) {
+        R.goa[i] = M.gaps[4 * R.gtrk[i] + kOpenA] * invT;
+        R.gea[i] = M.gaps[4 * R.gtrk[i] + kExtendA] * invT;
+    }
+    for (int i = 1; i <= m; ++i) {
+        R.gob[i] = M.gaps[4 * R.trk[i - 1] + kOpenB] * invT;
+        R.geb[i] = M.gaps[4 * R.trk[i - 1] + kExtendB] * invT;
+    }
+    // column-0 border: the charged chain of gaps in B (exact sums)
+    double s = 0;
+    for (int i = 1; i <= m; ++i) {
+        s += R.geb[i];
+        R.bx0[i] = linear ? -s : -(R.gob[1] + s);
+    }
+}
+
+struct SoftOut { double logz = 0; double* grad = nullptr; };
+
+void soft_affine(const Model& M, const uint8_t* a, int m, const uint8_t* b, int n,
+                 const uint16_t* track, const uint16_t* gtrack, double T, SoftOut& o) {
+    (void)a;
+    const double NI = -std::numeric_limits<double>::infinity();
+    const bool local = M.am == 1;
+    const double invT = 1.0 / T;
+    DRows R; setup_drows(R, M, a, m, track, gtrack, invT, false);
+    const size_t st = size_t(n) + 1, cells = size_t(m + 1) * st;
+    std::vector<double> FM(cells, NI), FX(cells, NI), FY(cells, NI);
+    auto I = [&](int i, int j) { return size_t(i) * st + j; };
+    auto sub = [&](int i, int j) { return M.mat[size_t(R.rs[i - 1]) * M.N + b[j - 1]] * invT; };
+    if (!local) {
+        FM[I(0, 0)] = 0.0;
+        for (int i = 1; i <= m; ++i) FX[I(i, 0)] = R.bx0[i];
+        for (int j = 1; j <= n; ++j) FY[I(0, j)] = -(R.goa[0] + double(j) * R.gea[0]);
+    } else {
+        for (int i = 0; i <= m; ++i) FM[I(i, 0)] = 0.0;
+        for (int j = 0; j <= n; ++j) FM[I(0, j)] = 0.0;
+    }
+    for (int i = 1; i <= m; ++i)
+        for (int j = 1; j <= n; ++j) {
+            const double diag = lse3(FM[I(i - 1, j - 1)], FX[I(i - 1, j - 1)], FY[I(i - 1, j - 1)]);
+            double mv = diag + sub(i, j);
+            const double gob = R.gob[i], geb = R.geb[i], goa = R.goa[i], gea = R.gea[i];
+            const double xv = lse3(FM[I(i - 1, j)] - gob - geb, FX[I(i - 1, j)] - geb, FY[I(i - 1, j)] - gob - geb);
+            const double yv = lse3(FM[I(i, j - 1)] - goa - gea, FX[I(i, j - 1)] - goa - gea, FY[I(i, j - 1)] - gea);
+            if (local) mv = lse2(mv, 0.0);
+            FM[I(i, j)] = mv; FX[I(i, j)] = xv; FY[I(i, j)] = yv;
+        }
+    double lz;
+    if (!local) lz = lse3(FM[I(m, n)], FX[I(m, n)], FY[I(m, n)]);
+    else {
+        lz = NI;
+        for (int i = 0; i <= m; ++i) for (int j = 0; j <= n; ++j)
+            lz = lse2(lz, lse3(FM[I(i, j)], FX[I(i, j)], FY[I(i, j)]));
+    }
+    std::vector<double> BM(cells, local ? 0.0 : NI), BX(BM), BY(BM);
+    if (!local) { BM[I(m, n)] = 0; BX[I(m, n)] = 0; BY[I(m, n)] = 0; }
+    for (int i = m; i >= 0; --i)
+        for (int j = n; j >= 0; --j) {
+            const double bm = BM[I(i, j)], bx = BX[I(i, j)], by = BY[I(i, j)];
+            if (bm != NI && i > 0 && j > 0) {
+                const double c = bm + sub(i, j);
+                BM[I(i - 1, j - 1)] = lse2(BM[I(i - 1, j - 1)], c);
+                BX[I(i - 1, j - 1)] = lse2(BX[I(i - 1, j - 1)], c);
+                BY[I(i - 1, j - 1)] = lse2(BY[I(i - 1, j - 1)], c);
+            }
+            if (bx != NI && i > 0) {
+                const double gob = R.gob[i], geb = R.geb[i];
+                BM[I(i - 1, j)] = lse2(BM[I(i - 1, j)], bx - gob - geb);
+                BX[I(i - 1, j)] = lse2(BX[I(i - 1, j)], bx - geb);
+                BY[I(i - 1, j)] = lse2(BY[I(i - 1, j)], bx - gob - geb);
+            }
+            if (by != NI && j > 0) {
+                const double goa = R.goa[i], gea = R.gea[i];
+                BM[I(i, j - 1)] = lse2(BM[I(i, j - 1)], by - goa - gea);
+                BX[I(i, j - 1)] = lse2(BX[I(i, j - 1)], by - goa - gea);
+                BY[I(i, j - 1)] = lse2(BY[I(i, j - 1)], by - gea);
+            }
+        }
+    const size_t NN = size_t(M.K) * M.N * M.N;
+    double* g = o.grad;
+    auto gap = [&](int set, int f) -> double& { return g[NN + 4 * size_t(set) + f]; };
+    const int gmin_j = local ? 1 : 0, gmin_i = local ? 1 : 0;
+    for (int i = 1; i <= m; ++i)
+        for (int j = 1; j <= n; ++j) {
+            const double bm = BM[I(i, j)];
+            if (bm == NI) continue;
+            const double pred = lse3(FM[I(i - 1, j - 1)], FX[I(i - 1, j - 1)], FY[I(i - 1, j - 1)]);
+            g[size_t(R.rs[i - 1]) * M.N + b[j - 1]] += std::exp(pred + sub(i, j) + bm - lz);
+        }
+    for (int i = 1; i <= m; ++i)
+        for (int j = 0; j <= n; ++j) {
+            const double fx = FX[I(i, j)], bx = BX[I(i, j)];
+            if (fx == NI || bx == NI) continue;
+            gap(R.trk[i - 1], kExtendB) -= std::exp(fx + bx - lz);
+        }
+    for (int i = 0; i <= m; ++i)
+        for (int j = 1; j <= n; ++j) {
+            const double fy = FY[I(i, j)], by = BY[I(i, j)];
+            if (fy == NI || by == NI) continue;
+            gap(R.gtrk[i], kExtendA) -= std::exp(fy + by - lz);
+        }
+    for (int i = 1; i <= m; ++i)
+        for (int j = gmin_j; j <= n; ++j) {
+            const double bx = BX[I(i, j)];
+            if (bx == NI) continue;
+            const double lo = lse2(FM[I(i - 1, j)], FY[I(i - 1, j)]) - R.gob[i] - R.geb[i] + bx - lz;
+            if (lo > -700) gap(R.trk[i - 1], kOpenB) -= std::exp(lo);
+        }
+    for (int i = gmin_i; i <= m; ++i)
+        for (int j = 1; j <= n; ++j) {
+            const double by = BY[I(i, j)];
+            if (by == NI) continue;
+            const double lo = lse2(FM[I(i, j - 1)], FX[I(i, j - 1)]) - R.goa[i] - R.gea[i] + by - lz;
+            if (lo > -700) gap(R.gtrk[i], kOpenA) -= std::exp(lo);
+        }
+    o.logz = lz * T;
+}
+
+void soft_linear(const Model& M, const uint8_t* a, int m, const uint8_t* b, int n,
+                 const uint16_t* track, const uint16_t* gtrack, double T, SoftOut& o) {
+    const double NI = -std::numeric_limits<double>::infinity();
+    const bool local = M.am == 1;
+    const double invT = 1.0 / T;
+    DRows R; setup_drows(R, M, a, m, track, gtrack, invT, true);
+    const size_t st = size_t(n) + 1, cells = size_t(m + 1) * st;
+    std::vector<double> F(cells, NI), B(cells, local ? 0.0 : NI);
+    auto I = [&](int i, int j) { return size_t(i) * st + j; };
+    auto sub = [&](int i, int j) { return M.mat[size_t(R.rs[i - 1]) * M.N + b[j - 1]] * invT; };
+    if (!local) {
+        F[I(0, 0)] = 0.0;
+        for (int i = 1; i <= m; ++i) F[I(i, 0)] = R.bx0[i];
+        for (int j = 1; j <= n; ++j) F[I(0, j)] = -double(j) * R.gea[0];
+    } else {
+        for (int i = 0; i <= m; ++i) F[I(i, 0)] = 0.0;
+        for (int j = 0; j <= n; ++j) F[I(0, j)] = 0.0;
+    }
+    for (int i = 1; i <= m; ++i)
+        for (int j = 1; j <= n; ++j) {
+            double v = lse3(F[I(i - 1, j - 1)] + sub(i, j), F[I(i - 1, j)] - R.geb[i], F[I(i, j - 1)] - R.gea[i]);
+            if (local) v = lse2(v, 0.0);
+            F[I(i, j)] = v;
+        }
+    double lz;
+    if (!local) lz = F[I(m, n)];
+    else { lz = NI; for (size_t k = 0; k < cells; ++k) lz = lse2(lz, F[k]); }
+    if (!local) B[I(m, n)] = 0.0;
+    for (int i = m; i >= 0; --i)
+        for (int j = n; j >= 0; --j) {
+            const double bv = B[I(i, j)];
+            if (bv == NI) continue;
+            if (i > 0 && j > 0) B[I(i - 1, j - 1)] = lse2(B[I(i - 1, j - 1)], bv + sub(i, j));
+            if (i > 0) B[I(i - 1, j)] = lse2(B[I(i - 1, j)], bv - R.geb[i]);
+            if (j > 0) B[I(i, j - 1)] = lse2(B[I(i, j - 1)], bv - R.gea[i]);
+        }
+    const size_t NN = size_t(M.K) * M.N * M.N;
+    double* g = o.grad;
+    auto gap = [&](int set, int f) -> double& { return g[NN + 4 * size_t(set) + f]; };
+    const int gmin_j = local ? 1 : 0, gmin_i = local ? 1 : 0;
+    for (int i = 1; i <= m; ++i)
+        for (int j = 1; j <= n; ++j) {
+            const double bv = B[I(i, j)];
+            if (bv == NI) continue;
+            g[size_t(R.rs[i - 1]) * M.N + b[j - 1]] += std::exp(F[I(i - 1, j - 1)] + sub(i, j) + bv - lz);
+        }
+    for (int i = 1; i <= m; ++i)
+        for (int j = gmin_j; j <= n; ++j) {
+            const double bv = B[I(i, j)], fv = F[I(i - 1, j)];
+            if (bv == NI || fv == NI) continue;
+            gap(R.trk[i - 1], kExtendB) -= std::exp(fv - R.geb[i] + bv - lz);
+        }
+    for (int i = gmin_i; i <= m; ++i)
+        for (int j = 1; j <= n; ++j) {
+            const double bv = B[I(i, j)], fv = F[I(i, j - 1)];
+            if (bv == NI || fv == NI) continue;
+            gap(R.gtrk[i], kExtendA) -= std::exp(fv - R.gea[i] + bv - lz);
+        }
+    o.logz = lz * T;
+}
+
+}  // namespace
+
+// ── C ABI for the test suite (ctypes) ─────────────────────────────────────────
+extern "C" {
+
+// A batch of pairs.  a / b: concatenated codes, oa / ob: n_pairs + 1 offsets.
+// tracks: concatenated per-residue sets of A (oa offsets) or null; gtracks: per DP row
+// (oa[p] + p offsets, m + 1 each) or null.  tracked: whether the batch is tracked (tracks
+// given or K > 1).  grads: n_pairs * (K*N*N + 4*K), zeroed here.  guides: (oa[p] + p)
+// offsets, m + 1 each, or null.  moves (optional): per pair moves_cap bytes, walk order.
+// band >= 0 with guides_in: the guide-banded DP.  prec: 32 float, 64 double.
+int orc_hard_batch(int prec, int gm, int am, int N, int K, const double* mat, const double* gaps,
+                   const uint8_t* a, const int64_t* oa, const uint8_t* b, const int64_t* ob,
+                   int64_t n_pairs, const uint16_t* tracks, const uint16_t* gtracks, int tracked,
+                   const int32_t* guides_in, int band,
+                   double* scores, double* grads, int32_t* guides,
+                   uint8_t* moves, int64_t moves_cap, int64_t* nmoves, int32_t* ends) {
+    Model M{gm, am, N, K, mat, gaps};
+    const size_t gs = size_t(K) * N * N + 4 * size_t(K);
+    for (int64_t p = 0; p < n_pairs; ++p) {
+        const int m = int(oa[p + 1] - oa[p]), n = int(ob[p + 1] - ob[p]);
+        HardOut o;
+        o.grad = grads ? grads + gs * p : nullptr;
+        if (o.grad) std::fill(o.grad, o.grad + gs, 0.0);
+        o.guide = guides ? guides + oa[p] + p : nullptr;
+        o.moves = moves ? moves + moves_cap * p : nullptr;
+        const uint16_t* tk = tracks ? tracks + oa[p] : nullptr;
+        const uint16_t* gk = gtracks ? gtracks + oa[p] + p : nullptr;
+        const int32_t* gi = guides_in ? guides_in + oa[p] + p : nullptr;
+        if (prec == 32)
+            hard_one<float>(M, a + oa[p], m, b + ob[p], n, tk, gk, tracked != 0, gi, band, o, moves_cap);
+        else
+            hard_one<double>(M, a + oa[p], m, b + ob[p], n, tk, gk, tracked != 0, gi, band, o, moves_cap);
+        scores[p] = o.score;
+        if (nmoves) nmoves[p] = o.nmoves;
+        if (ends) {
+            ends[4 * p] = o.end_i; ends[4 * p + 1] = o.end_j;
+            ends[4 * p + 2] = o.start_i; ends[4 * p + 3] = o.start_j;
+        }
+    }
+    return 0;
+}
+
+// Soft gradient in log space, double, at temperature T: scores = T * log Z(theta/T),
+// grads = expected counts under theta/T (gap fields negative).
+int orc_soft_batch(int gm, int am, int N, int K, const double* mat, const double* gaps,
+                   const uint8_t* a, const int64_t* oa, const uint8_t* b, const int64_t* ob,
+                   int64_t n_pairs, const uint16_t* tracks, const uint16_t* gtracks,
+                   double temperature, double* scores, double* grads) {
+    Model M{gm, am, N, K, mat, gaps};
+    const size_t gs = size_t(K) * N * N + 4 * size_t(K);
+    for (int64_t p = 0; p < n_pairs; ++p) {
+        const int m = int(oa[p + 1] - oa[p]), n = int(ob[p + 1] - ob[p]);
+        SoftOut o;
+        o.grad = grads + gs * p;
+        std::fill(o.grad, o.grad + gs, 0.0);
+        const uint16_t* tk = tracks ? tracks + oa[p] : nullptr;
+        const uint16_t* gk = gtracks ? gtracks + oa[p] + p : nullptr;
+        if (gm == 0) soft_linear(M, a + oa[p], m, b + ob[p], n, tk, gk, temperature, o);
+        else         soft_affine(M, a + oa[p], m, b + ob[p], n, tk, gk, temperature, o);
+        scores[p] = o.logz;
+    }
+    return 0;
+}
+
+// sum_p w[p] * g[p] in blocks of 4096 pairs: each block from 0.0 in pair order, then the
+// blocks in order (batch_engine.hpp:1788-1827).  w null: weights of one.
+int orc_blocked_sum(const double* g, int64_t n_pairs, int64_t gs, const double* w, double* out) {
+    const int64_t B = 4096;
+    for (int64_t k = 0; k < gs; ++k) out[k] = 0.0;
+    std::vector<double> acc(gs);
+    for (int64_t b0 = 0; b0 < n_pairs; b0 += B) {
+        std::fill(acc.begin(), acc.end(), 0.0);
+        const int64_t e = std::min(n_pairs, b0 + B);
+        for (int64_t p = b0; p < e; ++p)
+            for (int64_t k = 0; k < gs; ++k) {
+                const double v = w ? w[p] * g[p * gs + k] : g[p * gs + k];
+                acc[k] += v;
+            }
+        for (int64_t k = 0; k < gs; ++k) out[k] += acc[k];
+    }
+    return 0;
+}
+
+}  // extern "C"
