@@ -1,0 +1,361 @@
+#!/usr/bin/env python3
+"""Benchmark: soft-gradient global affine batch GCUPS on one B200 (and N GPUs as replicas).
+
+Workload (the soft-gradient batch configuration, seeded synthetic stand-in for the
+reference's protein fixtures): 100,000 homologous protein pairs over a 20-letter alphabet,
+A of length U[100, 500], B = A with 30 % substitutions and indels at rate 0.05 per position
+(geometric lengths, mean 3), plus 100,000 decoys (B shuffled); a symmetric integer matrix
+(off-diagonal U{-4..3}, diagonal U{4..11}), gap_open 11, gap_extend 1 on both sides.  One
+step = pos.score_and_grad() + neg.score_and_grad() + the contrastive margin gradient
+pos.compute_grad() - neg.compute_grad(), float32 DP.  GCUPS = sum of len(a) * len(b) over
+both batches / step time (the reference's cell definition, tools/fleetbench/arm.py:317).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints one JSON line (rank 0).  Under torchrun every rank aligns its own copy of the
+workload (weak scaling) and the margin gradients are summed over ranks (NCCL all-reduce).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+AA = "ACDEFGHIKLMNPQRSTVWY"
+OPS_PER_CELL_SOFT = 32.0          # soft affine: ~10 forward + ~22 backward/gradient FP32 ops
+OPS_PER_CELL_HARD = 22.0          # hard affine: 13 FP32 + 9 compare/select
+FP32_LANE_OPS_PEAK = 148 * 128 * 1.965e9   # ops/s at the maximum SM clock
+
+
+# ── workload ─────────────────────────────────────────────────────────────────
+def c2_matrix(rng):
+    m = rng.integers(-4, 4, size=(20, 20)).astype(np.float64)
+    m = np.triu(m) + np.triu(m, 1).T
+    m[np.diag_indices(20)] = rng.integers(4, 12, size=20)
+    return m
+
+
+def _mutate_codes(rng, a, freqs, sub=0.30, indel=0.05):
+    """B from A: substitutions at rate `sub`, indels at rate `indel` per position (half
+    insertions, half deletions), lengths geometric with mean 3."""
+    L = a.size
+    b = a.copy()
+    s = rng.random(L) < sub
+    b[s] = rng.choice(20, size=int(s.sum()), p=freqs)
+    ev = np.nonzero(rng.random(L) < indel)[0]
+    if ev.size == 0:
+        return b
+    parts = []
+    prev = 0
+    for pos in ev:
+        if pos < prev:
+            continue
+        k = int(rng.geometric(1.0 / 3.0))
+        if rng.random() < 0.5:   # insertion after pos
+            parts.append(b[prev:pos + 1])
+            parts.append(rng.choice(20, size=k, p=freqs).astype(np.uint8))
+            prev = pos + 1
+        else:                    # deletion of k residues from pos
+            parts.append(b[prev:pos])
+            prev = min(L, pos + k)
+    parts.append(b[prev:])
+    return np.concatenate(parts).astype(np.uint8)
+
+
+def c2_workload(n_pairs, seed=1):
+    """(mat, codes_a, off_a, codes_b_pos, off_b_pos, codes_b_neg, off_b_neg)."""
+    cache = os.path.join("/tmp", f"nwgrad_b200_c2_{n_pairs}_{seed}.npz")
+    if os.path.exists(cache):
+        z = np.load(cache)
+        return tuple(z[k] for k in ("mat", "a", "oa", "bp", "obp", "bn", "obn"))
+    rng = np.random.default_rng(seed)
+    freqs = rng.dirichlet(np.full(20, 5.0))
+    mat = c2_matrix(rng)
+    la = rng.integers(100, 501, size=n_pairs)
+    oa = np.zeros(n_pairs + 1, np.int64)
+    oa[1:] = np.cumsum(la)
+    a = rng.choice(20, size=int(oa[-1]), p=freqs).astype(np.uint8)
+    bs = [_mutate_codes(rng, a[oa[p]:oa[p + 1]], freqs) for p in range(n_pairs)]
+    obp = np.zeros(n_pairs + 1, np.int64)
+    obp[1:] = np.cumsum([x.size for x in bs])
+    bp = np.concatenate(bs)
+    bn = np.concatenate([rng.permutation(x) for x in bs])
+    obn = obp.copy()
+    try:
+        np.savez(cache, mat=mat, a=a, oa=oa, bp=bp, obp=obp, bn=bn, obn=obn)
+    except OSError:
+        pass
+    return mat, a, oa, bp, obp, bn, obn
+
+
+def cells_of(oa, ob):
+    return float(np.sum(np.diff(oa).astype(np.float64) * np.diff(ob).astype(np.float64)))
+
+
+# ── clocks ───────────────────────────────────────────────────────────────────
+class ClockSampler:
+    """nvidia-smi samples during the timed region (SM clock, max, throttle reasons)."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = max(mx, float(f[1]))
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[3 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ── the reference's CPU path ─────────────────────────────────────────────────
+def cpu_reference(mat, a, oa, bp, obp, bn, obn, sample_pairs, steps, warmup):
+    """Time the reference's own batch path (SeqPairBatchT<float>, soft, its default fill and
+    SIMD kernels, all physical host cores) on the first `sample_pairs` pairs of each batch,
+    in its own process (oracle/_ref/nwref_bench)."""
+    import oracle
+    if not oracle.ref_bench_available():
+        return None
+    k = sample_pairs
+    cells = cells_of(oa[:k + 1], obp[:k + 1]) + cells_of(oa[:k + 1], obn[:k + 1])
+    gaps = np.array([[11.0, 1.0, 11.0, 1.0]])
+    tp, _, threads, isa = oracle.ref_time_codes(32, 1, 0, 2, AA, mat[None], gaps, a, oa[:k + 1], bp, obp[:k + 1],
+                                                warmup=warmup, reps=steps)
+    tn, _, _, _ = oracle.ref_time_codes(32, 1, 0, 2, AA, mat[None], gaps, a, oa[:k + 1], bn, obn[:k + 1],
+                                        warmup=warmup, reps=steps)
+    per_step = tp + tn
+    return {"cells": cells, "seconds": per_step.tolist(), "threads": threads, "isa": isa,
+            "value": cells / float(np.min(per_step)) / 1e9}
+
+
+def cpu_model():
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+# ── main ─────────────────────────────────────────────────────────────────────
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--pairs", type=int, default=100000, help="pairs per batch (positives; as many decoys)")
+    ap.add_argument("--cpu-sample", type=int, default=4000, help="pairs per batch in the CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    mat, a, oa, bp, obp, bn, obn = c2_workload(args.pairs, seed=1)
+    cells = cells_of(oa, obp) + cells_of(oa, obn)
+    config = {"workload": "soft-gradient global affine batch, float32 DP: 100k homologous protein pairs "
+                          "(L 100-500, 30% subs, indels 0.05) + 100k shuffled decoys, margin gradient",
+              "pairs": 2 * args.pairs, "cells_per_step": cells, "alphabet": 20, "gap_open": 11,
+              "gap_extend": 1, "l2": "inputs+scratch > L2 and a 256 MiB L2 flush between timed steps",
+              "parallelism": f"replicas x{world}"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        r = cpu_reference(mat, a, oa, bp, obp, bn, obn, args.cpu_sample, max(args.steps, 1),
+                          max(args.warmup, 1))
+        if r is None:
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libnwref.so is not built"}))
+            return
+        v = r["value"]
+        best = float(np.min(r["seconds"]))
+        print(json.dumps({
+            "impl": "reference", "metric": "soft-grad batch GCUPS", "value": v, "unit": "GCUPS",
+            "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "ms_per_step": best * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded)", "config": dict(config, cpu_sample_pairs=2 * args.cpu_sample),
+            "cpu_baseline": {"value": v, "unit": "GCUPS", "cores": r["threads"], "kind": "reference",
+                             "sample": f"{2 * args.cpu_sample} pairs ({r['cells']:.3g} cells) of the workload, "
+                                       f"best of {len(r['seconds'])}, {cpu_model()}, isa {r['isa']}"},
+            "e2e": {"value": v, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
+
+    import torch
+    import nwgrad_b200 as nw
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    params = nw.AlignParams.from_arrays(mat[None], [[11.0, 1.0, 11.0, 1.0]], alphabet=nw.AA20)
+    pos = nw.SeqPairBatch.from_codes(a, oa, bp, obp, params, grad_mode="soft", device=local)
+    neg = nw.SeqPairBatch.from_codes(a, oa, bn, obn, params, grad_mode="soft", device=local)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+
+    def step():
+        pos.score_and_grad()
+        neg.score_and_grad()
+        g = pos.compute_grad() - neg.compute_grad()
+        return g
+
+    def allreduce(g):
+        if dist is None:
+            return g
+        t = torch.tensor(np.concatenate([g.matrices.ravel(), g.gaps.ravel()]), dtype=torch.float64,
+                         device=f"cuda:{local}")
+        dist.all_reduce(t)
+        return g
+
+    for _ in range(max(args.warmup, 3)):
+        allreduce(step())
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    kernel_ms = 0.0
+    launches = 0
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.zero_()                        # L2 flush, outside the timed events
+            torch.cuda.synchronize()
+            ev[k][0].record()
+            allreduce(step())
+            ev[k][1].record()
+            for b in (pos, neg):
+                ms_b, l_b = b.last_timing()
+                kernel_ms += ms_b
+                launches += l_b
+            launches += 4                        # two reductions per compute_grad
+        torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    step_ms = [e[0].elapsed_time(e[1]) for e in ev]
+    total_ms = float(np.sum(step_ms))
+    if dist is not None:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * cells * args.steps / (total_ms / 1e3) / 1e9
+
+    # end to end through the public API: host codes uploaded, aligned, gradient read back
+    e2e = None
+    if not args.no_e2e:
+        h2d = int(a.nbytes + bp.nbytes + bn.nbytes + 3 * oa.nbytes)
+        gs = params.num_sets * (20 * 20 + 4)
+        d2h = int(2 * gs * 8 + 8)
+        e2e_ms = []
+        for k in range(max(1, min(args.steps, 3))):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            p_ = nw.SeqPairBatch.from_codes(a, oa, bp, obp, params, grad_mode="soft", device=local)
+            n_ = nw.SeqPairBatch.from_codes(a, oa, bn, obn, params, grad_mode="soft", device=local)
+            s = p_.score_and_grad() - n_.score_and_grad()
+            g = p_.compute_grad() - n_.compute_grad()
+            allreduce(g)
+            torch.cuda.synchronize()
+            e2e_ms.append((time.perf_counter() - t0) * 1e3)
+            del p_, n_
+        em = float(np.min(e2e_ms))
+        if dist is not None:
+            t = torch.tensor([em], dtype=torch.float64, device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            em = float(t.item())
+        e2e = {"value": world * cells / (em / 1e3) / 1e9, "unit": "GCUPS", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "ms_per_step": em,
+               "path": "SeqPairBatch.from_codes (host codes -> HBM) + score_and_grad + compute_grad"}
+
+    clocks = clk.summary()
+    # roofline of the soft kernel: algorithmic FP32 ops per cell over the kernels' device time
+    kernel_s = kernel_ms / 1e3
+    ach = cells * args.steps * OPS_PER_CELL_SOFT / kernel_s / 1e12 if kernel_s > 0 else None
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "soft_kernel_traffic.json")
+    if os.path.exists(tpath):
+        try:
+            tj = json.load(open(tpath))
+            traffic = float(tj["bytes_per_cell"]) * cells / 2.0   # per launch (one batch)
+        except (OSError, ValueError, KeyError):
+            traffic = None
+    roofline = {"bound": "alu", "achieved": ach, "peak": FP32_LANE_OPS_PEAK / 1e12, "unit": "TOP/s",
+                "frac": (ach / (FP32_LANE_OPS_PEAK / 1e12)) if ach else None, "traffic": traffic,
+                "peak_note": "FP32 lane-op peak 148 SM x 128 lanes x 1.965 GHz (the recurrence is max-plus / "
+                             "sum-product: no tensor-core contraction)",
+                "ops_per_cell": OPS_PER_CELL_SOFT, "kernel_ms_per_step": kernel_ms / args.steps}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r = cpu_reference(mat, a, oa, bp, obp, bn, obn, args.cpu_sample, 2, 1)
+        if r is not None:
+            cpu = {"value": r["value"], "unit": "GCUPS", "cores": r["threads"], "kind": "reference",
+                   "sample": f"{2 * args.cpu_sample} pairs ({r['cells']:.3g} cells) of the workload, best of "
+                             f"{len(r['seconds'])}, {cpu_model()}, isa {r['isa']}"}
+    if rank == 0:
+        print(json.dumps({
+            "metric": "soft-grad batch GCUPS", "value": value, "unit": "GCUPS", "n_gpus": world,
+            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded)", "config": config, "e2e": e2e, "roofline": roofline,
+            "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches // max(args.steps, 1) * args.steps,
+            "step_ms": step_ms}))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,108 @@
+/* nwgrad_b200 -- C ABI of the B200 SeqPairBatch alignment path.
+ *
+ * One opaque store holds a batch of sequence pairs resident on one GPU (encoded codes,
+ * offsets, tracks), its parameters and its per-pair results; every entry point takes plain
+ * pointers and sizes and returns a status (0 = NWG_OK).  No C++ exception crosses this
+ * boundary; nwg_last_error() describes the last failure on the calling thread.
+ *
+ * Each entry point replaces one call of the reference's batch engine
+ * (michalsta/nwgrad, src/nwgrad/cpp/nwgrad/batch_engine.hpp), cited beside it.
+ */
+#ifndef NWGRAD_B200_H
+#define NWGRAD_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    NWG_OK = 0,
+    NWG_EINVAL = 1,    /* bad argument (a foreign code, a track entry out of range, ...) -> ValueError */
+    NWG_ECUDA = 2,     /* a CUDA call failed */
+    NWG_ENOMEM = 3,    /* device memory exhausted */
+    NWG_ESTATE = 4,    /* results not computed / no guide -> RuntimeError */
+    NWG_ERANGE = 5     /* soft path: a pair does not fit the scaled forward-backward -> ValueError */
+};
+
+typedef struct nwg_store nwg_store;
+
+typedef struct nwg_job {
+    int gap_model;     /* 0 linear, 1 affine */
+    int mode;          /* 0 global, 1 local */
+    int grad_mode;     /* 0 none (score only), 1 hard, 2 soft */
+    int precision;     /* 32 float32 DP, 64 float64 DP */
+    int band;          /* -1: full DP; >= 1: guide-banded re-alignment of this half-width */
+    int keep_paths;    /* hard: also keep every pair's path (moves) */
+    double temperature;/* soft: T > 0 */
+    int soft_double;   /* soft, precision 32: 0 float32 pass first (refused pairs rerun in double), 1 double only */
+    int lanes;         /* 0 auto; else lanes per pair (1 or 32) for every pair (tuning) */
+    int rows;          /* 0 auto; else rows per lane (tuning) */
+} nwg_job;
+
+/* Last error message of the calling thread ("" if none). */
+const char* nwg_last_error(void);
+
+/* Build a store: upload n_pairs pairs (codes of A and B, concatenated, with n_pairs + 1
+ * int64 offsets each), every code < nalpha.  tracks: per residue of A (off_a offsets) or
+ * NULL; gap_tracks: per DP row, m + 1 per pair at off_a[p] + p, or NULL.
+ * Replaces BatchEngine's constructor (batch_engine.hpp:284-350). */
+int nwg_store_create(const uint8_t* codes_a, const int64_t* off_a, const uint8_t* codes_b,
+                     const int64_t* off_b, int64_t n_pairs, int nalpha, const uint16_t* tracks,
+                     const uint16_t* gap_tracks, int device, nwg_store** out);
+int nwg_store_destroy(nwg_store* s);
+
+/* Parameters: K stacked N x N matrices (row-major) and K x 4 gaps (open_a, extend_a,
+ * open_b, extend_b), copied.  Invalidates results, keeps guides.
+ * Replaces BatchEngine::set_params (batch_engine.hpp:597-606). */
+int nwg_params_set(nwg_store* s, const double* mats, const double* gaps, int K, int N);
+
+/* Align every pair: scores, guides and (grad_mode 1/2) per-pair gradients, cached in the
+ * store; *total = the sum of scores in pair order.  job->band >= 1 re-aligns inside a band
+ * around each pair's stored guide.  stream: a cudaStream_t (NULL = the default stream).
+ * Replaces BatchEngine::score_and_grad (batch_engine.hpp:615-629) and banded_grad (:633-653). */
+int nwg_run(nwg_store* s, const nwg_job* job, void* stream, double* total);
+
+/* Per-pair scores (n_pairs doubles).  Replaces BatchEngine::scores (batch_engine.hpp:689). */
+int nwg_scores(nwg_store* s, double* out);
+
+/* Per-pair gradients, n_pairs x (K*N*N + 4K) doubles: the K matrices then K x 4 gaps.
+ * Replaces BatchEngine::grads_into (batch_engine.hpp:722-746). */
+int nwg_grads(nwg_store* s, double* out);
+
+/* sum_p w[p] * grad_p (w NULL: plain sum) into out (K*N*N + 4K doubles), in fixed blocks of
+ * 4096 pairs: each block in pair order, the blocks in order -- the reference's order, so
+ * bit-identical for identical per-pair gradients.
+ * Replaces BatchEngine::weighted_grad / compute_grad (batch_engine.hpp:703-718, 1788-1827). */
+int nwg_reduce(nwg_store* s, const double* w, double* out);
+
+/* Guides (guide_j: m + 1 ints per pair at off_a[p] + p), read and written.
+ * Replace SeqPair::guide_j (seq_pair_batch.hpp:236) and the guide a banded call bands around. */
+int nwg_guides(nwg_store* s, int32_t* out);
+int nwg_set_guides(nwg_store* s, const int32_t* in);
+
+/* Compute every pair's guide under the given parameters (a snapshot: the params a soft
+ * pass scored) with the hard fill, leaving the store's parameters and results untouched.
+ * Replaces the deferred-guide resolution of the soft path (batch_soft_defer.inl:1-60, 241). */
+int nwg_resolve_guides(nwg_store* s, const double* mats, const double* gaps, const nwg_job* job,
+                       void* stream);
+
+/* Kept paths (job.keep_paths): per pair the walk-order moves (0 M, 1 gap in B, 2 gap in A),
+ * concatenated at the offsets given by path_info; path_info: n_pairs x 3 int32 = number of
+ * moves, start_i, start_j; ends: n_pairs x 2 = end_i, end_j.
+ * Replaces the stored path of BatchEngine (batch_engine.hpp:515-590). */
+int nwg_paths(nwg_store* s, int64_t* moves_off, uint8_t* moves, int64_t moves_cap,
+              int32_t* path_info, int32_t* ends);
+
+/* Per-pair status of the last run: 0 ok, 1 refused by the float32 soft pass and rerun in
+ * double, 2 out of range in double too.  Mirrors the kF32Refused flag (batch_engine.hpp:1285). */
+int nwg_status(nwg_store* s, int32_t* out);
+
+/* Device time (ms) of the last nwg_run's kernels and how many kernels it launched. */
+int nwg_last_timing(nwg_store* s, double* ms, int64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NWGRAD_B200_H */

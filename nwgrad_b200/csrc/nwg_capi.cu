@@ -1,0 +1,891 @@
+// nwgrad_b200: the C ABI (include/nwgrad_b200.h) over the sm_100a kernels.
+//
+// The store keeps a batch resident in HBM: codes and offsets uploaded once, parameters cast
+// to the DP precision once per set_params, per-pair results (scores, end cells, guides,
+// gradients) kept on the device until read.  nwg_run plans the batch once per problem shape
+// (pairs sorted into length buckets, each bucket a launch of one kernel geometry: one lane
+// per pair for short pairs, one warp per pair otherwise) and replays the plan on every call.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <numeric>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/nwgrad_b200.h"
+#include "nwg_common.cuh"
+#include "nwg_hard.cuh"
+#include "nwg_soft.cuh"
+
+namespace {
+
+thread_local std::string g_err;
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define NWG_CUDA(call)                                                                     \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            throw Error(e_ == cudaErrorMemoryAllocation ? NWG_ENOMEM : NWG_ECUDA,          \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));               \
+    } while (0)
+
+// A device buffer that only grows.
+struct DBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    void need(size_t n) {
+        if (n <= bytes) return;
+        if (p) cudaFree(p);
+        p = nullptr; bytes = 0;
+        NWG_CUDA(cudaMalloc(&p, std::max<size_t>(n, 256)));
+        bytes = std::max<size_t>(n, 256);
+    }
+    void release() { if (p) cudaFree(p); p = nullptr; bytes = 0; }
+    template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+// ── reductions ────────────────────────────────────────────────────────────────
+// The reference's blocked sum: block b sums w[p] * g[p][k] over its pairs in pair order from
+// 0.0 (a product, then an add: no fused multiply-add), then the blocks are added in order.
+__global__ void blocked_partial_kernel(const double* __restrict__ g, const double* __restrict__ w,
+                                       int64_t n_pairs, int64_t gs, int64_t block, double* part) {
+    const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int64_t b = blockIdx.y;
+    if (k >= gs) return;
+    const int64_t p0 = b * block, p1 = min(n_pairs, p0 + block);
+    double acc = 0.0;
+    if (w) for (int64_t p = p0; p < p1; ++p) acc = __dadd_rn(acc, __dmul_rn(w[p], g[p * gs + k]));
+    else   for (int64_t p = p0; p < p1; ++p) acc = __dadd_rn(acc, g[p * gs + k]);
+    part[b * gs + k] = acc;
+}
+__global__ void blocked_total_kernel(const double* __restrict__ part, int64_t nblocks, int64_t gs,
+                                     double* out) {
+    const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= gs) return;
+    double t = 0.0;
+    for (int64_t b = 0; b < nblocks; ++b) t = __dadd_rn(t, part[b * gs + k]);
+    out[k] = t;
+}
+
+// Tracked Global/Local: the column-0 border per DP row by runs of bitwise-equal extends
+// (aligner.hpp:1986-2006), one thread per pair.
+template <class T, bool AFF>
+__global__ void bx0_kernel(const int64_t* oa, int64_t n_pairs, const uint16_t* tracks,
+                           const T* gapsT, T* bx0) {
+    const int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= n_pairs) return;
+    const int64_t ao = oa[p];
+    const int m = int(oa[p + 1] - ao);
+    const uint16_t* tk = tracks + ao;
+    T* out = bx0 + ao + p;
+    out[0] = T(0);
+    if (m == 0) return;
+    const T go = gapsT[4 * tk[0] + 2];
+    T csum = T(0);
+    int s = 1;
+    T prev = T(0);
+    for (int i = 1; i <= m; ++i) {
+        const T ge = gapsT[4 * tk[i - 1] + 3];
+        if (i > 1) {
+            bool differ;
+            if constexpr (sizeof(T) == 4) differ = __float_as_uint(float(ge)) != __float_as_uint(float(prev));
+            else differ = __double_as_longlong(double(ge)) != __double_as_longlong(double(prev));
+            if (differ) {
+                csum = (s == 1) ? nwg::mul_rn(static_cast<T>(i - 1), prev)
+                                : nwg::add_rn(csum, nwg::mul_rn(static_cast<T>(i - s), prev));
+                s = i;
+            }
+        }
+        if constexpr (AFF)
+            out[i] = (s == 1) ? -nwg::add_rn(go, nwg::mul_rn(static_cast<T>(i), ge))
+                              : -nwg::add_rn(go, nwg::add_rn(csum, nwg::mul_rn(static_cast<T>(i - s + 1), ge)));
+        else
+            out[i] = (s == 1) ? nwg::mul_rn(-static_cast<T>(i), ge)
+                              : -nwg::add_rn(csum, nwg::mul_rn(static_cast<T>(i - s + 1), ge));
+        prev = ge;
+    }
+}
+
+__global__ void mark_status_kernel(const int32_t* order, int64_t n, int32_t* status, int32_t v) {
+    const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k < n) status[order[k]] = v;
+}
+
+int sm_count(int dev) {
+    int v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    return v > 0 ? v : 148;
+}
+
+// ── kernel tables ─────────────────────────────────────────────────────────────
+using HardFn = void (*)(const nwg::HardArgs);
+using SoftFn = void (*)(const nwg::SoftArgs);
+
+struct Geo { int G, R; };
+// Geometries compiled: one lane per pair (short pairs) and one warp per pair.
+constexpr Geo kHardGeos[] = {{1, 8}, {1, 16}, {1, 24}, {1, 32}, {32, 1}, {32, 2}, {32, 4}, {32, 8}};
+constexpr Geo kSoftGeos[] = {{1, 8}, {1, 16}, {1, 24}, {1, 32}, {32, 2}, {32, 4}, {32, 8}};
+
+template <class T, bool AFF, bool LOC, bool TR>
+HardFn hard_fn(Geo g) {
+#define NWG_H(GG, RR) if (g.G == GG && g.R == RR) return &nwg::hard_fill_kernel<T, AFF, LOC, TR, GG, RR>;
+    NWG_H(1, 8) NWG_H(1, 16) NWG_H(1, 24) NWG_H(1, 32) NWG_H(32, 1) NWG_H(32, 2) NWG_H(32, 4) NWG_H(32, 8)
+#undef NWG_H
+    return nullptr;
+}
+template <class T>
+HardFn hard_fn_rt(bool aff, bool loc, bool tr, Geo g) {
+    if (aff) {
+        if (loc) return tr ? hard_fn<T, true, true, true>(g) : hard_fn<T, true, true, false>(g);
+        return tr ? hard_fn<T, true, false, true>(g) : hard_fn<T, true, false, false>(g);
+    }
+    if (loc) return tr ? hard_fn<T, false, true, true>(g) : hard_fn<T, false, true, false>(g);
+    return tr ? hard_fn<T, false, false, true>(g) : hard_fn<T, false, false, false>(g);
+}
+template <class T, bool AFF, bool LOC, bool TR>
+SoftFn soft_fn(Geo g) {
+#define NWG_S(GG, RR) if (g.G == GG && g.R == RR) return &nwg::soft_kernel<T, AFF, LOC, TR, GG, RR>;
+    NWG_S(1, 8) NWG_S(1, 16) NWG_S(1, 24) NWG_S(1, 32) NWG_S(32, 2) NWG_S(32, 4) NWG_S(32, 8)
+#undef NWG_S
+    return nullptr;
+}
+template <class T>
+SoftFn soft_fn_rt(bool aff, bool loc, bool tr, Geo g) {
+    if (aff) {
+        if (loc) return tr ? soft_fn<T, true, true, true>(g) : soft_fn<T, true, true, false>(g);
+        return tr ? soft_fn<T, true, false, true>(g) : soft_fn<T, true, false, false>(g);
+    }
+    if (loc) return tr ? soft_fn<T, false, true, true>(g) : soft_fn<T, false, true, false>(g);
+    return tr ? soft_fn<T, false, false, true>(g) : soft_fn<T, false, false, false>(g);
+}
+
+// Padded cells a geometry computes for an (m, n) problem over `rows` DP rows.
+double geo_cost(Geo g, int rows, int n, int extra_cols) {
+    const int GR = g.G * g.R;
+    const double stripes = std::ceil(double(rows) / GR);
+    return stripes * GR * double(n + extra_cols + g.G - 1);
+}
+
+// The geometry for one pair: a lane per pair when the rows fit one lane (up to 32 rows),
+// else the warp geometry that pads the fewest cells (ties: more rows per lane).
+Geo pick_geo(bool soft, int rows, int n, int lanes, int rpl, bool lane_ok) {
+    if (lanes == 1 || (lanes == 0 && lane_ok && rows <= 32)) {
+        int R = rpl;
+        if (!R) R = rows <= 8 ? 8 : rows <= 16 ? 16 : rows <= 24 ? 24 : 32;
+        return {1, R};
+    }
+    if (rpl) return {32, rpl};
+    Geo best{32, soft ? 4 : 4};
+    double bc = 1e300;
+    const int opts_h[] = {8, 4, 2, 1};
+    const int opts_s[] = {8, 4, 2};
+    const int* opts = soft ? opts_s : opts_h;
+    const int no = soft ? 3 : 4;
+    for (int k = 0; k < no; ++k) {
+        const Geo g{32, opts[k]};
+        // fewer rows per lane costs more shuffles per cell: weigh them in
+        const double c = geo_cost(g, rows, n, soft ? 1 : 0) * (1.0 + 0.75 / g.R);
+        if (c < bc) { bc = c; best = g; }
+    }
+    return best;
+}
+
+struct Bucket {
+    Geo geo;
+    std::vector<int32_t> pairs;
+    int64_t off = 0;           // into the store's order array
+    int maxn = 0;
+    int64_t max_soft_cells = 0;   // soft: max over pairs of nstripes * (n + G) * G * R
+};
+
+struct Plan {
+    bool valid = false;
+    int key_soft = -1, key_lanes = -1, key_rows = -1;
+    std::vector<Bucket> buckets;
+    std::vector<int64_t> code_off;   // hard: per pair
+    int64_t code_bytes = 0;
+};
+
+}  // namespace
+
+struct nwg_store {
+    int device = 0;
+    int64_t n = 0;
+    int nalpha = 0;
+    bool tracked_seq = false;   // tracks were given
+    int max_track = 0;          // the largest track / gap-track entry
+    std::vector<int64_t> oa, ob;
+    int64_t total_a = 0, total_b = 0;
+    DBuf a, b, doa, dob, tracks, gtracks;
+    // params
+    int K = 0, N = 0;
+    std::vector<double> mats, gaps;
+    DBuf matf, gapf, matd, gapd;       // Viterbi precision casts
+    DBuf bx0f, bx0d;                    // tracked column-0 borders
+    DBuf tmatf, tgapf, tmatd, tgapd, tbx0f, tbx0d, tscore, tend;   // a guide snapshot's copies
+    bool bx0f_ok = false, bx0d_ok = false;
+    // results
+    DBuf score, end, grad, guide, status, order, codes, code_off, scratch, part, red, moves, moves_off, path_info;
+    int64_t gstride = 0;
+    bool have_scores = false, have_grads = false, have_guides = false, have_paths = false;
+    int last_grad_mode = 0, last_gm = -1, last_am = -1, last_prec = 0;
+    Plan hard_plan, soft_plan;
+    std::vector<int32_t> h_status;
+    // timing
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double last_ms = 0;
+    int64_t last_launches = 0;
+    bool tracked() const { return tracked_seq || K > 1; }
+};
+
+namespace {
+
+void set_params_dev(nwg_store* s) {
+    const size_t nm = s->mats.size(), ng = s->gaps.size();
+    std::vector<float> mf(nm), gf(ng);
+    for (size_t k = 0; k < nm; ++k) mf[k] = static_cast<float>(s->mats[k]);
+    for (size_t k = 0; k < ng; ++k) gf[k] = static_cast<float>(s->gaps[k]);
+    s->matf.need(nm * 4); s->gapf.need(ng * 4);
+    s->matd.need(nm * 8); s->gapd.need(ng * 8);
+    NWG_CUDA(cudaMemcpy(s->matf.p, mf.data(), nm * 4, cudaMemcpyHostToDevice));
+    NWG_CUDA(cudaMemcpy(s->gapf.p, gf.data(), ng * 4, cudaMemcpyHostToDevice));
+    NWG_CUDA(cudaMemcpy(s->matd.p, s->mats.data(), nm * 8, cudaMemcpyHostToDevice));
+    NWG_CUDA(cudaMemcpy(s->gapd.p, s->gaps.data(), ng * 8, cudaMemcpyHostToDevice));
+    s->bx0f_ok = s->bx0d_ok = false;
+}
+
+template <class T>
+const T* ensure_bx0(nwg_store* s, bool aff, cudaStream_t st, bool& ok, DBuf& buf, const DBuf& gapsT) {
+    if (!s->tracked()) return nullptr;
+    const int64_t rows = s->total_a + s->n;
+    buf.need(size_t(rows) * sizeof(T));
+    if (!s->tracks.p) {
+        // K > 1 without tracks: every row is set 0 -- the untracked closed forms apply, but the
+        // kernels read the table: fill it the same way from an all-zero track.
+        s->tracks.need(size_t(std::max<int64_t>(s->total_a, 1)) * 2);
+        NWG_CUDA(cudaMemsetAsync(s->tracks.p, 0, size_t(std::max<int64_t>(s->total_a, 1)) * 2, st));
+    }
+    const int th = 128;
+    const int64_t bl = (s->n + th - 1) / th;
+    if (bl > 0) {
+        if (aff) bx0_kernel<T, true><<<unsigned(bl), th, 0, st>>>(s->doa.as<int64_t>(), s->n, s->tracks.as<uint16_t>(), gapsT.as<T>(), buf.as<T>());
+        else     bx0_kernel<T, false><<<unsigned(bl), th, 0, st>>>(s->doa.as<int64_t>(), s->n, s->tracks.as<uint16_t>(), gapsT.as<T>(), buf.as<T>());
+        NWG_CUDA(cudaGetLastError());
+        s->last_launches++;
+    }
+    ok = true;
+    return buf.as<T>();
+}
+
+void build_plan(nwg_store* s, Plan& P, bool soft, int lanes, int rpl, int elem_bytes) {
+    if (P.valid && P.key_soft == int(soft) && P.key_lanes == lanes && P.key_rows == rpl) return;
+    P = Plan{};
+    P.key_soft = soft; P.key_lanes = lanes; P.key_rows = rpl;
+    const int64_t n = s->n;
+    // one lane per pair keeps a K*N*N histogram per lane in shared memory (soft)
+    const bool lane_ok_soft = int64_t(s->K) * s->N * s->N * elem_bytes * 32 <= 48 * 1024;
+    std::map<std::pair<int, int>, int> idx;
+    std::vector<int> geo_of(n);
+    for (int64_t p = 0; p < n; ++p) {
+        const int m = int(s->oa[p + 1] - s->oa[p]), nb = int(s->ob[p + 1] - s->ob[p]);
+        const int rows = soft ? m + 1 : m;
+        const Geo g = pick_geo(soft, std::max(rows, 1), nb, lanes, rpl, soft ? lane_ok_soft : true);
+        auto key = std::make_pair(g.G, g.R);
+        auto itb = idx.find(key);
+        int bi;
+        if (itb == idx.end()) { bi = int(P.buckets.size()); idx[key] = bi; P.buckets.push_back(Bucket{g, {}, 0, 0, 0}); }
+        else bi = itb->second;
+        P.buckets[bi].pairs.push_back(int32_t(p));
+    }
+    std::vector<int32_t> order;
+    order.reserve(n);
+    if (!soft) P.code_off.assign(n + 1, 0);
+    for (auto& B : P.buckets) {
+        // longest first: the persistent groups then finish together
+        std::sort(B.pairs.begin(), B.pairs.end(), [&](int32_t x, int32_t y) {
+            const int64_t cx = (s->oa[x + 1] - s->oa[x]) * (s->ob[x + 1] - s->ob[x]);
+            const int64_t cy = (s->oa[y + 1] - s->oa[y]) * (s->ob[y + 1] - s->ob[y]);
+            return cx != cy ? cx > cy : x < y;
+        });
+        B.off = int64_t(order.size());
+        for (int32_t p : B.pairs) {
+            order.push_back(p);
+            const int m = int(s->oa[p + 1] - s->oa[p]), nb = int(s->ob[p + 1] - s->ob[p]);
+            B.maxn = std::max(B.maxn, nb);
+            const int GR = B.geo.G * B.geo.R;
+            if (soft) {
+                const int64_t st = (m + 1 + GR - 1) / GR;
+                B.max_soft_cells = std::max<int64_t>(B.max_soft_cells, st * (nb + B.geo.G) * GR);
+            }
+        }
+    }
+    if (!soft) {
+        // code tables: per pair nstripes * (n + G - 1) * G * R bytes, 16-byte aligned
+        int64_t off = 0;
+        for (auto& B : P.buckets)
+            for (int32_t p : B.pairs) {
+                const int m = int(s->oa[p + 1] - s->oa[p]), nb = int(s->ob[p + 1] - s->ob[p]);
+                const int GR = B.geo.G * B.geo.R;
+                const int64_t st = (m + GR - 1) / GR;
+                P.code_off[p] = off;
+                const int64_t bytes = (m && nb) ? st * (nb + B.geo.G - 1) * GR : 0;
+                off += (bytes + 15) & ~int64_t(15);
+            }
+        P.code_bytes = std::max<int64_t>(off, 16);
+    }
+    s->order.need(size_t(std::max<int64_t>(n, 1)) * 4);
+    if (n) NWG_CUDA(cudaMemcpy(s->order.p, order.data(), size_t(n) * 4, cudaMemcpyHostToDevice));
+    if (!soft) {
+        s->code_off.need(size_t(n + 1) * 8);
+        NWG_CUDA(cudaMemcpy(s->code_off.p, P.code_off.data(), size_t(n + 1) * 8, cudaMemcpyHostToDevice));
+    }
+    P.valid = true;
+}
+
+template <class T>
+void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, bool want_guide) {
+    const bool aff = J.gap_model == 1, loc = J.mode == 1, tr = s->tracked();
+    Plan& P = s->hard_plan;
+    build_plan(s, P, false, J.lanes, J.rows, sizeof(T));
+    s->codes.need(size_t(P.code_bytes));
+    const DBuf& matT = sizeof(T) == 4 ? s->matf : s->matd;
+    const DBuf& gapT = sizeof(T) == 4 ? s->gapf : s->gapd;
+    const T* bx0 = nullptr;
+    if (tr) {
+        if (sizeof(T) == 4) bx0 = reinterpret_cast<const T*>(ensure_bx0<float>(s, aff, st, s->bx0f_ok, s->bx0f, s->gapf));
+        else bx0 = reinterpret_cast<const T*>(ensure_bx0<double>(s, aff, st, s->bx0d_ok, s->bx0d, s->gapd));
+    }
+    s->score.need(size_t(std::max<int64_t>(s->n, 1)) * 8);
+    s->end.need(size_t(std::max<int64_t>(s->n, 1)) * 16);
+    const int sms = sm_count(s->device);
+    const size_t smem = (size_t(s->K) * s->N * s->N + 4 * size_t(s->K)) * sizeof(T);
+    // scratch: the stripe boundary row per group slot
+    int64_t max_slots = 0, max_stride = 0;
+    for (auto& B : P.buckets) {
+        const int gpb = 128 / B.geo.G;
+        const int64_t groups = int64_t(B.pairs.size());
+        const int64_t blocks = std::min<int64_t>((groups + gpb - 1) / gpb, int64_t(sms) * 16);
+        max_slots = std::max(max_slots, blocks * gpb);
+        max_stride = std::max<int64_t>(max_stride, 3 * (int64_t(B.maxn) + 1));
+    }
+    s->scratch.need(size_t(std::max<int64_t>(max_slots * max_stride, 1)) * sizeof(T));
+    for (auto& B : P.buckets) {
+        if (B.pairs.empty()) continue;
+        HardFn fn = hard_fn_rt<T>(aff, loc, tr, B.geo);
+        if (!fn) throw Error(NWG_EINVAL, "no kernel for this geometry");
+        if (smem > 48 * 1024) NWG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        nwg::HardArgs A{};
+        A.a = s->a.as<uint8_t>(); A.oa = s->doa.as<int64_t>();
+        A.b = s->b.as<uint8_t>(); A.ob = s->dob.as<int64_t>();
+        A.tracks = tr ? s->tracks.as<uint16_t>() : nullptr;
+        A.gtracks = tr ? s->gtracks.as<uint16_t>() : nullptr;
+        A.bx0 = bx0;
+        A.order = s->order.as<int32_t>() + B.off;
+        A.n_items = int64_t(B.pairs.size());
+        A.mat = matT.p; A.gaps = gapT.p; A.N = s->N; A.K = s->K;
+        A.codes = s->codes.as<uint8_t>(); A.code_off = s->code_off.as<int64_t>();
+        A.scratch = s->scratch.p; A.scratch_stride = max_stride;
+        A.score = s->score.as<double>(); A.end = s->end.as<int32_t>();
+        const int gpb = 128 / B.geo.G;
+        const int64_t blocks = std::min<int64_t>((A.n_items + gpb - 1) / gpb, int64_t(sms) * 16);
+        fn<<<unsigned(blocks), 128, smem, st>>>(A);
+        NWG_CUDA(cudaGetLastError());
+        s->last_launches++;
+    }
+    // traceback: gradient, guide, path
+    if (want_grad) { s->grad.need(size_t(s->n) * s->gstride * 8 + 8); }
+    if (want_guide) s->guide.need(size_t(s->total_a + s->n) * 4 + 4);
+    const bool keep = J.keep_paths != 0;
+    if (keep) {
+        std::vector<int64_t> mo(s->n + 1, 0);
+        for (int64_t p = 0; p < s->n; ++p) mo[p + 1] = mo[p] + (s->oa[p + 1] - s->oa[p]) + (s->ob[p + 1] - s->ob[p]);
+        s->moves.need(size_t(mo[s->n]) + 16);
+        s->moves_off.need(size_t(s->n + 1) * 8);
+        NWG_CUDA(cudaMemcpyAsync(s->moves_off.p, mo.data(), size_t(s->n + 1) * 8, cudaMemcpyHostToDevice, st));
+        NWG_CUDA(cudaStreamSynchronize(st));
+        s->path_info.need(size_t(s->n) * 12 + 12);
+    }
+    nwg::WalkArgs W{};
+    W.a = s->a.as<uint8_t>(); W.oa = s->doa.as<int64_t>();
+    W.b = s->b.as<uint8_t>(); W.ob = s->dob.as<int64_t>();
+    W.tracks = tr ? s->tracks.as<uint16_t>() : nullptr;
+    W.gtracks = tr ? s->gtracks.as<uint16_t>() : nullptr;
+    W.order = s->order.as<int32_t>(); W.n_items = s->n;
+    W.N = s->N; W.K = s->K; W.affine = aff; W.local = loc;
+    W.codes = s->codes.as<uint8_t>(); W.code_off = s->code_off.as<int64_t>();
+    W.end = s->end.as<int32_t>();
+    W.grad = want_grad ? s->grad.as<double>() : nullptr; W.gstride = s->gstride;
+    W.guide = want_guide ? s->guide.as<int32_t>() : nullptr;
+    W.moves = keep ? s->moves.as<uint8_t>() : nullptr;
+    W.moves_off = keep ? s->moves_off.as<int64_t>() : nullptr;
+    W.path_info = keep ? s->path_info.as<int32_t>() : nullptr;
+    if (s->n) {
+        nwg::walk_kernel<<<unsigned((s->n + 127) / 128), 128, 0, st>>>(W);
+        NWG_CUDA(cudaGetLastError());
+        s->last_launches++;
+    }
+}
+
+template <class T>
+void soft_weights(const nwg_store* s, const nwg_job& J, std::vector<T>& w, std::vector<T>& gw, bool& overflow) {
+    const int N = s->N, K = s->K, wc = N + 1;
+    const double invT = 1.0 / J.temperature;
+    w.assign(size_t(K * N + 1) * wc, T(0));
+    overflow = false;
+    auto cvt = [&](double x) {
+        const T v = static_cast<T>(x);
+        if (!std::isfinite(double(v))) overflow = true;
+        return v;
+    };
+    for (int r = 0; r < K * N; ++r)
+        for (int c = 0; c < N; ++c) w[size_t(r) * wc + c] = cvt(std::exp(s->mats[size_t(r) * N + c] * invT));
+    gw.assign(size_t(4) * K, T(0));
+    for (int k = 0; k < K; ++k) {
+        const double goa = s->gaps[4 * k], gea = s->gaps[4 * k + 1], gob = s->gaps[4 * k + 2], geb = s->gaps[4 * k + 3];
+        if (J.gap_model == 1) {
+            gw[4 * k + 0] = cvt(std::exp(-(goa + gea) * invT)); gw[4 * k + 1] = cvt(std::exp(-gea * invT));
+            gw[4 * k + 2] = cvt(std::exp(-(gob + geb) * invT)); gw[4 * k + 3] = cvt(std::exp(-geb * invT));
+        } else {
+            gw[4 * k + 0] = gw[4 * k + 1] = cvt(std::exp(-gea * invT));
+            gw[4 * k + 2] = gw[4 * k + 3] = cvt(std::exp(-geb * invT));
+        }
+    }
+}
+
+// One soft pass (precision T) over `pairs` (all pairs when null).
+template <class T>
+void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vector<int32_t>* subset) {
+    const bool aff = J.gap_model == 1, loc = J.mode == 1, tr = s->tracked();
+    std::vector<T> w, gw;
+    bool ovf;
+    soft_weights<T>(s, J, w, gw, ovf);
+    DBuf dw, dgw;   // small; freed at scope end
+    struct Free { DBuf& a; DBuf& b; ~Free() { a.release(); b.release(); } } fr{dw, dgw};
+    dw.need(w.size() * sizeof(T)); dgw.need(gw.size() * sizeof(T));
+    NWG_CUDA(cudaMemcpyAsync(dw.p, w.data(), w.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+    NWG_CUDA(cudaMemcpyAsync(dgw.p, gw.data(), gw.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+    Plan local_plan;
+    Plan* P;
+    std::vector<int32_t> order;
+    if (subset) {
+        // a plan over the subset only (double reruns): one bucket per geometry
+        P = &local_plan;
+        std::map<std::pair<int, int>, int> idx;
+        const bool lane_ok = int64_t(s->K) * s->N * s->N * sizeof(T) * 32 <= 48 * 1024;
+        for (int32_t p : *subset) {
+            const int m = int(s->oa[p + 1] - s->oa[p]), nb = int(s->ob[p + 1] - s->ob[p]);
+            const Geo g = pick_geo(true, m + 1, nb, J.lanes, J.rows, lane_ok);
+            auto key = std::make_pair(g.G, g.R);
+            auto itb = idx.find(key);
+            int bi;
+            if (itb == idx.end()) { bi = int(P->buckets.size()); idx[key] = bi; P->buckets.push_back(Bucket{g, {}, 0, 0, 0}); }
+            else bi = itb->second;
+            P->buckets[bi].pairs.push_back(p);
+        }
+        for (auto& B : P->buckets) {
+            B.off = int64_t(order.size());
+            for (int32_t p : B.pairs) {
+                order.push_back(p);
+                const int m = int(s->oa[p + 1] - s->oa[p]), nb = int(s->ob[p + 1] - s->ob[p]);
+                B.maxn = std::max(B.maxn, nb);
+                const int GR = B.geo.G * B.geo.R;
+                const int64_t stp = (m + 1 + GR - 1) / GR;
+                B.max_soft_cells = std::max<int64_t>(B.max_soft_cells, stp * (nb + B.geo.G) * GR);
+            }
+        }
+    } else {
+        P = &s->soft_plan;
+        build_plan(s, *P, true, J.lanes, J.rows, sizeof(T));
+    }
+    DBuf sub_order;
+    struct Free1 { DBuf& a; ~Free1() { a.release(); } } fr1{sub_order};
+    const int32_t* d_order = s->order.as<int32_t>();
+    if (subset) {
+        sub_order.need(order.size() * 4 + 4);
+        NWG_CUDA(cudaMemcpyAsync(sub_order.p, order.data(), order.size() * 4, cudaMemcpyHostToDevice, st));
+        d_order = sub_order.as<int32_t>();
+    }
+    const int sms = sm_count(s->device);
+    const int NV = aff ? 3 : 1;
+    for (auto& B : P->buckets) {
+        if (B.pairs.empty()) continue;
+        SoftFn fn = soft_fn_rt<T>(aff, loc, tr, B.geo);
+        if (!fn) throw Error(NWG_EINVAL, "no soft kernel for this geometry");
+        const int G = B.geo.G;
+        int block = 128;
+        const int K = s->K, N = s->N;
+        auto smem_for = [&](int blk) {
+            const int gpb = blk / G;
+            size_t b = size_t((K * N + 1) * (N + 1) + 4 * K) * sizeof(T);
+            b = (b + 15) & ~size_t(15);
+            if (tr) b += size_t(4 * K * gpb) * sizeof(double);
+            b += size_t(K) * N * N * gpb * sizeof(T);
+            return b;
+        };
+        while (block > 32 && smem_for(block) > 96 * 1024) block /= 2;
+        const size_t smem = smem_for(block);
+        if (smem > 227 * 1024) throw Error(NWG_EINVAL, "soft: the alphabet / parameter sets do not fit shared memory");
+        if (smem > 48 * 1024) NWG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        int occ = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, block, smem);
+        occ = std::max(occ, 1);
+        const int gpb = block / G;
+        const int64_t items = int64_t(B.pairs.size());
+        const int64_t blocks = std::min<int64_t>((items + gpb - 1) / gpb, int64_t(sms) * occ);
+        const int64_t slots = blocks * gpb;
+        const int64_t fwd_bytes = ((B.max_soft_cells * NV * int64_t(sizeof(T))) + 255) & ~int64_t(255);
+        const int64_t exp_bytes = ((B.max_soft_cells / B.geo.R) * 4 + 255) & ~int64_t(255);
+        const int64_t bnd_bytes = (int64_t(B.maxn) + 1) * (2 * NV * int64_t(sizeof(T)) + 8);
+        const int64_t stride = ((fwd_bytes + exp_bytes + bnd_bytes) + 255) & ~int64_t(255);
+        s->scratch.need(size_t(slots * stride));
+        nwg::SoftArgs A{};
+        A.a = s->a.as<uint8_t>(); A.oa = s->doa.as<int64_t>();
+        A.b = s->b.as<uint8_t>(); A.ob = s->dob.as<int64_t>();
+        A.tracks = tr ? s->tracks.as<uint16_t>() : nullptr;
+        A.gtracks = tr ? s->gtracks.as<uint16_t>() : nullptr;
+        A.order = d_order + B.off; A.n_items = items;
+        A.w = dw.p; A.gw = dgw.p; A.N = N; A.K = K;
+        A.scratch = s->scratch.p; A.scratch_stride = stride; A.fwd_bytes = fwd_bytes;
+        A.maxn = B.maxn; A.temperature = J.temperature;
+        A.score = s->score.as<double>(); A.grad = s->grad.as<double>(); A.gstride = s->gstride;
+        A.status = s->status.as<int32_t>();
+        if (ovf) {
+            // a weight overflows T: every pair of this bucket is out of range in T
+            mark_status_kernel<<<unsigned((items + 255) / 256), 256, 0, st>>>(A.order, items, A.status, 1);
+            NWG_CUDA(cudaGetLastError());
+            s->last_launches++;
+            continue;
+        }
+        fn<<<unsigned(blocks), block, smem, st>>>(A);
+        NWG_CUDA(cudaGetLastError());
+        s->last_launches++;
+    }
+}
+
+void run_soft(nwg_store* s, const nwg_job& J, cudaStream_t st) {
+    s->score.need(size_t(std::max<int64_t>(s->n, 1)) * 8);
+    s->grad.need(size_t(s->n) * s->gstride * 8 + 8);
+    s->status.need(size_t(std::max<int64_t>(s->n, 1)) * 4);
+    NWG_CUDA(cudaMemsetAsync(s->status.p, 0, size_t(std::max<int64_t>(s->n, 1)) * 4, st));
+    const bool f32 = J.precision == 32 && !J.soft_double;
+    if (f32) soft_pass<float>(s, J, st, nullptr);
+    else soft_pass<double>(s, J, st, nullptr);
+    s->h_status.assign(size_t(s->n), 0);
+    if (s->n) NWG_CUDA(cudaMemcpyAsync(s->h_status.data(), s->status.p, size_t(s->n) * 4, cudaMemcpyDeviceToHost, st));
+    NWG_CUDA(cudaStreamSynchronize(st));
+    std::vector<int32_t> refused;
+    for (int64_t p = 0; p < s->n; ++p) if (s->h_status[p]) refused.push_back(int32_t(p));
+    if (!refused.empty()) {
+        if (f32) {
+            soft_pass<double>(s, J, st, &refused);
+            std::vector<int32_t> hs(size_t(s->n));
+            NWG_CUDA(cudaMemcpyAsync(hs.data(), s->status.p, size_t(s->n) * 4, cudaMemcpyDeviceToHost, st));
+            NWG_CUDA(cudaStreamSynchronize(st));
+            for (int32_t p : refused) s->h_status[p] = hs[p] ? 2 : 1;
+        } else {
+            for (int32_t p : refused) s->h_status[p] = 2;
+        }
+        for (int32_t p : refused)
+            if (s->h_status[p] == 2) {
+                char buf[256];
+                std::snprintf(buf, sizeof buf,
+                              "nwgrad: soft path: pair %d (lengths %lld x %lld) does not fit the scaled "
+                              "probability-space forward-backward (a weight or a row overflows, typically a "
+                              "very low temperature or extreme scores)",
+                              p, (long long)(s->oa[p + 1] - s->oa[p]), (long long)(s->ob[p + 1] - s->ob[p]));
+                throw Error(NWG_ERANGE, buf);
+            }
+    }
+}
+
+template <class F>
+int guarded(F&& f) {
+    try {
+        f();
+        return NWG_OK;
+    } catch (const Error& e) {
+        g_err = e.what();
+        return e.code;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return NWG_EINVAL;
+    } catch (...) {
+        g_err = "unknown error";
+        return NWG_EINVAL;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* nwg_last_error(void) { return g_err.c_str(); }
+
+int nwg_store_create(const uint8_t* codes_a, const int64_t* off_a, const uint8_t* codes_b,
+                     const int64_t* off_b, int64_t n_pairs, int nalpha, const uint16_t* tracks,
+                     const uint16_t* gap_tracks, int device, nwg_store** out) {
+    return guarded([&] {
+        if (!out) throw Error(NWG_EINVAL, "out is null");
+        if (n_pairs < 0 || nalpha <= 0 || nalpha > 255) throw Error(NWG_EINVAL, "bad n_pairs / nalpha");
+        auto s = std::make_unique<nwg_store>();
+        s->device = device;
+        NWG_CUDA(cudaSetDevice(device));
+        s->n = n_pairs; s->nalpha = nalpha;
+        s->oa.assign(off_a, off_a + n_pairs + 1);
+        s->ob.assign(off_b, off_b + n_pairs + 1);
+        s->total_a = s->oa[n_pairs] - s->oa[0];
+        s->total_b = s->ob[n_pairs] - s->ob[0];
+        for (int64_t p = 0; p < n_pairs; ++p) {
+            if (s->oa[p + 1] < s->oa[p] || s->ob[p + 1] < s->ob[p]) throw Error(NWG_EINVAL, "offsets decrease");
+            if (s->oa[p + 1] - s->oa[p] > (1 << 30) || s->ob[p + 1] - s->ob[p] > (1 << 30))
+                throw Error(NWG_EINVAL, "sequence too long");
+        }
+        // rebase offsets to 0
+        const int64_t a0 = s->oa[0], b0 = s->ob[0];
+        for (auto& v : s->oa) v -= a0;
+        for (auto& v : s->ob) v -= b0;
+        for (int64_t k = 0; k < s->total_a; ++k)
+            if (codes_a[a0 + k] >= nalpha) throw Error(NWG_EINVAL, "code out of range in sequence A");
+        for (int64_t k = 0; k < s->total_b; ++k)
+            if (codes_b[b0 + k] >= nalpha) throw Error(NWG_EINVAL, "code out of range in sequence B");
+        s->a.need(size_t(s->total_a) + 16);
+        s->b.need(size_t(s->total_b) + 16);
+        if (s->total_a) NWG_CUDA(cudaMemcpy(s->a.p, codes_a + a0, size_t(s->total_a), cudaMemcpyHostToDevice));
+        if (s->total_b) NWG_CUDA(cudaMemcpy(s->b.p, codes_b + b0, size_t(s->total_b), cudaMemcpyHostToDevice));
+        s->doa.need(size_t(n_pairs + 1) * 8);
+        s->dob.need(size_t(n_pairs + 1) * 8);
+        NWG_CUDA(cudaMemcpy(s->doa.p, s->oa.data(), size_t(n_pairs + 1) * 8, cudaMemcpyHostToDevice));
+        NWG_CUDA(cudaMemcpy(s->dob.p, s->ob.data(), size_t(n_pairs + 1) * 8, cudaMemcpyHostToDevice));
+        if (tracks) {
+            s->tracked_seq = true;
+            s->tracks.need(size_t(std::max<int64_t>(s->total_a, 1)) * 2);
+            if (s->total_a) NWG_CUDA(cudaMemcpy(s->tracks.p, tracks + a0, size_t(s->total_a) * 2, cudaMemcpyHostToDevice));
+            for (int64_t k = 0; k < s->total_a; ++k) s->max_track = std::max<int>(s->max_track, tracks[a0 + k]);
+        }
+        if (gap_tracks) {
+            s->tracked_seq = true;
+            if (!tracks) {
+                // gap tracks alone: the track is all zero
+                s->tracks.need(size_t(std::max<int64_t>(s->total_a, 1)) * 2);
+                NWG_CUDA(cudaMemset(s->tracks.p, 0, size_t(std::max<int64_t>(s->total_a, 1)) * 2));
+            }
+            const int64_t rows = s->total_a + n_pairs;
+            s->gtracks.need(size_t(rows) * 2);
+            NWG_CUDA(cudaMemcpy(s->gtracks.p, gap_tracks + a0, size_t(rows) * 2, cudaMemcpyHostToDevice));
+            for (int64_t k = 0; k < rows; ++k) s->max_track = std::max<int>(s->max_track, gap_tracks[a0 + k]);
+        }
+        NWG_CUDA(cudaEventCreate(&s->ev0));
+        NWG_CUDA(cudaEventCreate(&s->ev1));
+        *out = s.release();
+    });
+}
+
+int nwg_store_destroy(nwg_store* s) {
+    return guarded([&] {
+        if (!s) return;
+        cudaSetDevice(s->device);
+        for (DBuf* b : {&s->a, &s->b, &s->doa, &s->dob, &s->tracks, &s->gtracks, &s->matf, &s->gapf, &s->matd,
+                        &s->gapd, &s->bx0f, &s->bx0d, &s->score, &s->end, &s->grad, &s->guide, &s->status,
+                        &s->order, &s->codes, &s->code_off, &s->scratch, &s->part, &s->red, &s->moves,
+                        &s->moves_off, &s->path_info, &s->tmatf, &s->tgapf, &s->tmatd, &s->tgapd,
+                        &s->tbx0f, &s->tbx0d, &s->tscore, &s->tend})
+            b->release();
+        if (s->ev0) cudaEventDestroy(s->ev0);
+        if (s->ev1) cudaEventDestroy(s->ev1);
+        delete s;
+    });
+}
+
+int nwg_params_set(nwg_store* s, const double* mats, const double* gaps, int K, int N) {
+    return guarded([&] {
+        if (!s || !mats || !gaps) throw Error(NWG_EINVAL, "null argument");
+        if (K < 1 || N < 1 || N != s->nalpha) throw Error(NWG_EINVAL, "params: alphabet size does not match the store");
+        if (s->K && (K != s->K)) throw Error(NWG_EINVAL, "set_params() cannot change the number of parameter sets");
+        NWG_CUDA(cudaSetDevice(s->device));
+        s->K = K; s->N = N;
+        s->mats.assign(mats, mats + size_t(K) * N * N);
+        s->gaps.assign(gaps, gaps + size_t(4) * K);
+        s->gstride = int64_t(K) * N * N + 4 * int64_t(K);
+        if (s->tracked_seq && s->max_track >= K)
+            throw Error(NWG_EINVAL, "nwgrad: a track entry (" + std::to_string(s->max_track) +
+                                        ") is not a parameter set (params has " + std::to_string(K) + ")");
+        set_params_dev(s);
+        s->have_scores = s->have_grads = s->have_paths = false;
+    });
+}
+
+int nwg_run(nwg_store* s, const nwg_job* job, void* stream, double* total) {
+    return guarded([&] {
+        if (!s || !job) throw Error(NWG_EINVAL, "null argument");
+        if (!s->K) throw Error(NWG_ESTATE, "params not set");
+        const nwg_job J = *job;
+        if (J.gap_model < 0 || J.gap_model > 1 || J.mode < 0 || J.mode > 1 || J.grad_mode < 0 || J.grad_mode > 2)
+            throw Error(NWG_EINVAL, "bad job");
+        if (J.precision != 32 && J.precision != 64) throw Error(NWG_EINVAL, "precision must be 32 or 64");
+        if (J.band >= 0) throw Error(NWG_EINVAL, "banded re-alignment is not available in this build");
+        NWG_CUDA(cudaSetDevice(s->device));
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        s->last_launches = 0;
+        NWG_CUDA(cudaEventRecord(s->ev0, st));
+        s->have_scores = s->have_grads = s->have_paths = false;
+        if (J.grad_mode == 2) {
+            run_soft(s, J, st);
+        } else {
+            const bool grad = J.grad_mode == 1;
+            if (J.precision == 32) run_hard<float>(s, J, st, grad, true);
+            else run_hard<double>(s, J, st, grad, true);
+            s->have_guides = true;
+            s->have_paths = J.keep_paths != 0;
+        }
+        NWG_CUDA(cudaEventRecord(s->ev1, st));
+        NWG_CUDA(cudaStreamSynchronize(st));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+        s->last_ms = ms;
+        s->have_scores = true;
+        s->have_grads = J.grad_mode != 0;
+        s->last_grad_mode = J.grad_mode; s->last_gm = J.gap_model; s->last_am = J.mode; s->last_prec = J.precision;
+        if (total) {
+            std::vector<double> sc(size_t(s->n));
+            if (s->n) NWG_CUDA(cudaMemcpy(sc.data(), s->score.p, size_t(s->n) * 8, cudaMemcpyDeviceToHost));
+            double t = 0.0;
+            for (double v : sc) t += v;
+            *total = t;
+        }
+    });
+}
+
+int nwg_resolve_guides(nwg_store* s, const double* mats, const double* gaps, const nwg_job* job, void* stream) {
+    return guarded([&] {
+        if (!s || !job || !mats || !gaps) throw Error(NWG_EINVAL, "null argument");
+        if (!s->K) throw Error(NWG_ESTATE, "params not set");
+        NWG_CUDA(cudaSetDevice(s->device));
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        nwg_job J = *job;
+        J.grad_mode = 0; J.keep_paths = 0; J.band = -1;
+        // the snapshot's parameters and scratch results, swapped in for the hard fill
+        std::vector<double> m0 = s->mats, g0 = s->gaps;
+        s->mats.assign(mats, mats + m0.size());
+        s->gaps.assign(gaps, gaps + g0.size());
+        std::swap(s->matf, s->tmatf); std::swap(s->gapf, s->tgapf);
+        std::swap(s->matd, s->tmatd); std::swap(s->gapd, s->tgapd);
+        std::swap(s->bx0f, s->tbx0f); std::swap(s->bx0d, s->tbx0d);
+        std::swap(s->score, s->tscore); std::swap(s->end, s->tend);
+        auto restore = [&] {
+            s->mats = m0; s->gaps = g0;
+            std::swap(s->matf, s->tmatf); std::swap(s->gapf, s->tgapf);
+            std::swap(s->matd, s->tmatd); std::swap(s->gapd, s->tgapd);
+            std::swap(s->bx0f, s->tbx0f); std::swap(s->bx0d, s->tbx0d);
+            std::swap(s->score, s->tscore); std::swap(s->end, s->tend);
+        };
+        try {
+            set_params_dev(s);
+            if (J.precision == 32) run_hard<float>(s, J, st, false, true);
+            else run_hard<double>(s, J, st, false, true);
+            NWG_CUDA(cudaStreamSynchronize(st));
+        } catch (...) { restore(); throw; }
+        restore();
+        s->have_guides = true;
+    });
+}
+
+int nwg_scores(nwg_store* s, double* out) {
+    return guarded([&] {
+        if (!s->have_scores) throw Error(NWG_ESTATE, "scores not computed; call score_and_grad() first");
+        if (s->n) NWG_CUDA(cudaMemcpy(out, s->score.p, size_t(s->n) * 8, cudaMemcpyDeviceToHost));
+    });
+}
+
+int nwg_grads(nwg_store* s, double* out) {
+    return guarded([&] {
+        if (!s->have_grads) throw Error(NWG_ESTATE, "gradient not computed; call score_and_grad() or banded_grad() first");
+        if (s->n) NWG_CUDA(cudaMemcpy(out, s->grad.p, size_t(s->n) * s->gstride * 8, cudaMemcpyDeviceToHost));
+    });
+}
+
+int nwg_reduce(nwg_store* s, const double* w, double* out) {
+    return guarded([&] {
+        if (!s->have_grads) throw Error(NWG_ESTATE, "gradient not computed; call score_and_grad() or banded_grad() first");
+        NWG_CUDA(cudaSetDevice(s->device));
+        const int64_t gs = s->gstride, n = s->n;
+        const int64_t B = 4096, nb = (n + B - 1) / B;
+        if (n == 0) { for (int64_t k = 0; k < gs; ++k) out[k] = 0.0; return; }
+        s->part.need(size_t(nb * gs) * 8);
+        s->red.need(size_t(gs) * 8 + size_t(w ? n : 0) * 8);
+        double* dw = nullptr;
+        if (w) {
+            dw = s->red.as<double>() + gs;
+            NWG_CUDA(cudaMemcpy(dw, w, size_t(n) * 8, cudaMemcpyHostToDevice));
+        }
+        dim3 grid(unsigned((gs + 127) / 128), unsigned(nb));
+        blocked_partial_kernel<<<grid, 128>>>(s->grad.as<double>(), dw, n, gs, B, s->part.as<double>());
+        NWG_CUDA(cudaGetLastError());
+        blocked_total_kernel<<<unsigned((gs + 127) / 128), 128>>>(s->part.as<double>(), nb, gs, s->red.as<double>());
+        NWG_CUDA(cudaGetLastError());
+        NWG_CUDA(cudaMemcpy(out, s->red.p, size_t(gs) * 8, cudaMemcpyDeviceToHost));
+    });
+}
+
+int nwg_guides(nwg_store* s, int32_t* out) {
+    return guarded([&] {
+        if (!s->have_guides) throw Error(NWG_ESTATE, "no guide: run score_and_grad() first");
+        const size_t k = size_t(s->total_a + s->n);
+        if (k) NWG_CUDA(cudaMemcpy(out, s->guide.p, k * 4, cudaMemcpyDeviceToHost));
+    });
+}
+
+int nwg_set_guides(nwg_store* s, const int32_t* in) {
+    return guarded([&] {
+        const size_t k = size_t(s->total_a + s->n);
+        s->guide.need(k * 4 + 4);
+        if (k) NWG_CUDA(cudaMemcpy(s->guide.p, in, k * 4, cudaMemcpyHostToDevice));
+        s->have_guides = true;
+    });
+}
+
+int nwg_paths(nwg_store* s, int64_t* moves_off, uint8_t* moves, int64_t moves_cap, int32_t* path_info,
+              int32_t* ends) {
+    return guarded([&] {
+        if (!s->have_paths) throw Error(NWG_ESTATE, "no stored path: score_and_grad(keep_paths=True) first");
+        std::vector<int64_t> mo(s->n + 1, 0);
+        for (int64_t p = 0; p < s->n; ++p) mo[p + 1] = mo[p] + (s->oa[p + 1] - s->oa[p]) + (s->ob[p + 1] - s->ob[p]);
+        if (moves_off) std::memcpy(moves_off, mo.data(), size_t(s->n + 1) * 8);
+        if (moves) {
+            if (moves_cap < mo[s->n]) throw Error(NWG_EINVAL, "moves buffer too small");
+            if (mo[s->n]) NWG_CUDA(cudaMemcpy(moves, s->moves.p, size_t(mo[s->n]), cudaMemcpyDeviceToHost));
+        }
+        if (path_info && s->n) NWG_CUDA(cudaMemcpy(path_info, s->path_info.p, size_t(s->n) * 12, cudaMemcpyDeviceToHost));
+        if (ends && s->n) {
+            std::vector<int32_t> e(size_t(s->n) * 4);
+            NWG_CUDA(cudaMemcpy(e.data(), s->end.p, e.size() * 4, cudaMemcpyDeviceToHost));
+            for (int64_t p = 0; p < s->n; ++p) { ends[2 * p] = e[4 * p]; ends[2 * p + 1] = e[4 * p + 1]; }
+        }
+    });
+}
+
+int nwg_status(nwg_store* s, int32_t* out) {
+    return guarded([&] {
+        for (int64_t p = 0; p < s->n; ++p) out[p] = p < int64_t(s->h_status.size()) ? s->h_status[p] : 0;
+    });
+}
+
+int nwg_last_timing(nwg_store* s, double* ms, int64_t* launches) {
+    return guarded([&] {
+        if (ms) *ms = s->last_ms;
+        if (launches) *launches = s->last_launches;
+    });
+}
+
+}  // extern "C"

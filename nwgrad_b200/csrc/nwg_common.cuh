@@ -1,0 +1,64 @@
+// Shared device helpers for the nwgrad_b200 kernels (sm_100a).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace nwg {
+
+// The reference's max: std::max keeps the first argument on ties and on a NaN second
+// argument: (a < b) ? b : a.  Kept as a compare + select (not fmaxf) so signed zeros and
+// NaNs propagate exactly as in the reference's scalar fill.
+template <class T> __device__ __forceinline__ T rmax(T a, T b) { return (a < b) ? b : a; }
+template <class T> __device__ __forceinline__ T rmax3(T a, T b, T c) { return rmax(rmax(a, b), c); }
+
+// The predecessor code of one state: 0 first argument (M), 1 second (X), 2 third (Y),
+// by >= in M, X, Y order (aligner.hpp:3977-3980).
+template <class T> __device__ __forceinline__ uint32_t pick3(T vm, T vx, T vy) {
+    const uint32_t kxy = vx >= vy ? 1u : 2u;
+    return vm >= rmax(vx, vy) ? 0u : kxy;
+}
+
+// Round-to-nearest multiply and add that the compiler never fuses into an FMA (the
+// reference is compiled with -ffp-contract=off: its closed-form borders round twice).
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+
+template <class T> __device__ __forceinline__ T ninf();
+template <> __device__ __forceinline__ float ninf<float>() { return __int_as_float(0xff800000u); }
+template <> __device__ __forceinline__ double ninf<double>() { return __longlong_as_double(0xfff0000000000000ull); }
+
+// Exact powers of two for the soft path's exponent bookkeeping: 2^e, flushed to 0 below
+// the normal range and to +inf above it.
+template <class T> __device__ __forceinline__ T pow2i(int e);
+template <> __device__ __forceinline__ float pow2i<float>(int e) {
+    if (e < -126) return 0.0f;
+    if (e > 127) return __int_as_float(0x7f800000);
+    return __int_as_float((e + 127) << 23);
+}
+template <> __device__ __forceinline__ double pow2i<double>(int e) {
+    if (e < -1022) return 0.0;
+    if (e > 1023) return __longlong_as_double(0x7ff0000000000000ll);
+    return __longlong_as_double(static_cast<long long>(e + 1023) << 52);
+}
+// floor(log2(x)) for a finite x > 0 (normal or subnormal handled via the bits).
+template <class T> __device__ __forceinline__ int ilog2(T x);
+template <> __device__ __forceinline__ int ilog2<float>(float x) {
+    const uint32_t u = __float_as_uint(x);
+    const int e = int((u >> 23) & 0xff);
+    if (e) return e - 127;
+    return -127 - __clz(u << 9);   // subnormal: position of the top set mantissa bit
+}
+template <> __device__ __forceinline__ int ilog2<double>(double x) {
+    const unsigned long long u = __double_as_longlong(x);
+    const int e = int((u >> 52) & 0x7ff);
+    if (e) return e - 1023;
+    return -1023 - __clzll(static_cast<long long>(u << 12));
+}
+__device__ __forceinline__ bool is_finite(float x) { return (__float_as_uint(x) & 0x7f800000u) != 0x7f800000u; }
+__device__ __forceinline__ bool is_finite(double x) {
+    return (static_cast<unsigned long long>(__double_as_longlong(x)) & 0x7ff0000000000000ull) != 0x7ff0000000000000ull;
+}
+
+}  // namespace nwg

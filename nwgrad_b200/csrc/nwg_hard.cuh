@@ -1,0 +1,452 @@
+// Hard (Viterbi) path: the guide-free full fill with predecessor codes, and the traceback.
+//
+// Fill.  A group of G lanes owns one pair; DP rows are cut into stripes of G*R rows and
+// lane g of the group owns rows [g*R, g*R + R) of the current stripe, its R cells of one
+// column held in registers.  Lanes run skewed by one column (a wavefront): at step t lane
+// g fills column j = t - g + 1, reading the row above from lane g-1 by a warp shuffle
+// (lane 0: from the previous stripe's bottom row in scratch, or the row-0 border).  G = 1
+// is the one-pair-per-lane ("inter-pair") kernel for short pairs; G = 32 one warp per pair.
+//
+// Every cell is the reference recurrence, expression for expression
+// (aligner.hpp:3955-4071 affine, 3756-3860 linear): (v - go) - ge left-associated, the
+// first-largest max, >= tie-breaks in M > X > Y order, parameters cast to T once.  The
+// evaluation order across cells differs, but each cell is a fixed expression of its three
+// neighbours, so the tables are bit-identical.
+//
+// Codes: one byte per cell, affine M | X << 2 | Y << 4, linear 0 diag / 1 up / 2 left with
+// 3 = stop (Local, value <= 0).  Layout per pair, per stripe s:
+//   byte ((s * S + t) * G + g) * R + r,  S = n + G - 1 steps,
+// the R cells a lane fills in one step contiguous, so every step is one coalesced store
+// per group.  Border cells (row 0, column 0) are not stored: the walk knows them.
+#pragma once
+#include "nwg_common.cuh"
+
+namespace nwg {
+
+struct HardArgs {
+    const uint8_t* a; const int64_t* oa;       // codes of A, n_pairs + 1 offsets
+    const uint8_t* b; const int64_t* ob;
+    const uint16_t* tracks;                    // per residue of A (oa offsets), or null
+    const uint16_t* gtracks;                   // per DP row (oa[p] + p offsets), or null
+    const void* bx0;                           // tracked: column-0 border per row (oa[p] + p), T
+    const int32_t* order;                      // the pairs of this launch
+    int64_t n_items;
+    const void* mat;                           // K*N*N in T
+    const void* gaps;                          // K*4 in T
+    int N, K;
+    uint8_t* codes; const int64_t* code_off;   // per pair code table
+    void* scratch; int64_t scratch_stride;     // per group slot: the stripe boundary row, 3*(n+1) T
+    double* score;                             // per pair
+    int32_t* end;                              // per pair: end_i, end_j, state, layout (G<<8|R)
+};
+
+template <class T> struct HardRowParams { T goa, gea, gob, geb; };
+
+// Column-0 border of DP row i >= 1 (Global): untracked closed form or the tracked table.
+template <class T, bool AFF, bool TR>
+__device__ __forceinline__ T border_col0(const HardArgs& A, const T* bx0p, int i, T gob, T geb) {
+    if constexpr (TR) return bx0p[i];
+    else {
+        if constexpr (AFF) return -add_rn(gob, mul_rn(static_cast<T>(i), geb));
+        else return mul_rn(-static_cast<T>(i), geb);
+    }
+}
+
+template <class T, bool AFF, bool LOC, bool TR, int G, int R>
+__global__ void __launch_bounds__(128) hard_fill_kernel(const HardArgs A) {
+    constexpr int GR = G * R;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* smat = reinterpret_cast<T*>(smem_raw);
+    const int nmat = A.K * A.N * A.N;
+    T* sgap = smat + nmat;
+    for (int k = threadIdx.x; k < nmat; k += blockDim.x) smat[k] = static_cast<const T*>(A.mat)[k];
+    for (int k = threadIdx.x; k < 4 * A.K; k += blockDim.x) sgap[k] = static_cast<const T*>(A.gaps)[k];
+    __syncthreads();
+
+    const int lane = threadIdx.x % G;
+    const int gpb = blockDim.x / G;
+    const int64_t slot = int64_t(blockIdx.x) * gpb + threadIdx.x / G;
+    unsigned gmask;
+    if constexpr (G == 32) gmask = 0xffffffffu;
+    else gmask = ((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1));
+    T* bnd = static_cast<T*>(A.scratch) + slot * A.scratch_stride;
+    const int N = A.N;
+
+    for (int64_t it = slot; it < A.n_items; it += int64_t(gridDim.x) * gpb) {
+        const int p = A.order[it];
+        const int64_t ao = A.oa[p], bo = A.ob[p];
+        const int m = int(A.oa[p + 1] - ao), n = int(A.ob[p + 1] - bo);
+        const uint8_t* __restrict__ ap = A.a + ao;
+        const uint8_t* __restrict__ bp = A.b + bo;
+        const uint16_t* tk = TR ? A.tracks + ao : nullptr;
+        const uint16_t* gk = (TR && A.gtracks) ? A.gtracks + ao + p : nullptr;
+        const T* bx0p = TR ? static_cast<const T*>(A.bx0) + ao + p : nullptr;
+        // set of DP row i: matches / gaps in B (tset, i >= 1), gaps in A (gset, i >= 0)
+        auto tset = [&](int i) -> int { return TR ? int(tk[i - 1]) : 0; };
+        auto gset = [&](int i) -> int {
+            if constexpr (!TR) return 0;
+            if (gk) return int(gk[i]);
+            return i == 0 ? (m ? int(tk[0]) : 0) : int(tk[i - 1]);
+        };
+        const T goa0 = sgap[4 * gset(0) + 0], gea0 = sgap[4 * gset(0) + 1];
+        const T ugob = sgap[2], ugeb = sgap[3], ugoa = sgap[0], ugea = sgap[1];
+        if (m == 0 || n == 0) {
+            if (lane == 0) {
+                T sc; int ei, ej, st;
+                if (LOC) { sc = T(0); ei = 0; ej = 0; st = 0; }
+                else if (m == 0 && n == 0) { sc = T(0); ei = 0; ej = 0; st = 0; }
+                else if (m == 0) {
+                    sc = AFF ? -add_rn(goa0, mul_rn(static_cast<T>(n), gea0)) : mul_rn(-static_cast<T>(n), gea0);
+                    ei = 0; ej = n; st = 2;
+                } else {
+                    const T gob = TR ? sgap[4 * tset(1) + 2] : ugob;
+                    const T geb = TR ? sgap[4 * tset(m) + 3] : ugeb;
+                    sc = border_col0<T, AFF, TR>(A, bx0p, m, gob, geb);
+                    ei = m; ej = 0; st = AFF ? 1 : 0;
+                }
+                A.score[p] = static_cast<double>(sc);
+                A.end[4 * p] = ei; A.end[4 * p + 1] = ej; A.end[4 * p + 2] = st;
+                A.end[4 * p + 3] = (G << 8) | R;
+            }
+            continue;
+        }
+        uint8_t* __restrict__ codes = A.codes + A.code_off[p];
+        const int nstripes = (m + GR - 1) / GR;
+        const int S = n + G - 1;
+
+        T bestv = T(0); int besti = 0, bestj = 0, bests = 0;   // Local: the first row-major max
+        T endM = ninf<T>(), endX = ninf<T>(), endY = ninf<T>();
+
+        for (int s = 0; s < nstripes; ++s) {
+            const int i0 = s * GR + lane * R + 1;   // this lane's first DP row
+            int rowbase[R];
+            T cM[R], cX[R], cY[R];
+            HardRowParams<T> rp[TR ? R : 1];
+            T rbest[LOC ? R : 1]; int rbj[LOC ? R : 1]; int rbs[LOC ? R : 1];
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int i = i0 + r;
+                const bool valid = i <= m;
+                const int key = valid ? (TR ? tset(i) * N + ap[i - 1] : int(ap[i - 1])) : 0;
+                rowbase[r] = key * N;
+                if constexpr (TR) {
+                    const int gs = valid ? gset(i) : 0, ts = valid ? tset(i) : 0;
+                    rp[r].goa = sgap[4 * gs + 0]; rp[r].gea = sgap[4 * gs + 1];
+                    rp[r].gob = sgap[4 * ts + 2]; rp[r].geb = sgap[4 * ts + 3];
+                }
+                if constexpr (LOC) { cM[r] = T(0); cX[r] = ninf<T>(); rbest[r] = T(0); rbj[r] = 0; rbs[r] = 0; }
+                else {
+                    cM[r] = ninf<T>();
+                    cX[r] = valid ? border_col0<T, AFF, TR>(A, bx0p, i, ugob, ugeb) : ninf<T>();
+                    if constexpr (!AFF) cM[r] = cX[r];   // linear: H lives in cM
+                }
+                cY[r] = ninf<T>();
+            }
+            // the row above this lane's first row, at column 0
+            T dgM, dgX, dgY;
+            {
+                const int i = i0 - 1;
+                if (i == 0) { dgM = T(0); dgX = ninf<T>(); dgY = ninf<T>(); }
+                else if (LOC) { dgM = T(0); dgX = ninf<T>(); dgY = ninf<T>(); }
+                else {
+                    dgX = border_col0<T, AFF, TR>(A, bx0p, i, ugob, ugeb);
+                    dgM = AFF ? ninf<T>() : dgX; dgY = ninf<T>();
+                }
+            }
+            T upM = ninf<T>(), upX = ninf<T>(), upY = ninf<T>();
+            uint8_t* cs = codes + int64_t(s) * S * GR;
+
+            for (int t = 0; t < S; ++t) {
+                const int j = t - lane + 1;
+                if (lane == 0 && j <= n) {
+                    if (s == 0) {
+                        if constexpr (LOC) { upM = T(0); upX = ninf<T>(); upY = ninf<T>(); }
+                        else if constexpr (AFF) { upM = ninf<T>(); upX = ninf<T>(); upY = -add_rn(goa0, mul_rn(static_cast<T>(j), gea0)); }
+                        else { upM = mul_rn(-static_cast<T>(j), gea0); }
+                    } else {
+                        upM = bnd[3 * j]; upX = bnd[3 * j + 1]; upY = bnd[3 * j + 2];
+                    }
+                }
+                const bool active = (j >= 1) && (j <= n);
+                if (active) {
+                    const int bj = bp[j - 1];
+                    T pM = dgM, pX = dgX, pY = dgY;   // row above, column j-1
+                    T qM = upM, qX = upX, qY = upY;   // row above, column j
+                    uint32_t w[(R + 3) / 4];
+#pragma unroll
+                    for (int k = 0; k < (R + 3) / 4; ++k) w[k] = 0u;
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        const T sub = smat[rowbase[r] + bj];
+                        T go_a, ge_a, go_b, ge_b;
+                        if constexpr (TR) { go_a = rp[r].goa; ge_a = rp[r].gea; go_b = rp[r].gob; ge_b = rp[r].geb; }
+                        else { go_a = ugoa; ge_a = ugea; go_b = ugob; ge_b = ugeb; }
+                        uint32_t code;
+                        if constexpr (AFF) {
+                            T mv = rmax3(pM, pX, pY) + sub;
+                            uint32_t km = pick3(pM, pX, pY);
+                            const T ux = (qM - go_b) - ge_b, vx = qX - ge_b, wx = (qY - go_b) - ge_b;
+                            const T xv = rmax3(ux, vx, wx);
+                            const uint32_t kx = pick3(ux, vx, wx);
+                            const T uy = (cM[r] - go_a) - ge_a, vy = (cX[r] - go_a) - ge_a, wy = cY[r] - ge_a;
+                            const T yv = rmax3(uy, vy, wy);
+                            const uint32_t ky = pick3(uy, vy, wy);
+                            if constexpr (LOC) {
+                                mv = rmax(mv, T(0));
+                                km |= 3u * uint32_t(mv <= T(0));
+                                const T v = rmax3(mv, xv, yv);
+                                if (v > rbest[r]) {
+                                    rbest[r] = v; rbj[r] = j;
+                                    rbs[r] = (mv >= xv && mv >= yv) ? 0 : (xv >= yv ? 1 : 2);
+                                }
+                            }
+                            pM = cM[r]; pX = cX[r]; pY = cY[r];
+                            cM[r] = mv; cX[r] = xv; cY[r] = yv;
+                            qM = mv; qX = xv; qY = yv;
+                            code = km | (kx << 2) | (ky << 4);
+                        } else {
+                            const T d0 = pM + sub;
+                            const T u = qM - ge_b;
+                            const T tt = rmax(d0, u);
+                            uint32_t c = uint32_t(d0 < u);
+                            const T l = cM[r] - ge_a;
+                            T v = rmax(tt, l);
+                            c = (tt < l) ? 2u : c;
+                            if constexpr (LOC) {
+                                v = rmax(v, T(0));
+                                c |= 3u * uint32_t(v <= T(0));
+                                if (v > rbest[r]) { rbest[r] = v; rbj[r] = j; }
+                            }
+                            pM = cM[r];
+                            cM[r] = v;
+                            qM = v;
+                            code = c;
+                        }
+                        w[r >> 2] |= code << (8 * (r & 3));
+                    }
+                    // one coalesced store of this lane's R codes
+                    uint8_t* dst = cs + (int64_t(t) * G + lane) * R;
+                    if constexpr (R % 16 == 0) {
+#pragma unroll
+                        for (int k = 0; k < R / 16; ++k)
+                            reinterpret_cast<uint4*>(dst)[k] = make_uint4(w[4 * k], w[4 * k + 1], w[4 * k + 2], w[4 * k + 3]);
+                    } else if constexpr (R % 8 == 0) {
+#pragma unroll
+                        for (int k = 0; k < R / 8; ++k) reinterpret_cast<uint2*>(dst)[k] = make_uint2(w[2 * k], w[2 * k + 1]);
+                    } else if constexpr (R % 4 == 0) {
+#pragma unroll
+                        for (int k = 0; k < R / 4; ++k) reinterpret_cast<uint32_t*>(dst)[k] = w[k];
+                    } else {
+#pragma unroll
+                        for (int r = 0; r < R; ++r) dst[r] = uint8_t(w[r >> 2] >> (8 * (r & 3)));
+                    }
+                    dgM = upM; dgX = upX; dgY = upY;
+                }
+                // hand the bottom row to the next lane (and, from the last lane, to the next stripe)
+                if constexpr (G > 1) {
+                    const T sM = __shfl_up_sync(gmask, cM[R - 1], 1, G);
+                    T sX = sM, sY = sM;
+                    if constexpr (AFF) {
+                        sX = __shfl_up_sync(gmask, cX[R - 1], 1, G);
+                        sY = __shfl_up_sync(gmask, cY[R - 1], 1, G);
+                    }
+                    if (lane > 0) { upM = sM; upX = sX; upY = sY; }
+                }
+                if (lane == G - 1 && active && s + 1 < nstripes) {
+                    bnd[3 * j] = cM[R - 1];
+                    if constexpr (AFF) { bnd[3 * j + 1] = cX[R - 1]; bnd[3 * j + 2] = cY[R - 1]; }
+                }
+            }
+            // the end cell (m, n): after the stripe each register holds column n
+            if constexpr (!LOC) {
+                if (m >= i0 && m < i0 + R) {
+#pragma unroll
+                    for (int r = 0; r < R; ++r)
+                        if (i0 + r == m) { endM = cM[r]; endX = cX[r]; endY = cY[r]; }
+                }
+            } else {
+                // this lane's first row-major best of the stripe, then the group's
+                T lv = T(0); int li = 0, lj = 0, ls = 0;
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    if (i0 + r <= m && rbest[r] > lv) { lv = rbest[r]; li = i0 + r; lj = rbj[r]; ls = rbs[r]; }
+                if constexpr (G > 1) {
+#pragma unroll
+                    for (int off = 1; off < G; off <<= 1) {
+                        const T ov = __shfl_down_sync(gmask, lv, off, G);
+                        const int oi = __shfl_down_sync(gmask, li, off, G);
+                        const int oj = __shfl_down_sync(gmask, lj, off, G);
+                        const int os = __shfl_down_sync(gmask, ls, off, G);
+                        const bool take = (lane + off < G) && (ov > lv || (ov == lv && ov > T(0) && oi < li));
+                        if (take) { lv = ov; li = oi; lj = oj; ls = os; }
+                    }
+                }
+                if (lv > bestv) { bestv = lv; besti = li; bestj = lj; bests = ls; }
+            }
+            if constexpr (G > 1) __syncwarp(gmask);
+        }
+        if constexpr (!LOC) {
+            if constexpr (G > 1) {
+                // the lane holding row m broadcasts its end values
+                const int src = ((m - 1) % GR) / R;
+                endM = __shfl_sync(gmask, endM, src, G);
+                endX = __shfl_sync(gmask, endX, src, G);
+                endY = __shfl_sync(gmask, endY, src, G);
+            }
+            if (lane == 0) {
+                T sc; int st;
+                if constexpr (AFF) {
+                    sc = rmax3(endM, endX, endY);
+                    st = (endM >= endX && endM >= endY) ? 0 : (endX >= endY ? 1 : 2);
+                } else { sc = endM; st = 0; }
+                A.score[p] = static_cast<double>(sc);
+                A.end[4 * p] = m; A.end[4 * p + 1] = n; A.end[4 * p + 2] = st;
+                A.end[4 * p + 3] = (G << 8) | R;
+            }
+        } else if (lane == 0) {
+            A.score[p] = static_cast<double>(bestv);
+            A.end[4 * p] = besti; A.end[4 * p + 1] = bestj; A.end[4 * p + 2] = bests;
+            A.end[4 * p + 3] = (G << 8) | R;
+        }
+    }
+}
+
+// ── Traceback: one thread per pair ────────────────────────────────────────────
+struct WalkArgs {
+    const uint8_t* a; const int64_t* oa;
+    const uint8_t* b; const int64_t* ob;
+    const uint16_t* tracks; const uint16_t* gtracks;
+    const int32_t* order; int64_t n_items;
+    int N, K;
+    int affine, local;
+    const uint8_t* codes; const int64_t* code_off;
+    const int32_t* end;
+    double* grad; int64_t gstride;     // per pair, zeroed here: K*N*N matrix stack + K*4 gaps
+    int32_t* guide;                    // per pair m+1 at oa[p] + p, or null
+    uint8_t* moves; const int64_t* moves_off;   // keep_paths: walk-order moves, or null
+    int32_t* path_info;                // per pair: n_moves, start_i, start_j (or null)
+};
+
+__device__ __forceinline__ uint8_t code_at(const uint8_t* codes, int i, int j, int n, int G, int R) {
+    const int GR = G * R;
+    const int s = (i - 1) / GR, w = (i - 1) % GR, g = w / R, r = w % R;
+    const int S = n + G - 1;
+    return codes[((int64_t(s) * S + (j - 1 + g)) * G + g) * R + r];
+}
+
+__global__ void walk_kernel(const WalkArgs A) {
+    const int64_t it = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (it >= A.n_items) return;
+    const int p = A.order[it];
+    const int64_t ao = A.oa[p], bo = A.ob[p];
+    const int m = int(A.oa[p + 1] - ao), n = int(A.ob[p + 1] - bo);
+    const uint8_t* ap = A.a + ao;
+    const uint8_t* bp = A.b + bo;
+    const uint16_t* tk = A.tracks ? A.tracks + ao : nullptr;
+    const uint16_t* gk = A.gtracks ? A.gtracks + ao + p : nullptr;
+    const int N = A.N;
+    const int64_t NN = int64_t(A.K) * N * N;
+    double* g = A.grad ? A.grad + A.gstride * p : nullptr;
+    if (g) for (int64_t k = 0; k < A.gstride; ++k) g[k] = 0.0;
+    const uint8_t* codes = A.codes + A.code_off[p];
+    const int lay = A.end[4 * p + 3];
+    const int G = lay >> 8, R = lay & 0xff;
+    auto tset = [&](int i) -> int { return tk ? int(tk[i - 1]) : 0; };
+    auto gset = [&](int i) -> int {
+        if (!tk) return 0;
+        if (gk) return int(gk[i]);
+        return i == 0 ? (m ? int(tk[0]) : 0) : int(tk[i - 1]);
+    };
+    int32_t* gj = A.guide ? A.guide + ao + p : nullptr;
+    if (gj) {
+        for (int k = 0; k <= m; ++k) gj[k] = -1;
+        gj[0] = 0; gj[m] = n;
+    }
+    int i = A.end[4 * p], j = A.end[4 * p + 1];
+    int tbl = A.end[4 * p + 2];
+    if (gj) gj[i] = j;
+    uint8_t* mv = A.moves ? A.moves + A.moves_off[p] : nullptr;
+    int64_t nm = 0;
+    // emit one move out of (i, j): 0 M, 1 X (gap in B), 2 Y (gap in A)
+    auto emit = [&](int s, int ii, int jj, bool open) {
+        if (mv) mv[nm] = uint8_t(s);
+        ++nm;
+        if (s == 0) {
+            if (g) g[int64_t(tset(ii) * N + ap[ii - 1]) * N + bp[jj - 1]] += 1.0;
+            if (gj) gj[ii - 1] = jj - 1;
+        } else if (s == 1) {
+            if (g) {
+                const int64_t o = NN + 4 * tset(ii);
+                g[o + 3] -= 1.0;
+                if (open) g[o + 2] -= 1.0;
+            }
+            if (gj) gj[ii - 1] = jj;
+        } else {
+            if (g) {
+                const int64_t o = NN + 4 * gset(ii);
+                g[o + 1] -= 1.0;
+                if (open) g[o + 0] -= 1.0;
+            }
+        }
+    };
+    if (A.affine) {
+        while (true) {
+            if (i == 0 && j == 0) break;
+            uint32_t c;
+            if (A.local) {
+                c = (i == 0 || j == 0) ? 3u : code_at(codes, i, j, n, G, R);
+                if (tbl == 0 && (c & 3u) == 3u) break;
+            } else {
+                if (i == 0) { for (; j > 0; --j) emit(2, 0, j, j == 1); break; }
+                if (j == 0) { for (; i > 0; --i) emit(1, i, 0, i == 1); break; }
+                c = code_at(codes, i, j, n, G, R);
+            }
+            if (i == 0) tbl = 2;
+            else if (j == 0) tbl = 1;
+            int prev;
+            auto from_code = [](uint32_t cc) { return cc == 1u ? 1 : (cc == 2u ? 2 : 0); };
+            if (tbl == 0) { prev = from_code(c & 3u); emit(0, i, j, false); --i; --j; }
+            else if (tbl == 1) { prev = from_code((c >> 2) & 3u); emit(1, i, j, prev != 1); --i; }
+            else { prev = from_code(c >> 4); emit(2, i, j, prev != 2); --j; }
+            tbl = prev;
+        }
+    } else {
+        while (true) {
+            if (i == 0 && j == 0) break;
+            int k;
+            if (i == 0) k = A.local ? 3 : 2;
+            else if (j == 0) k = A.local ? 3 : 1;
+            else k = code_at(codes, i, j, n, G, R);
+            if (k == 3) break;
+            if (k == 0) { emit(0, i, j, false); --i; --j; }
+            else if (k == 1) {
+                if (mv) mv[nm] = 1;
+                ++nm;
+                if (g) g[NN + 4 * tset(i) + 3] -= 1.0;
+                if (gj) gj[i - 1] = j;
+                --i;
+            } else {
+                if (mv) mv[nm] = 2;
+                ++nm;
+                if (g) g[NN + 4 * gset(i) + 1] -= 1.0;
+                --j;
+            }
+        }
+    }
+    if (A.path_info) { A.path_info[3 * p] = int32_t(nm); A.path_info[3 * p + 1] = i; A.path_info[3 * p + 2] = j; }
+    if (gj) {
+        // interpolate the rows the path does not fix (aligner.hpp:2734-2749)
+        const int L = m + 1;
+        int lo = 0;
+        while (lo < L) {
+            if (gj[lo] < 0) { ++lo; continue; }
+            int hi = lo + 1;
+            while (hi < L && gj[hi] < 0) ++hi;
+            if (hi == L) { for (int k = lo + 1; k < L; ++k) gj[k] = gj[lo]; break; }
+            for (int k = lo + 1; k < hi; ++k) gj[k] = gj[lo] + (gj[hi] - gj[lo]) * (k - lo) / (hi - lo);
+            lo = hi;
+        }
+    }
+}
+
+}  // namespace nwg

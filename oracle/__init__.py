@@ -205,6 +205,8 @@ def ref_run(prec, gm, am, grad_mode, alphabet, mat, gaps, seqs_a, seqs_b, tracks
             gaps2=None, simd=False):
     """Run the reference batch once; returns dict(scores, grads, guides, total)."""
     L = ref_lib(simd)
+    if n_threads <= 0:
+        n_threads = physical_cores()
     P, keep, oa = _problem(prec, gm, am, grad_mode, alphabet, mat, gaps, seqs_a, seqs_b, tracks,
                            gap_tracks, traceback, kernel, n_threads, temperature, soft_impl,
                            soft_f32, hb_cutoff, inter_fill)
@@ -228,6 +230,8 @@ def ref_time(prec, gm, am, grad_mode, alphabet, mat, gaps, seqs_a, seqs_b, track
              warmup=1, reps=3, simd=True):
     """Time the reference's own batch path: per-pass seconds of score_and_grad()+compute_grad()."""
     L = ref_lib(simd)
+    if n_threads <= 0:
+        n_threads = physical_cores()
     P, keep, _ = _problem(prec, gm, am, grad_mode, alphabet, mat, gaps, seqs_a, seqs_b, tracks,
                           gap_tracks, traceback, kernel, n_threads, temperature, 0, True, 0, True)
     secs = np.zeros(reps, np.float64)
@@ -238,7 +242,64 @@ def ref_time(prec, gm, am, grad_mode, alphabet, mat, gaps, seqs_a, seqs_b, track
     return secs, float(total[0])
 
 
+def physical_cores() -> int:
+    """Physical cores among the CPUs this process may run on (the reference's default
+    n_threads, parallel.hpp:165), counted here: the reference's own probe crashes when it
+    runs inside a process that has numpy loaded."""
+    cpus = sorted(os.sched_getaffinity(0))
+    seen = set()
+    for c in cpus:
+        try:
+            pkg = open(f"/sys/devices/system/cpu/cpu{c}/topology/physical_package_id").read().strip()
+            core = open(f"/sys/devices/system/cpu/cpu{c}/topology/core_id").read().strip()
+            seen.add((pkg, core))
+        except OSError:
+            seen.add(("?", str(c)))
+    return max(1, len(seen))
+
+
+def ref_bench_available() -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", "nwref_bench"))
+
+
+def ref_time_codes(prec, gm, am, grad_mode, alphabet, mat, gaps, a, oa, b, ob, n_threads=0,
+                   warmup=1, reps=3, kernel=-2):
+    """Time the reference's SIMD batch path (score_and_grad + compute_grad per pass) in its
+    own process (_ref/nwref_bench) on pairs given as codes: returns (seconds per pass,
+    total, threads, isa)."""
+    import json
+    import tempfile
+    if n_threads <= 0:
+        n_threads = physical_cores()
+    mat = np.ascontiguousarray(mat, np.float64)
+    gaps = np.ascontiguousarray(gaps, np.float64)
+    K, N = mat.shape[0], mat.shape[1]
+    sym = np.frombuffer(alphabet.encode(), dtype=np.uint8)
+    with tempfile.NamedTemporaryFile(suffix=".bin", delete=False) as f:
+        f.write(np.array([prec, gm, am, grad_mode, N, K, n_threads, warmup, reps, kernel], np.int32).tobytes())
+        f.write(np.array([len(oa) - 1], np.int64).tobytes())
+        f.write(np.array([len(alphabet)], np.int32).tobytes())
+        f.write(alphabet.encode())
+        f.write(mat.tobytes())
+        f.write(gaps.tobytes())
+        f.write(np.ascontiguousarray(oa - oa[0], np.int64).tobytes())
+        f.write(sym[np.asarray(a[oa[0]:oa[-1]], np.int64)].tobytes())
+        f.write(np.ascontiguousarray(ob - ob[0], np.int64).tobytes())
+        f.write(sym[np.asarray(b[ob[0]:ob[-1]], np.int64)].tobytes())
+        path = f.name
+    try:
+        r = subprocess.run([os.path.join(HERE, "_ref", "nwref_bench"), path], capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("nwref_bench failed: " + r.stderr.strip())
+        out = json.loads(r.stdout.strip().splitlines()[-1])
+    finally:
+        os.unlink(path)
+    return np.array(out["secs"]), out["total"], out["threads"], out["isa"]
+
+
 def ref_info(n_threads=0, simd=True):
+    if n_threads <= 0:
+        n_threads = physical_cores()
     L = ref_lib(simd)
     r = C.c_int(0)
     buf = C.create_string_buffer(64)

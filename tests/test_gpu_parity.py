@@ -1,0 +1,142 @@
+"""GPU parity: the CUDA path through the C ABI against the CPU oracle on the same inputs.
+
+Hard results (scores, per-pair gradient counts, guides) are compared bit for bit; soft
+results within 1e-4 relative of the oracle's double log-space forward-backward (the
+reference's float32-vs-double tolerance is 2e-4 / 1e-5 abs, test_soft_float32.py:26-29).
+"""
+import numpy as np
+import pytest
+
+import oracle
+from conftest import AA, encode, has_gpu, mutate, rand_matrix, rand_seqs
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not has_gpu(), reason="needs a CUDA GPU")]
+
+import nwgrad_b200 as nw  # noqa: E402
+
+SOFT_RTOL = 1e-4
+
+
+def _problem(rng, alpha, n, lo, hi, K=1, integer=True, tracked=False, homolog=False, gap_tracks=False):
+    N = len(alpha)
+    mat = rand_matrix(rng, N, K, integer)
+    if integer:
+        gaps = np.tile([11.0, 1.0, 11.0, 1.0], (K, 1))
+        if K > 1:
+            gaps = gaps + rng.integers(0, 3, size=(K, 4))
+    else:
+        gaps = rng.uniform(0.3, 4.0, size=(K, 4))
+    sa = rand_seqs(rng, n, lo, hi, alpha)
+    sb = [mutate(rng, s, alpha) for s in sa] if homolog else rand_seqs(rng, n, lo, hi, alpha)
+    tr = gt = None
+    if tracked:
+        tr = np.concatenate([rng.integers(0, K, size=len(s)) for s in sa] + [np.zeros(0, np.int64)]).astype(np.uint16)
+        if gap_tracks:
+            gt = np.concatenate([rng.integers(0, K, size=len(s) + 1) for s in sa]).astype(np.uint16)
+    return mat, gaps, sa, sb, tr, gt
+
+
+def _params(alpha, mat, gaps):
+    return nw.AlignParams.from_arrays(mat, gaps, alphabet=alpha)
+
+
+def _hard_check(prec, gm, am, alpha, mat, gaps, sa, sb, tr, gt, tracked):
+    cls = nw.SeqPairBatch if prec == 32 else nw.SeqPairBatchDouble
+    b = cls(sa, sb, _params(alpha, mat, gaps), gap_model=("linear", "affine")[gm],
+            mode=("global", "local")[am], grad_mode="hard", tracks=tr, gap_tracks=gt)
+    tot = b.score_and_grad()
+    enc = oracle.Encoded(encode(alpha, sa), encode(alpha, sb), tr, gt)
+    o = oracle.hard(prec, gm, am, mat, gaps, enc, tracked=tracked)
+    s = b.scores()
+    assert np.array_equal(s, o["scores"]), np.nonzero(s != o["scores"])[0][:5]
+    # the reference sums in pair order (Python's sum() compensates: use a running sum)
+    assert tot == (float(np.cumsum(o["scores"])[-1]) if len(sa) else 0.0)
+    gmat, ggap = b.grads()
+    K, N = mat.shape[0], mat.shape[1]
+    if not tracked:
+        gmat = gmat[:, None]
+        ggap = ggap[:, None]
+    flat = np.concatenate([gmat.reshape(len(sa), -1), ggap.reshape(len(sa), -1)], axis=1)
+    assert np.array_equal(flat, o["grads"]), np.nonzero((flat != o["grads"]).any(1))[0][:5]
+    gj = b.guides()
+    assert np.array_equal(gj, o["guides"])
+    cg = b.compute_grad()
+    ref = oracle.blocked_sum(o["grads"])
+    assert np.array_equal(np.concatenate([cg.matrices.ravel(), cg.gaps.ravel()]), ref)
+    w = np.linspace(-1.0, 2.0, len(sa))
+    wg = b.weighted_grad(w)
+    ref = oracle.blocked_sum(o["grads"], w)
+    assert np.array_equal(np.concatenate([wg.matrices.ravel(), wg.gaps.ravel()]), ref)
+
+
+@pytest.mark.parametrize("prec", [32, 64])
+@pytest.mark.parametrize("gm", [0, 1])
+@pytest.mark.parametrize("am", [0, 1])
+@pytest.mark.parametrize("integer", [True, False])
+def test_hard_bit_exact(prec, gm, am, integer):
+    rng = np.random.default_rng(100 + prec + 10 * gm + 20 * am + int(integer))
+    # short (one lane per pair), medium and multi-stripe pairs, plus empty sequences
+    mat, gaps, sa, sb, tr, gt = _problem(rng, AA, 60, 0, 40, integer=integer)
+    sa += ["", "ACD", "", "W" * 70] + rand_seqs(rng, 6, 200, 300, AA)
+    sb += ["KLM", "", "", "W" * 3] + rand_seqs(rng, 6, 150, 320, AA)
+    _hard_check(prec, gm, am, AA, mat, gaps, sa, sb, None, None, False)
+
+
+@pytest.mark.parametrize("gm", [0, 1])
+@pytest.mark.parametrize("am", [0, 1])
+@pytest.mark.parametrize("gap_tracks", [False, True])
+def test_hard_tracked_bit_exact(gm, am, gap_tracks):
+    rng = np.random.default_rng(7 + gm + 2 * am + 4 * gap_tracks)
+    alpha = "ACGTU"
+    mat, gaps, sa, sb, tr, gt = _problem(rng, alpha, 50, 1, 45, K=3, tracked=True, gap_tracks=gap_tracks,
+                                         integer=False)
+    _hard_check(32, gm, am, alpha, mat, gaps, sa, sb, tr, gt, True)
+
+
+def _soft_check(prec, gm, am, alpha, mat, gaps, sa, sb, tr, gt, T=1.0):
+    cls = nw.SeqPairBatch if prec == 32 else nw.SeqPairBatchDouble
+    b = cls(sa, sb, _params(alpha, mat, gaps), gap_model=("linear", "affine")[gm],
+            mode=("global", "local")[am], grad_mode="soft", tracks=tr, gap_tracks=gt)
+    b.soft_temperature = T
+    b.score_and_grad()
+    enc = oracle.Encoded(encode(alpha, sa), encode(alpha, sb), tr, gt)
+    so, go = oracle.soft(gm, am, mat, gaps, enc, T)
+    s = b.scores()
+    np.testing.assert_allclose(s, so, rtol=SOFT_RTOL, atol=1e-5)
+    K, N = mat.shape[0], mat.shape[1]
+    gmat, ggap = b.grads()
+    if gmat.ndim == 3:
+        gmat = gmat[:, None]
+        ggap = ggap[:, None]
+    flat = np.concatenate([gmat.reshape(len(sa), -1), ggap.reshape(len(sa), -1)], axis=1)
+    # relative to each pair's gradient scale (its largest entry), as the reference's tests do
+    scale = np.maximum(np.abs(go).max(axis=1, keepdims=True), 1.0)
+    err = np.abs(flat - go) / scale
+    assert err.max() <= SOFT_RTOL, (err.max(), np.unravel_index(err.argmax(), err.shape))
+
+
+@pytest.mark.parametrize("prec", [32, 64])
+@pytest.mark.parametrize("gm", [0, 1])
+@pytest.mark.parametrize("am", [0, 1])
+def test_soft_within_tolerance(prec, gm, am):
+    rng = np.random.default_rng(300 + prec + gm + 2 * am)
+    mat, gaps, sa, sb, tr, gt = _problem(rng, AA, 40, 1, 40, homolog=True)
+    sa += rand_seqs(rng, 4, 150, 260, AA) + ["", "A"]
+    sb += [mutate(rng, s, AA) for s in sa[-6:-2]] + ["AC", ""]
+    _soft_check(prec, gm, am, AA, mat, gaps, sa, sb, None, None)
+
+
+@pytest.mark.parametrize("gm", [0, 1])
+@pytest.mark.parametrize("am", [0, 1])
+def test_soft_tracked(gm, am):
+    rng = np.random.default_rng(500 + gm + 2 * am)
+    alpha = "ACGTU"
+    mat, gaps, sa, sb, tr, gt = _problem(rng, alpha, 40, 1, 30, K=3, tracked=True, gap_tracks=True)
+    _soft_check(32, gm, am, alpha, mat, gaps, sa, sb, tr, gt)
+
+
+@pytest.mark.parametrize("T", [0.5, 2.0])
+def test_soft_temperature(T):
+    rng = np.random.default_rng(77)
+    mat, gaps, sa, sb, tr, gt = _problem(rng, AA, 30, 5, 60, homolog=True)
+    _soft_check(32, 1, 0, AA, mat, gaps, sa, sb, None, None, T=T)
