@@ -20,9 +20,8 @@
 #include <vector>
 
 #include "../../include/nwgrad_b200.h"
-#include "nwg_common.cuh"
-#include "nwg_hard.cuh"
-#include "nwg_soft.cuh"
+#include "nwg_kernels.h"
+#include "nwg_walk.cuh"
 
 namespace {
 
@@ -129,46 +128,15 @@ int sm_count(int dev) {
     return v > 0 ? v : 148;
 }
 
-// ── kernel tables ─────────────────────────────────────────────────────────────
-using HardFn = void (*)(const nwg::HardArgs);
-using SoftFn = void (*)(const nwg::SoftArgs);
-
-struct Geo { int G, R; };
-// Geometries compiled: one lane per pair (short pairs) and one warp per pair.
-constexpr Geo kHardGeos[] = {{1, 8}, {1, 16}, {1, 24}, {1, 32}, {32, 1}, {32, 2}, {32, 4}, {32, 8}};
-constexpr Geo kSoftGeos[] = {{1, 8}, {1, 16}, {1, 24}, {1, 32}, {32, 2}, {32, 4}, {32, 8}};
-
-template <class T, bool AFF, bool LOC, bool TR>
-HardFn hard_fn(Geo g) {
-#define NWG_H(GG, RR) if (g.G == GG && g.R == RR) return &nwg::hard_fill_kernel<T, AFF, LOC, TR, GG, RR>;
-    NWG_H(1, 8) NWG_H(1, 16) NWG_H(1, 24) NWG_H(1, 32) NWG_H(32, 1) NWG_H(32, 2) NWG_H(32, 4) NWG_H(32, 8)
-#undef NWG_H
-    return nullptr;
+// ── kernel tables (instantiated in nwg_hard_inst.cu / nwg_soft_inst.cu) ─────────
+using HardFn = nwg::HardFn;
+using SoftFn = nwg::SoftFn;
+using Geo = nwg::Geo;
+template <class T> HardFn hard_fn_rt(bool aff, bool loc, bool tr, Geo g) {
+    return sizeof(T) == 4 ? nwg::hard_fn_f32(aff, loc, tr, g) : nwg::hard_fn_f64(aff, loc, tr, g);
 }
-template <class T>
-HardFn hard_fn_rt(bool aff, bool loc, bool tr, Geo g) {
-    if (aff) {
-        if (loc) return tr ? hard_fn<T, true, true, true>(g) : hard_fn<T, true, true, false>(g);
-        return tr ? hard_fn<T, true, false, true>(g) : hard_fn<T, true, false, false>(g);
-    }
-    if (loc) return tr ? hard_fn<T, false, true, true>(g) : hard_fn<T, false, true, false>(g);
-    return tr ? hard_fn<T, false, false, true>(g) : hard_fn<T, false, false, false>(g);
-}
-template <class T, bool AFF, bool LOC, bool TR>
-SoftFn soft_fn(Geo g) {
-#define NWG_S(GG, RR) if (g.G == GG && g.R == RR) return &nwg::soft_kernel<T, AFF, LOC, TR, GG, RR>;
-    NWG_S(1, 8) NWG_S(1, 16) NWG_S(1, 24) NWG_S(1, 32) NWG_S(32, 2) NWG_S(32, 4) NWG_S(32, 8)
-#undef NWG_S
-    return nullptr;
-}
-template <class T>
-SoftFn soft_fn_rt(bool aff, bool loc, bool tr, Geo g) {
-    if (aff) {
-        if (loc) return tr ? soft_fn<T, true, true, true>(g) : soft_fn<T, true, true, false>(g);
-        return tr ? soft_fn<T, true, false, true>(g) : soft_fn<T, true, false, false>(g);
-    }
-    if (loc) return tr ? soft_fn<T, false, true, true>(g) : soft_fn<T, false, true, false>(g);
-    return tr ? soft_fn<T, false, false, true>(g) : soft_fn<T, false, false, false>(g);
+template <class T> SoftFn soft_fn_rt(bool aff, bool loc, bool tr, Geo g) {
+    return sizeof(T) == 4 ? nwg::soft_fn_f32(aff, loc, tr, g) : nwg::soft_fn_f64(aff, loc, tr, g);
 }
 
 // Padded cells a geometry computes for an (m, n) problem over `rows` DP rows.
@@ -471,6 +439,19 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
     std::vector<T> w, gw;
     bool ovf;
     soft_weights<T>(s, J, w, gw, ovf);
+    // renormalisation period: between renormalisations a lane's largest value grows by at most
+    // 3 x the largest weight per step, from at most 2^(kLift + 1); keep it below 2^126 (float)
+    // or 2^1022 (double)
+    double wmax = 1.0;
+    for (T v : w) wmax = std::max(wmax, double(v));
+    for (T v : gw) wmax = std::max(wmax, double(v));
+    const double per_step = std::log2(3.0 * wmax);
+    const double room = (sizeof(T) == 4 ? 126.0 : 1022.0) - (nwg::kLift + 1);
+    int renorm = int(std::floor(room / per_step));
+    if (renorm < 1) ovf = true;
+    int pw = 1;
+    while (pw * 2 <= std::min(renorm, sizeof(T) == 4 ? 8 : 16)) pw *= 2;
+    renorm = pw;
     DBuf dw, dgw;   // small; freed at scope end
     struct Free { DBuf& a; DBuf& b; ~Free() { a.release(); b.release(); } } fr{dw, dgw};
     dw.need(w.size() * sizeof(T)); dgw.need(gw.size() * sizeof(T));
@@ -527,12 +508,7 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
         int block = 128;
         const int K = s->K, N = s->N;
         auto smem_for = [&](int blk) {
-            const int gpb = blk / G;
-            size_t b = size_t((K * N + 1) * (N + 1) + 4 * K) * sizeof(T);
-            b = (b + 15) & ~size_t(15);
-            if (tr) b += size_t(4 * K * gpb) * sizeof(double);
-            b += size_t(K) * N * N * gpb * sizeof(T);
-            return b;
+            return nwg::soft_smem_bytes(K, N, G, B.geo.R, blk, int(sizeof(T)), tr);
         };
         while (block > 32 && smem_for(block) > 96 * 1024) block /= 2;
         const size_t smem = smem_for(block);
@@ -559,6 +535,7 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
         A.w = dw.p; A.gw = dgw.p; A.N = N; A.K = K;
         A.scratch = s->scratch.p; A.scratch_stride = stride; A.fwd_bytes = fwd_bytes;
         A.maxn = B.maxn; A.temperature = J.temperature;
+        A.renorm_mask = renorm - 1;
         A.score = s->score.as<double>(); A.grad = s->grad.as<double>(); A.gstride = s->gstride;
         A.status = s->status.as<int32_t>();
         if (ovf) {

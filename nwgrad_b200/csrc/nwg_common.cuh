@@ -25,6 +25,9 @@ __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(
 __device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
 
+__device__ __forceinline__ float fmaf_t(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double fmaf_t(double a, double b, double c) { return fma(a, b, c); }
+
 template <class T> __device__ __forceinline__ T ninf();
 template <> __device__ __forceinline__ float ninf<float>() { return __int_as_float(0xff800000u); }
 template <> __device__ __forceinline__ double ninf<double>() { return __longlong_as_double(0xfff0000000000000ull); }

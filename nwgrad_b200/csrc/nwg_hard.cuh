@@ -311,142 +311,4 @@ __global__ void __launch_bounds__(128) hard_fill_kernel(const HardArgs A) {
     }
 }
 
-// ── Traceback: one thread per pair ────────────────────────────────────────────
-struct WalkArgs {
-    const uint8_t* a; const int64_t* oa;
-    const uint8_t* b; const int64_t* ob;
-    const uint16_t* tracks; const uint16_t* gtracks;
-    const int32_t* order; int64_t n_items;
-    int N, K;
-    int affine, local;
-    const uint8_t* codes; const int64_t* code_off;
-    const int32_t* end;
-    double* grad; int64_t gstride;     // per pair, zeroed here: K*N*N matrix stack + K*4 gaps
-    int32_t* guide;                    // per pair m+1 at oa[p] + p, or null
-    uint8_t* moves; const int64_t* moves_off;   // keep_paths: walk-order moves, or null
-    int32_t* path_info;                // per pair: n_moves, start_i, start_j (or null)
-};
-
-__device__ __forceinline__ uint8_t code_at(const uint8_t* codes, int i, int j, int n, int G, int R) {
-    const int GR = G * R;
-    const int s = (i - 1) / GR, w = (i - 1) % GR, g = w / R, r = w % R;
-    const int S = n + G - 1;
-    return codes[((int64_t(s) * S + (j - 1 + g)) * G + g) * R + r];
-}
-
-__global__ void walk_kernel(const WalkArgs A) {
-    const int64_t it = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (it >= A.n_items) return;
-    const int p = A.order[it];
-    const int64_t ao = A.oa[p], bo = A.ob[p];
-    const int m = int(A.oa[p + 1] - ao), n = int(A.ob[p + 1] - bo);
-    const uint8_t* ap = A.a + ao;
-    const uint8_t* bp = A.b + bo;
-    const uint16_t* tk = A.tracks ? A.tracks + ao : nullptr;
-    const uint16_t* gk = A.gtracks ? A.gtracks + ao + p : nullptr;
-    const int N = A.N;
-    const int64_t NN = int64_t(A.K) * N * N;
-    double* g = A.grad ? A.grad + A.gstride * p : nullptr;
-    if (g) for (int64_t k = 0; k < A.gstride; ++k) g[k] = 0.0;
-    const uint8_t* codes = A.codes + A.code_off[p];
-    const int lay = A.end[4 * p + 3];
-    const int G = lay >> 8, R = lay & 0xff;
-    auto tset = [&](int i) -> int { return tk ? int(tk[i - 1]) : 0; };
-    auto gset = [&](int i) -> int {
-        if (!tk) return 0;
-        if (gk) return int(gk[i]);
-        return i == 0 ? (m ? int(tk[0]) : 0) : int(tk[i - 1]);
-    };
-    int32_t* gj = A.guide ? A.guide + ao + p : nullptr;
-    if (gj) {
-        for (int k = 0; k <= m; ++k) gj[k] = -1;
-        gj[0] = 0; gj[m] = n;
-    }
-    int i = A.end[4 * p], j = A.end[4 * p + 1];
-    int tbl = A.end[4 * p + 2];
-    if (gj) gj[i] = j;
-    uint8_t* mv = A.moves ? A.moves + A.moves_off[p] : nullptr;
-    int64_t nm = 0;
-    // emit one move out of (i, j): 0 M, 1 X (gap in B), 2 Y (gap in A)
-    auto emit = [&](int s, int ii, int jj, bool open) {
-        if (mv) mv[nm] = uint8_t(s);
-        ++nm;
-        if (s == 0) {
-            if (g) g[int64_t(tset(ii) * N + ap[ii - 1]) * N + bp[jj - 1]] += 1.0;
-            if (gj) gj[ii - 1] = jj - 1;
-        } else if (s == 1) {
-            if (g) {
-                const int64_t o = NN + 4 * tset(ii);
-                g[o + 3] -= 1.0;
-                if (open) g[o + 2] -= 1.0;
-            }
-            if (gj) gj[ii - 1] = jj;
-        } else {
-            if (g) {
-                const int64_t o = NN + 4 * gset(ii);
-                g[o + 1] -= 1.0;
-                if (open) g[o + 0] -= 1.0;
-            }
-        }
-    };
-    if (A.affine) {
-        while (true) {
-            if (i == 0 && j == 0) break;
-            uint32_t c;
-            if (A.local) {
-                c = (i == 0 || j == 0) ? 3u : code_at(codes, i, j, n, G, R);
-                if (tbl == 0 && (c & 3u) == 3u) break;
-            } else {
-                if (i == 0) { for (; j > 0; --j) emit(2, 0, j, j == 1); break; }
-                if (j == 0) { for (; i > 0; --i) emit(1, i, 0, i == 1); break; }
-                c = code_at(codes, i, j, n, G, R);
-            }
-            if (i == 0) tbl = 2;
-            else if (j == 0) tbl = 1;
-            int prev;
-            auto from_code = [](uint32_t cc) { return cc == 1u ? 1 : (cc == 2u ? 2 : 0); };
-            if (tbl == 0) { prev = from_code(c & 3u); emit(0, i, j, false); --i; --j; }
-            else if (tbl == 1) { prev = from_code((c >> 2) & 3u); emit(1, i, j, prev != 1); --i; }
-            else { prev = from_code(c >> 4); emit(2, i, j, prev != 2); --j; }
-            tbl = prev;
-        }
-    } else {
-        while (true) {
-            if (i == 0 && j == 0) break;
-            int k;
-            if (i == 0) k = A.local ? 3 : 2;
-            else if (j == 0) k = A.local ? 3 : 1;
-            else k = code_at(codes, i, j, n, G, R);
-            if (k == 3) break;
-            if (k == 0) { emit(0, i, j, false); --i; --j; }
-            else if (k == 1) {
-                if (mv) mv[nm] = 1;
-                ++nm;
-                if (g) g[NN + 4 * tset(i) + 3] -= 1.0;
-                if (gj) gj[i - 1] = j;
-                --i;
-            } else {
-                if (mv) mv[nm] = 2;
-                ++nm;
-                if (g) g[NN + 4 * gset(i) + 1] -= 1.0;
-                --j;
-            }
-        }
-    }
-    if (A.path_info) { A.path_info[3 * p] = int32_t(nm); A.path_info[3 * p + 1] = i; A.path_info[3 * p + 2] = j; }
-    if (gj) {
-        // interpolate the rows the path does not fix (aligner.hpp:2734-2749)
-        const int L = m + 1;
-        int lo = 0;
-        while (lo < L) {
-            if (gj[lo] < 0) { ++lo; continue; }
-            int hi = lo + 1;
-            while (hi < L && gj[hi] < 0) ++hi;
-            if (hi == L) { for (int k = lo + 1; k < L; ++k) gj[k] = gj[lo]; break; }
-            for (int k = lo + 1; k < hi; ++k) gj[k] = gj[lo] + (gj[hi] - gj[lo]) * (k - lo) / (hi - lo);
-            lo = hi;
-        }
-    }
-}
-
 }  // namespace nwg

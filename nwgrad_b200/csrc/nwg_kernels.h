@@ -1,0 +1,17 @@
+// Kernel entry tables: the argument blocks and, per precision, the instantiated kernels for
+// each (gap model, mode, tracked, geometry).  The kernels live in nwg_hard_inst.cu and
+// nwg_soft_inst.cu (compiled once per precision), the host logic in nwg_capi.cu.
+#pragma once
+#include "nwg_common.cuh"
+#include "nwg_hard.cuh"
+#include "nwg_soft.cuh"
+
+namespace nwg {
+using HardFn = void (*)(const HardArgs);
+using SoftFn = void (*)(const SoftArgs);
+struct Geo { int G, R; };
+HardFn hard_fn_f32(bool aff, bool loc, bool tr, Geo g);
+HardFn hard_fn_f64(bool aff, bool loc, bool tr, Geo g);
+SoftFn soft_fn_f32(bool aff, bool loc, bool tr, Geo g);
+SoftFn soft_fn_f64(bool aff, bool loc, bool tr, Geo g);
+}  // namespace nwg

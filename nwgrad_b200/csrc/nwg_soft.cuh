@@ -13,13 +13,20 @@
 // Linear gaps are the one-state case (o = e).
 //
 // Layout: the hard kernel's lane strips (nwg_hard.cuh), here over rows 0..m and columns
-// 0..n.  Range: every lane keeps its own power-of-two exponent, renormalised after each
-// step so its largest value lies in [1, 2); values crossing lanes are converted by exact
-// power-of-two factors.  The forward values of every cell (3 per cell, scaled, plus one
-// exponent per lane step) go to a per-group scratch table that the backward pass reads in
-// reverse.  A value that overflows or turns NaN marks the pair refused; the host reruns
-// refused pairs in double precision.  Sums of exponentials and the gradient's gap fields
-// accumulate in double; substitution counts in a per-group shared-memory histogram.
+// 0..n.  Range: every lane keeps its own power-of-two exponent and renormalises its values
+// every `renorm` steps (the host picks the period so that no value can overflow in
+// between: growth per step is at most 3 * the largest weight); values crossing lanes are
+// converted by exact power-of-two factors.  The forward values of every cell (3 per cell,
+// scaled, plus one exponent per lane step) go to a per-group scratch table that the backward
+// pass reads in reverse.  A value that overflows or turns NaN marks the pair refused; the
+// host reruns refused pairs in double precision.
+//
+// Accumulation: each lane keeps its rows' substitution counts in shared memory, laid out
+// [b][lane][row] so one step's R rows update one contiguous R-vector (one 128-bit load and
+// store for R = 4) without conflicts; they are folded into the pair's histogram at the end
+// of every stripe.  Gap counts (untracked) accumulate per step in registers and per pair in
+// double; tracked gap counts per parameter set in shared memory.  log Z and the per-step
+// scale factors 2^(E_F + E_B - E_Z) are formed in double.
 #pragma once
 #include "nwg_common.cuh"
 
@@ -36,10 +43,16 @@ struct SoftArgs {
     void* scratch; int64_t scratch_stride;   // bytes per group slot
     int64_t fwd_bytes;                       // bytes of the forward table within a slot
     int maxn;                                // columns (n) the boundary rows are sized for
+    int renorm_mask;                         // renormalise when (step & renorm_mask) == 0
     double temperature;
     double* score; double* grad; int64_t gstride;
     int32_t* status;                         // per pair: 0 ok, 1 refused (out of range)
 };
+
+// A value handed to a lane whose exponent is more than 2^kLift below the sender's moves the
+// receiver's own state down instead of being scaled up: incoming values then grow by at most
+// 2^kLift, which bounds the renormalisation period the host picks (nwg_capi.cu).
+constexpr int kLift = 32;
 
 // Double accumulator with its own binary exponent: value = m * 2^e.
 struct XAcc {
@@ -53,10 +66,63 @@ struct XAcc {
     }
 };
 
+template <class T> __device__ __forceinline__ T tmax(T a, T b);
+template <> __device__ __forceinline__ float tmax<float>(float a, float b) { return fmaxf(a, b); }
+template <> __device__ __forceinline__ double tmax<double>(double a, double b) { return fmax(a, b); }
+
+// Vector load / store of n values of T (n a multiple of 4 floats or 2 doubles when possible).
+template <class T, int NV>
+__device__ __forceinline__ void vstore(T* dst, const T (&v)[NV]) {
+    if constexpr (sizeof(T) == 4 && NV % 4 == 0) {
+#pragma unroll
+        for (int k = 0; k < NV / 4; ++k)
+            reinterpret_cast<float4*>(dst)[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+    } else if constexpr (sizeof(T) == 8 && NV % 2 == 0) {
+#pragma unroll
+        for (int k = 0; k < NV / 2; ++k)
+            reinterpret_cast<double2*>(dst)[k] = make_double2(v[2 * k], v[2 * k + 1]);
+    } else {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) dst[k] = v[k];
+    }
+}
+template <class T, int NV>
+__device__ __forceinline__ void vload(T (&v)[NV], const T* src) {
+    if constexpr (sizeof(T) == 4 && NV % 4 == 0) {
+#pragma unroll
+        for (int k = 0; k < NV / 4; ++k) {
+            const float4 q = reinterpret_cast<const float4*>(src)[k];
+            v[4 * k] = q.x; v[4 * k + 1] = q.y; v[4 * k + 2] = q.z; v[4 * k + 3] = q.w;
+        }
+    } else if constexpr (sizeof(T) == 8 && NV % 2 == 0) {
+#pragma unroll
+        for (int k = 0; k < NV / 2; ++k) {
+            const double2 q = reinterpret_cast<const double2*>(src)[k];
+            v[2 * k] = q.x; v[2 * k + 1] = q.y;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) v[k] = src[k];
+    }
+}
+
+// Bytes of dynamic shared memory the soft kernel needs for a block of `block` threads.
+__host__ __device__ inline size_t soft_smem_bytes(int K, int N, int G, int R, int block, int tsize, bool tracked) {
+    const int gpb = block / G;
+    size_t b = size_t((K * N + 1) * (N + 1) + 4 * K) * tsize;
+    b = (b + 15) & ~size_t(15);
+    b += size_t(N + 1) * G * R * tsize * gpb;              // per-lane substitution counts
+    if (G > 1) b += size_t(K) * N * N * tsize * gpb;        // per-group histogram
+    b = (b + 15) & ~size_t(15);
+    if (tracked) b += size_t(4) * K * 8 * block;            // per-lane tracked gap sums
+    return b;
+}
+
 template <class T, bool AFF, bool LOC, bool TR, int G, int R>
 __global__ void __launch_bounds__(128) soft_kernel(const SoftArgs A) {
     constexpr int GR = G * R;
     constexpr int NV = AFF ? 3 : 1;          // values per cell
+    constexpr int CV = NV * R;               // values per lane column
     const int N = A.N, K = A.K;
     const int wcols = N + 1;
     const int nw = (K * N + 1) * wcols;
@@ -64,38 +130,42 @@ __global__ void __launch_bounds__(128) soft_kernel(const SoftArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* sw = reinterpret_cast<T*>(smem_raw);
     T* sgw = sw + nw;
-    // per group: the substitution-count histogram (K*N*N T) and tracked gap sums (4K double)
-    const int hsz = K * N * N;
     unsigned char* after = reinterpret_cast<unsigned char*>(sgw + 4 * K);
     after = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(after) + 15) & ~uintptr_t(15));
-    double* sgap_all = reinterpret_cast<double*>(after);
-    T* hist_all = reinterpret_cast<T*>(sgap_all + (TR ? 4 * K * gpb : 0));
+    T* macc_all = reinterpret_cast<T*>(after);
+    T* hist_all = macc_all + size_t(N + 1) * GR * gpb;
+    double* tg_all = reinterpret_cast<double*>(
+        (reinterpret_cast<uintptr_t>(hist_all + (G > 1 ? size_t(K) * N * N * gpb : 0)) + 15) & ~uintptr_t(15));
     for (int k = threadIdx.x; k < nw; k += blockDim.x) sw[k] = static_cast<const T*>(A.w)[k];
     for (int k = threadIdx.x; k < 4 * K; k += blockDim.x) sgw[k] = static_cast<const T*>(A.gw)[k];
 
     const int lane = threadIdx.x % G;
     const int gib = threadIdx.x / G;
     const int64_t slot = int64_t(blockIdx.x) * gpb + gib;
-    T* hist = hist_all + int64_t(gib) * hsz;
-    double* sgap = sgap_all + 4 * K * gib;
-    for (int k = lane; k < hsz; k += G) hist[k] = T(0);
-    if (TR) for (int k = lane; k < 4 * K; k += G) sgap[k] = 0.0;
+    T* macc = macc_all + size_t(N + 1) * GR * gib;          // [b][lane][r]
+    T* hist = hist_all + size_t(K) * N * N * gib;
+    double* tg = tg_all + size_t(4) * K * threadIdx.x;        // tracked gap sums of this lane
+    for (int k = lane; k < (N + 1) * GR; k += G) macc[k] = T(0);
+    if constexpr (G > 1) for (int k = lane; k < K * N * N; k += G) hist[k] = T(0);
+    if constexpr (TR) for (int k = 0; k < 4 * K; ++k) tg[k] = 0.0;
     __syncthreads();
 
     unsigned gmask;
     if constexpr (G == 32) gmask = 0xffffffffu;
     else gmask = ((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1));
+    const int rmask = A.renorm_mask;
 
     unsigned char* sbase = static_cast<unsigned char*>(A.scratch) + slot * A.scratch_stride;
     T* fwd = reinterpret_cast<T*>(sbase);
     int* fexp = reinterpret_cast<int*>(sbase + A.fwd_bytes);
-    // boundary rows: forward (values, exponent) and backward, (maxn + 1) columns each
     const int64_t nb = int64_t(A.maxn) + 1;
     unsigned char* bb = sbase + A.scratch_stride - nb * (2 * NV * sizeof(T) + 2 * sizeof(int));
     T* fbnd = reinterpret_cast<T*>(bb);
     T* bbnd = fbnd + NV * nb;
     int* fbndE = reinterpret_cast<int*>(bbnd + NV * nb);
     int* bbndE = fbndE + nb;
+    // untracked: the one set's gap weights
+    const T oa0 = sgw[0], ea0 = sgw[1], ob0 = sgw[2], eb0 = sgw[3];
 
     for (int64_t it = slot; it < A.n_items; it += int64_t(gridDim.x) * gpb) {
         const int p = A.order[it];
@@ -114,68 +184,70 @@ __global__ void __launch_bounds__(128) soft_kernel(const SoftArgs A) {
         const int rows = m + 1;                 // DP rows 0..m
         const int nstripes = (rows + GR - 1) / GR;
         const int S = n + G;                    // steps: columns 0..n plus the skew
-        const T one = T(1);
         bool bad = false;
 
         // ── forward ──────────────────────────────────────────────────────────
         XAcc zacc; zacc.init();                 // Local: the sum over every cell
         T zM = T(0), zX = T(0), zY = T(0); int zE = 0;   // Global: (m, n)
         for (int s = 0; s < nstripes; ++s) {
-            const int i0 = s * GR + lane * R;   // this lane's first DP row (0-based rows incl. row 0)
+            const int i0 = s * GR + lane * R;   // this lane's first DP row (rows 0..m)
             int key[R];
-            T roa[R], rea[R], rob[R], reb[R];
+            T roa[TR ? R : 1], rea[TR ? R : 1], rob[TR ? R : 1], reb[TR ? R : 1];
+            T vmask[R];
             T cM[R], cX[R], cY[R];
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 const int i = i0 + r;
                 const bool valid = i <= m;
+                vmask[r] = valid ? T(1) : T(0);
                 key[r] = (valid && i >= 1) ? (tset(i) * N + ap[i - 1]) * wcols : K * N * wcols;
-                const int gs = valid ? gset(i) : 0;
-                const int ts = (valid && i >= 1) ? tset(i) : 0;
-                roa[r] = sgw[4 * gs + 0]; rea[r] = sgw[4 * gs + 1];
-                rob[r] = sgw[4 * ts + 2]; reb[r] = sgw[4 * ts + 3];
+                if constexpr (TR) {
+                    const int gs = valid ? gset(i) : 0;
+                    const int ts = (valid && i >= 1) ? tset(i) : 0;
+                    roa[r] = sgw[4 * gs + 0]; rea[r] = sgw[4 * gs + 1];
+                    rob[r] = sgw[4 * ts + 2]; reb[r] = sgw[4 * ts + 3];
+                }
                 cM[r] = T(0); cX[r] = T(0); cY[r] = T(0);
             }
             int E = 0;
-            T lone = one;                         // 2^-E
-            T dgM = T(0), dgX = T(0), dgY = T(0); // row above, column j-1 (column -1: 0)
-            T upM = T(0), upX = T(0), upY = T(0);
-            T* fs = fwd + int64_t(s) * S * G * (NV * R);
+            T lone = T(1);                        // 2^-E: a free start's weight in lane units
+            T zpart = T(0);                       // Local: the cells' sum since the last renorm
+            T dgM = T(0), dgX = T(0), dgY = T(0); // row above, column j-1
+            T upM = T(0), upX = T(0), upY = T(0); // row above, column j
+            T* fs = fwd + int64_t(s) * S * G * CV;
             int* fe = fexp + int64_t(s) * S * G;
             for (int t = 0; t < S; ++t) {
                 const int j = t - lane;           // column 0..n
-                if (lane == 0 && j <= n) {
-                    if (s == 0) { upM = T(0); upX = T(0); upY = T(0); }
-                    else {
-                        const int eb = fbndE[j];
-                        const int d = eb - E;
-                        if (d > 100) {   // keep the incoming values in range: rescale own state down
-                            const T f = pow2i<T>(100 - d);
+                if (lane == 0 && j <= n && s > 0) {
+                    const int eb = fbndE[j];
+                    int d = eb - E;
+                    if (d > kLift) {   // keep the incoming values in range: move own state down
+                        const T f = pow2i<T>(kLift - d);
 #pragma unroll
-                            for (int r = 0; r < R; ++r) { cM[r] *= f; cX[r] *= f; cY[r] *= f; }
-                            dgM *= f; dgX *= f; dgY *= f;
-                            E = eb - 100; lone = pow2i<T>(-E);
-                        }
-                        const T f = pow2i<T>(eb - E);
-                        upM = fbnd[NV * j] * f;
-                        if constexpr (AFF) { upX = fbnd[NV * j + 1] * f; upY = fbnd[NV * j + 2] * f; }
+                        for (int r = 0; r < R; ++r) { cM[r] *= f; cX[r] *= f; cY[r] *= f; }
+                        dgM *= f; dgX *= f; dgY *= f; zpart *= f;
+                        E = eb - kLift; lone = pow2i<T>(-E); d = kLift;
                     }
+                    const T f = pow2i<T>(d);
+                    upM = fbnd[NV * j] * f;
+                    if constexpr (AFF) { upX = fbnd[NV * j + 1] * f; upY = fbnd[NV * j + 2] * f; }
                 }
                 const bool active = (j >= 0) && (j <= n);
                 if (active) {
                     const int bj = j >= 1 ? int(bp[j - 1]) : N;   // column 0: the zero column
                     T pM = dgM, pX = dgX, pY = dgY;
                     T qM = upM, qX = upX, qY = upY;
-                    T mx = T(0);
 #pragma unroll
                     for (int r = 0; r < R; ++r) {
                         const int i = i0 + r;
                         const T wv = sw[key[r] + bj];
+                        const T o_a = TR ? roa[r] : oa0, e_a = TR ? rea[r] : ea0;
+                        const T o_b = TR ? rob[r] : ob0, e_b = TR ? reb[r] : eb0;
                         T fm, fx = T(0), fy = T(0);
                         if constexpr (AFF) {
-                            fm = (pM + pX + pY) * wv;
-                            fx = (qM + qY) * rob[r] + qX * reb[r];
-                            fy = (cM[r] + cX[r]) * roa[r] + cY[r] * rea[r];
+                            fm = ((pM + pX) + pY) * wv;
+                            fx = fmaf_t(qM + qY, o_b, qX * e_b);
+                            fy = fmaf_t(cM[r] + cX[r], o_a, cY[r] * e_a);
                             if constexpr (LOC) {
                                 fm += lone;
                                 if (j == 0) fx = T(0);
@@ -184,7 +256,7 @@ __global__ void __launch_bounds__(128) soft_kernel(const SoftArgs A) {
                                 if (i == 0 && j == 0) fm = lone;
                             }
                         } else {
-                            fm = pM * wv + qM * reb[r] + cM[r] * rea[r];
+                            fm = fmaf_t(pM, wv, fmaf_t(qM, e_b, cM[r] * e_a));
                             if constexpr (LOC) {
                                 if (i == 0 || j == 0) fm = T(0);
                                 fm += lone;
@@ -192,40 +264,41 @@ __global__ void __launch_bounds__(128) soft_kernel(const SoftArgs A) {
                                 if (i == 0 && j == 0) fm = lone;
                             }
                         }
-                        if (i > m) { fm = T(0); fx = T(0); fy = T(0); }
                         pM = cM[r]; pX = cX[r]; pY = cY[r];
                         cM[r] = fm; cX[r] = fx; cY[r] = fy;
                         qM = fm; qX = fx; qY = fy;
-                        mx = rmax(mx, rmax3(fm, fx, fy));
+                        if constexpr (LOC) zpart = fmaf_t(vmask[r], (fm + fx) + fy, zpart);
                     }
                     dgM = upM; dgX = upX; dgY = upY;
-                    // renormalise: the lane's largest value into [1, 2)
-                    if (!is_finite(mx)) bad = true;
-                    else if (mx > T(0)) {
-                        int e = ilog2(mx);
-                        if (e < -120) e = -120;
-                        if (e != 0) {
-                            const T f = pow2i<T>(-e);
+                    if ((t & rmask) == 0 || j == n) {
+                        // renormalise: the lane's largest value into [1, 2)
+                        T mx = T(0);
 #pragma unroll
-                            for (int r = 0; r < R; ++r) { cM[r] *= f; cX[r] *= f; cY[r] *= f; }
-                            dgM *= f; dgX *= f; dgY *= f;
-                            E += e; lone = pow2i<T>(-E);
+                        for (int r = 0; r < R; ++r) mx = tmax(mx, tmax(cM[r], tmax(cX[r], cY[r])));
+                        if (!is_finite(mx)) bad = true;
+                        else if (mx > T(0)) {
+                            int e = ilog2(mx);
+                            if (e < -120) e = -120;
+                            if (LOC) zacc.add(static_cast<double>(zpart), E);
+                            zpart = T(0);
+                            if (e != 0) {
+                                const T f = pow2i<T>(-e);
+#pragma unroll
+                                for (int r = 0; r < R; ++r) { cM[r] *= f; cX[r] *= f; cY[r] *= f; }
+                                dgM *= f; dgX *= f; dgY *= f;
+                                E += e; lone = pow2i<T>(-E);
+                            }
                         }
                     }
                     // store the column for the backward pass
-                    T* dst = fs + (int64_t(t) * G + lane) * (NV * R);
+                    T v[CV];
 #pragma unroll
                     for (int r = 0; r < R; ++r) {
-                        dst[NV * r] = cM[r];
-                        if constexpr (AFF) { dst[NV * r + 1] = cX[r]; dst[NV * r + 2] = cY[r]; }
+                        v[NV * r] = cM[r];
+                        if constexpr (AFF) { v[NV * r + 1] = cX[r]; v[NV * r + 2] = cY[r]; }
                     }
+                    vstore<T, CV>(fs + (int64_t(t) * G + lane) * CV, v);
                     fe[int64_t(t) * G + lane] = E;
-                    if constexpr (LOC) {
-                        T cs = T(0);
-#pragma unroll
-                        for (int r = 0; r < R; ++r) cs += (cM[r] + cX[r]) + cY[r];
-                        zacc.add(static_cast<double>(cs), E);
-                    }
                 }
                 if constexpr (G > 1) {
                     const T sM = __shfl_up_sync(gmask, cM[R - 1], 1, G);
@@ -237,13 +310,12 @@ __global__ void __launch_bounds__(128) soft_kernel(const SoftArgs A) {
                     const int sE = __shfl_up_sync(gmask, E, 1, G);
                     if (lane > 0) {
                         int d = sE - E;
-                        if (d > 100) {
-                            const T f = pow2i<T>(100 - d);
+                        if (d > kLift) {
+                            const T f = pow2i<T>(kLift - d);
 #pragma unroll
                             for (int r = 0; r < R; ++r) { cM[r] *= f; cX[r] *= f; cY[r] *= f; }
-                            dgM *= f; dgX *= f; dgY *= f;
-                            E = sE - 100; lone = pow2i<T>(-E);
-                            d = 100;
+                            dgM *= f; dgX *= f; dgY *= f; zpart *= f;
+                            E = sE - kLift; lone = pow2i<T>(-E); d = kLift;
                         }
                         const T f = pow2i<T>(d);
                         upM = sM * f; upX = sX * f; upY = sY * f;
@@ -255,6 +327,7 @@ __global__ void __launch_bounds__(128) soft_kernel(const SoftArgs A) {
                     fbndE[j] = E;
                 }
             }
+            if constexpr (LOC) { zacc.add(static_cast<double>(zpart), E); }
             if constexpr (!LOC) {
                 if (m >= i0 && m < i0 + R) {
 #pragma unroll
@@ -274,12 +347,10 @@ __global__ void __launch_bounds__(128) soft_kernel(const SoftArgs A) {
                     const int oe = __shfl_xor_sync(gmask, zacc.e, off, G);
                     zacc.add(om, oe);
                 }
+                zacc.m = __shfl_sync(gmask, zacc.m, 0, G);
+                zacc.e = __shfl_sync(gmask, zacc.e, 0, G);
             }
             zm = zacc.m; ze = zacc.e;
-            if constexpr (G > 1) {   // one value for the whole group (lanes summed in different orders)
-                zm = __shfl_sync(gmask, zm, 0, G);
-                ze = __shfl_sync(gmask, ze, 0, G);
-            }
         } else {
             zm = static_cast<double>((zM + zX) + zY); ze = zE;
             if constexpr (G > 1) {
@@ -298,150 +369,162 @@ __global__ void __launch_bounds__(128) soft_kernel(const SoftArgs A) {
         const double invz = 1.0 / zhat;
 
         // ── backward, fused with the expected counts ─────────────────────────
-        double ga_o = 0, ga_e = 0, gb_o = 0, gb_e = 0;   // untracked gap sums (scaled counts)
+        double ga_o = 0, ga_x = 0, gb_o = 0, gb_x = 0;   // untracked: opens and extend-only moves
+        if constexpr (G == 1) {
+            double* g1 = A.grad + A.gstride * p;
+            for (int k = 0; k < K * N * N; ++k) g1[k] = 0.0;
+        }
         for (int s = nstripes - 1; s >= 0; --s) {
             const int i0 = s * GR + lane * R;
-            int keyd[R], hrow[R];
-            T roa[R], rea[R], rob[R], reb[R];      // rob/reb: the row BELOW (i+1)
-            int gsr[R], tsd[R];
+            int keyd[R], krow[R];
+            T roa[TR ? R : 1], rea[TR ? R : 1], rob[TR ? R : 1], reb[TR ? R : 1];   // rob/reb: row i+1
+            int gsr[TR ? R : 1], tsd[TR ? R : 1];
+            T vmask[R];
             T bM[R], bX[R], bY[R];
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 const int i = i0 + r;
                 const bool valid = i <= m;
-                const int gs = valid ? gset(i) : 0;
+                vmask[r] = valid ? T(1) : T(0);
                 const int td = (i + 1 <= m) ? tset(i + 1) : 0;
-                gsr[r] = gs; tsd[r] = td;
                 const int kd = (i + 1 <= m) ? (td * N + ap[i]) : K * N;
                 keyd[r] = kd * wcols;
-                hrow[r] = kd * N;
-                roa[r] = sgw[4 * gs + 0]; rea[r] = sgw[4 * gs + 1];
-                rob[r] = sgw[4 * td + 2]; reb[r] = sgw[4 * td + 3];
+                krow[r] = kd;
+                if constexpr (TR) {
+                    const int gs = valid ? gset(i) : 0;
+                    gsr[r] = gs; tsd[r] = td;
+                    roa[r] = sgw[4 * gs + 0]; rea[r] = sgw[4 * gs + 1];
+                    rob[r] = sgw[4 * td + 2]; reb[r] = sgw[4 * td + 3];
+                }
                 bM[r] = T(0); bX[r] = T(0); bY[r] = T(0);
             }
             int EB = 0;
-            T lone = one;
+            T lone = T(1);
             T dgM = T(0);                             // row below, column j+1 (BM only)
             T dnM = T(0), dnX = T(0), dnY = T(0);     // row below, column j
-            const T* fs = fwd + int64_t(s) * S * G * (NV * R);
+            const T* fs = fwd + int64_t(s) * S * G * CV;
             const int* fe = fexp + int64_t(s) * S * G;
             for (int t = 0; t < S; ++t) {
                 const int j = n - t + (G - 1 - lane);     // column n..0
-                if (lane == G - 1 && j >= 0) {
-                    if (s == nstripes - 1) { dnM = T(0); dnX = T(0); dnY = T(0); }
-                    else {
-                        const int eb = bbndE[j];
-                        int d = eb - EB;
-                        if (d > 100) {
-                            const T f = pow2i<T>(100 - d);
+                if (lane == G - 1 && j >= 0 && s < nstripes - 1) {
+                    const int eb = bbndE[j];
+                    int d = eb - EB;
+                    if (d > kLift) {
+                        const T f = pow2i<T>(kLift - d);
 #pragma unroll
-                            for (int r = 0; r < R; ++r) { bM[r] *= f; bX[r] *= f; bY[r] *= f; }
-                            dgM *= f;
-                            EB = eb - 100; lone = pow2i<T>(-EB);
-                            d = 100;
-                        }
-                        const T f = pow2i<T>(d);
-                        dnM = bbnd[NV * j] * f;
-                        if constexpr (AFF) { dnX = bbnd[NV * j + 1] * f; dnY = bbnd[NV * j + 2] * f; }
-                        else { dnX = dnM; dnY = dnM; }
+                        for (int r = 0; r < R; ++r) { bM[r] *= f; bX[r] *= f; bY[r] *= f; }
+                        dgM *= f;
+                        EB = eb - kLift; lone = pow2i<T>(-EB); d = kLift;
                     }
+                    const T f = pow2i<T>(d);
+                    dnM = bbnd[NV * j] * f;
+                    if constexpr (AFF) { dnX = bbnd[NV * j + 1] * f; dnY = bbnd[NV * j + 2] * f; }
+                    else { dnX = dnM; dnY = dnM; }
                 }
                 const bool active = (j >= 0) && (j <= n);
                 if (active) {
-                    const int bj1 = j < n ? int(bp[j]) : N;   // b code of column j+1
-                    const T* src = fs + (int64_t(j + lane) * G + lane) * (NV * R);
+                    const int bj1 = j < n ? int(bp[j]) : N;   // b code of column j+1 (N: none)
+                    T f[CV];
+                    vload<T, CV>(f, fs + (int64_t(j + lane) * G + lane) * CV);
                     const int EF = fe[int64_t(j + lane) * G + lane];
-                    T dM = dgM;                  // row below, column j+1
-                    T xM = dnM, xX = dnX, xY = dnY;   // row below, column j
-                    T sgo_a = T(0), sge_a = T(0), sgo_b = T(0), sge_b = T(0);
-                    // scale of this step's products: 2^(EF + EB - EZ) / zhat
+                    // scale of this step's products: 2^(E_F + E_B - E_Z) / zhat
                     const double facd = pow2i<double>(EF + EB - EZ) * invz;
                     const T fac = static_cast<T>(facd);
                     if (!is_finite(fac)) bad = true;
-                    T mx = T(0);
+                    T dM = dgM;                       // row below, column j+1
+                    T xM = dnM, xX = dnX, xY = dnY;   // row below, column j
+                    T so_b = T(0), sx_b = T(0), so_a = T(0), sx_a = T(0);
+                    T mc[R];
+                    const bool noX = LOC && j == 0;   // Local: no gap move into column 0
 #pragma unroll
                     for (int r = R - 1; r >= 0; --r) {
                         const int i = i0 + r;
                         const T wv = sw[keyd[r] + bj1];
-                        const T fm = src[NV * r];
-                        T fx = T(0), fy = T(0);
-                        if constexpr (AFF) { fx = src[NV * r + 1]; fy = src[NV * r + 2]; }
+                        const T fm = f[NV * r];
+                        const T o_a = TR ? roa[r] : oa0, e_a = TR ? rea[r] : ea0;
+                        const T o_b = TR ? rob[r] : ob0, e_b = TR ? reb[r] : eb0;
                         const T D = wv * dM;
                         T nM, nX, nY;
                         if constexpr (AFF) {
-                            T tX = rob[r] * xX, eX = reb[r] * xX;
-                            T tY = roa[r] * bY[r], eY = rea[r] * bY[r];
+                            const T fx = f[NV * r + 1], fy = f[NV * r + 2];
+                            T dX = noX ? T(0) : xX;                    // BX(i+1, j)
+                            T rY = (LOC && i == 0) ? T(0) : bY[r];     // BY(i, j+1)
+                            nM = fmaf_t(o_a, rY, fmaf_t(o_b, dX, D));
+                            nX = fmaf_t(o_a, rY, fmaf_t(e_b, dX, D));
+                            nY = fmaf_t(e_a, rY, fmaf_t(o_b, dX, D));
                             if constexpr (LOC) {
-                                if (j == 0) { tX = T(0); eX = T(0); }
-                                if (i == 0) { tY = T(0); eY = T(0); }
-                            }
-                            nM = D + tX + tY; nX = D + eX + tY; nY = D + tX + eY;
-                            if constexpr (LOC) { nM += lone; nX += lone; nY += lone; }
-                            else if (i == m && j == n) { nM = lone; nX = lone; nY = lone; }
-                            // counts of the moves out of (i, j)
-                            const T fsum = (fm + fx) + fy;
-                            if (i < m && j < n) {
-                                const T c = fsum * D * fac;
-                                atomicAdd(&hist[hrow[r] + bj1], c);
-                            }
-                            const T oX = (fm + fy) * tX, xx = fx * eX;
-                            const T oY = (fm + fx) * tY, yy = fy * eY;
+                                nM = fmaf_t(vmask[r], lone, nM);
+                                nX = fmaf_t(vmask[r], lone, nX);
+                                nY = fmaf_t(vmask[r], lone, nY);
+                            } else if (i == m && j == n) { nM = lone; nX = lone; nY = lone; }
+                            const T fmy = fm + fy, fmx = fm + fx;
+                            mc[r] = (fmy + fx) * D;
                             if constexpr (TR) {
-                                if (i < m) {
-                                    const double ob = static_cast<double>(oX) * facd;
-                                    atomicAdd(&sgap[4 * tsd[r] + 2], ob);
-                                    atomicAdd(&sgap[4 * tsd[r] + 3], ob + static_cast<double>(xx) * facd);
-                                }
-                                if (i <= m) {
-                                    const double oa = static_cast<double>(oY) * facd;
-                                    atomicAdd(&sgap[4 * gsr[r] + 0], oa);
-                                    atomicAdd(&sgap[4 * gsr[r] + 1], oa + static_cast<double>(yy) * facd);
-                                }
+                                const double ob_c = static_cast<double>(fmy * o_b * dX) * facd;
+                                const double eb_c = static_cast<double>(fx * e_b * dX) * facd;
+                                const double oa_c = static_cast<double>(fmx * o_a * rY) * facd;
+                                const double ea_c = static_cast<double>(fy * e_a * rY) * facd;
+                                double* gb = tg + 4 * tsd[r];
+                                double* ga = tg + 4 * gsr[r];
+                                gb[2] += ob_c; gb[3] += ob_c + eb_c;
+                                ga[0] += oa_c; ga[1] += oa_c + ea_c;
                             } else {
-                                if (i < m) { sgo_b += oX; sge_b += oX + xx; }
-                                if (i <= m) { sgo_a += oY; sge_a += oY + yy; }
+                                so_b = fmaf_t(fmy, dX, so_b); sx_b = fmaf_t(fx, dX, sx_b);
+                                so_a = fmaf_t(fmx, rY, so_a); sx_a = fmaf_t(fy, rY, sx_a);
                             }
                         } else {
-                            T tX = reb[r] * xM;
-                            T tY = rea[r] * bM[r];
-                            if constexpr (LOC) {
-                                if (j == 0) tX = T(0);
-                                if (i == 0) tY = T(0);
-                            }
-                            nM = D + tX + tY;
-                            if constexpr (LOC) nM += lone;
+                            T dX = noX ? T(0) : xM;
+                            T rY = (LOC && i == 0) ? T(0) : bM[r];
+                            nM = fmaf_t(e_a, rY, fmaf_t(e_b, dX, D));
+                            if constexpr (LOC) nM = fmaf_t(vmask[r], lone, nM);
                             else if (i == m && j == n) nM = lone;
                             nX = nM; nY = nM;
-                            if (i < m && j < n) atomicAdd(&hist[hrow[r] + bj1], fm * D * fac);
+                            mc[r] = fm * D;
                             if constexpr (TR) {
-                                if (i < m) atomicAdd(&sgap[4 * tsd[r] + 3], static_cast<double>(fm * tX) * facd);
-                                if (i <= m) atomicAdd(&sgap[4 * gsr[r] + 1], static_cast<double>(fm * tY) * facd);
+                                tg[4 * tsd[r] + 3] += static_cast<double>(fm * e_b * dX) * facd;
+                                tg[4 * gsr[r] + 1] += static_cast<double>(fm * e_a * rY) * facd;
                             } else {
-                                if (i < m) sge_b += fm * tX;
-                                if (i <= m) sge_a += fm * tY;
+                                sx_b = fmaf_t(fm, dX, sx_b);
+                                sx_a = fmaf_t(fm, rY, sx_a);
                             }
                         }
-                        if (i > m) { nM = T(0); nX = T(0); nY = T(0); }
                         dM = bM[r];
                         bM[r] = nM; bX[r] = nX; bY[r] = nY;
                         xM = nM; xX = nX; xY = nY;
-                        mx = rmax(mx, rmax3(nM, nX, nY));
+                    }
+                    // substitution counts of this column: one R-vector read-modify-write
+                    {
+                        T* dst = macc + (size_t(bj1) * G + lane) * R;
+                        T cur[R];
+                        vload<T, R>(cur, dst);
+#pragma unroll
+                        for (int r = 0; r < R; ++r) cur[r] = fmaf_t(mc[r], fac, cur[r]);
+                        vstore<T, R>(dst, cur);
                     }
                     if constexpr (!TR) {
-                        ga_o += static_cast<double>(sgo_a) * facd; ga_e += static_cast<double>(sge_a) * facd;
-                        gb_o += static_cast<double>(sgo_b) * facd; gb_e += static_cast<double>(sge_b) * facd;
+                        if constexpr (AFF) {
+                            gb_o = fma(static_cast<double>(so_b), facd, gb_o);
+                            ga_o = fma(static_cast<double>(so_a), facd, ga_o);
+                        }
+                        gb_x = fma(static_cast<double>(sx_b), facd, gb_x);
+                        ga_x = fma(static_cast<double>(sx_a), facd, ga_x);
                     }
                     dgM = dnM;
-                    if (!is_finite(mx)) bad = true;
-                    else if (mx > T(0)) {
-                        int e = ilog2(mx);
-                        if (e < -120) e = -120;
-                        if (e != 0) {
-                            const T f = pow2i<T>(-e);
+                    if ((t & rmask) == 0 || j == 0) {
+                        T mx = T(0);
 #pragma unroll
-                            for (int r = 0; r < R; ++r) { bM[r] *= f; bX[r] *= f; bY[r] *= f; }
-                            dgM *= f;
-                            EB += e; lone = pow2i<T>(-EB);
+                        for (int r = 0; r < R; ++r) mx = tmax(mx, tmax(bM[r], tmax(bX[r], bY[r])));
+                        if (!is_finite(mx)) bad = true;
+                        else if (mx > T(0)) {
+                            int e = ilog2(mx);
+                            if (e < -120) e = -120;
+                            if (e != 0) {
+                                const T fsc = pow2i<T>(-e);
+#pragma unroll
+                                for (int r = 0; r < R; ++r) { bM[r] *= fsc; bX[r] *= fsc; bY[r] *= fsc; }
+                                dgM *= fsc;
+                                EB += e; lone = pow2i<T>(-EB);
+                            }
                         }
                     }
                 }
@@ -455,16 +538,15 @@ __global__ void __launch_bounds__(128) soft_kernel(const SoftArgs A) {
                     const int sE = __shfl_down_sync(gmask, EB, 1, G);
                     if (lane < G - 1) {
                         int d = sE - EB;
-                        if (d > 100) {
-                            const T f = pow2i<T>(100 - d);
+                        if (d > kLift) {
+                            const T fsc = pow2i<T>(kLift - d);
 #pragma unroll
-                            for (int r = 0; r < R; ++r) { bM[r] *= f; bX[r] *= f; bY[r] *= f; }
-                            dgM *= f;
-                            EB = sE - 100; lone = pow2i<T>(-EB);
-                            d = 100;
+                            for (int r = 0; r < R; ++r) { bM[r] *= fsc; bX[r] *= fsc; bY[r] *= fsc; }
+                            dgM *= fsc;
+                            EB = sE - kLift; lone = pow2i<T>(-EB); d = kLift;
                         }
-                        const T f = pow2i<T>(d);
-                        dnM = sM * f; dnX = sX * f; dnY = sY * f;
+                        const T fsc = pow2i<T>(d);
+                        dnM = sM * fsc; dnX = sX * fsc; dnY = sY * fsc;
                     }
                 }
                 if (lane == 0 && active && s > 0) {
@@ -473,32 +555,72 @@ __global__ void __launch_bounds__(128) soft_kernel(const SoftArgs A) {
                     bbndE[j] = EB;
                 }
             }
-            if constexpr (G > 1) __syncwarp(gmask);
+            // fold this stripe's per-lane substitution counts into the pair's histogram (one
+            // lane per pair: straight into the pair's gradient, zeroed before the pass)
+            if constexpr (G == 1) {
+                double* g1 = A.grad + A.gstride * p;
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    if (krow[r] >= K * N) continue;
+                    for (int c = 0; c < N; ++c) {
+                        T& v = macc[(size_t(c) * G + lane) * R + r];
+                        if (v != T(0)) g1[krow[r] * N + c] += static_cast<double>(v);
+                        v = T(0);
+                    }
+                }
+            }
+            if constexpr (G > 1) {
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    if (krow[r] >= K * N) continue;
+                    for (int c = 0; c < N; ++c) {
+                        T& v = macc[(size_t(c) * G + lane) * R + r];
+                        if (v != T(0)) atomicAdd(&hist[krow[r] * N + c], v);
+                        v = T(0);
+                    }
+                }
+                __syncwarp(gmask);
+            }
         }
         if constexpr (G > 1) bad = __any_sync(gmask, bad);
-        // reduce the untracked gap sums over the group and write the pair's results
         if constexpr (!TR && G > 1) {
 #pragma unroll
             for (int off = G / 2; off > 0; off >>= 1) {
                 ga_o += __shfl_xor_sync(gmask, ga_o, off, G);
-                ga_e += __shfl_xor_sync(gmask, ga_e, off, G);
+                ga_x += __shfl_xor_sync(gmask, ga_x, off, G);
                 gb_o += __shfl_xor_sync(gmask, gb_o, off, G);
-                gb_e += __shfl_xor_sync(gmask, gb_e, off, G);
+                gb_x += __shfl_xor_sync(gmask, gb_x, off, G);
             }
         }
-        if constexpr (G > 1) __syncwarp(gmask);
         double* g = A.grad + A.gstride * p;
         const int64_t NN = int64_t(K) * N * N;
         if (bad) {
             if (lane == 0) { A.status[p] = 1; A.score[p] = 0.0; }
         } else {
-            for (int k = lane; k < hsz; k += G) g[k] = static_cast<double>(hist[k]);
+            if constexpr (G > 1)
+                for (int k = lane; k < K * N * N; k += G) g[k] = static_cast<double>(hist[k]);
             if constexpr (TR) {
-                for (int k = lane; k < 4 * K; k += G) g[NN + k] = -sgap[k];
+                for (int k = lane; k < 4 * K; k += G) g[NN + k] = 0.0;
+                if constexpr (G > 1) __syncwarp(gmask);
+                for (int k = 0; k < 4 * K; ++k) {
+                    double v = tg[k];
+                    if constexpr (G > 1) {
+#pragma unroll
+                        for (int off = G / 2; off > 0; off >>= 1) v += __shfl_xor_sync(gmask, v, off, G);
+                    }
+                    if (lane == 0) g[NN + k] = 0.0 - v;
+                }
             } else {
                 for (int k = lane; k < 4 * K; k += G) g[NN + k] = 0.0;
+                if constexpr (G > 1) __syncwarp(gmask);
                 if (lane == 0) {
-                    g[NN + 0] = -ga_o; g[NN + 1] = -ga_e; g[NN + 2] = -gb_o; g[NN + 3] = -gb_e;
+                    // opens carry o = exp(-(go+ge)/T); an opening move also extends
+                    const double cga_o = AFF ? static_cast<double>(oa0) * ga_o : 0.0;
+                    const double cgb_o = AFF ? static_cast<double>(ob0) * gb_o : 0.0;
+                    g[NN + 0] = 0.0 - cga_o;
+                    g[NN + 1] = 0.0 - (cga_o + static_cast<double>(ea0) * ga_x);
+                    g[NN + 2] = 0.0 - cgb_o;
+                    g[NN + 3] = 0.0 - (cgb_o + static_cast<double>(eb0) * gb_x);
                 }
             }
             if (lane == 0) {
@@ -506,9 +628,11 @@ __global__ void __launch_bounds__(128) soft_kernel(const SoftArgs A) {
                 A.score[p] = A.temperature * (log(zhat) + double(EZ) * 0.69314718055994530942);
             }
         }
-        if constexpr (G > 1) __syncwarp(gmask);
-        for (int k = lane; k < hsz; k += G) hist[k] = T(0);
-        if (TR) for (int k = lane; k < 4 * K; k += G) sgap[k] = 0.0;
+        if constexpr (G > 1) {
+            __syncwarp(gmask);
+            for (int k = lane; k < K * N * N; k += G) hist[k] = T(0);
+        }
+        if constexpr (TR) for (int k = 0; k < 4 * K; ++k) tg[k] = 0.0;
         if constexpr (G > 1) __syncwarp(gmask);
     }
 }

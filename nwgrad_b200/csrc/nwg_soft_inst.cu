@@ -1,0 +1,24 @@
+// Soft-path kernels for one precision (NWG_T: float or double), every compiled geometry.
+#include "nwg_kernels.h"
+
+namespace nwg {
+namespace {
+template <class T, bool AFF, bool LOC, bool TR>
+SoftFn pick(Geo g) {
+#define NWG_S(GG, RR) if (g.G == GG && g.R == RR) return &soft_kernel<T, AFF, LOC, TR, GG, RR>;
+    NWG_S(1, 8) NWG_S(1, 16) NWG_S(1, 24) NWG_S(1, 32) NWG_S(32, 2) NWG_S(32, 4) NWG_S(32, 8)
+#undef NWG_S
+    return nullptr;
+}
+}  // namespace
+
+SoftFn NWG_SOFT_FN(bool aff, bool loc, bool tr, Geo g) {
+    using T = NWG_T;
+    if (aff) {
+        if (loc) return tr ? pick<T, true, true, true>(g) : pick<T, true, true, false>(g);
+        return tr ? pick<T, true, false, true>(g) : pick<T, true, false, false>(g);
+    }
+    if (loc) return tr ? pick<T, false, true, true>(g) : pick<T, false, true, false>(g);
+    return tr ? pick<T, false, false, true>(g) : pick<T, false, false, false>(g);
+}
+}  // namespace nwg

@@ -1,0 +1,145 @@
+"""Generate the golden fixtures in tests/golden/ from the REFERENCE itself.
+
+Run in a checkout that has the reference sources (michalsta/nwgrad) at REF below and the
+reference driver built (``make -C oracle ref``):
+
+    python tests/golden/make_golden.py
+
+Two sources, both the reference's own code run here:
+
+* ``bruteforce.npz`` -- the reference test suite's exhaustive path enumerator
+  (tests/Python/bruteforce.py, imported from the reference tree): global / local scores,
+  global log Z and expected (soft) counts, and hard counts on unique optima, for tiny pairs.
+* ``reference_batches.npz`` -- the reference's C++ batch engine (SeqPairBatchT, scalar
+  backend, traceback "pointers"; soft: SeqPairBatchT<double>, log space) on seeded random
+  batches: per-pair scores, gradients and guides, hard at float32 and float64, soft at
+  T = 1 and 0.5, tracked with three parameter sets, and banded re-alignment after a step.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+REF = os.environ.get("NWGRAD_REFERENCE", "/root/reference")
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(REF, "tests", "Python"))
+
+import oracle  # noqa: E402
+from nwgrad_b200.params import AlignParams  # noqa: E402
+
+DNA = "ACGT"
+
+
+def brute_fixtures():
+    import bruteforce as bf   # the reference's own enumerator
+    rng = np.random.default_rng(2024)
+    rows = []
+    for case in range(40):
+        la, lb = int(rng.integers(1, 6)), int(rng.integers(1, 6))
+        a = "".join(rng.choice(list(DNA), size=la))
+        b = "".join(rng.choice(list(DNA), size=lb))
+        mat = rng.integers(-3, 6, size=(4, 4)).astype(np.float64)
+        gaps = rng.uniform(0.5, 3.0, size=4).round(2)
+        p = AlignParams(mat, *gaps, alphabet=DNA)
+        for affine in (True, False):
+            gs = bf.global_score(a, b, p, affine)
+            ls = bf.local_score(a, b, p, affine)
+            lz = bf.global_log_z(a, b, p, affine)
+            pairs, oa, ea, ob, eb = bf.global_soft_counts(a, b, p, affine)
+            soft = np.zeros(16 + 4)
+            for (x, y), v in pairs.items():
+                soft[DNA.index(x) * 4 + DNA.index(y)] += v
+            soft[16:] = [-oa, -ea, -ob, -eb]   # counts -> gradient sign convention
+            # hard counts only where the optimum is unique
+            scored = list(bf._scored_paths(a, b, p, affine))
+            best = max(s for _, s in scored)
+            unique = sum(1 for _, s in scored if s == best) == 1
+            hard = np.full(20, np.nan)
+            if unique:
+                hp, hoa, hea, hob, heb = bf.global_hard_counts(a, b, p, affine)
+                hard[:] = 0
+                for (x, y), v in hp.items():
+                    hard[DNA.index(x) * 4 + DNA.index(y)] += v
+                hard[16:] = [-hoa, -hea, -hob, -heb]
+            rows.append(dict(a=a, b=b, mat=mat, gaps=gaps, affine=affine, global_score=gs, local_score=ls,
+                             log_z=lz, soft=soft, hard=hard))
+    np.savez_compressed(os.path.join(HERE, "bruteforce.npz"),
+                        a=np.array([r["a"] for r in rows]), b=np.array([r["b"] for r in rows]),
+                        mat=np.stack([r["mat"] for r in rows]), gaps=np.stack([r["gaps"] for r in rows]),
+                        affine=np.array([r["affine"] for r in rows]),
+                        global_score=np.array([r["global_score"] for r in rows]),
+                        local_score=np.array([r["local_score"] for r in rows]),
+                        log_z=np.array([r["log_z"] for r in rows]),
+                        soft=np.stack([r["soft"] for r in rows]), hard=np.stack([r["hard"] for r in rows]))
+    print("bruteforce.npz:", len(rows), "cases")
+
+
+def ref_fixtures():
+    rng = np.random.default_rng(99)
+    AA = "ACDEFGHIKLMNPQRSTVWY"
+    out = {}
+    cases = []
+    for name, alpha, K, n, lo, hi, integer in (("prot", AA, 1, 24, 0, 60, True),
+                                                ("protf", AA, 1, 16, 1, 50, False),
+                                                ("rna3", "ACGTU", 3, 24, 1, 40, False)):
+        N = len(alpha)
+        if integer:
+            mat = rng.integers(-4, 4, size=(K, N, N)).astype(np.float64)
+            for k in range(K):
+                mat[k][np.diag_indices(N)] = rng.integers(4, 12, size=N)
+            gaps = np.tile([11.0, 1.0, 11.0, 1.0], (K, 1))
+        else:
+            mat = rng.normal(0, 2, size=(K, N, N)).round(3)
+            gaps = rng.uniform(0.3, 4.0, size=(K, 4)).round(3)
+        sa = ["".join(rng.choice(list(alpha), size=int(rng.integers(lo, hi + 1)))) for _ in range(n)]
+        sb = ["".join(rng.choice(list(alpha), size=int(rng.integers(lo, hi + 1)))) for _ in range(n)]
+        tr = gt = None
+        if K > 1:
+            tr = np.concatenate([rng.integers(0, K, size=len(s)) for s in sa]).astype(np.uint16)
+            gt = np.concatenate([rng.integers(0, K, size=len(s) + 1) for s in sa]).astype(np.uint16)
+        mat2 = (mat + rng.normal(0, 0.3, size=mat.shape)).round(3)
+        gaps2 = (gaps + rng.uniform(0, 0.2, size=gaps.shape)).round(3)
+        cases.append((name, alpha, mat, gaps, sa, sb, tr, gt, mat2, gaps2))
+    for name, alpha, mat, gaps, sa, sb, tr, gt, mat2, gaps2 in cases:
+        pre = f"{name}_"
+        out[pre + "alpha"] = np.array(alpha)
+        out[pre + "mat"] = mat
+        out[pre + "gaps"] = gaps
+        out[pre + "mat2"] = mat2
+        out[pre + "gaps2"] = gaps2
+        out[pre + "sa"] = np.array(sa)
+        out[pre + "sb"] = np.array(sb)
+        if tr is not None:
+            out[pre + "tracks"] = tr
+            out[pre + "gap_tracks"] = gt
+        for gm in (0, 1):
+            for am in (0, 1):
+                for prec in (32, 64):
+                    r = oracle.ref_run(prec, gm, am, 1, alpha, mat, gaps, sa, sb, tracks=tr, gap_tracks=gt)
+                    key = f"{pre}hard{prec}_g{gm}_m{am}_"
+                    out[key + "scores"] = r["scores"]
+                    out[key + "grads"] = r["grads"]
+                    out[key + "guides"] = r["guides"]
+                    rb = oracle.ref_run(prec, gm, am, 1, alpha, mat, gaps, sa, sb, tracks=tr, gap_tracks=gt,
+                                        band=4, mat2=mat2, gaps2=gaps2)
+                    key = f"{pre}band{prec}_g{gm}_m{am}_"
+                    out[key + "scores"] = rb["scores"]
+                    out[key + "grads"] = rb["grads"]
+                    out[key + "guides"] = rb["guides"]
+                for T in (1.0, 0.5):
+                    r = oracle.ref_run(64, gm, am, 2, alpha, mat, gaps, sa, sb, tracks=tr, gap_tracks=gt,
+                                       soft_impl=2, temperature=T)
+                    key = f"{pre}soft_T{T}_g{gm}_m{am}_"
+                    out[key + "scores"] = r["scores"]
+                    out[key + "grads"] = r["grads"]
+    np.savez_compressed(os.path.join(HERE, "reference_batches.npz"), **out)
+    print("reference_batches.npz:", len(out), "arrays")
+
+
+if __name__ == "__main__":
+    brute_fixtures()
+    ref_fixtures()

@@ -1,0 +1,105 @@
+"""The oracle pinned to the reference: its golden fixtures (the reference's brute-force
+enumerator and its C++ batch engine, tests/golden/make_golden.py) and, where the reference
+driver is built here, live random cases."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import AA, encode, rand_matrix, rand_seqs
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+DNA = "ACGT"
+
+
+def _enc1(alpha, a, b):
+    return oracle.Encoded(encode(alpha, [a]), encode(alpha, [b]))
+
+
+def test_bruteforce_fixtures():
+    z = np.load(os.path.join(GOLD, "bruteforce.npz"))
+    for k in range(len(z["a"])):
+        a, b = str(z["a"][k]), str(z["b"][k])
+        mat, gaps = z["mat"][k][None], z["gaps"][k][None]
+        gm = 1 if bool(z["affine"][k]) else 0
+        enc = _enc1(DNA, a, b)
+        h = oracle.hard(64, gm, 0, mat, gaps, enc)
+        assert h["scores"][0] == pytest.approx(z["global_score"][k], abs=1e-9)
+        hl = oracle.hard(64, gm, 1, mat, gaps, enc)
+        assert hl["scores"][0] == pytest.approx(z["local_score"][k], abs=1e-9)
+        s, g = oracle.soft(gm, 0, mat, gaps, enc)
+        assert s[0] == pytest.approx(z["log_z"][k], rel=1e-12, abs=1e-12)
+        np.testing.assert_allclose(g[0], z["soft"][k], rtol=1e-9, atol=1e-12)
+        if not np.isnan(z["hard"][k][0]):
+            np.testing.assert_array_equal(h["grads"][0], z["hard"][k])
+
+
+def _ref_cases():
+    z = np.load(os.path.join(GOLD, "reference_batches.npz"))
+    names = sorted({k.split("_")[0] for k in z.files})
+    return z, names
+
+
+@pytest.mark.parametrize("name", ["prot", "protf", "rna3"])
+def test_reference_batch_fixtures(name):
+    z, _ = _ref_cases()
+    pre = name + "_"
+    alpha = str(z[pre + "alpha"])
+    sa, sb = [str(s) for s in z[pre + "sa"]], [str(s) for s in z[pre + "sb"]]
+    tr = z[pre + "tracks"] if pre + "tracks" in z.files else None
+    gt = z[pre + "gap_tracks"] if pre + "gap_tracks" in z.files else None
+    enc = oracle.Encoded(encode(alpha, sa), encode(alpha, sb), tr, gt)
+    tracked = tr is not None
+    mat, gaps, mat2, gaps2 = z[pre + "mat"], z[pre + "gaps"], z[pre + "mat2"], z[pre + "gaps2"]
+    for gm in (0, 1):
+        for am in (0, 1):
+            for prec in (32, 64):
+                key = f"{pre}hard{prec}_g{gm}_m{am}_"
+                o = oracle.hard(prec, gm, am, mat, gaps, enc, tracked=tracked)
+                np.testing.assert_array_equal(o["scores"], z[key + "scores"])
+                np.testing.assert_array_equal(o["grads"], z[key + "grads"])
+                np.testing.assert_array_equal(o["guides"], z[key + "guides"])
+                key = f"{pre}band{prec}_g{gm}_m{am}_"
+                ob = oracle.hard(prec, gm, am, mat2, gaps2, enc, tracked=tracked, guides_in=o["guides"], band=4)
+                np.testing.assert_array_equal(ob["scores"], z[key + "scores"])
+                np.testing.assert_array_equal(ob["grads"], z[key + "grads"])
+                np.testing.assert_array_equal(ob["guides"], z[key + "guides"])
+            for T in (1.0, 0.5):
+                key = f"{pre}soft_T{T}_g{gm}_m{am}_"
+                s, g = oracle.soft(gm, am, mat, gaps, enc, T)
+                np.testing.assert_allclose(s, z[key + "scores"], rtol=1e-11, atol=1e-11)
+                np.testing.assert_allclose(g, z[key + "grads"], rtol=1e-9, atol=1e-10)
+
+
+def test_blocked_sum_order():
+    """Blocks of 4096 in pair order, then the blocks in order (batch_engine.hpp:1788-1827)."""
+    rng = np.random.default_rng(3)
+    g = rng.normal(size=(9000, 7))
+    w = rng.normal(size=9000)
+    out = oracle.blocked_sum(g, w)
+    ref = np.zeros(7)
+    for b0 in range(0, 9000, 4096):
+        acc = np.zeros(7)
+        for p in range(b0, min(9000, b0 + 4096)):
+            acc = acc + w[p] * g[p]
+        ref = ref + acc
+    np.testing.assert_array_equal(out, ref)
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference driver not built here")
+@pytest.mark.parametrize("gm", [0, 1])
+@pytest.mark.parametrize("am", [0, 1])
+def test_live_reference_random(gm, am):
+    rng = np.random.default_rng(50 + gm + 2 * am)
+    for prec in (32, 64):
+        mat = rand_matrix(rng, 20, 1, integer=False)
+        gaps = rng.uniform(0.2, 3.0, size=(1, 4))
+        sa = rand_seqs(rng, 30, 0, 50, AA)
+        sb = rand_seqs(rng, 30, 0, 50, AA)
+        enc = oracle.Encoded(encode(AA, sa), encode(AA, sb))
+        o = oracle.hard(prec, gm, am, mat, gaps, enc)
+        r = oracle.ref_run(prec, gm, am, 1, AA, mat, gaps, sa, sb)
+        np.testing.assert_array_equal(o["scores"], r["scores"])
+        np.testing.assert_array_equal(o["grads"], r["grads"])
+        np.testing.assert_array_equal(o["guides"], r["guides"])
