@@ -102,6 +102,24 @@ int nwg_status(nwg_store* s, int32_t* out);
 /* Device time (ms) of the last nwg_run's kernels and how many kernels it launched. */
 int nwg_last_timing(nwg_store* s, double* ms, int64_t* launches);
 
+/* Viterbi scores of n_pairs pairs WITHOUT any device allocation (no counterpart in the
+ * reference: it is a CPU library).  For callers whose host framework owns all device memory
+ * (its own caching allocator or a fixed per-plugin budget) and forbids cudaMalloc, which also
+ * synchronises the device.  All pointers but mat / gaps are device pointers the caller
+ * allocated: codes and int64 offsets as nwg_store_create takes them, scores (n_pairs doubles)
+ * the output.  mat (nalpha x nalpha, nalpha <= 32) and gaps (4) are host doubles.  The
+ * float32 score-only fill of nwg_run (bit-identical scores), one parameter set, untracked.
+ * Scratch comes from a 24 MiB array every GPU that loads the library reserves until exit;
+ * limit: B at most 2047 residues (max_len_b states the batch's longest B; larger: NWG_EINVAL).
+ * The first call on a device looks the array up (cudaGetSymbolAddress) -- make it before any
+ * stream capture.  Calls share that array: calls whose kernels overlap on the GPU race.
+ * Errors: nwg_noalloc_last_error(). */
+int nwg_scores_noalloc(const uint8_t* codes_a, const int64_t* off_a, const uint8_t* codes_b,
+                       const int64_t* off_b, int64_t n_pairs, int max_len_b, int nalpha,
+                       const double* mat, const double* gaps, int gap_model, int mode,
+                       double* scores, void* stream);
+const char* nwg_noalloc_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

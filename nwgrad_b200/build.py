@@ -26,9 +26,10 @@ UNITS = [
     ("hard_f64", "nwg_hard_inst.cu", ["-DNWG_T=double", "-DNWG_HARD_FN=hard_fn_f64"]),
     ("soft_f32", "nwg_soft_inst.cu", ["-DNWG_T=float", "-DNWG_SOFT_FN=soft_fn_f32"]),
     ("soft_f64", "nwg_soft_inst.cu", ["-DNWG_T=double", "-DNWG_SOFT_FN=soft_fn_f64"]),
+    ("noalloc", "nwg_noalloc.cu", []),
 ]
 DEPS = ["nwg_capi.cu", "nwg_common.cuh", "nwg_hard.cuh", "nwg_walk.cuh", "nwg_soft.cuh", "nwg_kernels.h",
-        "nwg_hard_inst.cu", "nwg_soft_inst.cu"]
+        "nwg_hard_inst.cu", "nwg_soft_inst.cu", "nwg_noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
