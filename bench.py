@@ -97,6 +97,20 @@ def c2_workload(n_pairs, seed=1):
     return mat, a, oa, bp, obp, bn, obn
 
 
+def c1_workload(n_pairs=10000, seed=0):
+    """Plain global affine hard batch: A and B independent, lengths U[50, 300]."""
+    rng = np.random.default_rng(seed)
+    freqs = rng.dirichlet(np.full(20, 5.0))
+    mat = c2_matrix(rng)
+    la = rng.integers(50, 301, size=n_pairs)
+    lb = rng.integers(50, 301, size=n_pairs)
+    oa = np.zeros(n_pairs + 1, np.int64); oa[1:] = np.cumsum(la)
+    ob = np.zeros(n_pairs + 1, np.int64); ob[1:] = np.cumsum(lb)
+    a = rng.choice(20, size=int(oa[-1]), p=freqs).astype(np.uint8)
+    b = rng.choice(20, size=int(ob[-1]), p=freqs).astype(np.uint8)
+    return mat, a, oa, b, ob
+
+
 def cells_of(oa, ob):
     return float(np.sum(np.diff(oa).astype(np.float64) * np.diff(ob).astype(np.float64)))
 
@@ -199,7 +213,11 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=4000, help="pairs per batch in the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", default="c2-soft", choices=["c2-soft", "c1-hard"],
+                    help="c2-soft (default): the soft-gradient batch; c1-hard: the plain hard batch (side measurement)")
     args = ap.parse_args()
+    if args.workload == "c1-hard":
+        return bench_c1(args)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -355,6 +373,32 @@ def main():
             "step_ms": step_ms}))
     if dist is not None:
         dist.destroy_process_group()
+
+
+def bench_c1(args):
+    """Side measurement: the plain global affine hard batch (10k pairs L 50-300), GCUPS of
+    score_and_grad() + compute_grad() with the codes resident."""
+    import torch
+    import nwgrad_b200 as nw
+    mat, a, oa, b, ob = c1_workload()
+    cells = cells_of(oa, ob)
+    params = nw.AlignParams.from_arrays(mat[None], [[11.0, 1.0, 11.0, 1.0]], alphabet=nw.AA20)
+    bt = nw.SeqPairBatch.from_codes(a, oa, b, ob, params, grad_mode="hard")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    for _ in range(max(args.warmup, 3)):
+        bt.score_and_grad(); bt.compute_grad()
+    ms = []
+    kms = 0.0
+    for _ in range(args.steps):
+        flush.zero_(); torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(); bt.score_and_grad(); bt.compute_grad(); e1.record(); torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1)); kms += bt.last_timing()[0]
+    tot = float(np.sum(ms))
+    print(json.dumps({"metric": "hard-grad batch GCUPS", "value": cells * args.steps / (tot / 1e3) / 1e9,
+                      "unit": "GCUPS", "n_gpus": 1, "steps": args.steps, "ms_per_step": tot / args.steps,
+                      "kernel_ms_per_step": kms / args.steps, "config": {"workload": "c1 hard global affine float32, "
+                      "10k pairs L 50-300", "cells_per_step": cells}, "step_ms": ms}))
 
 
 if __name__ == "__main__":

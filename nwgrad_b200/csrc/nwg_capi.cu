@@ -65,8 +65,21 @@ __global__ void blocked_partial_kernel(const double* __restrict__ g, const doubl
     if (k >= gs) return;
     const int64_t p0 = b * block, p1 = min(n_pairs, p0 + block);
     double acc = 0.0;
-    if (w) for (int64_t p = p0; p < p1; ++p) acc = __dadd_rn(acc, __dmul_rn(w[p], g[p * gs + k]));
-    else   for (int64_t p = p0; p < p1; ++p) acc = __dadd_rn(acc, g[p * gs + k]);
+    constexpr int U = 16;   // loads in flight; the adds stay in pair order
+    int64_t p = p0;
+    for (; p + U <= p1; p += U) {
+        double v[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) v[u] = g[(p + u) * gs + k];
+        if (w) {
+#pragma unroll
+            for (int u = 0; u < U; ++u) acc = __dadd_rn(acc, __dmul_rn(w[p + u], v[u]));
+        } else {
+#pragma unroll
+            for (int u = 0; u < U; ++u) acc = __dadd_rn(acc, v[u]);
+        }
+    }
+    for (; p < p1; ++p) acc = w ? __dadd_rn(acc, __dmul_rn(w[p], g[p * gs + k])) : __dadd_rn(acc, g[p * gs + k]);
     part[b * gs + k] = acc;
 }
 __global__ void blocked_total_kernel(const double* __restrict__ part, int64_t nblocks, int64_t gs,
@@ -158,9 +171,9 @@ Geo pick_geo(bool soft, int rows, int n, int lanes, int rpl, bool lane_ok) {
     Geo best{32, soft ? 4 : 4};
     double bc = 1e300;
     const int opts_h[] = {8, 4, 2, 1};
-    const int opts_s[] = {8, 4, 2};
+    const int opts_s[] = {4, 2};
     const int* opts = soft ? opts_s : opts_h;
-    const int no = soft ? 3 : 4;
+    const int no = soft ? 2 : 4;
     for (int k = 0; k < no; ++k) {
         const Geo g{32, opts[k]};
         // fewer rows per lane costs more shuffles per cell: weigh them in
@@ -180,10 +193,16 @@ struct Bucket {
 
 struct Plan {
     bool valid = false;
-    int key_soft = -1, key_lanes = -1, key_rows = -1;
+    int key_soft = -1, key_lanes = -1, key_rows = -1, key_band = -1;
     std::vector<Bucket> buckets;
     std::vector<int64_t> code_off;   // hard: per pair
     int64_t code_bytes = 0;
+    int64_t n_stripes = 0;           // banded: stripes over all pairs
+    DBuf order, dcode_off, stripe_base;
+    void reset() {
+        order.release(); dcode_off.release(); stripe_base.release();
+        valid = false; buckets.clear(); code_off.clear(); code_bytes = 0; n_stripes = 0;
+    }
 };
 
 }  // namespace
@@ -205,11 +224,12 @@ struct nwg_store {
     DBuf tmatf, tgapf, tmatd, tgapd, tbx0f, tbx0d, tscore, tend;   // a guide snapshot's copies
     bool bx0f_ok = false, bx0d_ok = false;
     // results
-    DBuf score, end, grad, guide, status, order, codes, code_off, scratch, part, red, moves, moves_off, path_info;
+    DBuf score, end, grad, guide, status, codes, scratch, part, red, moves, moves_off, path_info;
     int64_t gstride = 0;
     bool have_scores = false, have_grads = false, have_guides = false, have_paths = false;
     int last_grad_mode = 0, last_gm = -1, last_am = -1, last_prec = 0;
-    Plan hard_plan, soft_plan;
+    Plan hard_plan, soft_plan, band_plan;
+    DBuf stripe_tab;
     std::vector<int32_t> h_status;
     // timing
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -257,10 +277,10 @@ const T* ensure_bx0(nwg_store* s, bool aff, cudaStream_t st, bool& ok, DBuf& buf
     return buf.as<T>();
 }
 
-void build_plan(nwg_store* s, Plan& P, bool soft, int lanes, int rpl, int elem_bytes) {
-    if (P.valid && P.key_soft == int(soft) && P.key_lanes == lanes && P.key_rows == rpl) return;
-    P = Plan{};
-    P.key_soft = soft; P.key_lanes = lanes; P.key_rows = rpl;
+void build_plan(nwg_store* s, Plan& P, bool soft, int lanes, int rpl, int elem_bytes, bool band = false) {
+    if (P.valid && P.key_soft == int(soft) && P.key_lanes == lanes && P.key_rows == rpl && P.key_band == int(band)) return;
+    P.reset();
+    P.key_soft = soft; P.key_lanes = lanes; P.key_rows = rpl; P.key_band = band;
     const int64_t n = s->n;
     // one lane per pair keeps a K*N*N histogram per lane in shared memory (soft)
     const bool lane_ok_soft = int64_t(s->K) * s->N * s->N * elem_bytes * 32 <= 48 * 1024;
@@ -269,7 +289,7 @@ void build_plan(nwg_store* s, Plan& P, bool soft, int lanes, int rpl, int elem_b
     for (int64_t p = 0; p < n; ++p) {
         const int m = int(s->oa[p + 1] - s->oa[p]), nb = int(s->ob[p + 1] - s->ob[p]);
         const int rows = soft ? m + 1 : m;
-        const Geo g = pick_geo(soft, std::max(rows, 1), nb, lanes, rpl, soft ? lane_ok_soft : true);
+        Geo g = band ? Geo{32, 2, true} : pick_geo(soft, std::max(rows, 1), nb, lanes, rpl, soft ? lane_ok_soft : true);
         auto key = std::make_pair(g.G, g.R);
         auto itb = idx.find(key);
         int bi;
@@ -308,16 +328,27 @@ void build_plan(nwg_store* s, Plan& P, bool soft, int lanes, int rpl, int elem_b
                 const int GR = B.geo.G * B.geo.R;
                 const int64_t st = (m + GR - 1) / GR;
                 P.code_off[p] = off;
-                const int64_t bytes = (m && nb) ? st * (nb + B.geo.G - 1) * GR : 0;
+                const int64_t bytes = (m && nb) ? st * (((nb + B.geo.G - 1) + 7) & ~int64_t(7)) * GR : 0;
                 off += (bytes + 15) & ~int64_t(15);
             }
         P.code_bytes = std::max<int64_t>(off, 16);
     }
-    s->order.need(size_t(std::max<int64_t>(n, 1)) * 4);
-    if (n) NWG_CUDA(cudaMemcpy(s->order.p, order.data(), size_t(n) * 4, cudaMemcpyHostToDevice));
+    P.order.need(size_t(std::max<int64_t>(n, 1)) * 4);
+    if (n) NWG_CUDA(cudaMemcpy(P.order.p, order.data(), size_t(n) * 4, cudaMemcpyHostToDevice));
     if (!soft) {
-        s->code_off.need(size_t(n + 1) * 8);
-        NWG_CUDA(cudaMemcpy(s->code_off.p, P.code_off.data(), size_t(n + 1) * 8, cudaMemcpyHostToDevice));
+        P.dcode_off.need(size_t(n + 1) * 8);
+        NWG_CUDA(cudaMemcpy(P.dcode_off.p, P.code_off.data(), size_t(n + 1) * 8, cudaMemcpyHostToDevice));
+    }
+    if (band) {
+        // per pair the index of its first stripe in the stripe table
+        std::vector<int64_t> sb(size_t(n) + 1, 0);
+        for (int64_t p = 0; p < n; ++p) {
+            const int m = int(s->oa[p + 1] - s->oa[p]);
+            sb[p + 1] = sb[p] + (m + 63) / 64;
+        }
+        P.n_stripes = sb[n];
+        P.stripe_base.need(size_t(n + 1) * 8);
+        NWG_CUDA(cudaMemcpy(P.stripe_base.p, sb.data(), size_t(n + 1) * 8, cudaMemcpyHostToDevice));
     }
     P.valid = true;
 }
@@ -325,9 +356,11 @@ void build_plan(nwg_store* s, Plan& P, bool soft, int lanes, int rpl, int elem_b
 template <class T>
 void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, bool want_guide) {
     const bool aff = J.gap_model == 1, loc = J.mode == 1, tr = s->tracked();
-    Plan& P = s->hard_plan;
-    build_plan(s, P, false, J.lanes, J.rows, sizeof(T));
+    const bool band = J.band >= 0;
+    Plan& P = band ? s->band_plan : s->hard_plan;
+    build_plan(s, P, false, band ? 32 : J.lanes, band ? 2 : J.rows, sizeof(T), band);
     s->codes.need(size_t(P.code_bytes));
+    if (band) s->stripe_tab.need(size_t(std::max<int64_t>(P.n_stripes, 1)) * 16);
     const DBuf& matT = sizeof(T) == 4 ? s->matf : s->matd;
     const DBuf& gapT = sizeof(T) == 4 ? s->gapf : s->gapd;
     const T* bx0 = nullptr;
@@ -360,10 +393,14 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
         A.tracks = tr ? s->tracks.as<uint16_t>() : nullptr;
         A.gtracks = tr ? s->gtracks.as<uint16_t>() : nullptr;
         A.bx0 = bx0;
-        A.order = s->order.as<int32_t>() + B.off;
+        A.order = P.order.as<int32_t>() + B.off;
         A.n_items = int64_t(B.pairs.size());
         A.mat = matT.p; A.gaps = gapT.p; A.N = s->N; A.K = s->K;
-        A.codes = s->codes.as<uint8_t>(); A.code_off = s->code_off.as<int64_t>();
+        A.codes = s->codes.as<uint8_t>(); A.code_off = P.dcode_off.as<int64_t>();
+        if (band) {
+            A.guide = s->guide.as<int32_t>(); A.band = J.band;
+            A.stripe_base = P.stripe_base.as<int64_t>(); A.stripe_tab = s->stripe_tab.as<int64_t>();
+        }
         A.scratch = s->scratch.p; A.scratch_stride = max_stride;
         A.score = s->score.as<double>(); A.end = s->end.as<int32_t>();
         const int gpb = 128 / B.geo.G;
@@ -373,7 +410,10 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
         s->last_launches++;
     }
     // traceback: gradient, guide, path
-    if (want_grad) { s->grad.need(size_t(s->n) * s->gstride * 8 + 8); }
+    if (want_grad) {
+        s->grad.need(size_t(s->n) * s->gstride * 8 + 8);
+        NWG_CUDA(cudaMemsetAsync(s->grad.p, 0, size_t(s->n) * s->gstride * 8, st));
+    }
     if (want_guide) s->guide.need(size_t(s->total_a + s->n) * 4 + 4);
     const bool keep = J.keep_paths != 0;
     if (keep) {
@@ -390,9 +430,11 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
     W.b = s->b.as<uint8_t>(); W.ob = s->dob.as<int64_t>();
     W.tracks = tr ? s->tracks.as<uint16_t>() : nullptr;
     W.gtracks = tr ? s->gtracks.as<uint16_t>() : nullptr;
-    W.order = s->order.as<int32_t>(); W.n_items = s->n;
+    W.order = P.order.as<int32_t>(); W.n_items = s->n;
+    W.stripe_base = band ? P.stripe_base.as<int64_t>() : nullptr;
+    W.stripe_tab = band ? s->stripe_tab.as<int64_t>() : nullptr;
     W.N = s->N; W.K = s->K; W.affine = aff; W.local = loc;
-    W.codes = s->codes.as<uint8_t>(); W.code_off = s->code_off.as<int64_t>();
+    W.codes = s->codes.as<uint8_t>(); W.code_off = P.dcode_off.as<int64_t>();
     W.end = s->end.as<int32_t>();
     W.grad = want_grad ? s->grad.as<double>() : nullptr; W.gstride = s->gstride;
     W.guide = want_guide ? s->guide.as<int32_t>() : nullptr;
@@ -492,7 +534,7 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
     }
     DBuf sub_order;
     struct Free1 { DBuf& a; ~Free1() { a.release(); } } fr1{sub_order};
-    const int32_t* d_order = s->order.as<int32_t>();
+    const int32_t* d_order = P->order.as<int32_t>();
     if (subset) {
         sub_order.need(order.size() * 4 + 4);
         NWG_CUDA(cudaMemcpyAsync(sub_order.p, order.data(), order.size() * 4, cudaMemcpyHostToDevice, st));
@@ -673,9 +715,10 @@ int nwg_store_destroy(nwg_store* s) {
     return guarded([&] {
         if (!s) return;
         cudaSetDevice(s->device);
+        s->hard_plan.reset(); s->soft_plan.reset(); s->band_plan.reset();
         for (DBuf* b : {&s->a, &s->b, &s->doa, &s->dob, &s->tracks, &s->gtracks, &s->matf, &s->gapf, &s->matd,
                         &s->gapd, &s->bx0f, &s->bx0d, &s->score, &s->end, &s->grad, &s->guide, &s->status,
-                        &s->order, &s->codes, &s->code_off, &s->scratch, &s->part, &s->red, &s->moves,
+                        &s->stripe_tab, &s->codes, &s->scratch, &s->part, &s->red, &s->moves,
                         &s->moves_off, &s->path_info, &s->tmatf, &s->tgapf, &s->tmatd, &s->tgapd,
                         &s->tbx0f, &s->tbx0d, &s->tscore, &s->tend})
             b->release();
@@ -711,7 +754,8 @@ int nwg_run(nwg_store* s, const nwg_job* job, void* stream, double* total) {
         if (J.gap_model < 0 || J.gap_model > 1 || J.mode < 0 || J.mode > 1 || J.grad_mode < 0 || J.grad_mode > 2)
             throw Error(NWG_EINVAL, "bad job");
         if (J.precision != 32 && J.precision != 64) throw Error(NWG_EINVAL, "precision must be 32 or 64");
-        if (J.band >= 0) throw Error(NWG_EINVAL, "banded re-alignment is not available in this build");
+        if (J.band >= 0 && J.grad_mode == 2) throw Error(NWG_EINVAL, "soft banded re-alignment is not available in this build");
+        if (J.band >= 0 && !s->have_guides) throw Error(NWG_ESTATE, "banded_grad() needs a guide; call score_and_grad() first");
         NWG_CUDA(cudaSetDevice(s->device));
         cudaStream_t st = static_cast<cudaStream_t>(stream);
         s->last_launches = 0;
@@ -806,8 +850,8 @@ int nwg_reduce(nwg_store* s, const double* w, double* out) {
             dw = s->red.as<double>() + gs;
             NWG_CUDA(cudaMemcpy(dw, w, size_t(n) * 8, cudaMemcpyHostToDevice));
         }
-        dim3 grid(unsigned((gs + 127) / 128), unsigned(nb));
-        blocked_partial_kernel<<<grid, 128>>>(s->grad.as<double>(), dw, n, gs, B, s->part.as<double>());
+        dim3 grid(unsigned((gs + 31) / 32), unsigned(nb));
+        blocked_partial_kernel<<<grid, 32>>>(s->grad.as<double>(), dw, n, gs, B, s->part.as<double>());
         NWG_CUDA(cudaGetLastError());
         blocked_total_kernel<<<unsigned((gs + 127) / 128), 128>>>(s->part.as<double>(), nb, gs, s->red.as<double>());
         NWG_CUDA(cudaGetLastError());

@@ -11,11 +11,16 @@ namespace nwg {
 template <class T> __device__ __forceinline__ T rmax(T a, T b) { return (a < b) ? b : a; }
 template <class T> __device__ __forceinline__ T rmax3(T a, T b, T c) { return rmax(rmax(a, b), c); }
 
+// The hardware max (FMNMX): equal to rmax except for the sign of an exact zero and NaNs.
+__device__ __forceinline__ float hmax(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double hmax(double a, double b) { return fmax(a, b); }
+template <class T> __device__ __forceinline__ T hmax3(T a, T b, T c) { return hmax(hmax(a, b), c); }
+
 // The predecessor code of one state: 0 first argument (M), 1 second (X), 2 third (Y),
 // by >= in M, X, Y order (aligner.hpp:3977-3980).
 template <class T> __device__ __forceinline__ uint32_t pick3(T vm, T vx, T vy) {
     const uint32_t kxy = vx >= vy ? 1u : 2u;
-    return vm >= rmax(vx, vy) ? 0u : kxy;
+    return vm >= hmax(vx, vy) ? 0u : kxy;
 }
 
 // Round-to-nearest multiply and add that the compiler never fuses into an FMA (the

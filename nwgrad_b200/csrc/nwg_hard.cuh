@@ -8,16 +8,21 @@
 // is the one-pair-per-lane ("inter-pair") kernel for short pairs; G = 32 one warp per pair.
 //
 // Every cell is the reference recurrence, expression for expression
-// (aligner.hpp:3955-4071 affine, 3756-3860 linear): (v - go) - ge left-associated, the
-// first-largest max, >= tie-breaks in M > X > Y order, parameters cast to T once.  The
-// evaluation order across cells differs, but each cell is a fixed expression of its three
-// neighbours, so the tables are bit-identical.
+// (aligner.hpp:3955-4071 affine, 3756-3860 linear): (v - go) - ge left-associated, >=
+// tie-breaks in M > X > Y order, parameters cast to T once.  The evaluation order across cells
+// differs, but each cell is a fixed expression of its three neighbours, so the tables are
+// bit-identical.  Maxima use the hardware max (fmax): it returns the same value as the
+// reference's std::max except for the sign of an exact zero (the parameters are finite, so no
+// NaN arises), and the codes, end cells and gradients depend only on comparisons, which do
+// not see that sign.
 //
 // Codes: one byte per cell, affine M | X << 2 | Y << 4, linear 0 diag / 1 up / 2 left with
-// 3 = stop (Local, value <= 0).  Layout per pair, per stripe s:
-//   byte ((s * S + t) * G + g) * R + r,  S = n + G - 1 steps,
-// the R cells a lane fills in one step contiguous, so every step is one coalesced store
-// per group.  Border cells (row 0, column 0) are not stored: the walk knows them.
+// 3 = stop (Local, value <= 0).  Layout per pair, per stripe s (S8 = n + G - 1 steps rounded
+// up to a multiple of 8):
+//   byte s * S8 * G * R + ((t / 8 * G + g) * 8 + t % 8) * R + r,
+// i.e. tiles of 8 steps x R rows per lane: the fill's per-step store is R bytes per lane, and
+// the traceback, which mostly steps diagonally (t - 1, r - 1), reads one tile for several
+// steps.  Border cells (row 0, column 0) are not stored: the walk knows them.
 #pragma once
 #include "nwg_common.cuh"
 
@@ -38,6 +43,23 @@ struct HardArgs {
     void* scratch; int64_t scratch_stride;     // per group slot: the stripe boundary row, 3*(n+1) T
     double* score;                             // per pair
     int32_t* end;                              // per pair: end_i, end_j, state, layout (G<<8|R)
+    // guide-banded re-alignment (BAND kernels only)
+    const int32_t* guide;                      // per pair m+1 at oa[p] + p
+    int band;                                  // half-width
+    const int64_t* stripe_base;                // per pair: first entry in stripe_tab
+    int64_t* stripe_tab;                       // per stripe: code offset in the pair, first column
+};
+
+// The band of DP row i around guide g (aligner.hpp:2644-2700): columns [jlo, jhi].
+struct BandRows {
+    const int32_t* g; int band, m, n; bool global;
+    __device__ __forceinline__ int jlo(int i) const { return max(1, g[i] - band); }
+    __device__ __forceinline__ int jhi(int i) const {
+        if (global && i == m) return n;
+        int hi = g[i] + band;
+        if (i < m) hi = max(hi, g[i + 1] - 1 + band);
+        return min(n, hi);
+    }
 };
 
 template <class T> struct HardRowParams { T goa, gea, gob, geb; };
@@ -52,7 +74,7 @@ __device__ __forceinline__ T border_col0(const HardArgs& A, const T* bx0p, int i
     }
 }
 
-template <class T, bool AFF, bool LOC, bool TR, int G, int R>
+template <class T, bool AFF, bool LOC, bool TR, int G, int R, bool BAND = false>
 __global__ void __launch_bounds__(128) hard_fill_kernel(const HardArgs A) {
     constexpr int GR = G * R;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -112,13 +134,49 @@ __global__ void __launch_bounds__(128) hard_fill_kernel(const HardArgs A) {
         }
         uint8_t* __restrict__ codes = A.codes + A.code_off[p];
         const int nstripes = (m + GR - 1) / GR;
-        const int S = n + G - 1;
+        // the band (full DP: every column of every row; borders reach every row / column)
+        BandRows bw{BAND ? A.guide + ao + p : nullptr, A.band, m, n, !LOC};
+        int brows = m, bcols = n;            // rows / columns whose border cells are charged
+        if constexpr (BAND) {
+            brows = 0;
+            while (brows < m && bw.g[brows + 1] <= A.band) ++brows;
+            bcols = bw.jhi(0);
+        }
+        int64_t soff = 0;                     // this stripe's code offset within the pair
+        int pmin = 1, pmax = 0;               // the previous stripe's columns
 
         T bestv = T(0); int besti = 0, bestj = 0, bests = 0;   // Local: the first row-major max
         T endM = ninf<T>(), endX = ninf<T>(), endY = ninf<T>();
 
         for (int s = 0; s < nstripes; ++s) {
             const int i0 = s * GR + lane * R + 1;   // this lane's first DP row
+            // the stripe's columns [cmin, cmax]: the union of its rows' bands
+            int cmin = 1, cmax = n;
+            int rlo[BAND ? R : 1], rhi[BAND ? R : 1];
+            if constexpr (BAND) {
+                int lo = n + 1, hi = 0;
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const int i = i0 + r;
+                    rlo[r] = i <= m ? bw.jlo(i) : n + 1;
+                    rhi[r] = i <= m ? bw.jhi(i) : 0;
+                    if (rlo[r] <= rhi[r]) { lo = min(lo, rlo[r]); hi = max(hi, rhi[r]); }
+                }
+                if constexpr (G > 1) {
+#pragma unroll
+                    for (int off = G / 2; off > 0; off >>= 1) {
+                        lo = min(lo, __shfl_xor_sync(gmask, lo, off, G));
+                        hi = max(hi, __shfl_xor_sync(gmask, hi, off, G));
+                    }
+                }
+                cmin = lo; cmax = hi;
+                if (lane == 0) {
+                    A.stripe_tab[2 * (A.stripe_base[p] + s)] = soff;
+                    A.stripe_tab[2 * (A.stripe_base[p] + s) + 1] = cmin;
+                }
+            }
+            const int S = cmax >= cmin ? (cmax - cmin + 1) + G - 1 : 0;
+            const int S8 = (S + 7) & ~7;
             int rowbase[R];
             T cM[R], cX[R], cY[R];
             HardRowParams<T> rp[TR ? R : 1];
@@ -134,40 +192,57 @@ __global__ void __launch_bounds__(128) hard_fill_kernel(const HardArgs A) {
                     rp[r].goa = sgap[4 * gs + 0]; rp[r].gea = sgap[4 * gs + 1];
                     rp[r].gob = sgap[4 * ts + 2]; rp[r].geb = sgap[4 * ts + 3];
                 }
-                if constexpr (LOC) { cM[r] = T(0); cX[r] = ninf<T>(); rbest[r] = T(0); rbj[r] = 0; rbs[r] = 0; }
-                else {
+                // the cell left of the stripe's first column: column 0's border, or out of band
+                if constexpr (LOC) {
+                    cM[r] = cmin == 1 ? T(0) : ninf<T>(); cX[r] = ninf<T>();
+                    rbest[r] = T(0); rbj[r] = 0; rbs[r] = 0;
+                } else {
                     cM[r] = ninf<T>();
-                    cX[r] = valid ? border_col0<T, AFF, TR>(A, bx0p, i, ugob, ugeb) : ninf<T>();
+                    cX[r] = (valid && cmin == 1 && i <= brows) ? border_col0<T, AFF, TR>(A, bx0p, i, ugob, ugeb) : ninf<T>();
                     if constexpr (!AFF) cM[r] = cX[r];   // linear: H lives in cM
                 }
                 cY[r] = ninf<T>();
             }
-            // the row above this lane's first row, at column 0
+            // row 0 at column j (Global: the charged gap chain up to bcols; Local: free starts)
+            auto row0 = [&](int j, T& vM, T& vX, T& vY) {
+                vX = ninf<T>();
+                if constexpr (LOC) { vM = T(0); vY = ninf<T>(); }
+                else if (j == 0) { vM = T(0); vY = ninf<T>(); }
+                else if constexpr (AFF) {
+                    vM = ninf<T>();
+                    vY = j <= bcols ? -add_rn(goa0, mul_rn(static_cast<T>(j), gea0)) : ninf<T>();
+                } else {
+                    vM = j <= bcols ? mul_rn(-static_cast<T>(j), gea0) : ninf<T>(); vY = ninf<T>();
+                }
+            };
+            // the row above this lane's first row, at column cmin - 1
             T dgM, dgX, dgY;
             {
                 const int i = i0 - 1;
-                if (i == 0) { dgM = T(0); dgX = ninf<T>(); dgY = ninf<T>(); }
-                else if (LOC) { dgM = T(0); dgX = ninf<T>(); dgY = ninf<T>(); }
-                else {
-                    dgX = border_col0<T, AFF, TR>(A, bx0p, i, ugob, ugeb);
-                    dgM = AFF ? ninf<T>() : dgX; dgY = ninf<T>();
-                }
+                if (cmin == 1) {
+                    if (i == 0) { dgM = T(0); dgX = ninf<T>(); dgY = ninf<T>(); }
+                    else if (LOC) { dgM = T(0); dgX = ninf<T>(); dgY = ninf<T>(); }
+                    else {
+                        dgX = i <= brows ? border_col0<T, AFF, TR>(A, bx0p, i, ugob, ugeb) : ninf<T>();
+                        dgM = AFF ? ninf<T>() : dgX; dgY = ninf<T>();
+                    }
+                } else if (lane == 0 && s == 0) {
+                    row0(cmin - 1, dgM, dgX, dgY);
+                } else if (lane == 0 && cmin - 1 >= pmin && cmin - 1 <= pmax) {
+                    dgM = bnd[3 * (cmin - 1)]; dgX = bnd[3 * (cmin - 1) + 1]; dgY = bnd[3 * (cmin - 1) + 2];
+                } else { dgM = ninf<T>(); dgX = ninf<T>(); dgY = ninf<T>(); }
             }
             T upM = ninf<T>(), upX = ninf<T>(), upY = ninf<T>();
-            uint8_t* cs = codes + int64_t(s) * S * GR;
+            uint8_t* cs = codes + (BAND ? soff : int64_t(s) * S8 * GR);
 
             for (int t = 0; t < S; ++t) {
-                const int j = t - lane + 1;
-                if (lane == 0 && j <= n) {
-                    if (s == 0) {
-                        if constexpr (LOC) { upM = T(0); upX = ninf<T>(); upY = ninf<T>(); }
-                        else if constexpr (AFF) { upM = ninf<T>(); upX = ninf<T>(); upY = -add_rn(goa0, mul_rn(static_cast<T>(j), gea0)); }
-                        else { upM = mul_rn(-static_cast<T>(j), gea0); }
-                    } else {
-                        upM = bnd[3 * j]; upX = bnd[3 * j + 1]; upY = bnd[3 * j + 2];
-                    }
+                const int j = cmin + t - lane;
+                if (lane == 0 && j <= cmax) {
+                    if (s == 0) row0(j, upM, upX, upY);
+                    else if (!BAND || (j >= pmin && j <= pmax)) { upM = bnd[3 * j]; upX = bnd[3 * j + 1]; upY = bnd[3 * j + 2]; }
+                    else { upM = ninf<T>(); upX = ninf<T>(); upY = ninf<T>(); }
                 }
-                const bool active = (j >= 1) && (j <= n);
+                const bool active = (j >= cmin) && (j <= cmax);
                 if (active) {
                     const int bj = bp[j - 1];
                     T pM = dgM, pX = dgX, pY = dgY;   // row above, column j-1
@@ -182,38 +257,44 @@ __global__ void __launch_bounds__(128) hard_fill_kernel(const HardArgs A) {
                         if constexpr (TR) { go_a = rp[r].goa; ge_a = rp[r].gea; go_b = rp[r].gob; ge_b = rp[r].geb; }
                         else { go_a = ugoa; ge_a = ugea; go_b = ugob; ge_b = ugeb; }
                         uint32_t code;
+                        const bool inb = !BAND || (j >= rlo[BAND ? r : 0] && j <= rhi[BAND ? r : 0]);
                         if constexpr (AFF) {
-                            T mv = rmax3(pM, pX, pY) + sub;
+                            T mv = hmax3(pM, pX, pY) + sub;
                             uint32_t km = pick3(pM, pX, pY);
                             const T ux = (qM - go_b) - ge_b, vx = qX - ge_b, wx = (qY - go_b) - ge_b;
-                            const T xv = rmax3(ux, vx, wx);
+                            const T xv = hmax3(ux, vx, wx);
                             const uint32_t kx = pick3(ux, vx, wx);
                             const T uy = (cM[r] - go_a) - ge_a, vy = (cX[r] - go_a) - ge_a, wy = cY[r] - ge_a;
-                            const T yv = rmax3(uy, vy, wy);
+                            const T yv = hmax3(uy, vy, wy);
                             const uint32_t ky = pick3(uy, vy, wy);
+                            T xo = xv, yo = yv;
+                            if constexpr (LOC) mv = hmax(mv, T(0));
+                            if constexpr (BAND) {
+                                if (!inb) { mv = ninf<T>(); xo = ninf<T>(); yo = ninf<T>(); }
+                            }
                             if constexpr (LOC) {
-                                mv = rmax(mv, T(0));
                                 km |= 3u * uint32_t(mv <= T(0));
-                                const T v = rmax3(mv, xv, yv);
+                                const T v = hmax3(mv, xo, yo);
                                 if (v > rbest[r]) {
                                     rbest[r] = v; rbj[r] = j;
-                                    rbs[r] = (mv >= xv && mv >= yv) ? 0 : (xv >= yv ? 1 : 2);
+                                    rbs[r] = (mv >= xo && mv >= yo) ? 0 : (xo >= yo ? 1 : 2);
                                 }
                             }
                             pM = cM[r]; pX = cX[r]; pY = cY[r];
-                            cM[r] = mv; cX[r] = xv; cY[r] = yv;
-                            qM = mv; qX = xv; qY = yv;
+                            cM[r] = mv; cX[r] = xo; cY[r] = yo;
+                            qM = mv; qX = xo; qY = yo;
                             code = km | (kx << 2) | (ky << 4);
                         } else {
                             const T d0 = pM + sub;
                             const T u = qM - ge_b;
-                            const T tt = rmax(d0, u);
+                            const T tt = hmax(d0, u);
                             uint32_t c = uint32_t(d0 < u);
                             const T l = cM[r] - ge_a;
-                            T v = rmax(tt, l);
+                            T v = hmax(tt, l);
                             c = (tt < l) ? 2u : c;
+                            if constexpr (LOC) v = hmax(v, T(0));
+                            if constexpr (BAND) { if (!inb) v = ninf<T>(); }
                             if constexpr (LOC) {
-                                v = rmax(v, T(0));
                                 c |= 3u * uint32_t(v <= T(0));
                                 if (v > rbest[r]) { rbest[r] = v; rbj[r] = j; }
                             }
@@ -225,7 +306,7 @@ __global__ void __launch_bounds__(128) hard_fill_kernel(const HardArgs A) {
                         w[r >> 2] |= code << (8 * (r & 3));
                     }
                     // one coalesced store of this lane's R codes
-                    uint8_t* dst = cs + (int64_t(t) * G + lane) * R;
+                    uint8_t* dst = cs + ((int64_t(t >> 3) * G + lane) * 8 + (t & 7)) * R;
                     if constexpr (R % 16 == 0) {
 #pragma unroll
                         for (int k = 0; k < R / 16; ++k)
@@ -257,7 +338,10 @@ __global__ void __launch_bounds__(128) hard_fill_kernel(const HardArgs A) {
                     if constexpr (AFF) { bnd[3 * j + 1] = cX[R - 1]; bnd[3 * j + 2] = cY[R - 1]; }
                 }
             }
-            // the end cell (m, n): after the stripe each register holds column n
+            pmin = cmin; pmax = cmax;
+            soff += int64_t(S8) * GR;
+            // the end cell (m, n): after the stripe each register holds column n (a banded
+            // Global stripe holding row m always reaches column n)
             if constexpr (!LOC) {
                 if (m >= i0 && m < i0 + R) {
 #pragma unroll

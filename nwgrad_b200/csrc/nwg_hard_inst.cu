@@ -4,7 +4,14 @@
 namespace nwg {
 namespace {
 template <class T, bool AFF, bool LOC, bool TR>
+HardFn pick_band(Geo g) {
+    if (g.G == 32 && g.R == 1) return &hard_fill_kernel<T, AFF, LOC, TR, 32, 1, true>;
+    if (g.G == 32 && g.R == 2) return &hard_fill_kernel<T, AFF, LOC, TR, 32, 2, true>;
+    return nullptr;
+}
+template <class T, bool AFF, bool LOC, bool TR>
 HardFn pick(Geo g) {
+    if (g.band) return pick_band<T, AFF, LOC, TR>(g);
 #define NWG_H(GG, RR) if (g.G == GG && g.R == RR) return &hard_fill_kernel<T, AFF, LOC, TR, GG, RR>;
     NWG_H(1, 8) NWG_H(1, 16) NWG_H(1, 24) NWG_H(1, 32) NWG_H(32, 1) NWG_H(32, 2) NWG_H(32, 4) NWG_H(32, 8)
 #undef NWG_H

@@ -9,7 +9,7 @@
 namespace nwg {
 using HardFn = void (*)(const HardArgs);
 using SoftFn = void (*)(const SoftArgs);
-struct Geo { int G, R; };
+struct Geo { int G, R; bool band = false; };
 HardFn hard_fn_f32(bool aff, bool loc, bool tr, Geo g);
 HardFn hard_fn_f64(bool aff, bool loc, bool tr, Geo g);
 SoftFn soft_fn_f32(bool aff, bool loc, bool tr, Geo g);

@@ -119,7 +119,7 @@ __host__ __device__ inline size_t soft_smem_bytes(int K, int N, int G, int R, in
 }
 
 template <class T, bool AFF, bool LOC, bool TR, int G, int R>
-__global__ void __launch_bounds__(128) soft_kernel(const SoftArgs A) {
+__global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftArgs A) {
     constexpr int GR = G * R;
     constexpr int NV = AFF ? 3 : 1;          // values per cell
     constexpr int CV = NV * R;               // values per lane column
@@ -216,6 +216,7 @@ __global__ void __launch_bounds__(128) soft_kernel(const SoftArgs A) {
             T upM = T(0), upX = T(0), upY = T(0); // row above, column j
             T* fs = fwd + int64_t(s) * S * G * CV;
             int* fe = fexp + int64_t(s) * S * G;
+            int nbj = N;
             for (int t = 0; t < S; ++t) {
                 const int j = t - lane;           // column 0..n
                 if (lane == 0 && j <= n && s > 0) {
@@ -234,7 +235,8 @@ __global__ void __launch_bounds__(128) soft_kernel(const SoftArgs A) {
                 }
                 const bool active = (j >= 0) && (j <= n);
                 if (active) {
-                    const int bj = j >= 1 ? int(bp[j - 1]) : N;   // column 0: the zero column
+                    const int bj = nbj;                   // column 0: the zero column
+                    nbj = j < n ? int(bp[j]) : N;         // the next column's code, one step ahead
                     T pM = dgM, pX = dgX, pY = dgY;
                     T qM = upM, qX = upX, qY = upY;
 #pragma unroll
@@ -404,6 +406,9 @@ __global__ void __launch_bounds__(128) soft_kernel(const SoftArgs A) {
             T dnM = T(0), dnX = T(0), dnY = T(0);     // row below, column j
             const T* fs = fwd + int64_t(s) * S * G * CV;
             const int* fe = fexp + int64_t(s) * S * G;
+            T nf[CV];
+            int nEF = 0, nbj = N;
+            bool have_next = false;
             for (int t = 0; t < S; ++t) {
                 const int j = n - t + (G - 1 - lane);     // column n..0
                 if (lane == G - 1 && j >= 0 && s < nstripes - 1) {
@@ -423,10 +428,24 @@ __global__ void __launch_bounds__(128) soft_kernel(const SoftArgs A) {
                 }
                 const bool active = (j >= 0) && (j <= n);
                 if (active) {
-                    const int bj1 = j < n ? int(bp[j]) : N;   // b code of column j+1 (N: none)
+                    // this column's forward values were loaded one step ahead (or now, on
+                    // the lane's first step); issue the next column's loads before the math
+                    if (!have_next) {
+                        vload<T, CV>(nf, fs + (int64_t(j + lane) * G + lane) * CV);
+                        nEF = fe[int64_t(j + lane) * G + lane];
+                        nbj = j < n ? int(bp[j]) : N;
+                    }
                     T f[CV];
-                    vload<T, CV>(f, fs + (int64_t(j + lane) * G + lane) * CV);
-                    const int EF = fe[int64_t(j + lane) * G + lane];
+#pragma unroll
+                    for (int k = 0; k < CV; ++k) f[k] = nf[k];
+                    const int EF = nEF;
+                    const int bj1 = nbj;              // b code of column j+1 (N: none)
+                    have_next = j > 0;
+                    if (have_next) {
+                        vload<T, CV>(nf, fs + (int64_t(j - 1 + lane) * G + lane) * CV);
+                        nEF = fe[int64_t(j - 1 + lane) * G + lane];
+                        nbj = int(bp[j - 1]);
+                    }
                     // scale of this step's products: 2^(E_F + E_B - E_Z) / zhat
                     const double facd = pow2i<double>(EF + EB - EZ) * invz;
                     const T fac = static_cast<T>(facd);

@@ -19,13 +19,25 @@ struct WalkArgs {
     int32_t* guide;                    // per pair m+1 at oa[p] + p, or null
     uint8_t* moves; const int64_t* moves_off;   // keep_paths: walk-order moves, or null
     int32_t* path_info;                // per pair: n_moves, start_i, start_j (or null)
+    const int64_t* stripe_base;        // banded: per pair first entry of stripe_tab (else null)
+    const int64_t* stripe_tab;
 };
 
-__device__ __forceinline__ uint8_t code_at(const uint8_t* codes, int i, int j, int n, int G, int R) {
+// Byte of cell (i, j) in the fill's tiled layout; banded fills record each stripe's code
+// offset and first column in `tab` (null: the full DP, stripes of n + G - 1 steps from column 1).
+__device__ __forceinline__ uint8_t code_at(const uint8_t* codes, int i, int j, int n, int G, int R,
+                                           const int64_t* tab) {
     const int GR = G * R;
     const int s = (i - 1) / GR, w = (i - 1) % GR, g = w / R, r = w % R;
-    const int S = n + G - 1;
-    return codes[((int64_t(s) * S + (j - 1 + g)) * G + g) * R + r];
+    int64_t base;
+    int t;
+    if (tab) { base = tab[2 * s]; t = j - int(tab[2 * s + 1]) + g; }
+    else {
+        const int S8 = (n + G - 1 + 7) & ~7;
+        base = int64_t(s) * S8 * GR;
+        t = j - 1 + g;
+    }
+    return codes[base + ((int64_t(t >> 3) * G + g) * 8 + (t & 7)) * R + r];
 }
 
 __global__ void walk_kernel(const WalkArgs A) {
@@ -40,9 +52,9 @@ __global__ void walk_kernel(const WalkArgs A) {
     const uint16_t* gk = A.gtracks ? A.gtracks + ao + p : nullptr;
     const int N = A.N;
     const int64_t NN = int64_t(A.K) * N * N;
-    double* g = A.grad ? A.grad + A.gstride * p : nullptr;
-    if (g) for (int64_t k = 0; k < A.gstride; ++k) g[k] = 0.0;
+    double* g = A.grad ? A.grad + A.gstride * p : nullptr;   // zeroed by the host
     const uint8_t* codes = A.codes + A.code_off[p];
+    const int64_t* tab = A.stripe_tab ? A.stripe_tab + 2 * A.stripe_base[p] : nullptr;
     const int lay = A.end[4 * p + 3];
     const int G = lay >> 8, R = lay & 0xff;
     auto tset = [&](int i) -> int { return tk ? int(tk[i - 1]) : 0; };
@@ -88,12 +100,12 @@ __global__ void walk_kernel(const WalkArgs A) {
             if (i == 0 && j == 0) break;
             uint32_t c;
             if (A.local) {
-                c = (i == 0 || j == 0) ? 3u : code_at(codes, i, j, n, G, R);
+                c = (i == 0 || j == 0) ? 3u : code_at(codes, i, j, n, G, R, tab);
                 if (tbl == 0 && (c & 3u) == 3u) break;
             } else {
                 if (i == 0) { for (; j > 0; --j) emit(2, 0, j, j == 1); break; }
                 if (j == 0) { for (; i > 0; --i) emit(1, i, 0, i == 1); break; }
-                c = code_at(codes, i, j, n, G, R);
+                c = code_at(codes, i, j, n, G, R, tab);
             }
             if (i == 0) tbl = 2;
             else if (j == 0) tbl = 1;
@@ -110,7 +122,7 @@ __global__ void walk_kernel(const WalkArgs A) {
             int k;
             if (i == 0) k = A.local ? 3 : 2;
             else if (j == 0) k = A.local ? 3 : 1;
-            else k = code_at(codes, i, j, n, G, R);
+            else k = code_at(codes, i, j, n, G, R, tab);
             if (k == 3) break;
             if (k == 0) { emit(0, i, j, false); --i; --j; }
             else if (k == 1) {

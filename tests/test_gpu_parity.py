@@ -140,3 +140,82 @@ def test_soft_temperature(T):
     rng = np.random.default_rng(77)
     mat, gaps, sa, sb, tr, gt = _problem(rng, AA, 30, 5, 60, homolog=True)
     _soft_check(32, 1, 0, AA, mat, gaps, sa, sb, None, None, T=T)
+
+
+@pytest.mark.parametrize("gm", [0, 1])
+@pytest.mark.parametrize("am", [0, 1])
+@pytest.mark.parametrize("bw", [1, 5, 64])
+def test_banded_bit_exact(gm, am, bw):
+    """set_params + banded_grad around the guides of a full pass (batch_engine.hpp:633-653)."""
+    rng = np.random.default_rng(900 + gm + 2 * am + bw)
+    mat, gaps, sa, sb, tr, gt = _problem(rng, AA, 40, 1, 60, integer=False, homolog=True)
+    sa += rand_seqs(rng, 3, 150, 300, AA)
+    sb += [mutate(rng, s, AA) for s in sa[-3:]]
+    mat2 = mat + rng.normal(0, 0.3, size=mat.shape)
+    gaps2 = gaps + rng.uniform(0, 0.2, size=gaps.shape)
+    for prec in (32, 64):
+        cls = nw.SeqPairBatch if prec == 32 else nw.SeqPairBatchDouble
+        b = cls(sa, sb, _params(AA, mat, gaps), gap_model=("linear", "affine")[gm],
+                mode=("global", "local")[am], grad_mode="hard")
+        b.score_and_grad()
+        b.set_params(_params(AA, mat2, gaps2))
+        tot = b.banded_grad(bw)
+        enc = oracle.Encoded(encode(AA, sa), encode(AA, sb))
+        o0 = oracle.hard(prec, gm, am, mat, gaps, enc)
+        o = oracle.hard(prec, gm, am, mat2, gaps2, enc, guides_in=o0["guides"], band=bw)
+        assert np.array_equal(b.scores(), o["scores"]), np.nonzero(b.scores() != o["scores"])[0][:5]
+        gmat, ggap = b.grads()
+        flat = np.concatenate([gmat.reshape(len(sa), -1), ggap.reshape(len(sa), -1)], axis=1)
+        assert np.array_equal(flat, o["grads"])
+        assert np.array_equal(b.guides(), o["guides"])
+        assert tot == float(np.cumsum(o["scores"])[-1])
+
+
+@pytest.mark.parametrize("name", ["prot", "protf", "rna3"])
+def test_golden_reference_batches(name):
+    """The GPU path against the reference's own outputs (tests/golden/make_golden.py)."""
+    import os
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "reference_batches.npz"))
+    pre = name + "_"
+    alpha = str(z[pre + "alpha"])
+    sa, sb = [str(s) for s in z[pre + "sa"]], [str(s) for s in z[pre + "sb"]]
+    tr = z[pre + "tracks"] if pre + "tracks" in z.files else None
+    gt = z[pre + "gap_tracks"] if pre + "gap_tracks" in z.files else None
+    mat, gaps, mat2, gaps2 = z[pre + "mat"], z[pre + "gaps"], z[pre + "mat2"], z[pre + "gaps2"]
+    for gm in (0, 1):
+        for am in (0, 1):
+            for prec in (32, 64):
+                cls = nw.SeqPairBatch if prec == 32 else nw.SeqPairBatchDouble
+                b = cls(sa, sb, _params(alpha, mat, gaps), gap_model=("linear", "affine")[gm],
+                        mode=("global", "local")[am], grad_mode="hard", tracks=tr, gap_tracks=gt)
+                b.score_and_grad()
+                key = f"{pre}hard{prec}_g{gm}_m{am}_"
+                assert np.array_equal(b.scores(), z[key + "scores"])
+                gmat, ggap = b.grads()
+                if gmat.ndim == 3:
+                    gmat, ggap = gmat[:, None], ggap[:, None]
+                flat = np.concatenate([gmat.reshape(len(sa), -1), ggap.reshape(len(sa), -1)], axis=1)
+                assert np.array_equal(flat, z[key + "grads"])
+                assert np.array_equal(b.guides(), z[key + "guides"])
+                if tr is None:
+                    b.set_params(_params(alpha, mat2, gaps2))
+                    b.banded_grad(4)
+                    key = f"{pre}band{prec}_g{gm}_m{am}_"
+                    assert np.array_equal(b.scores(), z[key + "scores"])
+                    gmat, ggap = b.grads()
+                    flat = np.concatenate([gmat.reshape(len(sa), -1), ggap.reshape(len(sa), -1)], axis=1)
+                    assert np.array_equal(flat, z[key + "grads"])
+            for T in (1.0, 0.5):
+                b = nw.SeqPairBatch(sa, sb, _params(alpha, mat, gaps), gap_model=("linear", "affine")[gm],
+                                    mode=("global", "local")[am], grad_mode="soft", tracks=tr, gap_tracks=gt)
+                b.soft_temperature = T
+                b.score_and_grad()
+                key = f"{pre}soft_T{T}_g{gm}_m{am}_"
+                np.testing.assert_allclose(b.scores(), z[key + "scores"], rtol=SOFT_RTOL, atol=1e-5)
+                gmat, ggap = b.grads()
+                if gmat.ndim == 3:
+                    gmat, ggap = gmat[:, None], ggap[:, None]
+                flat = np.concatenate([gmat.reshape(len(sa), -1), ggap.reshape(len(sa), -1)], axis=1)
+                ref = z[key + "grads"]
+                scale = np.maximum(np.abs(ref).max(axis=1, keepdims=True), 1.0)
+                assert (np.abs(flat - ref) / scale).max() <= SOFT_RTOL
