@@ -53,6 +53,14 @@ int nwg_store_create(const uint8_t* codes_a, const int64_t* off_a, const uint8_t
                      const uint16_t* gap_tracks, int device, nwg_store** out);
 int nwg_store_destroy(nwg_store* s);
 
+/* Replace a store's pairs (same alphabet), reusing its device buffers (they only grow): every
+ * result, guide and plan of the previous pairs is dropped, the parameters stay.  The serving
+ * loop's way to run one batch after another without reallocating.  No direct counterpart in
+ * the reference (a batch there is built once); the equivalent of constructing a new batch. */
+int nwg_store_load(nwg_store* s, const uint8_t* codes_a, const int64_t* off_a, const uint8_t* codes_b,
+                   const int64_t* off_b, int64_t n_pairs, const uint16_t* tracks,
+                   const uint16_t* gap_tracks, void* stream);
+
 /* Parameters: K stacked N x N matrices (row-major) and K x 4 gaps (open_a, extend_a,
  * open_b, extend_b), copied.  Invalidates results, keeps guides.
  * Replaces BatchEngine::set_params (batch_engine.hpp:597-606). */
@@ -76,6 +84,12 @@ int nwg_grads(nwg_store* s, double* out);
  * bit-identical for identical per-pair gradients.
  * Replaces BatchEngine::weighted_grad / compute_grad (batch_engine.hpp:703-718, 1788-1827). */
 int nwg_reduce(nwg_store* s, const double* w, double* out);
+
+/* The reduction and scores of nwg_reduce / nwg_scores over the pairs [start, end) only, the
+ * blocks of 4096 counted from start: a request's own gradient inside a served batch is the
+ * same bits as when that request is a batch by itself.  (weighted_grad / scores over a view.) */
+int nwg_reduce_range(nwg_store* s, int64_t start, int64_t end, const double* w, double* out);
+int nwg_scores_range(nwg_store* s, int64_t start, int64_t end, double* out);
 
 /* Guides (guide_j: m + 1 ints per pair at off_a[p] + p), read and written.
  * Replace SeqPair::guide_j (seq_pair_batch.hpp:236) and the guide a banded call bands around. */
@@ -101,6 +115,30 @@ int nwg_status(nwg_store* s, int32_t* out);
 
 /* Device time (ms) of the last nwg_run's kernels and how many kernels it launched. */
 int nwg_last_timing(nwg_store* s, double* ms, int64_t* launches);
+
+/* ── Serving: continuous batching (no counterpart in the reference, a CPU library with
+ * no request loop; each request's results equal those of SeqPairBatch.score_and_grad +
+ * compute_grad on its pairs alone, batch_engine.hpp:615, 714) ──────────────────────────
+ * A server owns `workers` threads, each with a reusable store and stream.  Requests (host
+ * codes + offsets, one parameter snapshot each: the params current at submit) queue on
+ * submit; a free worker batches the queue's head requests within max_batch_pairs and the
+ * server-wide hbm_budget_bytes (estimated from DP sizes), aligns them with `job`, and hands
+ * every request its own scores and summed gradient (K*N*N + 4K doubles, the same bits as the
+ * request aligned alone).  Batches of different workers run concurrently on the GPU. */
+typedef struct nwg_server nwg_server;
+int nwg_server_create(int device, const nwg_job* job, int nalpha, const double* mats, const double* gaps,
+                      int K, int workers, int64_t hbm_budget_bytes, int64_t max_batch_pairs,
+                      nwg_server** out);
+int nwg_server_set_params(nwg_server* s, const double* mats, const double* gaps, int K);
+int nwg_server_submit(nwg_server* s, const uint8_t* codes_a, const int64_t* off_a, const uint8_t* codes_b,
+                      const int64_t* off_b, int64_t n_pairs, int64_t* ticket);
+/* Block until the request is done; scores: n_pairs doubles; grad: K*N*N + 4K (grad_mode != 0). */
+int nwg_server_wait(nwg_server* s, int64_t ticket, double* scores, double* grad, double* latency_ms);
+/* Latency p50 / p99 (ms) of completed requests, throughput since the first submit. */
+int nwg_server_stats(nwg_server* s, double* p50_ms, double* p99_ms, double* gcups, int64_t* done,
+                     int64_t* batches);
+int nwg_server_destroy(nwg_server* s);
+const char* nwg_server_last_error(void);
 
 /* Viterbi scores of n_pairs pairs WITHOUT any device allocation (no counterpart in the
  * reference: it is a CPU library).  For callers whose host framework owns all device memory

@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <tuple>
 #include <memory>
 #include <numeric>
 #include <stdexcept>
@@ -183,6 +184,13 @@ Geo pick_geo(bool soft, int rows, int n, int lanes, int rpl, bool lane_ok) {
     return best;
 }
 
+// Pairs are bucketed by geometry and by size class (the binary order of magnitude of the
+// padded DP), so a bucket's scratch stride is sized close to its own pairs.
+int size_class(int rows, int n) {
+    const double cells = double(std::max(rows, 1)) * double(std::max(n, 1));
+    return int(std::ceil(std::log2(cells)));
+}
+
 struct Bucket {
     Geo geo;
     std::vector<int32_t> pairs;
@@ -229,6 +237,7 @@ struct nwg_store {
     bool have_scores = false, have_grads = false, have_guides = false, have_paths = false;
     int last_grad_mode = 0, last_gm = -1, last_am = -1, last_prec = 0;
     Plan hard_plan, soft_plan, band_plan;
+    int64_t scratch_budget = int64_t(24) << 30;   // bytes of soft scratch one call may hold
     DBuf stripe_tab;
     std::vector<int32_t> h_status;
     // timing
@@ -284,13 +293,12 @@ void build_plan(nwg_store* s, Plan& P, bool soft, int lanes, int rpl, int elem_b
     const int64_t n = s->n;
     // one lane per pair keeps a K*N*N histogram per lane in shared memory (soft)
     const bool lane_ok_soft = int64_t(s->K) * s->N * s->N * elem_bytes * 32 <= 48 * 1024;
-    std::map<std::pair<int, int>, int> idx;
-    std::vector<int> geo_of(n);
+    std::map<std::tuple<int, int, int>, int> idx;
     for (int64_t p = 0; p < n; ++p) {
         const int m = int(s->oa[p + 1] - s->oa[p]), nb = int(s->ob[p + 1] - s->ob[p]);
         const int rows = soft ? m + 1 : m;
         Geo g = band ? Geo{32, 2, true} : pick_geo(soft, std::max(rows, 1), nb, lanes, rpl, soft ? lane_ok_soft : true);
-        auto key = std::make_pair(g.G, g.R);
+        auto key = std::make_tuple(g.G, g.R, size_class(rows, nb));
         auto itb = idx.find(key);
         int bi;
         if (itb == idx.end()) { bi = int(P.buckets.size()); idx[key] = bi; P.buckets.push_back(Bucket{g, {}, 0, 0, 0}); }
@@ -505,12 +513,12 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
     if (subset) {
         // a plan over the subset only (double reruns): one bucket per geometry
         P = &local_plan;
-        std::map<std::pair<int, int>, int> idx;
+        std::map<std::tuple<int, int, int>, int> idx;
         const bool lane_ok = int64_t(s->K) * s->N * s->N * sizeof(T) * 32 <= 48 * 1024;
         for (int32_t p : *subset) {
             const int m = int(s->oa[p + 1] - s->oa[p]), nb = int(s->ob[p + 1] - s->ob[p]);
             const Geo g = pick_geo(true, m + 1, nb, J.lanes, J.rows, lane_ok);
-            auto key = std::make_pair(g.G, g.R);
+            auto key = std::make_tuple(g.G, g.R, size_class(m + 1, nb));
             auto itb = idx.find(key);
             int bi;
             if (itb == idx.end()) { bi = int(P->buckets.size()); idx[key] = bi; P->buckets.push_back(Bucket{g, {}, 0, 0, 0}); }
@@ -561,12 +569,14 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
         occ = std::max(occ, 1);
         const int gpb = block / G;
         const int64_t items = int64_t(B.pairs.size());
-        const int64_t blocks = std::min<int64_t>((items + gpb - 1) / gpb, int64_t(sms) * occ);
-        const int64_t slots = blocks * gpb;
         const int64_t fwd_bytes = ((B.max_soft_cells * NV * int64_t(sizeof(T))) + 255) & ~int64_t(255);
         const int64_t exp_bytes = ((B.max_soft_cells / B.geo.R) * 4 + 255) & ~int64_t(255);
         const int64_t bnd_bytes = (int64_t(B.maxn) + 1) * (2 * NV * int64_t(sizeof(T)) + 8);
         const int64_t stride = ((fwd_bytes + exp_bytes + bnd_bytes) + 255) & ~int64_t(255);
+        // as many resident groups as fit the device (occupancy) and the scratch budget
+        int64_t blocks = std::min<int64_t>((items + gpb - 1) / gpb, int64_t(sms) * occ);
+        blocks = std::max<int64_t>(1, std::min<int64_t>(blocks, s->scratch_budget / std::max<int64_t>(1, stride * gpb)));
+        const int64_t slots = blocks * gpb;
         s->scratch.need(size_t(slots * stride));
         nwg::SoftArgs A{};
         A.a = s->a.as<uint8_t>(); A.oa = s->doa.as<int64_t>();
@@ -646,6 +656,66 @@ int guarded(F&& f) {
     }
 }
 
+// Upload a batch of pairs into a store (new or reused: buffers only grow), dropping every
+// result, guide and plan of the previous pairs; the parameters stay.
+void load_pairs(nwg_store* s, const uint8_t* codes_a, const int64_t* off_a, const uint8_t* codes_b,
+                const int64_t* off_b, int64_t n_pairs, const uint16_t* tracks, const uint16_t* gap_tracks,
+                cudaStream_t st) {
+    if (n_pairs < 0) throw Error(NWG_EINVAL, "bad n_pairs");
+    const int nalpha = s->nalpha;
+    s->n = n_pairs;
+    s->oa.assign(off_a, off_a + n_pairs + 1);
+    s->ob.assign(off_b, off_b + n_pairs + 1);
+    s->total_a = s->oa[n_pairs] - s->oa[0];
+    s->total_b = s->ob[n_pairs] - s->ob[0];
+    for (int64_t p = 0; p < n_pairs; ++p) {
+        if (s->oa[p + 1] < s->oa[p] || s->ob[p + 1] < s->ob[p]) throw Error(NWG_EINVAL, "offsets decrease");
+        if (s->oa[p + 1] - s->oa[p] > (1 << 30) || s->ob[p + 1] - s->ob[p] > (1 << 30))
+            throw Error(NWG_EINVAL, "sequence too long");
+    }
+    const int64_t a0 = s->oa[0], b0 = s->ob[0];
+    for (auto& v : s->oa) v -= a0;
+    for (auto& v : s->ob) v -= b0;
+    for (int64_t k = 0; k < s->total_a; ++k)
+        if (codes_a[a0 + k] >= nalpha) throw Error(NWG_EINVAL, "code out of range in sequence A");
+    for (int64_t k = 0; k < s->total_b; ++k)
+        if (codes_b[b0 + k] >= nalpha) throw Error(NWG_EINVAL, "code out of range in sequence B");
+    s->a.need(size_t(s->total_a) + 16);
+    s->b.need(size_t(s->total_b) + 16);
+    if (s->total_a) NWG_CUDA(cudaMemcpyAsync(s->a.p, codes_a + a0, size_t(s->total_a), cudaMemcpyHostToDevice, st));
+    if (s->total_b) NWG_CUDA(cudaMemcpyAsync(s->b.p, codes_b + b0, size_t(s->total_b), cudaMemcpyHostToDevice, st));
+    s->doa.need(size_t(n_pairs + 1) * 8);
+    s->dob.need(size_t(n_pairs + 1) * 8);
+    NWG_CUDA(cudaMemcpyAsync(s->doa.p, s->oa.data(), size_t(n_pairs + 1) * 8, cudaMemcpyHostToDevice, st));
+    NWG_CUDA(cudaMemcpyAsync(s->dob.p, s->ob.data(), size_t(n_pairs + 1) * 8, cudaMemcpyHostToDevice, st));
+    s->tracked_seq = false;
+    s->max_track = 0;
+    if (tracks) {
+        s->tracked_seq = true;
+        s->tracks.need(size_t(std::max<int64_t>(s->total_a, 1)) * 2);
+        if (s->total_a) NWG_CUDA(cudaMemcpyAsync(s->tracks.p, tracks + a0, size_t(s->total_a) * 2, cudaMemcpyHostToDevice, st));
+        for (int64_t k = 0; k < s->total_a; ++k) s->max_track = std::max<int>(s->max_track, tracks[a0 + k]);
+    }
+    if (gap_tracks) {
+        s->tracked_seq = true;
+        if (!tracks) {   // gap tracks alone: the track is all zero
+            s->tracks.need(size_t(std::max<int64_t>(s->total_a, 1)) * 2);
+            NWG_CUDA(cudaMemsetAsync(s->tracks.p, 0, size_t(std::max<int64_t>(s->total_a, 1)) * 2, st));
+        }
+        const int64_t rows = s->total_a + n_pairs;
+        s->gtracks.need(size_t(rows) * 2);
+        NWG_CUDA(cudaMemcpyAsync(s->gtracks.p, gap_tracks + a0, size_t(rows) * 2, cudaMemcpyHostToDevice, st));
+        for (int64_t k = 0; k < rows; ++k) s->max_track = std::max<int>(s->max_track, gap_tracks[a0 + k]);
+    }
+    if (s->K && s->tracked_seq && s->max_track >= s->K)
+        throw Error(NWG_EINVAL, "nwgrad: a track entry is not a parameter set");
+    // the host buffers may be reused by the caller after this returns
+    NWG_CUDA(cudaStreamSynchronize(st));
+    s->hard_plan.reset(); s->soft_plan.reset(); s->band_plan.reset();
+    s->have_scores = s->have_grads = s->have_guides = s->have_paths = false;
+    s->h_status.clear();
+}
+
 }  // namespace
 
 extern "C" {
@@ -657,57 +727,25 @@ int nwg_store_create(const uint8_t* codes_a, const int64_t* off_a, const uint8_t
                      const uint16_t* gap_tracks, int device, nwg_store** out) {
     return guarded([&] {
         if (!out) throw Error(NWG_EINVAL, "out is null");
-        if (n_pairs < 0 || nalpha <= 0 || nalpha > 255) throw Error(NWG_EINVAL, "bad n_pairs / nalpha");
+        if (nalpha <= 0 || nalpha > 255) throw Error(NWG_EINVAL, "bad nalpha");
         auto s = std::make_unique<nwg_store>();
         s->device = device;
         NWG_CUDA(cudaSetDevice(device));
-        s->n = n_pairs; s->nalpha = nalpha;
-        s->oa.assign(off_a, off_a + n_pairs + 1);
-        s->ob.assign(off_b, off_b + n_pairs + 1);
-        s->total_a = s->oa[n_pairs] - s->oa[0];
-        s->total_b = s->ob[n_pairs] - s->ob[0];
-        for (int64_t p = 0; p < n_pairs; ++p) {
-            if (s->oa[p + 1] < s->oa[p] || s->ob[p + 1] < s->ob[p]) throw Error(NWG_EINVAL, "offsets decrease");
-            if (s->oa[p + 1] - s->oa[p] > (1 << 30) || s->ob[p + 1] - s->ob[p] > (1 << 30))
-                throw Error(NWG_EINVAL, "sequence too long");
-        }
-        // rebase offsets to 0
-        const int64_t a0 = s->oa[0], b0 = s->ob[0];
-        for (auto& v : s->oa) v -= a0;
-        for (auto& v : s->ob) v -= b0;
-        for (int64_t k = 0; k < s->total_a; ++k)
-            if (codes_a[a0 + k] >= nalpha) throw Error(NWG_EINVAL, "code out of range in sequence A");
-        for (int64_t k = 0; k < s->total_b; ++k)
-            if (codes_b[b0 + k] >= nalpha) throw Error(NWG_EINVAL, "code out of range in sequence B");
-        s->a.need(size_t(s->total_a) + 16);
-        s->b.need(size_t(s->total_b) + 16);
-        if (s->total_a) NWG_CUDA(cudaMemcpy(s->a.p, codes_a + a0, size_t(s->total_a), cudaMemcpyHostToDevice));
-        if (s->total_b) NWG_CUDA(cudaMemcpy(s->b.p, codes_b + b0, size_t(s->total_b), cudaMemcpyHostToDevice));
-        s->doa.need(size_t(n_pairs + 1) * 8);
-        s->dob.need(size_t(n_pairs + 1) * 8);
-        NWG_CUDA(cudaMemcpy(s->doa.p, s->oa.data(), size_t(n_pairs + 1) * 8, cudaMemcpyHostToDevice));
-        NWG_CUDA(cudaMemcpy(s->dob.p, s->ob.data(), size_t(n_pairs + 1) * 8, cudaMemcpyHostToDevice));
-        if (tracks) {
-            s->tracked_seq = true;
-            s->tracks.need(size_t(std::max<int64_t>(s->total_a, 1)) * 2);
-            if (s->total_a) NWG_CUDA(cudaMemcpy(s->tracks.p, tracks + a0, size_t(s->total_a) * 2, cudaMemcpyHostToDevice));
-            for (int64_t k = 0; k < s->total_a; ++k) s->max_track = std::max<int>(s->max_track, tracks[a0 + k]);
-        }
-        if (gap_tracks) {
-            s->tracked_seq = true;
-            if (!tracks) {
-                // gap tracks alone: the track is all zero
-                s->tracks.need(size_t(std::max<int64_t>(s->total_a, 1)) * 2);
-                NWG_CUDA(cudaMemset(s->tracks.p, 0, size_t(std::max<int64_t>(s->total_a, 1)) * 2));
-            }
-            const int64_t rows = s->total_a + n_pairs;
-            s->gtracks.need(size_t(rows) * 2);
-            NWG_CUDA(cudaMemcpy(s->gtracks.p, gap_tracks + a0, size_t(rows) * 2, cudaMemcpyHostToDevice));
-            for (int64_t k = 0; k < rows; ++k) s->max_track = std::max<int>(s->max_track, gap_tracks[a0 + k]);
-        }
+        s->nalpha = nalpha;
         NWG_CUDA(cudaEventCreate(&s->ev0));
         NWG_CUDA(cudaEventCreate(&s->ev1));
+        load_pairs(s.get(), codes_a, off_a, codes_b, off_b, n_pairs, tracks, gap_tracks, nullptr);
         *out = s.release();
+    });
+}
+
+int nwg_store_load(nwg_store* s, const uint8_t* codes_a, const int64_t* off_a, const uint8_t* codes_b,
+                   const int64_t* off_b, int64_t n_pairs, const uint16_t* tracks, const uint16_t* gap_tracks,
+                   void* stream) {
+    return guarded([&] {
+        if (!s) throw Error(NWG_EINVAL, "null store");
+        NWG_CUDA(cudaSetDevice(s->device));
+        load_pairs(s, codes_a, off_a, codes_b, off_b, n_pairs, tracks, gap_tracks, static_cast<cudaStream_t>(stream));
     });
 }
 
@@ -856,6 +894,38 @@ int nwg_reduce(nwg_store* s, const double* w, double* out) {
         blocked_total_kernel<<<unsigned((gs + 127) / 128), 128>>>(s->part.as<double>(), nb, gs, s->red.as<double>());
         NWG_CUDA(cudaGetLastError());
         NWG_CUDA(cudaMemcpy(out, s->red.p, size_t(gs) * 8, cudaMemcpyDeviceToHost));
+    });
+}
+
+int nwg_reduce_range(nwg_store* s, int64_t start, int64_t end, const double* w, double* out) {
+    return guarded([&] {
+        if (!s->have_grads) throw Error(NWG_ESTATE, "gradient not computed; call score_and_grad() or banded_grad() first");
+        if (start < 0 || end > s->n || start > end) throw Error(NWG_EINVAL, "bad pair range");
+        NWG_CUDA(cudaSetDevice(s->device));
+        const int64_t gs = s->gstride, n = end - start;
+        const int64_t B = 4096, nb = (n + B - 1) / B;
+        if (n == 0) { for (int64_t k = 0; k < gs; ++k) out[k] = 0.0; return; }
+        s->part.need(size_t(nb * gs) * 8);
+        s->red.need(size_t(gs) * 8 + size_t(w ? n : 0) * 8);
+        double* dw = nullptr;
+        if (w) {
+            dw = s->red.as<double>() + gs;
+            NWG_CUDA(cudaMemcpy(dw, w, size_t(n) * 8, cudaMemcpyHostToDevice));
+        }
+        dim3 grid(unsigned((gs + 31) / 32), unsigned(nb));
+        blocked_partial_kernel<<<grid, 32>>>(s->grad.as<double>() + start * gs, dw, n, gs, B, s->part.as<double>());
+        NWG_CUDA(cudaGetLastError());
+        blocked_total_kernel<<<unsigned((gs + 127) / 128), 128>>>(s->part.as<double>(), nb, gs, s->red.as<double>());
+        NWG_CUDA(cudaGetLastError());
+        NWG_CUDA(cudaMemcpy(out, s->red.p, size_t(gs) * 8, cudaMemcpyDeviceToHost));
+    });
+}
+
+int nwg_scores_range(nwg_store* s, int64_t start, int64_t end, double* out) {
+    return guarded([&] {
+        if (!s->have_scores) throw Error(NWG_ESTATE, "scores not computed; call score_and_grad() first");
+        if (start < 0 || end > s->n || start > end) throw Error(NWG_EINVAL, "bad pair range");
+        if (end > start) NWG_CUDA(cudaMemcpy(out, s->score.as<double>() + start, size_t(end - start) * 8, cudaMemcpyDeviceToHost));
     });
 }
 

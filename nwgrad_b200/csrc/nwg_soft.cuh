@@ -589,16 +589,21 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
                 }
             }
             if constexpr (G > 1) {
+                // lane by lane, so the sum's order (and bits) never depends on scheduling
+                for (int l = 0; l < G; ++l) {
+                    if (lane == l) {
 #pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    if (krow[r] >= K * N) continue;
-                    for (int c = 0; c < N; ++c) {
-                        T& v = macc[(size_t(c) * G + lane) * R + r];
-                        if (v != T(0)) atomicAdd(&hist[krow[r] * N + c], v);
-                        v = T(0);
+                        for (int r = 0; r < R; ++r) {
+                            if (krow[r] >= K * N) continue;
+                            for (int c = 0; c < N; ++c) {
+                                T& v = macc[(size_t(c) * G + lane) * R + r];
+                                hist[krow[r] * N + c] += v;
+                                v = T(0);
+                            }
+                        }
                     }
+                    __syncwarp(gmask);
                 }
-                __syncwarp(gmask);
             }
         }
         if constexpr (G > 1) bad = __any_sync(gmask, bad);
