@@ -1,5 +1,6 @@
 #!/usr/bin/env python3
-"""Benchmark: soft-gradient global affine batch GCUPS on one B200 (and N GPUs as replicas).
+"""Benchmark: soft-gradient global affine batch GCUPS on one B200 (and N GPUs as replicas),
+against the plain GPU fill, plus p50/p99 serving latency.
 
 Workload (the soft-gradient batch configuration, seeded synthetic stand-in for the
 reference's protein fixtures): 100,000 homologous protein pairs over a 20-letter alphabet,
@@ -11,6 +12,13 @@ pos.compute_grad() - neg.compute_grad(), float32 DP.  GCUPS = sum of len(a) * le
 both batches / step time (the reference's cell definition, tools/fleetbench/arm.py:317).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+The headline arm runs the autotuned geometries (``SeqPairBatch.autotune``); the plain arm
+runs the same steps with the plain fill (one fixed geometry, 32 lanes x 4 rows, one launch
+per size bucket).  The serving arm streams requests (lengths log-uniform 20-5000, batch sizes
+log-uniform 1-4096, B a mutated copy of A) through the continuous-batching server and, for
+comparison, through plain-fill batches one request at a time, first as a burst (throughput)
+then as Poisson arrivals at 70 % of the plain arm's capacity (p50/p99 latency).
 
 Prints one JSON line (rank 0).  Under torchrun every rank aligns its own copy of the
 workload (weak scaling) and the margin gradients are summed over ranks (NCCL all-reduce).
@@ -111,6 +119,34 @@ def c1_workload(n_pairs=10000, seed=0):
     return mat, a, oa, b, ob
 
 
+def c5_requests(n_req, seed=5, max_batch=4096):
+    """Serving requests: batch size log-uniform 1..max_batch, A lengths log-uniform 20-5000,
+    B = A with 30 % substitutions and single-residue insertions / deletions at 2.5 % each."""
+    rng = np.random.default_rng(seed)
+    freqs = rng.dirichlet(np.full(20, 5.0))
+    out = []
+    for _ in range(n_req):
+        k = min(max_batch, int(np.exp(rng.uniform(0.0, np.log(max_batch + 1)))))
+        la = np.exp(rng.uniform(np.log(20), np.log(5000), size=k)).astype(np.int64)
+        oa = np.zeros(k + 1, np.int64)
+        np.cumsum(la, out=oa[1:])
+        a = rng.choice(20, size=int(oa[-1]), p=freqs).astype(np.uint8)
+        b = a.copy()
+        s = rng.random(b.size) < 0.30
+        b[s] = rng.choice(20, size=int(s.sum()), p=freqs)
+        keep = (rng.random(b.size) >= 0.025).astype(np.int64)
+        ins = rng.random(b.size) < 0.025
+        cnt = keep + ins
+        cnt[oa[1:] - 1] = np.maximum(cnt[oa[1:] - 1], 1)     # no pair's B comes out empty
+        bb = b[np.repeat(np.arange(b.size), cnt)]
+        last = np.cumsum(cnt) - 1
+        bb[last[ins]] = rng.choice(20, size=int(ins.sum()), p=freqs)
+        ob = np.zeros(k + 1, np.int64)
+        np.cumsum(np.add.reduceat(cnt, oa[:-1]), out=ob[1:])
+        out.append((a, oa, bb.astype(np.uint8), ob))
+    return out
+
+
 def cells_of(oa, ob):
     return float(np.sum(np.diff(oa).astype(np.float64) * np.diff(ob).astype(np.float64)))
 
@@ -202,6 +238,95 @@ def cpu_model():
     return "unknown"
 
 
+# ── serving ──────────────────────────────────────────────────────────────────
+def _quantiles(lat):
+    v = np.sort(np.asarray(lat, np.float64))
+    q = lambda f: float(v[min(v.size, max(1, int(np.ceil(f * v.size)))) - 1]) if v.size else None  # noqa: E731
+    return q(0.50), q(0.99)
+
+
+def serve_server(params, reqs, arrivals, device, workers=3):
+    """Requests through the continuous-batching server; arrivals in seconds from the start
+    (all zero: a burst).  Returns (p50 ms, p99 ms, GCUPS over the makespan, batches)."""
+    import queue
+    from nwgrad_b200.serve import Server
+    q = queue.Queue()
+    lat = []
+    cells = sum(cells_of(oa, ob) for _, oa, _, ob in reqs)
+
+    def waiter(srv):
+        while True:
+            item = q.get()
+            if item is None:
+                return
+            t, k = item
+            lat.append(srv.wait(t, k)[2])
+
+    with Server(params, grad_mode="soft", workers=workers, hbm_budget_gb=96.0, max_batch_pairs=16384,
+                device=device) as srv:
+        th = threading.Thread(target=waiter, args=(srv,), daemon=True)
+        th.start()
+        t0 = time.perf_counter()
+        for (a, oa, b, ob), at in zip(reqs, arrivals):
+            d = at - (time.perf_counter() - t0)
+            if d > 0:
+                time.sleep(d)
+            q.put((srv.submit_codes(a, oa, b, ob), len(oa) - 1))
+        q.put(None)
+        th.join()
+        span = time.perf_counter() - t0
+        st = srv.stats()
+    p50, p99 = _quantiles(lat)
+    return {"p50_ms": p50, "p99_ms": p99, "gcups": cells / span / 1e9, "seconds": span,
+            "batches": int(st["batches"]), "requests": len(reqs)}
+
+
+def serve_plain(params, reqs, arrivals, device):
+    """The same requests through plain-fill batches, one request at a time in arrival order
+    (upload, align, read back): latency = done - arrival."""
+    import nwgrad_b200 as nw
+    lat = []
+    cells = sum(cells_of(oa, ob) for _, oa, _, ob in reqs)
+    t0 = time.perf_counter()
+    for (a, oa, b, ob), at in zip(reqs, arrivals):
+        d = at - (time.perf_counter() - t0)
+        if d > 0:
+            time.sleep(d)
+        bt = nw.SeqPairBatch.from_codes(a, oa, b, ob, params, grad_mode="soft", device=device)
+        bt.use_plain_fill()
+        bt.score_and_grad()
+        bt.scores()
+        bt.compute_grad()
+        lat.append((time.perf_counter() - t0 - at) * 1e3)
+        del bt
+    span = time.perf_counter() - t0
+    p50, p99 = _quantiles(lat)
+    return {"p50_ms": p50, "p99_ms": p99, "gcups": cells / span / 1e9, "seconds": span, "requests": len(reqs)}
+
+
+def serve_bench(params, n_req, device, seed=5):
+    reqs = c5_requests(n_req, seed=seed)
+    cells = sum(cells_of(oa, ob) for _, oa, _, ob in reqs)
+    burst = [0.0] * len(reqs)
+    # warm both paths (library, pools, plans) on a few requests
+    serve_server(params, reqs[:8], burst[:8], device)
+    serve_plain(params, reqs[:8], burst[:8], device)
+    srv_burst = serve_server(params, reqs, burst, device)
+    plain_burst = serve_plain(params, reqs, burst, device)
+    # Poisson arrivals at 70 % of the plain arm's capacity
+    rate = 0.7 * len(reqs) / plain_burst["seconds"]
+    rng = np.random.default_rng(seed + 1000)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(reqs))).tolist()
+    srv_poisson = serve_server(params, reqs, arrivals, device)
+    plain_poisson = serve_plain(params, reqs, arrivals, device)
+    return {"requests": len(reqs), "pairs": int(sum(len(oa) - 1 for _, oa, _, _ in reqs)), "cells": cells,
+            "workload": "lengths log-uniform 20-5000, batch sizes log-uniform 1-4096, B = A mutated "
+                        "(30% subs, 2.5% ins, 2.5% del), soft global affine f32",
+            "offered_rate_per_s": rate,
+            "server": {"burst": srv_burst, "poisson": srv_poisson, "workers": 3},
+            "plain_fill_one_at_a_time": {"burst": plain_burst, "poisson": plain_poisson}}
+
+
 # ── main ─────────────────────────────────────────────────────────────────────
 def main():
     ap = argparse.ArgumentParser()
@@ -213,6 +338,10 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=4000, help="pairs per batch in the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain-fill arm")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving arm")
+    ap.add_argument("--serve-requests", type=int, default=1000)
+    ap.add_argument("--no-tune", action="store_true", help="the planner's geometries instead of the autotuner's")
     ap.add_argument("--workload", default="c2-soft", choices=["c2-soft", "c1-hard"],
                     help="c2-soft (default): the soft-gradient batch; c1-hard: the plain hard batch (side measurement)")
     args = ap.parse_args()
@@ -264,6 +393,10 @@ def main():
     pos = nw.SeqPairBatch.from_codes(a, oa, bp, obp, params, grad_mode="soft", device=local)
     neg = nw.SeqPairBatch.from_codes(a, oa, bn, obn, params, grad_mode="soft", device=local)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    tune_table = {}
+    if not args.no_tune:
+        tune_table = pos.autotune()
+        neg.autotune()
 
     def step():
         pos.score_and_grad()
@@ -279,38 +412,61 @@ def main():
         dist.all_reduce(t)
         return g
 
-    for _ in range(max(args.warmup, 3)):
-        allreduce(step())
-    torch.cuda.synchronize()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    kernel_ms = 0.0
-    launches = 0
-    if dist is not None:
-        dist.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
-        for k in range(args.steps):
-            flush.zero_()                        # L2 flush, outside the timed events
-            torch.cuda.synchronize()
-            ev[k][0].record()
+    def timed(sample_clocks):
+        for _ in range(max(args.warmup, 3)):
             allreduce(step())
-            ev[k][1].record()
-            for b in (pos, neg):
-                ms_b, l_b = b.last_timing()
-                kernel_ms += ms_b
-                launches += l_b
-            launches += 4                        # two reductions per compute_grad
         torch.cuda.synchronize()
-    if dist is not None:
-        dist.barrier()
-    torch.cuda.synchronize()
-    step_ms = [e[0].elapsed_time(e[1]) for e in ev]
-    total_ms = float(np.sum(step_ms))
-    if dist is not None:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(args.steps)]
+        kernel_ms = 0.0
+        launches = 0
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        clk = ClockSampler(local) if sample_clocks else None
+        if clk:
+            clk.__enter__()
+        try:
+            for k in range(args.steps):
+                flush.zero_()                        # L2 flush, outside the timed events
+                torch.cuda.synchronize()
+                ev[k][0].record()
+                allreduce(step())
+                ev[k][1].record()
+                for b in (pos, neg):
+                    ms_b, l_b = b.last_timing()
+                    kernel_ms += ms_b
+                    launches += l_b
+                launches += 4                        # two reductions per compute_grad
+            torch.cuda.synchronize()
+        finally:
+            if clk:
+                clk.__exit__()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        step_ms = [e[0].elapsed_time(e[1]) for e in ev]
+        total_ms = float(np.sum(step_ms))
+        if dist is not None:
+            t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            total_ms = float(t.item())
+        return total_ms, step_ms, kernel_ms, launches, clk
+
+    total_ms, step_ms, kernel_ms, launches, clk = timed(True)
     value = world * cells * args.steps / (total_ms / 1e3) / 1e9
+    plain = None
+    if not args.no_plain:
+        pos.use_plain_fill()
+        neg.use_plain_fill()
+        p_total, p_steps, p_kms, p_launch, _ = timed(False)
+        plain = {"value": world * cells * args.steps / (p_total / 1e3) / 1e9, "unit": "GCUPS",
+                 "ms_per_step": p_total / args.steps, "kernel_ms_per_step": p_kms / args.steps,
+                 "geometry": "32 lanes x 4 rows for every pair, one launch per size bucket",
+                 "tuned_over_plain": (value / (world * cells * args.steps / (p_total / 1e3) / 1e9))}
+        if not args.no_tune:
+            pos.autotune()
+            neg.autotune()
 
     # end to end through the public API: host codes uploaded, aligned, gradient read back
     e2e = None
@@ -324,6 +480,9 @@ def main():
             t0 = time.perf_counter()
             p_ = nw.SeqPairBatch.from_codes(a, oa, bp, obp, params, grad_mode="soft", device=local)
             n_ = nw.SeqPairBatch.from_codes(a, oa, bn, obn, params, grad_mode="soft", device=local)
+            if not args.no_tune:
+                p_.autotune()
+                n_.autotune()
             s = p_.score_and_grad() - n_.score_and_grad()
             g = p_.compute_grad() - n_.compute_grad()
             allreduce(g)
@@ -337,7 +496,8 @@ def main():
             em = float(t.item())
         e2e = {"value": world * cells / (em / 1e3) / 1e9, "unit": "GCUPS", "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "ms_per_step": em,
-               "path": "SeqPairBatch.from_codes (host codes -> HBM) + score_and_grad + compute_grad"}
+               "path": "SeqPairBatch.from_codes (host codes -> HBM) + autotune (cached table) + "
+                       "score_and_grad + compute_grad"}
 
     clocks = clk.summary()
     # roofline of the soft kernel: algorithmic FP32 ops per cell over the kernels' device time
@@ -363,13 +523,18 @@ def main():
             cpu = {"value": r["value"], "unit": "GCUPS", "cores": r["threads"], "kind": "reference",
                    "sample": f"{2 * args.cpu_sample} pairs ({r['cells']:.3g} cells) of the workload, best of "
                              f"{len(r['seconds'])}, {cpu_model()}, isa {r['isa']}"}
+    serve = None
+    if rank == 0 and world == 1 and not args.no_serve and args.serve_requests > 0:
+        serve = serve_bench(params, args.serve_requests, local)
     if rank == 0:
         print(json.dumps({
             "metric": "soft-grad batch GCUPS", "value": value, "unit": "GCUPS", "n_gpus": world,
             "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": total_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded)", "config": config, "e2e": e2e, "roofline": roofline,
-            "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches // max(args.steps, 1) * args.steps,
+            "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
+            "plain_fill": plain, "serve": serve,
+            "autotune": {str(k): f"{v[0]} lanes x {v[1]} rows" for k, v in tune_table.items()},
             "step_ms": step_ms}))
     if dist is not None:
         dist.destroy_process_group()

@@ -72,6 +72,22 @@ int nwg_params_set(nwg_store* s, const double* mats, const double* gaps, int K, 
  * Replaces BatchEngine::score_and_grad (batch_engine.hpp:615-629) and banded_grad (:633-653). */
 int nwg_run(nwg_store* s, const nwg_job* job, void* stream, double* total);
 
+/* Kernel geometry: pairs of a size class (max(20, ceil(log2(rows * columns)))) run with `lanes`
+ * lanes per pair and `rows` DP rows per lane from now on (soft != 0: the soft path, else the
+ * hard fill).  size_class -1 forgets every such choice (the planner picks per pair);
+ * size_class -2 selects the plain fill (one fixed geometry, 32 lanes x 4 rows, for every
+ * pair).  Results do not depend on the geometry.  No counterpart in the reference (its
+ * kernel / fill choice is a CPU ISA dispatch). */
+int nwg_set_geometry(nwg_store* s, int soft, int size_class, int lanes, int rows);
+
+/* Device memory of soft runs: scratch_budget_bytes caps the forward tables one call holds
+ * (fewer pairs run at once when they are large); a pair whose whole forward table would be
+ * above checkpoint_bytes keeps only its stripe boundaries and recomputes each stripe just
+ * before that stripe's backward (results are bit-identical either way).  A value < 0 keeps the
+ * current setting (defaults 24 GiB and 16 MiB).  No counterpart in the reference (its CPU
+ * path keeps a whole table per thread). */
+int nwg_set_memory(nwg_store* s, int64_t scratch_budget_bytes, int64_t checkpoint_bytes);
+
 /* Per-pair scores (n_pairs doubles).  Replaces BatchEngine::scores (batch_engine.hpp:689). */
 int nwg_scores(nwg_store* s, double* out);
 

@@ -53,9 +53,11 @@ def lib():
     L.nwg_paths.argtypes = [C.c_void_p, _i64p, _u8p, C.c_int64, _i32p, _i32p]
     L.nwg_status.argtypes = [C.c_void_p, _i32p]
     L.nwg_last_timing.argtypes = [C.c_void_p, _dp, _i64p]
+    L.nwg_set_memory.argtypes = [C.c_void_p, C.c_int64, C.c_int64]
+    L.nwg_set_geometry.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int]
     for name in ("nwg_store_create", "nwg_store_destroy", "nwg_params_set", "nwg_run", "nwg_scores",
                  "nwg_grads", "nwg_reduce", "nwg_guides", "nwg_set_guides", "nwg_resolve_guides", "nwg_paths", "nwg_status",
-                 "nwg_last_timing"):
+                 "nwg_last_timing", "nwg_set_memory", "nwg_set_geometry"):
         getattr(L, name).restype = C.c_int
     _lib = L
     return L

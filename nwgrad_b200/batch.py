@@ -481,6 +481,30 @@ class SeqPairBatch:
     def params(self) -> AlignParams:
         return self._params.copy()
 
+    def autotune(self, sample_pairs: int = 8192, force: bool = False, verbose: bool = False) -> dict:
+        """Pick the fastest kernel geometry per size class of this batch (measured on a sample of
+        its own pairs, cached per device and problem type) and use it from now on.  Results do
+        not change: every geometry computes the same cells.  Returns {size class: (lanes, rows)}."""
+        from . import tune
+        if self._store is None or self._n == 0:
+            return {}
+        table = tune.tune(self, sample_pairs=sample_pairs, force=force, verbose=verbose)
+        tune.apply(self, table)
+        return table
+
+    def use_plain_fill(self) -> None:
+        """Run every pair with one fixed geometry (32 lanes x 4 rows), bucketed by size only:
+        the untuned baseline the autotuner is measured against."""
+        from . import tune
+        if self._store is not None:
+            tune.plain(self)
+
+    def set_memory(self, scratch_budget_bytes: int = -1, checkpoint_bytes: int = -1) -> None:
+        """Device memory of soft runs: the forward-table budget of one call, and the per-pair
+        table size above which only stripe boundaries are kept and each stripe is recomputed
+        before its backward (bit-identical results).  -1 keeps the current value."""
+        check(self._store._L.nwg_set_memory(self._store.h, int(scratch_budget_bytes), int(checkpoint_bytes)))
+
     def last_timing(self):
         """(device ms, kernel launches) of the last GPU call."""
         ms = C.c_double(0)

@@ -41,20 +41,44 @@ struct Error : std::runtime_error {
                         std::string(#call) + ": " + cudaGetErrorString(e_));               \
     } while (0)
 
-// A device buffer that only grows.
+// A device buffer that only grows, from the device's stream-ordered memory pool (which keeps
+// freed memory for reuse: a batch built after another reuses its blocks without a cudaMalloc).
+// With a stream, need() and release() free and allocate in that stream's order; without one
+// they wait for the whole device first, so no launch on any stream still uses the old block.
 struct DBuf {
     void* p = nullptr;
     size_t bytes = 0;
-    void need(size_t n) {
+    void need(size_t n, cudaStream_t st = nullptr) {
         if (n <= bytes) return;
-        if (p) cudaFree(p);
+        if (!st) NWG_CUDA(cudaDeviceSynchronize());
+        if (p) cudaFreeAsync(p, st);
         p = nullptr; bytes = 0;
-        NWG_CUDA(cudaMalloc(&p, std::max<size_t>(n, 256)));
-        bytes = std::max<size_t>(n, 256);
+        const size_t want = std::max<size_t>(n + n / 8, 256);
+        NWG_CUDA(cudaMallocAsync(&p, want, st));
+        if (!st) NWG_CUDA(cudaStreamSynchronize(nullptr));
+        bytes = want;
     }
-    void release() { if (p) cudaFree(p); p = nullptr; bytes = 0; }
+    void release(cudaStream_t st = nullptr) {
+        if (!p) return;
+        if (!st) cudaDeviceSynchronize();
+        cudaFreeAsync(p, st);
+        if (!st) cudaStreamSynchronize(nullptr);
+        p = nullptr; bytes = 0;
+    }
     template <class T> T* as() const { return static_cast<T*>(p); }
 };
+
+// The pool keeps what it frees (no release threshold): repeated batches reuse device memory.
+void keep_pool(int dev) {
+    static bool done[64] = {};
+    if (dev < 0 || dev >= 64 || done[dev]) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t thr = ~uint64_t(0);
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    done[dev] = true;
+}
 
 // ── reductions ────────────────────────────────────────────────────────────────
 // The reference's blocked sum: block b sums w[p] * g[p][k] over its pairs in pair order from
@@ -184,11 +208,20 @@ Geo pick_geo(bool soft, int rows, int n, int lanes, int rpl, bool lane_ok) {
     return best;
 }
 
-// Pairs are bucketed by geometry and by size class (the binary order of magnitude of the
-// padded DP), so a bucket's scratch stride is sized close to its own pairs.
+// Pairs are bucketed by geometry and by size class: the binary order of magnitude of the DP
+// (rows x columns), with everything up to 2^20 cells in one class.  Small pairs share a
+// launch (their scratch strides are small anyway); large pairs get a bucket per doubling, so
+// a bucket's scratch stride is sized close to its own pairs.
 int size_class(int rows, int n) {
     const double cells = double(std::max(rows, 1)) * double(std::max(n, 1));
-    return int(std::ceil(std::log2(cells)));
+    return std::max(20, int(std::ceil(std::log2(cells))));
+}
+
+// The kernel geometries (lanes per pair G, rows per lane R) each path is instantiated for.
+bool geo_available(bool soft, int G, int R) {
+    if (G == 1) return R == 8 || R == 16 || R == 24 || R == 32;
+    if (soft) return (G == 32 && (R == 2 || R == 4)) || (G == 16 && (R == 2 || R == 4)) || (G == 8 && R == 4);
+    return G == 32 && (R == 1 || R == 2 || R == 4 || R == 8);
 }
 
 struct Bucket {
@@ -197,6 +230,7 @@ struct Bucket {
     int64_t off = 0;           // into the store's order array
     int maxn = 0;
     int64_t max_soft_cells = 0;   // soft: max over pairs of nstripes * (n + G) * G * R
+    int max_rows = 0;             // soft: DP rows (m + 1) of the bucket's tallest pair
 };
 
 struct Plan {
@@ -237,7 +271,11 @@ struct nwg_store {
     bool have_scores = false, have_grads = false, have_guides = false, have_paths = false;
     int last_grad_mode = 0, last_gm = -1, last_am = -1, last_prec = 0;
     Plan hard_plan, soft_plan, band_plan;
+    // geometry per (soft, size class) chosen by the autotuner; plain: one fixed geometry
+    std::map<std::pair<int, int>, std::pair<int, int>> geo_table;
+    bool plain = false;
     int64_t scratch_budget = int64_t(24) << 30;   // bytes of soft scratch one call may hold
+    int64_t ck_threshold = int64_t(16) << 20;     // soft: forward tables above this are checkpointed
     DBuf stripe_tab;
     std::vector<int32_t> h_status;
     // timing
@@ -297,8 +335,17 @@ void build_plan(nwg_store* s, Plan& P, bool soft, int lanes, int rpl, int elem_b
     for (int64_t p = 0; p < n; ++p) {
         const int m = int(s->oa[p + 1] - s->oa[p]), nb = int(s->ob[p + 1] - s->ob[p]);
         const int rows = soft ? m + 1 : m;
+        const int sc = size_class(rows, nb);
         Geo g = band ? Geo{32, 2, true} : pick_geo(soft, std::max(rows, 1), nb, lanes, rpl, soft ? lane_ok_soft : true);
-        auto key = std::make_tuple(g.G, g.R, size_class(rows, nb));
+        if (!band && !lanes && !rpl) {
+            if (s->plain) g = Geo{32, 4};
+            else {
+                auto it = s->geo_table.find({int(soft), sc});
+                if (it != s->geo_table.end() && (!soft || it->second.first > 1 || lane_ok_soft))
+                    g = Geo{it->second.first, it->second.second};
+            }
+        }
+        auto key = std::make_tuple(g.G, g.R, sc);
         auto itb = idx.find(key);
         int bi;
         if (itb == idx.end()) { bi = int(P.buckets.size()); idx[key] = bi; P.buckets.push_back(Bucket{g, {}, 0, 0, 0}); }
@@ -324,6 +371,7 @@ void build_plan(nwg_store* s, Plan& P, bool soft, int lanes, int rpl, int elem_b
             if (soft) {
                 const int64_t st = (m + 1 + GR - 1) / GR;
                 B.max_soft_cells = std::max<int64_t>(B.max_soft_cells, st * (nb + B.geo.G) * GR);
+                B.max_rows = std::max(B.max_rows, m + 1);
             }
         }
     }
@@ -367,8 +415,8 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
     const bool band = J.band >= 0;
     Plan& P = band ? s->band_plan : s->hard_plan;
     build_plan(s, P, false, band ? 32 : J.lanes, band ? 2 : J.rows, sizeof(T), band);
-    s->codes.need(size_t(P.code_bytes));
-    if (band) s->stripe_tab.need(size_t(std::max<int64_t>(P.n_stripes, 1)) * 16);
+    s->codes.need(size_t(P.code_bytes), st);
+    if (band) s->stripe_tab.need(size_t(std::max<int64_t>(P.n_stripes, 1)) * 16, st);
     const DBuf& matT = sizeof(T) == 4 ? s->matf : s->matd;
     const DBuf& gapT = sizeof(T) == 4 ? s->gapf : s->gapd;
     const T* bx0 = nullptr;
@@ -376,8 +424,8 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
         if (sizeof(T) == 4) bx0 = reinterpret_cast<const T*>(ensure_bx0<float>(s, aff, st, s->bx0f_ok, s->bx0f, s->gapf));
         else bx0 = reinterpret_cast<const T*>(ensure_bx0<double>(s, aff, st, s->bx0d_ok, s->bx0d, s->gapd));
     }
-    s->score.need(size_t(std::max<int64_t>(s->n, 1)) * 8);
-    s->end.need(size_t(std::max<int64_t>(s->n, 1)) * 16);
+    s->score.need(size_t(std::max<int64_t>(s->n, 1)) * 8, st);
+    s->end.need(size_t(std::max<int64_t>(s->n, 1)) * 16, st);
     const int sms = sm_count(s->device);
     const size_t smem = (size_t(s->K) * s->N * s->N + 4 * size_t(s->K)) * sizeof(T);
     // scratch: the stripe boundary row per group slot
@@ -389,7 +437,7 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
         max_slots = std::max(max_slots, blocks * gpb);
         max_stride = std::max<int64_t>(max_stride, 3 * (int64_t(B.maxn) + 1));
     }
-    s->scratch.need(size_t(std::max<int64_t>(max_slots * max_stride, 1)) * sizeof(T));
+    s->scratch.need(size_t(std::max<int64_t>(max_slots * max_stride, 1)) * sizeof(T), st);
     for (auto& B : P.buckets) {
         if (B.pairs.empty()) continue;
         HardFn fn = hard_fn_rt<T>(aff, loc, tr, B.geo);
@@ -419,10 +467,10 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
     }
     // traceback: gradient, guide, path
     if (want_grad) {
-        s->grad.need(size_t(s->n) * s->gstride * 8 + 8);
+        s->grad.need(size_t(s->n) * s->gstride * 8 + 8, st);
         NWG_CUDA(cudaMemsetAsync(s->grad.p, 0, size_t(s->n) * s->gstride * 8, st));
     }
-    if (want_guide) s->guide.need(size_t(s->total_a + s->n) * 4 + 4);
+    if (want_guide) s->guide.need(size_t(s->total_a + s->n) * 4 + 4, st);
     const bool keep = J.keep_paths != 0;
     if (keep) {
         std::vector<int64_t> mo(s->n + 1, 0);
@@ -503,8 +551,8 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
     while (pw * 2 <= std::min(renorm, sizeof(T) == 4 ? 8 : 16)) pw *= 2;
     renorm = pw;
     DBuf dw, dgw;   // small; freed at scope end
-    struct Free { DBuf& a; DBuf& b; ~Free() { a.release(); b.release(); } } fr{dw, dgw};
-    dw.need(w.size() * sizeof(T)); dgw.need(gw.size() * sizeof(T));
+    struct Free { DBuf& a; DBuf& b; cudaStream_t st; ~Free() { a.release(st); b.release(st); } } fr{dw, dgw, st};
+    dw.need(w.size() * sizeof(T), st); dgw.need(gw.size() * sizeof(T), st);
     NWG_CUDA(cudaMemcpyAsync(dw.p, w.data(), w.size() * sizeof(T), cudaMemcpyHostToDevice, st));
     NWG_CUDA(cudaMemcpyAsync(dgw.p, gw.data(), gw.size() * sizeof(T), cudaMemcpyHostToDevice, st));
     Plan local_plan;
@@ -534,6 +582,7 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
                 const int GR = B.geo.G * B.geo.R;
                 const int64_t stp = (m + 1 + GR - 1) / GR;
                 B.max_soft_cells = std::max<int64_t>(B.max_soft_cells, stp * (nb + B.geo.G) * GR);
+                B.max_rows = std::max(B.max_rows, m + 1);
             }
         }
     } else {
@@ -541,10 +590,10 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
         build_plan(s, *P, true, J.lanes, J.rows, sizeof(T));
     }
     DBuf sub_order;
-    struct Free1 { DBuf& a; ~Free1() { a.release(); } } fr1{sub_order};
+    struct Free1 { DBuf& a; cudaStream_t st; ~Free1() { a.release(st); } } fr1{sub_order, st};
     const int32_t* d_order = P->order.as<int32_t>();
     if (subset) {
-        sub_order.need(order.size() * 4 + 4);
+        sub_order.need(order.size() * 4 + 4, st);
         NWG_CUDA(cudaMemcpyAsync(sub_order.p, order.data(), order.size() * 4, cudaMemcpyHostToDevice, st));
         d_order = sub_order.as<int32_t>();
     }
@@ -569,15 +618,23 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
         occ = std::max(occ, 1);
         const int gpb = block / G;
         const int64_t items = int64_t(B.pairs.size());
-        const int64_t fwd_bytes = ((B.max_soft_cells * NV * int64_t(sizeof(T))) + 255) & ~int64_t(255);
-        const int64_t exp_bytes = ((B.max_soft_cells / B.geo.R) * 4 + 255) & ~int64_t(255);
-        const int64_t bnd_bytes = (int64_t(B.maxn) + 1) * (2 * NV * int64_t(sizeof(T)) + 8);
+        // checkpointed when a pair's whole forward table would be large: only stripe
+        // boundaries are kept, each stripe's table is recomputed just before its backward
+        const int64_t GRb = int64_t(G) * B.geo.R;
+        const int64_t nb1 = int64_t(B.maxn) + 1;
+        const int64_t max_stripes = (B.max_rows + GRb - 1) / GRb;
+        const bool ck = B.max_soft_cells * NV * int64_t(sizeof(T)) > s->ck_threshold;
+        const int64_t tab_cells = ck ? (nb1 + G) * GRb : B.max_soft_cells;
+        const int64_t fwd_bytes = ((tab_cells * NV * int64_t(sizeof(T))) + 255) & ~int64_t(255);
+        const int64_t exp_bytes = ((tab_cells / B.geo.R) * 4 + 255) & ~int64_t(255);
+        const int64_t nbrows = ck ? max_stripes : 1;
+        const int64_t bnd_bytes = nb1 * (nbrows + 1) * (NV * int64_t(sizeof(T)) + 4);
         const int64_t stride = ((fwd_bytes + exp_bytes + bnd_bytes) + 255) & ~int64_t(255);
         // as many resident groups as fit the device (occupancy) and the scratch budget
         int64_t blocks = std::min<int64_t>((items + gpb - 1) / gpb, int64_t(sms) * occ);
         blocks = std::max<int64_t>(1, std::min<int64_t>(blocks, s->scratch_budget / std::max<int64_t>(1, stride * gpb)));
         const int64_t slots = blocks * gpb;
-        s->scratch.need(size_t(slots * stride));
+        s->scratch.need(size_t(slots * stride), st);
         nwg::SoftArgs A{};
         A.a = s->a.as<uint8_t>(); A.oa = s->doa.as<int64_t>();
         A.b = s->b.as<uint8_t>(); A.ob = s->dob.as<int64_t>();
@@ -587,6 +644,7 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
         A.w = dw.p; A.gw = dgw.p; A.N = N; A.K = K;
         A.scratch = s->scratch.p; A.scratch_stride = stride; A.fwd_bytes = fwd_bytes;
         A.maxn = B.maxn; A.temperature = J.temperature;
+        A.ck = ck; A.max_stripes = int(std::max<int64_t>(max_stripes, 1)); A.bnd_off = fwd_bytes + exp_bytes;
         A.renorm_mask = renorm - 1;
         A.score = s->score.as<double>(); A.grad = s->grad.as<double>(); A.gstride = s->gstride;
         A.status = s->status.as<int32_t>();
@@ -604,9 +662,9 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
 }
 
 void run_soft(nwg_store* s, const nwg_job& J, cudaStream_t st) {
-    s->score.need(size_t(std::max<int64_t>(s->n, 1)) * 8);
-    s->grad.need(size_t(s->n) * s->gstride * 8 + 8);
-    s->status.need(size_t(std::max<int64_t>(s->n, 1)) * 4);
+    s->score.need(size_t(std::max<int64_t>(s->n, 1)) * 8, st);
+    s->grad.need(size_t(s->n) * s->gstride * 8 + 8, st);
+    s->status.need(size_t(std::max<int64_t>(s->n, 1)) * 4, st);
     NWG_CUDA(cudaMemsetAsync(s->status.p, 0, size_t(std::max<int64_t>(s->n, 1)) * 4, st));
     const bool f32 = J.precision == 32 && !J.soft_double;
     if (f32) soft_pass<float>(s, J, st, nullptr);
@@ -680,12 +738,12 @@ void load_pairs(nwg_store* s, const uint8_t* codes_a, const int64_t* off_a, cons
         if (codes_a[a0 + k] >= nalpha) throw Error(NWG_EINVAL, "code out of range in sequence A");
     for (int64_t k = 0; k < s->total_b; ++k)
         if (codes_b[b0 + k] >= nalpha) throw Error(NWG_EINVAL, "code out of range in sequence B");
-    s->a.need(size_t(s->total_a) + 16);
-    s->b.need(size_t(s->total_b) + 16);
+    s->a.need(size_t(s->total_a) + 16, st);
+    s->b.need(size_t(s->total_b) + 16, st);
     if (s->total_a) NWG_CUDA(cudaMemcpyAsync(s->a.p, codes_a + a0, size_t(s->total_a), cudaMemcpyHostToDevice, st));
     if (s->total_b) NWG_CUDA(cudaMemcpyAsync(s->b.p, codes_b + b0, size_t(s->total_b), cudaMemcpyHostToDevice, st));
-    s->doa.need(size_t(n_pairs + 1) * 8);
-    s->dob.need(size_t(n_pairs + 1) * 8);
+    s->doa.need(size_t(n_pairs + 1) * 8, st);
+    s->dob.need(size_t(n_pairs + 1) * 8, st);
     NWG_CUDA(cudaMemcpyAsync(s->doa.p, s->oa.data(), size_t(n_pairs + 1) * 8, cudaMemcpyHostToDevice, st));
     NWG_CUDA(cudaMemcpyAsync(s->dob.p, s->ob.data(), size_t(n_pairs + 1) * 8, cudaMemcpyHostToDevice, st));
     s->tracked_seq = false;
@@ -732,6 +790,7 @@ int nwg_store_create(const uint8_t* codes_a, const int64_t* off_a, const uint8_t
         s->device = device;
         NWG_CUDA(cudaSetDevice(device));
         s->nalpha = nalpha;
+        keep_pool(device);
         NWG_CUDA(cudaEventCreate(&s->ev0));
         NWG_CUDA(cudaEventCreate(&s->ev1));
         load_pairs(s.get(), codes_a, off_a, codes_b, off_b, n_pairs, tracks, gap_tracks, nullptr);
@@ -857,6 +916,29 @@ int nwg_resolve_guides(nwg_store* s, const double* mats, const double* gaps, con
         } catch (...) { restore(); throw; }
         restore();
         s->have_guides = true;
+    });
+}
+
+int nwg_set_geometry(nwg_store* s, int soft, int size_class_, int lanes, int rows) {
+    return guarded([&] {
+        if (!s) throw Error(NWG_EINVAL, "null store");
+        if (size_class_ < 0) {   // -1: forget every tuned geometry; -2: the plain fill
+            s->geo_table.clear();
+            s->plain = size_class_ == -2;
+        } else {
+            if (!geo_available(soft != 0, lanes, rows)) throw Error(NWG_EINVAL, "no kernel for this geometry");
+            s->geo_table[{soft ? 1 : 0, size_class_}] = {lanes, rows};
+            s->plain = false;
+        }
+        s->hard_plan.reset(); s->soft_plan.reset();
+    });
+}
+
+int nwg_set_memory(nwg_store* s, int64_t scratch_budget_bytes, int64_t checkpoint_bytes) {
+    return guarded([&] {
+        if (!s) throw Error(NWG_EINVAL, "null store");
+        if (scratch_budget_bytes >= 0) s->scratch_budget = std::max<int64_t>(scratch_budget_bytes, 1);
+        if (checkpoint_bytes >= 0) s->ck_threshold = checkpoint_bytes;
     });
 }
 

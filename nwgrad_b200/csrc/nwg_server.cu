@@ -62,6 +62,7 @@ struct nwg_server {
     nwg_job job{};
     int nalpha = 0;
     int64_t budget = 0;            // bytes of device memory the in-flight batches may hold
+    int64_t scratch_share = 0;     // soft: bytes of forward tables one worker's batch may hold
     int64_t max_batch_pairs = 0;
     std::shared_ptr<const Params> params;
     std::mutex mu;
@@ -90,7 +91,9 @@ double request_bytes(const nwg_job& J, const std::vector<int64_t>& oa, const std
     for (int64_t p = 0; p < n; ++p) {
         const double m = double(oa[p + 1] - oa[p]), nn = double(ob[p + 1] - ob[p]);
         b += m + nn + 64 + 8.0 * (double(K) * N * N + 4 * K) + 4 * (m + 1);
-        b += J.grad_mode == 2 ? 16.0 * (m + 64) * (nn + 40) / 64.0 : 1.2 * (m + 64) * (nn + 40);
+        // hard: the code table (1 byte a cell); soft: the forward tables live in the worker's
+        // scratch, which has its own cap (the budget's share of one worker)
+        if (J.grad_mode != 2) b += 1.2 * (m + 64) * (nn + 40);
     }
     return b;
 }
@@ -120,6 +123,7 @@ void run_batch(nwg_server* S, nwg_store*& store, cudaStream_t st, std::vector<st
     if (!store) {
         if (!ck(nwg_store_create(a.data(), oa.data(), b.data(), ob.data(), n, S->nalpha, nullptr, nullptr, S->device, &store)))
             store = nullptr;
+        else ck(nwg_set_memory(store, S->scratch_share, -1));
     } else {
         ck(nwg_store_load(store, a.data(), oa.data(), b.data(), ob.data(), n, nullptr, nullptr, st));
     }
@@ -218,6 +222,8 @@ int nwg_server_create(int device, const nwg_job* job, int nalpha, const double* 
         S->nalpha = nalpha;
         S->budget = hbm_budget_bytes > 0 ? hbm_budget_bytes : (int64_t(32) << 30);
         S->max_batch_pairs = max_batch_pairs > 0 ? max_batch_pairs : 65536;
+        // half the budget for the workers' forward tables, the rest for the batches themselves
+        S->scratch_share = std::max<int64_t>(S->budget / (2 * int64_t(workers)), int64_t(64) << 20);
         auto P = std::make_shared<Params>();
         P->K = K; P->N = nalpha;
         P->mats.assign(mats, mats + size_t(K) * nalpha * nalpha);

@@ -18,7 +18,10 @@
 // between: growth per step is at most 3 * the largest weight); values crossing lanes are
 // converted by exact power-of-two factors.  The forward values of every cell (3 per cell,
 // scaled, plus one exponent per lane step) go to a per-group scratch table that the backward
-// pass reads in reverse.  A value that overflows or turns NaN marks the pair refused; the
+// pass reads in reverse.  Checkpointed (long pairs): the forward pass keeps only each
+// stripe's bottom row; the backward pass recomputes one stripe's table from the row above it
+// just before it walks that stripe, so the table holds one stripe (twice the forward work,
+// a table ~nstripes times smaller).  A value that overflows or turns NaN marks the pair refused; the
 // host reruns refused pairs in double precision.
 //
 // Accumulation: each lane keeps its rows' substitution counts in shared memory, laid out
@@ -43,6 +46,11 @@ struct SoftArgs {
     void* scratch; int64_t scratch_stride;   // bytes per group slot
     int64_t fwd_bytes;                       // bytes of the forward table within a slot
     int maxn;                                // columns (n) the boundary rows are sized for
+    int ck;                                  // checkpointed: keep every stripe's bottom row in the
+                                             // forward pass, recompute a stripe's table before its
+                                             // backward (the table then holds one stripe)
+    int max_stripes;                         // ck: stripes the boundary rows are sized for
+    int64_t bnd_off;                         // bytes from a slot's start to its boundary rows
     int renorm_mask;                         // renormalise when (step & renorm_mask) == 0
     double temperature;
     double* score; double* grad; int64_t gstride;
@@ -159,11 +167,13 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
     T* fwd = reinterpret_cast<T*>(sbase);
     int* fexp = reinterpret_cast<int*>(sbase + A.fwd_bytes);
     const int64_t nb = int64_t(A.maxn) + 1;
-    unsigned char* bb = sbase + A.scratch_stride - nb * (2 * NV * sizeof(T) + 2 * sizeof(int));
-    T* fbnd = reinterpret_cast<T*>(bb);
-    T* bbnd = fbnd + NV * nb;
-    int* fbndE = reinterpret_cast<int*>(bbnd + NV * nb);
-    int* bbndE = fbndE + nb;
+    const bool ck = A.ck != 0;
+    const int nbrows = ck ? A.max_stripes : 1;              // forward boundary rows kept
+    unsigned char* bb = sbase + A.bnd_off;
+    T* fbnd = reinterpret_cast<T*>(bb);                      // [nbrows][NV * nb]
+    T* bbnd = fbnd + NV * nb * nbrows;                       // [NV * nb]
+    int* fbndE = reinterpret_cast<int*>(bbnd + NV * nb);     // [nbrows][nb]
+    int* bbndE = fbndE + nb * nbrows;                        // [nb]
     // untracked: the one set's gap weights
     const T oa0 = sgw[0], ea0 = sgw[1], ob0 = sgw[2], eb0 = sgw[3];
 
@@ -189,8 +199,16 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
         // ── forward ──────────────────────────────────────────────────────────
         XAcc zacc; zacc.init();                 // Local: the sum over every cell
         T zM = T(0), zX = T(0), zY = T(0); int zE = 0;   // Global: (m, n)
-        for (int s = 0; s < nstripes; ++s) {
+        // One stripe of the forward pass.  pass1: the first pass (Z, boundary rows; the table
+        // too unless checkpointed); else the recompute of a checkpointed stripe's table, which
+        // repeats the first pass's arithmetic from the same boundary row: the same bits.
+        auto fwd_stripe = [&](const int s, const bool pass1) {
             const int i0 = s * GR + lane * R;   // this lane's first DP row (rows 0..m)
+            const bool store_table = !ck || !pass1;
+            T* const fb_in = fbnd + (ck ? int64_t(s - 1) * NV * nb : 0);
+            int* const fbE_in = fbndE + (ck ? int64_t(s - 1) * nb : 0);
+            T* const fb_out = fbnd + (ck ? int64_t(s) * NV * nb : 0);
+            int* const fbE_out = fbndE + (ck ? int64_t(s) * nb : 0);
             int key[R];
             T roa[TR ? R : 1], rea[TR ? R : 1], rob[TR ? R : 1], reb[TR ? R : 1];
             T vmask[R];
@@ -214,13 +232,13 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
             T zpart = T(0);                       // Local: the cells' sum since the last renorm
             T dgM = T(0), dgX = T(0), dgY = T(0); // row above, column j-1
             T upM = T(0), upX = T(0), upY = T(0); // row above, column j
-            T* fs = fwd + int64_t(s) * S * G * CV;
-            int* fe = fexp + int64_t(s) * S * G;
+            T* fs = fwd + (ck ? 0 : int64_t(s) * S * G * CV);
+            int* fe = fexp + (ck ? 0 : int64_t(s) * S * G);
             int nbj = N;
             for (int t = 0; t < S; ++t) {
                 const int j = t - lane;           // column 0..n
                 if (lane == 0 && j <= n && s > 0) {
-                    const int eb = fbndE[j];
+                    const int eb = fbE_in[j];
                     int d = eb - E;
                     if (d > kLift) {   // keep the incoming values in range: move own state down
                         const T f = pow2i<T>(kLift - d);
@@ -230,8 +248,8 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
                         E = eb - kLift; lone = pow2i<T>(-E); d = kLift;
                     }
                     const T f = pow2i<T>(d);
-                    upM = fbnd[NV * j] * f;
-                    if constexpr (AFF) { upX = fbnd[NV * j + 1] * f; upY = fbnd[NV * j + 2] * f; }
+                    upM = fb_in[NV * j] * f;
+                    if constexpr (AFF) { upX = fb_in[NV * j + 1] * f; upY = fb_in[NV * j + 2] * f; }
                 }
                 const bool active = (j >= 0) && (j <= n);
                 if (active) {
@@ -281,7 +299,7 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
                         else if (mx > T(0)) {
                             int e = ilog2(mx);
                             if (e < -120) e = -120;
-                            if (LOC) zacc.add(static_cast<double>(zpart), E);
+                            if (LOC && pass1) zacc.add(static_cast<double>(zpart), E);
                             zpart = T(0);
                             if (e != 0) {
                                 const T f = pow2i<T>(-e);
@@ -293,14 +311,16 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
                         }
                     }
                     // store the column for the backward pass
-                    T v[CV];
+                    if (store_table) {
+                        T v[CV];
 #pragma unroll
-                    for (int r = 0; r < R; ++r) {
-                        v[NV * r] = cM[r];
-                        if constexpr (AFF) { v[NV * r + 1] = cX[r]; v[NV * r + 2] = cY[r]; }
+                        for (int r = 0; r < R; ++r) {
+                            v[NV * r] = cM[r];
+                            if constexpr (AFF) { v[NV * r + 1] = cX[r]; v[NV * r + 2] = cY[r]; }
+                        }
+                        vstore<T, CV>(fs + (int64_t(t) * G + lane) * CV, v);
+                        fe[int64_t(t) * G + lane] = E;
                     }
-                    vstore<T, CV>(fs + (int64_t(t) * G + lane) * CV, v);
-                    fe[int64_t(t) * G + lane] = E;
                 }
                 if constexpr (G > 1) {
                     const T sM = __shfl_up_sync(gmask, cM[R - 1], 1, G);
@@ -323,22 +343,25 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
                         upM = sM * f; upX = sX * f; upY = sY * f;
                     }
                 }
-                if (lane == G - 1 && active && s + 1 < nstripes) {
-                    fbnd[NV * j] = cM[R - 1];
-                    if constexpr (AFF) { fbnd[NV * j + 1] = cX[R - 1]; fbnd[NV * j + 2] = cY[R - 1]; }
-                    fbndE[j] = E;
+                if (pass1 && lane == G - 1 && active && s + 1 < nstripes) {
+                    fb_out[NV * j] = cM[R - 1];
+                    if constexpr (AFF) { fb_out[NV * j + 1] = cX[R - 1]; fb_out[NV * j + 2] = cY[R - 1]; }
+                    fbE_out[j] = E;
                 }
             }
-            if constexpr (LOC) { zacc.add(static_cast<double>(zpart), E); }
-            if constexpr (!LOC) {
-                if (m >= i0 && m < i0 + R) {
+            if (pass1) {
+                if constexpr (LOC) { zacc.add(static_cast<double>(zpart), E); }
+                if constexpr (!LOC) {
+                    if (m >= i0 && m < i0 + R) {
 #pragma unroll
-                    for (int r = 0; r < R; ++r)
-                        if (i0 + r == m) { zM = cM[r]; zX = cX[r]; zY = cY[r]; zE = E; }
+                        for (int r = 0; r < R; ++r)
+                            if (i0 + r == m) { zM = cM[r]; zX = cX[r]; zY = cY[r]; zE = E; }
+                    }
                 }
             }
             if constexpr (G > 1) __syncwarp(gmask);
-        }
+        };
+        for (int s = 0; s < nstripes; ++s) fwd_stripe(s, true);
         // Z = zhat * 2^EZ with zhat in [1, 2)
         double zm; int ze;
         if constexpr (LOC) {
@@ -377,6 +400,7 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
             for (int k = 0; k < K * N * N; ++k) g1[k] = 0.0;
         }
         for (int s = nstripes - 1; s >= 0; --s) {
+            if (ck) fwd_stripe(s, false);       // this stripe's forward table, from its checkpoint
             const int i0 = s * GR + lane * R;
             int keyd[R], krow[R];
             T roa[TR ? R : 1], rea[TR ? R : 1], rob[TR ? R : 1], reb[TR ? R : 1];   // rob/reb: row i+1
@@ -404,8 +428,8 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
             T lone = T(1);
             T dgM = T(0);                             // row below, column j+1 (BM only)
             T dnM = T(0), dnX = T(0), dnY = T(0);     // row below, column j
-            const T* fs = fwd + int64_t(s) * S * G * CV;
-            const int* fe = fexp + int64_t(s) * S * G;
+            const T* fs = fwd + (ck ? 0 : int64_t(s) * S * G * CV);
+            const int* fe = fexp + (ck ? 0 : int64_t(s) * S * G);
             T nf[CV];
             int nEF = 0, nbj = N;
             bool have_next = false;

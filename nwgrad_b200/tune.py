@@ -1,0 +1,188 @@
+"""Autotuner: the fastest kernel geometry per size class of a batch, measured on the device.
+
+A geometry is (lanes per pair, DP rows per lane): one lane per pair (the inter-pair fill), a
+quarter, half or whole warp per pair, with 2 to 32 rows per lane.  Every geometry computes
+the same cells, so results do not change; speed does, through padding (rows rounded up to
+whole stripes), skew (the wavefront's ramp), parallelism and shared memory per group.
+
+Pairs are grouped in size classes: max(20, ceil(log2(rows * columns))), the same rule as the
+library's planner (so every pair up to 2^20 cells is one class).  For each class in a batch
+the tuner aligns a sample of the class's own pairs with every candidate geometry, times the
+device work (``SeqPairBatch.last_timing``), keeps the fastest and stores the choice in a JSON
+cache keyed by device, problem type and class.  ``apply`` hands the table to the library
+(``nwg_set_geometry``); ``plain`` selects the plain fill instead (one fixed geometry, 32
+lanes x 4 rows, for every pair).
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+
+import numpy as np
+
+HARD_GEOS = [(32, 4), (32, 2), (32, 1), (32, 8), (1, 8), (1, 16), (1, 24), (1, 32)]
+SOFT_GEOS = [(32, 4), (32, 2), (16, 4), (16, 2), (8, 4), (1, 8), (1, 16), (1, 24), (1, 32)]
+
+
+def size_class(rows: int, cols: int) -> int:
+    return max(20, int(math.ceil(math.log2(max(rows, 1) * max(cols, 1)))))
+
+
+def _cache_path() -> str:
+    p = os.environ.get("NWGRAD_B200_TUNE_CACHE")
+    if p:
+        return p
+    return os.path.join(os.path.expanduser("~"), ".cache", "nwgrad_b200", "tune.json")
+
+
+def _load_cache() -> dict:
+    try:
+        with open(_cache_path()) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def _save_cache(c: dict) -> None:
+    path = _cache_path()
+    try:
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        tmp = path + f".{os.getpid()}.tmp"
+        with open(tmp, "w") as f:
+            json.dump(c, f, indent=1, sort_keys=True)
+        os.replace(tmp, path)
+    except OSError:
+        pass
+
+
+def _device_name(dev: int) -> str:
+    try:
+        import torch
+        return torch.cuda.get_device_name(dev)
+    except Exception:   # noqa: BLE001 - the name only keys the cache
+        return f"cuda:{dev}"
+
+
+def _soft(batch) -> bool:
+    return batch._grad_mode == "soft"
+
+
+def _classes(batch) -> dict:
+    """size class -> indices of the batch's pairs in it."""
+    m = np.diff(batch._oa).astype(np.int64)
+    n = np.diff(batch._ob).astype(np.int64)
+    rows = m + 1 if _soft(batch) else m
+    cells = np.maximum(rows, 1).astype(np.float64) * np.maximum(n, 1).astype(np.float64)
+    sc = np.maximum(20, np.ceil(np.log2(cells))).astype(np.int64)
+    return {int(c): np.nonzero(sc == c)[0] for c in np.unique(sc)}
+
+
+def _codes(batch):
+    """Concatenated codes of both sides (the batch's own encoding)."""
+    if getattr(batch, "_codes", None) is not None:
+        return batch._codes
+    from .batch import _encode_all
+    a, _, _ = _encode_all(batch._alpha, batch._seqs_a, "A")
+    b, _, _ = _encode_all(batch._alpha, batch._seqs_b, "B")
+    return a, b
+
+
+def _subset(batch, idx, codes):
+    """A batch of the same type over the pairs idx (tracks carried along)."""
+    a, b = codes
+    oa, ob = batch._oa, batch._ob
+    la = (oa[idx + 1] - oa[idx]).astype(np.int64)
+    lb = (ob[idx + 1] - ob[idx]).astype(np.int64)
+    sa = np.concatenate([a[oa[p]:oa[p + 1]] for p in idx]) if la.sum() else np.zeros(0, np.uint8)
+    sb = np.concatenate([b[ob[p]:ob[p + 1]] for p in idx]) if lb.sum() else np.zeros(0, np.uint8)
+    noa = np.zeros(len(idx) + 1, np.int64); np.cumsum(la, out=noa[1:])
+    nob = np.zeros(len(idx) + 1, np.int64); np.cumsum(lb, out=nob[1:])
+    kw = dict(gap_model=batch._gap_model, mode=batch._mode, grad_mode=batch._grad_mode, device=batch._device)
+    if batch._flat_t is not None:
+        kw["tracks"] = np.concatenate([batch._flat_t[oa[p]:oa[p + 1]] for p in idx])
+    if batch._flat_g is not None:
+        kw["gap_tracks"] = np.concatenate([batch._flat_g[oa[p] + p:oa[p + 1] + p + 1] for p in idx])
+    sub = type(batch).from_codes(sa, noa, sb, nob, batch._params, **kw)
+    sub.soft_temperature = batch.soft_temperature
+    sub.soft_precision = batch.soft_precision
+    return sub, float(np.sum(la.astype(np.float64) * lb.astype(np.float64)))
+
+
+def _candidates(batch):
+    K, N = batch._params.num_sets, batch._alpha.size
+    elem = 4 if batch._precision == 32 else 8
+    if _soft(batch):
+        lane_ok = K * N * N * elem * 32 <= 48 * 1024
+        return [g for g in SOFT_GEOS if g[0] > 1 or lane_ok]
+    return list(HARD_GEOS)
+
+
+def _key(batch, sc: int) -> str:
+    return "|".join(str(x) for x in (_device_name(batch._device), "soft" if _soft(batch) else "hard",
+                                     batch._gap_model, batch._mode, batch._precision, batch._alpha.size,
+                                     batch._params.num_sets, int(batch._tracked), sc))
+
+
+def tune(batch, sample_pairs: int = 8192, force: bool = False, verbose: bool = False, reps: int = 2) -> dict:
+    """{size class: (lanes, rows)} for the classes of ``batch``, measured (or from the cache)."""
+    grad = {"none": 0, "hard": 1, "soft": 2}[batch._grad_mode]
+    cache = _load_cache()
+    table = {}
+    codes = None
+    dirty = False
+    for sc, idx in sorted(_classes(batch).items()):
+        key = _key(batch, sc)
+        if not force and key in cache:
+            table[sc] = tuple(cache[key]["geo"])
+            continue
+        if codes is None:
+            codes = _codes(batch)
+        if idx.size > sample_pairs:   # evenly spread over the class
+            idx = idx[np.linspace(0, idx.size - 1, sample_pairs).astype(np.int64)]
+        sub, cells = _subset(batch, idx, codes)
+        best, best_ms, times = None, float("inf"), {}
+        for geo in _candidates(batch):
+            sub._tune = geo
+            try:
+                sub._run(grad)                      # warm: plan, first launch
+                ms = min(_timed(sub, grad) for _ in range(reps))
+            except (ValueError, RuntimeError):
+                continue
+            times[f"{geo[0]}x{geo[1]}"] = ms
+            if ms < best_ms:
+                best, best_ms = geo, ms
+        del sub
+        if best is None:
+            continue
+        table[sc] = best
+        cache[key] = {"geo": list(best), "gcups": cells / (best_ms / 1e3) / 1e9 if best_ms > 0 else None,
+                      "ms": times, "sample_pairs": int(idx.size)}
+        dirty = True
+        if verbose:
+            print(f"size class 2^{sc}: {idx.size} pairs, best {best[0]} lanes x {best[1]} rows "
+                  f"({best_ms:.3f} ms); " + ", ".join(f"{k} {v:.3f}" for k, v in times.items()))
+    if dirty:
+        _save_cache(cache)
+    return table
+
+
+def _timed(sub, grad) -> float:
+    sub._run(grad)
+    return sub.last_timing()[0]
+
+
+def apply(batch, table: dict) -> None:
+    """Use the table's geometries for the batch's later runs."""
+    from ._capi import check
+    L = batch._store._L
+    check(L.nwg_set_geometry(batch._store.h, 0, -1, 0, 0))
+    soft = 1 if _soft(batch) else 0
+    for sc, (lanes, rows) in table.items():
+        check(L.nwg_set_geometry(batch._store.h, soft, int(sc), int(lanes), int(rows)))
+
+
+def plain(batch) -> None:
+    """The plain fill: one fixed geometry for every pair."""
+    from ._capi import check
+    check(batch._store._L.nwg_set_geometry(batch._store.h, 0, -2, 0, 0))

@@ -219,3 +219,83 @@ def test_golden_reference_batches(name):
                 ref = z[key + "grads"]
                 scale = np.maximum(np.abs(ref).max(axis=1, keepdims=True), 1.0)
                 assert (np.abs(flat - ref) / scale).max() <= SOFT_RTOL
+
+
+@pytest.mark.parametrize("gm", [0, 1])
+@pytest.mark.parametrize("am", [0, 1])
+@pytest.mark.parametrize("geo", [(1, 8), (32, 2), (32, 4), (16, 4), (8, 4)])
+def test_soft_checkpointed(gm, am, geo):
+    """Stripe checkpoints (each stripe's forward recomputed before its backward) give the same
+    bits as the whole-table pass, and both agree with the oracle."""
+    rng = np.random.default_rng(1300 + gm + 2 * am + geo[1] + geo[0])
+    mat, gaps, sa, sb, tr, gt = _problem(rng, AA, 24, 1, 90, homolog=True)
+    sa += rand_seqs(rng, 3, 200, 420, AA) + ["", "W"]
+    sb += [mutate(rng, s, AA) for s in sa[-5:-2]] + ["MK", ""]
+    alpha = AA
+    if geo[0] == 1:   # one lane per pair keeps a per-lane histogram: a small alphabet
+        alpha = "ACGT"
+        mat, gaps, sa, sb, tr, gt = _problem(rng, alpha, 24, 1, 90, homolog=True)
+        sa += rand_seqs(rng, 3, 200, 420, alpha)
+        sb += [mutate(rng, s, alpha) for s in sa[-3:]]
+    out = []
+    for ckb in (-1, 0):
+        b = nw.SeqPairBatch(sa, sb, _params(alpha, mat, gaps), gap_model=("linear", "affine")[gm],
+                            mode=("global", "local")[am], grad_mode="soft")
+        b._tune = geo
+        b.set_memory(checkpoint_bytes=ckb)
+        b.score_and_grad()
+        gmat, ggap = b.grads()
+        out.append((b.scores(), gmat.copy(), ggap.copy()))
+    for x, y in zip(out[0], out[1]):
+        assert np.array_equal(x, y)
+    enc = oracle.Encoded(encode(alpha, sa), encode(alpha, sb))
+    so, go = oracle.soft(gm, am, mat, gaps, enc)
+    np.testing.assert_allclose(out[1][0], so, rtol=SOFT_RTOL, atol=1e-5)
+    flat = np.concatenate([out[1][1].reshape(len(sa), -1), out[1][2].reshape(len(sa), -1)], axis=1)
+    scale = np.maximum(np.abs(go).max(axis=1, keepdims=True), 1.0)
+    assert (np.abs(flat - go) / scale).max() <= SOFT_RTOL
+
+
+def test_soft_small_scratch_budget():
+    """A scratch budget of one table runs the pairs a few at a time, with the same bits."""
+    rng = np.random.default_rng(1400)
+    mat, gaps, sa, sb, tr, gt = _problem(rng, AA, 300, 10, 120, homolog=True)
+    res = []
+    for budget in (-1, 1):
+        b = nw.SeqPairBatch(sa, sb, _params(AA, mat, gaps), grad_mode="soft")
+        b.set_memory(scratch_budget_bytes=budget)
+        b.score_and_grad()
+        res.append((b.scores(), b.compute_grad()))
+    assert np.array_equal(res[0][0], res[1][0])
+    assert np.array_equal(res[0][1].matrices, res[1][1].matrices)
+    assert np.array_equal(res[0][1].gaps, res[1][1].gaps)
+
+
+@pytest.mark.parametrize("grad_mode", ["hard", "soft"])
+def test_autotuned_and_plain_fill_same_results(grad_mode, tmp_path, monkeypatch):
+    """The autotuned geometries and the plain fill compute the same results as the planner's."""
+    monkeypatch.setenv("NWGRAD_B200_TUNE_CACHE", str(tmp_path / "tune.json"))
+    rng = np.random.default_rng(1500)
+    mat, gaps, sa, sb, tr, gt = _problem(rng, AA, 200, 5, 400, homolog=True)
+    sa += rand_seqs(rng, 4, 1100, 1500, AA)
+    sb += [mutate(rng, s, AA) for s in sa[-4:]]
+    res = []
+    for how in ("planner", "tuned", "plain"):
+        b = nw.SeqPairBatch(sa, sb, _params(AA, mat, gaps), grad_mode=grad_mode)
+        if how == "tuned":
+            table = b.autotune(sample_pairs=64)
+            assert table and all(isinstance(v, tuple) for v in table.values())
+        elif how == "plain":
+            b.use_plain_fill()
+        b.score_and_grad()
+        gmat, ggap = b.grads()
+        res.append((b.scores(), gmat.copy(), ggap.copy()))
+    for other in res[1:]:
+        if grad_mode == "hard":
+            for x, y in zip(res[0], other):
+                assert np.array_equal(x, y)
+        else:
+            np.testing.assert_allclose(other[0], res[0][0], rtol=1e-6, atol=1e-6)
+            for x, y in zip(res[0][1:], other[1:]):
+                scale = max(1.0, float(np.abs(x).max()))
+                assert np.abs(x - y).max() <= 1e-5 * scale
