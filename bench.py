@@ -407,10 +407,8 @@ def main():
     def allreduce(g):
         if dist is None:
             return g
-        t = torch.tensor(np.concatenate([g.matrices.ravel(), g.gaps.ravel()]), dtype=torch.float64,
-                         device=f"cuda:{local}")
-        dist.all_reduce(t)
-        return g
+        from nwgrad_b200.replicas import allreduce_grad
+        return allreduce_grad(g, device=torch.device("cuda", local))
 
     def timed(sample_clocks):
         for _ in range(max(args.warmup, 3)):

@@ -168,6 +168,7 @@ class SeqPairBatch:
         self.schedule = "dynamic"
         self.track_storage = "paths"
         self._tune = (0, 0)     # (lanes per pair, rows per lane): 0 = the planner's choice
+        self._run_id = 0        # counts device runs (the autograd binding checks it)
         self._store = None
         self._n = 0
         self._params = None
@@ -280,6 +281,7 @@ class SeqPairBatch:
         if self._store is None:
             return 0.0
         job = self._job(grad_mode, band, keep_paths)
+        self._run_id += 1
         tot = C.c_double(0.0)
         check(self._store._L.nwg_run(self._store.h, C.byref(job), stream, C.byref(tot)))
         return float(tot.value)

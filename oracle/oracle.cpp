@@ -16,6 +16,8 @@
 //   soft (log space) forward/backward ...... aligner.hpp:6231-6330 (linear), 6362-6524 (affine)
 //   soft temperature: theta/T, log Z * T ... aligner.hpp:6594-6626
 //   blocked weighted sum of gradients ...... batch_engine.hpp:1788-1827
+//   Hirschberg (exact and prefix-max carry)  aligner.hpp:4151-4560 (hb_fwd, hb_rev, hb_base,
+//                                            hb_solve, score replay), 5191-5249 (grad, guide)
 //
 // Arithmetic follows the reference expression for expression (same association, same
 // >= tie-breaks, parameters cast to T once), compiled with -ffp-contract=off, so hard
@@ -152,6 +154,7 @@ struct HardOut {
     int32_t* guide = nullptr;    // m+1
     uint8_t* moves = nullptr;    // walk order (end -> start): 0 M, 1 X (gap in B), 2 Y (gap in A)
     int64_t nmoves = 0;
+    int64_t moves_cap = 0;       // Hirschberg: bytes of moves
     int32_t end_i = 0, end_j = 0, start_i = 0, start_j = 0;
 };
 
@@ -763,6 +766,200 @@ void soft_linear(const Model& M, const uint8_t* a, int m, const uint8_t* b, int 
     o.logz = lz * T;
 }
 
+// ── Hirschberg, affine Global, untracked (aligner.hpp:4151-4560) ───────────────
+// Divide and conquer: split the block's rows at p = i0 + H/2, sweep rows (i0, p] forward
+// and [p, i1) backward keeping only the last row (hb_fwd :4151, hb_rev :4210), join at the
+// first column of the strictly largest f + g, or an X run straddling the cut with one
+// go_b refunded (hb_solve :4458-4518), recurse; blocks of at most `cutoff` rows are solved
+// by a Pointers fill with the block's own borders (hb_base :4318-4400).  in_x / out_x: the
+// block's path leaves its origin / enters its corner by a vertical move of an inherited
+// run.  Pmax: the horizontal carry by the closed-form prefix max (hirschberg_pmax).  The
+// score is replayed along the path in T (:4530-4552).
+template <class T, bool Pmax>
+struct Hb {
+    int N; const T* blk; const uint8_t* a; const uint8_t* b; int cutoff;
+    T go_a, ge_a, go_b, ge_b;
+    std::vector<uint8_t> hops;                 // 0 M, 1 X (down), 2 Y (right), path order
+    T sub(int r, int c) const { return blk[size_t(a[r - 1]) * N + b[c - 1]]; }   // 1-based
+
+    // row 0 of a sweep block: the origin, then Y moves along it
+    void row0(bool flag, int W, std::vector<T>& pM, std::vector<T>& pX, std::vector<T>& pY) const {
+        pM[0] = flag ? ninf<T>() : T(0); pX[0] = ninf<T>(); pY[0] = ninf<T>();
+        for (int c = 1; c <= W; ++c) {
+            pM[c] = ninf<T>(); pX[c] = ninf<T>();
+            pY[c] = mx3<T>((pM[c - 1] - go_a) - ge_a, (pX[c - 1] - go_a) - ge_a, pY[c - 1] - ge_a);
+        }
+    }
+    // One sweep: H rows; sub_of(t, c) the substitution of swept row t (1..H), column c.
+    template <class F>
+    void sweep(int H, int W, bool flag, F sub_of, std::vector<T>& pM, std::vector<T>& pX,
+               std::vector<T>& pY) const {
+        std::vector<T> cM(W + 1), cX(W + 1), cY(W + 1), rmp(W + 1);
+        if (Pmax) for (int k = 0; k <= W; ++k) rmp[k] = static_cast<T>(k) * ge_a;
+        row0(flag, W, pM, pX, pY);
+        for (int t = 1; t <= H; ++t) {
+            cM[0] = ninf<T>();
+            cX[0] = mx3<T>((pM[0] - go_b) - ge_b, pX[0] - ge_b, (pY[0] - go_b) - ge_b);
+            if (flag && t == 1) cX[0] = T(0) - ge_b;
+            cY[0] = ninf<T>();
+            T P = cY[0] - ge_a;
+            for (int c = 1; c <= W; ++c) {
+                cM[c] = mx3<T>(pM[c - 1], pX[c - 1], pY[c - 1]) + sub_of(t, c);
+                cX[c] = mx3<T>((pM[c] - go_b) - ge_b, pX[c] - ge_b, (pY[c] - go_b) - ge_b);
+                if (Pmax) {
+                    const T g = (mx<T>(cM[c - 1], cX[c - 1]) - go_a) - ge_a;
+                    P = mx<T>(g + rmp[c - 1], P);
+                    cY[c] = P - rmp[c - 1];
+                } else {
+                    cY[c] = mx3<T>((cM[c - 1] - go_a) - ge_a, (cX[c - 1] - go_a) - ge_a, cY[c - 1] - ge_a);
+                }
+            }
+            std::swap(pM, cM); std::swap(pX, cX); std::swap(pY, cY);
+        }
+    }
+    static uint8_t pick(T vm, T vx, T vy) {
+        if (vm >= vx && vm >= vy) return 0;
+        return (vx >= vy) ? 1 : 2;
+    }
+    void base(int i0, int i1, int j0, int j1, bool in_x, bool out_x) {
+        const int H = i1 - i0, W = j1 - j0;
+        if (H == 0 && W == 0) return;
+        const size_t st = size_t(W) + 1;
+        std::vector<uint8_t> D(size_t(H + 1) * st);
+        std::vector<T> pM(st), pX(st), pY(st), cM(st), cX(st), cY(st);
+        auto pack = [](unsigned km, unsigned kx, unsigned ky) { return uint8_t(km | kx << 2 | ky << 4); };
+        pM[0] = in_x ? ninf<T>() : T(0); pX[0] = ninf<T>(); pY[0] = ninf<T>();
+        D[0] = pack(3, 3, 3);
+        for (int c = 1; c <= W; ++c) {
+            pM[c] = ninf<T>(); pX[c] = ninf<T>();
+            const T uy = (pM[c - 1] - go_a) - ge_a, vy = (pX[c - 1] - go_a) - ge_a, wy = pY[c - 1] - ge_a;
+            pY[c] = mx3<T>(uy, vy, wy);
+            D[c] = pack(3, 3, pick(uy, vy, wy));
+        }
+        for (int r = 1; r <= H; ++r) {
+            const size_t rb = size_t(r) * st;
+            const T ux0 = (pM[0] - go_b) - ge_b, vx0 = pX[0] - ge_b, wx0 = (pY[0] - go_b) - ge_b;
+            cM[0] = ninf<T>(); cX[0] = mx3<T>(ux0, vx0, wx0); cY[0] = ninf<T>();
+            D[rb] = pack(3, pick(ux0, vx0, wx0), 3);
+            if (in_x && r == 1) { cX[0] = T(0) - ge_b; D[rb] = pack(3, 1, 3); }
+            for (int c = 1; c <= W; ++c) {
+                const T dgM = pM[c - 1], dgX = pX[c - 1], dgY = pY[c - 1];
+                cM[c] = mx3<T>(dgM, dgX, dgY) + sub(i0 + r, j0 + c);
+                const T ux = (pM[c] - go_b) - ge_b, vx = pX[c] - ge_b, wx = (pY[c] - go_b) - ge_b;
+                cX[c] = mx3<T>(ux, vx, wx);
+                const T uy = (cM[c - 1] - go_a) - ge_a, vy = (cX[c - 1] - go_a) - ge_a, wy = cY[c - 1] - ge_a;
+                cY[c] = mx3<T>(uy, vy, wy);
+                D[rb + c] = pack(pick(dgM, dgX, dgY), pick(ux, vx, wx), pick(uy, vy, wy));
+            }
+            std::swap(pM, cM); std::swap(pX, cX); std::swap(pY, cY);
+        }
+        int r = H, c = W;
+        Tbl tbl;
+        if (out_x) tbl = TX;
+        else {
+            const T vm = pM[W], vx = pX[W], vy = pY[W];
+            tbl = (vm >= vx && vm >= vy) ? TM : ((vx >= vy) ? TX : TY);
+        }
+        const size_t first = hops.size();
+        while (r > 0 || c > 0) {
+            const uint8_t p = D[size_t(r) * st + size_t(c)];
+            uint8_t code;
+            if (tbl == TM)      { code = p & 3;        hops.push_back(0); --r; --c; }
+            else if (tbl == TX) { code = (p >> 2) & 3; hops.push_back(1); --r; }
+            else                { code = p >> 4;       hops.push_back(2); --c; }
+            tbl = (code == 1) ? TX : (code == 2 ? TY : TM);
+        }
+        std::reverse(hops.begin() + std::ptrdiff_t(first), hops.end());
+    }
+    void solve(int i0, int i1, int j0, int j1, bool in_x, bool out_x) {
+        const int H = i1 - i0, W = j1 - j0;
+        if (H <= cutoff) { base(i0, i1, j0, j1, in_x, out_x); return; }
+        const int p = i0 + H / 2;
+        std::vector<T> FM(W + 1), FX(W + 1), FY(W + 1), rM(W + 1), rX(W + 1), rY(W + 1);
+        // forward: swept row t is DP row i0 + t, column c pairs b[j0 + c - 1]
+        sweep(p - i0, W, in_x, [&](int t, int cc) { return sub(i0 + t, j0 + cc); }, FM, FX, FY);
+        // reverse: swept row t consumes a[i1 - t] (DP row i1 - t + 1), column d pairs b[j1 - d]
+        sweep(i1 - p, W, out_x, [&](int t, int d) { return sub(i1 - t + 1, j1 - d + 1); }, rM, rX, rY);
+        T best = ninf<T>();
+        int cstar = 0;
+        bool span = false;
+        for (int cc = 0; cc <= W; ++cc) {
+            const int d = W - cc;
+            const T f = mx3<T>(FM[cc], FX[cc], FY[cc]);
+            const T g = mx3<T>(rM[d], rX[d], rY[d]);
+            const T plain = f + g;
+            if (plain > best) { best = plain; cstar = cc; span = false; }
+            if (FX[cc] > ninf<T>() && rX[d] > ninf<T>()) {
+                const T joined = (FX[cc] + rX[d]) + go_b;
+                if (joined > best) { best = joined; cstar = cc; span = true; }
+            }
+        }
+        const int jstar = j0 + cstar;
+        solve(i0, p, j0, jstar, in_x, span);
+        solve(p, i1, jstar, j1, span, out_x);
+    }
+};
+
+// One pair by Hirschberg when it splits (m > cutoff); else the Pointers path (aligner.hpp
+// :1360, run_viterbi: a pair that never splits runs AS Pointers).  Guide in the recursion's
+// convention: the column where the path enters each row (guide_j_affine_hb :5233-5249).
+template <class T>
+int hb_one(const Model& M, const uint8_t* a, int m, const uint8_t* b, int n, int cutoff, bool pmax,
+           HardOut& o) {
+    if (m <= cutoff) return hard_one<T>(M, a, m, b, n, nullptr, nullptr, false, nullptr, -1, o, 0);
+    std::vector<T> blk(size_t(M.N) * M.N);
+    for (size_t k = 0; k < blk.size(); ++k) blk[k] = static_cast<T>(M.mat[k]);
+    const T go_a = static_cast<T>(M.gaps[kOpenA]), ge_a = static_cast<T>(M.gaps[kExtendA]);
+    const T go_b = static_cast<T>(M.gaps[kOpenB]), ge_b = static_cast<T>(M.gaps[kExtendB]);
+    std::vector<uint8_t> hops;
+    if (pmax) {
+        Hb<T, true> h{M.N, blk.data(), a, b, cutoff, go_a, ge_a, go_b, ge_b, {}};
+        h.solve(0, m, 0, n, false, false);
+        hops.swap(h.hops);
+    } else {
+        Hb<T, false> h{M.N, blk.data(), a, b, cutoff, go_a, ge_a, go_b, ge_b, {}};
+        h.solve(0, m, 0, n, false, false);
+        hops.swap(h.hops);
+    }
+    T s = T(0);
+    int i = 0, j = 0;
+    uint8_t prev = 3;
+    std::vector<int32_t> gj(size_t(m) + 1, -1);
+    gj[0] = 0;
+    for (uint8_t op : hops) {
+        if (op == 0) {
+            ++i; ++j;
+            s += blk[size_t(a[i - 1]) * M.N + b[j - 1]];
+            if (o.grad) o.grad[size_t(a[i - 1]) * M.N + b[j - 1]] += 1.0;
+            gj[i] = j;
+        } else if (op == 1) {
+            ++i;
+            if (prev != 1) { s -= go_b; if (o.grad) o.grad[size_t(M.N) * M.N + kOpenB] -= 1.0; }
+            s -= ge_b;
+            if (o.grad) o.grad[size_t(M.N) * M.N + kExtendB] -= 1.0;
+            gj[i] = j;
+        } else {
+            if (prev != 2) { s -= go_a; if (o.grad) o.grad[size_t(M.N) * M.N + kOpenA] -= 1.0; }
+            s -= ge_a;
+            if (o.grad) o.grad[size_t(M.N) * M.N + kExtendA] -= 1.0;
+            ++j;
+        }
+        prev = op;
+    }
+    gj[m] = n;
+    fill_guide_gaps(gj);
+    if (o.guide) std::memcpy(o.guide, gj.data(), sizeof(int32_t) * (m + 1));
+    if (o.moves) {
+        const int64_t k = std::min<int64_t>(int64_t(hops.size()), o.moves_cap);
+        for (int64_t q = 0; q < k; ++q) o.moves[q] = hops[q];
+    }
+    o.nmoves = int64_t(hops.size());
+    o.score = static_cast<double>(s);
+    o.end_i = m; o.end_j = n; o.start_i = 0; o.start_j = 0;
+    return 0;
+}
+
+
 }  // namespace
 
 // ── C ABI for the test suite (ctypes) ─────────────────────────────────────────
@@ -824,6 +1021,31 @@ int orc_soft_batch(int gm, int am, int N, int K, const double* mat, const double
         if (gm == 0) soft_linear(M, a + oa[p], m, b + ob[p], n, tk, gk, temperature, o);
         else         soft_affine(M, a + oa[p], m, b + ob[p], n, tk, gk, temperature, o);
         scores[p] = o.logz;
+    }
+    return 0;
+}
+
+// Hirschberg (affine Global, untracked, K = 1): pairs longer than `cutoff` rows split,
+// the rest run the Pointers path.  pmax: the closed-form horizontal carry.  Outputs as
+// orc_hard_batch (moves in path order, start to end).
+int orc_hb_batch(int prec, int pmax, int cutoff, int N, const double* mat, const double* gaps,
+                 const uint8_t* a, const int64_t* oa, const uint8_t* b, const int64_t* ob, int64_t n_pairs,
+                 double* scores, double* grads, int32_t* guides, uint8_t* moves, int64_t moves_cap,
+                 int64_t* nmoves) {
+    Model M{1, 0, N, 1, mat, gaps};
+    const size_t gs = size_t(N) * N + 4;
+    for (int64_t p = 0; p < n_pairs; ++p) {
+        const int m = int(oa[p + 1] - oa[p]), n = int(ob[p + 1] - ob[p]);
+        HardOut o;
+        o.grad = grads ? grads + gs * p : nullptr;
+        if (o.grad) std::fill(o.grad, o.grad + gs, 0.0);
+        o.guide = guides ? guides + oa[p] + p : nullptr;
+        o.moves = moves ? moves + moves_cap * p : nullptr;
+        o.moves_cap = moves_cap;
+        if (prec == 32) hb_one<float>(M, a + oa[p], m, b + ob[p], n, cutoff, pmax != 0, o);
+        else            hb_one<double>(M, a + oa[p], m, b + ob[p], n, cutoff, pmax != 0, o);
+        scores[p] = o.score;
+        if (nmoves) nmoves[p] = o.nmoves;
     }
     return 0;
 }

@@ -14,6 +14,8 @@ Two sources, both the reference's own code run here:
   backend, traceback "pointers"; soft: SeqPairBatchT<double>, log space) on seeded random
   batches: per-pair scores, gradients and guides, hard at float32 and float64, soft at
   T = 1 and 0.5, tracked with three parameter sets, and banded re-alignment after a step.
+* ``hirschberg.npz`` -- the same engine with traceback "hirschberg" and "hirschberg_pmax"
+  (affine Global, small hb_cutoff so pairs split several times), float32 and float64.
 """
 from __future__ import annotations
 
@@ -140,6 +142,43 @@ def ref_fixtures():
     print("reference_batches.npz:", len(out), "arrays")
 
 
+def hb_fixtures():
+    rng = np.random.default_rng(123)
+    AA = "ACDEFGHIKLMNPQRSTVWY"
+    out = {}
+    for name, integer in (("int", True), ("flt", False)):
+        mat = rng.integers(-4, 4, size=(1, 20, 20)).astype(np.float64) if integer else \
+            rng.normal(0, 2, size=(1, 20, 20)).round(3)
+        if integer:
+            mat[0][np.diag_indices(20)] = rng.integers(4, 12, size=20)
+        gaps = np.array([[11.0, 1.0, 11.0, 1.0]]) if integer else rng.uniform(0.3, 4.0, size=(1, 4)).round(3)
+        sa = ["".join(rng.choice(list(AA), size=int(rng.integers(1, 400)))) for _ in range(16)]
+        sb = []
+        for k, s in enumerate(sa):
+            if k % 2:
+                t = [c if rng.random() > 0.25 else str(rng.choice(list(AA))) for c in s]
+                sb.append("".join(t))
+            else:
+                sb.append("".join(rng.choice(list(AA), size=int(rng.integers(1, 400)))))
+        out[f"{name}_mat"], out[f"{name}_gaps"] = mat, gaps
+        out[f"{name}_sa"], out[f"{name}_sb"] = np.array(sa), np.array(sb)
+        for prec in (32, 64):
+            for tb in ("hirschberg", "hirschberg_pmax"):
+                for cut in (8, 64):
+                    r = oracle.ref_run(prec, 1, 0, 1, AA, mat, gaps, sa, sb, traceback=tb, hb_cutoff=cut)
+                    key = f"{name}_{tb}_{prec}_c{cut}_"
+                    out[key + "scores"] = r["scores"]
+                    out[key + "grads"] = r["grads"]
+                    out[key + "guides"] = r["guides"]
+    np.savez_compressed(os.path.join(HERE, "hirschberg.npz"), **out)
+    print("hirschberg.npz:", len(out), "arrays")
+
+
 if __name__ == "__main__":
-    brute_fixtures()
-    ref_fixtures()
+    which = sys.argv[1:] or ["brute", "ref", "hb"]
+    if "brute" in which:
+        brute_fixtures()
+    if "ref" in which:
+        ref_fixtures()
+    if "hb" in which:
+        hb_fixtures()

@@ -103,3 +103,21 @@ def test_live_reference_random(gm, am):
         np.testing.assert_array_equal(o["scores"], r["scores"])
         np.testing.assert_array_equal(o["grads"], r["grads"])
         np.testing.assert_array_equal(o["guides"], r["guides"])
+
+
+def test_hirschberg_fixtures():
+    """The Hirschberg restatement (exact and prefix-max carry) against the reference's own
+    engine with traceback hirschberg / hirschberg_pmax (tests/golden/hirschberg.npz)."""
+    z = np.load(os.path.join(GOLD, "hirschberg.npz"))
+    for name in ("int", "flt"):
+        sa, sb = [str(s) for s in z[f"{name}_sa"]], [str(s) for s in z[f"{name}_sb"]]
+        enc = oracle.Encoded(encode(AA, sa), encode(AA, sb))
+        for prec in (32, 64):
+            for tb in ("hirschberg", "hirschberg_pmax"):
+                for cut in (8, 64):
+                    key = f"{name}_{tb}_{prec}_c{cut}_"
+                    o = oracle.hirschberg(prec, z[f"{name}_mat"], z[f"{name}_gaps"], enc, cutoff=cut,
+                                          pmax=tb.endswith("pmax"))
+                    np.testing.assert_array_equal(o["scores"], z[key + "scores"])
+                    np.testing.assert_array_equal(o["grads"], z[key + "grads"])
+                    np.testing.assert_array_equal(o["guides"], z[key + "guides"])
