@@ -39,6 +39,9 @@ typedef struct nwg_job {
     int soft_double;   /* soft, precision 32: 0 float32 pass first (refused pairs rerun in double), 1 double only */
     int lanes;         /* 0 auto; else lanes per pair (1 or 32) for every pair (tuning) */
     int rows;          /* 0 auto; else rows per lane (tuning) */
+    int traceback;     /* hard, affine Global, untracked: 3 hirschberg, 4 hirschberg_pmax (pairs
+                          longer than hb_cutoff rows split); anything else the Pointers path */
+    int hb_cutoff;     /* Hirschberg base-case rows (>= 1; 0: 512) */
 } nwg_job;
 
 /* Last error message of the calling thread ("" if none). */

@@ -159,7 +159,7 @@ class SeqPairBatch:
         self._grad_mode = grad_mode
         self._kernel = kernel
         self._device = _device_index(device)
-        self.hb_cutoff = 512
+        self._hb_cutoff = 512
         self.soft_temperature = 1.0
         self.soft_impl = "scaled"
         self.soft_precision = "float32" if self._precision == 32 else "double"
@@ -274,8 +274,35 @@ class SeqPairBatch:
     def _job(self, grad_mode, band=-1, keep_paths=False):
         lanes, rows = self._tune
         soft_double = 1 if (self._precision == 64 or self.soft_precision == "double") else 0
+        tb = {"hirschberg": 3, "hirschberg_pmax": 4}.get(self._traceback, 0)
+        if tb and grad_mode != 2 and band < 0:
+            self._check_hirschberg()
         return Job(_GAP[self._gap_model], _MODE[self._mode], grad_mode, self._precision, band,
-                   int(bool(keep_paths)), float(self.soft_temperature), soft_double, lanes, rows)
+                   int(bool(keep_paths)), float(self.soft_temperature), soft_double, lanes, rows,
+                   tb, int(self._hb_cutoff))
+
+    def _check_hirschberg(self):
+        """Hirschberg splits pairs longer than hb_cutoff rows; this build implements the split
+        for affine Global untracked batches (the reference's viterbi_affine_hirschberg)."""
+        if self._gap_model == "affine" and self._mode == "global" and not self._tracked:
+            return
+        if self._n and int(np.max(np.diff(self._oa))) > self._hb_cutoff:
+            raise NotImplementedError(
+                f"nwgrad_b200: traceback=\"{self._traceback}\" splits pairs longer than hb_cutoff only for "
+                f"affine global untracked batches in this build (this batch: {self._gap_model} {self._mode}"
+                f"{', tracked' if self._tracked else ''}); use traceback=\"pointers\" or \"auto\"")
+
+    @property
+    def hb_cutoff(self) -> int:
+        """Hirschberg base-case size in rows: pairs longer than this split."""
+        return self._hb_cutoff
+
+    @hb_cutoff.setter
+    def hb_cutoff(self, v):
+        v = int(v)
+        if v < 1:
+            raise ValueError("nwgrad: hb_cutoff must be >= 1")
+        self._hb_cutoff = v
 
     def _run(self, grad_mode, band=-1, keep_paths=False, stream=None) -> float:
         if self._store is None:

@@ -28,9 +28,10 @@ UNITS = [
     ("soft_f64", "nwg_soft_inst.cu", ["-DNWG_T=double", "-DNWG_SOFT_FN=soft_fn_f64"]),
     ("noalloc", "nwg_noalloc.cu", []),
     ("server", "nwg_server.cu", []),
+    ("hb", "nwg_hb.cu", []),
 ]
 DEPS = ["nwg_capi.cu", "nwg_common.cuh", "nwg_hard.cuh", "nwg_walk.cuh", "nwg_soft.cuh", "nwg_kernels.h",
-        "nwg_hard_inst.cu", "nwg_soft_inst.cu", "nwg_noalloc.cu", "nwg_server.cu"]
+        "nwg_hard_inst.cu", "nwg_soft_inst.cu", "nwg_noalloc.cu", "nwg_server.cu", "nwg_hb.cu", "nwg_hb.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

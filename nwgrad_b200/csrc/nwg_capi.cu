@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "../../include/nwgrad_b200.h"
+#include "nwg_hb.h"
 #include "nwg_kernels.h"
 #include "nwg_walk.cuh"
 
@@ -235,7 +236,8 @@ struct Bucket {
 
 struct Plan {
     bool valid = false;
-    int key_soft = -1, key_lanes = -1, key_rows = -1, key_band = -1;
+    int key_soft = -1, key_lanes = -1, key_rows = -1, key_band = -1, key_hb = -1;
+    int64_t n_planned = 0;           // pairs in the buckets (hard: those not split by Hirschberg)
     std::vector<Bucket> buckets;
     std::vector<int64_t> code_off;   // hard: per pair
     int64_t code_bytes = 0;
@@ -277,6 +279,7 @@ struct nwg_store {
     int64_t scratch_budget = int64_t(24) << 30;   // bytes of soft scratch one call may hold
     int64_t ck_threshold = int64_t(16) << 20;     // soft: forward tables above this are checkpointed
     DBuf stripe_tab;
+    DBuf hb_pairs;                      // the pairs a Hirschberg run splits
     std::vector<int32_t> h_status;
     // timing
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -324,16 +327,20 @@ const T* ensure_bx0(nwg_store* s, bool aff, cudaStream_t st, bool& ok, DBuf& buf
     return buf.as<T>();
 }
 
-void build_plan(nwg_store* s, Plan& P, bool soft, int lanes, int rpl, int elem_bytes, bool band = false) {
-    if (P.valid && P.key_soft == int(soft) && P.key_lanes == lanes && P.key_rows == rpl && P.key_band == int(band)) return;
+// hb_cut > 0 (hard, full DP): pairs longer than hb_cut rows are left out (Hirschberg runs them).
+void build_plan(nwg_store* s, Plan& P, bool soft, int lanes, int rpl, int elem_bytes, bool band = false,
+                int hb_cut = 0) {
+    if (P.valid && P.key_soft == int(soft) && P.key_lanes == lanes && P.key_rows == rpl && P.key_band == int(band) &&
+        P.key_hb == hb_cut) return;
     P.reset();
-    P.key_soft = soft; P.key_lanes = lanes; P.key_rows = rpl; P.key_band = band;
+    P.key_soft = soft; P.key_lanes = lanes; P.key_rows = rpl; P.key_band = band; P.key_hb = hb_cut;
     const int64_t n = s->n;
     // one lane per pair keeps a K*N*N histogram per lane in shared memory (soft)
     const bool lane_ok_soft = int64_t(s->K) * s->N * s->N * elem_bytes * 32 <= 48 * 1024;
     std::map<std::tuple<int, int, int>, int> idx;
     for (int64_t p = 0; p < n; ++p) {
         const int m = int(s->oa[p + 1] - s->oa[p]), nb = int(s->ob[p + 1] - s->ob[p]);
+        if (hb_cut > 0 && m > hb_cut) continue;
         const int rows = soft ? m + 1 : m;
         const int sc = size_class(rows, nb);
         Geo g = band ? Geo{32, 2, true} : pick_geo(soft, std::max(rows, 1), nb, lanes, rpl, soft ? lane_ok_soft : true);
@@ -389,8 +396,9 @@ void build_plan(nwg_store* s, Plan& P, bool soft, int lanes, int rpl, int elem_b
             }
         P.code_bytes = std::max<int64_t>(off, 16);
     }
+    P.n_planned = int64_t(order.size());
     P.order.need(size_t(std::max<int64_t>(n, 1)) * 4);
-    if (n) NWG_CUDA(cudaMemcpy(P.order.p, order.data(), size_t(n) * 4, cudaMemcpyHostToDevice));
+    if (!order.empty()) NWG_CUDA(cudaMemcpy(P.order.p, order.data(), order.size() * 4, cudaMemcpyHostToDevice));
     if (!soft) {
         P.dcode_off.need(size_t(n + 1) * 8);
         NWG_CUDA(cudaMemcpy(P.dcode_off.p, P.code_off.data(), size_t(n + 1) * 8, cudaMemcpyHostToDevice));
@@ -413,8 +421,19 @@ template <class T>
 void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, bool want_guide) {
     const bool aff = J.gap_model == 1, loc = J.mode == 1, tr = s->tracked();
     const bool band = J.band >= 0;
+    // Hirschberg (affine Global, untracked, full DP): pairs longer than the cutoff split
+    const bool hb = !band && aff && !loc && !tr && (J.traceback == 3 || J.traceback == 4);
+    const int hb_cut = hb ? (J.hb_cutoff > 0 ? J.hb_cutoff : 512) : 0;
+    std::vector<int32_t> hb_pairs;
+    if (hb) {
+        for (int64_t p = 0; p < s->n; ++p)
+            if (s->oa[p + 1] - s->oa[p] > hb_cut) hb_pairs.push_back(int32_t(p));
+        if (!hb_pairs.empty() && !(s->gaps[0] >= 0.0 && s->gaps[1] >= 0.0 && s->gaps[2] >= 0.0 && s->gaps[3] >= 0.0))
+            throw Error(NWG_EINVAL, "nwgrad: traceback=\"hirschberg\" / \"hirschberg_pmax\" needs non-negative "
+                                    "gap penalties (got a negative one); use traceback=\"pointers\" or \"auto\"");
+    }
     Plan& P = band ? s->band_plan : s->hard_plan;
-    build_plan(s, P, false, band ? 32 : J.lanes, band ? 2 : J.rows, sizeof(T), band);
+    build_plan(s, P, false, band ? 32 : J.lanes, band ? 2 : J.rows, sizeof(T), band, hb_cut);
     s->codes.need(size_t(P.code_bytes), st);
     if (band) s->stripe_tab.need(size_t(std::max<int64_t>(P.n_stripes, 1)) * 16, st);
     const DBuf& matT = sizeof(T) == 4 ? s->matf : s->matd;
@@ -486,7 +505,7 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
     W.b = s->b.as<uint8_t>(); W.ob = s->dob.as<int64_t>();
     W.tracks = tr ? s->tracks.as<uint16_t>() : nullptr;
     W.gtracks = tr ? s->gtracks.as<uint16_t>() : nullptr;
-    W.order = P.order.as<int32_t>(); W.n_items = s->n;
+    W.order = P.order.as<int32_t>(); W.n_items = P.n_planned;
     W.stripe_base = band ? P.stripe_base.as<int64_t>() : nullptr;
     W.stripe_tab = band ? s->stripe_tab.as<int64_t>() : nullptr;
     W.N = s->N; W.K = s->K; W.affine = aff; W.local = loc;
@@ -497,10 +516,34 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
     W.moves = keep ? s->moves.as<uint8_t>() : nullptr;
     W.moves_off = keep ? s->moves_off.as<int64_t>() : nullptr;
     W.path_info = keep ? s->path_info.as<int32_t>() : nullptr;
-    if (s->n) {
-        nwg::walk_kernel<<<unsigned((s->n + 127) / 128), 128, 0, st>>>(W);
+    if (P.n_planned) {
+        nwg::walk_kernel<<<unsigned((P.n_planned + 127) / 128), 128, 0, st>>>(W);
         NWG_CUDA(cudaGetLastError());
         s->last_launches++;
+    }
+    if (!hb_pairs.empty()) {
+        s->hb_pairs.need(hb_pairs.size() * 4, st);
+        NWG_CUDA(cudaMemcpyAsync(s->hb_pairs.p, hb_pairs.data(), hb_pairs.size() * 4, cudaMemcpyHostToDevice, st));
+        nwg::HbRun H{};
+        H.a = s->a.as<uint8_t>(); H.b = s->b.as<uint8_t>();
+        H.oa = s->doa.as<int64_t>(); H.ob = s->dob.as<int64_t>();
+        H.pairs = s->hb_pairs.as<int32_t>();
+        H.mat = matT.p; H.N = s->N;
+        H.go_a = s->gaps[0]; H.ge_a = s->gaps[1]; H.go_b = s->gaps[2]; H.ge_b = s->gaps[3];
+        H.score = s->score.as<double>(); H.end = s->end.as<int32_t>();
+        H.grad = want_grad ? s->grad.as<double>() : nullptr; H.gstride = s->gstride;
+        H.guide = want_guide ? s->guide.as<int32_t>() : nullptr;
+        H.moves = keep ? s->moves.as<uint8_t>() : nullptr;
+        H.moves_off = keep ? s->moves_off.as<int64_t>() : nullptr;
+        H.path_info = keep ? s->path_info.as<int32_t>() : nullptr;
+        H.h_pairs = hb_pairs.data(); H.n_pairs = int64_t(hb_pairs.size());
+        H.h_oa = s->oa.data(); H.h_ob = s->ob.data();
+        H.cutoff = hb_cut; H.pmax = J.traceback == 4;
+        try {
+            s->last_launches += nwg::hb_run(H, int(sizeof(T)), st, sms);
+        } catch (const std::runtime_error& e) {
+            throw Error(NWG_ECUDA, e.what());
+        }
     }
 }
 
@@ -817,7 +860,7 @@ int nwg_store_destroy(nwg_store* s) {
                         &s->gapd, &s->bx0f, &s->bx0d, &s->score, &s->end, &s->grad, &s->guide, &s->status,
                         &s->stripe_tab, &s->codes, &s->scratch, &s->part, &s->red, &s->moves,
                         &s->moves_off, &s->path_info, &s->tmatf, &s->tgapf, &s->tmatd, &s->tgapd,
-                        &s->tbx0f, &s->tbx0d, &s->tscore, &s->tend})
+                        &s->tbx0f, &s->tbx0d, &s->tscore, &s->tend, &s->hb_pairs})
             b->release();
         if (s->ev0) cudaEventDestroy(s->ev0);
         if (s->ev1) cudaEventDestroy(s->ev1);

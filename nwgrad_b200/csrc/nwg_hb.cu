@@ -1,0 +1,564 @@
+// Hirschberg re-alignment (affine Global, untracked) on the GPU: linear memory for long pairs.
+//
+// The reference's recursion (aligner.hpp:4151-4560): a block (rows i0..i1, columns j0..j1,
+// boundary states in_x / out_x) longer than the cutoff is split at row p = i0 + H/2; a
+// forward sweep over rows (i0, p] and a reverse sweep over rows [p, i1) keep only their last
+// rows; the join picks the first column of the strictly best sum (or an X run straddling the
+// cut, one open refunded); the two halves recurse.  Blocks of at most `cutoff` rows are
+// solved by a Pointers fill with the block's own borders and walked back.  The score is then
+// replayed along the whole path in T, the gradient counted and the guide read off it.
+//
+// B200 layout: the recursion runs breadth first, one level at a time over every block of
+// every pair, so each launch has all of a level's work.
+//   * hb_sweep_kernel -- one thread block per half-sweep, a pipeline of NW warps over the
+//     block's stripes (32 lanes x R rows each): warp w fills stripe round * NW + w two chunks
+//     of 32 columns behind warp w - 1, whose bottom row it reads from a shared-memory ring;
+//     the last warp's bottom row reaches the next round's first warp through a row buffer in
+//     global memory.  One __syncthreads per chunk; no spin waits.
+//   * hb_join_kernel -- one thread block per split block: the first best column.
+//   * hb_base_kernel -- one warp per base block: the lane-strip Pointers fill into a
+//     row-major code table, then lane 0 walks it.
+//   * hb_replay_kernel -- one thread per pair: the base blocks' moves in path order.
+// Cells use the reference's expressions ((v - go) - ge, max of three, the prefix-max carry's
+// rounded multiply and add), so the path, score, gradient and guide are bit-identical.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "nwg_common.cuh"
+#include "nwg_hb.h"
+
+namespace nwg {
+namespace {
+
+constexpr int kHbC = 32;             // steps per pipeline chunk
+constexpr int kHbRing = 4 * kHbC;    // ring slots per warp boundary
+
+struct SweepJob {
+    int64_t a_base; int64_t b_base;  // row t >= 1 reads a[a_base + a_step (t - 1)]; column c >= 1 b[b_base + b_step (c - 1)]
+    int a_step, b_step;
+    int H, W, flag, pad;
+    int64_t out;                     // T offset of the last row: M, X, Y arrays of W + 1
+    int64_t wrap;                    // T offset of the wrap row buffer (3 (W + 1))
+};
+
+struct BaseJob {
+    int64_t a_base, b_base;          // row t >= 1 reads a[a_base + t - 1]; column c >= 1 b[b_base + c - 1]
+    int H, W, in_x, out_x;
+    int64_t codes;                   // byte offset of the (H + 1) x (W + 1) code table
+    int64_t bnd;                     // T offset of the stripe boundary row (3 (W + 1))
+    int64_t moves;                   // byte offset of the moves (walk order, H + W at most)
+};
+
+template <class T> struct Gaps { T go_a, ge_a, go_b, ge_b; };
+
+template <class T>
+__device__ __forceinline__ T chain_y(T lm, T lx, T ly, const Gaps<T>& g) {
+    return hmax3((lm - g.go_a) - g.ge_a, (lx - g.go_a) - g.ge_a, ly - g.ge_a);
+}
+template <class T>
+__device__ __forceinline__ T chain_x(T um, T ux, T uy, const Gaps<T>& g) {
+    return hmax3((um - g.go_b) - g.ge_b, ux - g.ge_b, (uy - g.go_b) - g.ge_b);
+}
+
+// ── sweep ─────────────────────────────────────────────────────────────────────
+template <class T, bool PMAX, int R>
+__global__ void __launch_bounds__(512) hb_sweep_kernel(const uint8_t* __restrict__ a, const uint8_t* __restrict__ b,
+                                                       const T* __restrict__ mat, int N, Gaps<T> gp,
+                                                       const SweepJob* __restrict__ jobs, int n_jobs,
+                                                       T* __restrict__ out, T* __restrict__ wrapbuf) {
+    constexpr int G = 32, GR = G * R;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* smat = reinterpret_cast<T*>(smem_raw);
+    T* ring = smat + ((N * N + 3) & ~3);                   // [NW][3][kHbRing]
+    for (int k = threadIdx.x; k < N * N; k += blockDim.x) smat[k] = mat[k];
+    __syncthreads();
+    const int NW = blockDim.x / G;
+    const int w = threadIdx.x / G, lane = threadIdx.x % G;
+    T* myring = ring + size_t(w) * 3 * kHbRing;
+    const T* inring = ring + size_t(w > 0 ? w - 1 : 0) * 3 * kHbRing;
+    const T NI = ninf<T>();
+
+    for (int jb = blockIdx.x; jb < n_jobs; jb += gridDim.x) {
+        const SweepJob J = jobs[jb];
+        const int H = J.H, W = J.W;
+        const int ns = (H + 1 + GR - 1) / GR;              // stripes over rows 0..H
+        const int rounds = (ns + NW - 1) / NW;
+        const int S = W + G;                               // steps: columns 0..W plus the skew
+        int Ct = (S + kHbC - 1) / kHbC;
+        Ct = max(Ct, 2 * NW);                              // a wrap row is read a round after it is written
+        const int64_t chunks = int64_t(rounds) * Ct;
+        const int64_t supers = chunks + 2 * (NW - 1);
+        T* oM = out + J.out; T* oX = oM + (W + 1); T* oY = oX + (W + 1);
+        T* wM = wrapbuf + J.wrap; T* wX = wM + (W + 1); T* wY = wX + (W + 1);
+
+        int sn = 0, i0 = 0;
+        int key[R];
+        T cM[R], cX[R], cY[R], P[R];
+        T dgM = NI, dgX = NI, dgY = NI, upM = NI, upX = NI, upY = NI;
+        for (int64_t K = 0; K < supers; ++K) {
+            const int64_t v = K - 2 * w;
+            if (v >= 0 && v < chunks) {
+                const int round = int(v / Ct), chunk = int(v % Ct);
+                if (chunk == 0) {                          // a new stripe for this warp
+                    sn = round * NW + w;
+                    i0 = sn * GR + lane * R;
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        const int t = i0 + r;
+                        key[r] = (t >= 1 && t <= H) ? int(a[J.a_base + int64_t(J.a_step) * (t - 1)]) * N : 0;
+                        cM[r] = NI; cX[r] = NI; cY[r] = NI; P[r] = NI;
+                    }
+                    dgM = dgX = dgY = NI; upM = upX = upY = NI;
+                }
+                if (sn < ns) {
+                    for (int tt = 0; tt < kHbC; ++tt) {
+                        const int tau = chunk * kHbC + tt;
+                        const int64_t vstep = v * kHbC + tt;
+                        const int c = tau - lane;
+                        if (lane == 0 && sn > 0 && c <= W) {
+                            if (w > 0) {
+                                const int sl = int(vstep % kHbRing);
+                                upM = inring[sl]; upX = inring[kHbRing + sl]; upY = inring[2 * kHbRing + sl];
+                            } else {
+                                upM = wM[c]; upX = wX[c]; upY = wY[c];
+                            }
+                        }
+                        const bool active = c >= 0 && c <= W;
+                        if (active) {
+                            const int bj = c >= 1 ? int(b[J.b_base + int64_t(J.b_step) * (c - 1)]) : 0;
+                            T pM = dgM, pX = dgX, pY = dgY;      // row above, column c - 1
+                            T qM = upM, qX = upX, qY = upY;      // row above, column c
+#pragma unroll
+                            for (int r = 0; r < R; ++r) {
+                                const int t = i0 + r;
+                                T mv, xv, yv;
+                                if (t == 0) {
+                                    if (c == 0) { mv = J.flag ? NI : T(0); xv = NI; yv = NI; }
+                                    else { mv = NI; xv = NI; yv = chain_y(cM[r], cX[r], cY[r], gp); }
+                                } else if (c == 0) {
+                                    mv = NI; yv = NI;
+                                    xv = (t == 1 && J.flag) ? T(0) - gp.ge_b : chain_x(qM, qX, qY, gp);
+                                } else {
+                                    mv = hmax3(pM, pX, pY) + smat[key[r] + bj];
+                                    xv = chain_x(qM, qX, qY, gp);
+                                    if constexpr (PMAX) {
+                                        const T g = (hmax(cM[r], cX[r]) - gp.go_a) - gp.ge_a;
+                                        const T rm = mul_rn(static_cast<T>(c - 1), gp.ge_a);
+                                        P[r] = hmax(add_rn(g, rm), P[r]);
+                                        yv = P[r] - rm;
+                                    } else {
+                                        yv = chain_y(cM[r], cX[r], cY[r], gp);
+                                    }
+                                }
+                                pM = cM[r]; pX = cX[r]; pY = cY[r];
+                                cM[r] = mv; cX[r] = xv; cY[r] = yv;
+                                qM = mv; qX = xv; qY = yv;
+                                if (t == H) { oM[c] = mv; oX[c] = xv; oY[c] = yv; }
+                            }
+                            dgM = upM; dgX = upX; dgY = upY;
+                        }
+                        const T sM = __shfl_up_sync(0xffffffffu, cM[R - 1], 1);
+                        const T sX = __shfl_up_sync(0xffffffffu, cX[R - 1], 1);
+                        const T sY = __shfl_up_sync(0xffffffffu, cY[R - 1], 1);
+                        if (lane > 0) { upM = sM; upX = sX; upY = sY; }
+                        if (lane == G - 1 && active && sn + 1 < ns) {
+                            if (w + 1 < NW) {
+                                const int sl = int((vstep - (G - 1)) % kHbRing);
+                                myring[sl] = cM[R - 1]; myring[kHbRing + sl] = cX[R - 1]; myring[2 * kHbRing + sl] = cY[R - 1];
+                            } else {
+                                wM[c] = cM[R - 1]; wX[c] = cX[R - 1]; wY[c] = cY[R - 1];
+                            }
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// ── join ──────────────────────────────────────────────────────────────────────
+// Split block k: forward sweep 2k, reverse sweep 2k + 1.  res[2k] = column, res[2k+1] = span.
+template <class T>
+__global__ void hb_join_kernel(const SweepJob* __restrict__ jobs, int n_blocks, const T* __restrict__ out,
+                               T go_b, int32_t* __restrict__ res) {
+    __shared__ T sv[256];
+    __shared__ int sc[256], ss[256];
+    const T NI = ninf<T>();
+    for (int k = blockIdx.x; k < n_blocks; k += gridDim.x) {
+        const SweepJob F = jobs[2 * k], Rv = jobs[2 * k + 1];
+        const int W = F.W;
+        const T* FM = out + F.out; const T* FX = FM + (W + 1); const T* FY = FX + (W + 1);
+        const T* rM = out + Rv.out; const T* rX = rM + (W + 1); const T* rY = rX + (W + 1);
+        T best = NI; int bc = 0x7fffffff, bs = 0;
+        for (int c = threadIdx.x; c <= W; c += blockDim.x) {
+            const int d = W - c;
+            const T f = hmax3(FM[c], FX[c], FY[c]);
+            const T g = hmax3(rM[d], rX[d], rY[d]);
+            T val = f + g;
+            int sp = 0;
+            if (FX[c] > NI && rX[d] > NI) {
+                const T joined = (FX[c] + rX[d]) + go_b;
+                if (joined > val) { val = joined; sp = 1; }
+            }
+            if (val > best) { best = val; bc = c; bs = sp; }
+        }
+        sv[threadIdx.x] = best; sc[threadIdx.x] = bc; ss[threadIdx.x] = bs;
+        __syncthreads();
+        for (int off = blockDim.x / 2; off > 0; off >>= 1) {
+            if (threadIdx.x < off) {
+                const T ov = sv[threadIdx.x + off];
+                const int oc = sc[threadIdx.x + off];
+                if (ov > sv[threadIdx.x] || (ov == sv[threadIdx.x] && oc < sc[threadIdx.x])) {
+                    sv[threadIdx.x] = ov; sc[threadIdx.x] = oc; ss[threadIdx.x] = ss[threadIdx.x + off];
+                }
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            const bool none = sc[0] == 0x7fffffff;
+            res[2 * k] = none ? 0 : sc[0];
+            res[2 * k + 1] = none ? 0 : ss[0];
+        }
+        __syncthreads();
+    }
+}
+
+// ── base blocks ───────────────────────────────────────────────────────────────
+template <class T>
+__device__ __forceinline__ uint32_t pick_hb(T vm, T vx, T vy) {
+    if (vm >= vx && vm >= vy) return 0u;
+    return vx >= vy ? 1u : 2u;
+}
+
+template <class T, int R>
+__global__ void __launch_bounds__(128) hb_base_kernel(const uint8_t* __restrict__ a, const uint8_t* __restrict__ b,
+                                                      const T* __restrict__ mat, int N, Gaps<T> gp,
+                                                      const BaseJob* __restrict__ jobs, int n_jobs,
+                                                      uint8_t* __restrict__ codes, T* __restrict__ bndbuf,
+                                                      uint8_t* __restrict__ moves, int32_t* __restrict__ nmoves) {
+    constexpr int G = 32, GR = G * R;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* smat = reinterpret_cast<T*>(smem_raw);
+    for (int k = threadIdx.x; k < N * N; k += blockDim.x) smat[k] = mat[k];
+    __syncthreads();
+    const int lane = threadIdx.x % G;
+    const int wpb = blockDim.x / G;
+    const T NI = ninf<T>();
+    for (int jb = blockIdx.x * wpb + threadIdx.x / G; jb < n_jobs; jb += gridDim.x * wpb) {
+        const BaseJob J = jobs[jb];
+        const int H = J.H, W = J.W;
+        const int64_t st = int64_t(W) + 1;
+        uint8_t* D = codes + J.codes;
+        T* bM = bndbuf + J.bnd; T* bX = bM + st; T* bY = bX + st;
+        const int ns = (H + 1 + GR - 1) / GR;
+        T eM = NI, eX = NI, eY = NI;                       // row H, column W (its owner lane)
+        for (int s = 0; s < ns; ++s) {
+            const int i0 = s * GR + lane * R;
+            int key[R];
+            T cM[R], cX[R], cY[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int t = i0 + r;
+                key[r] = (t >= 1 && t <= H) ? int(a[J.a_base + t - 1]) * N : 0;
+                cM[r] = NI; cX[r] = NI; cY[r] = NI;
+            }
+            T dgM = NI, dgX = NI, dgY = NI, upM = NI, upX = NI, upY = NI;
+            for (int tau = 0; tau < W + G; ++tau) {
+                const int c = tau - lane;
+                if (lane == 0 && s > 0 && c <= W) { upM = bM[c]; upX = bX[c]; upY = bY[c]; }
+                const bool active = c >= 0 && c <= W;
+                if (active) {
+                    const int bj = c >= 1 ? int(b[J.b_base + c - 1]) : 0;
+                    T pM = dgM, pX = dgX, pY = dgY;
+                    T qM = upM, qX = upX, qY = upY;
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        const int t = i0 + r;
+                        T mv, xv, yv;
+                        uint32_t code;
+                        if (t == 0) {
+                            if (c == 0) { mv = J.in_x ? NI : T(0); xv = NI; yv = NI; code = 3u | (3u << 2) | (3u << 4); }
+                            else {
+                                const T uy = (cM[r] - gp.go_a) - gp.ge_a, vy = (cX[r] - gp.go_a) - gp.ge_a, wy = cY[r] - gp.ge_a;
+                                mv = NI; xv = NI; yv = hmax3(uy, vy, wy);
+                                code = 3u | (3u << 2) | (pick_hb(uy, vy, wy) << 4);
+                            }
+                        } else if (c == 0) {
+                            const T ux = (qM - gp.go_b) - gp.ge_b, vx = qX - gp.ge_b, wx = (qY - gp.go_b) - gp.ge_b;
+                            mv = NI; yv = NI; xv = hmax3(ux, vx, wx);
+                            code = 3u | (pick_hb(ux, vx, wx) << 2) | (3u << 4);
+                            if (J.in_x && t == 1) { xv = T(0) - gp.ge_b; code = 3u | (1u << 2) | (3u << 4); }
+                        } else {
+                            const T ux = (qM - gp.go_b) - gp.ge_b, vx = qX - gp.ge_b, wx = (qY - gp.go_b) - gp.ge_b;
+                            const T uy = (cM[r] - gp.go_a) - gp.ge_a, vy = (cX[r] - gp.go_a) - gp.ge_a, wy = cY[r] - gp.ge_a;
+                            mv = hmax3(pM, pX, pY) + smat[key[r] + bj];
+                            xv = hmax3(ux, vx, wx);
+                            yv = hmax3(uy, vy, wy);
+                            code = pick_hb(pM, pX, pY) | (pick_hb(ux, vx, wx) << 2) | (pick_hb(uy, vy, wy) << 4);
+                        }
+                        if (t <= H) D[int64_t(t) * st + c] = uint8_t(code);
+                        pM = cM[r]; pX = cX[r]; pY = cY[r];
+                        cM[r] = mv; cX[r] = xv; cY[r] = yv;
+                        qM = mv; qX = xv; qY = yv;
+                        if (t == H && c == W) { eM = mv; eX = xv; eY = yv; }
+                    }
+                    dgM = upM; dgX = upX; dgY = upY;
+                }
+                const T sM = __shfl_up_sync(0xffffffffu, cM[R - 1], 1);
+                const T sX = __shfl_up_sync(0xffffffffu, cX[R - 1], 1);
+                const T sY = __shfl_up_sync(0xffffffffu, cY[R - 1], 1);
+                if (lane > 0) { upM = sM; upX = sX; upY = sY; }
+                if (lane == G - 1 && active && s + 1 < ns) { bM[c] = cM[R - 1]; bX[c] = cX[R - 1]; bY[c] = cY[R - 1]; }
+            }
+            __syncwarp();
+        }
+        const int owner = (H % GR) / R;
+        eM = __shfl_sync(0xffffffffu, eM, owner);
+        eX = __shfl_sync(0xffffffffu, eX, owner);
+        eY = __shfl_sync(0xffffffffu, eY, owner);
+        __syncwarp();
+        if (lane == 0) {
+            uint8_t* mv = moves + J.moves;
+            int r = H, c = W, k = 0;
+            int tbl = J.out_x ? 1 : ((eM >= eX && eM >= eY) ? 0 : (eX >= eY ? 1 : 2));
+            while ((r > 0 || c > 0) && r >= 0 && c >= 0 && k <= H + W) {
+                const uint32_t p = D[int64_t(r) * st + c];
+                uint32_t code;
+                if (tbl == 0)      { code = p & 3u;        mv[k++] = 0; --r; --c; }
+                else if (tbl == 1) { code = (p >> 2) & 3u; mv[k++] = 1; --r; }
+                else               { code = p >> 4;        mv[k++] = 2; --c; }
+                tbl = code == 1u ? 1 : (code == 2u ? 2 : 0);
+            }
+            nmoves[jb] = k;
+        }
+        __syncwarp();
+    }
+}
+
+// ── replay ────────────────────────────────────────────────────────────────────
+template <class T>
+__global__ void hb_replay_kernel(const HbRun P, const BaseJob* __restrict__ jobs, const int64_t* __restrict__ first,
+                                 const uint8_t* __restrict__ moves, const int32_t* __restrict__ nmoves, int n) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int p = P.pairs[k];
+    const int64_t ao = P.oa[p], bo = P.ob[p];
+    const int m = int(P.oa[p + 1] - ao), nb = int(P.ob[p + 1] - bo);
+    const uint8_t* ap = P.a + ao;
+    const uint8_t* bp = P.b + bo;
+    const T* mat = static_cast<const T*>(P.mat);
+    const int N = P.N;
+    const T go_a = static_cast<T>(P.go_a), ge_a = static_cast<T>(P.ge_a);
+    const T go_b = static_cast<T>(P.go_b), ge_b = static_cast<T>(P.ge_b);
+    double* g = P.grad ? P.grad + P.gstride * p : nullptr;
+    const int64_t NN = int64_t(N) * N;
+    int32_t* gj = P.guide ? P.guide + ao + p : nullptr;
+    if (gj) { for (int q = 0; q <= m; ++q) gj[q] = -1; gj[0] = 0; }
+    uint8_t* keep = P.moves ? P.moves + P.moves_off[p] : nullptr;
+    int64_t total = 0;
+    for (int64_t q = first[k]; q < first[k + 1]; ++q) total += nmoves[q];
+    T s = T(0);
+    int i = 0, j = 0;
+    int prev = 3;
+    int64_t idx = 0;
+    for (int64_t q = first[k]; q < first[k + 1]; ++q) {
+        const uint8_t* mv = moves + jobs[q].moves;
+        for (int e = nmoves[q] - 1; e >= 0; --e) {
+            const int op = mv[e];
+            if (op == 0) {
+                ++i; ++j;
+                const int64_t cell = int64_t(ap[i - 1]) * N + bp[j - 1];
+                s += mat[cell];
+                if (g) g[cell] += 1.0;
+                if (gj) gj[i] = j;
+            } else if (op == 1) {
+                ++i;
+                if (prev != 1) { s -= go_b; if (g) g[NN + 2] -= 1.0; }
+                s -= ge_b;
+                if (g) g[NN + 3] -= 1.0;
+                if (gj) gj[i] = j;
+            } else {
+                if (prev != 2) { s -= go_a; if (g) g[NN + 0] -= 1.0; }
+                s -= ge_a;
+                if (g) g[NN + 1] -= 1.0;
+                ++j;
+            }
+            if (keep) keep[total - 1 - idx] = uint8_t(op);   // walk order: end to start
+            ++idx;
+            prev = op;
+        }
+    }
+    P.score[p] = static_cast<double>(s);
+    P.end[4 * p] = m; P.end[4 * p + 1] = nb; P.end[4 * p + 2] = prev == 1 ? 1 : (prev == 2 ? 2 : 0);
+    P.end[4 * p + 3] = 0;
+    if (P.path_info) { P.path_info[3 * p] = int32_t(total); P.path_info[3 * p + 1] = 0; P.path_info[3 * p + 2] = 0; }
+    if (gj) {
+        gj[m] = nb;
+        const int L = m + 1;
+        int lo = 0;
+        while (lo < L) {
+            if (gj[lo] < 0) { ++lo; continue; }
+            int hi = lo + 1;
+            while (hi < L && gj[hi] < 0) ++hi;
+            if (hi == L) { for (int q = lo + 1; q < L; ++q) gj[q] = gj[lo]; break; }
+            for (int q = lo + 1; q < hi; ++q) gj[q] = gj[lo] + (gj[hi] - gj[lo]) * (q - lo) / (hi - lo);
+            lo = hi;
+        }
+    }
+}
+
+// ── host driver ───────────────────────────────────────────────────────────────
+struct Blk { int k; int i0, i1, j0, j1; int in_x, out_x; };   // k: index into P.pairs
+
+#define HB_CUDA(call)                                                                      \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess) throw std::runtime_error(std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// A device buffer for one run, from the stream-ordered pool.
+struct Tmp {
+    void* p = nullptr; cudaStream_t st;
+    explicit Tmp(cudaStream_t s) : st(s) {}
+    void* get(size_t n) {
+        if (p) { cudaFreeAsync(p, st); p = nullptr; }
+        HB_CUDA(cudaMallocAsync(&p, std::max<size_t>(n, 256), st));
+        return p;
+    }
+    ~Tmp() { if (p) cudaFreeAsync(p, st); }
+};
+
+template <class T>
+int64_t hb_run_t(const HbRun& P, cudaStream_t st, int sms) {
+    const int n = int(P.n_pairs);
+    if (n == 0) return 0;
+    int64_t launches = 0;
+    const Gaps<T> gp{static_cast<T>(P.go_a), static_cast<T>(P.ge_a), static_cast<T>(P.go_b), static_cast<T>(P.ge_b)};
+    std::vector<Blk> cur;
+    cur.reserve(size_t(n));
+    for (int k = 0; k < n; ++k) {
+        const int p = P.h_pairs[k];
+        cur.push_back(Blk{k, 0, int(P.h_oa[p + 1] - P.h_oa[p]), 0, int(P.h_ob[p + 1] - P.h_ob[p]), 0, 0});
+    }
+    Tmp djobs(st), dout(st), dwrap(st), dres(st);
+    constexpr int R = 4;
+    const int NWmax = 16;
+    const size_t ring_bytes_per_warp = size_t(3) * kHbRing * sizeof(T);
+    const size_t mat_bytes = size_t((P.N * P.N + 3) & ~3) * sizeof(T);
+    while (true) {
+        std::vector<int> split;
+        for (int q = 0; q < int(cur.size()); ++q)
+            if (cur[q].i1 - cur[q].i0 > P.cutoff) split.push_back(q);
+        if (split.empty()) break;
+        // the level's half-sweeps, largest first for the grid-stride order
+        std::vector<SweepJob> jobs(2 * split.size());
+        int64_t out_off = 0, wrap_off = 0;
+        int max_ns = 1;
+        for (size_t s = 0; s < split.size(); ++s) {
+            const Blk& B = cur[split[s]];
+            const int p = P.h_pairs[B.k];
+            const int mid = B.i0 + (B.i1 - B.i0) / 2, W = B.j1 - B.j0;
+            SweepJob& F = jobs[2 * s];
+            F.a_base = P.h_oa[p] + B.i0; F.a_step = 1; F.b_base = P.h_ob[p] + B.j0; F.b_step = 1;
+            F.H = mid - B.i0; F.W = W; F.flag = B.in_x; F.pad = 0;
+            SweepJob& Rv = jobs[2 * s + 1];
+            Rv.a_base = P.h_oa[p] + B.i1 - 1; Rv.a_step = -1; Rv.b_base = P.h_ob[p] + B.j1 - 1; Rv.b_step = -1;
+            Rv.H = B.i1 - mid; Rv.W = W; Rv.flag = B.out_x; Rv.pad = 0;
+            for (SweepJob* x : {&F, &Rv}) {
+                x->out = out_off; out_off += 3 * (int64_t(W) + 1);
+                x->wrap = wrap_off; wrap_off += 3 * (int64_t(W) + 1);
+                max_ns = std::max(max_ns, (x->H + 1 + 32 * R - 1) / (32 * R));
+            }
+        }
+        int NW = 1;
+        while (NW < NWmax && NW < max_ns) NW *= 2;
+        SweepJob* dj = static_cast<SweepJob*>(djobs.get(jobs.size() * sizeof(SweepJob)));
+        HB_CUDA(cudaMemcpyAsync(dj, jobs.data(), jobs.size() * sizeof(SweepJob), cudaMemcpyHostToDevice, st));
+        T* o = static_cast<T*>(dout.get(size_t(out_off) * sizeof(T)));
+        T* wr = static_cast<T*>(dwrap.get(size_t(wrap_off) * sizeof(T)));
+        const size_t smem = mat_bytes + NW * ring_bytes_per_warp;
+        auto fn = P.pmax ? hb_sweep_kernel<T, true, R> : hb_sweep_kernel<T, false, R>;
+        if (smem > 48 * 1024) HB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        int occ = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 32 * NW, smem);
+        const int grid = int(std::min<int64_t>(int64_t(jobs.size()), int64_t(sms) * std::max(occ, 1)));
+        fn<<<grid, 32 * NW, smem, st>>>(P.a, P.b, static_cast<const T*>(P.mat), P.N, gp, dj, int(jobs.size()), o, wr);
+        HB_CUDA(cudaGetLastError());
+        int32_t* res = static_cast<int32_t*>(dres.get(split.size() * 2 * sizeof(int32_t)));
+        const int jgrid = int(std::min<int64_t>(int64_t(split.size()), int64_t(sms) * 8));
+        hb_join_kernel<T><<<jgrid, 256, 0, st>>>(dj, int(split.size()), o, gp.go_b, res);
+        HB_CUDA(cudaGetLastError());
+        launches += 2;
+        std::vector<int32_t> h(split.size() * 2);
+        HB_CUDA(cudaMemcpyAsync(h.data(), res, h.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        HB_CUDA(cudaStreamSynchronize(st));
+        std::vector<Blk> next;
+        next.reserve(cur.size() + split.size());
+        size_t si = 0;
+        for (int q = 0; q < int(cur.size()); ++q) {
+            const Blk& B = cur[q];
+            if (si < split.size() && split[si] == q) {
+                const int mid = B.i0 + (B.i1 - B.i0) / 2;
+                const int js = B.j0 + h[2 * si];
+                const int span = h[2 * si + 1];
+                next.push_back(Blk{B.k, B.i0, mid, B.j0, js, B.in_x, span});
+                next.push_back(Blk{B.k, mid, B.i1, js, B.j1, span, B.out_x});
+                ++si;
+            } else {
+                next.push_back(B);
+            }
+        }
+        cur.swap(next);
+    }
+    // base blocks (path order per pair), then the replay
+    std::vector<BaseJob> bj(cur.size());
+    std::vector<int64_t> first(size_t(n) + 1, 0);
+    int64_t code_off = 0, bnd_off = 0, mv_off = 0;
+    for (size_t q = 0; q < cur.size(); ++q) {
+        const Blk& B = cur[q];
+        const int p = P.h_pairs[B.k];
+        BaseJob& J = bj[q];
+        J.a_base = P.h_oa[p] + B.i0; J.b_base = P.h_ob[p] + B.j0;
+        J.H = B.i1 - B.i0; J.W = B.j1 - B.j0; J.in_x = B.in_x; J.out_x = B.out_x;
+        J.codes = code_off; code_off += ((int64_t(J.H) + 1) * (int64_t(J.W) + 1) + 15) & ~int64_t(15);
+        J.bnd = bnd_off; bnd_off += 3 * (int64_t(J.W) + 1);
+        J.moves = mv_off; mv_off += int64_t(J.H) + J.W + 1;
+        first[size_t(B.k) + 1] = int64_t(q) + 1;
+    }
+    for (int k = 0; k < n; ++k) first[size_t(k) + 1] = std::max(first[size_t(k) + 1], first[size_t(k)]);
+    Tmp dbj(st), dcodes(st), dbnd(st), dmv(st), dnm(st), dfirst(st);
+    BaseJob* dB = static_cast<BaseJob*>(dbj.get(bj.size() * sizeof(BaseJob)));
+    HB_CUDA(cudaMemcpyAsync(dB, bj.data(), bj.size() * sizeof(BaseJob), cudaMemcpyHostToDevice, st));
+    uint8_t* cd = static_cast<uint8_t*>(dcodes.get(size_t(code_off)));
+    T* bd = static_cast<T*>(dbnd.get(size_t(bnd_off) * sizeof(T)));
+    uint8_t* mvd = static_cast<uint8_t*>(dmv.get(size_t(mv_off)));
+    int32_t* nm = static_cast<int32_t*>(dnm.get(bj.size() * sizeof(int32_t)));
+    int64_t* fd = static_cast<int64_t*>(dfirst.get(first.size() * sizeof(int64_t)));
+    HB_CUDA(cudaMemcpyAsync(fd, first.data(), first.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+    {
+        const int wpb = 4;
+        const int grid = int(std::min<int64_t>((int64_t(bj.size()) + wpb - 1) / wpb, int64_t(sms) * 8));
+        hb_base_kernel<T, R><<<grid, 32 * wpb, mat_bytes, st>>>(P.a, P.b, static_cast<const T*>(P.mat), P.N, gp, dB,
+                                                               int(bj.size()), cd, bd, mvd, nm);
+        HB_CUDA(cudaGetLastError());
+        hb_replay_kernel<T><<<(n + 127) / 128, 128, 0, st>>>(P, dB, fd, mvd, nm, n);
+        HB_CUDA(cudaGetLastError());
+        launches += 2;
+    }
+    HB_CUDA(cudaStreamSynchronize(st));
+    return launches;
+}
+
+}  // namespace
+
+int64_t hb_run(const HbRun& P, int elem_bytes, cudaStream_t st, int sms) {
+    return elem_bytes == 4 ? hb_run_t<float>(P, st, sms) : hb_run_t<double>(P, st, sms);
+}
+
+}  // namespace nwg

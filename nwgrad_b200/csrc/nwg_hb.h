@@ -1,0 +1,32 @@
+// Hirschberg re-alignment on the GPU (nwg_hb.cu): the host driver's interface.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace nwg {
+
+// One Hirschberg run over a set of pairs (affine Global, untracked, one parameter set).
+struct HbRun {
+    // device
+    const uint8_t* a; const uint8_t* b;        // the store's codes
+    const int64_t* oa; const int64_t* ob;      // the store's offsets
+    const int32_t* pairs;                      // the pairs to run
+    const void* mat; int N;                    // N x N in T
+    double go_a, ge_a, go_b, ge_b;             // cast to T as the reference does
+    double* score; int32_t* end;               // per pair
+    double* grad; int64_t gstride;             // per pair, zeroed by the caller (or null)
+    int32_t* guide;                            // per pair m + 1 at oa[p] + p (or null)
+    uint8_t* moves; const int64_t* moves_off;  // keep_paths: walk-order moves (or null)
+    int32_t* path_info;                        // per pair n_moves, start_i, start_j (or null)
+    // host
+    const int32_t* h_pairs; int64_t n_pairs;
+    const int64_t* h_oa; const int64_t* h_ob;
+    int cutoff;                                // rows at which blocks stop splitting (>= 1)
+    int pmax;                                  // the closed-form prefix-max horizontal carry
+};
+
+// Runs P on stream st (synchronising it); returns the number of kernel launches.  Throws
+// std::runtime_error on a CUDA error.
+int64_t hb_run(const HbRun& P, int elem_bytes, cudaStream_t st, int sms);
+
+}  // namespace nwg

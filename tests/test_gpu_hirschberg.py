@@ -1,0 +1,99 @@
+"""Hirschberg re-alignment on the GPU (traceback "hirschberg" / "hirschberg_pmax", affine
+Global): scores, gradients and guides bit for bit against the reference's own engine
+(tests/golden/hirschberg.npz) and against the oracle's restatement on longer pairs."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import AA, encode, has_gpu, mutate, rand_matrix, rand_seqs
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not has_gpu(), reason="needs a CUDA GPU")]
+
+import nwgrad_b200 as nw  # noqa: E402
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _run(prec, tb, cut, mat, gaps, sa, sb):
+    cls = nw.SeqPairBatch if prec == 32 else nw.SeqPairBatchDouble
+    b = cls(sa, sb, nw.AlignParams.from_arrays(mat, gaps, alphabet=AA), grad_mode="hard", traceback=tb)
+    b.hb_cutoff = cut
+    tot = b.score_and_grad()
+    gm, gg = b.grads()
+    flat = np.concatenate([gm.reshape(len(sa), -1), gg.reshape(len(sa), -1)], axis=1)
+    return b.scores(), flat, b.guides(), tot
+
+
+@pytest.mark.parametrize("name", ["int", "flt"])
+@pytest.mark.parametrize("prec", [32, 64])
+@pytest.mark.parametrize("tb", ["hirschberg", "hirschberg_pmax"])
+@pytest.mark.parametrize("cut", [8, 64])
+def test_reference_fixtures(name, prec, tb, cut):
+    z = np.load(os.path.join(GOLD, "hirschberg.npz"))
+    sa, sb = [str(s) for s in z[f"{name}_sa"]], [str(s) for s in z[f"{name}_sb"]]
+    s, g, gj, tot = _run(prec, tb, cut, z[f"{name}_mat"], z[f"{name}_gaps"], sa, sb)
+    key = f"{name}_{tb}_{prec}_c{cut}_"
+    assert np.array_equal(s, z[key + "scores"]), np.nonzero(s != z[key + "scores"])[0][:5]
+    assert np.array_equal(g, z[key + "grads"])
+    assert np.array_equal(gj, z[key + "guides"])
+    assert tot == float(np.cumsum(z[key + "scores"])[-1])
+
+
+@pytest.mark.parametrize("prec", [32, 64])
+@pytest.mark.parametrize("pmax", [False, True])
+def test_long_pairs_against_the_oracle(prec, pmax):
+    """Pairs of 1,000-6,000 residues (several recursion levels, multi-round pipelines) mixed
+    with short pairs that run the Pointers path."""
+    rng = np.random.default_rng(2000 + prec + pmax)
+    mat = rand_matrix(rng, 20, integer=False)
+    gaps = np.array([[3.1, 0.7, 2.9, 0.8]])
+    sa = rand_seqs(rng, 6, 1000, 6000, AA) + rand_seqs(rng, 10, 1, 300, AA)
+    sb = [mutate(rng, s, AA) if k % 3 else rand_seqs(rng, 1, 500, 4000, AA)[0] for k, s in enumerate(sa)]
+    cut = 256
+    s, g, gj, _ = _run(prec, "hirschberg_pmax" if pmax else "hirschberg", cut, mat, gaps, sa, sb)
+    o = oracle.hirschberg(prec, mat, gaps, oracle.Encoded(encode(AA, sa), encode(AA, sb)), cutoff=cut, pmax=pmax)
+    assert np.array_equal(s, o["scores"]), np.nonzero(s != o["scores"])[0][:5]
+    assert np.array_equal(g, o["grads"]), np.nonzero((g != o["grads"]).any(1))[0][:5]
+    assert np.array_equal(gj, o["guides"])
+
+
+def test_score_matches_pointers_and_banded_follows():
+    """Where the optimum is unique Hirschberg and Pointers agree; banded re-alignment then
+    runs around the Hirschberg guide."""
+    rng = np.random.default_rng(2100)
+    mat = rand_matrix(rng, 20, integer=False)
+    gaps = np.array([[3.0, 0.5, 3.0, 0.5]])
+    sa = rand_seqs(rng, 4, 800, 1500, AA)
+    sb = [mutate(rng, s, AA) for s in sa]
+    p = nw.AlignParams.from_arrays(mat, gaps, alphabet=AA)
+    hb = nw.SeqPairBatch(sa, sb, p, grad_mode="hard", traceback="hirschberg")
+    hb.hb_cutoff = 128
+    hb.score_and_grad()
+    pt = nw.SeqPairBatch(sa, sb, p, grad_mode="hard", traceback="pointers")
+    pt.score_and_grad()
+    np.testing.assert_allclose(hb.scores(), pt.scores(), rtol=1e-5)
+    hb.set_params(nw.AlignParams.from_arrays(mat + 1e-3, gaps, alphabet=AA))
+    hb.banded_grad(64)
+    enc = oracle.Encoded(encode(AA, sa), encode(AA, sb))
+    o0 = oracle.hirschberg(32, mat, gaps, enc, cutoff=128)
+    o = oracle.hard(32, 1, 0, mat + 1e-3, gaps, enc, guides_in=o0["guides"], band=64)
+    assert np.array_equal(hb.scores(), o["scores"])
+
+
+def test_errors():
+    rng = np.random.default_rng(2200)
+    mat = rand_matrix(rng, 20)
+    sa = rand_seqs(rng, 2, 600, 700, AA)
+    sb = [mutate(rng, s, AA) for s in sa]
+    neg = nw.AlignParams.from_arrays(mat, [[-1.0, 1.0, 11.0, 1.0]], alphabet=AA)
+    b = nw.SeqPairBatch(sa, sb, neg, grad_mode="hard", traceback="hirschberg")
+    with pytest.raises(ValueError, match="non-negative"):
+        b.score_and_grad()
+    lin = nw.SeqPairBatch(sa, sb, nw.AlignParams.from_arrays(mat, [[11.0, 1.0, 11.0, 1.0]], alphabet=AA),
+                          gap_model="linear", grad_mode="hard", traceback="hirschberg")
+    with pytest.raises(NotImplementedError):
+        lin.score_and_grad()
+    with pytest.raises(ValueError):
+        lin.hb_cutoff = 0
