@@ -340,7 +340,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-fill arm")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving arm")
-    ap.add_argument("--serve-requests", type=int, default=1000)
+    ap.add_argument("--serve-requests", type=int, default=200)
     ap.add_argument("--no-tune", action="store_true", help="the planner's geometries instead of the autotuner's")
     ap.add_argument("--workload", default="c2-soft", choices=["c2-soft", "c1-hard"],
                     help="c2-soft (default): the soft-gradient batch; c1-hard: the plain hard batch (side measurement)")

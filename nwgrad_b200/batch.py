@@ -510,7 +510,7 @@ class SeqPairBatch:
     def params(self) -> AlignParams:
         return self._params.copy()
 
-    def autotune(self, sample_pairs: int = 8192, force: bool = False, verbose: bool = False) -> dict:
+    def autotune(self, sample_pairs: int = 65536, force: bool = False, verbose: bool = False) -> dict:
         """Pick the fastest kernel geometry per size class of this batch (measured on a sample of
         its own pairs, cached per device and problem type) and use it from now on.  Results do
         not change: every geometry computes the same cells.  Returns {size class: (lanes, rows)}."""

@@ -124,8 +124,12 @@ def _key(batch, sc: int) -> str:
                                      batch._params.num_sets, int(batch._tracked), sc))
 
 
-def tune(batch, sample_pairs: int = 8192, force: bool = False, verbose: bool = False, reps: int = 2) -> dict:
-    """{size class: (lanes, rows)} for the classes of ``batch``, measured (or from the cache)."""
+def tune(batch, sample_pairs: int = 65536, force: bool = False, verbose: bool = False, reps: int = 2) -> dict:
+    """{size class: (lanes, rows)} for the classes of ``batch``, measured (or from the cache).
+
+    The sample should fill the device many times over for every candidate (the narrower
+    geometries run several times as many pairs at once): a sample that does not would
+    favour them falsely."""
     grad = {"none": 0, "hard": 1, "soft": 2}[batch._grad_mode]
     cache = _load_cache()
     table = {}
