@@ -342,6 +342,9 @@ def main():
     ap.add_argument("--no-serve", action="store_true", help="skip the serving arm")
     ap.add_argument("--serve-requests", type=int, default=200)
     ap.add_argument("--no-tune", action="store_true", help="the planner's geometries instead of the autotuner's")
+    ap.add_argument("--checkpoint-mb", type=float, default=-1,
+                    help="soft: per-pair forward tables above this many MiB are checkpointed (-1: default)")
+    ap.add_argument("--geometry", default=None, help="LANESxROWS for every pair (no tuning), e.g. 32x4")
     ap.add_argument("--workload", default="c2-soft", choices=["c2-soft", "c1-hard"],
                     help="c2-soft (default): the soft-gradient batch; c1-hard: the plain hard batch (side measurement)")
     args = ap.parse_args()
@@ -393,8 +396,16 @@ def main():
     pos = nw.SeqPairBatch.from_codes(a, oa, bp, obp, params, grad_mode="soft", device=local)
     neg = nw.SeqPairBatch.from_codes(a, oa, bn, obn, params, grad_mode="soft", device=local)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    if args.checkpoint_mb >= 0:
+        for b in (pos, neg):
+            b.set_memory(checkpoint_bytes=int(args.checkpoint_mb * (1 << 20)))
     tune_table = {}
-    if not args.no_tune:
+    if args.geometry:
+        geo = tuple(int(x) for x in args.geometry.lower().split("x"))
+        pos._tune = neg._tune = geo
+        args.no_tune = True
+        tune_table = {"all": geo}
+    elif not args.no_tune:
         tune_table = pos.autotune()
         neg.autotune()
 
@@ -455,6 +466,8 @@ def main():
     value = world * cells * args.steps / (total_ms / 1e3) / 1e9
     plain = None
     if not args.no_plain:
+        saved = pos._tune
+        pos._tune = neg._tune = (0, 0)
         pos.use_plain_fill()
         neg.use_plain_fill()
         p_total, p_steps, p_kms, p_launch, _ = timed(False)
@@ -462,6 +475,7 @@ def main():
                  "ms_per_step": p_total / args.steps, "kernel_ms_per_step": p_kms / args.steps,
                  "geometry": "32 lanes x 4 rows for every pair, one launch per size bucket",
                  "tuned_over_plain": (value / (world * cells * args.steps / (p_total / 1e3) / 1e9))}
+        pos._tune = neg._tune = saved
         if not args.no_tune:
             pos.autotune()
             neg.autotune()
@@ -478,7 +492,9 @@ def main():
             t0 = time.perf_counter()
             p_ = nw.SeqPairBatch.from_codes(a, oa, bp, obp, params, grad_mode="soft", device=local)
             n_ = nw.SeqPairBatch.from_codes(a, oa, bn, obn, params, grad_mode="soft", device=local)
-            if not args.no_tune:
+            if args.geometry:
+                p_._tune = n_._tune = pos._tune
+            elif not args.no_tune:
                 p_.autotune()
                 n_.autotune()
             s = p_.score_and_grad() - n_.score_and_grad()

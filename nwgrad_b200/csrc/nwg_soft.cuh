@@ -27,9 +27,10 @@
 // Accumulation: each lane keeps its rows' substitution counts in shared memory, laid out
 // [b][lane][row] so one step's R rows update one contiguous R-vector (one 128-bit load and
 // store for R = 4) without conflicts; they are folded into the pair's histogram at the end
-// of every stripe.  Gap counts (untracked) accumulate per step in registers and per pair in
-// double; tracked gap counts per parameter set in shared memory.  log Z and the per-step
-// scale factors 2^(E_F + E_B - E_Z) are formed in double.
+// of every stripe.  Gap counts (untracked) accumulate in T per lane and stripe and per pair in
+// double; tracked gap counts per parameter set in shared memory (double).  log Z is formed in
+// double; the per-step scale factor 2^(E_F + E_B - E_Z) / Z is an exact power of two times
+// 1 / zhat in T.
 #pragma once
 #include "nwg_common.cuh"
 
@@ -392,6 +393,7 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
         const int EZ = ze + ilog2(zm);
         const double zhat = zm * pow2i<double>(ze - EZ);
         const double invz = 1.0 / zhat;
+        const T invzT = static_cast<T>(invz);
 
         // ── backward, fused with the expected counts ─────────────────────────
         double ga_o = 0, ga_x = 0, gb_o = 0, gb_x = 0;   // untracked: opens and extend-only moves
@@ -426,6 +428,7 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
             }
             int EB = 0;
             T lone = T(1);
+            T sgb_o = T(0), sga_o = T(0), sgb_x = T(0), sga_x = T(0);   // untracked: this stripe's gap sums
             T dgM = T(0);                             // row below, column j+1 (BM only)
             T dnM = T(0), dnX = T(0), dnY = T(0);     // row below, column j
             const T* fs = fwd + (ck ? 0 : int64_t(s) * S * G * CV);
@@ -470,9 +473,10 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
                         nEF = fe[int64_t(j - 1 + lane) * G + lane];
                         nbj = int(bp[j - 1]);
                     }
-                    // scale of this step's products: 2^(E_F + E_B - E_Z) / zhat
-                    const double facd = pow2i<double>(EF + EB - EZ) * invz;
-                    const T fac = static_cast<T>(facd);
+                    // scale of this step's products: 2^(E_F + E_B - E_Z) / zhat (an exact power of
+                    // two times 1 / zhat rounded to T)
+                    const double facd = TR ? pow2i<double>(EF + EB - EZ) * invz : 0.0;
+                    const T fac = TR ? static_cast<T>(facd) : pow2i<T>(EF + EB - EZ) * invzT;
                     if (!is_finite(fac)) bad = true;
                     T dM = dgM;                       // row below, column j+1
                     T xM = dnM, xX = dnX, xY = dnY;   // row below, column j
@@ -546,11 +550,11 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
                     }
                     if constexpr (!TR) {
                         if constexpr (AFF) {
-                            gb_o = fma(static_cast<double>(so_b), facd, gb_o);
-                            ga_o = fma(static_cast<double>(so_a), facd, ga_o);
+                            sgb_o = fmaf_t(so_b, fac, sgb_o);
+                            sga_o = fmaf_t(so_a, fac, sga_o);
                         }
-                        gb_x = fma(static_cast<double>(sx_b), facd, gb_x);
-                        ga_x = fma(static_cast<double>(sx_a), facd, ga_x);
+                        sgb_x = fmaf_t(sx_b, fac, sgb_x);
+                        sga_x = fmaf_t(sx_a, fac, sga_x);
                     }
                     dgM = dnM;
                     if ((t & rmask) == 0 || j == 0) {
@@ -598,6 +602,10 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
                     bbndE[j] = EB;
                 }
             }
+            if constexpr (!TR) {   // the stripe's gap sums into the pair's (double)
+                gb_o += static_cast<double>(sgb_o); ga_o += static_cast<double>(sga_o);
+                gb_x += static_cast<double>(sgb_x); ga_x += static_cast<double>(sga_x);
+            }
             // fold this stripe's per-lane substitution counts into the pair's histogram (one
             // lane per pair: straight into the pair's gradient, zeroed before the pass)
             if constexpr (G == 1) {
@@ -613,21 +621,24 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
                 }
             }
             if constexpr (G > 1) {
-                // lane by lane, so the sum's order (and bits) never depends on scheduling
+                // lane c adds column c of every (lane, row) accumulator, in (lane, row) order:
+                // the sum's order (and bits) never depends on scheduling, and the group's lanes
+                // work on distinct histogram entries at once
+                __syncwarp(gmask);
                 for (int l = 0; l < G; ++l) {
-                    if (lane == l) {
 #pragma unroll
-                        for (int r = 0; r < R; ++r) {
-                            if (krow[r] >= K * N) continue;
-                            for (int c = 0; c < N; ++c) {
-                                T& v = macc[(size_t(c) * G + lane) * R + r];
-                                hist[krow[r] * N + c] += v;
+                    for (int r = 0; r < R; ++r) {
+                        const int kr = __shfl_sync(gmask, krow[r], l, G);
+                        if (kr < K * N) {
+                            for (int c = lane; c < N; c += G) {
+                                T& v = macc[(size_t(c) * G + l) * R + r];
+                                hist[kr * N + c] += v;
                                 v = T(0);
                             }
                         }
                     }
-                    __syncwarp(gmask);
                 }
+                __syncwarp(gmask);
             }
         }
         if constexpr (G > 1) bad = __any_sync(gmask, bad);
