@@ -178,6 +178,13 @@ template <class T> SoftFn soft_fn_rt(bool aff, bool loc, bool tr, Geo g) {
     return sizeof(T) == 4 ? nwg::soft_fn_f32(aff, loc, tr, g) : nwg::soft_fn_f64(aff, loc, tr, g);
 }
 
+// The kernel geometries (lanes per pair G, rows per lane R) each path is instantiated for.
+bool geo_available(bool soft, int G, int R) {
+    if (G == 1) return R == 8 || R == 16 || R == 24 || R == 32;
+    if (soft) return (G == 32 && (R == 2 || R == 4)) || (G == 16 && (R == 2 || R == 4)) || (G == 8 && R == 4);
+    return G == 32 && (R == 1 || R == 2 || R == 4 || R == 8);
+}
+
 // Padded cells a geometry computes for an (m, n) problem over `rows` DP rows.
 double geo_cost(Geo g, int rows, int n, int extra_cols) {
     const int GR = g.G * g.R;
@@ -187,21 +194,24 @@ double geo_cost(Geo g, int rows, int n, int extra_cols) {
 
 // The geometry for one pair: a lane per pair when the rows fit one lane (up to 32 rows),
 // else the warp geometry that pads the fewest cells (ties: more rows per lane).
+// lanes / rpl > 0 force the lanes per pair / rows per lane (the tuner's measurements).
 Geo pick_geo(bool soft, int rows, int n, int lanes, int rpl, bool lane_ok) {
     if (lanes == 1 || (lanes == 0 && lane_ok && rows <= 32)) {
         int R = rpl;
         if (!R) R = rows <= 8 ? 8 : rows <= 16 ? 16 : rows <= 24 ? 24 : 32;
         return {1, R};
     }
-    if (rpl) return {32, rpl};
-    Geo best{32, soft ? 4 : 4};
+    const int G = lanes > 1 ? lanes : 32;
+    if (rpl) return {G, rpl};
+    Geo best{G, 4};
     double bc = 1e300;
     const int opts_h[] = {8, 4, 2, 1};
     const int opts_s[] = {4, 2};
     const int* opts = soft ? opts_s : opts_h;
     const int no = soft ? 2 : 4;
     for (int k = 0; k < no; ++k) {
-        const Geo g{32, opts[k]};
+        const Geo g{G, opts[k]};
+        if (!geo_available(soft, g.G, g.R)) continue;
         // fewer rows per lane costs more shuffles per cell: weigh them in
         const double c = geo_cost(g, rows, n, soft ? 1 : 0) * (1.0 + 0.75 / g.R);
         if (c < bc) { bc = c; best = g; }
@@ -218,12 +228,7 @@ int size_class(int rows, int n) {
     return std::max(20, int(std::ceil(std::log2(cells))));
 }
 
-// The kernel geometries (lanes per pair G, rows per lane R) each path is instantiated for.
-bool geo_available(bool soft, int G, int R) {
-    if (G == 1) return R == 8 || R == 16 || R == 24 || R == 32;
-    if (soft) return (G == 32 && (R == 2 || R == 4)) || (G == 16 && (R == 2 || R == 4)) || (G == 8 && R == 4);
-    return G == 32 && (R == 1 || R == 2 || R == 4 || R == 8);
-}
+
 
 struct Bucket {
     Geo geo;

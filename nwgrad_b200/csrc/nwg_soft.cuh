@@ -236,10 +236,22 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
             T* fs = fwd + (ck ? 0 : int64_t(s) * S * G * CV);
             int* fe = fexp + (ck ? 0 : int64_t(s) * S * G);
             int nbj = N;
+            // lane 0: the row above (the previous stripe's bottom row) one column ahead, so
+            // the load is in flight while the current column is computed
+            T nuM = T(0), nuX = T(0), nuY = T(0); int nuE = 0;
+            auto fetch_up = [&](int jj) {
+                if (lane == 0 && s > 0 && jj <= n) {
+                    nuE = fbE_in[jj]; nuM = fb_in[NV * jj];
+                    if constexpr (AFF) { nuX = fb_in[NV * jj + 1]; nuY = fb_in[NV * jj + 2]; }
+                }
+            };
+            fetch_up(0);
             for (int t = 0; t < S; ++t) {
                 const int j = t - lane;           // column 0..n
                 if (lane == 0 && j <= n && s > 0) {
-                    const int eb = fbE_in[j];
+                    const int eb = nuE;
+                    const T ubM = nuM, ubX = nuX, ubY = nuY;
+                    fetch_up(j + 1);
                     int d = eb - E;
                     if (d > kLift) {   // keep the incoming values in range: move own state down
                         const T f = pow2i<T>(kLift - d);
@@ -249,8 +261,8 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
                         E = eb - kLift; lone = pow2i<T>(-E); d = kLift;
                     }
                     const T f = pow2i<T>(d);
-                    upM = fb_in[NV * j] * f;
-                    if constexpr (AFF) { upX = fb_in[NV * j + 1] * f; upY = fb_in[NV * j + 2] * f; }
+                    upM = ubM * f;
+                    if constexpr (AFF) { upX = ubX * f; upY = ubY * f; }
                 }
                 const bool active = (j >= 0) && (j <= n);
                 if (active) {
@@ -436,10 +448,21 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
             T nf[CV];
             int nEF = 0, nbj = N;
             bool have_next = false;
+            // lane G-1: the row below (the next stripe's top row) one column ahead
+            T ndM = T(0), ndX = T(0), ndY = T(0); int ndE = 0;
+            auto fetch_dn = [&](int jj) {
+                if (lane == G - 1 && s < nstripes - 1 && jj >= 0) {
+                    ndE = bbndE[jj]; ndM = bbnd[NV * jj];
+                    if constexpr (AFF) { ndX = bbnd[NV * jj + 1]; ndY = bbnd[NV * jj + 2]; }
+                }
+            };
+            fetch_dn(n);
             for (int t = 0; t < S; ++t) {
                 const int j = n - t + (G - 1 - lane);     // column n..0
                 if (lane == G - 1 && j >= 0 && s < nstripes - 1) {
-                    const int eb = bbndE[j];
+                    const int eb = ndE;
+                    const T dbM = ndM, dbX = ndX, dbY = ndY;
+                    fetch_dn(j - 1);
                     int d = eb - EB;
                     if (d > kLift) {
                         const T f = pow2i<T>(kLift - d);
@@ -449,8 +472,8 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
                         EB = eb - kLift; lone = pow2i<T>(-EB); d = kLift;
                     }
                     const T f = pow2i<T>(d);
-                    dnM = bbnd[NV * j] * f;
-                    if constexpr (AFF) { dnX = bbnd[NV * j + 1] * f; dnY = bbnd[NV * j + 2] * f; }
+                    dnM = dbM * f;
+                    if constexpr (AFF) { dnX = dbX * f; dnY = dbY * f; }
                     else { dnX = dnM; dnY = dnM; }
                 }
                 const bool active = (j >= 0) && (j <= n);
