@@ -219,6 +219,11 @@ Geo pick_geo(bool soft, int rows, int n, int lanes, int rpl, bool lane_ok) {
     return best;
 }
 
+// Soft pairs of at least this many DP rows run with several warps per pair (a pipeline over
+// the pair's stripes) instead of one: a long pair is then not a single warp's serial work.
+constexpr int kLongRows = 1536;
+constexpr int kLongWarps = 4;
+
 // Pairs are bucketed by geometry and by size class: the binary order of magnitude of the DP
 // (rows x columns), with everything up to 2^20 cells in one class.  Small pairs share a
 // launch (their scratch strides are small anyway); large pairs get a bucket per doubling, so
@@ -351,13 +356,14 @@ void build_plan(nwg_store* s, Plan& P, bool soft, int lanes, int rpl, int elem_b
         Geo g = band ? Geo{32, 2, true} : pick_geo(soft, std::max(rows, 1), nb, lanes, rpl, soft ? lane_ok_soft : true);
         if (!band && !lanes && !rpl) {
             if (s->plain) g = Geo{32, 4};
+            else if (soft && !s->tracked() && rows >= kLongRows && nb >= 256) g = Geo{32, 4, false, kLongWarps};
             else {
                 auto it = s->geo_table.find({int(soft), sc});
                 if (it != s->geo_table.end() && (!soft || it->second.first > 1 || lane_ok_soft))
                     g = Geo{it->second.first, it->second.second};
             }
         }
-        auto key = std::make_tuple(g.G, g.R, sc);
+        auto key = std::make_tuple(g.G, g.R * 100 + g.mw, sc);
         auto itb = idx.find(key);
         int bi;
         if (itb == idx.end()) { bi = int(P.buckets.size()); idx[key] = bi; P.buckets.push_back(Bucket{g, {}, 0, 0, 0}); }
@@ -652,12 +658,13 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
         SoftFn fn = soft_fn_rt<T>(aff, loc, tr, B.geo);
         if (!fn) throw Error(NWG_EINVAL, "no soft kernel for this geometry");
         const int G = B.geo.G;
-        int block = 128;
+        const bool mw = B.geo.mw > 1;            // several warps per pair (long pairs)
+        int block = mw ? 32 * B.geo.mw : 128;
         const int K = s->K, N = s->N;
         auto smem_for = [&](int blk) {
-            return nwg::soft_smem_bytes(K, N, G, B.geo.R, blk, int(sizeof(T)), tr);
+            return nwg::soft_smem_bytes(K, N, G, B.geo.R, blk, int(sizeof(T)), tr, mw);
         };
-        while (block > 32 && smem_for(block) > 96 * 1024) block /= 2;
+        while (!mw && block > 32 && smem_for(block) > 96 * 1024) block /= 2;
         const size_t smem = smem_for(block);
         if (smem > 227 * 1024) throw Error(NWG_EINVAL, "soft: the alphabet / parameter sets do not fit shared memory");
         if (smem > 48 * 1024) NWG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
@@ -671,17 +678,21 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
         const int64_t GRb = int64_t(G) * B.geo.R;
         const int64_t nb1 = int64_t(B.maxn) + 1;
         const int64_t max_stripes = (B.max_rows + GRb - 1) / GRb;
-        const bool ck = B.max_soft_cells * NV * int64_t(sizeof(T)) > s->ck_threshold;
+        const bool ck = mw || B.max_soft_cells * NV * int64_t(sizeof(T)) > s->ck_threshold;
         const int64_t tab_cells = ck ? (nb1 + G) * GRb : B.max_soft_cells;
         const int64_t fwd_bytes = ((tab_cells * NV * int64_t(sizeof(T))) + 255) & ~int64_t(255);
         const int64_t exp_bytes = ((tab_cells / B.geo.R) * 4 + 255) & ~int64_t(255);
         const int64_t nbrows = ck ? max_stripes : 1;
-        const int64_t bnd_bytes = nb1 * (nbrows + 1) * (NV * int64_t(sizeof(T)) + 4);
-        const int64_t stride = ((fwd_bytes + exp_bytes + bnd_bytes) + 255) & ~int64_t(255);
+        const int64_t nbrows_b = mw ? max_stripes : 1;
+        const int64_t bnd_bytes = nb1 * (nbrows + nbrows_b) * (NV * int64_t(sizeof(T)) + 4);
+        const int64_t warp_bytes = fwd_bytes + exp_bytes;
+        // a slot: one group's table and boundary rows, or (several warps per pair) one block's
+        const int64_t stride = (((mw ? gpb : 1) * warp_bytes + bnd_bytes) + 255) & ~int64_t(255);
+        const int64_t per_block = mw ? stride : stride * gpb;
         // as many resident groups as fit the device (occupancy) and the scratch budget
-        int64_t blocks = std::min<int64_t>((items + gpb - 1) / gpb, int64_t(sms) * occ);
-        blocks = std::max<int64_t>(1, std::min<int64_t>(blocks, s->scratch_budget / std::max<int64_t>(1, stride * gpb)));
-        const int64_t slots = blocks * gpb;
+        int64_t blocks = std::min<int64_t>(mw ? items : (items + gpb - 1) / gpb, int64_t(sms) * occ);
+        blocks = std::max<int64_t>(1, std::min<int64_t>(blocks, s->scratch_budget / std::max<int64_t>(1, per_block)));
+        const int64_t slots = mw ? blocks : blocks * gpb;
         s->scratch.need(size_t(slots * stride), st);
         nwg::SoftArgs A{};
         A.a = s->a.as<uint8_t>(); A.oa = s->doa.as<int64_t>();
@@ -692,7 +703,9 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
         A.w = dw.p; A.gw = dgw.p; A.N = N; A.K = K;
         A.scratch = s->scratch.p; A.scratch_stride = stride; A.fwd_bytes = fwd_bytes;
         A.maxn = B.maxn; A.temperature = J.temperature;
-        A.ck = ck; A.max_stripes = int(std::max<int64_t>(max_stripes, 1)); A.bnd_off = fwd_bytes + exp_bytes;
+        A.ck = ck; A.max_stripes = int(std::max<int64_t>(max_stripes, 1));
+        A.warp_stride = mw ? warp_bytes : 0;
+        A.bnd_off = (mw ? gpb : 1) * warp_bytes;
         A.renorm_mask = renorm - 1;
         A.score = s->score.as<double>(); A.grad = s->grad.as<double>(); A.gstride = s->gstride;
         A.status = s->status.as<int32_t>();
@@ -721,7 +734,12 @@ void run_soft(nwg_store* s, const nwg_job& J, cudaStream_t st) {
     if (s->n) NWG_CUDA(cudaMemcpyAsync(s->h_status.data(), s->status.p, size_t(s->n) * 4, cudaMemcpyDeviceToHost, st));
     NWG_CUDA(cudaStreamSynchronize(st));
     std::vector<int32_t> refused;
-    for (int64_t p = 0; p < s->n; ++p) if (s->h_status[p]) refused.push_back(int32_t(p));
+    for (int64_t p = 0; p < s->n; ++p) {
+        if (s->h_status[p] == 3)
+            throw Error(NWG_ECUDA, "nwgrad_b200: soft pass: a wait between the warps of pair " + std::to_string(p) +
+                                   " ran out (the kernel gave up instead of hanging)");
+        if (s->h_status[p]) refused.push_back(int32_t(p));
+    }
     if (!refused.empty()) {
         if (f32) {
             soft_pass<double>(s, J, st, &refused);

@@ -52,6 +52,8 @@ struct SoftArgs {
                                              // backward (the table then holds one stripe)
     int max_stripes;                         // ck: stripes the boundary rows are sized for
     int64_t bnd_off;                         // bytes from a slot's start to its boundary rows
+    int64_t warp_stride;                     // several warps per pair: bytes of one warp's table
+                                             // and exponents (each warp recomputes its stripes)
     int renorm_mask;                         // renormalise when (step & renorm_mask) == 0
     double temperature;
     double* score; double* grad; int64_t gstride;
@@ -116,7 +118,8 @@ __device__ __forceinline__ void vload(T (&v)[NV], const T* src) {
 }
 
 // Bytes of dynamic shared memory the soft kernel needs for a block of `block` threads.
-__host__ __device__ inline size_t soft_smem_bytes(int K, int N, int G, int R, int block, int tsize, bool tracked) {
+__host__ __device__ inline size_t soft_smem_bytes(int K, int N, int G, int R, int block, int tsize, bool tracked,
+                                                  bool multiwarp = false) {
     const int gpb = block / G;
     size_t b = size_t((K * N + 1) * (N + 1) + 4 * K) * tsize;
     b = (b + 15) & ~size_t(15);
@@ -124,11 +127,19 @@ __host__ __device__ inline size_t soft_smem_bytes(int K, int N, int G, int R, in
     if (G > 1) b += size_t(K) * N * N * tsize * gpb;        // per-group histogram
     b = (b + 15) & ~size_t(15);
     if (tracked) b += size_t(4) * K * 8 * block;            // per-lane tracked gap sums
+    if (multiwarp) b += size_t(gpb) * 8 * 8 + size_t(gpb) * 4 + 16;   // per-warp partials, progress
     return b;
 }
 
-template <class T, bool AFF, bool LOC, bool TR, int G, int R>
+// Several warps per pair (long pairs): warp w fills stripes w, w + NW, ... and waits, every 32
+// steps, until the warp filling the stripe above (below, in the backward pass) has published
+// enough progress.  The wait is bounded: past kSpinLimit polls the pair is marked failed
+// (status 3) and every warp finishes the pass without waiting further.
+constexpr int kSpinLimit = 1 << 22;
+
+template <class T, bool AFF, bool LOC, bool TR, int G, int R, bool MW = false>
 __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftArgs A) {
+    static_assert(!MW || (G == 32 && !TR), "several warps per pair: 32 lanes, untracked");
     constexpr int GR = G * R;
     constexpr int NV = AFF ? 3 : 1;          // values per cell
     constexpr int CV = NV * R;               // values per lane column
@@ -145,12 +156,15 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
     T* hist_all = macc_all + size_t(N + 1) * GR * gpb;
     double* tg_all = reinterpret_cast<double*>(
         (reinterpret_cast<uintptr_t>(hist_all + (G > 1 ? size_t(K) * N * N * gpb : 0)) + 15) & ~uintptr_t(15));
+    double* cpart = tg_all + (TR ? size_t(4) * K * blockDim.x : 0);        // MW: [warp][8] partials
+    volatile int* prog = reinterpret_cast<volatile int*>(cpart + (MW ? 8 * gpb : 0));   // MW: per warp
     for (int k = threadIdx.x; k < nw; k += blockDim.x) sw[k] = static_cast<const T*>(A.w)[k];
     for (int k = threadIdx.x; k < 4 * K; k += blockDim.x) sgw[k] = static_cast<const T*>(A.gw)[k];
 
     const int lane = threadIdx.x % G;
     const int gib = threadIdx.x / G;
-    const int64_t slot = int64_t(blockIdx.x) * gpb + gib;
+    const int64_t slot = MW ? int64_t(blockIdx.x) : int64_t(blockIdx.x) * gpb + gib;
+    const int NWp = MW ? gpb : 1;                            // warps per pair
     T* macc = macc_all + size_t(N + 1) * GR * gib;          // [b][lane][r]
     T* hist = hist_all + size_t(K) * N * N * gib;
     double* tg = tg_all + size_t(4) * K * threadIdx.x;        // tracked gap sums of this lane
@@ -165,20 +179,42 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
     const int rmask = A.renorm_mask;
 
     unsigned char* sbase = static_cast<unsigned char*>(A.scratch) + slot * A.scratch_stride;
-    T* fwd = reinterpret_cast<T*>(sbase);
-    int* fexp = reinterpret_cast<int*>(sbase + A.fwd_bytes);
+    T* fwd = reinterpret_cast<T*>(sbase + (MW ? gib * A.warp_stride : 0));
+    int* fexp = reinterpret_cast<int*>(reinterpret_cast<unsigned char*>(fwd) + A.fwd_bytes);
     const int64_t nb = int64_t(A.maxn) + 1;
-    const bool ck = A.ck != 0;
+    const bool ck = MW || A.ck != 0;
     const int nbrows = ck ? A.max_stripes : 1;              // forward boundary rows kept
+    const int nbrows_b = MW ? A.max_stripes : 1;            // backward boundary rows kept
     unsigned char* bb = sbase + A.bnd_off;
     T* fbnd = reinterpret_cast<T*>(bb);                      // [nbrows][NV * nb]
-    T* bbnd = fbnd + NV * nb * nbrows;                       // [NV * nb]
-    int* fbndE = reinterpret_cast<int*>(bbnd + NV * nb);     // [nbrows][nb]
-    int* bbndE = fbndE + nb * nbrows;                        // [nb]
+    T* bbnd = fbnd + NV * nb * nbrows;                       // [nbrows_b][NV * nb]
+    int* fbndE = reinterpret_cast<int*>(bbnd + NV * nb * nbrows_b);   // [nbrows][nb]
+    int* bbndE = fbndE + nb * nbrows;                        // [nbrows_b][nb]
+    const int pw = (gib + NWp - 1) % NWp;                    // MW: the warp of the neighbouring stripe
+    // MW: wait until the neighbouring stripe's warp has published `target` (bounded)
+    bool stalled = false;
+    auto wait_for = [&](int target) {
+        if constexpr (MW) {
+            int k = 0;
+            while (!stalled && prog[pw] < target) {
+                if (++k > kSpinLimit) stalled = true;
+                else __nanosleep(64);
+            }
+            __syncwarp();
+            __threadfence_block();
+        }
+    };
+    auto publish = [&](int v) {
+        if constexpr (MW) {
+            __syncwarp();
+            __threadfence_block();
+            if (lane == 0) prog[gib] = v;
+        }
+    };
     // untracked: the one set's gap weights
     const T oa0 = sgw[0], ea0 = sgw[1], ob0 = sgw[2], eb0 = sgw[3];
 
-    for (int64_t it = slot; it < A.n_items; it += int64_t(gridDim.x) * gpb) {
+    for (int64_t it = slot; it < A.n_items; it += MW ? int64_t(gridDim.x) : int64_t(gridDim.x) * gpb) {
         const int p = A.order[it];
         const int64_t ao = A.oa[p], bo = A.ob[p];
         const int m = int(A.oa[p + 1] - ao), n = int(A.ob[p + 1] - bo);
@@ -195,7 +231,12 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
         const int rows = m + 1;                 // DP rows 0..m
         const int nstripes = (rows + GR - 1) / GR;
         const int S = n + G;                    // steps: columns 0..n plus the skew
+        const int SP = S + 1;                   // MW: progress key per stripe
         bool bad = false;
+        if constexpr (MW) {
+            if (lane == 0) prog[gib] = -1;
+            __syncthreads();
+        }
 
         // ── forward ──────────────────────────────────────────────────────────
         XAcc zacc; zacc.init();                 // Local: the sum over every cell
@@ -245,9 +286,15 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
                     if constexpr (AFF) { nuX = fb_in[NV * jj + 1]; nuY = fb_in[NV * jj + 2]; }
                 }
             };
+            // MW: the stripe above has written column c by its step c + G - 1; lane 0 reads
+            // columns t .. t + 32 in the next 32 steps
+            const bool waits = MW && pass1 && s > 0;
+            if (waits) wait_for((s - 1) * SP + min(S, 2 * G + 1));
             fetch_up(0);
             for (int t = 0; t < S; ++t) {
                 const int j = t - lane;           // column 0..n
+                if (waits && t > 0 && (t & 31) == 0) wait_for((s - 1) * SP + min(S, t + 2 * G + 1));
+                if (MW && pass1 && t > 0 && (t & 7) == 0) publish(s * SP + t);   // steps 0 .. t-1 done
                 if (lane == 0 && j <= n && s > 0) {
                     const int eb = nuE;
                     const T ubM = nuM, ubX = nuX, ubY = nuY;
@@ -362,6 +409,7 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
                     fbE_out[j] = E;
                 }
             }
+            if (MW && pass1) publish(s * SP + S);
             if (pass1) {
                 if constexpr (LOC) { zacc.add(static_cast<double>(zpart), E); }
                 if constexpr (!LOC) {
@@ -374,7 +422,7 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
             }
             if constexpr (G > 1) __syncwarp(gmask);
         };
-        for (int s = 0; s < nstripes; ++s) fwd_stripe(s, true);
+        for (int s = MW ? gib : 0; s < nstripes; s += NWp) fwd_stripe(s, true);
         // Z = zhat * 2^EZ with zhat in [1, 2)
         double zm; int ze;
         if constexpr (LOC) {
@@ -398,8 +446,35 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
             }
         }
         if constexpr (G > 1) bad = __any_sync(gmask, bad);
+        if constexpr (MW) {
+            // every warp's part of Z: Global, the warp holding row m; Local, the sum in warp order
+            stalled = __any_sync(gmask, stalled);
+            if (lane == 0) {
+                cpart[8 * gib + 0] = zm; cpart[8 * gib + 1] = double(ze);
+                cpart[8 * gib + 2] = bad ? 1.0 : 0.0; cpart[8 * gib + 3] = stalled ? 1.0 : 0.0;
+            }
+            __syncthreads();
+            bool anybad = false, anystall = false;
+            if constexpr (LOC) {
+                XAcc za; za.init();
+                for (int w = 0; w < NWp; ++w) za.add(cpart[8 * w], int(cpart[8 * w + 1]));
+                zm = za.m; ze = za.e;
+            } else {
+                const int ow = (nstripes - 1) % NWp;
+                zm = cpart[8 * ow]; ze = int(cpart[8 * ow + 1]);
+            }
+            for (int w = 0; w < NWp; ++w) { anybad |= cpart[8 * w + 2] != 0.0; anystall |= cpart[8 * w + 3] != 0.0; }
+            bad = anybad; stalled = anystall;
+            if (lane == 0) prog[gib] = -1;
+            __syncthreads();
+            if (stalled) {
+                if (threadIdx.x == 0) { A.status[p] = 3; A.score[p] = 0.0; }
+                stalled = false;
+                continue;
+            }
+        }
         if (!(zm > 0.0) || !(zm < 1e300) || bad) {
-            if (lane == 0) { A.status[p] = 1; A.score[p] = 0.0; }
+            if (lane == 0 && (!MW || gib == 0)) { A.status[p] = 1; A.score[p] = 0.0; }
             continue;
         }
         const int EZ = ze + ilog2(zm);
@@ -413,8 +488,14 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
             double* g1 = A.grad + A.gstride * p;
             for (int k = 0; k < K * N * N; ++k) g1[k] = 0.0;
         }
-        for (int s = nstripes - 1; s >= 0; --s) {
+        for (int s = nstripes - 1 - (MW ? gib : 0); s >= 0; s -= NWp) {
             if (ck) fwd_stripe(s, false);       // this stripe's forward table, from its checkpoint
+            // this stripe's row below (read) and its own top row (written): MW keeps one per stripe
+            T* const bb_in = bbnd + (MW ? int64_t(s + 1) * NV * nb : 0);
+            int* const bbE_in = bbndE + (MW ? int64_t(s + 1) * nb : 0);
+            T* const bb_out = bbnd + (MW ? int64_t(s) * NV * nb : 0);
+            int* const bbE_out = bbndE + (MW ? int64_t(s) * nb : 0);
+            const int bkey = nstripes - 1 - s;   // MW: progress keys grow as the pass goes up
             const int i0 = s * GR + lane * R;
             int keyd[R], krow[R];
             T roa[TR ? R : 1], rea[TR ? R : 1], rob[TR ? R : 1], reb[TR ? R : 1];   // rob/reb: row i+1
@@ -452,13 +533,19 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
             T ndM = T(0), ndX = T(0), ndY = T(0); int ndE = 0;
             auto fetch_dn = [&](int jj) {
                 if (lane == G - 1 && s < nstripes - 1 && jj >= 0) {
-                    ndE = bbndE[jj]; ndM = bbnd[NV * jj];
-                    if constexpr (AFF) { ndX = bbnd[NV * jj + 1]; ndY = bbnd[NV * jj + 2]; }
+                    ndE = bbE_in[jj]; ndM = bb_in[NV * jj];
+                    if constexpr (AFF) { ndX = bb_in[NV * jj + 1]; ndY = bb_in[NV * jj + 2]; }
                 }
             };
+            // MW: the stripe below has written column c by its step n - c + G - 1; lane G-1
+            // reads columns n - t .. n - t - 32 in the next 32 steps
+            const bool bwaits = MW && s < nstripes - 1;
+            if (bwaits) wait_for((bkey - 1) * SP + min(S, 2 * G + 1));
             fetch_dn(n);
             for (int t = 0; t < S; ++t) {
                 const int j = n - t + (G - 1 - lane);     // column n..0
+                if (bwaits && t > 0 && (t & 31) == 0) wait_for((bkey - 1) * SP + min(S, t + 2 * G + 1));
+                if (MW && t > 0 && (t & 7) == 0) publish(bkey * SP + t);
                 if (lane == G - 1 && j >= 0 && s < nstripes - 1) {
                     const int eb = ndE;
                     const T dbM = ndM, dbX = ndX, dbY = ndY;
@@ -620,11 +707,12 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
                     }
                 }
                 if (lane == 0 && active && s > 0) {
-                    bbnd[NV * j] = bM[0];
-                    if constexpr (AFF) { bbnd[NV * j + 1] = bX[0]; bbnd[NV * j + 2] = bY[0]; }
-                    bbndE[j] = EB;
+                    bb_out[NV * j] = bM[0];
+                    if constexpr (AFF) { bb_out[NV * j + 1] = bX[0]; bb_out[NV * j + 2] = bY[0]; }
+                    bbE_out[j] = EB;
                 }
             }
+            if constexpr (MW) publish(bkey * SP + S);
             if constexpr (!TR) {   // the stripe's gap sums into the pair's (double)
                 gb_o += static_cast<double>(sgb_o); ga_o += static_cast<double>(sga_o);
                 gb_x += static_cast<double>(sgb_x); ga_x += static_cast<double>(sga_x);
@@ -676,7 +764,44 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
         }
         double* g = A.grad + A.gstride * p;
         const int64_t NN = int64_t(K) * N * N;
-        if (bad) {
+        if constexpr (MW) {
+            // the pair's totals: every warp's histogram and gap sums, added in warp order
+            stalled = __any_sync(gmask, stalled);
+            if (lane == 0) {
+                cpart[8 * gib + 0] = ga_o; cpart[8 * gib + 1] = ga_x;
+                cpart[8 * gib + 2] = gb_o; cpart[8 * gib + 3] = gb_x;
+                cpart[8 * gib + 4] = bad ? 1.0 : 0.0; cpart[8 * gib + 5] = stalled ? 1.0 : 0.0;
+            }
+            __syncthreads();
+            double to_a = 0, tx_a = 0, to_b = 0, tx_b = 0;
+            bool anybad = false, anystall = false;
+            for (int w = 0; w < NWp; ++w) {
+                to_a += cpart[8 * w + 0]; tx_a += cpart[8 * w + 1];
+                to_b += cpart[8 * w + 2]; tx_b += cpart[8 * w + 3];
+                anybad |= cpart[8 * w + 4] != 0.0; anystall |= cpart[8 * w + 5] != 0.0;
+            }
+            if (anystall || anybad) {
+                if (threadIdx.x == 0) { A.status[p] = anystall ? 3 : 1; A.score[p] = 0.0; }
+            } else {
+                for (int k = threadIdx.x; k < K * N * N; k += blockDim.x) {
+                    double v = 0.0;
+                    for (int w = 0; w < NWp; ++w) v += static_cast<double>(hist_all[size_t(K) * N * N * w + k]);
+                    g[k] = v;
+                }
+                if (threadIdx.x == 0) {
+                    const double cga_o = AFF ? static_cast<double>(oa0) * to_a : 0.0;
+                    const double cgb_o = AFF ? static_cast<double>(ob0) * to_b : 0.0;
+                    g[NN + 0] = 0.0 - cga_o;
+                    g[NN + 1] = 0.0 - (cga_o + static_cast<double>(ea0) * tx_a);
+                    g[NN + 2] = 0.0 - cgb_o;
+                    g[NN + 3] = 0.0 - (cgb_o + static_cast<double>(eb0) * tx_b);
+                    A.status[p] = 0;
+                    A.score[p] = A.temperature * (log(zhat) + double(EZ) * 0.69314718055994530942);
+                }
+            }
+            stalled = false;
+            __syncthreads();
+        } else if (bad) {
             if (lane == 0) { A.status[p] = 1; A.score[p] = 0.0; }
         } else {
             if constexpr (G > 1)

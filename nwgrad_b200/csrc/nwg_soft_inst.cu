@@ -5,6 +5,11 @@ namespace nwg {
 namespace {
 template <class T, bool AFF, bool LOC, bool TR>
 SoftFn pick(Geo g) {
+    if constexpr (!TR) {
+        if (g.mw > 1) return (g.G == 32 && g.R == 4) ? &soft_kernel<T, AFF, LOC, false, 32, 4, true> : nullptr;
+    } else {
+        if (g.mw > 1) return nullptr;
+    }
 #define NWG_S(GG, RR) if (g.G == GG && g.R == RR) return &soft_kernel<T, AFF, LOC, TR, GG, RR>;
     NWG_S(1, 8) NWG_S(1, 16) NWG_S(1, 24) NWG_S(1, 32) NWG_S(32, 2) NWG_S(32, 4)
     NWG_S(16, 2) NWG_S(16, 4) NWG_S(8, 4)

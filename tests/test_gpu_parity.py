@@ -299,3 +299,31 @@ def test_autotuned_and_plain_fill_same_results(grad_mode, tmp_path, monkeypatch)
             for x, y in zip(res[0][1:], other[1:]):
                 scale = max(1.0, float(np.abs(x).max()))
                 assert np.abs(x - y).max() <= 1e-5 * scale
+
+
+@pytest.mark.parametrize("gm", [0, 1])
+@pytest.mark.parametrize("am", [0, 1])
+def test_soft_long_pairs_several_warps_per_pair(gm, am):
+    """Pairs of 1,600+ rows run with four warps per pair (a pipeline over their stripes):
+    within tolerance of the oracle and of the one-warp kernel on the same pairs."""
+    rng = np.random.default_rng(1600 + gm + 2 * am)
+    mat, gaps, sa, sb, tr, gt = _problem(rng, AA, 6, 5, 200, homolog=True)
+    sa += rand_seqs(rng, 3, 1600, 2400, AA)
+    sb += [mutate(rng, s, AA) for s in sa[-3:]]
+    kw = dict(gap_model=("linear", "affine")[gm], mode=("global", "local")[am], grad_mode="soft")
+    b = nw.SeqPairBatch(sa, sb, _params(AA, mat, gaps), **kw)
+    b.score_and_grad()
+    one = nw.SeqPairBatch(sa, sb, _params(AA, mat, gaps), **kw)
+    one._tune = (32, 4)                       # forced geometry: one warp per pair
+    one.score_and_grad()
+    np.testing.assert_allclose(b.scores(), one.scores(), rtol=1e-6, atol=1e-6)
+    ga, gb = b.grads()
+    oa_, ob_ = one.grads()
+    scale = max(1.0, float(np.abs(oa_).max()))
+    assert np.abs(ga - oa_).max() <= 1e-5 * scale and np.abs(gb - ob_).max() <= 1e-5 * max(1.0, float(np.abs(ob_).max()))
+    enc = oracle.Encoded(encode(AA, sa), encode(AA, sb))
+    so, go = oracle.soft(gm, am, mat, gaps, enc)
+    np.testing.assert_allclose(b.scores(), so, rtol=SOFT_RTOL, atol=1e-5)
+    flat = np.concatenate([ga.reshape(len(sa), -1), gb.reshape(len(sa), -1)], axis=1)
+    sc = np.maximum(np.abs(go).max(axis=1, keepdims=True), 1.0)
+    assert (np.abs(flat - go) / sc).max() <= SOFT_RTOL
