@@ -42,6 +42,15 @@ AA = "ACDEFGHIKLMNPQRSTVWY"
 OPS_PER_CELL_SOFT = 32.0          # soft affine: ~10 forward + ~22 backward/gradient FP32 ops
 OPS_PER_CELL_HARD = 22.0          # hard affine: 13 FP32 + 9 compare/select
 FP32_LANE_OPS_PEAK = 148 * 128 * 1.965e9   # ops/s at the maximum SM clock
+SOFT_DRAM_BYTES_PER_CELL = 31.1            # ncu, soft kernel 32x4 on 800+800 pairs of this workload
+
+
+def measured_hbm_gbs():
+    """The pool's measured copy bandwidth, when the measured peaks file is present."""
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+    except (OSError, ValueError, KeyError):
+        return 6650.0
 
 
 # ── workload ─────────────────────────────────────────────────────────────────
@@ -345,11 +354,19 @@ def main():
     ap.add_argument("--checkpoint-mb", type=float, default=-1,
                     help="soft: per-pair forward tables above this many MiB are checkpointed (-1: default)")
     ap.add_argument("--geometry", default=None, help="LANESxROWS for every pair (no tuning), e.g. 32x4")
-    ap.add_argument("--workload", default="c2-soft", choices=["c2-soft", "c1-hard"],
-                    help="c2-soft (default): the soft-gradient batch; c1-hard: the plain hard batch (side measurement)")
+    ap.add_argument("--workload", default="c2-soft", choices=["c2-soft", "c1-hard", "c4-long", "c3-short"],
+                    help="c2-soft (default): the soft-gradient batch; side measurements: c1-hard (plain hard "
+                         "batch), c4-long (64 long pairs: Pointers, Hirschberg, soft, banded), c3-short "
+                         "(many short local linear tracked pairs, hard and soft)")
+    ap.add_argument("--long-pairs", type=int, default=64)
+    ap.add_argument("--short-pairs", type=int, default=2_000_000)
     args = ap.parse_args()
     if args.workload == "c1-hard":
         return bench_c1(args)
+    if args.workload == "c4-long":
+        return bench_c4(args)
+    if args.workload == "c3-short":
+        return bench_c3(args)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -517,16 +534,17 @@ def main():
     # roofline of the soft kernel: algorithmic FP32 ops per cell over the kernels' device time
     kernel_s = kernel_ms / 1e3
     ach = cells * args.steps * OPS_PER_CELL_SOFT / kernel_s / 1e12 if kernel_s > 0 else None
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "soft_kernel_traffic.json")
-    if os.path.exists(tpath):
-        try:
-            tj = json.load(open(tpath))
-            traffic = float(tj["bytes_per_cell"]) * cells / 2.0   # per launch (one batch)
-        except (OSError, ValueError, KeyError):
-            traffic = None
+    # DRAM traffic of one launch (one batch): bytes per cell from an ncu capture of the same
+    # kernel on a small case (dram__bytes_read.sum + dram__bytes_write.sum over its cells),
+    # scaled by this launch's cells (the forward table is per cell)
+    traffic = SOFT_DRAM_BYTES_PER_CELL * cells / 2.0
+    kernel_launch_s = kernel_s / (2 * args.steps) if kernel_s > 0 else None
+    hbm_peak = measured_hbm_gbs()
+    hbm = {"achieved": traffic / kernel_launch_s / 1e9 if kernel_launch_s else None, "peak": hbm_peak,
+           "unit": "GB/s", "frac": (traffic / kernel_launch_s / 1e9 / hbm_peak) if kernel_launch_s and hbm_peak else None,
+           "peak_note": "measured copy bandwidth (of measured)"}
     roofline = {"bound": "alu", "achieved": ach, "peak": FP32_LANE_OPS_PEAK / 1e12, "unit": "TOP/s",
-                "frac": (ach / (FP32_LANE_OPS_PEAK / 1e12)) if ach else None, "traffic": traffic,
+                "frac": (ach / (FP32_LANE_OPS_PEAK / 1e12)) if ach else None, "traffic": traffic, "hbm": hbm,
                 "peak_note": "FP32 lane-op peak 148 SM x 128 lanes x 1.965 GHz (the recurrence is max-plus / "
                              "sum-product: no tensor-core contraction)",
                 "ops_per_cell": OPS_PER_CELL_SOFT, "kernel_ms_per_step": kernel_ms / args.steps}
@@ -552,6 +570,129 @@ def main():
             "step_ms": step_ms}))
     if dist is not None:
         dist.destroy_process_group()
+
+
+def c4_workload(n_pairs=64, seed=4):
+    """Long pairs: A of length log-uniform 5,000-36,000, B = A with 20 % substitutions and
+    single-residue indels (2.5 % each)."""
+    rng = np.random.default_rng(seed)
+    freqs = rng.dirichlet(np.full(20, 5.0))
+    mat = c2_matrix(rng)
+    la = np.exp(rng.uniform(np.log(5000), np.log(36000), size=n_pairs)).astype(np.int64)
+    oa = np.zeros(n_pairs + 1, np.int64); np.cumsum(la, out=oa[1:])
+    a = rng.choice(20, size=int(oa[-1]), p=freqs).astype(np.uint8)
+    b = a.copy()
+    s = rng.random(b.size) < 0.20
+    b[s] = rng.choice(20, size=int(s.sum()), p=freqs)
+    keep = (rng.random(b.size) >= 0.025).astype(np.int64)
+    ins = rng.random(b.size) < 0.025
+    cnt = keep + ins
+    cnt[oa[1:] - 1] = np.maximum(cnt[oa[1:] - 1], 1)
+    bb = b[np.repeat(np.arange(b.size), cnt)]
+    bb[(np.cumsum(cnt) - 1)[ins]] = rng.choice(20, size=int(ins.sum()), p=freqs)
+    ob = np.zeros(n_pairs + 1, np.int64); np.cumsum(np.add.reduceat(cnt, oa[:-1]), out=ob[1:])
+    return mat, a, oa, bb.astype(np.uint8), ob
+
+
+def _timed_run(fn, reps=1):
+    import torch
+    best = None
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        fn()
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        best = dt if best is None else min(best, dt)
+    return best
+
+
+def bench_c4(args):
+    """Side measurement: long pairs (log-uniform 5k-36k).  Hard gradient by Pointers (several
+    warps per pair) and by Hirschberg (float32 prefix-max carry and float64 exact carry), soft
+    gradient (several warps per pair, stripe checkpoints), then banded re-alignment (bandwidth
+    64) after a 1e-3 parameter step.  GCUPS per stage from wall time around each call."""
+    import nwgrad_b200 as nw
+    mat, a, oa, b, ob = c4_workload(args.long_pairs)
+    cells = cells_of(oa, ob)
+    p = nw.AlignParams.from_arrays(mat[None], [[11.0, 1.0, 11.0, 1.0]], alphabet=nw.AA20)
+    out = {"metric": "long-pair GCUPS per stage", "unit": "GCUPS", "n_gpus": 1,
+           "config": {"workload": f"{args.long_pairs} pairs, A log-uniform 5k-36k, B = A 20% mutated",
+                      "cells": cells, "max_len": int(np.diff(oa).max())}, "stages": {}}
+    for name, cls, tb in (("hard_pointers_f32", nw.SeqPairBatch, "pointers"),
+                          ("hard_hirschberg_pmax_f32", nw.SeqPairBatch, "hirschberg_pmax"),
+                          ("hard_hirschberg_f64", nw.SeqPairBatchDouble, "hirschberg")):
+        bt = cls.from_codes(a, oa, b, ob, p, grad_mode="hard", traceback=tb)
+        bt.score_and_grad()                                     # warm
+        t = _timed_run(lambda: (bt.score_and_grad(), bt.compute_grad()))
+        out["stages"][name] = {"seconds": t, "gcups": cells / t / 1e9}
+        if name == "hard_hirschberg_pmax_f32":
+            g = bt.compute_grad()
+            bt.set_params(p + g * 1e-3)
+            t = _timed_run(lambda: (bt.banded_grad(64), bt.compute_grad()))
+            band_cells = float(np.sum(np.diff(oa) * 129))
+            out["stages"]["banded64_after_step_f32"] = {"seconds": t, "gcups_full_equivalent": cells / t / 1e9,
+                                                         "band_cells": band_cells}
+        del bt
+    bt = nw.SeqPairBatch.from_codes(a, oa, b, ob, p, grad_mode="soft")
+    bt.score_and_grad()
+    t = _timed_run(lambda: (bt.score_and_grad(), bt.compute_grad()))
+    out["stages"]["soft_f32"] = {"seconds": t, "gcups": cells / t / 1e9}
+    print(json.dumps(out))
+
+
+def c3_workload(n_pairs, seed=3):
+    """Many short pairs: A a 22-nt RNA (ACGU), B 30-50 nt DNA (ACGT) with the reverse complement
+    of A[1:8] (6-8 nt) at a random offset; alphabet ACGTU; track of A: 0 seed (A[1:8]), 1 the
+    3' region (A[13:]), 2 the rest."""
+    rng = np.random.default_rng(seed)
+    A = np.array([0, 1, 2, 4], np.uint8)           # A C G U in "ACGTU"
+    comp = {0: 4, 1: 2, 2: 1, 4: 0}                # RNA -> complementary DNA base (U pairs with A)
+    a = A[rng.integers(0, 4, size=(n_pairs, 22))]
+    lb = rng.integers(30, 51, size=n_pairs)
+    ob = np.zeros(n_pairs + 1, np.int64); np.cumsum(lb, out=ob[1:])
+    b = rng.integers(0, 4, size=int(ob[-1])).astype(np.uint8)   # A C G T
+    seed_len = rng.integers(6, 9, size=n_pairs)
+    lut = np.array([3, 2, 1, 0, 0], np.uint8)      # complement of A C G T U as DNA: T G C A A
+    for p in range(0, n_pairs):
+        k = int(seed_len[p]); off = int(rng.integers(0, lb[p] - k + 1))
+        site = lut[a[p, 1:1 + k][::-1]]
+        b[ob[p] + off: ob[p] + off + k] = site
+    oa = np.arange(n_pairs + 1, dtype=np.int64) * 22
+    tr = np.full((n_pairs, 22), 2, np.uint16); tr[:, 1:8] = 0; tr[:, 13:] = 1
+    mat = np.full((3, 5, 5), -4.0)
+    for k in range(3):
+        for x, y in ((0, 3), (1, 2), (2, 1), (3, 0), (4, 0), (2, 4)):   # A-T, C-G, G-C, T-A, U-A, G-U wobble
+            mat[k, x, y] = 5.0
+    gaps = np.tile([6.0, 6.0, 6.0, 6.0], (3, 1))
+    return mat, gaps, a.reshape(-1), oa, b, ob, tr.reshape(-1)
+
+
+def bench_c3(args):
+    """Side measurement: many short pairs, local linear, K = 3 parameter sets by a per-residue
+    track of A; hard and soft; one launch per geometry bucket, autotuned."""
+    import nwgrad_b200 as nw
+    mat, gaps, a, oa, b, ob, tr = c3_workload(args.short_pairs)
+    cells = cells_of(oa, ob)
+    p = nw.AlignParams.from_arrays(mat, gaps, alphabet="ACGTU")
+    out = {"metric": "short-pair GCUPS", "unit": "GCUPS", "n_gpus": 1,
+           "config": {"workload": f"{args.short_pairs} pairs, A 22 nt, B 30-50 nt, local linear, K=3 tracked",
+                      "cells": cells}, "modes": {}}
+    for mode in ("hard", "soft"):
+        bt = nw.SeqPairBatch.from_codes(a, oa, b, ob, p, grad_mode=mode, gap_model="linear", mode="local",
+                                        tracks=tr)
+        table = bt.autotune()
+        bt.score_and_grad()
+        t = _timed_run(lambda: (bt.score_and_grad(), bt.compute_grad()), reps=3)
+        ms, launches = bt.last_timing()
+        bt.use_plain_fill()
+        bt.score_and_grad()
+        tp = _timed_run(lambda: (bt.score_and_grad(), bt.compute_grad()), reps=3)
+        out["modes"][mode] = {"gcups": cells / t / 1e9, "seconds": t, "device_ms": ms, "launches": launches,
+                              "plain_fill_gcups": cells / tp / 1e9,
+                              "autotune": {str(k): f"{v[0]}x{v[1]}" for k, v in table.items()}}
+        del bt
+    print(json.dumps(out))
 
 
 def bench_c1(args):

@@ -357,6 +357,7 @@ void build_plan(nwg_store* s, Plan& P, bool soft, int lanes, int rpl, int elem_b
         if (!band && !lanes && !rpl) {
             if (s->plain) g = Geo{32, 4};
             else if (soft && !s->tracked() && rows >= kLongRows && nb >= 256) g = Geo{32, 4, false, kLongWarps};
+            else if (!soft && rows >= kLongRows && nb >= 256) g = Geo{32, 8, false, kLongWarps};
             else {
                 auto it = s->geo_table.find({int(soft), sc});
                 if (it != s->geo_table.end() && (!soft || it->second.first > 1 || lane_ok_soft))
@@ -457,21 +458,39 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
     s->score.need(size_t(std::max<int64_t>(s->n, 1)) * 8, st);
     s->end.need(size_t(std::max<int64_t>(s->n, 1)) * 16, st);
     const int sms = sm_count(s->device);
-    const size_t smem = (size_t(s->K) * s->N * s->N + 4 * size_t(s->K)) * sizeof(T);
-    // scratch: the stripe boundary row per group slot
-    int64_t max_slots = 0, max_stride = 0;
-    for (auto& B : P.buckets) {
+    const size_t smem_base = (size_t(s->K) * s->N * s->N + 4 * size_t(s->K)) * sizeof(T);
+    // scratch per slot: the stripe boundary row (one group per pair), or one row per stripe
+    // (several warps per pair: a slot is a block)
+    auto bucket_shape = [&](const Bucket& B, int64_t& blocks, int64_t& slots, int64_t& stride) {
         const int gpb = 128 / B.geo.G;
-        const int64_t groups = int64_t(B.pairs.size());
-        const int64_t blocks = std::min<int64_t>((groups + gpb - 1) / gpb, int64_t(sms) * 16);
-        max_slots = std::max(max_slots, blocks * gpb);
-        max_stride = std::max<int64_t>(max_stride, 3 * (int64_t(B.maxn) + 1));
+        const int64_t items = int64_t(B.pairs.size());
+        const int64_t row = 3 * (int64_t(B.maxn) + 1);
+        if (B.geo.mw > 1) {
+            const int GR = B.geo.G * B.geo.R;
+            int64_t ns = 0;
+            for (int32_t p : B.pairs) ns = std::max<int64_t>(ns, (s->oa[p + 1] - s->oa[p] + GR - 1) / GR);
+            blocks = std::min<int64_t>(items, int64_t(sms) * 4);
+            slots = blocks;
+            stride = std::max<int64_t>(ns, 1) * row;
+        } else {
+            blocks = std::min<int64_t>((items + gpb - 1) / gpb, int64_t(sms) * 16);
+            slots = blocks * gpb;
+            stride = row;
+        }
+    };
+    int64_t max_total = 1;
+    for (auto& B : P.buckets) {
+        if (B.pairs.empty()) continue;
+        int64_t bl, sl, sd;
+        bucket_shape(B, bl, sl, sd);
+        max_total = std::max(max_total, sl * sd);
     }
-    s->scratch.need(size_t(std::max<int64_t>(max_slots * max_stride, 1)) * sizeof(T), st);
+    s->scratch.need(size_t(max_total) * sizeof(T), st);
     for (auto& B : P.buckets) {
         if (B.pairs.empty()) continue;
         HardFn fn = hard_fn_rt<T>(aff, loc, tr, B.geo);
         if (!fn) throw Error(NWG_EINVAL, "no kernel for this geometry");
+        const size_t smem = smem_base + (B.geo.mw > 1 ? nwg::hard_mw_smem_bytes(128 / B.geo.G, int(sizeof(T))) : 0);
         if (smem > 48 * 1024) NWG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
         nwg::HardArgs A{};
         A.a = s->a.as<uint8_t>(); A.oa = s->doa.as<int64_t>();
@@ -487,13 +506,28 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
             A.guide = s->guide.as<int32_t>(); A.band = J.band;
             A.stripe_base = P.stripe_base.as<int64_t>(); A.stripe_tab = s->stripe_tab.as<int64_t>();
         }
-        A.scratch = s->scratch.p; A.scratch_stride = max_stride;
+        int64_t blocks, slots, stride;
+        bucket_shape(B, blocks, slots, stride);
+        A.scratch = s->scratch.p; A.scratch_stride = stride;
+        A.row_stride = 3 * (int64_t(B.maxn) + 1);
         A.score = s->score.as<double>(); A.end = s->end.as<int32_t>();
-        const int gpb = 128 / B.geo.G;
-        const int64_t blocks = std::min<int64_t>((A.n_items + gpb - 1) / gpb, int64_t(sms) * 16);
         fn<<<unsigned(blocks), 128, smem, st>>>(A);
         NWG_CUDA(cudaGetLastError());
         s->last_launches++;
+    }
+    // several warps per pair: a wait between warps that ran out fails the call (end state 3)
+    bool any_mw = false;
+    for (auto& B : P.buckets) any_mw |= (B.geo.mw > 1 && !B.pairs.empty());
+    if (any_mw && s->n) {
+        std::vector<int32_t> e(size_t(s->n) * 4);
+        NWG_CUDA(cudaMemcpyAsync(e.data(), s->end.p, e.size() * 4, cudaMemcpyDeviceToHost, st));
+        NWG_CUDA(cudaStreamSynchronize(st));
+        for (auto& B : P.buckets)
+            if (B.geo.mw > 1)
+                for (int32_t p : B.pairs)
+                    if (e[4 * size_t(p) + 2] == 3)
+                        throw Error(NWG_ECUDA, "nwgrad_b200: hard fill: a wait between the warps of pair " +
+                                                   std::to_string(p) + " ran out (the kernel gave up instead of hanging)");
     }
     // traceback: gradient, guide, path
     if (want_grad) {

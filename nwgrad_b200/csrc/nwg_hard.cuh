@@ -41,6 +41,7 @@ struct HardArgs {
     int N, K;
     uint8_t* codes; const int64_t* code_off;   // per pair code table
     void* scratch; int64_t scratch_stride;     // per group slot: the stripe boundary row, 3*(n+1) T
+    int64_t row_stride;                        // several warps per pair: T per boundary row (one per stripe)
     double* score;                             // per pair
     int32_t* end;                              // per pair: end_i, end_j, state, layout (G<<8|R)
     // guide-banded re-alignment (BAND kernels only)
@@ -74,27 +75,71 @@ __device__ __forceinline__ T border_col0(const HardArgs& A, const T* bx0p, int i
     }
 }
 
-template <class T, bool AFF, bool LOC, bool TR, int G, int R, bool BAND = false>
+// Shared memory beyond the parameters that several warps per pair use: per warp a best value,
+// its cell and state, and a progress counter.
+__host__ __device__ inline size_t hard_mw_smem_bytes(int warps, int tsize) {
+    return size_t(warps) * (tsize + 4 * 4) + size_t(warps) * 4 + 64;
+}
+
+// Several warps per pair (MW, long pairs): warp w fills stripes w, w + NW, ..., each stripe's
+// bottom row in its own scratch row, and waits (every 32 steps, bounded) until the warp filling
+// the stripe above has published enough steps -- the protocol of the soft kernel
+// (nwg_soft.cuh).  A wait that runs out marks the pair's end state 3 and the host fails the call.
+constexpr int kHardSpinLimit = 1 << 22;
+
+template <class T, bool AFF, bool LOC, bool TR, int G, int R, bool BAND = false, bool MW = false>
 __global__ void __launch_bounds__(128) hard_fill_kernel(const HardArgs A) {
+    static_assert(!MW || (G == 32 && !BAND), "several warps per pair: 32 lanes, full DP");
     constexpr int GR = G * R;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* smat = reinterpret_cast<T*>(smem_raw);
     const int nmat = A.K * A.N * A.N;
     T* sgap = smat + nmat;
+    unsigned char* mw_raw = reinterpret_cast<unsigned char*>(
+        (reinterpret_cast<uintptr_t>(sgap + 4 * A.K) + 15) & ~uintptr_t(15));
+    T* wbest = reinterpret_cast<T*>(mw_raw);                                   // MW: [warp]
+    int* wcell = reinterpret_cast<int*>(wbest + (blockDim.x / G));             // MW: [warp][4]
+    volatile int* prog = wcell + 4 * (blockDim.x / G);                         // MW: [warp]
     for (int k = threadIdx.x; k < nmat; k += blockDim.x) smat[k] = static_cast<const T*>(A.mat)[k];
     for (int k = threadIdx.x; k < 4 * A.K; k += blockDim.x) sgap[k] = static_cast<const T*>(A.gaps)[k];
     __syncthreads();
 
     const int lane = threadIdx.x % G;
     const int gpb = blockDim.x / G;
-    const int64_t slot = int64_t(blockIdx.x) * gpb + threadIdx.x / G;
+    const int gib = threadIdx.x / G;
+    const int NWp = MW ? gpb : 1;
+    const int pw = (gib + NWp - 1) % NWp;                   // MW: the warp of the stripe above
+    const int64_t slot = MW ? int64_t(blockIdx.x) : int64_t(blockIdx.x) * gpb + gib;
     unsigned gmask;
     if constexpr (G == 32) gmask = 0xffffffffu;
     else gmask = ((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1));
-    T* bnd = static_cast<T*>(A.scratch) + slot * A.scratch_stride;
+    T* const bnd0 = static_cast<T*>(A.scratch) + slot * A.scratch_stride;
     const int N = A.N;
+    bool stalled = false;
+    auto wait_for = [&](int target) {
+        if constexpr (MW) {
+            int k = 0;
+            while (!stalled && prog[pw] < target) {
+                if (++k > kHardSpinLimit) stalled = true;
+                else __nanosleep(64);
+            }
+            __syncwarp();
+            __threadfence_block();
+        }
+    };
+    auto publish = [&](int v) {
+        if constexpr (MW) {
+            __syncwarp();
+            __threadfence_block();
+            if (lane == 0) prog[gib] = v;
+        }
+    };
 
-    for (int64_t it = slot; it < A.n_items; it += int64_t(gridDim.x) * gpb) {
+    for (int64_t it = MW ? int64_t(blockIdx.x) : slot; it < A.n_items; it += MW ? int64_t(gridDim.x) : int64_t(gridDim.x) * gpb) {
+        if constexpr (MW) {
+            if (lane == 0) prog[gib] = -1;
+            __syncthreads();
+        }
         const int p = A.order[it];
         const int64_t ao = A.oa[p], bo = A.ob[p];
         const int m = int(A.oa[p + 1] - ao), n = int(A.ob[p + 1] - bo);
@@ -113,7 +158,7 @@ __global__ void __launch_bounds__(128) hard_fill_kernel(const HardArgs A) {
         const T goa0 = sgap[4 * gset(0) + 0], gea0 = sgap[4 * gset(0) + 1];
         const T ugob = sgap[2], ugeb = sgap[3], ugoa = sgap[0], ugea = sgap[1];
         if (m == 0 || n == 0) {
-            if (lane == 0) {
+            if (lane == 0 && (!MW || gib == 0)) {
                 T sc; int ei, ej, st;
                 if (LOC) { sc = T(0); ei = 0; ej = 0; st = 0; }
                 else if (m == 0 && n == 0) { sc = T(0); ei = 0; ej = 0; st = 0; }
@@ -148,7 +193,12 @@ __global__ void __launch_bounds__(128) hard_fill_kernel(const HardArgs A) {
         T bestv = T(0); int besti = 0, bestj = 0, bests = 0;   // Local: the first row-major max
         T endM = ninf<T>(), endX = ninf<T>(), endY = ninf<T>();
 
-        for (int s = 0; s < nstripes; ++s) {
+        const int S_full = n + G - 1;          // MW: steps per stripe (full DP)
+        const int SP = S_full + 1;             // MW: progress key per stripe
+        for (int s = MW ? gib : 0; s < nstripes; s += NWp) {
+            // the previous stripe's bottom row (read) and this stripe's (written)
+            T* const bnd = bnd0 + (MW ? int64_t(s - 1) * A.row_stride : 0);
+            T* const bnd_out = bnd0 + (MW ? int64_t(s) * A.row_stride : 0);
             const int i0 = s * GR + lane * R + 1;   // this lane's first DP row
             // the stripe's columns [cmin, cmax]: the union of its rows' bands
             int cmin = 1, cmax = n;
@@ -234,13 +284,25 @@ __global__ void __launch_bounds__(128) hard_fill_kernel(const HardArgs A) {
             }
             T upM = ninf<T>(), upX = ninf<T>(), upY = ninf<T>();
             uint8_t* cs = codes + (BAND ? soff : int64_t(s) * S8 * GR);
+            // lane 0: the row above one column ahead, so the load is in flight meanwhile
+            T nuM = ninf<T>(), nuX = ninf<T>(), nuY = ninf<T>();
+            auto fetch_up = [&](int jj) {
+                if (lane == 0 && s > 0 && jj <= cmax) {
+                    if (!BAND || (jj >= pmin && jj <= pmax)) { nuM = bnd[3 * jj]; nuX = bnd[3 * jj + 1]; nuY = bnd[3 * jj + 2]; }
+                    else { nuM = ninf<T>(); nuX = ninf<T>(); nuY = ninf<T>(); }
+                }
+            };
+            const bool waits = MW && s > 0;
+            if (waits) wait_for((s - 1) * SP + min(S_full, 2 * G + 1));
+            fetch_up(cmin);
 
             for (int t = 0; t < S; ++t) {
                 const int j = cmin + t - lane;
+                if (waits && t > 0 && (t & 31) == 0) wait_for((s - 1) * SP + min(S_full, t + 2 * G + 1));
+                if (MW && t > 0 && (t & 7) == 0) publish(s * SP + t);
                 if (lane == 0 && j <= cmax) {
                     if (s == 0) row0(j, upM, upX, upY);
-                    else if (!BAND || (j >= pmin && j <= pmax)) { upM = bnd[3 * j]; upX = bnd[3 * j + 1]; upY = bnd[3 * j + 2]; }
-                    else { upM = ninf<T>(); upX = ninf<T>(); upY = ninf<T>(); }
+                    else { upM = nuM; upX = nuX; upY = nuY; fetch_up(j + 1); }
                 }
                 const bool active = (j >= cmin) && (j <= cmax);
                 if (active) {
@@ -334,10 +396,11 @@ __global__ void __launch_bounds__(128) hard_fill_kernel(const HardArgs A) {
                     if (lane > 0) { upM = sM; upX = sX; upY = sY; }
                 }
                 if (lane == G - 1 && active && s + 1 < nstripes) {
-                    bnd[3 * j] = cM[R - 1];
-                    if constexpr (AFF) { bnd[3 * j + 1] = cX[R - 1]; bnd[3 * j + 2] = cY[R - 1]; }
+                    bnd_out[3 * j] = cM[R - 1];
+                    if constexpr (AFF) { bnd_out[3 * j + 1] = cX[R - 1]; bnd_out[3 * j + 2] = cY[R - 1]; }
                 }
             }
+            if constexpr (MW) publish(s * SP + S_full);
             pmin = cmin; pmax = cmax;
             soff += int64_t(S8) * GR;
             // the end cell (m, n): after the stripe each register holds column n (a banded
@@ -369,6 +432,42 @@ __global__ void __launch_bounds__(128) hard_fill_kernel(const HardArgs A) {
             }
             if constexpr (G > 1) __syncwarp(gmask);
         }
+        if constexpr (MW) {
+            // a wait that ran out fails the pair; Local: the warps' bests, first row-major max
+            stalled = __any_sync(gmask, stalled);
+            if (lane == 0) {
+                wbest[gib] = bestv;
+                wcell[4 * gib] = besti; wcell[4 * gib + 1] = bestj; wcell[4 * gib + 2] = bests;
+                wcell[4 * gib + 3] = stalled ? 1 : 0;
+            }
+            __syncthreads();
+            bool anystall = false;
+            for (int w = 0; w < NWp; ++w) anystall |= wcell[4 * w + 3] != 0;
+            if (anystall) {
+                if (threadIdx.x == 0) {
+                    A.score[p] = 0.0;
+                    A.end[4 * p] = 0; A.end[4 * p + 1] = 0; A.end[4 * p + 2] = 3; A.end[4 * p + 3] = (G << 8) | R;
+                }
+                __syncthreads();
+                stalled = false;
+                continue;
+            }
+            if constexpr (LOC) {
+                if (threadIdx.x == 0) {
+                    T bv = T(0); int bi = 0, bj = 0, bs = 0;
+                    for (int w = 0; w < NWp; ++w) {
+                        const T v = wbest[w];
+                        const int wi = wcell[4 * w];
+                        if (v > bv || (v == bv && v > T(0) && wi < bi)) { bv = v; bi = wi; bj = wcell[4 * w + 1]; bs = wcell[4 * w + 2]; }
+                    }
+                    A.score[p] = static_cast<double>(bv);
+                    A.end[4 * p] = bi; A.end[4 * p + 1] = bj; A.end[4 * p + 2] = bs;
+                    A.end[4 * p + 3] = (G << 8) | R;
+                }
+                __syncthreads();
+                continue;
+            }
+        }
         if constexpr (!LOC) {
             if constexpr (G > 1) {
                 // the lane holding row m broadcasts its end values
@@ -377,7 +476,7 @@ __global__ void __launch_bounds__(128) hard_fill_kernel(const HardArgs A) {
                 endX = __shfl_sync(gmask, endX, src, G);
                 endY = __shfl_sync(gmask, endY, src, G);
             }
-            if (lane == 0) {
+            if (lane == 0 && (!MW || gib == (nstripes - 1) % NWp)) {
                 T sc; int st;
                 if constexpr (AFF) {
                     sc = rmax3(endM, endX, endY);
@@ -387,6 +486,7 @@ __global__ void __launch_bounds__(128) hard_fill_kernel(const HardArgs A) {
                 A.end[4 * p] = m; A.end[4 * p + 1] = n; A.end[4 * p + 2] = st;
                 A.end[4 * p + 3] = (G << 8) | R;
             }
+            if constexpr (MW) __syncthreads();
         } else if (lane == 0) {
             A.score[p] = static_cast<double>(bestv);
             A.end[4 * p] = besti; A.end[4 * p + 1] = bestj; A.end[4 * p + 2] = bests;

@@ -12,6 +12,11 @@ HardFn pick_band(Geo g) {
 template <class T, bool AFF, bool LOC, bool TR>
 HardFn pick(Geo g) {
     if (g.band) return pick_band<T, AFF, LOC, TR>(g);
+    if (g.mw > 1) {   // several warps per pair
+        if (g.G == 32 && g.R == 4) return &hard_fill_kernel<T, AFF, LOC, TR, 32, 4, false, true>;
+        if (g.G == 32 && g.R == 8) return &hard_fill_kernel<T, AFF, LOC, TR, 32, 8, false, true>;
+        return nullptr;
+    }
 #define NWG_H(GG, RR) if (g.G == GG && g.R == RR) return &hard_fill_kernel<T, AFF, LOC, TR, GG, RR>;
     NWG_H(1, 8) NWG_H(1, 16) NWG_H(1, 24) NWG_H(1, 32) NWG_H(32, 1) NWG_H(32, 2) NWG_H(32, 4) NWG_H(32, 8)
 #undef NWG_H

@@ -327,3 +327,23 @@ def test_soft_long_pairs_several_warps_per_pair(gm, am):
     flat = np.concatenate([ga.reshape(len(sa), -1), gb.reshape(len(sa), -1)], axis=1)
     sc = np.maximum(np.abs(go).max(axis=1, keepdims=True), 1.0)
     assert (np.abs(flat - go) / sc).max() <= SOFT_RTOL
+
+
+@pytest.mark.parametrize("prec", [32, 64])
+@pytest.mark.parametrize("gm", [0, 1])
+@pytest.mark.parametrize("am", [0, 1])
+def test_hard_long_pairs_several_warps_per_pair(prec, gm, am):
+    """Pairs of 1,600+ rows fill with four warps per pair: bit for bit the oracle's
+    (scores, per-pair gradients, guides), with short pairs in the same batch."""
+    rng = np.random.default_rng(1700 + prec + gm + 2 * am)
+    mat, gaps, sa, sb, tr, gt = _problem(rng, AA, 8, 1, 150, integer=(gm == 1), homolog=True)
+    sa += rand_seqs(rng, 3, 1600, 2600, AA)
+    sb += [mutate(rng, s, AA) for s in sa[-3:]]
+    _hard_check(prec, gm, am, AA, mat, gaps, sa, sb, None, None, False)
+
+
+def test_hard_long_tracked_several_warps_per_pair():
+    rng = np.random.default_rng(1800)
+    alpha = "ACGTU"
+    mat, gaps, sa, sb, tr, gt = _problem(rng, alpha, 3, 1600, 2200, K=3, tracked=True, gap_tracks=True)
+    _hard_check(32, 1, 0, alpha, mat, gaps, sa, sb, tr, gt, True)
