@@ -219,10 +219,14 @@ Geo pick_geo(bool soft, int rows, int n, int lanes, int rpl, bool lane_ok) {
     return best;
 }
 
-// Soft pairs of at least this many DP rows run with several warps per pair (a pipeline over
-// the pair's stripes) instead of one: a long pair is then not a single warp's serial work.
+// Pairs of at least this many DP rows run with several warps per pair (a pipeline over the
+// pair's stripes) instead of one: a long pair is then not a single warp's serial work.  The
+// warps per pair grow with the pair's stripes (each warp keeps at least 3 stripes).
 constexpr int kLongRows = 1536;
-constexpr int kLongWarps = 4;
+int long_warps(int rows, int GR) {
+    const int ns = (rows + GR - 1) / GR;
+    return ns >= 64 ? 16 : ns >= 24 ? 8 : 4;
+}
 
 // Pairs are bucketed by geometry and by size class: the binary order of magnitude of the DP
 // (rows x columns), with everything up to 2^20 cells in one class.  Small pairs share a
@@ -282,7 +286,7 @@ struct nwg_store {
     int64_t gstride = 0;
     bool have_scores = false, have_grads = false, have_guides = false, have_paths = false;
     int last_grad_mode = 0, last_gm = -1, last_am = -1, last_prec = 0;
-    Plan hard_plan, soft_plan, band_plan;
+    Plan hard_plan, soft_plan, band_plan, soft_band_plan;
     // geometry per (soft, size class) chosen by the autotuner; plain: one fixed geometry
     std::map<std::pair<int, int>, std::pair<int, int>> geo_table;
     bool plain = false;
@@ -353,11 +357,12 @@ void build_plan(nwg_store* s, Plan& P, bool soft, int lanes, int rpl, int elem_b
         if (hb_cut > 0 && m > hb_cut) continue;
         const int rows = soft ? m + 1 : m;
         const int sc = size_class(rows, nb);
-        Geo g = band ? Geo{32, 2, true} : pick_geo(soft, std::max(rows, 1), nb, lanes, rpl, soft ? lane_ok_soft : true);
+        Geo g = band ? (soft ? Geo{32, 4, true} : Geo{32, 2, true})
+                     : pick_geo(soft, std::max(rows, 1), nb, lanes, rpl, soft ? lane_ok_soft : true);
         if (!band && !lanes && !rpl) {
             if (s->plain) g = Geo{32, 4};
-            else if (soft && !s->tracked() && rows >= kLongRows && nb >= 256) g = Geo{32, 4, false, kLongWarps};
-            else if (!soft && rows >= kLongRows && nb >= 256) g = Geo{32, 8, false, kLongWarps};
+            else if (soft && !s->tracked() && rows >= kLongRows && nb >= 256) g = Geo{32, 4, false, long_warps(rows, 128)};
+            else if (!soft && rows >= kLongRows && nb >= 256) g = Geo{32, 8, false, long_warps(rows, 256)};
             else {
                 auto it = s->geo_table.find({int(soft), sc});
                 if (it != s->geo_table.end() && (!soft || it->second.first > 1 || lane_ok_soft))
@@ -469,7 +474,7 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
             const int GR = B.geo.G * B.geo.R;
             int64_t ns = 0;
             for (int32_t p : B.pairs) ns = std::max<int64_t>(ns, (s->oa[p + 1] - s->oa[p] + GR - 1) / GR);
-            blocks = std::min<int64_t>(items, int64_t(sms) * 4);
+            blocks = std::min<int64_t>(items, int64_t(sms) * std::max(1, 16 / B.geo.mw));
             slots = blocks;
             stride = std::max<int64_t>(ns, 1) * row;
         } else {
@@ -490,7 +495,8 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
         if (B.pairs.empty()) continue;
         HardFn fn = hard_fn_rt<T>(aff, loc, tr, B.geo);
         if (!fn) throw Error(NWG_EINVAL, "no kernel for this geometry");
-        const size_t smem = smem_base + (B.geo.mw > 1 ? nwg::hard_mw_smem_bytes(128 / B.geo.G, int(sizeof(T))) : 0);
+        const int hblock = B.geo.mw > 1 ? 32 * B.geo.mw : 128;
+        const size_t smem = smem_base + (B.geo.mw > 1 ? nwg::hard_mw_smem_bytes(B.geo.mw, int(sizeof(T))) : 0);
         if (smem > 48 * 1024) NWG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
         nwg::HardArgs A{};
         A.a = s->a.as<uint8_t>(); A.oa = s->doa.as<int64_t>();
@@ -511,7 +517,7 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
         A.scratch = s->scratch.p; A.scratch_stride = stride;
         A.row_stride = 3 * (int64_t(B.maxn) + 1);
         A.score = s->score.as<double>(); A.end = s->end.as<int32_t>();
-        fn<<<unsigned(blocks), 128, smem, st>>>(A);
+        fn<<<unsigned(blocks), hblock, smem, st>>>(A);
         NWG_CUDA(cudaGetLastError());
         s->last_launches++;
     }
@@ -653,7 +659,7 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
         const bool lane_ok = int64_t(s->K) * s->N * s->N * sizeof(T) * 32 <= 48 * 1024;
         for (int32_t p : *subset) {
             const int m = int(s->oa[p + 1] - s->oa[p]), nb = int(s->ob[p + 1] - s->ob[p]);
-            const Geo g = pick_geo(true, m + 1, nb, J.lanes, J.rows, lane_ok);
+            const Geo g = J.band >= 0 ? Geo{32, 4, true} : pick_geo(true, m + 1, nb, J.lanes, J.rows, lane_ok);
             auto key = std::make_tuple(g.G, g.R, size_class(m + 1, nb));
             auto itb = idx.find(key);
             int bi;
@@ -673,6 +679,9 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
                 B.max_rows = std::max(B.max_rows, m + 1);
             }
         }
+    } else if (J.band >= 0) {
+        P = &s->soft_band_plan;
+        build_plan(s, *P, true, 32, 4, sizeof(T), true);
     } else {
         P = &s->soft_plan;
         build_plan(s, *P, true, J.lanes, J.rows, sizeof(T));
@@ -699,6 +708,7 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
             return nwg::soft_smem_bytes(K, N, G, B.geo.R, blk, int(sizeof(T)), tr, mw);
         };
         while (!mw && block > 32 && smem_for(block) > 96 * 1024) block /= 2;
+        while (mw && block > 128 && smem_for(block) > 200 * 1024) block /= 2;   // fewer warps per pair
         const size_t smem = smem_for(block);
         if (smem > 227 * 1024) throw Error(NWG_EINVAL, "soft: the alphabet / parameter sets do not fit shared memory");
         if (smem > 48 * 1024) NWG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
@@ -739,6 +749,7 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
         A.maxn = B.maxn; A.temperature = J.temperature;
         A.ck = ck; A.max_stripes = int(std::max<int64_t>(max_stripes, 1));
         A.warp_stride = mw ? warp_bytes : 0;
+        A.guide = J.band >= 0 ? s->guide.as<int32_t>() : nullptr; A.band = J.band;
         A.bnd_off = (mw ? gpb : 1) * warp_bytes;
         A.renorm_mask = renorm - 1;
         A.score = s->score.as<double>(); A.grad = s->grad.as<double>(); A.gstride = s->gstride;
@@ -869,7 +880,7 @@ void load_pairs(nwg_store* s, const uint8_t* codes_a, const int64_t* off_a, cons
         throw Error(NWG_EINVAL, "nwgrad: a track entry is not a parameter set");
     // the host buffers may be reused by the caller after this returns
     NWG_CUDA(cudaStreamSynchronize(st));
-    s->hard_plan.reset(); s->soft_plan.reset(); s->band_plan.reset();
+    s->hard_plan.reset(); s->soft_plan.reset(); s->band_plan.reset(); s->soft_band_plan.reset();
     s->have_scores = s->have_grads = s->have_guides = s->have_paths = false;
     s->h_status.clear();
 }
@@ -912,7 +923,7 @@ int nwg_store_destroy(nwg_store* s) {
     return guarded([&] {
         if (!s) return;
         cudaSetDevice(s->device);
-        s->hard_plan.reset(); s->soft_plan.reset(); s->band_plan.reset();
+        s->hard_plan.reset(); s->soft_plan.reset(); s->band_plan.reset(); s->soft_band_plan.reset();
         for (DBuf* b : {&s->a, &s->b, &s->doa, &s->dob, &s->tracks, &s->gtracks, &s->matf, &s->gapf, &s->matd,
                         &s->gapd, &s->bx0f, &s->bx0d, &s->score, &s->end, &s->grad, &s->guide, &s->status,
                         &s->stripe_tab, &s->codes, &s->scratch, &s->part, &s->red, &s->moves,
@@ -951,7 +962,6 @@ int nwg_run(nwg_store* s, const nwg_job* job, void* stream, double* total) {
         if (J.gap_model < 0 || J.gap_model > 1 || J.mode < 0 || J.mode > 1 || J.grad_mode < 0 || J.grad_mode > 2)
             throw Error(NWG_EINVAL, "bad job");
         if (J.precision != 32 && J.precision != 64) throw Error(NWG_EINVAL, "precision must be 32 or 64");
-        if (J.band >= 0 && J.grad_mode == 2) throw Error(NWG_EINVAL, "soft banded re-alignment is not available in this build");
         if (J.band >= 0 && !s->have_guides) throw Error(NWG_ESTATE, "banded_grad() needs a guide; call score_and_grad() first");
         NWG_CUDA(cudaSetDevice(s->device));
         cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -1030,7 +1040,7 @@ int nwg_set_geometry(nwg_store* s, int soft, int size_class_, int lanes, int row
             s->geo_table[{soft ? 1 : 0, size_class_}] = {lanes, rows};
             s->plain = false;
         }
-        s->hard_plan.reset(); s->soft_plan.reset();
+        s->hard_plan.reset(); s->soft_plan.reset(); s->soft_band_plan.reset();
     });
 }
 

@@ -88,7 +88,7 @@ __host__ __device__ inline size_t hard_mw_smem_bytes(int warps, int tsize) {
 constexpr int kHardSpinLimit = 1 << 22;
 
 template <class T, bool AFF, bool LOC, bool TR, int G, int R, bool BAND = false, bool MW = false>
-__global__ void __launch_bounds__(128) hard_fill_kernel(const HardArgs A) {
+__global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArgs A) {
     static_assert(!MW || (G == 32 && !BAND), "several warps per pair: 32 lanes, full DP");
     constexpr int GR = G * R;
     extern __shared__ __align__(16) unsigned char smem_raw[];

@@ -54,6 +54,8 @@ struct SoftArgs {
     int64_t bnd_off;                         // bytes from a slot's start to its boundary rows
     int64_t warp_stride;                     // several warps per pair: bytes of one warp's table
                                              // and exponents (each warp recomputes its stripes)
+    const int32_t* guide;                    // banded: per pair m + 1 guide columns at oa[p] + p
+    int band;                                // banded: half-width
     int renorm_mask;                         // renormalise when (step & renorm_mask) == 0
     double temperature;
     double* score; double* grad; int64_t gstride;
@@ -137,9 +139,15 @@ __host__ __device__ inline size_t soft_smem_bytes(int K, int N, int G, int R, in
 // (status 3) and every warp finishes the pass without waiting further.
 constexpr int kSpinLimit = 1 << 22;
 
-template <class T, bool AFF, bool LOC, bool TR, int G, int R, bool MW = false>
-__global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftArgs A) {
+// BAND: the guide-banded forward-backward (aligner.hpp:6231-6524 with AlignBand::GuideBanded):
+// the full DP is swept, and cells outside the band are zero -- forward cells of row i >= 1
+// outside [jlo(i), jhi(i)], Global border cells past border_rows / border_cols, backward cells
+// outside [jlo0(i), jhi0(i)]; Local log Z sums the band only.  Zero cells neither receive nor
+// pass on probability, which is what the reference's band-limited tables compute.
+template <class T, bool AFF, bool LOC, bool TR, int G, int R, bool MW = false, bool BAND = false>
+__global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? 4 : 1))) soft_kernel(const SoftArgs A) {
     static_assert(!MW || (G == 32 && !TR), "several warps per pair: 32 lanes, untracked");
+    static_assert(!BAND || (G == 32 && !MW), "banded: 32 lanes, one warp per pair");
     constexpr int GR = G * R;
     constexpr int NV = AFF ? 3 : 1;          // values per cell
     constexpr int CV = NV * R;               // values per lane column
@@ -230,6 +238,28 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
         };
         const int rows = m + 1;                 // DP rows 0..m
         const int nstripes = (rows + GR - 1) / GR;
+        // banded: the band of row i (aligner.hpp:2644-2700) and the charged borders
+        const int32_t* gd = BAND ? A.guide + ao + p : nullptr;
+        const int bw = A.band;
+        auto jlo_of = [&](int i) { return max(1, gd[i] - bw); };
+        auto jlo0_of = [&](int i) { return max(0, gd[i] - bw); };
+        auto jhi_of = [&](int i) {
+            if (!LOC && i == m) return n;
+            int hi = gd[i] + bw;
+            if (i < m) hi = max(hi, gd[i + 1] - 1 + bw);
+            return min(n, hi);
+        };
+        int brows = m, bcols = n;
+        if constexpr (BAND) {
+            // border rows: the leading rows 1.. whose guide is within the band of column 0
+            brows = m;
+            for (int base = 1; base <= m; base += G) {
+                const int i = base + lane;
+                const unsigned over = __ballot_sync(gmask, i <= m && gd[i] > bw);
+                if (over) { brows = base + __ffs(over) - 2; break; }
+            }
+            bcols = jhi_of(0);
+        }
         const int S = n + G;                    // steps: columns 0..n plus the skew
         const int SP = S + 1;                   // MW: progress key per stripe
         bool bad = false;
@@ -255,10 +285,16 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
             T roa[TR ? R : 1], rea[TR ? R : 1], rob[TR ? R : 1], reb[TR ? R : 1];
             T vmask[R];
             T cM[R], cX[R], cY[R];
+            int blo[BAND ? R : 1], bhi[BAND ? R : 1], blo0[BAND ? R : 1];
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 const int i = i0 + r;
                 const bool valid = i <= m;
+                if constexpr (BAND) {
+                    blo[r] = valid ? jlo_of(i) : n + 1;
+                    bhi[r] = valid ? jhi_of(i) : -1;
+                    blo0[r] = valid ? jlo0_of(i) : n + 1;
+                }
                 vmask[r] = valid ? T(1) : T(0);
                 key[r] = (valid && i >= 1) ? (tset(i) * N + ap[i - 1]) * wcols : K * N * wcols;
                 if constexpr (TR) {
@@ -344,10 +380,22 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
                                 if (i == 0 && j == 0) fm = lone;
                             }
                         }
+                        if constexpr (BAND) {
+                            if (i >= 1 && j >= 1) {
+                                if (j < blo[r] || j > bhi[r]) { fm = T(0); fx = T(0); fy = T(0); }
+                            } else if constexpr (!LOC) {
+                                if (i == 0 && j > bcols) fy = T(0);
+                                if (j == 0 && i > brows) fx = T(0);
+                            }
+                        }
                         pM = cM[r]; pX = cX[r]; pY = cY[r];
                         cM[r] = fm; cX[r] = fx; cY[r] = fy;
                         qM = fm; qX = fx; qY = fy;
-                        if constexpr (LOC) zpart = fmaf_t(vmask[r], (fm + fx) + fy, zpart);
+                        if constexpr (LOC) {
+                            T zm_ = vmask[r];
+                            if constexpr (BAND) zm_ = (j >= blo0[r] && j <= bhi[r]) ? zm_ : T(0);
+                            zpart = fmaf_t(zm_, (fm + fx) + fy, zpart);
+                        }
                     }
                     dgM = upM; dgX = upX; dgY = upY;
                     if ((t & rmask) == 0 || j == n) {
@@ -502,10 +550,15 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
             int gsr[TR ? R : 1], tsd[TR ? R : 1];
             T vmask[R];
             T bM[R], bX[R], bY[R];
+            int bblo0[BAND ? R : 1], bbhi[BAND ? R : 1];
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 const int i = i0 + r;
                 const bool valid = i <= m;
+                if constexpr (BAND) {
+                    bblo0[r] = valid ? jlo0_of(i) : n + 1;
+                    bbhi[r] = valid ? jhi_of(i) : -1;
+                }
                 vmask[r] = valid ? T(1) : T(0);
                 const int td = (i + 1 <= m) ? tset(i + 1) : 0;
                 const int kd = (i + 1 <= m) ? (td * N + ap[i]) : K * N;
@@ -644,6 +697,9 @@ __global__ void __launch_bounds__(128, (G > 1 ? 4 : 1)) soft_kernel(const SoftAr
                                 sx_b = fmaf_t(fm, dX, sx_b);
                                 sx_a = fmaf_t(fm, rY, sx_a);
                             }
+                        }
+                        if constexpr (BAND) {
+                            if (j < bblo0[r] || j > bbhi[r]) { nM = T(0); nX = T(0); nY = T(0); }
                         }
                         dM = bM[r];
                         bM[r] = nM; bX[r] = nX; bY[r] = nY;

@@ -5,6 +5,7 @@ namespace nwg {
 namespace {
 template <class T, bool AFF, bool LOC, bool TR>
 SoftFn pick(Geo g) {
+    if (g.band) return (g.G == 32 && g.R == 4 && g.mw <= 1) ? &soft_kernel<T, AFF, LOC, TR, 32, 4, false, true> : nullptr;
     if constexpr (!TR) {
         if (g.mw > 1) return (g.G == 32 && g.R == 4) ? &soft_kernel<T, AFF, LOC, false, 32, 4, true> : nullptr;
     } else {

@@ -51,7 +51,7 @@ def lib():
                                                       _dp, _dp, _i32p, _u8p, C.c_int64, _i64p, _i32p]
         L.orc_hard_batch.restype = C.c_int
         L.orc_soft_batch.argtypes = [C.c_int] * 4 + [_dp, _dp, _u8p, _i64p, _u8p, _i64p, C.c_int64,
-                                                      _u16p, _u16p, C.c_double, _dp, _dp]
+                                                      _u16p, _u16p, C.c_double, _dp, _dp, _i32p, C.c_int]
         L.orc_soft_batch.restype = C.c_int
         L.orc_hb_batch.argtypes = [C.c_int] * 4 + [_dp, _dp, _u8p, _i64p, _u8p, _i64p, C.c_int64,
                                                     _dp, _dp, _i32p, _u8p, C.c_int64, _i64p]
@@ -138,8 +138,9 @@ def hirschberg(prec, mat, gaps, enc: Encoded, cutoff=512, pmax=False, moves_cap=
     return dict(scores=scores, grads=grads, guides=guides, moves=moves, nmoves=nmoves)
 
 
-def soft(gm, am, mat, gaps, enc: Encoded, temperature=1.0):
-    """Log-space double forward-backward: (scores = T log Z, grads = expected counts)."""
+def soft(gm, am, mat, gaps, enc: Encoded, temperature=1.0, guides_in=None, band=-1):
+    """Log-space double forward-backward: (scores = T log Z, grads = expected counts); with
+    guides_in and band >= 0 the guide-banded one."""
     L = lib()
     mat = np.ascontiguousarray(mat, np.float64)
     gaps = np.ascontiguousarray(gaps, np.float64)
@@ -150,7 +151,9 @@ def soft(gm, am, mat, gaps, enc: Encoded, temperature=1.0):
     rc = L.orc_soft_batch(gm, am, N, K, _p(mat, _dp), _p(gaps, _dp), _p(enc.a, _u8p),
                           _p(enc.oa, _i64p), _p(enc.b, _u8p), _p(enc.ob, _i64p), enc.n,
                           _p(enc.tracks, _u16p), _p(enc.gap_tracks, _u16p), float(temperature),
-                          _p(scores, _dp), _p(grads, _dp))
+                          _p(scores, _dp), _p(grads, _dp),
+                          _p(None if guides_in is None else np.ascontiguousarray(guides_in, np.int32), _i32p),
+                          int(band))
     assert rc == 0
     return scores, grads
 

@@ -13,7 +13,8 @@
 //   guide_j and its gap interpolation ...... aligner.hpp:3155-3160, 2734-2749
 //   tracks: per-row sets, column-0 border by runs of equal extends ... aligner.hpp:1919-2007
 //   banded rows (guide band) ............... aligner.hpp:2644-2700 (jlo/jhi/border_rows)
-//   soft (log space) forward/backward ...... aligner.hpp:6231-6330 (linear), 6362-6524 (affine)
+//   soft (log space) forward/backward ...... aligner.hpp:6231-6330 (linear), 6362-6524 (affine),
+//                                            guide-banded too (jlo/jhi/jlo0/jhi0, 2644-2700)
 //   soft temperature: theta/T, log Z * T ... aligner.hpp:6594-6626
 //   blocked weighted sum of gradients ...... batch_engine.hpp:1788-1827
 //   Hirschberg (exact and prefix-max carry)  aligner.hpp:4151-4560 (hb_fwd, hb_rev, hb_base,
@@ -605,8 +606,12 @@ void setup_drows(DRows& R, const Model& M, const uint8_t* a, int m, const uint16
 
 struct SoftOut { double logz = 0; double* grad = nullptr; };
 
+// Band bd (full when bd.band < 0): the guide-banded forward-backward (aligner.hpp:6362-6524
+// with AlignBand::GuideBanded): forward cells j in [jlo(i), jhi(i)], borders limited to
+// border_rows / border_cols (Global), Local log Z over [jlo0(i), jhi0(i)], backward sources
+// and gradient sums over the band; cells outside it read -inf.
 void soft_affine(const Model& M, const uint8_t* a, int m, const uint8_t* b, int n,
-                 const uint16_t* track, const uint16_t* gtrack, double T, SoftOut& o) {
+                 const uint16_t* track, const uint16_t* gtrack, double T, SoftOut& o, const Band& bd) {
     (void)a;
     const double NI = -std::numeric_limits<double>::infinity();
     const bool local = M.am == 1;
@@ -618,14 +623,15 @@ void soft_affine(const Model& M, const uint8_t* a, int m, const uint8_t* b, int 
     auto sub = [&](int i, int j) { return M.mat[size_t(R.rs[i - 1]) * M.N + b[j - 1]] * invT; };
     if (!local) {
         FM[I(0, 0)] = 0.0;
-        for (int i = 1; i <= m; ++i) FX[I(i, 0)] = R.bx0[i];
-        for (int j = 1; j <= n; ++j) FY[I(0, j)] = -(R.goa[0] + double(j) * R.gea[0]);
+        const int bi = bd.border_rows(), bj = bd.border_cols();
+        for (int i = 1; i <= bi; ++i) FX[I(i, 0)] = R.bx0[i];
+        for (int j = 1; j <= bj; ++j) FY[I(0, j)] = -(R.goa[0] + double(j) * R.gea[0]);
     } else {
         for (int i = 0; i <= m; ++i) FM[I(i, 0)] = 0.0;
         for (int j = 0; j <= n; ++j) FM[I(0, j)] = 0.0;
     }
     for (int i = 1; i <= m; ++i)
-        for (int j = 1; j <= n; ++j) {
+        for (int j = bd.jlo(i); j <= bd.jhi(i); ++j) {
             const double diag = lse3(FM[I(i - 1, j - 1)], FX[I(i - 1, j - 1)], FY[I(i - 1, j - 1)]);
             double mv = diag + sub(i, j);
             const double gob = R.gob[i], geb = R.geb[i], goa = R.goa[i], gea = R.gea[i];
@@ -638,13 +644,13 @@ void soft_affine(const Model& M, const uint8_t* a, int m, const uint8_t* b, int 
     if (!local) lz = lse3(FM[I(m, n)], FX[I(m, n)], FY[I(m, n)]);
     else {
         lz = NI;
-        for (int i = 0; i <= m; ++i) for (int j = 0; j <= n; ++j)
+        for (int i = 0; i <= m; ++i) for (int j = bd.jlo0(i); j <= bd.jhi0(i); ++j)
             lz = lse2(lz, lse3(FM[I(i, j)], FX[I(i, j)], FY[I(i, j)]));
     }
     std::vector<double> BM(cells, local ? 0.0 : NI), BX(BM), BY(BM);
     if (!local) { BM[I(m, n)] = 0; BX[I(m, n)] = 0; BY[I(m, n)] = 0; }
     for (int i = m; i >= 0; --i)
-        for (int j = n; j >= 0; --j) {
+        for (int j = bd.jhi0(i); j >= bd.jlo0(i); --j) {
             const double bm = BM[I(i, j)], bx = BX[I(i, j)], by = BY[I(i, j)];
             if (bm != NI && i > 0 && j > 0) {
                 const double c = bm + sub(i, j);
@@ -670,33 +676,33 @@ void soft_affine(const Model& M, const uint8_t* a, int m, const uint8_t* b, int 
     auto gap = [&](int set, int f) -> double& { return g[NN + 4 * size_t(set) + f]; };
     const int gmin_j = local ? 1 : 0, gmin_i = local ? 1 : 0;
     for (int i = 1; i <= m; ++i)
-        for (int j = 1; j <= n; ++j) {
+        for (int j = bd.jlo(i); j <= bd.jhi(i); ++j) {
             const double bm = BM[I(i, j)];
             if (bm == NI) continue;
             const double pred = lse3(FM[I(i - 1, j - 1)], FX[I(i - 1, j - 1)], FY[I(i - 1, j - 1)]);
             g[size_t(R.rs[i - 1]) * M.N + b[j - 1]] += std::exp(pred + sub(i, j) + bm - lz);
         }
     for (int i = 1; i <= m; ++i)
-        for (int j = 0; j <= n; ++j) {
+        for (int j = bd.jlo0(i); j <= bd.jhi0(i); ++j) {
             const double fx = FX[I(i, j)], bx = BX[I(i, j)];
             if (fx == NI || bx == NI) continue;
             gap(R.trk[i - 1], kExtendB) -= std::exp(fx + bx - lz);
         }
     for (int i = 0; i <= m; ++i)
-        for (int j = 1; j <= n; ++j) {
+        for (int j = std::max(1, bd.jlo0(i)); j <= bd.jhi0(i); ++j) {
             const double fy = FY[I(i, j)], by = BY[I(i, j)];
             if (fy == NI || by == NI) continue;
             gap(R.gtrk[i], kExtendA) -= std::exp(fy + by - lz);
         }
     for (int i = 1; i <= m; ++i)
-        for (int j = gmin_j; j <= n; ++j) {
+        for (int j = std::max(gmin_j, bd.jlo0(i)); j <= bd.jhi0(i); ++j) {
             const double bx = BX[I(i, j)];
             if (bx == NI) continue;
             const double lo = lse2(FM[I(i - 1, j)], FY[I(i - 1, j)]) - R.gob[i] - R.geb[i] + bx - lz;
             if (lo > -700) gap(R.trk[i - 1], kOpenB) -= std::exp(lo);
         }
     for (int i = gmin_i; i <= m; ++i)
-        for (int j = 1; j <= n; ++j) {
+        for (int j = std::max(1, bd.jlo0(i)); j <= bd.jhi0(i); ++j) {
             const double by = BY[I(i, j)];
             if (by == NI) continue;
             const double lo = lse2(FM[I(i, j - 1)], FX[I(i, j - 1)]) - R.goa[i] - R.gea[i] + by - lz;
@@ -706,7 +712,7 @@ void soft_affine(const Model& M, const uint8_t* a, int m, const uint8_t* b, int 
 }
 
 void soft_linear(const Model& M, const uint8_t* a, int m, const uint8_t* b, int n,
-                 const uint16_t* track, const uint16_t* gtrack, double T, SoftOut& o) {
+                 const uint16_t* track, const uint16_t* gtrack, double T, SoftOut& o, const Band& bd) {
     const double NI = -std::numeric_limits<double>::infinity();
     const bool local = M.am == 1;
     const double invT = 1.0 / T;
@@ -717,24 +723,28 @@ void soft_linear(const Model& M, const uint8_t* a, int m, const uint8_t* b, int 
     auto sub = [&](int i, int j) { return M.mat[size_t(R.rs[i - 1]) * M.N + b[j - 1]] * invT; };
     if (!local) {
         F[I(0, 0)] = 0.0;
-        for (int i = 1; i <= m; ++i) F[I(i, 0)] = R.bx0[i];
-        for (int j = 1; j <= n; ++j) F[I(0, j)] = -double(j) * R.gea[0];
+        const int bi = bd.border_rows(), bj = bd.border_cols();
+        for (int i = 1; i <= bi; ++i) F[I(i, 0)] = R.bx0[i];
+        for (int j = 1; j <= bj; ++j) F[I(0, j)] = -double(j) * R.gea[0];
     } else {
         for (int i = 0; i <= m; ++i) F[I(i, 0)] = 0.0;
         for (int j = 0; j <= n; ++j) F[I(0, j)] = 0.0;
     }
     for (int i = 1; i <= m; ++i)
-        for (int j = 1; j <= n; ++j) {
+        for (int j = bd.jlo(i); j <= bd.jhi(i); ++j) {
             double v = lse3(F[I(i - 1, j - 1)] + sub(i, j), F[I(i - 1, j)] - R.geb[i], F[I(i, j - 1)] - R.gea[i]);
             if (local) v = lse2(v, 0.0);
             F[I(i, j)] = v;
         }
     double lz;
     if (!local) lz = F[I(m, n)];
-    else { lz = NI; for (size_t k = 0; k < cells; ++k) lz = lse2(lz, F[k]); }
+    else {
+        lz = NI;
+        for (int i = 0; i <= m; ++i) for (int j = bd.jlo0(i); j <= bd.jhi0(i); ++j) lz = lse2(lz, F[I(i, j)]);
+    }
     if (!local) B[I(m, n)] = 0.0;
     for (int i = m; i >= 0; --i)
-        for (int j = n; j >= 0; --j) {
+        for (int j = bd.jhi0(i); j >= bd.jlo0(i); --j) {
             const double bv = B[I(i, j)];
             if (bv == NI) continue;
             if (i > 0 && j > 0) B[I(i - 1, j - 1)] = lse2(B[I(i - 1, j - 1)], bv + sub(i, j));
@@ -746,19 +756,19 @@ void soft_linear(const Model& M, const uint8_t* a, int m, const uint8_t* b, int 
     auto gap = [&](int set, int f) -> double& { return g[NN + 4 * size_t(set) + f]; };
     const int gmin_j = local ? 1 : 0, gmin_i = local ? 1 : 0;
     for (int i = 1; i <= m; ++i)
-        for (int j = 1; j <= n; ++j) {
+        for (int j = bd.jlo(i); j <= bd.jhi(i); ++j) {
             const double bv = B[I(i, j)];
             if (bv == NI) continue;
             g[size_t(R.rs[i - 1]) * M.N + b[j - 1]] += std::exp(F[I(i - 1, j - 1)] + sub(i, j) + bv - lz);
         }
     for (int i = 1; i <= m; ++i)
-        for (int j = gmin_j; j <= n; ++j) {
+        for (int j = std::max(gmin_j, bd.jlo0(i)); j <= bd.jhi0(i); ++j) {
             const double bv = B[I(i, j)], fv = F[I(i - 1, j)];
             if (bv == NI || fv == NI) continue;
             gap(R.trk[i - 1], kExtendB) -= std::exp(fv - R.geb[i] + bv - lz);
         }
     for (int i = gmin_i; i <= m; ++i)
-        for (int j = 1; j <= n; ++j) {
+        for (int j = std::max(1, bd.jlo0(i)); j <= bd.jhi0(i); ++j) {
             const double bv = B[I(i, j)], fv = F[I(i, j - 1)];
             if (bv == NI || fv == NI) continue;
             gap(R.gtrk[i], kExtendA) -= std::exp(fv - R.gea[i] + bv - lz);
@@ -1005,10 +1015,11 @@ int orc_hard_batch(int prec, int gm, int am, int N, int K, const double* mat, co
 
 // Soft gradient in log space, double, at temperature T: scores = T * log Z(theta/T),
 // grads = expected counts under theta/T (gap fields negative).
+// guides_in (oa[p] + p offsets, m + 1 each) with band >= 0: the guide-banded forward-backward.
 int orc_soft_batch(int gm, int am, int N, int K, const double* mat, const double* gaps,
                    const uint8_t* a, const int64_t* oa, const uint8_t* b, const int64_t* ob,
                    int64_t n_pairs, const uint16_t* tracks, const uint16_t* gtracks,
-                   double temperature, double* scores, double* grads) {
+                   double temperature, double* scores, double* grads, const int32_t* guides_in, int band) {
     Model M{gm, am, N, K, mat, gaps};
     const size_t gs = size_t(K) * N * N + 4 * size_t(K);
     for (int64_t p = 0; p < n_pairs; ++p) {
@@ -1018,8 +1029,10 @@ int orc_soft_batch(int gm, int am, int N, int K, const double* mat, const double
         std::fill(o.grad, o.grad + gs, 0.0);
         const uint16_t* tk = tracks ? tracks + oa[p] : nullptr;
         const uint16_t* gk = gtracks ? gtracks + oa[p] + p : nullptr;
-        if (gm == 0) soft_linear(M, a + oa[p], m, b + ob[p], n, tk, gk, temperature, o);
-        else         soft_affine(M, a + oa[p], m, b + ob[p], n, tk, gk, temperature, o);
+        Band bd; bd.m = m; bd.n = n; bd.global = am == 0;
+        if (guides_in && band >= 0) { bd.band = band; bd.g = guides_in + oa[p] + p; }
+        if (gm == 0) soft_linear(M, a + oa[p], m, b + ob[p], n, tk, gk, temperature, o, bd);
+        else         soft_affine(M, a + oa[p], m, b + ob[p], n, tk, gk, temperature, o, bd);
         scores[p] = o.logz;
     }
     return 0;

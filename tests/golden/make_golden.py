@@ -16,6 +16,8 @@ Two sources, both the reference's own code run here:
   T = 1 and 0.5, tracked with three parameter sets, and banded re-alignment after a step.
 * ``hirschberg.npz`` -- the same engine with traceback "hirschberg" and "hirschberg_pmax"
   (affine Global, small hb_cutoff so pairs split several times), float32 and float64.
+* ``soft_banded.npz`` -- SeqPairBatchT<double> soft (log space): score_and_grad, set_params,
+  banded_grad(bw) around the Viterbi guides, every gap model and mode, bw 1, 3, 8.
 """
 from __future__ import annotations
 
@@ -174,11 +176,37 @@ def hb_fixtures():
     print("hirschberg.npz:", len(out), "arrays")
 
 
+def soft_banded_fixtures():
+    rng = np.random.default_rng(321)
+    AA = "ACDEFGHIKLMNPQRSTVWY"
+    out = {}
+    mat = rng.normal(0, 2, size=(1, 20, 20)).round(3)
+    gaps = rng.uniform(0.3, 3.0, size=(1, 4)).round(3)
+    mat2 = (mat + rng.normal(0, 0.3, size=mat.shape)).round(3)
+    gaps2 = (gaps + rng.uniform(0, 0.2, size=gaps.shape)).round(3)
+    sa = ["".join(rng.choice(list(AA), size=int(rng.integers(1, 90)))) for _ in range(14)]
+    sb = []
+    for s in sa:
+        t = [c if rng.random() > 0.25 else str(rng.choice(list(AA))) for c in s]
+        sb.append("".join(t) if rng.random() > 0.2 else "".join(rng.choice(list(AA), size=int(rng.integers(1, 90)))))
+    out.update(mat=mat, gaps=gaps, mat2=mat2, gaps2=gaps2, sa=np.array(sa), sb=np.array(sb))
+    for gm in (0, 1):
+        for am in (0, 1):
+            for bw in (1, 3, 8):
+                r = oracle.ref_run(64, gm, am, 2, AA, mat, gaps, sa, sb, soft_impl=2, band=bw, mat2=mat2, gaps2=gaps2)
+                out[f"g{gm}_m{am}_b{bw}_scores"] = r["scores"]
+                out[f"g{gm}_m{am}_b{bw}_grads"] = r["grads"]
+    np.savez_compressed(os.path.join(HERE, "soft_banded.npz"), **out)
+    print("soft_banded.npz:", len(out), "arrays")
+
+
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["brute", "ref", "hb"]
+    which = sys.argv[1:] or ["brute", "ref", "hb", "sb"]
     if "brute" in which:
         brute_fixtures()
     if "ref" in which:
         ref_fixtures()
     if "hb" in which:
         hb_fixtures()
+    if "sb" in which:
+        soft_banded_fixtures()

@@ -347,3 +347,32 @@ def test_hard_long_tracked_several_warps_per_pair():
     alpha = "ACGTU"
     mat, gaps, sa, sb, tr, gt = _problem(rng, alpha, 3, 1600, 2200, K=3, tracked=True, gap_tracks=True)
     _hard_check(32, 1, 0, alpha, mat, gaps, sa, sb, tr, gt, True)
+
+
+@pytest.mark.parametrize("prec", [32, 64])
+@pytest.mark.parametrize("gm", [0, 1])
+@pytest.mark.parametrize("am", [0, 1])
+@pytest.mark.parametrize("bw", [1, 5, 64])
+def test_soft_banded(prec, gm, am, bw):
+    """Soft banded re-alignment after set_params, around the Viterbi guides of the first
+    parameters (the deferred soft guide), within tolerance of the oracle's banded pass."""
+    rng = np.random.default_rng(1900 + prec + gm + 2 * am + bw)
+    mat, gaps, sa, sb, tr, gt = _problem(rng, AA, 30, 1, 120, integer=False, homolog=True)
+    sa += rand_seqs(rng, 2, 300, 500, AA) + ["", "C"]
+    sb += [mutate(rng, s, AA) for s in sa[-4:-2]] + ["W", ""]
+    mat2 = mat + rng.normal(0, 0.3, size=mat.shape)
+    gaps2 = gaps + rng.uniform(0, 0.2, size=gaps.shape)
+    cls = nw.SeqPairBatch if prec == 32 else nw.SeqPairBatchDouble
+    b = cls(sa, sb, _params(AA, mat, gaps), gap_model=("linear", "affine")[gm], mode=("global", "local")[am],
+            grad_mode="soft")
+    b.score_and_grad()
+    b.set_params(_params(AA, mat2, gaps2))
+    b.banded_grad(bw)
+    enc = oracle.Encoded(encode(AA, sa), encode(AA, sb))
+    g0 = oracle.hard(prec, gm, am, mat, gaps, enc)["guides"]
+    so, go = oracle.soft(gm, am, mat2, gaps2, enc, guides_in=g0, band=bw)
+    np.testing.assert_allclose(b.scores(), so, rtol=SOFT_RTOL, atol=1e-5)
+    gmat, ggap = b.grads()
+    flat = np.concatenate([gmat.reshape(len(sa), -1), ggap.reshape(len(sa), -1)], axis=1)
+    scale = np.maximum(np.abs(go).max(axis=1, keepdims=True), 1.0)
+    assert (np.abs(flat - go) / scale).max() <= SOFT_RTOL

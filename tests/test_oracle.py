@@ -121,3 +121,19 @@ def test_hirschberg_fixtures():
                     np.testing.assert_array_equal(o["scores"], z[key + "scores"])
                     np.testing.assert_array_equal(o["grads"], z[key + "grads"])
                     np.testing.assert_array_equal(o["guides"], z[key + "guides"])
+
+
+def test_soft_banded_fixtures():
+    """The guide-banded soft restatement against the reference's own engine
+    (tests/golden/soft_banded.npz): guides from the Viterbi pass under the first parameters,
+    the banded forward-backward under the second."""
+    z = np.load(os.path.join(GOLD, "soft_banded.npz"))
+    sa, sb = [str(s) for s in z["sa"]], [str(s) for s in z["sb"]]
+    enc = oracle.Encoded(encode(AA, sa), encode(AA, sb))
+    for gm in (0, 1):
+        for am in (0, 1):
+            g0 = oracle.hard(64, gm, am, z["mat"], z["gaps"], enc)["guides"]
+            for bw in (1, 3, 8):
+                s, g = oracle.soft(gm, am, z["mat2"], z["gaps2"], enc, guides_in=g0, band=bw)
+                np.testing.assert_allclose(s, z[f"g{gm}_m{am}_b{bw}_scores"], rtol=1e-12, atol=1e-12)
+                np.testing.assert_allclose(g, z[f"g{gm}_m{am}_b{bw}_grads"], rtol=1e-10, atol=1e-12)
