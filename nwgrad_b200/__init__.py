@@ -9,11 +9,11 @@ kernels behind the C ABI in include/nwgrad_b200.h (libnwgrad_b200.so).
 """
 from .params import (AA20, AlignParams, Alphabet, DNA, DNA_N, IUPAC_DNA, NCBI_PROTEIN, PROTEIN,
                      PROTEIN_UO, PROTEIN_UOX, PROTEIN_X, RNA, RNA_N, SubstMatrix)
-from .batch import SeqPair, SeqPairBatch, SeqPairBatchDouble, SeqPairDouble
+from .batch import BatchResult, SeqPair, SeqPairBatch, SeqPairBatchDouble, SeqPairDouble, guide_j_from_aligned
 
 __all__ = ["AA20", "AlignParams", "Alphabet", "DNA", "DNA_N", "IUPAC_DNA", "NCBI_PROTEIN", "PROTEIN",
            "PROTEIN_UO", "PROTEIN_UOX", "PROTEIN_X", "RNA", "RNA_N", "SubstMatrix", "SeqPair",
-           "SeqPairBatch", "SeqPairBatchDouble", "SeqPairDouble"]
+           "SeqPairBatch", "SeqPairBatchDouble", "SeqPairDouble", "BatchResult", "guide_j_from_aligned"]
 __version__ = "0.1.0"
 
 

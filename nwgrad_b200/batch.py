@@ -309,6 +309,7 @@ class SeqPairBatch:
             return 0.0
         job = self._job(grad_mode, band, keep_paths)
         self._run_id += 1
+        self._path_cache = None
         tot = C.c_double(0.0)
         check(self._store._L.nwg_run(self._store.h, C.byref(job), stream, C.byref(tot)))
         return float(tot.value)
@@ -374,6 +375,7 @@ class SeqPairBatch:
         tot = self._run(gm, band=int(bandwidth), keep_paths=keep_paths)
         self._valid_scores = True
         self._valid_grads = gm != 0
+        self._paths = bool(keep_paths) and gm != 2
         self._guides = None
         return tot
 
@@ -458,8 +460,170 @@ class SeqPairBatch:
             self._guides = g
         return self._guides
 
+    def align(self, seqs_a, seqs_b, params, band: int = 0, aligned_a=(), aligned_b=(), kernel="auto", *,
+              tracks=None, gap_tracks=None) -> BatchResult:
+        """Align (seqs_a[i], seqs_b[i]) under params WITHOUT adding them to this batch: the
+        batch's problem type, grad mode and settings, one transient device store; returns the
+        scores and the gradient summed over the pairs.  band > 0 bands every pair around the
+        guide of aligned_a[i] / aligned_b[i] (the diagonal when none are given)."""
+        if kernel not in _KERNELS:
+            raise ValueError(f"nwgrad: unknown kernel \"{kernel}\"")
+        if len(seqs_a) != len(seqs_b):
+            raise ValueError("nwgrad: seqs_a and seqs_b need equal length")
+        aligned_a, aligned_b = list(aligned_a), list(aligned_b)
+        if (aligned_a or aligned_b) and (len(aligned_a) != len(seqs_a) or len(aligned_b) != len(seqs_a)):
+            raise ValueError("nwgrad: aligned_a / aligned_b need one gapped string per pair")
+        tmp = type(self)(seqs_a, seqs_b, params, gap_model=self._gap_model, mode=self._mode,
+                         grad_mode=self._grad_mode, traceback=self._traceback, tracks=tracks,
+                         gap_tracks=gap_tracks, device=self._device)
+        tmp.soft_temperature = self.soft_temperature
+        tmp.soft_precision = self.soft_precision
+        tmp._hb_cutoff = self._hb_cutoff
+        n = len(seqs_a)
+        if n == 0:
+            return BatchResult(np.zeros(0), AlignParams.zeros_like(params))
+        if band and int(band) > 0:
+            guides = []
+            for i in range(n):
+                m_i, n_i = len(seqs_a[i]), len(seqs_b[i])
+                g = guide_j_from_aligned(aligned_a[i], aligned_b[i]) if aligned_a else _diagonal_guide(m_i, n_i)
+                _validate_guide(g, m_i, n_i)
+                guides.extend(g)
+            gv = np.ascontiguousarray(guides, dtype=np.int32)
+            check(tmp._store._L.nwg_set_guides(tmp._store.h, ptr(gv, _capi._i32p)))
+            tmp._have_guides = True
+            tmp._guides_pending = None
+            gm = _GRAD[tmp._grad_mode]
+            tmp._run(gm, band=int(band))
+            tmp._valid_scores = True
+            tmp._valid_grads = gm != 0
+        else:
+            tmp.score_and_grad()
+        scores = tmp.scores()
+        grad = tmp.compute_grad() if tmp._grad_mode != "none" else AlignParams.zeros_like(params)
+        del tmp
+        return BatchResult(scores, grad)
+
     def drop_paths(self):
+        """Free the stored paths; scores, gradients and guides stay."""
         self._paths = False
+        self._path_cache = None
+
+    # ── stored paths (score_and_grad / banded_grad with keep_paths=True) ─────
+    def _check_stored(self):
+        if not self._valid_scores:
+            raise RuntimeError("nwgrad: alignment not computed; call align() first")
+        if not self._paths:
+            raise RuntimeError("nwgrad: stored path unavailable; use align(keep_paths=True) or "
+                               "banded_align(keep_paths=True)")
+
+    def _stored(self):
+        """(moves_off, moves in walk order, path_info [n_moves, start_i, start_j] per pair)."""
+        self._check_stored()
+        pc = getattr(self, "_path_cache", None)
+        if pc is None:
+            n = self._n
+            mo = np.zeros(n + 1, np.int64)
+            check(self._store._L.nwg_paths(self._store.h, ptr(mo, _capi._i64p), None, 0, None, None))
+            mv = np.zeros(max(int(mo[-1]), 1), np.uint8)
+            info = np.zeros(3 * max(n, 1), np.int32)
+            check(self._store._L.nwg_paths(self._store.h, None, ptr(mv, _capi._u8p), int(mv.size),
+                                           ptr(info, _capi._i32p), None))
+            pc = (mo, mv, info.reshape(-1, 3))
+            self._path_cache = pc
+        return pc
+
+    def _runs(self, i):
+        """Pair i's path as (start_i, start_j, runs of (op, length)): op 0 aligned, 1 a residue
+        of A against a gap, 2 a residue of B against a gap, start to end."""
+        mo, mv, info = self._stored()
+        k, si, sj = int(info[i, 0]), int(info[i, 1]), int(info[i, 2])
+        ops = mv[mo[i]:mo[i] + k][::-1]
+        runs = []
+        for op in ops.tolist():
+            if runs and runs[-1][0] == op:
+                runs[-1][1] += 1
+            else:
+                runs.append([op, 1])
+        return si, sj, runs
+
+    def _codes_of(self, i):
+        if getattr(self, "_codes", None) is not None:
+            a, b = self._codes
+            return a[self._oa[i]:self._oa[i + 1]], b[self._ob[i]:self._ob[i + 1]]
+        return (self._alpha.encode(self._seqs_a[i]), self._alpha.encode(self._seqs_b[i]))
+
+    def aligned(self, i: int):
+        """Pair i's stored alignment as two gapped strings (batch_engine.hpp:515-535)."""
+        si, sj, runs = self._runs(i)
+        ca, cb = self._codes_of(i)
+        sym = self._alpha.symbols
+        a, b = [], []
+        ia, jb = si, sj
+        for op, ln in runs:
+            a.append("".join(sym[x] for x in ca[ia:ia + ln]) if op != 2 else "-" * ln)
+            b.append("".join(sym[x] for x in cb[jb:jb + ln]) if op != 1 else "-" * ln)
+            if op != 2:
+                ia += ln
+            if op != 1:
+                jb += ln
+        return "".join(a), "".join(b)
+
+    def coordinates(self, i: int) -> np.ndarray:
+        """Biopython-style coordinates (2, k) of pair i's stored alignment (batch_engine.hpp:536-550)."""
+        si, sj, runs = self._runs(i)
+        x, y = si, sj
+        ci, cj = [x], [y]
+        for k, (op, ln) in enumerate(runs):
+            if op != 2:
+                x += ln
+            if op != 1:
+                y += ln
+            if k + 1 < len(runs):
+                ci.append(x); cj.append(y)
+        ci.append(x); cj.append(y)
+        return np.array([ci, cj], dtype=np.int64)
+
+    def cigar(self, i: int, extended: bool = False, soft_clip: bool = False) -> str:
+        """Pair i's stored alignment as a SAM CIGAR, seq_a the query (batch_engine.hpp:557-582)."""
+        si, sj, runs = self._runs(i)
+        ca, cb = self._codes_of(i)
+        out = []
+        state = {"op": None, "run": 0}
+
+        def emit(op, n):
+            if not n:
+                return
+            if op == state["op"]:
+                state["run"] += n
+                return
+            if state["run"]:
+                out.append(f"{state['run']}{state['op']}")
+            state["op"], state["run"] = op, n
+
+        if soft_clip:
+            emit("S", si)
+        ia, jb = si, sj
+        for op, ln in runs:
+            if op == 1:
+                emit("I", ln); ia += ln
+            elif op == 2:
+                emit("D", ln); jb += ln
+            elif not extended:
+                emit("M", ln); ia += ln; jb += ln
+            else:
+                for _ in range(ln):
+                    emit("=" if ca[ia] == cb[jb] else "X", 1)
+                    ia += 1; jb += 1
+        if soft_clip:
+            emit("S", len(ca) - ia)
+        if state["run"]:
+            out.append(f"{state['run']}{state['op']}")
+        return "".join(out)
+
+    def cigars(self, extended: bool = False, soft_clip: bool = False) -> list:
+        """Every pair's cigar(), in pair order."""
+        return [self.cigar(i, extended, soft_clip) for i in range(self._n)]
 
     def __getitem__(self, i: int):
         n = self._n
@@ -542,6 +706,66 @@ class SeqPairBatch:
         return float(ms.value), int(n.value)
 
 
+def guide_j_from_aligned(a_aligned: str, b_aligned: str) -> list:
+    """The guide of a gapped alignment: guide[i] = the column of B reached after i residues of
+    A (aligner.hpp:171-190)."""
+    if len(a_aligned) != len(b_aligned):
+        raise ValueError("aligned strings must have equal length")
+    gj = [0]
+    j = 0
+    for x, y in zip(a_aligned, b_aligned):
+        ag, bg = x == "-", y == "-"
+        if ag and bg:
+            raise ValueError("aligned strings have a column with two gaps")
+        if not ag and not bg:
+            j += 1
+            gj.append(j)
+        elif ag:
+            j += 1
+        else:
+            gj.append(j)
+    return gj
+
+
+def _diagonal_guide(m: int, n: int) -> list:
+    """round(i * n / m), halves away from zero (aligner.hpp:1781-1789)."""
+    if m == 0:
+        return [0]
+    return [int(np.floor(i * n / m + 0.5)) for i in range(m + 1)]
+
+
+def _validate_guide(g, m: int, n: int):
+    """A guide must describe the pair: m + 1 columns of B, never moving left."""
+    if len(g) != m + 1:
+        raise ValueError(f"nwgrad: guide_j has {len(g)} entries, but sequence A of length {m} needs {m + 1}")
+    for i, v in enumerate(g):
+        if v < 0 or v > n:
+            raise ValueError(f"nwgrad: guide_j[{i}] = {v} is outside [0, {n}] for sequence B of length {n}")
+        if i > 0 and v < g[i - 1]:
+            raise ValueError(f"nwgrad: guide_j decreases at row {i} ({g[i - 1]} -> {v})")
+
+
+class BatchResult:
+    """What a streaming align() returns: the pairs' scores and their summed gradient."""
+
+    def __init__(self, scores: np.ndarray, grad: AlignParams):
+        self._scores = scores
+        self._grad = grad
+
+    @property
+    def scores(self) -> np.ndarray:
+        """Alignment scores, shape (N,)."""
+        return self._scores
+
+    @property
+    def grad(self) -> AlignParams:
+        """Summed gradient over the batch as an AlignParams object."""
+        return self._grad
+
+    def __repr__(self):
+        return f"BatchResult(n={len(self._scores)})"
+
+
 class SeqPairBatchDouble(SeqPairBatch):
     """SeqPairBatch with the DP in float64."""
     _precision = 64
@@ -581,6 +805,37 @@ class SeqPair:
     def banded_align(self, bandwidth, keep_paths=True) -> float:
         self._batch.banded_grad(bandwidth, keep_paths=keep_paths)
         return self.score
+
+    def aligned(self):
+        """The alignment as a pair of gapped strings (seq_a, seq_b)."""
+        return self._batch.aligned(self._i)
+
+    def coordinates(self) -> np.ndarray:
+        """The alignment as Biopython-style coordinates, an int64 array of shape (2, k)."""
+        return self._batch.coordinates(self._i)
+
+    def cigar(self, *, extended: bool = False, soft_clip: bool = False) -> str:
+        """The alignment as a SAM CIGAR string, seq_a the query and seq_b the reference."""
+        return self._batch.cigar(self._i, extended, soft_clip)
+
+    def formatted(self, width: int = 60) -> str:
+        """Pretty-printed alignment block, wrapped at `width` columns (0 = no wrap)."""
+        a, b = self.aligned()
+        match = "".join(" " if (x == "-" or y == "-") else ("|" if x == y else ".") for x, y in zip(a, b))
+        if width <= 0:
+            width = len(a)
+        blocks = []
+        for off in range(0, len(a), max(width, 1)):
+            blocks.append(a[off:off + width] + "\n" + match[off:off + width] + "\n" + b[off:off + width])
+        return "\n\n".join(blocks)
+
+    def drop_paths(self):
+        self._batch.drop_paths()
+
+    @property
+    def stored_path_valid(self):
+        b = self._batch
+        return bool(b._valid_scores and b._paths)
 
     def set_params(self, params):
         if not self._standalone:

@@ -364,28 +364,30 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? 4 : 1))) so
                             fm = ((pM + pX) + pY) * wv;
                             fx = fmaf_t(qM + qY, o_b, qX * e_b);
                             fy = fmaf_t(cM[r] + cX[r], o_a, cY[r] * e_a);
+                            // row 0 is only ever a lane's first row (r == 0): the test vanishes for r > 0
                             if constexpr (LOC) {
                                 fm += lone;
                                 if (j == 0) fx = T(0);
-                                if (i == 0) fy = T(0);
+                                if (r == 0 && i == 0) fy = T(0);
                             } else {
-                                if (i == 0 && j == 0) fm = lone;
+                                if (r == 0 && i == 0 && j == 0) fm = lone;
                             }
                         } else {
                             fm = fmaf_t(pM, wv, fmaf_t(qM, e_b, cM[r] * e_a));
                             if constexpr (LOC) {
-                                if (i == 0 || j == 0) fm = T(0);
+                                if ((r == 0 && i == 0) || j == 0) fm = T(0);
                                 fm += lone;
                             } else {
-                                if (i == 0 && j == 0) fm = lone;
+                                if (r == 0 && i == 0 && j == 0) fm = lone;
                             }
                         }
                         if constexpr (BAND) {
                             if (i >= 1 && j >= 1) {
                                 if (j < blo[r] || j > bhi[r]) { fm = T(0); fx = T(0); fy = T(0); }
                             } else if constexpr (!LOC) {
-                                if (i == 0 && j > bcols) fy = T(0);
-                                if (j == 0 && i > brows) fx = T(0);
+                                // the charged borders (linear keeps them in M)
+                                if (i == 0 && j > bcols) { fy = T(0); if constexpr (!AFF) fm = T(0); }
+                                if (j == 0 && i > brows) { fx = T(0); if constexpr (!AFF) fm = T(0); }
                             }
                         }
                         pM = cM[r]; pX = cX[r]; pY = cY[r];
@@ -658,7 +660,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? 4 : 1))) so
                         if constexpr (AFF) {
                             const T fx = f[NV * r + 1], fy = f[NV * r + 2];
                             T dX = noX ? T(0) : xX;                    // BX(i+1, j)
-                            T rY = (LOC && i == 0) ? T(0) : bY[r];     // BY(i, j+1)
+                            T rY = (LOC && r == 0 && i == 0) ? T(0) : bY[r];     // BY(i, j+1)
                             nM = fmaf_t(o_a, rY, fmaf_t(o_b, dX, D));
                             nX = fmaf_t(o_a, rY, fmaf_t(e_b, dX, D));
                             nY = fmaf_t(e_a, rY, fmaf_t(o_b, dX, D));
@@ -684,7 +686,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? 4 : 1))) so
                             }
                         } else {
                             T dX = noX ? T(0) : xM;
-                            T rY = (LOC && i == 0) ? T(0) : bM[r];
+                            T rY = (LOC && r == 0 && i == 0) ? T(0) : bM[r];
                             nM = fmaf_t(e_a, rY, fmaf_t(e_b, dX, D));
                             if constexpr (LOC) nM = fmaf_t(vmask[r], lone, nM);
                             else if (i == m && j == n) nM = lone;
