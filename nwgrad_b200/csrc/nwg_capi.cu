@@ -181,7 +181,7 @@ template <class T> SoftFn soft_fn_rt(bool aff, bool loc, bool tr, Geo g) {
 // The kernel geometries (lanes per pair G, rows per lane R) each path is instantiated for.
 bool geo_available(bool soft, int G, int R) {
     if (G == 1) return R == 8 || R == 16 || R == 24 || R == 32;
-    if (soft) return (G == 32 && (R == 2 || R == 4)) || (G == 16 && (R == 2 || R == 4)) || (G == 8 && R == 4);
+    if (soft) return (G == 32 && (R == 2 || R == 4 || R == 8)) || (G == 16 && (R == 2 || R == 4 || R == 8)) || (G == 8 && R == 4);
     return G == 32 && (R == 1 || R == 2 || R == 4 || R == 8);
 }
 

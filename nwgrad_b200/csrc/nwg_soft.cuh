@@ -145,7 +145,7 @@ constexpr int kSpinLimit = 1 << 22;
 // outside [jlo0(i), jhi0(i)]; Local log Z sums the band only.  Zero cells neither receive nor
 // pass on probability, which is what the reference's band-limited tables compute.
 template <class T, bool AFF, bool LOC, bool TR, int G, int R, bool MW = false, bool BAND = false>
-__global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? 4 : 1))) soft_kernel(const SoftArgs A) {
+__global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2 : 4) : 1))) soft_kernel(const SoftArgs A) {
     static_assert(!MW || (G == 32 && !TR), "several warps per pair: 32 lanes, untracked");
     static_assert(!BAND || (G == 32 && !MW), "banded: 32 lanes, one warp per pair");
     constexpr int GR = G * R;
@@ -534,6 +534,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? 4 : 1))) so
 
         // ── backward, fused with the expected counts ─────────────────────────
         double ga_o = 0, ga_x = 0, gb_o = 0, gb_x = 0;   // untracked: opens and extend-only moves
+        bool cnt_nf = false;                             // one lane per pair: a count not finite
         if constexpr (G == 1) {
             double* g1 = A.grad + A.gstride * p;
             for (int k = 0; k < K * N * N; ++k) g1[k] = 0.0;
@@ -784,7 +785,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? 4 : 1))) so
                     if (krow[r] >= K * N) continue;
                     for (int c = 0; c < N; ++c) {
                         T& v = macc[(size_t(c) * G + lane) * R + r];
-                        if (v != T(0)) g1[krow[r] * N + c] += static_cast<double>(v);
+                        if (v != T(0)) { g1[krow[r] * N + c] += static_cast<double>(v); cnt_nf |= !is_finite(v); }
                         v = T(0);
                     }
                 }
@@ -822,6 +823,17 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? 4 : 1))) so
         }
         double* g = A.grad + A.gstride * p;
         const int64_t NN = int64_t(K) * N * N;
+        // counts that left the range of T (a scale factor that overflowed where a product with
+        // it was zero) refuse the pair like any other overflow: the host reruns it in double
+        if (!bad) {
+            bool nf = false;
+            if constexpr (G > 1) { for (int k = lane; k < K * N * N; k += G) nf |= !is_finite(hist[k]); }
+            else nf |= cnt_nf;
+            if constexpr (!TR) nf |= !(is_finite(ga_o) && is_finite(ga_x) && is_finite(gb_o) && is_finite(gb_x));
+            else { for (int k = 0; k < 4 * K; ++k) nf |= !is_finite(tg[k]); }
+            if constexpr (G > 1) nf = __any_sync(gmask, nf);
+            bad = nf;
+        }
         if constexpr (MW) {
             // the pair's totals: every warp's histogram and gap sums, added in warp order
             stalled = __any_sync(gmask, stalled);

@@ -13,7 +13,7 @@ SoftFn pick(Geo g) {
     }
 #define NWG_S(GG, RR) if (g.G == GG && g.R == RR) return &soft_kernel<T, AFF, LOC, TR, GG, RR>;
     NWG_S(1, 8) NWG_S(1, 16) NWG_S(1, 24) NWG_S(1, 32) NWG_S(32, 2) NWG_S(32, 4)
-    NWG_S(16, 2) NWG_S(16, 4) NWG_S(8, 4)
+    NWG_S(16, 2) NWG_S(16, 4) NWG_S(8, 4) NWG_S(16, 8) NWG_S(32, 8)
 #undef NWG_S
     return nullptr;
 }

@@ -22,7 +22,7 @@ import os
 import numpy as np
 
 HARD_GEOS = [(32, 4), (32, 2), (32, 1), (32, 8), (1, 8), (1, 16), (1, 24), (1, 32)]
-SOFT_GEOS = [(32, 4), (32, 2), (16, 4), (16, 2), (8, 4), (1, 8), (1, 16), (1, 24), (1, 32)]
+SOFT_GEOS = [(32, 4), (32, 2), (32, 8), (16, 4), (16, 2), (16, 8), (8, 4), (1, 8), (1, 16), (1, 24), (1, 32)]
 
 
 def size_class(rows: int, cols: int) -> int:
