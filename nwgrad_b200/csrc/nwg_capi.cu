@@ -772,7 +772,10 @@ void run_soft(nwg_store* s, const nwg_job& J, cudaStream_t st) {
     s->grad.need(size_t(s->n) * s->gstride * 8 + 8, st);
     s->status.need(size_t(std::max<int64_t>(s->n, 1)) * 4, st);
     NWG_CUDA(cudaMemsetAsync(s->status.p, 0, size_t(std::max<int64_t>(s->n, 1)) * 4, st));
-    const bool f32 = J.precision == 32 && !J.soft_double;
+    // Banded: the band masks leave whole lane-columns at zero, and a lane whose values are all
+    // zero keeps a stale power-of-two exponent; over a narrow band that can misalign values in
+    // float's range.  The double pass's range makes it harmless, so banded runs go to double.
+    const bool f32 = J.precision == 32 && !J.soft_double && J.band < 0;
     if (f32) soft_pass<float>(s, J, st, nullptr);
     else soft_pass<double>(s, J, st, nullptr);
     s->h_status.assign(size_t(s->n), 0);
