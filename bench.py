@@ -354,12 +354,16 @@ def main():
     ap.add_argument("--checkpoint-mb", type=float, default=-1,
                     help="soft: per-pair forward tables above this many MiB are checkpointed (-1: default)")
     ap.add_argument("--geometry", default=None, help="LANESxROWS for every pair (no tuning), e.g. 32x4")
-    ap.add_argument("--workload", default="c2-soft", choices=["c2-soft", "c1-hard", "c4-long", "c3-short"],
+    ap.add_argument("--workload", default="c2-soft",
+                    choices=["c2-soft", "c1-hard", "c4-long", "c3-short", "c5-serve-train"],
                     help="c2-soft (default): the soft-gradient batch; side measurements: c1-hard (plain hard "
                          "batch), c4-long (64 long pairs: Pointers, Hirschberg, soft, banded), c3-short "
-                         "(many short local linear tracked pairs, hard and soft)")
+                         "(many short local linear tracked pairs, hard and soft), c5-serve-train (the "
+                         "server under a Poisson stream while an autograd loop trains the parameters)")
     ap.add_argument("--long-pairs", type=int, default=64)
     ap.add_argument("--short-pairs", type=int, default=2_000_000)
+    ap.add_argument("--train-pairs", type=int, default=2000, help="c5-serve-train: homolog pairs (as many decoys)")
+    ap.add_argument("--train-steps", type=int, default=200)
     args = ap.parse_args()
     if args.workload == "c1-hard":
         return bench_c1(args)
@@ -367,6 +371,8 @@ def main():
         return bench_c4(args)
     if args.workload == "c3-short":
         return bench_c3(args)
+    if args.workload == "c5-serve-train":
+        return bench_c5(args)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -719,6 +725,106 @@ def bench_c1(args):
                       "unit": "GCUPS", "n_gpus": 1, "steps": args.steps, "ms_per_step": tot / args.steps,
                       "kernel_ms_per_step": kms / args.steps, "config": {"workload": "c1 hard global affine float32, "
                       "10k pairs L 50-300", "cells_per_step": cells}, "step_ms": ms}))
+
+
+def _trainer(pos, neg, mat, gaps0, steps, srv=None):
+    """Adam (lr 1e-3) on the matrix and the four gap costs, maximising the mean homolog - decoy
+    soft-score margin; with a server, it takes the parameters after every step."""
+    import torch
+    import nwgrad_b200 as nw
+    from nwgrad_b200.autograd import align_scores
+    M = torch.tensor(mat[None], dtype=torch.float64, requires_grad=True)
+    G = torch.tensor(gaps0, dtype=torch.float64, requires_grad=True)
+    opt = torch.optim.Adam([M, G], lr=1e-3)
+    margins = []
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        opt.zero_grad()
+        margin = (align_scores(pos, M, G) - align_scores(neg, M, G)).mean()
+        (-margin).backward()
+        opt.step()
+        margins.append(float(margin))
+        if srv is not None:
+            srv.set_params(nw.AlignParams.from_arrays(M.detach().numpy().copy(), G.detach().numpy().copy(),
+                                                      alphabet=nw.AA20))
+    return time.perf_counter() - t0, margins
+
+
+def bench_c5(args):
+    """Side measurement: serving plus an autograd training loop.  A Poisson stream of requests
+    (A lengths log-uniform 20-5000, batch sizes log-uniform 1-4096, B a mutated copy) goes
+    through the continuous-batching server while 200 Adam steps (lr 1e-3) train the 20x20
+    matrix and four gap costs on the soft-gradient batch's pair distribution; after every
+    step the server takes the new parameters.  Each half is also run alone."""
+    import queue
+    import nwgrad_b200 as nw
+    from nwgrad_b200.serve import Server
+    mat, a, oa, bp, obp, bn, obn = c2_workload(args.train_pairs, seed=1)
+    gaps0 = np.array([[11.0, 1.0, 11.0, 1.0]])
+    p0 = nw.AlignParams.from_arrays(mat[None], gaps0, alphabet=nw.AA20)
+    pos = nw.SeqPairBatch.from_codes(a, oa, bp, obp, p0, grad_mode="soft")
+    neg = nw.SeqPairBatch.from_codes(a, oa, bn, obn, p0, grad_mode="soft")
+    train_cells = cells_of(oa, obp) + cells_of(oa, obn)
+    reqs = c5_requests(args.serve_requests)
+    req_cells = sum(cells_of(o1, o2) for _, o1, _, o2 in reqs)
+    steps = args.train_steps
+    _trainer(pos, neg, mat, gaps0, 3)                       # warm: plans, graphs, pools
+    serve_server(p0, reqs[:8], [0.0] * 8, 0)
+    train_alone, margins = _trainer(pos, neg, mat, gaps0, steps)
+    burst = serve_server(p0, reqs, [0.0] * len(reqs), 0)
+    rate = 0.7 * len(reqs) / burst["seconds"]
+    rng = np.random.default_rng(1005)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(reqs))).tolist()
+    serve_alone = serve_server(p0, reqs, arrivals, 0)
+    # both at once
+    lat = []
+    q = queue.Queue()
+    out = {}
+    with Server(p0, grad_mode="soft", workers=3, hbm_budget_gb=96.0, max_batch_pairs=16384, device=0) as srv:
+        def waiter():
+            while True:
+                item = q.get()
+                if item is None:
+                    return
+                lat.append(srv.wait(item[0], item[1])[2])
+
+        def train():
+            out["train"] = _trainer(pos, neg, mat, gaps0, steps, srv)
+
+        wt = threading.Thread(target=waiter, daemon=True)
+        tt = threading.Thread(target=train, daemon=True)
+        wt.start()
+        t0 = time.perf_counter()
+        tt.start()
+        for (ca, o1, cb, o2), at in zip(reqs, arrivals):
+            d = at - (time.perf_counter() - t0)
+            if d > 0:
+                time.sleep(d)
+            q.put((srv.submit_codes(ca, o1, cb, o2), len(o1) - 1))
+        q.put(None)
+        wt.join()
+        serve_span = time.perf_counter() - t0
+        tt.join()
+    p50, p99 = _quantiles(lat)
+    train_mixed, margins_mixed = out["train"]
+    print(json.dumps({
+        "metric": "serve p50/p99 latency and training GCUPS, both at once", "n_gpus": 1,
+        "config": {"workload": "Poisson request stream (lengths log-uniform 20-5000, batch sizes log-uniform "
+                               "1-4096, B mutated) through the server, offered at 70% of its burst capacity, "
+                               f"while {steps} Adam steps (lr 1e-3) train the matrix and gaps on "
+                               f"{args.train_pairs} homolog + {args.train_pairs} decoy pairs (L 100-500); "
+                               "set_params into the server after every step",
+                   "requests": len(reqs), "request_cells": req_cells, "train_cells_per_step": train_cells,
+                   "offered_rate_per_s": rate},
+        "serve_alone": {"p50_ms": serve_alone["p50_ms"], "p99_ms": serve_alone["p99_ms"],
+                        "gcups": serve_alone["gcups"]},
+        "train_alone": {"seconds": train_alone, "steps_per_s": steps / train_alone,
+                        "gcups": train_cells * steps / train_alone / 1e9,
+                        "margin_first": margins[0], "margin_last": margins[-1]},
+        "mixed": {"serve_p50_ms": p50, "serve_p99_ms": p99, "serve_gcups": req_cells / serve_span / 1e9,
+                  "train_seconds": train_mixed, "train_gcups": train_cells * steps / train_mixed / 1e9,
+                  "margin_last": margins_mixed[-1]},
+    }))
 
 
 if __name__ == "__main__":

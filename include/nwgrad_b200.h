@@ -135,6 +135,14 @@ int nwg_status(nwg_store* s, int32_t* out);
 /* Device time (ms) of the last nwg_run's kernels and how many kernels it launched. */
 int nwg_last_timing(nwg_store* s, double* ms, int64_t* launches);
 
+/* Captured bucket sequences (no counterpart in the reference).  With graphs on (the default)
+ * nwg_run runs a plan's per-bucket launches as one CUDA graph, captured on the first call and
+ * replayed while the launches (kernels, shapes, arguments) are unchanged -- across set_params
+ * steps, for one.  Results are the same either way.  nwg_graph_stats counts captures and
+ * replays since the store was made. */
+int nwg_set_graphs(nwg_store* s, int enable);
+int nwg_graph_stats(nwg_store* s, int64_t* captures, int64_t* replays);
+
 /* ── Serving: continuous batching (no counterpart in the reference, a CPU library with
  * no request loop; each request's results equal those of SeqPairBatch.score_and_grad +
  * compute_grad on its pairs alone, batch_engine.hpp:615, 714) ──────────────────────────

@@ -698,6 +698,19 @@ class SeqPairBatch:
         before its backward (bit-identical results).  -1 keeps the current value."""
         check(self._store._L.nwg_set_memory(self._store.h, int(scratch_budget_bytes), int(checkpoint_bytes)))
 
+    def use_graphs(self, enable: bool = True) -> None:
+        """Run each plan's per-bucket launches as one captured CUDA graph (the default), replayed
+        while the launches are unchanged (set_params steps keep them); False launches every
+        bucket directly.  Results are the same either way."""
+        check(self._store._L.nwg_set_graphs(self._store.h, 1 if enable else 0))
+
+    def graph_stats(self):
+        """(captures, replays) of bucket-sequence graphs since the batch was made."""
+        cap = C.c_int64(0)
+        rep = C.c_int64(0)
+        check(self._store._L.nwg_graph_stats(self._store.h, C.byref(cap), C.byref(rep)))
+        return int(cap.value), int(rep.value)
+
     def last_timing(self):
         """(device ms, kernel launches) of the last GPU call."""
         ms = C.c_double(0)

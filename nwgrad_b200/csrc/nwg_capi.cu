@@ -167,6 +167,39 @@ int sm_count(int dev) {
     return v > 0 ? v : 148;
 }
 
+// ── captured launch sequences ────────────────────────────────────────────────
+// A kernel launch held for replay: the function, its shape and its one argument (the
+// kernels take a single plain-data struct).
+struct Launch {
+    const void* fn = nullptr;
+    unsigned grid = 0;
+    int block = 0;
+    size_t smem = 0;
+    std::vector<unsigned char> arg;
+};
+template <class A>
+Launch make_launch(const void* fn, unsigned grid, int block, size_t smem, const A& a) {
+    Launch l;
+    l.fn = fn; l.grid = grid; l.block = block; l.smem = smem;
+    l.arg.resize(sizeof(A));
+    std::memcpy(l.arg.data(), &a, sizeof(A));
+    return l;
+}
+
+// One bucket sequence's CUDA graph: the launches of a plan (one per length bucket) captured
+// once and replayed while the sequence -- functions, shapes and argument bytes, pointers
+// included -- is unchanged.  set_params does not change it (the weights live in buffers that
+// keep their address), a new batch or a grown scratch buffer does (a new capture).
+struct GraphCache {
+    std::vector<unsigned char> key;
+    cudaGraphExec_t exec = nullptr;
+    void reset() {
+        if (exec) cudaGraphExecDestroy(exec);
+        exec = nullptr;
+        key.clear();
+    }
+};
+
 // ── kernel tables (instantiated in nwg_hard_inst.cu / nwg_soft_inst.cu) ─────────
 using HardFn = nwg::HardFn;
 using SoftFn = nwg::SoftFn;
@@ -295,6 +328,14 @@ struct nwg_store {
     DBuf stripe_tab;
     DBuf hb_pairs;                      // the pairs a Hirschberg run splits
     std::vector<int32_t> h_status;
+    // soft weights per precision (kept: a captured graph reads them at a fixed address)
+    DBuf swf, sgwf, swd, sgwd;
+    // captured bucket sequences, replayed on a private stream ordered after the caller's
+    GraphCache g_soft[2], g_soft_band, g_hard[2], g_hard_band;
+    bool use_graphs = true;
+    cudaStream_t gstream = nullptr;
+    cudaEvent_t gev_in = nullptr, gev_out = nullptr;
+    int64_t graph_captures = 0, graph_replays = 0, graph_failures = 0;
     // timing
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double last_ms = 0;
@@ -303,6 +344,77 @@ struct nwg_store {
 };
 
 namespace {
+
+// Run a bucket sequence on `st`.  With graphs on (and a cache given), the sequence runs as a
+// CUDA graph on the store's private stream, which waits for `st` before and makes `st` wait
+// for it after: one graph launch in place of a launch per bucket, captured again only when
+// the sequence changes.
+void run_launches(nwg_store* s, GraphCache* gc, const std::vector<Launch>& L, cudaStream_t st) {
+    if (L.empty()) return;
+    s->last_launches += int64_t(L.size());
+    auto launch_all = [&](cudaStream_t on) {
+        for (const Launch& l : L) {
+            void* args[] = {const_cast<unsigned char*>(l.arg.data())};
+            NWG_CUDA(cudaLaunchKernel(l.fn, dim3(l.grid), dim3(unsigned(l.block)), args, l.smem, on));
+        }
+    };
+    if (!gc || !s->use_graphs) {
+        launch_all(st);
+        return;
+    }
+    std::vector<unsigned char> key;
+    for (const Launch& l : L) {
+        const unsigned char* f = reinterpret_cast<const unsigned char*>(&l.fn);
+        key.insert(key.end(), f, f + sizeof(l.fn));
+        const int64_t shape[3] = {int64_t(l.grid), int64_t(l.block), int64_t(l.smem)};
+        const unsigned char* sh = reinterpret_cast<const unsigned char*>(shape);
+        key.insert(key.end(), sh, sh + sizeof(shape));
+        key.insert(key.end(), l.arg.begin(), l.arg.end());
+    }
+    if (!s->gstream) {
+        NWG_CUDA(cudaStreamCreateWithFlags(&s->gstream, cudaStreamNonBlocking));
+        NWG_CUDA(cudaEventCreateWithFlags(&s->gev_in, cudaEventDisableTiming));
+        NWG_CUDA(cudaEventCreateWithFlags(&s->gev_out, cudaEventDisableTiming));
+    }
+    NWG_CUDA(cudaEventRecord(s->gev_in, st));
+    NWG_CUDA(cudaStreamWaitEvent(s->gstream, s->gev_in, 0));
+    if (!gc->exec || key != gc->key) {
+        gc->reset();
+        cudaGraph_t g = nullptr;
+        NWG_CUDA(cudaStreamBeginCapture(s->gstream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t le = cudaSuccess;
+        for (const Launch& l : L) {
+            void* args[] = {const_cast<unsigned char*>(l.arg.data())};
+            le = cudaLaunchKernel(l.fn, dim3(l.grid), dim3(unsigned(l.block)), args, l.smem, s->gstream);
+            if (le != cudaSuccess) break;
+        }
+        const cudaError_t ee = cudaStreamEndCapture(s->gstream, &g);
+        cudaError_t ie = cudaErrorStreamCaptureInvalidated;
+        if (le == cudaSuccess && ee == cudaSuccess && g) ie = cudaGraphInstantiate(&gc->exec, g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (ie != cudaSuccess) {
+            // a capture that another thread's call invalidated (or that failed to instantiate):
+            // this call launches directly, the next one tries again
+            cudaGetLastError();
+            gc->exec = nullptr;
+            gc->key.clear();
+            s->graph_failures++;
+            if (le != cudaSuccess && le != cudaErrorStreamCaptureInvalidated && le != cudaErrorStreamCaptureUnsupported)
+                NWG_CUDA(le);
+            launch_all(s->gstream);
+            NWG_CUDA(cudaEventRecord(s->gev_out, s->gstream));
+            NWG_CUDA(cudaStreamWaitEvent(st, s->gev_out, 0));
+            return;
+        }
+        gc->key = std::move(key);
+        s->graph_captures++;
+    } else {
+        s->graph_replays++;
+    }
+    NWG_CUDA(cudaGraphLaunch(gc->exec, s->gstream));
+    NWG_CUDA(cudaEventRecord(s->gev_out, s->gstream));
+    NWG_CUDA(cudaStreamWaitEvent(st, s->gev_out, 0));
+}
 
 void set_params_dev(nwg_store* s) {
     const size_t nm = s->mats.size(), ng = s->gaps.size();
@@ -491,6 +603,7 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
         max_total = std::max(max_total, sl * sd);
     }
     s->scratch.need(size_t(max_total) * sizeof(T), st);
+    std::vector<Launch> fills;
     for (auto& B : P.buckets) {
         if (B.pairs.empty()) continue;
         HardFn fn = hard_fn_rt<T>(aff, loc, tr, B.geo);
@@ -517,25 +630,9 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
         A.scratch = s->scratch.p; A.scratch_stride = stride;
         A.row_stride = 3 * (int64_t(B.maxn) + 1);
         A.score = s->score.as<double>(); A.end = s->end.as<int32_t>();
-        fn<<<unsigned(blocks), hblock, smem, st>>>(A);
-        NWG_CUDA(cudaGetLastError());
-        s->last_launches++;
+        fills.push_back(make_launch(reinterpret_cast<const void*>(fn), unsigned(blocks), hblock, smem, A));
     }
-    // several warps per pair: a wait between warps that ran out fails the call (end state 3)
-    bool any_mw = false;
-    for (auto& B : P.buckets) any_mw |= (B.geo.mw > 1 && !B.pairs.empty());
-    if (any_mw && s->n) {
-        std::vector<int32_t> e(size_t(s->n) * 4);
-        NWG_CUDA(cudaMemcpyAsync(e.data(), s->end.p, e.size() * 4, cudaMemcpyDeviceToHost, st));
-        NWG_CUDA(cudaStreamSynchronize(st));
-        for (auto& B : P.buckets)
-            if (B.geo.mw > 1)
-                for (int32_t p : B.pairs)
-                    if (e[4 * size_t(p) + 2] == 3)
-                        throw Error(NWG_ECUDA, "nwgrad_b200: hard fill: a wait between the warps of pair " +
-                                                   std::to_string(p) + " ran out (the kernel gave up instead of hanging)");
-    }
-    // traceback: gradient, guide, path
+    // traceback buffers: gradient, guide, path
     if (want_grad) {
         s->grad.need(size_t(s->n) * s->gstride * 8 + 8, st);
         NWG_CUDA(cudaMemsetAsync(s->grad.p, 0, size_t(s->n) * s->gstride * 8, st));
@@ -567,11 +664,28 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
     W.moves = keep ? s->moves.as<uint8_t>() : nullptr;
     W.moves_off = keep ? s->moves_off.as<int64_t>() : nullptr;
     W.path_info = keep ? s->path_info.as<int32_t>() : nullptr;
-    if (P.n_planned) {
-        nwg::walk_kernel<<<unsigned((P.n_planned + 127) / 128), 128, 0, st>>>(W);
-        NWG_CUDA(cudaGetLastError());
-        s->last_launches++;
+    const Launch walk = make_launch(reinterpret_cast<const void*>(&nwg::walk_kernel),
+                                    unsigned((P.n_planned + 127) / 128), 128, 0, W);
+    // several warps per pair: a wait between warps that ran out fails the call (end state 3),
+    // which the host checks between the fills and the walk; otherwise the fills and the walk
+    // are one captured sequence
+    bool any_mw = false;
+    for (auto& B : P.buckets) any_mw |= (B.geo.mw > 1 && !B.pairs.empty());
+    GraphCache* gc = band ? &s->g_hard_band : &s->g_hard[sizeof(T) == 4 ? 0 : 1];
+    if (!any_mw && P.n_planned) fills.push_back(walk);
+    run_launches(s, gc, fills, st);
+    if (any_mw && s->n) {
+        std::vector<int32_t> e(size_t(s->n) * 4);
+        NWG_CUDA(cudaMemcpyAsync(e.data(), s->end.p, e.size() * 4, cudaMemcpyDeviceToHost, st));
+        NWG_CUDA(cudaStreamSynchronize(st));
+        for (auto& B : P.buckets)
+            if (B.geo.mw > 1)
+                for (int32_t p : B.pairs)
+                    if (e[4 * size_t(p) + 2] == 3)
+                        throw Error(NWG_ECUDA, "nwgrad_b200: hard fill: a wait between the warps of pair " +
+                                                   std::to_string(p) + " ran out (the kernel gave up instead of hanging)");
     }
+    if (any_mw && P.n_planned) run_launches(s, nullptr, std::vector<Launch>{walk}, st);
     if (!hb_pairs.empty()) {
         s->hb_pairs.need(hb_pairs.size() * 4, st);
         NWG_CUDA(cudaMemcpyAsync(s->hb_pairs.p, hb_pairs.data(), hb_pairs.size() * 4, cudaMemcpyHostToDevice, st));
@@ -644,8 +758,10 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
     int pw = 1;
     while (pw * 2 <= std::min(renorm, sizeof(T) == 4 ? 8 : 16)) pw *= 2;
     renorm = pw;
-    DBuf dw, dgw;   // small; freed at scope end
-    struct Free { DBuf& a; DBuf& b; cudaStream_t st; ~Free() { a.release(st); b.release(st); } } fr{dw, dgw, st};
+    // the weights go to buffers the store keeps (one per precision), so a captured sequence
+    // reads this call's weights at the same address
+    DBuf& dw = sizeof(T) == 4 ? s->swf : s->swd;
+    DBuf& dgw = sizeof(T) == 4 ? s->sgwf : s->sgwd;
     dw.need(w.size() * sizeof(T), st); dgw.need(gw.size() * sizeof(T), st);
     NWG_CUDA(cudaMemcpyAsync(dw.p, w.data(), w.size() * sizeof(T), cudaMemcpyHostToDevice, st));
     NWG_CUDA(cudaMemcpyAsync(dgw.p, gw.data(), gw.size() * sizeof(T), cudaMemcpyHostToDevice, st));
@@ -696,6 +812,9 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
     }
     const int sms = sm_count(s->device);
     const int NV = aff ? 3 : 1;
+    std::vector<Launch> launches;
+    std::vector<nwg::SoftArgs> args;
+    int64_t scratch_total = 0;
     for (auto& B : P->buckets) {
         if (B.pairs.empty()) continue;
         SoftFn fn = soft_fn_rt<T>(aff, loc, tr, B.geo);
@@ -737,7 +856,7 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
         int64_t blocks = std::min<int64_t>(mw ? items : (items + gpb - 1) / gpb, int64_t(sms) * occ);
         blocks = std::max<int64_t>(1, std::min<int64_t>(blocks, s->scratch_budget / std::max<int64_t>(1, per_block)));
         const int64_t slots = mw ? blocks : blocks * gpb;
-        s->scratch.need(size_t(slots * stride), st);
+        scratch_total = std::max<int64_t>(scratch_total, slots * stride);
         nwg::SoftArgs A{};
         A.a = s->a.as<uint8_t>(); A.oa = s->doa.as<int64_t>();
         A.b = s->b.as<uint8_t>(); A.ob = s->dob.as<int64_t>();
@@ -745,7 +864,7 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
         A.gtracks = tr ? s->gtracks.as<uint16_t>() : nullptr;
         A.order = d_order + B.off; A.n_items = items;
         A.w = dw.p; A.gw = dgw.p; A.N = N; A.K = K;
-        A.scratch = s->scratch.p; A.scratch_stride = stride; A.fwd_bytes = fwd_bytes;
+        A.scratch = nullptr; A.scratch_stride = stride; A.fwd_bytes = fwd_bytes;   // set below
         A.maxn = B.maxn; A.temperature = J.temperature;
         A.ck = ck; A.max_stripes = int(std::max<int64_t>(max_stripes, 1));
         A.warp_stride = mw ? warp_bytes : 0;
@@ -761,10 +880,18 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
             s->last_launches++;
             continue;
         }
-        fn<<<unsigned(blocks), block, smem, st>>>(A);
-        NWG_CUDA(cudaGetLastError());
-        s->last_launches++;
+        launches.push_back(make_launch(reinterpret_cast<const void*>(fn), unsigned(blocks), block, smem, A));
+        args.push_back(A);
     }
+    if (launches.empty()) return;
+    // one scratch buffer for the sequence (the buckets run one after another)
+    s->scratch.need(size_t(scratch_total), st);
+    for (size_t k = 0; k < launches.size(); ++k) {
+        args[k].scratch = s->scratch.p;
+        std::memcpy(launches[k].arg.data(), &args[k], sizeof(nwg::SoftArgs));
+    }
+    GraphCache* gc = subset ? nullptr : J.band >= 0 ? &s->g_soft_band : &s->g_soft[sizeof(T) == 4 ? 0 : 1];
+    run_launches(s, gc, launches, st);
 }
 
 void run_soft(nwg_store* s, const nwg_job& J, cudaStream_t st) {
@@ -935,8 +1062,15 @@ int nwg_store_destroy(nwg_store* s) {
                         &s->gapd, &s->bx0f, &s->bx0d, &s->score, &s->end, &s->grad, &s->guide, &s->status,
                         &s->stripe_tab, &s->codes, &s->scratch, &s->part, &s->red, &s->moves,
                         &s->moves_off, &s->path_info, &s->tmatf, &s->tgapf, &s->tmatd, &s->tgapd,
-                        &s->tbx0f, &s->tbx0d, &s->tscore, &s->tend, &s->hb_pairs})
+                        &s->tbx0f, &s->tbx0d, &s->tscore, &s->tend, &s->hb_pairs, &s->swf, &s->sgwf,
+                        &s->swd, &s->sgwd})
             b->release();
+        for (GraphCache* g : {&s->g_soft[0], &s->g_soft[1], &s->g_soft_band, &s->g_hard[0], &s->g_hard[1],
+                              &s->g_hard_band})
+            g->reset();
+        if (s->gstream) cudaStreamDestroy(s->gstream);
+        if (s->gev_in) cudaEventDestroy(s->gev_in);
+        if (s->gev_out) cudaEventDestroy(s->gev_out);
         if (s->ev0) cudaEventDestroy(s->ev0);
         if (s->ev1) cudaEventDestroy(s->ev1);
         delete s;
@@ -1168,6 +1302,21 @@ int nwg_paths(nwg_store* s, int64_t* moves_off, uint8_t* moves, int64_t moves_ca
 int nwg_status(nwg_store* s, int32_t* out) {
     return guarded([&] {
         for (int64_t p = 0; p < s->n; ++p) out[p] = p < int64_t(s->h_status.size()) ? s->h_status[p] : 0;
+    });
+}
+
+int nwg_set_graphs(nwg_store* s, int enable) {
+    return guarded([&] {
+        if (!s) throw Error(NWG_EINVAL, "null argument");
+        s->use_graphs = enable != 0;
+    });
+}
+
+int nwg_graph_stats(nwg_store* s, int64_t* captures, int64_t* replays) {
+    return guarded([&] {
+        if (!s) throw Error(NWG_EINVAL, "null argument");
+        if (captures) *captures = s->graph_captures;
+        if (replays) *replays = s->graph_replays;
     });
 }
 

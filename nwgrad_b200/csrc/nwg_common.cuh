@@ -64,6 +64,14 @@ template <> __device__ __forceinline__ int ilog2<double>(double x) {
     if (e) return e - 1023;
     return -1023 - __clzll(static_cast<long long>(u << 12));
 }
+// Bring [p, p + bytes) into L2 ahead of its use (the bulk-copy engine's prefetch: p 16-byte
+// aligned, bytes a multiple of 16); no data returns to the issuing thread.
+__device__ __forceinline__ void prefetch_l2_bulk(const void* p, unsigned bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p) : "memory");
+}
 __device__ __forceinline__ bool is_finite(float x) { return (__float_as_uint(x) & 0x7f800000u) != 0x7f800000u; }
 __device__ __forceinline__ bool is_finite(double x) {
     return (static_cast<unsigned long long>(__double_as_longlong(x)) & 0x7ff0000000000000ull) != 0x7ff0000000000000ull;

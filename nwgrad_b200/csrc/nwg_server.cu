@@ -123,7 +123,12 @@ void run_batch(nwg_server* S, nwg_store*& store, cudaStream_t st, std::vector<st
     if (!store) {
         if (!ck(nwg_store_create(a.data(), oa.data(), b.data(), ob.data(), n, S->nalpha, nullptr, nullptr, S->device, &store)))
             store = nullptr;
-        else ck(nwg_set_memory(store, S->scratch_share, -1));
+        else {
+            ck(nwg_set_memory(store, S->scratch_share, -1));
+            // every served batch is a new plan: a captured sequence would never replay, and a
+            // capture must not overlap the other workers' synchronising calls
+            ck(nwg_set_graphs(store, 0));
+        }
     } else {
         ck(nwg_store_load(store, a.data(), oa.data(), b.data(), ob.data(), n, nullptr, nullptr, st));
     }

@@ -139,6 +139,14 @@ __host__ __device__ inline size_t soft_smem_bytes(int K, int N, int G, int R, in
 // (status 3) and every warp finishes the pass without waiting further.
 constexpr int kSpinLimit = 1 << 22;
 
+// The backward pass reads the forward table one lane-step row (G lanes x R rows x 3 values)
+// per step, in reverse; the row kPrefetchSteps steps ahead is asked into L2 meanwhile, so the
+// register prefetch one step ahead finds it there instead of waiting on HBM.
+#ifndef NWG_SOFT_PREFETCH_STEPS
+#define NWG_SOFT_PREFETCH_STEPS 4
+#endif
+constexpr int kPrefetchSteps = NWG_SOFT_PREFETCH_STEPS;
+
 // BAND: the guide-banded forward-backward (aligner.hpp:6231-6524 with AlignBand::GuideBanded):
 // the full DP is swept, and cells outside the band are zero -- forward cells of row i >= 1
 // outside [jlo(i), jhi(i)], Global border cells past border_rows / border_cols, backward cells
@@ -276,7 +284,9 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
         // repeats the first pass's arithmetic from the same boundary row: the same bits.
         auto fwd_stripe = [&](const int s, const bool pass1) {
             const int i0 = s * GR + lane * R;   // this lane's first DP row (rows 0..m)
-            const bool store_table = !ck || !pass1;
+            // a lane wholly below row m (the last stripe's padding) keeps no table: its backward
+            // values are zero, so its forward values are never needed
+            const bool store_table = (!ck || !pass1) && i0 <= m;
             T* const fb_in = fbnd + (ck ? int64_t(s - 1) * NV * nb : 0);
             int* const fbE_in = fbndE + (ck ? int64_t(s - 1) * nb : 0);
             T* const fb_out = fbnd + (ck ? int64_t(s) * NV * nb : 0);
@@ -326,27 +336,27 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
             // columns t .. t + 32 in the next 32 steps
             const bool waits = MW && pass1 && s > 0;
             if (waits) wait_for((s - 1) * SP + min(S, 2 * G + 1));
+            // the next column's row-above values (lane 0: the previous stripe's bottom row; the
+            // other lanes: the lane above's bottom row) into this lane's units
+            auto take_up = [&](const T iM, const T iX, const T iY, const int iE) {
+                int d = iE - E;
+                if (d > kLift) {   // keep the incoming values in range: move own state down
+                    const T f = pow2i<T>(kLift - d);
+#pragma unroll
+                    for (int r = 0; r < R; ++r) { cM[r] *= f; cX[r] *= f; cY[r] *= f; }
+                    dgM *= f; dgX *= f; dgY *= f; zpart *= f;
+                    E = iE - kLift; lone = pow2i<T>(-E); d = kLift;
+                }
+                const T f = pow2i<T>(d);
+                upM = iM * f;
+                if constexpr (AFF) { upX = iX * f; upY = iY * f; }
+            };
             fetch_up(0);
+            if (lane == 0 && s > 0) { take_up(nuM, nuX, nuY, nuE); fetch_up(1); }
             for (int t = 0; t < S; ++t) {
                 const int j = t - lane;           // column 0..n
                 if (waits && t > 0 && (t & 31) == 0) wait_for((s - 1) * SP + min(S, t + 2 * G + 1));
                 if (MW && pass1 && t > 0 && (t & 7) == 0) publish(s * SP + t);   // steps 0 .. t-1 done
-                if (lane == 0 && j <= n && s > 0) {
-                    const int eb = nuE;
-                    const T ubM = nuM, ubX = nuX, ubY = nuY;
-                    fetch_up(j + 1);
-                    int d = eb - E;
-                    if (d > kLift) {   // keep the incoming values in range: move own state down
-                        const T f = pow2i<T>(kLift - d);
-#pragma unroll
-                        for (int r = 0; r < R; ++r) { cM[r] *= f; cX[r] *= f; cY[r] *= f; }
-                        dgM *= f; dgX *= f; dgY *= f; zpart *= f;
-                        E = eb - kLift; lone = pow2i<T>(-E); d = kLift;
-                    }
-                    const T f = pow2i<T>(d);
-                    upM = ubM * f;
-                    if constexpr (AFF) { upX = ubX * f; upY = ubY * f; }
-                }
                 const bool active = (j >= 0) && (j <= n);
                 if (active) {
                     const int bj = nbj;                   // column 0: the zero column
@@ -432,6 +442,12 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                         fe[int64_t(t) * G + lane] = E;
                     }
                 }
+                if (pass1 && lane == G - 1 && active && s + 1 < nstripes) {
+                    fb_out[NV * j] = cM[R - 1];
+                    if constexpr (AFF) { fb_out[NV * j + 1] = cX[R - 1]; fb_out[NV * j + 2] = cY[R - 1]; }
+                    fbE_out[j] = E;
+                }
+                // the row above of the next step's column: one exponent alignment for every lane
                 if constexpr (G > 1) {
                     const T sM = __shfl_up_sync(gmask, cM[R - 1], 1, G);
                     T sX = sM, sY = sM;
@@ -440,23 +456,13 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                         sY = __shfl_up_sync(gmask, cY[R - 1], 1, G);
                     }
                     const int sE = __shfl_up_sync(gmask, E, 1, G);
-                    if (lane > 0) {
-                        int d = sE - E;
-                        if (d > kLift) {
-                            const T f = pow2i<T>(kLift - d);
-#pragma unroll
-                            for (int r = 0; r < R; ++r) { cM[r] *= f; cX[r] *= f; cY[r] *= f; }
-                            dgM *= f; dgX *= f; dgY *= f; zpart *= f;
-                            E = sE - kLift; lone = pow2i<T>(-E); d = kLift;
-                        }
-                        const T f = pow2i<T>(d);
-                        upM = sM * f; upX = sX * f; upY = sY * f;
+                    const bool top = lane == 0;
+                    if (!top || (s > 0 && j < n)) {
+                        take_up(top ? nuM : sM, top ? nuX : sX, top ? nuY : sY, top ? nuE : sE);
+                        fetch_up(j + 2);
                     }
-                }
-                if (pass1 && lane == G - 1 && active && s + 1 < nstripes) {
-                    fb_out[NV * j] = cM[R - 1];
-                    if constexpr (AFF) { fb_out[NV * j + 1] = cX[R - 1]; fb_out[NV * j + 2] = cY[R - 1]; }
-                    fbE_out[j] = E;
+                } else {
+                    if (s > 0 && j < n) { take_up(nuM, nuX, nuY, nuE); fetch_up(j + 2); }
                 }
             }
             if (MW && pass1) publish(s * SP + S);
@@ -582,7 +588,12 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
             T dnM = T(0), dnX = T(0), dnY = T(0);     // row below, column j
             const T* fs = fwd + (ck ? 0 : int64_t(s) * S * G * CV);
             const int* fe = fexp + (ck ? 0 : int64_t(s) * S * G);
+            // a lane wholly below row m has no table (its backward values are zero): it reads
+            // zeros and scales by zero
+            const bool lane_rows = i0 <= m;
             T nf[CV];
+#pragma unroll
+            for (int k = 0; k < CV; ++k) nf[k] = T(0);
             int nEF = 0, nbj = N;
             bool have_next = false;
             // lane G-1: the row below (the next stripe's top row) one column ahead
@@ -597,35 +608,47 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
             // reads columns n - t .. n - t - 32 in the next 32 steps
             const bool bwaits = MW && s < nstripes - 1;
             if (bwaits) wait_for((bkey - 1) * SP + min(S, 2 * G + 1));
+            // the next column's row-below values (lane G-1: the next stripe's top row; the other
+            // lanes: the lane below's top row) into this lane's units
+            auto take_dn = [&](const T iM, const T iX, const T iY, const int iE) {
+                int d = iE - EB;
+                if (d > kLift) {
+                    const T f = pow2i<T>(kLift - d);
+#pragma unroll
+                    for (int r = 0; r < R; ++r) { bM[r] *= f; bX[r] *= f; bY[r] *= f; }
+                    dgM *= f;
+                    EB = iE - kLift; lone = pow2i<T>(-EB); d = kLift;
+                }
+                const T f = pow2i<T>(d);
+                dnM = iM * f;
+                if constexpr (AFF) { dnX = iX * f; dnY = iY * f; }
+                else { dnX = dnM; dnY = dnM; }
+            };
             fetch_dn(n);
+            if (lane == G - 1 && s < nstripes - 1) { take_dn(ndM, ndX, ndY, ndE); fetch_dn(n - 1); }
             for (int t = 0; t < S; ++t) {
                 const int j = n - t + (G - 1 - lane);     // column n..0
+                if constexpr (kPrefetchSteps > 0) {
+                    // every lane reads table row n + G - 1 - t at step t (its column j plus its
+                    // lane index): the row kPrefetchSteps ahead goes to L2 now
+                    const int u = n + G - 1 - t - kPrefetchSteps;
+                    if (lane == 0 && u >= 0) {
+                        prefetch_l2_bulk(fs + int64_t(u) * G * CV, unsigned(G * CV * sizeof(T)));
+                        if constexpr ((G * sizeof(int)) % 16 == 0) prefetch_l2_bulk(fe + int64_t(u) * G, unsigned(G * sizeof(int)));
+                        else prefetch_l2(fe + int64_t(u) * G);
+                    }
+                }
                 if (bwaits && t > 0 && (t & 31) == 0) wait_for((bkey - 1) * SP + min(S, t + 2 * G + 1));
                 if (MW && t > 0 && (t & 7) == 0) publish(bkey * SP + t);
-                if (lane == G - 1 && j >= 0 && s < nstripes - 1) {
-                    const int eb = ndE;
-                    const T dbM = ndM, dbX = ndX, dbY = ndY;
-                    fetch_dn(j - 1);
-                    int d = eb - EB;
-                    if (d > kLift) {
-                        const T f = pow2i<T>(kLift - d);
-#pragma unroll
-                        for (int r = 0; r < R; ++r) { bM[r] *= f; bX[r] *= f; bY[r] *= f; }
-                        dgM *= f;
-                        EB = eb - kLift; lone = pow2i<T>(-EB); d = kLift;
-                    }
-                    const T f = pow2i<T>(d);
-                    dnM = dbM * f;
-                    if constexpr (AFF) { dnX = dbX * f; dnY = dbY * f; }
-                    else { dnX = dnM; dnY = dnM; }
-                }
                 const bool active = (j >= 0) && (j <= n);
                 if (active) {
                     // this column's forward values were loaded one step ahead (or now, on
                     // the lane's first step); issue the next column's loads before the math
                     if (!have_next) {
-                        vload<T, CV>(nf, fs + (int64_t(j + lane) * G + lane) * CV);
-                        nEF = fe[int64_t(j + lane) * G + lane];
+                        if (lane_rows) {
+                            vload<T, CV>(nf, fs + (int64_t(j + lane) * G + lane) * CV);
+                            nEF = fe[int64_t(j + lane) * G + lane];
+                        }
                         nbj = j < n ? int(bp[j]) : N;
                     }
                     T f[CV];
@@ -635,14 +658,16 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                     const int bj1 = nbj;              // b code of column j+1 (N: none)
                     have_next = j > 0;
                     if (have_next) {
-                        vload<T, CV>(nf, fs + (int64_t(j - 1 + lane) * G + lane) * CV);
-                        nEF = fe[int64_t(j - 1 + lane) * G + lane];
+                        if (lane_rows) {
+                            vload<T, CV>(nf, fs + (int64_t(j - 1 + lane) * G + lane) * CV);
+                            nEF = fe[int64_t(j - 1 + lane) * G + lane];
+                        }
                         nbj = int(bp[j - 1]);
                     }
                     // scale of this step's products: 2^(E_F + E_B - E_Z) / zhat (an exact power of
                     // two times 1 / zhat rounded to T)
-                    const double facd = TR ? pow2i<double>(EF + EB - EZ) * invz : 0.0;
-                    const T fac = TR ? static_cast<T>(facd) : pow2i<T>(EF + EB - EZ) * invzT;
+                    const double facd = (TR && lane_rows) ? pow2i<double>(EF + EB - EZ) * invz : 0.0;
+                    const T fac = TR ? static_cast<T>(facd) : lane_rows ? pow2i<T>(EF + EB - EZ) * invzT : T(0);
                     if (!is_finite(fac)) bad = true;
                     T dM = dgM;                       // row below, column j+1
                     T xM = dnM, xX = dnX, xY = dnY;   // row below, column j
@@ -744,6 +769,12 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                         }
                     }
                 }
+                if (lane == 0 && active && s > 0) {
+                    bb_out[NV * j] = bM[0];
+                    if constexpr (AFF) { bb_out[NV * j + 1] = bX[0]; bb_out[NV * j + 2] = bY[0]; }
+                    bbE_out[j] = EB;
+                }
+                // the row below of the next step's column: one exponent alignment for every lane
                 if constexpr (G > 1) {
                     const T sM = __shfl_down_sync(gmask, bM[0], 1, G);
                     T sX = sM, sY = sM;
@@ -752,23 +783,13 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                         sY = __shfl_down_sync(gmask, bY[0], 1, G);
                     }
                     const int sE = __shfl_down_sync(gmask, EB, 1, G);
-                    if (lane < G - 1) {
-                        int d = sE - EB;
-                        if (d > kLift) {
-                            const T fsc = pow2i<T>(kLift - d);
-#pragma unroll
-                            for (int r = 0; r < R; ++r) { bM[r] *= fsc; bX[r] *= fsc; bY[r] *= fsc; }
-                            dgM *= fsc;
-                            EB = sE - kLift; lone = pow2i<T>(-EB); d = kLift;
-                        }
-                        const T fsc = pow2i<T>(d);
-                        dnM = sM * fsc; dnX = sX * fsc; dnY = sY * fsc;
+                    const bool bot = lane == G - 1;
+                    if (!bot || (s < nstripes - 1 && j > 0)) {
+                        take_dn(bot ? ndM : sM, bot ? ndX : sX, bot ? ndY : sY, bot ? ndE : sE);
+                        fetch_dn(j - 2);
                     }
-                }
-                if (lane == 0 && active && s > 0) {
-                    bb_out[NV * j] = bM[0];
-                    if constexpr (AFF) { bb_out[NV * j + 1] = bX[0]; bb_out[NV * j + 2] = bY[0]; }
-                    bbE_out[j] = EB;
+                } else {
+                    if (s < nstripes - 1 && j > 0) { take_dn(ndM, ndX, ndY, ndE); fetch_dn(j - 2); }
                 }
             }
             if constexpr (MW) publish(bkey * SP + S);
