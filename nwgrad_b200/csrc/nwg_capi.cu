@@ -610,7 +610,7 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
         if (!fn) throw Error(NWG_EINVAL, "no kernel for this geometry");
         const int hblock = B.geo.mw > 1 ? 32 * B.geo.mw : 128;
         const size_t smem = smem_base + (B.geo.mw > 1 ? nwg::hard_mw_smem_bytes(B.geo.mw, int(sizeof(T))) : 0);
-        if (smem > 48 * 1024) NWG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        NWG_CUDA(nwg::allow_smem(reinterpret_cast<const void*>(fn), smem));
         nwg::HardArgs A{};
         A.a = s->a.as<uint8_t>(); A.oa = s->doa.as<int64_t>();
         A.b = s->b.as<uint8_t>(); A.ob = s->dob.as<int64_t>();
@@ -827,10 +827,10 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
             return nwg::soft_smem_bytes(K, N, G, B.geo.R, blk, int(sizeof(T)), tr, mw);
         };
         while (!mw && block > 32 && smem_for(block) > 96 * 1024) block /= 2;
-        while (mw && block > 128 && smem_for(block) > 200 * 1024) block /= 2;   // fewer warps per pair
+        while (mw && block > 128 && smem_for(block) > 227 * 1024) block /= 2;   // fewer warps per pair
         const size_t smem = smem_for(block);
         if (smem > 227 * 1024) throw Error(NWG_EINVAL, "soft: the alphabet / parameter sets do not fit shared memory");
-        if (smem > 48 * 1024) NWG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        NWG_CUDA(nwg::allow_smem(reinterpret_cast<const void*>(fn), smem));
         int occ = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, block, smem);
         occ = std::max(occ, 1);
@@ -847,7 +847,8 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
         const int64_t exp_bytes = ((tab_cells / B.geo.R) * 4 + 255) & ~int64_t(255);
         const int64_t nbrows = ck ? max_stripes : 1;
         const int64_t nbrows_b = mw ? max_stripes : 1;
-        const int64_t bnd_bytes = nb1 * (nbrows + nbrows_b) * (NV * int64_t(sizeof(T)) + 4);
+        // boundary rows: per column M (X, Y) and the exponent, as a 2- or 4-vector of T
+        const int64_t bnd_bytes = nb1 * (nbrows + nbrows_b) * (aff ? 4 : 2) * int64_t(sizeof(T));
         const int64_t warp_bytes = fwd_bytes + exp_bytes;
         // a slot: one group's table and boundary rows, or (several warps per pair) one block's
         const int64_t stride = (((mw ? gpb : 1) * warp_bytes + bnd_bytes) + 255) & ~int64_t(255);

@@ -1,9 +1,29 @@
 // Shared device helpers for the nwgrad_b200 kernels (sm_100a).
 #pragma once
-#include <cstdint>
 #include <cuda_runtime.h>
 
+#include <cstdint>
+#include <map>
+#include <mutex>
+
 namespace nwg {
+
+// Let `fn` launch with `bytes` of dynamic shared memory.  The attribute only ever grows, under
+// a lock: a launch prepared (or captured) with a larger size by another bucket or thread stays
+// valid.
+inline cudaError_t allow_smem(const void* fn, size_t bytes) {
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, size_t> set;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(mu);
+    size_t& cur = set[{dev, fn}];
+    if (bytes <= cur) return cudaSuccess;
+    const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+    if (e == cudaSuccess) cur = bytes;
+    return e;
+}
 
 // The reference's max: std::max keeps the first argument on ties and on a NaN second
 // argument: (a < b) ? b : a.  Kept as a compare + select (not fmaxf) so signed zeros and

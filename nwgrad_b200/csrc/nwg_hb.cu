@@ -484,7 +484,7 @@ int64_t hb_run_t(const HbRun& P, cudaStream_t st, int sms) {
         T* wr = static_cast<T*>(dwrap.get(size_t(wrap_off) * sizeof(T)));
         const size_t smem = mat_bytes + NW * ring_bytes_per_warp;
         auto fn = P.pmax ? hb_sweep_kernel<T, true, R> : hb_sweep_kernel<T, false, R>;
-        if (smem > 48 * 1024) HB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        HB_CUDA(allow_smem(reinterpret_cast<const void*>(fn), smem));
         int occ = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 32 * NW, smem);
         const int grid = int(std::min<int64_t>(int64_t(jobs.size()), int64_t(sms) * std::max(occ, 1)));

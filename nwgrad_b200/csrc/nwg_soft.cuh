@@ -94,6 +94,8 @@ __device__ __forceinline__ void vstore(T* dst, const T (&v)[NV]) {
 #pragma unroll
         for (int k = 0; k < NV / 2; ++k)
             reinterpret_cast<double2*>(dst)[k] = make_double2(v[2 * k], v[2 * k + 1]);
+    } else if constexpr (sizeof(T) == 4 && NV == 2) {
+        *reinterpret_cast<float2*>(dst) = make_float2(v[0], v[1]);
     } else {
 #pragma unroll
         for (int k = 0; k < NV; ++k) dst[k] = v[k];
@@ -113,11 +115,20 @@ __device__ __forceinline__ void vload(T (&v)[NV], const T* src) {
             const double2 q = reinterpret_cast<const double2*>(src)[k];
             v[2 * k] = q.x; v[2 * k + 1] = q.y;
         }
+    } else if constexpr (sizeof(T) == 4 && NV == 2) {
+        const float2 q = *reinterpret_cast<const float2*>(src);
+        v[0] = q.x; v[1] = q.y;
     } else {
 #pragma unroll
         for (int k = 0; k < NV; ++k) v[k] = src[k];
     }
 }
+
+// A boundary-row column: M (X, Y) and the lane exponent, the exponent carried as T's bits.
+__device__ __forceinline__ float exp_bits(int e, float) { return __int_as_float(e); }
+__device__ __forceinline__ double exp_bits(int e, double) { return __longlong_as_double(static_cast<long long>(e)); }
+__device__ __forceinline__ int bits_exp(float v) { return __float_as_int(v); }
+__device__ __forceinline__ int bits_exp(double v) { return static_cast<int>(__double_as_longlong(v)); }
 
 // Bytes of dynamic shared memory the soft kernel needs for a block of `block` threads.
 __host__ __device__ inline size_t soft_smem_bytes(int K, int N, int G, int R, int block, int tsize, bool tracked,
@@ -128,6 +139,7 @@ __host__ __device__ inline size_t soft_smem_bytes(int K, int N, int G, int R, in
     b += size_t(N + 1) * G * R * tsize * gpb;              // per-lane substitution counts
     if (G > 1) b += size_t(K) * N * N * tsize * gpb;        // per-group histogram
     b = (b + 15) & ~size_t(15);
+    b += size_t(block) * 2 * 4 * tsize;                    // per-group boundary staging (write, read)
     if (tracked) b += size_t(4) * K * 8 * block;            // per-lane tracked gap sums
     if (multiwarp) b += size_t(gpb) * 8 * 8 + size_t(gpb) * 4 + 16;   // per-warp partials, progress
     return b;
@@ -159,6 +171,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
     constexpr int GR = G * R;
     constexpr int NV = AFF ? 3 : 1;          // values per cell
     constexpr int CV = NV * R;               // values per lane column
+    constexpr int BW = AFF ? 4 : 2;          // boundary-row values per column: M (X, Y), exponent
     const int N = A.N, K = A.K;
     const int wcols = N + 1;
     const int nw = (K * N + 1) * wcols;
@@ -170,8 +183,9 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
     after = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(after) + 15) & ~uintptr_t(15));
     T* macc_all = reinterpret_cast<T*>(after);
     T* hist_all = macc_all + size_t(N + 1) * GR * gpb;
-    double* tg_all = reinterpret_cast<double*>(
+    T* stage_all = reinterpret_cast<T*>(
         (reinterpret_cast<uintptr_t>(hist_all + (G > 1 ? size_t(K) * N * N * gpb : 0)) + 15) & ~uintptr_t(15));
+    double* tg_all = reinterpret_cast<double*>(stage_all + size_t(blockDim.x) * 2 * 4);
     double* cpart = tg_all + (TR ? size_t(4) * K * blockDim.x : 0);        // MW: [warp][8] partials
     volatile int* prog = reinterpret_cast<volatile int*>(cpart + (MW ? 8 * gpb : 0));   // MW: per warp
     for (int k = threadIdx.x; k < nw; k += blockDim.x) sw[k] = static_cast<const T*>(A.w)[k];
@@ -183,6 +197,11 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
     const int NWp = MW ? gpb : 1;                            // warps per pair
     T* macc = macc_all + size_t(N + 1) * GR * gib;          // [b][lane][r]
     T* hist = hist_all + size_t(K) * N * N * gib;
+    // boundary rows pass through shared memory G columns at a time: the producing lane stages
+    // its column every step and the group writes the G columns as one coalesced row segment;
+    // the consuming lane reads a staged segment the group loaded one segment ahead
+    T* stw = stage_all + size_t(gib) * G * 2 * 4;            // [G][BW] produced columns
+    T* str = stw + G * 4;                                    // [G][BW] columns to consume
     double* tg = tg_all + size_t(4) * K * threadIdx.x;        // tracked gap sums of this lane
     for (int k = lane; k < (N + 1) * GR; k += G) macc[k] = T(0);
     if constexpr (G > 1) for (int k = lane; k < K * N * N; k += G) hist[k] = T(0);
@@ -202,10 +221,8 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
     const int nbrows = ck ? A.max_stripes : 1;              // forward boundary rows kept
     const int nbrows_b = MW ? A.max_stripes : 1;            // backward boundary rows kept
     unsigned char* bb = sbase + A.bnd_off;
-    T* fbnd = reinterpret_cast<T*>(bb);                      // [nbrows][NV * nb]
-    T* bbnd = fbnd + NV * nb * nbrows;                       // [nbrows_b][NV * nb]
-    int* fbndE = reinterpret_cast<int*>(bbnd + NV * nb * nbrows_b);   // [nbrows][nb]
-    int* bbndE = fbndE + nb * nbrows;                        // [nbrows_b][nb]
+    T* fbnd = reinterpret_cast<T*>(bb);                      // [nbrows][nb][BW]
+    T* bbnd = fbnd + BW * nb * nbrows;                       // [nbrows_b][nb][BW]
     const int pw = (gib + NWp - 1) % NWp;                    // MW: the warp of the neighbouring stripe
     // MW: wait until the neighbouring stripe's warp has published `target` (bounded)
     bool stalled = false;
@@ -287,10 +304,8 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
             // a lane wholly below row m (the last stripe's padding) keeps no table: its backward
             // values are zero, so its forward values are never needed
             const bool store_table = (!ck || !pass1) && i0 <= m;
-            T* const fb_in = fbnd + (ck ? int64_t(s - 1) * NV * nb : 0);
-            int* const fbE_in = fbndE + (ck ? int64_t(s - 1) * nb : 0);
-            T* const fb_out = fbnd + (ck ? int64_t(s) * NV * nb : 0);
-            int* const fbE_out = fbndE + (ck ? int64_t(s) * nb : 0);
+            T* const fb_in = fbnd + (ck ? int64_t(s - 1) * BW * nb : 0);
+            T* const fb_out = fbnd + (ck ? int64_t(s) * BW * nb : 0);
             int key[R];
             T roa[TR ? R : 1], rea[TR ? R : 1], rob[TR ? R : 1], reb[TR ? R : 1];
             T vmask[R];
@@ -323,19 +338,24 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
             T* fs = fwd + (ck ? 0 : int64_t(s) * S * G * CV);
             int* fe = fexp + (ck ? 0 : int64_t(s) * S * G);
             int nbj = N;
-            // lane 0: the row above (the previous stripe's bottom row) one column ahead, so
-            // the load is in flight while the current column is computed
-            T nuM = T(0), nuX = T(0), nuY = T(0); int nuE = 0;
-            auto fetch_up = [&](int jj) {
-                if (lane == 0 && s > 0 && jj <= n) {
-                    nuE = fbE_in[jj]; nuM = fb_in[NV * jj];
-                    if constexpr (AFF) { nuX = fb_in[NV * jj + 1]; nuY = fb_in[NV * jj + 2]; }
-                }
+            // the row above (the previous stripe's bottom row): one lane per pair reads it one
+            // column ahead; a group loads it G columns at a time, one segment ahead (rb), into
+            // the staging row lane 0 reads
+            T rb[BW];
+#pragma unroll
+            for (int k = 0; k < BW; ++k) rb[k] = T(0);
+            auto load_seg = [&](int c0) {   // group: columns c0 .. c0 + G - 1 into rb
+                if (c0 + lane <= n) vload<T, BW>(rb, fb_in + int64_t(c0 + lane) * BW);
             };
-            // MW: the stripe above has written column c by its step c + G - 1; lane 0 reads
-            // columns t .. t + 32 in the next 32 steps
+            auto stage_seg = [&]() {        // group: rb into the staging row
+                __syncwarp(gmask);
+                vstore<T, BW>(str + lane * 4, rb);
+                __syncwarp(gmask);
+            };
+            // MW: the stripe above has written column c by its step c + 2G - 2 (a segment is
+            // written once complete); the group reads columns up to t + 2G within step t
             const bool waits = MW && pass1 && s > 0;
-            if (waits) wait_for((s - 1) * SP + min(S, 2 * G + 1));
+            if (waits) wait_for((s - 1) * SP + min(S, 4 * G + 1));
             // the next column's row-above values (lane 0: the previous stripe's bottom row; the
             // other lanes: the lane above's bottom row) into this lane's units
             auto take_up = [&](const T iM, const T iX, const T iY, const int iE) {
@@ -351,11 +371,25 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                 upM = iM * f;
                 if constexpr (AFF) { upX = iX * f; upY = iY * f; }
             };
-            fetch_up(0);
-            if (lane == 0 && s > 0) { take_up(nuM, nuX, nuY, nuE); fetch_up(1); }
+            if (s > 0) {
+                if constexpr (G == 1) {
+                    load_seg(0);
+                    take_up(rb[0], AFF ? rb[1] : T(0), AFF ? rb[2] : T(0), bits_exp(rb[BW - 1]));
+                    load_seg(1);
+                } else {
+                    load_seg(0);
+                    stage_seg();
+                    load_seg(G);
+                    if (lane == 0) {
+                        T v[BW];
+                        vload<T, BW>(v, str);
+                        take_up(v[0], AFF ? v[1] : T(0), AFF ? v[2] : T(0), bits_exp(v[BW - 1]));
+                    }
+                }
+            }
             for (int t = 0; t < S; ++t) {
                 const int j = t - lane;           // column 0..n
-                if (waits && t > 0 && (t & 31) == 0) wait_for((s - 1) * SP + min(S, t + 2 * G + 1));
+                if (waits && t > 0 && (t & 31) == 0) wait_for((s - 1) * SP + min(S, t + 4 * G + 1));
                 if (MW && pass1 && t > 0 && (t & 7) == 0) publish(s * SP + t);   // steps 0 .. t-1 done
                 const bool active = (j >= 0) && (j <= n);
                 if (active) {
@@ -442,10 +476,28 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                         fe[int64_t(t) * G + lane] = E;
                     }
                 }
-                if (pass1 && lane == G - 1 && active && s + 1 < nstripes) {
-                    fb_out[NV * j] = cM[R - 1];
-                    if constexpr (AFF) { fb_out[NV * j + 1] = cX[R - 1]; fb_out[NV * j + 2] = cY[R - 1]; }
-                    fbE_out[j] = E;
+                // this stripe's bottom row (lane G-1's column t - G + 1) for the stripe below
+                if (pass1 && s + 1 < nstripes) {
+                    const int c = t - (G - 1);
+                    T v[BW];
+                    v[0] = cM[R - 1];
+                    if constexpr (AFF) { v[1] = cX[R - 1]; v[2] = cY[R - 1]; }
+                    v[BW - 1] = exp_bits(E, T(0));
+                    if constexpr (G == 1) {
+                        if (c >= 0) vstore<T, BW>(fb_out + int64_t(c) * BW, v);
+                    } else {
+                        if (lane == G - 1 && c >= 0) vstore<T, BW>(stw + (c & (G - 1)) * 4, v);
+                        if (c >= 0 && ((c & (G - 1)) == G - 1 || c == n)) {   // a full segment (or the last)
+                            __syncwarp(gmask);
+                            const int cc = c - (c & (G - 1)) + lane;
+                            if (cc <= c) {
+                                T w[BW];
+                                vload<T, BW>(w, stw + lane * 4);
+                                vstore<T, BW>(fb_out + int64_t(cc) * BW, w);
+                            }
+                            __syncwarp(gmask);
+                        }
+                    }
                 }
                 // the row above of the next step's column: one exponent alignment for every lane
                 if constexpr (G > 1) {
@@ -456,13 +508,22 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                         sY = __shfl_up_sync(gmask, cY[R - 1], 1, G);
                     }
                     const int sE = __shfl_up_sync(gmask, E, 1, G);
-                    const bool top = lane == 0;
-                    if (!top || (s > 0 && j < n)) {
-                        take_up(top ? nuM : sM, top ? nuX : sX, top ? nuY : sY, top ? nuE : sE);
-                        fetch_up(j + 2);
+                    const int cn = t + 1;                 // lane 0's next column
+                    if (s > 0 && cn <= n && (cn & (G - 1)) == 0) {   // a new segment: stage it, load the next
+                        stage_seg();
+                        load_seg(cn + G);
                     }
+                    const bool top = lane == 0;
+                    T v[BW];
+                    vload<T, BW>(v, str + (cn & (G - 1)) * 4);
+                    if (!top || (s > 0 && cn <= n))
+                        take_up(top ? v[0] : sM, top ? (AFF ? v[1] : T(0)) : sX, top ? (AFF ? v[2] : T(0)) : sY,
+                                top ? bits_exp(v[BW - 1]) : sE);
                 } else {
-                    if (s > 0 && j < n) { take_up(nuM, nuX, nuY, nuE); fetch_up(j + 2); }
+                    if (s > 0 && j < n) {
+                        take_up(rb[0], AFF ? rb[1] : T(0), AFF ? rb[2] : T(0), bits_exp(rb[BW - 1]));
+                        load_seg(j + 2);
+                    }
                 }
             }
             if (MW && pass1) publish(s * SP + S);
@@ -548,10 +609,8 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
         for (int s = nstripes - 1 - (MW ? gib : 0); s >= 0; s -= NWp) {
             if (ck) fwd_stripe(s, false);       // this stripe's forward table, from its checkpoint
             // this stripe's row below (read) and its own top row (written): MW keeps one per stripe
-            T* const bb_in = bbnd + (MW ? int64_t(s + 1) * NV * nb : 0);
-            int* const bbE_in = bbndE + (MW ? int64_t(s + 1) * nb : 0);
-            T* const bb_out = bbnd + (MW ? int64_t(s) * NV * nb : 0);
-            int* const bbE_out = bbndE + (MW ? int64_t(s) * nb : 0);
+            T* const bb_in = bbnd + (MW ? int64_t(s + 1) * BW * nb : 0);
+            T* const bb_out = bbnd + (MW ? int64_t(s) * BW * nb : 0);
             const int bkey = nstripes - 1 - s;   // MW: progress keys grow as the pass goes up
             const int i0 = s * GR + lane * R;
             int keyd[R], krow[R];
@@ -596,18 +655,24 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
             for (int k = 0; k < CV; ++k) nf[k] = T(0);
             int nEF = 0, nbj = N;
             bool have_next = false;
-            // lane G-1: the row below (the next stripe's top row) one column ahead
-            T ndM = T(0), ndX = T(0), ndY = T(0); int ndE = 0;
-            auto fetch_dn = [&](int jj) {
-                if (lane == G - 1 && s < nstripes - 1 && jj >= 0) {
-                    ndE = bbE_in[jj]; ndM = bb_in[NV * jj];
-                    if constexpr (AFF) { ndX = bb_in[NV * jj + 1]; ndY = bb_in[NV * jj + 2]; }
-                }
+            // the row below (the next stripe's top row), by distance d = n - column from the
+            // right end: as in the forward pass, one lane per pair reads it one column ahead, a
+            // group G columns at a time, one segment ahead (rb), through the staging row
+            T rb[BW];
+#pragma unroll
+            for (int k = 0; k < BW; ++k) rb[k] = T(0);
+            auto load_seg = [&](int d0) {   // group: distances d0 .. d0 + G - 1 into rb
+                if (d0 + lane <= n) vload<T, BW>(rb, bb_in + int64_t(n - d0 - lane) * BW);
             };
-            // MW: the stripe below has written column c by its step n - c + G - 1; lane G-1
-            // reads columns n - t .. n - t - 32 in the next 32 steps
+            auto stage_seg = [&]() {
+                __syncwarp(gmask);
+                vstore<T, BW>(str + lane * 4, rb);
+                __syncwarp(gmask);
+            };
+            // MW: the stripe below has written distance d by its step d + 2G - 2 (a segment is
+            // written once complete); the group reads distances up to t + 2G within step t
             const bool bwaits = MW && s < nstripes - 1;
-            if (bwaits) wait_for((bkey - 1) * SP + min(S, 2 * G + 1));
+            if (bwaits) wait_for((bkey - 1) * SP + min(S, 4 * G + 1));
             // the next column's row-below values (lane G-1: the next stripe's top row; the other
             // lanes: the lane below's top row) into this lane's units
             auto take_dn = [&](const T iM, const T iX, const T iY, const int iE) {
@@ -624,8 +689,22 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                 if constexpr (AFF) { dnX = iX * f; dnY = iY * f; }
                 else { dnX = dnM; dnY = dnM; }
             };
-            fetch_dn(n);
-            if (lane == G - 1 && s < nstripes - 1) { take_dn(ndM, ndX, ndY, ndE); fetch_dn(n - 1); }
+            if (s < nstripes - 1) {
+                if constexpr (G == 1) {
+                    load_seg(0);
+                    take_dn(rb[0], AFF ? rb[1] : T(0), AFF ? rb[2] : T(0), bits_exp(rb[BW - 1]));
+                    load_seg(1);
+                } else {
+                    load_seg(0);
+                    stage_seg();
+                    load_seg(G);
+                    if (lane == G - 1) {
+                        T v[BW];
+                        vload<T, BW>(v, str);
+                        take_dn(v[0], AFF ? v[1] : T(0), AFF ? v[2] : T(0), bits_exp(v[BW - 1]));
+                    }
+                }
+            }
             for (int t = 0; t < S; ++t) {
                 const int j = n - t + (G - 1 - lane);     // column n..0
                 if constexpr (kPrefetchSteps > 0) {
@@ -638,7 +717,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                         else prefetch_l2(fe + int64_t(u) * G);
                     }
                 }
-                if (bwaits && t > 0 && (t & 31) == 0) wait_for((bkey - 1) * SP + min(S, t + 2 * G + 1));
+                if (bwaits && t > 0 && (t & 31) == 0) wait_for((bkey - 1) * SP + min(S, t + 4 * G + 1));
                 if (MW && t > 0 && (t & 7) == 0) publish(bkey * SP + t);
                 const bool active = (j >= 0) && (j <= n);
                 if (active) {
@@ -769,10 +848,28 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                         }
                     }
                 }
-                if (lane == 0 && active && s > 0) {
-                    bb_out[NV * j] = bM[0];
-                    if constexpr (AFF) { bb_out[NV * j + 1] = bX[0]; bb_out[NV * j + 2] = bY[0]; }
-                    bbE_out[j] = EB;
+                // this stripe's top row (lane 0's distance t - G + 1) for the stripe above
+                if (s > 0) {
+                    const int d = t - (G - 1);
+                    T v[BW];
+                    v[0] = bM[0];
+                    if constexpr (AFF) { v[1] = bX[0]; v[2] = bY[0]; }
+                    v[BW - 1] = exp_bits(EB, T(0));
+                    if constexpr (G == 1) {
+                        if (d >= 0) vstore<T, BW>(bb_out + int64_t(n - d) * BW, v);
+                    } else {
+                        if (lane == 0 && d >= 0) vstore<T, BW>(stw + (d & (G - 1)) * 4, v);
+                        if (d >= 0 && ((d & (G - 1)) == G - 1 || d == n)) {   // a full segment (or the last)
+                            __syncwarp(gmask);
+                            const int dd = d - (d & (G - 1)) + lane;
+                            if (dd <= d) {
+                                T w[BW];
+                                vload<T, BW>(w, stw + lane * 4);
+                                vstore<T, BW>(bb_out + int64_t(n - dd) * BW, w);
+                            }
+                            __syncwarp(gmask);
+                        }
+                    }
                 }
                 // the row below of the next step's column: one exponent alignment for every lane
                 if constexpr (G > 1) {
@@ -783,13 +880,22 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                         sY = __shfl_down_sync(gmask, bY[0], 1, G);
                     }
                     const int sE = __shfl_down_sync(gmask, EB, 1, G);
-                    const bool bot = lane == G - 1;
-                    if (!bot || (s < nstripes - 1 && j > 0)) {
-                        take_dn(bot ? ndM : sM, bot ? ndX : sX, bot ? ndY : sY, bot ? ndE : sE);
-                        fetch_dn(j - 2);
+                    const int dn = t + 1;                 // lane G-1's next distance
+                    if (s < nstripes - 1 && dn <= n && (dn & (G - 1)) == 0) {   // a new segment
+                        stage_seg();
+                        load_seg(dn + G);
                     }
+                    const bool bot = lane == G - 1;
+                    T v[BW];
+                    vload<T, BW>(v, str + (dn & (G - 1)) * 4);
+                    if (!bot || (s < nstripes - 1 && dn <= n))
+                        take_dn(bot ? v[0] : sM, bot ? (AFF ? v[1] : T(0)) : sX, bot ? (AFF ? v[2] : T(0)) : sY,
+                                bot ? bits_exp(v[BW - 1]) : sE);
                 } else {
-                    if (s < nstripes - 1 && j > 0) { take_dn(ndM, ndX, ndY, ndE); fetch_dn(j - 2); }
+                    if (s < nstripes - 1 && j > 0) {
+                        take_dn(rb[0], AFF ? rb[1] : T(0), AFF ? rb[2] : T(0), bits_exp(rb[BW - 1]));
+                        load_seg(n - j + 2);
+                    }
                 }
             }
             if constexpr (MW) publish(bkey * SP + S);
