@@ -725,6 +725,7 @@ void soft_weights(const nwg_store* s, const nwg_job& J, std::vector<T>& w, std::
     };
     for (int r = 0; r < K * N; ++r)
         for (int c = 0; c < N; ++c) w[size_t(r) * wc + c] = cvt(std::exp(s->mats[size_t(r) * N + c] * invT));
+    w[size_t(K * N) * wc + N] = T(1);   // the padding corner: carries the Global seed at (m, n)
     gw.assign(size_t(4) * K, T(0));
     for (int k = 0; k < K; ++k) {
         const double goa = s->gaps[4 * k], gea = s->gaps[4 * k + 1], gob = s->gaps[4 * k + 2], geb = s->gaps[4 * k + 3];

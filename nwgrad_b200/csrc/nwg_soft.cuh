@@ -41,7 +41,8 @@ struct SoftArgs {
     const uint8_t* b; const int64_t* ob;
     const uint16_t* tracks; const uint16_t* gtracks;
     const int32_t* order; int64_t n_items;
-    const void* w;       // weights, (K*N + 1) rows x (N + 1) columns in T; row K*N and column N are 0
+    const void* w;       // weights, (K*N + 1) rows x (N + 1) columns in T; row K*N and column N
+                         // are 0 but for w[K*N][N] = 1, which carries the Global corner seed
     const void* gw;      // per set: o_a, e_a, o_b, e_b in T
     int N, K;
     void* scratch; int64_t scratch_stride;   // bytes per group slot
@@ -99,6 +100,41 @@ __device__ __forceinline__ void vstore(T* dst, const T (&v)[NV]) {
     } else {
 #pragma unroll
         for (int k = 0; k < NV; ++k) dst[k] = v[k];
+    }
+}
+// The forward table: written once and read once much later -- stores stream past the caches
+// (evict first), loads take the read-only path.
+template <class T, int NV>
+__device__ __forceinline__ void vstore_stream(T* dst, const T (&v)[NV]) {
+    if constexpr (sizeof(T) == 4 && NV % 4 == 0) {
+#pragma unroll
+        for (int k = 0; k < NV / 4; ++k)
+            __stcs(reinterpret_cast<float4*>(dst) + k, make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]));
+    } else if constexpr (sizeof(T) == 8 && NV % 2 == 0) {
+#pragma unroll
+        for (int k = 0; k < NV / 2; ++k) __stcs(reinterpret_cast<double2*>(dst) + k, make_double2(v[2 * k], v[2 * k + 1]));
+    } else {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) __stcs(dst + k, v[k]);
+    }
+}
+template <class T, int NV>
+__device__ __forceinline__ void vload_ro(T (&v)[NV], const T* src) {
+    if constexpr (sizeof(T) == 4 && NV % 4 == 0) {
+#pragma unroll
+        for (int k = 0; k < NV / 4; ++k) {
+            const float4 q = __ldg(reinterpret_cast<const float4*>(src) + k);
+            v[4 * k] = q.x; v[4 * k + 1] = q.y; v[4 * k + 2] = q.z; v[4 * k + 3] = q.w;
+        }
+    } else if constexpr (sizeof(T) == 8 && NV % 2 == 0) {
+#pragma unroll
+        for (int k = 0; k < NV / 2; ++k) {
+            const double2 q = __ldg(reinterpret_cast<const double2*>(src) + k);
+            v[2 * k] = q.x; v[2 * k + 1] = q.y;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) v[k] = __ldg(src + k);
     }
 }
 template <class T, int NV>
@@ -472,8 +508,8 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                             v[NV * r] = cM[r];
                             if constexpr (AFF) { v[NV * r + 1] = cX[r]; v[NV * r + 2] = cY[r]; }
                         }
-                        vstore<T, CV>(fs + (int64_t(t) * G + lane) * CV, v);
-                        fe[int64_t(t) * G + lane] = E;
+                        vstore_stream<T, CV>(fs + (int64_t(t) * G + lane) * CV, v);
+                        __stcs(fe + int64_t(t) * G + lane, E);
                     }
                 }
                 // this stripe's bottom row (lane G-1's column t - G + 1) for the stripe below
@@ -644,6 +680,17 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
             T lone = T(1);
             T sgb_o = T(0), sga_o = T(0), sgb_x = T(0), sga_x = T(0);   // untracked: this stripe's gap sums
             T dgM = T(0);                             // row below, column j+1 (BM only)
+            // Global affine: the seed B = 1 at (m, n) enters every state through the diagonal
+            // term, as B_M(m+1, n+1) = 1 with the padding weight w[K*N][N] = 1 (the cell and
+            // everything else it reaches in the padding are zero), so no cell tests for it
+            if constexpr (AFF && !LOC) {
+                if (s == nstripes - 1) {
+                    const int rc = m - i0;
+#pragma unroll
+                    for (int r = 1; r < R; ++r) bM[r] = (r == rc + 1) ? T(1) : bM[r];
+                    if (rc == R - 1) dgM = T(1);
+                }
+            }
             T dnM = T(0), dnX = T(0), dnY = T(0);     // row below, column j
             const T* fs = fwd + (ck ? 0 : int64_t(s) * S * G * CV);
             const int* fe = fexp + (ck ? 0 : int64_t(s) * S * G);
@@ -725,8 +772,8 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                     // the lane's first step); issue the next column's loads before the math
                     if (!have_next) {
                         if (lane_rows) {
-                            vload<T, CV>(nf, fs + (int64_t(j + lane) * G + lane) * CV);
-                            nEF = fe[int64_t(j + lane) * G + lane];
+                            vload_ro<T, CV>(nf, fs + (int64_t(j + lane) * G + lane) * CV);
+                            nEF = __ldg(fe + int64_t(j + lane) * G + lane);
                         }
                         nbj = j < n ? int(bp[j]) : N;
                     }
@@ -738,8 +785,8 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                     have_next = j > 0;
                     if (have_next) {
                         if (lane_rows) {
-                            vload<T, CV>(nf, fs + (int64_t(j - 1 + lane) * G + lane) * CV);
-                            nEF = fe[int64_t(j - 1 + lane) * G + lane];
+                            vload_ro<T, CV>(nf, fs + (int64_t(j - 1 + lane) * G + lane) * CV);
+                            nEF = __ldg(fe + int64_t(j - 1 + lane) * G + lane);
                         }
                         nbj = int(bp[j - 1]);
                     }
@@ -773,7 +820,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                                 nM = fmaf_t(vmask[r], lone, nM);
                                 nX = fmaf_t(vmask[r], lone, nX);
                                 nY = fmaf_t(vmask[r], lone, nY);
-                            } else if (i == m && j == n) { nM = lone; nX = lone; nY = lone; }
+                            }
                             const T fmy = fm + fy, fmx = fm + fx;
                             mc[r] = (fmy + fx) * D;
                             if constexpr (TR) {
