@@ -237,6 +237,11 @@ def cpu_reference(mat, a, oa, bp, obp, bn, obn, sample_pairs, steps, warmup):
             "value": cells / float(np.min(per_step)) / 1e9}
 
 
+def _tune_mod():
+    from nwgrad_b200 import tune
+    return tune
+
+
 def cpu_model():
     try:
         for ln in open("/proc/cpuinfo"):
@@ -572,7 +577,7 @@ def main():
             "data": "synthetic (seeded)", "config": config, "e2e": e2e, "roofline": roofline,
             "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
             "plain_fill": plain, "serve": serve,
-            "autotune": {str(k): f"{v[0]} lanes x {v[1]} rows" for k, v in tune_table.items()},
+            "autotune": {str(k): _tune_mod().describe(v) for k, v in tune_table.items()},
             "step_ms": step_ms}))
     if dist is not None:
         dist.destroy_process_group()
@@ -696,7 +701,7 @@ def bench_c3(args):
         tp = _timed_run(lambda: (bt.score_and_grad(), bt.compute_grad()), reps=3)
         out["modes"][mode] = {"gcups": cells / t / 1e9, "seconds": t, "device_ms": ms, "launches": launches,
                               "plain_fill_gcups": cells / tp / 1e9,
-                              "autotune": {str(k): f"{v[0]}x{v[1]}" for k, v in table.items()}}
+                              "autotune": {str(k): _tune_mod().describe(v) for k, v in table.items()}}
         del bt
     print(json.dumps(out))
 

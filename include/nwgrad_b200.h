@@ -83,6 +83,14 @@ int nwg_run(nwg_store* s, const nwg_job* job, void* stream, double* total);
  * kernel / fill choice is a CPU ISA dispatch). */
 int nwg_set_geometry(nwg_store* s, int soft, int size_class, int lanes, int rows);
 
+/* Kernel geometry by cost model: each pair of the size class runs with the geometry (lanes[k],
+ * rows[k]) that minimises ns_per_cell[k] x the pair's padded cells (whole stripes of
+ * lanes x rows DP rows, columns plus the lanes' skew) -- the autotuner's measured cost per
+ * padded cell, so pairs whose rows fill stripes badly under one geometry take another.
+ * Replaces a single geometry set for the class.  No counterpart in the reference. */
+int nwg_set_geometry_costs(nwg_store* s, int soft, int size_class, int n, const int* lanes, const int* rows,
+                           const double* ns_per_cell);
+
 /* Device memory of soft runs: scratch_budget_bytes caps the forward tables one call holds
  * (fewer pairs run at once when they are large); a pair whose whole forward table would be
  * above checkpoint_bytes keeps only its stripe boundaries and recomputes each stripe just

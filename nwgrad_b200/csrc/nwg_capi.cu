@@ -322,6 +322,10 @@ struct nwg_store {
     Plan hard_plan, soft_plan, band_plan, soft_band_plan;
     // geometry per (soft, size class) chosen by the autotuner; plain: one fixed geometry
     std::map<std::pair<int, int>, std::pair<int, int>> geo_table;
+    // per (soft, size class): measured cost per padded cell of each geometry; a pair of the
+    // class runs with the geometry whose cost x the pair's padded cells is least
+    struct GeoCost { int G, R; double ns_per_cell; };
+    std::map<std::pair<int, int>, std::vector<GeoCost>> geo_costs;
     bool plain = false;
     int64_t scratch_budget = int64_t(24) << 30;   // bytes of soft scratch one call may hold
     int64_t ck_threshold = int64_t(16) << 20;     // soft: forward tables above this are checkpointed
@@ -476,8 +480,17 @@ void build_plan(nwg_store* s, Plan& P, bool soft, int lanes, int rpl, int elem_b
             else if (soft && !s->tracked() && rows >= kLongRows && nb >= 256) g = Geo{32, 4, false, long_warps(rows, 128)};
             else if (!soft && rows >= kLongRows && nb >= 256) g = Geo{32, 8, false, long_warps(rows, 256)};
             else {
+                auto ic = s->geo_costs.find({int(soft), sc});
+                if (ic != s->geo_costs.end()) {
+                    double best = 1e300;
+                    for (const auto& gc : ic->second) {
+                        if (soft && gc.G == 1 && !lane_ok_soft) continue;
+                        const double t = gc.ns_per_cell * geo_cost(Geo{gc.G, gc.R}, std::max(rows, 1), nb, soft ? 1 : 0);
+                        if (t < best) { best = t; g = Geo{gc.G, gc.R}; }
+                    }
+                }
                 auto it = s->geo_table.find({int(soft), sc});
-                if (it != s->geo_table.end() && (!soft || it->second.first > 1 || lane_ok_soft))
+                if (ic == s->geo_costs.end() && it != s->geo_table.end() && (!soft || it->second.first > 1 || lane_ok_soft))
                     g = Geo{it->second.first, it->second.second};
             }
         }
@@ -1177,12 +1190,31 @@ int nwg_set_geometry(nwg_store* s, int soft, int size_class_, int lanes, int row
         if (!s) throw Error(NWG_EINVAL, "null store");
         if (size_class_ < 0) {   // -1: forget every tuned geometry; -2: the plain fill
             s->geo_table.clear();
+            s->geo_costs.clear();
             s->plain = size_class_ == -2;
         } else {
             if (!geo_available(soft != 0, lanes, rows)) throw Error(NWG_EINVAL, "no kernel for this geometry");
             s->geo_table[{soft ? 1 : 0, size_class_}] = {lanes, rows};
+            s->geo_costs.erase({soft ? 1 : 0, size_class_});
             s->plain = false;
         }
+        s->hard_plan.reset(); s->soft_plan.reset(); s->soft_band_plan.reset();
+    });
+}
+
+int nwg_set_geometry_costs(nwg_store* s, int soft, int size_class_, int n, const int* lanes, const int* rows,
+                           const double* ns_per_cell) {
+    return guarded([&] {
+        if (!s || n < 1 || !lanes || !rows || !ns_per_cell || size_class_ < 0) throw Error(NWG_EINVAL, "bad argument");
+        std::vector<nwg_store::GeoCost> v;
+        for (int k = 0; k < n; ++k) {
+            if (!geo_available(soft != 0, lanes[k], rows[k])) throw Error(NWG_EINVAL, "no kernel for this geometry");
+            if (!(ns_per_cell[k] > 0.0) || !std::isfinite(ns_per_cell[k])) throw Error(NWG_EINVAL, "costs must be positive");
+            v.push_back({lanes[k], rows[k], ns_per_cell[k]});
+        }
+        s->geo_costs[{soft ? 1 : 0, size_class_}] = std::move(v);
+        s->geo_table.erase({soft ? 1 : 0, size_class_});
+        s->plain = false;
         s->hard_plan.reset(); s->soft_plan.reset(); s->soft_band_plan.reset();
     });
 }

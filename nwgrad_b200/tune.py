@@ -9,9 +9,15 @@ Pairs are grouped in size classes: max(20, ceil(log2(rows * columns))), the same
 library's planner (so every pair up to 2^20 cells is one class).  For each class in a batch
 the tuner aligns a sample of the class's own pairs with every candidate geometry, times the
 device work (``SeqPairBatch.last_timing``), keeps the fastest and stores the choice in a JSON
-cache keyed by device, problem type and class.  ``apply`` hands the table to the library
-(``nwg_set_geometry``); ``plain`` selects the plain fill instead (one fixed geometry, 32
-lanes x 4 rows, for every pair).
+cache keyed by device, problem type and class.
+
+Per pair, geometries differ mainly in padding: a pair's rows are rounded up to whole stripes
+of lanes x rows DP rows, and each stripe adds the lanes' skew to its columns.  So the tuner
+also turns each geometry's measured time into a cost per padded cell and tries the mixed
+plan in which every pair of the class takes the geometry with the least cost x padded cells
+(``nwg_set_geometry_costs``); the mixed plan is kept when it measures faster than the best
+single geometry.  ``apply`` hands the table to the library; ``plain`` selects the plain fill
+instead (one fixed geometry, 32 lanes x 4 rows, for every pair).
 """
 from __future__ import annotations
 
@@ -118,14 +124,43 @@ def _candidates(batch):
     return list(HARD_GEOS)
 
 
+def _padded(batch, idx, geo) -> float:
+    """Cells the geometry computes for the pairs idx: whole stripes, columns plus the skew."""
+    G, R = geo
+    m = (batch._oa[idx + 1] - batch._oa[idx]).astype(np.float64)
+    n = (batch._ob[idx + 1] - batch._ob[idx]).astype(np.float64)
+    rows = m + 1 if _soft(batch) else m
+    extra = 1 if _soft(batch) else 0
+    stripes = np.ceil(np.maximum(rows, 1) / (G * R))
+    return float(np.sum(stripes * G * R * (n + extra + G - 1)))
+
+
+def _set_costs(batch, sc: int, costs) -> None:
+    from ._capi import check, ptr, _i32p, _dp
+    lanes = np.array([g for g, _, _ in costs], np.int32)
+    rows = np.array([r for _, r, _ in costs], np.int32)
+    ns = np.array([c for _, _, c in costs], np.float64)
+    check(batch._store._L.nwg_set_geometry_costs(batch._store.h, 1 if _soft(batch) else 0, int(sc), len(costs),
+                                                ptr(lanes, _i32p), ptr(rows, _i32p), ptr(ns, _dp)))
+
+
+def describe(entry) -> str:
+    """A table entry in words."""
+    if isinstance(entry, dict):
+        return "per pair by cost: " + ", ".join(f"{g}x{r}" for g, r, _ in entry["costs"])
+    return f"{entry[0]} lanes x {entry[1]} rows"
+
+
 def _key(batch, sc: int) -> str:
     return "|".join(str(x) for x in (_device_name(batch._device), "soft" if _soft(batch) else "hard",
                                      batch._gap_model, batch._mode, batch._precision, batch._alpha.size,
                                      batch._params.num_sets, int(batch._tracked), sc))
 
 
-def tune(batch, sample_pairs: int = 65536, force: bool = False, verbose: bool = False, reps: int = 2) -> dict:
-    """{size class: (lanes, rows)} for the classes of ``batch``, measured (or from the cache).
+def tune(batch, sample_pairs: int = 65536, force: bool = False, verbose: bool = False, reps: int = 2,
+         mixed: bool = True) -> dict:
+    """{size class: (lanes, rows) or {"costs": [(lanes, rows, ns per padded cell), ...]}} for the
+    classes of ``batch``, measured (or from the cache).
 
     The sample should fill the device many times over for every candidate (the narrower
     geometries run several times as many pairs at once): a sample that does not would
@@ -138,7 +173,8 @@ def tune(batch, sample_pairs: int = 65536, force: bool = False, verbose: bool = 
     for sc, idx in sorted(_classes(batch).items()):
         key = _key(batch, sc)
         if not force and key in cache:
-            table[sc] = tuple(cache[key]["geo"])
+            ent = cache[key]
+            table[sc] = {"costs": [tuple(x) for x in ent["costs"]]} if "costs" in ent else tuple(ent["geo"])
             continue
         if codes is None:
             codes = _codes(batch)
@@ -156,16 +192,42 @@ def tune(batch, sample_pairs: int = 65536, force: bool = False, verbose: bool = 
             times[f"{geo[0]}x{geo[1]}"] = ms
             if ms < best_ms:
                 best, best_ms = geo, ms
-        del sub
         if best is None:
+            del sub
             continue
-        table[sc] = best
-        cache[key] = {"geo": list(best), "gcups": cells / (best_ms / 1e3) / 1e9 if best_ms > 0 else None,
-                      "ms": times, "sample_pairs": int(idx.size)}
+        entry = best
+        mixed_ms = None
+        if mixed and len(times) > 1:
+            # the mixed plan: every pair takes the geometry with the least measured cost x its
+            # padded cells; kept when it beats the best single geometry
+            sidx = np.arange(len(idx), dtype=np.int64)
+            costs = []
+            for geo in _candidates(batch):
+                k = f"{geo[0]}x{geo[1]}"
+                if k in times:
+                    costs.append((geo[0], geo[1], times[k] * 1e6 / max(_padded(sub, sidx, geo), 1.0)))
+            try:
+                sub._tune = (0, 0)
+                _set_costs(sub, sc, costs)
+                sub._run(grad)
+                mixed_ms = min(_timed(sub, grad) for _ in range(reps))
+            except (ValueError, RuntimeError):
+                mixed_ms = None
+            if mixed_ms is not None and mixed_ms < 0.99 * best_ms:
+                entry = {"costs": costs}
+        del sub
+        table[sc] = entry
+        use_ms = mixed_ms if isinstance(entry, dict) else best_ms
+        cache[key] = {"gcups": cells / (use_ms / 1e3) / 1e9 if use_ms > 0 else None, "ms": times,
+                      "mixed_ms": mixed_ms, "sample_pairs": int(idx.size)}
+        if isinstance(entry, dict):
+            cache[key]["costs"] = [list(x) for x in entry["costs"]]
+        else:
+            cache[key]["geo"] = list(entry)
         dirty = True
         if verbose:
-            print(f"size class 2^{sc}: {idx.size} pairs, best {best[0]} lanes x {best[1]} rows "
-                  f"({best_ms:.3f} ms); " + ", ".join(f"{k} {v:.3f}" for k, v in times.items()))
+            print(f"size class 2^{sc}: {idx.size} pairs, best single {best[0]} lanes x {best[1]} rows "
+                  f"({best_ms:.3f} ms), mixed {mixed_ms}; " + ", ".join(f"{k} {v:.3f}" for k, v in times.items()))
     if dirty:
         _save_cache(cache)
     return table
@@ -182,8 +244,12 @@ def apply(batch, table: dict) -> None:
     L = batch._store._L
     check(L.nwg_set_geometry(batch._store.h, 0, -1, 0, 0))
     soft = 1 if _soft(batch) else 0
-    for sc, (lanes, rows) in table.items():
-        check(L.nwg_set_geometry(batch._store.h, soft, int(sc), int(lanes), int(rows)))
+    for sc, entry in table.items():
+        if isinstance(entry, dict):
+            _set_costs(batch, sc, entry["costs"])
+        else:
+            lanes, rows = entry
+            check(L.nwg_set_geometry(batch._store.h, soft, int(sc), int(lanes), int(rows)))
 
 
 def plain(batch) -> None:

@@ -280,13 +280,19 @@ def test_autotuned_and_plain_fill_same_results(grad_mode, tmp_path, monkeypatch)
     sa += rand_seqs(rng, 4, 1100, 1500, AA)
     sb += [mutate(rng, s, AA) for s in sa[-4:]]
     res = []
-    for how in ("planner", "tuned", "plain"):
+    from nwgrad_b200 import tune
+    for how in ("planner", "tuned", "plain", "mixed"):
         b = nw.SeqPairBatch(sa, sb, _params(AA, mat, gaps), grad_mode=grad_mode)
         if how == "tuned":
             table = b.autotune(sample_pairs=64)
-            assert table and all(isinstance(v, tuple) for v in table.values())
+            assert table and all(isinstance(v, (tuple, dict)) for v in table.values())
         elif how == "plain":
             b.use_plain_fill()
+        elif how == "mixed":
+            # equal costs: every pair takes the geometry that pads it least (a mix of buckets)
+            geos = tune.SOFT_GEOS if grad_mode == "soft" else tune.HARD_GEOS
+            costs = [(g, r, 1.0) for g, r in geos if g > 1]
+            tune.apply(b, {sc: {"costs": costs} for sc in tune._classes(b)})
         b.score_and_grad()
         gmat, ggap = b.grads()
         res.append((b.scores(), gmat.copy(), ggap.copy()))
