@@ -913,6 +913,141 @@ struct Hb {
 // One pair by Hirschberg when it splits (m > cutoff); else the Pointers path (aligner.hpp
 // :1360, run_viterbi: a pair that never splits runs AS Pointers).  Guide in the recursion's
 // convention: the column where the path enters each row (guide_j_affine_hb :5233-5249).
+// The endpoint scan of Local Hirschberg (hb_scan_scalar, aligner.hpp:4611-4698) over rows
+// [i0, i1), columns [j0, j1): forward (reverse = false) or from the far corner back; `local`:
+// the clamped Smith-Waterman recurrence with free starts on row 0 and column 0, else the
+// global borders (row 0 the charged Y chain, column 0 the X chain).  The best cell is the
+// first strictly larger max(M, X, Y) in row-major scan order from 0 (topmost row, then
+// leftmost column), in block coordinates (rows 1..H, columns 1..NC); (0, 0) with best 0
+// when no cell is positive.  Pmax: the prefix-max horizontal carry.
+template <class T>
+void hb_scan(const T* blk, int N, const uint8_t* a, const uint8_t* b, T go_a, T ge_a, T go_b, T ge_b, bool pmax,
+             bool local, bool reverse, int i0, int i1, int j0, int j1, T& best, int& bi, int& bj) {
+    const int H = i1 - i0, NC = j1 - j0;
+    best = T(0); bi = 0; bj = 0;
+    if (H == 0 || NC == 0) return;
+    const int a_start = reverse ? i1 - 1 : i0, a_step = reverse ? -1 : 1;
+    const int b_start = reverse ? j1 - 1 : j0, b_step = reverse ? -1 : 1;
+    std::vector<T> pM(NC + 1), pX(NC + 1), pY(NC + 1), cM(NC + 1), cX(NC + 1), cY(NC + 1), rmp(NC + 1);
+    if (pmax) for (int k = 0; k < NC; ++k) rmp[k] = static_cast<T>(k) * ge_a;
+    pM[0] = T(0); pX[0] = ninf<T>(); pY[0] = ninf<T>();
+    for (int cc = 1; cc <= NC; ++cc) {
+        if (local) { pM[cc] = T(0); pX[cc] = ninf<T>(); pY[cc] = ninf<T>(); }
+        else {
+            pM[cc] = ninf<T>(); pX[cc] = ninf<T>();
+            pY[cc] = mx<T>((mx<T>(pM[cc - 1], pX[cc - 1]) - go_a) - ge_a, pY[cc - 1] - ge_a);
+        }
+    }
+    T gbest = T(0); int gi = 0, gj = 0;
+    for (int t = 0; t < H; ++t) {
+        const int arow = a_start + t * a_step;
+        cM[0] = local ? T(0) : ninf<T>();
+        cX[0] = mx<T>(mx<T>((pM[0] - go_b) - ge_b, pX[0] - ge_b), (pY[0] - go_b) - ge_b);
+        cY[0] = ninf<T>();
+        T P = cY[0] - ge_a;
+        for (int cc = 1; cc <= NC; ++cc) {
+            const int bcol = b_start + (cc - 1) * b_step;
+            T mv = mx3<T>(pM[cc - 1], pX[cc - 1], pY[cc - 1]) + blk[size_t(a[arow]) * N + b[bcol]];
+            if (local) mv = mx<T>(mv, T(0));
+            const T xv = mx<T>(mx<T>((pM[cc] - go_b) - ge_b, pX[cc] - ge_b), (pY[cc] - go_b) - ge_b);
+            T yv;
+            if (pmax) {
+                const T g = (mx<T>(cM[cc - 1], cX[cc - 1]) - go_a) - ge_a;
+                P = mx<T>(g + rmp[cc - 1], P);
+                yv = P - rmp[cc - 1];
+            } else {
+                yv = mx<T>(mx<T>((cM[cc - 1] - go_a) - ge_a, (cX[cc - 1] - go_a) - ge_a), cY[cc - 1] - ge_a);
+            }
+            cM[cc] = mv; cX[cc] = xv; cY[cc] = yv;
+            const T here = mx3<T>(mv, xv, yv);
+            if (here > gbest) { gbest = here; gi = t + 1; gj = cc; }
+        }
+        std::swap(pM, cM); std::swap(pX, cX); std::swap(pY, cY);
+    }
+    best = gbest; bi = gi; bj = gj;
+}
+
+// The path's score in T, counts and guide, replayed from (i0, j0) (aligner.hpp:4530-4552,
+// hard_fields :776-790, guide_j_affine_hb :5233-5249).
+template <class T>
+void hb_replay(const Model& M, const uint8_t* a, int m, const uint8_t* b, int n, const std::vector<uint8_t>& hops,
+               const std::vector<T>& blk, T go_a, T ge_a, T go_b, T ge_b, int i0, int j0, int ie, int je, HardOut& o) {
+    T s = T(0);
+    int i = i0, j = j0;
+    uint8_t prev = 3;
+    std::vector<int32_t> gj(size_t(m) + 1, -1);
+    gj[0] = 0;
+    gj[i0] = j0;
+    for (uint8_t op : hops) {
+        if (op == 0) {
+            ++i; ++j;
+            s += blk[size_t(a[i - 1]) * M.N + b[j - 1]];
+            if (o.grad) o.grad[size_t(a[i - 1]) * M.N + b[j - 1]] += 1.0;
+            gj[i] = j;
+        } else if (op == 1) {
+            ++i;
+            if (prev != 1) { s -= go_b; if (o.grad) o.grad[size_t(M.N) * M.N + kOpenB] -= 1.0; }
+            s -= ge_b;
+            if (o.grad) o.grad[size_t(M.N) * M.N + kExtendB] -= 1.0;
+            gj[i] = j;
+        } else {
+            if (prev != 2) { s -= go_a; if (o.grad) o.grad[size_t(M.N) * M.N + kOpenA] -= 1.0; }
+            s -= ge_a;
+            if (o.grad) o.grad[size_t(M.N) * M.N + kExtendA] -= 1.0;
+            ++j;
+        }
+        prev = op;
+    }
+    gj[m] = n;
+    fill_guide_gaps(gj);
+    if (o.guide) std::memcpy(o.guide, gj.data(), sizeof(int32_t) * (m + 1));
+    if (o.moves) {
+        const int64_t k = std::min<int64_t>(int64_t(hops.size()), o.moves_cap);
+        for (int64_t q = 0; q < k; ++q) o.moves[q] = hops[q];
+    }
+    o.nmoves = int64_t(hops.size());
+    o.score = static_cast<double>(s);
+    o.end_i = ie; o.end_j = je; o.start_i = i0; o.start_j = j0;
+}
+
+// Local affine Hirschberg (viterbi_affine_hirschberg_local, aligner.hpp:4746-4790), for a
+// pair longer than the cutoff (shorter ones run the Pointers path): the
+// forward clamped scan gives the end cell (ie, je) and the score; none positive: the empty
+// alignment (score 0 at (0, 0)).  Else the reverse global-suffix scan over rows [0, ie),
+// columns [0, je) gives the start (is, js) = (ie - p, je - q); the box A[is, ie) x B[js, je)
+// is solved globally by the recursion (short boxes by its base case) and the path replayed.
+template <class T>
+int hb_local_one(const Model& M, const uint8_t* a, int m, const uint8_t* b, int n, int cutoff, bool pmax,
+                 HardOut& o) {
+    // a pair of at most `cutoff` rows runs AS Pointers (hb_splits, aligner.hpp:137-141)
+    if (m <= cutoff) return hard_one<T>(M, a, m, b, n, nullptr, nullptr, false, nullptr, -1, o, 0);
+    std::vector<T> blk(size_t(M.N) * M.N);
+    for (size_t k = 0; k < blk.size(); ++k) blk[k] = static_cast<T>(M.mat[k]);
+    const T go_a = static_cast<T>(M.gaps[kOpenA]), ge_a = static_cast<T>(M.gaps[kExtendA]);
+    const T go_b = static_cast<T>(M.gaps[kOpenB]), ge_b = static_cast<T>(M.gaps[kExtendB]);
+    T sf; int ie, je;
+    hb_scan<T>(blk.data(), M.N, a, b, go_a, ge_a, go_b, ge_b, pmax, true, false, 0, m, 0, n, sf, ie, je);
+    std::vector<uint8_t> hops;
+    if (!(sf > T(0)) || ie <= 0 || je <= 0) {
+        hb_replay<T>(M, a, m, b, n, hops, blk, go_a, ge_a, go_b, ge_b, 0, 0, 0, 0, o);
+        return 0;
+    }
+    T sr; int p, q;
+    hb_scan<T>(blk.data(), M.N, a, b, go_a, ge_a, go_b, ge_b, pmax, false, true, 0, ie, 0, je, sr, p, q);
+    const int is = ie - p, js = je - q;
+    if (pmax) {
+        Hb<T, true> h{M.N, blk.data(), a, b, cutoff, go_a, ge_a, go_b, ge_b, {}};
+        h.solve(is, ie, js, je, false, false);
+        hops.swap(h.hops);
+    } else {
+        Hb<T, false> h{M.N, blk.data(), a, b, cutoff, go_a, ge_a, go_b, ge_b, {}};
+        h.solve(is, ie, js, je, false, false);
+        hops.swap(h.hops);
+    }
+    hb_replay<T>(M, a, m, b, n, hops, blk, go_a, ge_a, go_b, ge_b, is, js, ie, je, o);
+    return 0;
+}
+
 template <class T>
 int hb_one(const Model& M, const uint8_t* a, int m, const uint8_t* b, int n, int cutoff, bool pmax,
            HardOut& o) {
@@ -1044,8 +1179,8 @@ int orc_soft_batch(int gm, int am, int N, int K, const double* mat, const double
 int orc_hb_batch(int prec, int pmax, int cutoff, int N, const double* mat, const double* gaps,
                  const uint8_t* a, const int64_t* oa, const uint8_t* b, const int64_t* ob, int64_t n_pairs,
                  double* scores, double* grads, int32_t* guides, uint8_t* moves, int64_t moves_cap,
-                 int64_t* nmoves) {
-    Model M{1, 0, N, 1, mat, gaps};
+                 int64_t* nmoves, int local, int32_t* ends) {
+    Model M{1, local ? 1 : 0, N, 1, mat, gaps};
     const size_t gs = size_t(N) * N + 4;
     for (int64_t p = 0; p < n_pairs; ++p) {
         const int m = int(oa[p + 1] - oa[p]), n = int(ob[p + 1] - ob[p]);
@@ -1055,10 +1190,16 @@ int orc_hb_batch(int prec, int pmax, int cutoff, int N, const double* mat, const
         o.guide = guides ? guides + oa[p] + p : nullptr;
         o.moves = moves ? moves + moves_cap * p : nullptr;
         o.moves_cap = moves_cap;
-        if (prec == 32) hb_one<float>(M, a + oa[p], m, b + ob[p], n, cutoff, pmax != 0, o);
-        else            hb_one<double>(M, a + oa[p], m, b + ob[p], n, cutoff, pmax != 0, o);
+        if (local) {
+            if (prec == 32) hb_local_one<float>(M, a + oa[p], m, b + ob[p], n, cutoff, pmax != 0, o);
+            else            hb_local_one<double>(M, a + oa[p], m, b + ob[p], n, cutoff, pmax != 0, o);
+        } else {
+            if (prec == 32) hb_one<float>(M, a + oa[p], m, b + ob[p], n, cutoff, pmax != 0, o);
+            else            hb_one<double>(M, a + oa[p], m, b + ob[p], n, cutoff, pmax != 0, o);
+        }
         scores[p] = o.score;
         if (nmoves) nmoves[p] = o.nmoves;
+        if (ends) { ends[4 * p] = o.start_i; ends[4 * p + 1] = o.start_j; ends[4 * p + 2] = o.end_i; ends[4 * p + 3] = o.end_j; }
     }
     return 0;
 }

@@ -167,11 +167,12 @@ def hb_fixtures():
         for prec in (32, 64):
             for tb in ("hirschberg", "hirschberg_pmax"):
                 for cut in (8, 64):
-                    r = oracle.ref_run(prec, 1, 0, 1, AA, mat, gaps, sa, sb, traceback=tb, hb_cutoff=cut)
-                    key = f"{name}_{tb}_{prec}_c{cut}_"
-                    out[key + "scores"] = r["scores"]
-                    out[key + "grads"] = r["grads"]
-                    out[key + "guides"] = r["guides"]
+                    for am, tag in ((0, ""), (1, "L_")):   # global, local
+                        r = oracle.ref_run(prec, 1, am, 1, AA, mat, gaps, sa, sb, traceback=tb, hb_cutoff=cut)
+                        key = f"{name}_{tag}{tb}_{prec}_c{cut}_"
+                        out[key + "scores"] = r["scores"]
+                        out[key + "grads"] = r["grads"]
+                        out[key + "guides"] = r["guides"]
     np.savez_compressed(os.path.join(HERE, "hirschberg.npz"), **out)
     print("hirschberg.npz:", len(out), "arrays")
 

@@ -106,8 +106,9 @@ def test_live_reference_random(gm, am):
 
 
 def test_hirschberg_fixtures():
-    """The Hirschberg restatement (exact and prefix-max carry) against the reference's own
-    engine with traceback hirschberg / hirschberg_pmax (tests/golden/hirschberg.npz)."""
+    """The Hirschberg restatement (exact and prefix-max carry; Global and Local) against the
+    reference's own engine with traceback hirschberg / hirschberg_pmax
+    (tests/golden/hirschberg.npz)."""
     z = np.load(os.path.join(GOLD, "hirschberg.npz"))
     for name in ("int", "flt"):
         sa, sb = [str(s) for s in z[f"{name}_sa"]], [str(s) for s in z[f"{name}_sb"]]
@@ -115,12 +116,13 @@ def test_hirschberg_fixtures():
         for prec in (32, 64):
             for tb in ("hirschberg", "hirschberg_pmax"):
                 for cut in (8, 64):
-                    key = f"{name}_{tb}_{prec}_c{cut}_"
-                    o = oracle.hirschberg(prec, z[f"{name}_mat"], z[f"{name}_gaps"], enc, cutoff=cut,
-                                          pmax=tb.endswith("pmax"))
-                    np.testing.assert_array_equal(o["scores"], z[key + "scores"])
-                    np.testing.assert_array_equal(o["grads"], z[key + "grads"])
-                    np.testing.assert_array_equal(o["guides"], z[key + "guides"])
+                    for local, tag in ((False, ""), (True, "L_")):
+                        key = f"{name}_{tag}{tb}_{prec}_c{cut}_"
+                        o = oracle.hirschberg(prec, z[f"{name}_mat"], z[f"{name}_gaps"], enc, cutoff=cut,
+                                              pmax=tb.endswith("pmax"), local=local)
+                        np.testing.assert_array_equal(o["scores"], z[key + "scores"])
+                        np.testing.assert_array_equal(o["grads"], z[key + "grads"])
+                        np.testing.assert_array_equal(o["guides"], z[key + "guides"])
 
 
 def test_soft_banded_fixtures():
