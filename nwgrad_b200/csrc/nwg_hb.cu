@@ -1,4 +1,5 @@
-// Hirschberg re-alignment (affine Global, untracked) on the GPU: linear memory for long pairs.
+// Hirschberg re-alignment (affine Global and Local, untracked) on the GPU: linear memory for
+// long pairs.
 //
 // The reference's recursion (aligner.hpp:4151-4560): a block (rows i0..i1, columns j0..j1,
 // boundary states in_x / out_x) longer than the cutoff is split at row p = i0 + H/2; a
@@ -21,6 +22,12 @@
 //   * hb_replay_kernel -- one thread per pair: the base blocks' moves in path order.
 // Cells use the reference's expressions ((v - go) - ge, max of three, the prefix-max carry's
 // rounded multiply and add), so the path, score, gradient and guide are bit-identical.
+//
+// Local (viterbi_affine_hirschberg_local, aligner.hpp:4746-4790): hb_scan_kernel runs the
+// forward clamped scan of each pair for its end cell (ie, je) -- none positive: the empty
+// alignment -- then the reverse global-suffix scan over rows [0, ie), columns [0, je) for the
+// start (is, js); the box A[is, ie) x B[js, je) then goes through the same recursion as a
+// Global pair, and the replay starts at (is, js).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -54,6 +61,12 @@ struct BaseJob {
     int64_t moves;                   // byte offset of the moves (walk order, H + W at most)
 };
 
+struct ScanJob {
+    int64_t a_base, b_base;          // row t >= 1 reads a[a_base + a_step (t - 1)]; column c >= 1 b[b_base + b_step (c - 1)]
+    int a_step, b_step;
+    int H, W, local, pad;
+};
+
 template <class T> struct Gaps { T go_a, ge_a, go_b, ge_b; };
 
 template <class T>
@@ -63,6 +76,130 @@ __device__ __forceinline__ T chain_y(T lm, T lx, T ly, const Gaps<T>& g) {
 template <class T>
 __device__ __forceinline__ T chain_x(T um, T ux, T uy, const Gaps<T>& g) {
     return hmax3((um - g.go_b) - g.ge_b, ux - g.ge_b, (uy - g.go_b) - g.ge_b);
+}
+
+// ── endpoint scan ─────────────────────────────────────────────────────────────
+// hb_scan_scalar (aligner.hpp:4611-4698) over one block: `local`, the clamped recurrence with
+// free starts on row 0 and column 0; else the global borders (row 0 the charged Y chain,
+// column 0 the X chain).  The best cell is the first strictly larger max(M, X, Y) in
+// row-major order from 0: each lane keeps the lexicographically least (row, column) among its
+// largest cells, then the warp reduces with the same order.  One warp per block: lanes own R
+// rows of a 32R-row stripe, skewed by one column; the row above arrives by shuffle, lane 0's
+// from the previous stripe's bottom row (a per-warp row in global memory) or row 0.
+template <class T, bool PMAX, int R>
+__global__ void __launch_bounds__(128) hb_scan_kernel(const uint8_t* __restrict__ a, const uint8_t* __restrict__ b,
+                                                      const T* __restrict__ mat, int N, Gaps<T> gp,
+                                                      const ScanJob* __restrict__ jobs, int n_jobs, T* rows,
+                                                      int64_t row_stride, int32_t* __restrict__ res) {
+    extern __shared__ __align__(16) unsigned char hb_smem[];
+    T* smat = reinterpret_cast<T*>(hb_smem);
+    for (int k = threadIdx.x; k < N * N; k += blockDim.x) smat[k] = mat[k];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    const int64_t wg = int64_t(blockIdx.x) * wpb + (threadIdx.x >> 5);
+    const int64_t nwarps = int64_t(gridDim.x) * wpb;
+    T* bnd = rows + wg * row_stride;
+    const T NI = ninf<T>();
+    const T go_a = gp.go_a, ge_a = gp.ge_a, go_b = gp.go_b, ge_b = gp.ge_b;
+    for (int64_t jb = wg; jb < n_jobs; jb += nwarps) {
+        const ScanJob J = jobs[jb];
+        const int H = J.H, W = J.W;
+        const bool loc = J.local != 0;
+        T bv = T(0); int bi = 0, bj = 0;
+        if (H > 0 && W > 0) {
+            const int nst = (H + 32 * R - 1) / (32 * R);
+            for (int s = 0; s < nst; ++s) {
+                const int i0 = s * 32 * R + lane * R + 1;   // block row of this lane's first row
+                int code[R];
+                bool valid[R];
+                T cM[R], cX[R], cY[R], P[R];
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const int i = i0 + r;
+                    valid[r] = i <= H;
+                    code[r] = valid[r] ? int(a[J.a_base + int64_t(J.a_step) * (i - 1)]) * N : 0;
+                    cM[r] = NI; cX[r] = NI; cY[r] = NI; P[r] = NI;
+                }
+                T dgM = NI, dgX = NI, dgY = NI;       // row above, column c - 1
+                T upM = NI, upX = NI, upY = NI;       // row above, column c
+                T r0M = T(0), r0X = NI, r0Y = NI;     // row 0 at column c - 1 (lane 0, stripe 0)
+                // lane 0, s > 0: the previous stripe's bottom row one column ahead
+                T nuM = NI, nuX = NI, nuY = NI;
+                if (lane == 0 && s > 0) { nuM = bnd[0]; nuX = bnd[1]; nuY = bnd[2]; }
+                const int S = W + 32;
+                for (int t = 0; t < S; ++t) {
+                    const int c = t - lane;
+                    if (lane == 0 && c <= W) {
+                        if (s == 0) {
+                            if (c == 0 || loc) { upM = T(0); upX = NI; upY = NI; }
+                            else {
+                                upM = NI; upX = NI;
+                                upY = hmax((hmax(r0M, r0X) - go_a) - ge_a, r0Y - ge_a);
+                            }
+                            r0M = upM; r0X = upX; r0Y = upY;
+                        } else {
+                            upM = nuM; upX = nuX; upY = nuY;
+                            if (c < W) { nuM = bnd[4 * (c + 1)]; nuX = bnd[4 * (c + 1) + 1]; nuY = bnd[4 * (c + 1) + 2]; }
+                        }
+                    }
+                    if (c >= 0 && c <= W) {
+                        T qM = upM, qX = upX, qY = upY;
+                        T pM = dgM, pX = dgX, pY = dgY;
+                        const int bc = c >= 1 ? int(b[J.b_base + int64_t(J.b_step) * (c - 1)]) : 0;
+                        const T rmpc = (PMAX && c >= 1) ? static_cast<T>(c - 1) * ge_a : T(0);
+#pragma unroll
+                        for (int r = 0; r < R; ++r) {
+                            T m, x, y;
+                            x = hmax3((qM - go_b) - ge_b, qX - ge_b, (qY - go_b) - ge_b);
+                            if (c == 0) {
+                                m = loc ? T(0) : NI;
+                                y = NI;
+                                if constexpr (PMAX) P[r] = y - ge_a;
+                            } else {
+                                m = hmax3(pM, pX, pY) + smat[code[r] + bc];
+                                if (loc) m = hmax(m, T(0));
+                                if constexpr (PMAX) {
+                                    const T gg = (hmax(cM[r], cX[r]) - go_a) - ge_a;
+                                    P[r] = hmax(gg + rmpc, P[r]);
+                                    y = P[r] - rmpc;
+                                } else {
+                                    y = hmax3((cM[r] - go_a) - ge_a, (cX[r] - go_a) - ge_a, cY[r] - ge_a);
+                                }
+                                if (valid[r]) {
+                                    const T here = hmax3(m, x, y);
+                                    const int i = i0 + r;
+                                    if (here > bv || (here == bv && i < bi)) { bv = here; bi = i; bj = c; }
+                                }
+                            }
+                            pM = cM[r]; pX = cX[r]; pY = cY[r];
+                            cM[r] = m; cX[r] = x; cY[r] = y;
+                            qM = m; qX = x; qY = y;
+                        }
+                        dgM = upM; dgX = upX; dgY = upY;
+                    }
+                    const T sM = __shfl_up_sync(0xffffffffu, cM[R - 1], 1);
+                    const T sX = __shfl_up_sync(0xffffffffu, cX[R - 1], 1);
+                    const T sY = __shfl_up_sync(0xffffffffu, cY[R - 1], 1);
+                    if (lane > 0) { upM = sM; upX = sX; upY = sY; }
+                    if (lane == 31 && c >= 0 && c <= W && s + 1 < nst) {
+                        bnd[4 * c] = cM[R - 1]; bnd[4 * c + 1] = cX[R - 1]; bnd[4 * c + 2] = cY[R - 1];
+                    }
+                }
+                __syncwarp();
+            }
+        }
+        // the warp's best: largest value, then least row, then least column
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const T ov = __shfl_xor_sync(0xffffffffu, bv, off);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+            const int oj = __shfl_xor_sync(0xffffffffu, bj, off);
+            if (ov > bv || (ov == bv && (oi < bi || (oi == bi && oj < bj)))) { bv = ov; bi = oi; bj = oj; }
+        }
+        if (lane == 0) { res[3 * jb] = bv > T(0) ? 1 : 0; res[3 * jb + 1] = bi; res[3 * jb + 2] = bj; }
+        __syncwarp();
+    }
 }
 
 // ── sweep ─────────────────────────────────────────────────────────────────────
@@ -344,7 +481,8 @@ __global__ void __launch_bounds__(128) hb_base_kernel(const uint8_t* __restrict_
 // ── replay ────────────────────────────────────────────────────────────────────
 template <class T>
 __global__ void hb_replay_kernel(const HbRun P, const BaseJob* __restrict__ jobs, const int64_t* __restrict__ first,
-                                 const uint8_t* __restrict__ moves, const int32_t* __restrict__ nmoves, int n) {
+                                 const uint8_t* __restrict__ moves, const int32_t* __restrict__ nmoves, int n,
+                                 const int32_t* __restrict__ boxes) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const int p = P.pairs[k];
@@ -359,12 +497,16 @@ __global__ void hb_replay_kernel(const HbRun P, const BaseJob* __restrict__ jobs
     double* g = P.grad ? P.grad + P.gstride * p : nullptr;
     const int64_t NN = int64_t(N) * N;
     int32_t* gj = P.guide ? P.guide + ao + p : nullptr;
-    if (gj) { for (int q = 0; q <= m; ++q) gj[q] = -1; gj[0] = 0; }
+    // Local: the path runs from its box's start (is, js) to its end (ie, je); Global: (0, 0)
+    // to (m, n)
+    const int is = boxes ? boxes[4 * k] : 0, js = boxes ? boxes[4 * k + 1] : 0;
+    const int ie = boxes ? boxes[4 * k + 2] : m, je = boxes ? boxes[4 * k + 3] : nb;
+    if (gj) { for (int q = 0; q <= m; ++q) gj[q] = -1; gj[0] = 0; gj[is] = js; }
     uint8_t* keep = P.moves ? P.moves + P.moves_off[p] : nullptr;
     int64_t total = 0;
     for (int64_t q = first[k]; q < first[k + 1]; ++q) total += nmoves[q];
     T s = T(0);
-    int i = 0, j = 0;
+    int i = is, j = js;
     int prev = 3;
     int64_t idx = 0;
     for (int64_t q = first[k]; q < first[k + 1]; ++q) {
@@ -395,9 +537,9 @@ __global__ void hb_replay_kernel(const HbRun P, const BaseJob* __restrict__ jobs
         }
     }
     P.score[p] = static_cast<double>(s);
-    P.end[4 * p] = m; P.end[4 * p + 1] = nb; P.end[4 * p + 2] = prev == 1 ? 1 : (prev == 2 ? 2 : 0);
+    P.end[4 * p] = ie; P.end[4 * p + 1] = je; P.end[4 * p + 2] = prev == 1 ? 1 : (prev == 2 ? 2 : 0);
     P.end[4 * p + 3] = 0;
-    if (P.path_info) { P.path_info[3 * p] = int32_t(total); P.path_info[3 * p + 1] = 0; P.path_info[3 * p + 2] = 0; }
+    if (P.path_info) { P.path_info[3 * p] = int32_t(total); P.path_info[3 * p + 1] = is; P.path_info[3 * p + 2] = js; }
     if (gj) {
         gj[m] = nb;
         const int L = m + 1;
@@ -442,12 +584,73 @@ int64_t hb_run_t(const HbRun& P, cudaStream_t st, int sms) {
     const Gaps<T> gp{static_cast<T>(P.go_a), static_cast<T>(P.ge_a), static_cast<T>(P.go_b), static_cast<T>(P.ge_b)};
     std::vector<Blk> cur;
     cur.reserve(size_t(n));
-    for (int k = 0; k < n; ++k) {
-        const int p = P.h_pairs[k];
-        cur.push_back(Blk{k, 0, int(P.h_oa[p + 1] - P.h_oa[p]), 0, int(P.h_ob[p + 1] - P.h_ob[p]), 0, 0});
-    }
-    Tmp djobs(st), dout(st), dwrap(st), dres(st);
     constexpr int R = 4;
+    Tmp djobs(st), dout(st), dwrap(st), dres(st), dboxes(st);
+    std::vector<int32_t> boxes;
+    if (!P.local) {
+        for (int k = 0; k < n; ++k) {
+            const int p = P.h_pairs[k];
+            cur.push_back(Blk{k, 0, int(P.h_oa[p + 1] - P.h_oa[p]), 0, int(P.h_ob[p + 1] - P.h_ob[p]), 0, 0});
+        }
+    } else {
+        // Local: the forward clamped scan of every pair, then the reverse global-suffix scan of
+        // the pairs with a positive best, give each pair's box
+        boxes.assign(size_t(n) * 4, 0);
+        const size_t mat_b = size_t((P.N * P.N + 3) & ~3) * sizeof(T);
+        auto run_scans = [&](const std::vector<ScanJob>& sj, std::vector<int32_t>& out) {
+            out.assign(sj.size() * 3, 0);
+            if (sj.empty()) return;
+            int maxw = 1;
+            for (const ScanJob& x : sj) maxw = std::max(maxw, x.W);
+            const int wpb = 4;
+            const int grid = int(std::min<int64_t>((int64_t(sj.size()) + wpb - 1) / wpb, int64_t(sms) * 4));
+            const int64_t stride = 4 * (int64_t(maxw) + 1);
+            ScanJob* dj = static_cast<ScanJob*>(djobs.get(sj.size() * sizeof(ScanJob)));
+            HB_CUDA(cudaMemcpyAsync(dj, sj.data(), sj.size() * sizeof(ScanJob), cudaMemcpyHostToDevice, st));
+            T* rw = static_cast<T*>(dwrap.get(size_t(grid) * wpb * stride * sizeof(T)));
+            int32_t* rs = static_cast<int32_t*>(dres.get(out.size() * sizeof(int32_t)));
+            auto fn = P.pmax ? hb_scan_kernel<T, true, R> : hb_scan_kernel<T, false, R>;
+            HB_CUDA(allow_smem(reinterpret_cast<const void*>(fn), mat_b));
+            fn<<<grid, 32 * wpb, mat_b, st>>>(P.a, P.b, static_cast<const T*>(P.mat), P.N, gp, dj, int(sj.size()), rw,
+                                              stride, rs);
+            HB_CUDA(cudaGetLastError());
+            launches++;
+            HB_CUDA(cudaMemcpyAsync(out.data(), rs, out.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+            HB_CUDA(cudaStreamSynchronize(st));
+        };
+        std::vector<ScanJob> scan_f;
+        scan_f.reserve(size_t(n));
+        for (int k = 0; k < n; ++k) {
+            const int p = P.h_pairs[k];
+            ScanJob J{};
+            J.a_base = P.h_oa[p]; J.a_step = 1; J.b_base = P.h_ob[p]; J.b_step = 1;
+            J.H = int(P.h_oa[p + 1] - P.h_oa[p]); J.W = int(P.h_ob[p + 1] - P.h_ob[p]); J.local = 1; J.pad = 0;
+            scan_f.push_back(J);
+        }
+        std::vector<int32_t> fr, rr;
+        run_scans(scan_f, fr);
+        std::vector<ScanJob> rev;
+        std::vector<int> rk;
+        for (int k = 0; k < n; ++k) {
+            if (!fr[3 * k] || fr[3 * k + 1] <= 0 || fr[3 * k + 2] <= 0) continue;   // no positive cell: empty
+            const int p = P.h_pairs[k];
+            const int ie = fr[3 * k + 1], je = fr[3 * k + 2];
+            ScanJob J{};
+            J.a_base = P.h_oa[p] + ie - 1; J.a_step = -1; J.b_base = P.h_ob[p] + je - 1; J.b_step = -1;
+            J.H = ie; J.W = je; J.local = 0;
+            rev.push_back(J);
+            rk.push_back(k);
+        }
+        run_scans(rev, rr);
+        for (size_t q = 0; q < rk.size(); ++q) {
+            const int k = rk[q];
+            const int ie = fr[3 * k + 1], je = fr[3 * k + 2];
+            const int is = ie - rr[3 * q + 1], js = je - rr[3 * q + 2];
+            boxes[4 * size_t(k)] = is; boxes[4 * size_t(k) + 1] = js;
+            boxes[4 * size_t(k) + 2] = ie; boxes[4 * size_t(k) + 3] = je;
+            cur.push_back(Blk{k, is, ie, js, je, 0, 0});
+        }
+    }
     const int NWmax = 16;
     const size_t ring_bytes_per_warp = size_t(3) * kHbRing * sizeof(T);
     const size_t mat_bytes = size_t((P.N * P.N + 3) & ~3) * sizeof(T);
@@ -544,10 +747,17 @@ int64_t hb_run_t(const HbRun& P, cudaStream_t st, int sms) {
     {
         const int wpb = 4;
         const int grid = int(std::min<int64_t>((int64_t(bj.size()) + wpb - 1) / wpb, int64_t(sms) * 8));
-        hb_base_kernel<T, R><<<grid, 32 * wpb, mat_bytes, st>>>(P.a, P.b, static_cast<const T*>(P.mat), P.N, gp, dB,
-                                                               int(bj.size()), cd, bd, mvd, nm);
-        HB_CUDA(cudaGetLastError());
-        hb_replay_kernel<T><<<(n + 127) / 128, 128, 0, st>>>(P, dB, fd, mvd, nm, n);
+        if (grid > 0) {
+            hb_base_kernel<T, R><<<grid, 32 * wpb, mat_bytes, st>>>(P.a, P.b, static_cast<const T*>(P.mat), P.N, gp,
+                                                                   dB, int(bj.size()), cd, bd, mvd, nm);
+            HB_CUDA(cudaGetLastError());
+        }
+        int32_t* bx = nullptr;
+        if (P.local) {
+            bx = static_cast<int32_t*>(dboxes.get(boxes.size() * sizeof(int32_t)));
+            HB_CUDA(cudaMemcpyAsync(bx, boxes.data(), boxes.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+        }
+        hb_replay_kernel<T><<<(n + 127) / 128, 128, 0, st>>>(P, dB, fd, mvd, nm, n, bx);
         HB_CUDA(cudaGetLastError());
         launches += 2;
     }

@@ -1,5 +1,5 @@
 """Hirschberg re-alignment on the GPU (traceback "hirschberg" / "hirschberg_pmax", affine
-Global): scores, gradients and guides bit for bit against the reference's own engine
+Global and Local): scores, gradients and guides bit for bit against the reference's own engine
 (tests/golden/hirschberg.npz) and against the oracle's restatement on longer pairs."""
 import os
 
@@ -16,9 +16,9 @@ import nwgrad_b200 as nw  # noqa: E402
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
 
 
-def _run(prec, tb, cut, mat, gaps, sa, sb):
+def _run(prec, tb, cut, mat, gaps, sa, sb, mode="global"):
     cls = nw.SeqPairBatch if prec == 32 else nw.SeqPairBatchDouble
-    b = cls(sa, sb, nw.AlignParams.from_arrays(mat, gaps, alphabet=AA), grad_mode="hard", traceback=tb)
+    b = cls(sa, sb, nw.AlignParams.from_arrays(mat, gaps, alphabet=AA), grad_mode="hard", traceback=tb, mode=mode)
     b.hb_cutoff = cut
     tot = b.score_and_grad()
     gm, gg = b.grads()
@@ -30,11 +30,12 @@ def _run(prec, tb, cut, mat, gaps, sa, sb):
 @pytest.mark.parametrize("prec", [32, 64])
 @pytest.mark.parametrize("tb", ["hirschberg", "hirschberg_pmax"])
 @pytest.mark.parametrize("cut", [8, 64])
-def test_reference_fixtures(name, prec, tb, cut):
+@pytest.mark.parametrize("mode", ["global", "local"])
+def test_reference_fixtures(name, prec, tb, cut, mode):
     z = np.load(os.path.join(GOLD, "hirschberg.npz"))
     sa, sb = [str(s) for s in z[f"{name}_sa"]], [str(s) for s in z[f"{name}_sb"]]
-    s, g, gj, tot = _run(prec, tb, cut, z[f"{name}_mat"], z[f"{name}_gaps"], sa, sb)
-    key = f"{name}_{tb}_{prec}_c{cut}_"
+    s, g, gj, tot = _run(prec, tb, cut, z[f"{name}_mat"], z[f"{name}_gaps"], sa, sb, mode)
+    key = f"{name}_{'L_' if mode == 'local' else ''}{tb}_{prec}_c{cut}_"
     assert np.array_equal(s, z[key + "scores"]), np.nonzero(s != z[key + "scores"])[0][:5]
     assert np.array_equal(g, z[key + "grads"])
     assert np.array_equal(gj, z[key + "guides"])
@@ -43,17 +44,23 @@ def test_reference_fixtures(name, prec, tb, cut):
 
 @pytest.mark.parametrize("prec", [32, 64])
 @pytest.mark.parametrize("pmax", [False, True])
-def test_long_pairs_against_the_oracle(prec, pmax):
+@pytest.mark.parametrize("mode", ["global", "local"])
+def test_long_pairs_against_the_oracle(prec, pmax, mode):
     """Pairs of 1,000-6,000 residues (several recursion levels, multi-round pipelines) mixed
-    with short pairs that run the Pointers path."""
-    rng = np.random.default_rng(2000 + prec + pmax)
+    with short pairs that run the Pointers path; Local: homologous cores inside unrelated
+    flanks (a box well inside the pair), and unrelated pairs."""
+    rng = np.random.default_rng(2000 + prec + pmax + 10 * (mode == "local"))
     mat = rand_matrix(rng, 20, integer=False)
     gaps = np.array([[3.1, 0.7, 2.9, 0.8]])
     sa = rand_seqs(rng, 6, 1000, 6000, AA) + rand_seqs(rng, 10, 1, 300, AA)
     sb = [mutate(rng, s, AA) if k % 3 else rand_seqs(rng, 1, 500, 4000, AA)[0] for k, s in enumerate(sa)]
+    if mode == "local":
+        sb = [rand_seqs(rng, 1, 10, 400, AA)[0] + t + rand_seqs(rng, 1, 10, 400, AA)[0] if k % 3 else t
+              for k, t in enumerate(sb)]
     cut = 256
-    s, g, gj, _ = _run(prec, "hirschberg_pmax" if pmax else "hirschberg", cut, mat, gaps, sa, sb)
-    o = oracle.hirschberg(prec, mat, gaps, oracle.Encoded(encode(AA, sa), encode(AA, sb)), cutoff=cut, pmax=pmax)
+    s, g, gj, _ = _run(prec, "hirschberg_pmax" if pmax else "hirschberg", cut, mat, gaps, sa, sb, mode)
+    o = oracle.hirschberg(prec, mat, gaps, oracle.Encoded(encode(AA, sa), encode(AA, sb)), cutoff=cut, pmax=pmax,
+                          local=mode == "local")
     assert np.array_equal(s, o["scores"]), np.nonzero(s != o["scores"])[0][:5]
     assert np.array_equal(g, o["grads"]), np.nonzero((g != o["grads"]).any(1))[0][:5]
     assert np.array_equal(gj, o["guides"])
@@ -95,5 +102,8 @@ def test_errors():
                           gap_model="linear", grad_mode="hard", traceback="hirschberg")
     with pytest.raises(NotImplementedError):
         lin.score_and_grad()
+    nlocal = nw.SeqPairBatch(sa, sb, neg, mode="local", grad_mode="hard", traceback="hirschberg_pmax")
+    with pytest.raises(ValueError, match="non-negative"):
+        nlocal.score_and_grad()
     with pytest.raises(ValueError):
         lin.hb_cutoff = 0
