@@ -54,7 +54,7 @@ def lib():
                                                       _u16p, _u16p, C.c_double, _dp, _dp, _i32p, C.c_int]
         L.orc_soft_batch.restype = C.c_int
         L.orc_hb_batch.argtypes = [C.c_int] * 4 + [_dp, _dp, _u8p, _i64p, _u8p, _i64p, C.c_int64,
-                                                    _dp, _dp, _i32p, _u8p, C.c_int64, _i64p, C.c_int, _i32p]
+                                                    _dp, _dp, _i32p, _u8p, C.c_int64, _i64p, C.c_int, _i32p, C.c_int]
         L.orc_hb_batch.restype = C.c_int
         L.orc_blocked_sum.argtypes = [_dp, C.c_int64, C.c_int64, _dp, _dp]
         L.orc_blocked_sum.restype = C.c_int
@@ -117,10 +117,10 @@ def hard(prec, gm, am, mat, gaps, enc: Encoded, tracked=False, guides_in=None, b
     return dict(scores=scores, grads=grads, guides=guides, ends=ends, moves=moves, nmoves=nmoves)
 
 
-def hirschberg(prec, mat, gaps, enc: Encoded, cutoff=512, pmax=False, moves_cap=0, local=False):
-    """Affine Hirschberg (untracked, one parameter set).  Global: pairs longer than `cutoff`
-    rows split, shorter ones run the Pointers path.  Local: every pair by the endpoint scans
-    and the global solve of its box.  Returns dict(scores, grads, guides, moves (n, moves_cap)
+def hirschberg(prec, mat, gaps, enc: Encoded, cutoff=512, pmax=False, moves_cap=0, local=False, linear=False):
+    """Hirschberg, affine or linear gaps (untracked, one parameter set).  Pairs longer than
+    `cutoff` rows split, shorter ones run the Pointers path; Local: the endpoint scans give the
+    box that is solved as Global (pmax: the affine prefix-max carry; linear has one sweep).  Returns dict(scores, grads, guides, moves (n, moves_cap)
     path order start to end, nmoves, ends (n, 4): start i, start j, end i, end j)."""
     L = lib()
     mat = np.ascontiguousarray(mat, np.float64).reshape(-1, np.shape(mat)[-1], np.shape(mat)[-1])[:1]
@@ -136,7 +136,7 @@ def hirschberg(prec, mat, gaps, enc: Encoded, cutoff=512, pmax=False, moves_cap=
     rc = L.orc_hb_batch(prec, int(bool(pmax)), int(cutoff), N, _p(mat, _dp), _p(gaps, _dp), _p(enc.a, _u8p),
                         _p(enc.oa, _i64p), _p(enc.b, _u8p), _p(enc.ob, _i64p), n, _p(scores, _dp),
                         _p(grads, _dp), _p(guides, _i32p), _p(moves, _u8p), int(moves_cap), _p(nmoves, _i64p),
-                        int(bool(local)), _p(ends, _i32p))
+                        int(bool(local)), _p(ends, _i32p), int(bool(linear)))
     assert rc == 0
     return dict(scores=scores, grads=grads, guides=guides, moves=moves, nmoves=nmoves, ends=ends)
 

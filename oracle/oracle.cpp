@@ -1048,6 +1048,174 @@ int hb_local_one(const Model& M, const uint8_t* a, int m, const uint8_t* b, int 
     return 0;
 }
 
+// Linear-gap Hirschberg (viterbi_linear_hirschberg, aligner.hpp:5020-5185): no gap state
+// crosses a cut, so the join is the first column of the strictly largest F + R; sweeps
+// (lhb_sweep :4844-4913) keep one row, borders the Global gap chains; base blocks of at most
+// `cutoff` rows are Pointers fills of the box (lhb_base :4917-4997; ties: M, then X, then Y),
+// walked back.  Local: the forward clamped scan for the end (first strictly larger cell,
+// row-major), then the unclamped global-suffix scan over [0, ie) x [0, je) for the start
+// (row ie first with its columns ascending, then rows upward, column je first in each, then
+// columns downward; strict >), then the box solved as Global.
+template <class T>
+struct Lhb {
+    int N; const T* blk; const uint8_t* a; const uint8_t* b; int cutoff;
+    T ge_a, ge_b;
+    std::vector<uint8_t> hops;
+    T sub(int r, int c) const { return blk[size_t(a[r - 1]) * N + b[c - 1]]; }   // 1-based
+    void sweep(bool rev, int i0, int i1, int j0, int j1, std::vector<T>& row) const {
+        const int W = j1 - j0;
+        row.assign(size_t(W) + 1, T(0));
+        for (int cc = 1; cc <= W; ++cc) row[cc] = row[cc - 1] - ge_a;
+        for (int r = 1; r <= i1 - i0; ++r) {
+            const int i = rev ? i1 - r + 1 : i0 + r;
+            T diag = row[0];
+            row[0] = row[0] - ge_b;
+            T left = row[0];
+            for (int cc = 1; cc <= W; ++cc) {
+                const int bcol = rev ? j1 - cc : j0 + cc - 1;   // 0-based
+                T v = diag + blk[size_t(a[i - 1]) * N + b[bcol]];
+                const T u = row[cc] - ge_b, l = left - ge_a;
+                if (v < u) v = u;
+                if (v < l) v = l;
+                diag = row[cc];
+                row[cc] = v;
+                left = v;
+            }
+        }
+    }
+    void base(int i0, int i1, int j0, int j1) {
+        const int H = i1 - i0, W = j1 - j0;
+        const size_t st = size_t(W) + 1;
+        std::vector<uint8_t> D(size_t(H + 1) * st);
+        std::vector<T> prev(st), cur(st);
+        prev[0] = T(0);
+        for (int cc = 1; cc <= W; ++cc) { prev[cc] = prev[cc - 1] - ge_a; D[cc] = 2; }
+        for (int r = 1; r <= H; ++r) {
+            uint8_t* d = D.data() + size_t(r) * st;
+            cur[0] = prev[0] - ge_b; d[0] = 1;
+            T left = cur[0];
+            for (int cc = 1; cc <= W; ++cc) {
+                T v = prev[cc - 1] + sub(i0 + r, j0 + cc);
+                uint8_t k = 0;
+                const T u = prev[cc] - ge_b, l = left - ge_a;
+                if (v < u) { v = u; k = 1; }
+                if (v < l) { v = l; k = 2; }
+                cur[cc] = v; d[cc] = k; left = v;
+            }
+            std::swap(prev, cur);
+        }
+        const size_t first = hops.size();
+        int r = H, cc = W;
+        while (r > 0 || cc > 0) {
+            const uint8_t k = D[size_t(r) * st + size_t(cc)];
+            hops.push_back(k);
+            if (k == 0) { --r; --cc; } else if (k == 1) --r; else --cc;
+        }
+        std::reverse(hops.begin() + std::ptrdiff_t(first), hops.end());
+    }
+    void solve(int i0, int i1, int j0, int j1) {
+        const int H = i1 - i0, W = j1 - j0;
+        if (H <= cutoff) { base(i0, i1, j0, j1); return; }
+        const int p = i0 + H / 2;
+        std::vector<T> F, R;
+        sweep(false, i0, p, j0, j1, F);
+        sweep(true, p, i1, j0, j1, R);
+        T best = ninf<T>();
+        int cstar = 0;
+        for (int cc = 0; cc <= W; ++cc) {
+            const T v = F[cc] + R[W - cc];
+            if (v > best) { best = v; cstar = cc; }
+        }
+        solve(i0, p, j0, j0 + cstar);
+        solve(p, i1, j0 + cstar, j1);
+    }
+};
+
+template <class T>
+int lhb_one(const Model& M, const uint8_t* a, int m, const uint8_t* b, int n, int cutoff, HardOut& o) {
+    if (m <= cutoff) return hard_one<T>(M, a, m, b, n, nullptr, nullptr, false, nullptr, -1, o, 0);
+    std::vector<T> blk(size_t(M.N) * M.N);
+    for (size_t k = 0; k < blk.size(); ++k) blk[k] = static_cast<T>(M.mat[k]);
+    const T ge_a = static_cast<T>(M.gaps[kExtendA]), ge_b = static_cast<T>(M.gaps[kExtendB]);
+    Lhb<T> h{M.N, blk.data(), a, b, cutoff, ge_a, ge_b, {}};
+    int is = 0, js = 0, ie = m, je = n;
+    bool empty = false;
+    if (M.am == 1) {
+        std::vector<T> row(size_t(n) + 1, T(0));
+        T best = T(0); ie = 0; je = 0;
+        for (int i = 1; i <= m; ++i) {
+            T diag = row[0];
+            for (int j = 1; j <= n; ++j) {
+                T v = diag + blk[size_t(a[i - 1]) * M.N + b[j - 1]];
+                const T u = row[j] - ge_b, l = row[j - 1] - ge_a;
+                if (v < u) v = u;
+                if (v < l) v = l;
+                v = mx<T>(v, T(0));
+                diag = row[j];
+                row[j] = v;
+                if (v > best) { best = v; ie = i; je = j; }
+            }
+        }
+        if (!(best > T(0))) { empty = true; ie = 0; je = 0; }
+        else {
+            std::vector<T> g(size_t(je) + 1);
+            g[je] = T(0);
+            for (int q = je - 1; q >= 0; --q) g[q] = g[q + 1] - ge_a;
+            T sbest = g[0]; is = ie; js = 0;
+            for (int q = 0; q <= je; ++q) if (g[q] > sbest) { sbest = g[q]; js = q; }
+            for (int pi = ie - 1; pi >= 0; --pi) {
+                T diag = g[je];
+                g[je] = g[je] - ge_b;
+                if (g[je] > sbest) { sbest = g[je]; is = pi; js = je; }
+                for (int q = je - 1; q >= 0; --q) {
+                    T v = diag + blk[size_t(a[pi]) * M.N + b[q]];
+                    const T u = g[q] - ge_b, l = g[q + 1] - ge_a;
+                    if (v < u) v = u;
+                    if (v < l) v = l;
+                    diag = g[q];
+                    g[q] = v;
+                    if (v > sbest) { sbest = v; is = pi; js = q; }
+                }
+            }
+        }
+    }
+    if (!empty) h.solve(is, ie, js, je);
+    // replay: score in T, counts, guide (guide_j_affine_hb :5233-5249, gap-model free)
+    T s = T(0);
+    int i = is, j = js;
+    std::vector<int32_t> gj(size_t(m) + 1, -1);
+    gj[0] = 0;
+    gj[is] = js;
+    for (uint8_t op : h.hops) {
+        if (op == 0) {
+            ++i; ++j;
+            s += blk[size_t(a[i - 1]) * M.N + b[j - 1]];
+            if (o.grad) o.grad[size_t(a[i - 1]) * M.N + b[j - 1]] += 1.0;
+            gj[i] = j;
+        } else if (op == 1) {
+            ++i;
+            s -= ge_b;
+            if (o.grad) o.grad[size_t(M.N) * M.N + kExtendB] -= 1.0;
+            gj[i] = j;
+        } else {
+            s -= ge_a;
+            if (o.grad) o.grad[size_t(M.N) * M.N + kExtendA] -= 1.0;
+            ++j;
+        }
+    }
+    gj[m] = n;
+    fill_guide_gaps(gj);
+    if (o.guide) std::memcpy(o.guide, gj.data(), sizeof(int32_t) * (m + 1));
+    if (o.moves) {
+        const int64_t k = std::min<int64_t>(int64_t(h.hops.size()), o.moves_cap);
+        for (int64_t q = 0; q < k; ++q) o.moves[q] = h.hops[q];
+    }
+    o.nmoves = int64_t(h.hops.size());
+    o.score = static_cast<double>(s);
+    o.end_i = ie; o.end_j = je; o.start_i = is; o.start_j = js;
+    return 0;
+}
+
 template <class T>
 int hb_one(const Model& M, const uint8_t* a, int m, const uint8_t* b, int n, int cutoff, bool pmax,
            HardOut& o) {
@@ -1179,8 +1347,8 @@ int orc_soft_batch(int gm, int am, int N, int K, const double* mat, const double
 int orc_hb_batch(int prec, int pmax, int cutoff, int N, const double* mat, const double* gaps,
                  const uint8_t* a, const int64_t* oa, const uint8_t* b, const int64_t* ob, int64_t n_pairs,
                  double* scores, double* grads, int32_t* guides, uint8_t* moves, int64_t moves_cap,
-                 int64_t* nmoves, int local, int32_t* ends) {
-    Model M{1, local ? 1 : 0, N, 1, mat, gaps};
+                 int64_t* nmoves, int local, int32_t* ends, int linear) {
+    Model M{linear ? 0 : 1, local ? 1 : 0, N, 1, mat, gaps};
     const size_t gs = size_t(N) * N + 4;
     for (int64_t p = 0; p < n_pairs; ++p) {
         const int m = int(oa[p + 1] - oa[p]), n = int(ob[p + 1] - ob[p]);
@@ -1190,7 +1358,10 @@ int orc_hb_batch(int prec, int pmax, int cutoff, int N, const double* mat, const
         o.guide = guides ? guides + oa[p] + p : nullptr;
         o.moves = moves ? moves + moves_cap * p : nullptr;
         o.moves_cap = moves_cap;
-        if (local) {
+        if (linear) {
+            if (prec == 32) lhb_one<float>(M, a + oa[p], m, b + ob[p], n, cutoff, o);
+            else            lhb_one<double>(M, a + oa[p], m, b + ob[p], n, cutoff, o);
+        } else if (local) {
             if (prec == 32) hb_local_one<float>(M, a + oa[p], m, b + ob[p], n, cutoff, pmax != 0, o);
             else            hb_local_one<double>(M, a + oa[p], m, b + ob[p], n, cutoff, pmax != 0, o);
         } else {

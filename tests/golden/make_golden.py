@@ -167,8 +167,8 @@ def hb_fixtures():
         for prec in (32, 64):
             for tb in ("hirschberg", "hirschberg_pmax"):
                 for cut in (8, 64):
-                    for am, tag in ((0, ""), (1, "L_")):   # global, local
-                        r = oracle.ref_run(prec, 1, am, 1, AA, mat, gaps, sa, sb, traceback=tb, hb_cutoff=cut)
+                    for gm, am, tag in ((1, 0, ""), (1, 1, "L_"), (0, 0, "lin_"), (0, 1, "linL_")):
+                        r = oracle.ref_run(prec, gm, am, 1, AA, mat, gaps, sa, sb, traceback=tb, hb_cutoff=cut)
                         key = f"{name}_{tag}{tb}_{prec}_c{cut}_"
                         out[key + "scores"] = r["scores"]
                         out[key + "grads"] = r["grads"]

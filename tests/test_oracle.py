@@ -106,7 +106,7 @@ def test_live_reference_random(gm, am):
 
 
 def test_hirschberg_fixtures():
-    """The Hirschberg restatement (exact and prefix-max carry; Global and Local) against the
+    """The Hirschberg restatement (affine exact and prefix-max carry, linear; Global and Local) against the
     reference's own engine with traceback hirschberg / hirschberg_pmax
     (tests/golden/hirschberg.npz)."""
     z = np.load(os.path.join(GOLD, "hirschberg.npz"))
@@ -116,10 +116,11 @@ def test_hirschberg_fixtures():
         for prec in (32, 64):
             for tb in ("hirschberg", "hirschberg_pmax"):
                 for cut in (8, 64):
-                    for local, tag in ((False, ""), (True, "L_")):
+                    for linear, local, tag in ((False, False, ""), (False, True, "L_"), (True, False, "lin_"),
+                                               (True, True, "linL_")):
                         key = f"{name}_{tag}{tb}_{prec}_c{cut}_"
                         o = oracle.hirschberg(prec, z[f"{name}_mat"], z[f"{name}_gaps"], enc, cutoff=cut,
-                                              pmax=tb.endswith("pmax"), local=local)
+                                              pmax=tb.endswith("pmax"), local=local, linear=linear)
                         np.testing.assert_array_equal(o["scores"], z[key + "scores"])
                         np.testing.assert_array_equal(o["grads"], z[key + "grads"])
                         np.testing.assert_array_equal(o["guides"], z[key + "guides"])
