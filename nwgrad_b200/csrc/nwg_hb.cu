@@ -521,12 +521,12 @@ __global__ void hb_replay_kernel(const HbRun P, const BaseJob* __restrict__ jobs
                 if (gj) gj[i] = j;
             } else if (op == 1) {
                 ++i;
-                if (prev != 1) { s -= go_b; if (g) g[NN + 2] -= 1.0; }
+                if (!P.linear && prev != 1) { s -= go_b; if (g) g[NN + 2] -= 1.0; }
                 s -= ge_b;
                 if (g) g[NN + 3] -= 1.0;
                 if (gj) gj[i] = j;
             } else {
-                if (prev != 2) { s -= go_a; if (g) g[NN + 0] -= 1.0; }
+                if (!P.linear && prev != 2) { s -= go_a; if (g) g[NN + 0] -= 1.0; }
                 s -= ge_a;
                 if (g) g[NN + 1] -= 1.0;
                 ++j;
@@ -552,6 +552,253 @@ __global__ void hb_replay_kernel(const HbRun P, const BaseJob* __restrict__ jobs
             for (int q = lo + 1; q < hi; ++q) gj[q] = gj[lo] + (gj[hi] - gj[lo]) * (q - lo) / (hi - lo);
             lo = hi;
         }
+    }
+}
+
+// ── linear gaps ───────────────────────────────────────────────────────────────
+// viterbi_linear_hirschberg (aligner.hpp:5020-5185): one state per cell,
+// v = diag + s; u = up - ge_b; l = left - ge_a; v < u -> u; v < l -> l (ties: M, then X, then
+// Y).  lhb_kernel, one warp per block (lanes own R rows of a 32R-row stripe, skewed by one
+// column; the row above by shuffle, lane 0's from a per-warp row in global memory):
+//   MODE 0 -- a half-sweep (lhb_sweep :4844-4913), Global borders, the last row out;
+//   MODE 1 -- Local's forward clamped scan: the first strictly larger cell, row-major;
+//   MODE 2 -- Local's global-suffix scan (mirrored): row 0 seeds the best in its own order
+//             (columns from the last down, strict >), then rows in order, column 0 first.
+struct LhbJob {
+    int64_t a_base, b_base;          // row t >= 1 reads a[a_base + a_step (t - 1)]; column c >= 1 b[b_base + b_step (c - 1)]
+    int a_step, b_step;
+    int H, W;
+    int64_t out;                     // MODE 0: T offset of the last row (W + 1)
+};
+
+template <class T, int R, int MODE>
+__global__ void __launch_bounds__(128) lhb_kernel(const uint8_t* __restrict__ a, const uint8_t* __restrict__ b,
+                                                  const T* __restrict__ mat, int N, T ga, T gb,
+                                                  const LhbJob* __restrict__ jobs, int n_jobs, T* rows,
+                                                  int64_t row_stride, T* __restrict__ out,
+                                                  int32_t* __restrict__ res) {
+    extern __shared__ __align__(16) unsigned char hb_smem[];
+    T* smat = reinterpret_cast<T*>(hb_smem);
+    for (int k = threadIdx.x; k < N * N; k += blockDim.x) smat[k] = mat[k];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    const int64_t wg = int64_t(blockIdx.x) * wpb + (threadIdx.x >> 5);
+    const int64_t nwarps = int64_t(gridDim.x) * wpb;
+    T* bnd = rows + wg * row_stride;
+    constexpr bool LOC = MODE == 1;
+    for (int64_t jb = wg; jb < n_jobs; jb += nwarps) {
+        const LhbJob J = jobs[jb];
+        const int H = J.H, W = J.W;
+        T bv = T(0); int bi = 0, bj = 0;
+        if constexpr (MODE == 2) {
+            // row 0 (the end cell's row) seeds the best, its columns visited from W down: the
+            // chain 0, -ga, -2ga, ... never rises (ga >= 0: Hirschberg needs non-negative
+            // penalties), so the first largest is column 0, or column W when ga is 0
+            bv = T(0); bi = 0; bj = (ga > T(0)) ? 0 : W;
+        }
+        if (MODE == 0 && H == 0) {   // no rows: row 0 is the last
+            if (lane == 0) { T v = T(0); out[J.out] = v; for (int c = 1; c <= W; ++c) { v = v - ga; out[J.out + c] = v; } }
+        }
+        if (H > 0) {
+            const int nst = (H + 32 * R - 1) / (32 * R);
+            const int lst = (H - 1) / (32 * R), llane = ((H - 1) % (32 * R)) / R, lrow = (H - 1) % R;
+            for (int s = 0; s < nst; ++s) {
+                const int i0 = s * 32 * R + lane * R + 1;
+                int code[R];
+                bool valid[R];
+                T cur[R];
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const int i = i0 + r;
+                    valid[r] = i <= H;
+                    code[r] = valid[r] ? int(a[J.a_base + int64_t(J.a_step) * (i - 1)]) * N : 0;
+                    cur[r] = T(0);
+                }
+                T dg = T(0), up = T(0);       // row above at column c - 1, c
+                T r0 = T(0);                   // row 0 at column c - 1 (lane 0, stripe 0)
+                T nu = T(0);
+                if (lane == 0 && s > 0) nu = bnd[0];
+                const int S = W + 32;
+                for (int t = 0; t < S; ++t) {
+                    const int c = t - lane;
+                    if (lane == 0 && c <= W) {
+                        if (s == 0) {
+                            if (c == 0 || LOC) up = T(0);
+                            else up = r0 - ga;
+                            r0 = up;
+                        } else {
+                            up = nu;
+                            if (c < W) nu = bnd[c + 1];
+                        }
+                    }
+                    if (c >= 0 && c <= W) {
+                        T q = up, pd = dg;
+                        const int bc = c >= 1 ? int(b[J.b_base + int64_t(J.b_step) * (c - 1)]) : 0;
+#pragma unroll
+                        for (int r = 0; r < R; ++r) {
+                            T v;
+                            if (c == 0) {
+                                v = LOC ? T(0) : q - gb;
+                            } else {
+                                v = pd + smat[code[r] + bc];
+                                const T u = q - gb, l = cur[r] - ga;
+                                if (v < u) v = u;
+                                if (v < l) v = l;
+                                if constexpr (LOC) v = (v < T(0)) ? T(0) : v;
+                            }
+                            if constexpr (MODE != 0) {
+                                if (valid[r] && (MODE == 2 || c >= 1)) {
+                                    const int i = i0 + r;
+                                    if (v > bv || (v == bv && (i < bi || (i == bi && c < bj)))) { bv = v; bi = i; bj = c; }
+                                }
+                            }
+                            if constexpr (MODE == 0) {
+                                if (s == lst && lane == llane && r == lrow) out[J.out + c] = v;
+                            }
+                            pd = cur[r];
+                            cur[r] = v;
+                            q = v;
+                        }
+                        dg = up;
+                    }
+                    const T sv = __shfl_up_sync(0xffffffffu, cur[R - 1], 1);
+                    if (lane > 0) up = sv;
+                    if (lane == 31 && c >= 0 && c <= W && s + 1 < nst) bnd[c] = cur[R - 1];
+                }
+                __syncwarp();
+            }
+        }
+        if constexpr (MODE != 0) {
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                const T ov = __shfl_xor_sync(0xffffffffu, bv, off);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+                const int oj = __shfl_xor_sync(0xffffffffu, bj, off);
+                if (ov > bv || (ov == bv && (oi < bi || (oi == bi && oj < bj)))) { bv = ov; bi = oi; bj = oj; }
+            }
+            if (lane == 0) { res[3 * jb] = bv > T(0) ? 1 : 0; res[3 * jb + 1] = bi; res[3 * jb + 2] = bj; }
+        }
+        __syncwarp();
+    }
+}
+
+// The join of a linear split (lhb_solve :4999-5017): the first column of the strictly largest
+// F[c] + R[W - c].  One thread block per split block.
+template <class T>
+__global__ void lhb_join_kernel(const LhbJob* __restrict__ jobs, int n_blocks, const T* __restrict__ out,
+                                int32_t* __restrict__ res) {
+    __shared__ T sv[256];
+    __shared__ int sc[256];
+    for (int q = blockIdx.x; q < n_blocks; q += gridDim.x) {
+        const LhbJob& F = jobs[2 * q];
+        const LhbJob& Rv = jobs[2 * q + 1];
+        const int W = F.W;
+        T best = ninf<T>(); int cb = 0;
+        for (int c = threadIdx.x; c <= W; c += blockDim.x) {
+            const T v = out[F.out + c] + out[Rv.out + (W - c)];
+            if (v > best) { best = v; cb = c; }
+        }
+        sv[threadIdx.x] = best; sc[threadIdx.x] = cb;
+        __syncthreads();
+        for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+            if (threadIdx.x < h) {
+                const T ov = sv[threadIdx.x + h]; const int oc = sc[threadIdx.x + h];
+                if (ov > sv[threadIdx.x] || (ov == sv[threadIdx.x] && oc < sc[threadIdx.x])) {
+                    sv[threadIdx.x] = ov; sc[threadIdx.x] = oc;
+                }
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) res[q] = sc[0];
+        __syncthreads();
+    }
+}
+
+// Base block of a linear split (lhb_base :4917-4997): the Pointers fill of the box with the
+// Global borders into a row-major code table, walked back from its corner by lane 0.
+template <class T, int R>
+__global__ void __launch_bounds__(128) lhb_base_kernel(const uint8_t* __restrict__ a, const uint8_t* __restrict__ b,
+                                                       const T* __restrict__ mat, int N, T ga, T gb,
+                                                       const BaseJob* __restrict__ jobs, int n_jobs,
+                                                       uint8_t* __restrict__ codes, T* __restrict__ bnds,
+                                                       uint8_t* __restrict__ moves, int32_t* __restrict__ nmoves) {
+    extern __shared__ __align__(16) unsigned char hb_smem[];
+    T* smat = reinterpret_cast<T*>(hb_smem);
+    for (int k = threadIdx.x; k < N * N; k += blockDim.x) smat[k] = mat[k];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    for (int64_t jb = int64_t(blockIdx.x) * wpb + (threadIdx.x >> 5); jb < n_jobs; jb += int64_t(gridDim.x) * wpb) {
+        const BaseJob J = jobs[jb];
+        const int H = J.H, W = J.W;
+        const int64_t st = int64_t(W) + 1;
+        uint8_t* D = codes + J.codes;
+        T* bnd = bnds + J.bnd;
+        if (lane == 0) { D[0] = 3; for (int c = 1; c <= W; ++c) D[c] = 2; }
+        if (H > 0) {
+            const int nst = (H + 32 * R - 1) / (32 * R);
+            for (int s = 0; s < nst; ++s) {
+                const int i0 = s * 32 * R + lane * R + 1;
+                int code[R];
+                T cur[R];
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const int i = i0 + r;
+                    code[r] = i <= H ? int(a[J.a_base + i - 1]) * N : 0;
+                    cur[r] = T(0);
+                }
+                T dg = T(0), up = T(0), r0 = T(0), nu = T(0);
+                if (lane == 0 && s > 0) nu = bnd[0];
+                const int S = W + 32;
+                for (int t = 0; t < S; ++t) {
+                    const int c = t - lane;
+                    if (lane == 0 && c <= W) {
+                        if (s == 0) { up = c == 0 ? T(0) : r0 - ga; r0 = up; }
+                        else { up = nu; if (c < W) nu = bnd[c + 1]; }
+                    }
+                    if (c >= 0 && c <= W) {
+                        T q = up, pd = dg;
+                        const int bc = c >= 1 ? int(b[J.b_base + c - 1]) : 0;
+#pragma unroll
+                        for (int r = 0; r < R; ++r) {
+                            const int i = i0 + r;
+                            T v;
+                            uint8_t k;
+                            if (c == 0) { v = q - gb; k = 1; }
+                            else {
+                                v = pd + smat[code[r] + bc];
+                                k = 0;
+                                const T u = q - gb, l = cur[r] - ga;
+                                if (v < u) { v = u; k = 1; }
+                                if (v < l) { v = l; k = 2; }
+                            }
+                            if (i <= H) D[int64_t(i) * st + c] = k;
+                            pd = cur[r];
+                            cur[r] = v;
+                            q = v;
+                        }
+                        dg = up;
+                    }
+                    const T sv = __shfl_up_sync(0xffffffffu, cur[R - 1], 1);
+                    if (lane > 0) up = sv;
+                    if (lane == 31 && c >= 0 && c <= W && s + 1 < nst) bnd[c] = cur[R - 1];
+                }
+                __syncwarp();
+            }
+        }
+        __syncwarp();
+        if (lane == 0) {
+            uint8_t* mv = moves + J.moves;
+            int r = H, c = W, k = 0;
+            while (r > 0 || c > 0) {
+                const uint8_t op = D[int64_t(r) * st + c];
+                mv[k++] = op;
+                if (op == 0) { --r; --c; } else if (op == 1) --r; else --c;
+            }
+            nmoves[jb] = k;
+        }
+        __syncwarp();
     }
 }
 
@@ -765,9 +1012,178 @@ int64_t hb_run_t(const HbRun& P, cudaStream_t st, int sms) {
     return launches;
 }
 
+// Linear gaps: the same breadth-first recursion with lhb_kernel sweeps, lhb_join_kernel and
+// lhb_base_kernel; Local first finds each pair's box with the two scans.
+template <class T>
+int64_t lhb_run_t(const HbRun& P, cudaStream_t st, int sms) {
+    const int n = int(P.n_pairs);
+    if (n == 0) return 0;
+    int64_t launches = 0;
+    constexpr int R = 4;
+    const T ga = static_cast<T>(P.ge_a), gb = static_cast<T>(P.ge_b);
+    const T* mat = static_cast<const T*>(P.mat);
+    const size_t mat_bytes = size_t((P.N * P.N + 3) & ~3) * sizeof(T);
+    Tmp djobs(st), dout(st), drows(st), dres(st), dboxes(st);
+    const int wpb = 4;
+    // one launch of lhb_kernel<MODE> over jobs (MODE 0: rows out; else results back to the host)
+    auto launch = [&](int mode, const std::vector<LhbJob>& jobs, T* o, std::vector<int32_t>* res) {
+        if (jobs.empty()) return;
+        int maxw = 1;
+        for (const LhbJob& x : jobs) maxw = std::max(maxw, x.W);
+        const int grid = int(std::min<int64_t>((int64_t(jobs.size()) + wpb - 1) / wpb, int64_t(sms) * 4));
+        const int64_t stride = int64_t(maxw) + 1;
+        LhbJob* dj = static_cast<LhbJob*>(djobs.get(jobs.size() * sizeof(LhbJob)));
+        HB_CUDA(cudaMemcpyAsync(dj, jobs.data(), jobs.size() * sizeof(LhbJob), cudaMemcpyHostToDevice, st));
+        T* rw = static_cast<T*>(drows.get(size_t(grid) * wpb * stride * sizeof(T)));
+        int32_t* rs = res ? static_cast<int32_t*>(dres.get(jobs.size() * 3 * sizeof(int32_t))) : nullptr;
+        auto fn = mode == 0 ? lhb_kernel<T, R, 0> : mode == 1 ? lhb_kernel<T, R, 1> : lhb_kernel<T, R, 2>;
+        HB_CUDA(allow_smem(reinterpret_cast<const void*>(fn), mat_bytes));
+        fn<<<grid, 32 * wpb, mat_bytes, st>>>(P.a, P.b, mat, P.N, ga, gb, dj, int(jobs.size()), rw, stride, o, rs);
+        HB_CUDA(cudaGetLastError());
+        launches++;
+        if (res) {
+            res->assign(jobs.size() * 3, 0);
+            HB_CUDA(cudaMemcpyAsync(res->data(), rs, res->size() * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+            HB_CUDA(cudaStreamSynchronize(st));
+        }
+    };
+    std::vector<Blk> cur;
+    std::vector<int32_t> boxes;
+    if (!P.local) {
+        for (int k = 0; k < n; ++k) {
+            const int p = P.h_pairs[k];
+            cur.push_back(Blk{k, 0, int(P.h_oa[p + 1] - P.h_oa[p]), 0, int(P.h_ob[p + 1] - P.h_ob[p]), 0, 0});
+        }
+    } else {
+        boxes.assign(size_t(n) * 4, 0);
+        std::vector<LhbJob> jf;
+        for (int k = 0; k < n; ++k) {
+            const int p = P.h_pairs[k];
+            LhbJob J{};
+            J.a_base = P.h_oa[p]; J.a_step = 1; J.b_base = P.h_ob[p]; J.b_step = 1;
+            J.H = int(P.h_oa[p + 1] - P.h_oa[p]); J.W = int(P.h_ob[p + 1] - P.h_ob[p]);
+            jf.push_back(J);
+        }
+        std::vector<int32_t> fr, rr;
+        launch(1, jf, nullptr, &fr);
+        std::vector<LhbJob> jr;
+        std::vector<int> rk;
+        for (int k = 0; k < n; ++k) {
+            if (!fr[3 * k] || fr[3 * k + 1] <= 0 || fr[3 * k + 2] <= 0) continue;   // empty alignment
+            const int p = P.h_pairs[k];
+            const int ie = fr[3 * k + 1], je = fr[3 * k + 2];
+            LhbJob J{};
+            J.a_base = P.h_oa[p] + ie - 1; J.a_step = -1; J.b_base = P.h_ob[p] + je - 1; J.b_step = -1;
+            J.H = ie; J.W = je;
+            jr.push_back(J);
+            rk.push_back(k);
+        }
+        launch(2, jr, nullptr, &rr);
+        for (size_t q = 0; q < rk.size(); ++q) {
+            const int k = rk[q];
+            const int ie = fr[3 * k + 1], je = fr[3 * k + 2];
+            const int is = ie - rr[3 * q + 1], js = je - rr[3 * q + 2];
+            boxes[4 * size_t(k)] = is; boxes[4 * size_t(k) + 1] = js;
+            boxes[4 * size_t(k) + 2] = ie; boxes[4 * size_t(k) + 3] = je;
+            cur.push_back(Blk{k, is, ie, js, je, 0, 0});
+        }
+    }
+    while (true) {
+        std::vector<int> split;
+        for (int q = 0; q < int(cur.size()); ++q)
+            if (cur[q].i1 - cur[q].i0 > P.cutoff) split.push_back(q);
+        if (split.empty()) break;
+        std::vector<LhbJob> jobs(2 * split.size());
+        int64_t out_off = 0;
+        for (size_t s = 0; s < split.size(); ++s) {
+            const Blk& B = cur[split[s]];
+            const int p = P.h_pairs[B.k];
+            const int mid = B.i0 + (B.i1 - B.i0) / 2, W = B.j1 - B.j0;
+            LhbJob& F = jobs[2 * s];
+            F.a_base = P.h_oa[p] + B.i0; F.a_step = 1; F.b_base = P.h_ob[p] + B.j0; F.b_step = 1;
+            F.H = mid - B.i0; F.W = W;
+            LhbJob& Rv = jobs[2 * s + 1];
+            Rv.a_base = P.h_oa[p] + B.i1 - 1; Rv.a_step = -1; Rv.b_base = P.h_ob[p] + B.j1 - 1; Rv.b_step = -1;
+            Rv.H = B.i1 - mid; Rv.W = W;
+            F.out = out_off; out_off += int64_t(W) + 1;
+            Rv.out = out_off; out_off += int64_t(W) + 1;
+        }
+        T* o = static_cast<T*>(dout.get(size_t(out_off) * sizeof(T)));
+        launch(0, jobs, o, nullptr);
+        // the join reads the jobs launch() left on the device
+        int32_t* res = static_cast<int32_t*>(dres.get(split.size() * sizeof(int32_t)));
+        const int jgrid = int(std::min<int64_t>(int64_t(split.size()), int64_t(sms) * 8));
+        lhb_join_kernel<T><<<jgrid, 256, 0, st>>>(static_cast<const LhbJob*>(djobs.p), int(split.size()), o, res);
+        HB_CUDA(cudaGetLastError());
+        launches++;
+        std::vector<int32_t> h(split.size());
+        HB_CUDA(cudaMemcpyAsync(h.data(), res, h.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        HB_CUDA(cudaStreamSynchronize(st));
+        std::vector<Blk> next;
+        next.reserve(cur.size() + split.size());
+        size_t si = 0;
+        for (int q = 0; q < int(cur.size()); ++q) {
+            const Blk& B = cur[q];
+            if (si < split.size() && split[si] == q) {
+                const int mid = B.i0 + (B.i1 - B.i0) / 2;
+                const int js = B.j0 + h[si];
+                next.push_back(Blk{B.k, B.i0, mid, B.j0, js, 0, 0});
+                next.push_back(Blk{B.k, mid, B.i1, js, B.j1, 0, 0});
+                ++si;
+            } else {
+                next.push_back(B);
+            }
+        }
+        cur.swap(next);
+    }
+    std::vector<BaseJob> bj(cur.size());
+    std::vector<int64_t> first(size_t(n) + 1, 0);
+    int64_t code_off = 0, bnd_off = 0, mv_off = 0;
+    for (size_t q = 0; q < cur.size(); ++q) {
+        const Blk& B = cur[q];
+        const int p = P.h_pairs[B.k];
+        BaseJob& J = bj[q];
+        J.a_base = P.h_oa[p] + B.i0; J.b_base = P.h_ob[p] + B.j0;
+        J.H = B.i1 - B.i0; J.W = B.j1 - B.j0; J.in_x = 0; J.out_x = 0;
+        J.codes = code_off; code_off += ((int64_t(J.H) + 1) * (int64_t(J.W) + 1) + 15) & ~int64_t(15);
+        J.bnd = bnd_off; bnd_off += int64_t(J.W) + 1;
+        J.moves = mv_off; mv_off += int64_t(J.H) + J.W + 1;
+        first[size_t(B.k) + 1] = int64_t(q) + 1;
+    }
+    for (int k = 0; k < n; ++k) first[size_t(k) + 1] = std::max(first[size_t(k) + 1], first[size_t(k)]);
+    Tmp dbj(st), dcodes(st), dbnd(st), dmv(st), dnm(st), dfirst(st);
+    BaseJob* dB = static_cast<BaseJob*>(dbj.get(bj.size() * sizeof(BaseJob)));
+    if (!bj.empty()) HB_CUDA(cudaMemcpyAsync(dB, bj.data(), bj.size() * sizeof(BaseJob), cudaMemcpyHostToDevice, st));
+    uint8_t* cd = static_cast<uint8_t*>(dcodes.get(size_t(code_off)));
+    T* bd = static_cast<T*>(dbnd.get(size_t(bnd_off) * sizeof(T)));
+    uint8_t* mvd = static_cast<uint8_t*>(dmv.get(size_t(mv_off)));
+    int32_t* nm = static_cast<int32_t*>(dnm.get(bj.size() * sizeof(int32_t)));
+    int64_t* fd = static_cast<int64_t*>(dfirst.get(first.size() * sizeof(int64_t)));
+    HB_CUDA(cudaMemcpyAsync(fd, first.data(), first.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+    const int grid = int(std::min<int64_t>((int64_t(bj.size()) + wpb - 1) / wpb, int64_t(sms) * 8));
+    if (grid > 0) {
+        HB_CUDA(allow_smem(reinterpret_cast<const void*>(lhb_base_kernel<T, R>), mat_bytes));
+        lhb_base_kernel<T, R><<<grid, 32 * wpb, mat_bytes, st>>>(P.a, P.b, mat, P.N, ga, gb, dB, int(bj.size()), cd, bd,
+                                                                 mvd, nm);
+        HB_CUDA(cudaGetLastError());
+        launches++;
+    }
+    int32_t* bx = nullptr;
+    if (P.local) {
+        bx = static_cast<int32_t*>(dboxes.get(boxes.size() * sizeof(int32_t)));
+        HB_CUDA(cudaMemcpyAsync(bx, boxes.data(), boxes.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    }
+    hb_replay_kernel<T><<<(n + 127) / 128, 128, 0, st>>>(P, dB, fd, mvd, nm, n, bx);
+    HB_CUDA(cudaGetLastError());
+    launches++;
+    HB_CUDA(cudaStreamSynchronize(st));
+    return launches;
+}
+
 }  // namespace
 
 int64_t hb_run(const HbRun& P, int elem_bytes, cudaStream_t st, int sms) {
+    if (P.linear) return elem_bytes == 4 ? lhb_run_t<float>(P, st, sms) : lhb_run_t<double>(P, st, sms);
     return elem_bytes == 4 ? hb_run_t<float>(P, st, sms) : hb_run_t<double>(P, st, sms);
 }
 

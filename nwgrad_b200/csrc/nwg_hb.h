@@ -5,7 +5,8 @@
 
 namespace nwg {
 
-// One Hirschberg run over a set of pairs (affine Global or Local, untracked, one parameter set).
+// One Hirschberg run over a set of pairs (affine or linear, Global or Local, untracked, one
+// parameter set).
 struct HbRun {
     // device
     const uint8_t* a; const uint8_t* b;        // the store's codes
@@ -24,6 +25,7 @@ struct HbRun {
     int cutoff;                                // rows at which blocks stop splitting (>= 1)
     int pmax;                                  // the closed-form prefix-max horizontal carry
     int local;                                 // Local: endpoint scans, then the box's global solve
+    int linear;                                // linear gaps (one state; pmax does not apply)
 };
 
 // Runs P on stream st (synchronising it); returns the number of kernel launches.  Throws

@@ -1,5 +1,5 @@
-"""Hirschberg re-alignment on the GPU (traceback "hirschberg" / "hirschberg_pmax", affine
-Global and Local): scores, gradients and guides bit for bit against the reference's own engine
+"""Hirschberg re-alignment on the GPU (traceback "hirschberg" / "hirschberg_pmax"; affine and
+linear gaps, Global and Local): scores, gradients and guides bit for bit against the reference's own engine
 (tests/golden/hirschberg.npz) and against the oracle's restatement on longer pairs."""
 import os
 
@@ -16,9 +16,10 @@ import nwgrad_b200 as nw  # noqa: E402
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
 
 
-def _run(prec, tb, cut, mat, gaps, sa, sb, mode="global"):
+def _run(prec, tb, cut, mat, gaps, sa, sb, mode="global", gap_model="affine"):
     cls = nw.SeqPairBatch if prec == 32 else nw.SeqPairBatchDouble
-    b = cls(sa, sb, nw.AlignParams.from_arrays(mat, gaps, alphabet=AA), grad_mode="hard", traceback=tb, mode=mode)
+    b = cls(sa, sb, nw.AlignParams.from_arrays(mat, gaps, alphabet=AA), grad_mode="hard", traceback=tb, mode=mode,
+            gap_model=gap_model)
     b.hb_cutoff = cut
     tot = b.score_and_grad()
     gm, gg = b.grads()
@@ -31,11 +32,13 @@ def _run(prec, tb, cut, mat, gaps, sa, sb, mode="global"):
 @pytest.mark.parametrize("tb", ["hirschberg", "hirschberg_pmax"])
 @pytest.mark.parametrize("cut", [8, 64])
 @pytest.mark.parametrize("mode", ["global", "local"])
-def test_reference_fixtures(name, prec, tb, cut, mode):
+@pytest.mark.parametrize("gap_model", ["affine", "linear"])
+def test_reference_fixtures(name, prec, tb, cut, mode, gap_model):
     z = np.load(os.path.join(GOLD, "hirschberg.npz"))
     sa, sb = [str(s) for s in z[f"{name}_sa"]], [str(s) for s in z[f"{name}_sb"]]
-    s, g, gj, tot = _run(prec, tb, cut, z[f"{name}_mat"], z[f"{name}_gaps"], sa, sb, mode)
-    key = f"{name}_{'L_' if mode == 'local' else ''}{tb}_{prec}_c{cut}_"
+    s, g, gj, tot = _run(prec, tb, cut, z[f"{name}_mat"], z[f"{name}_gaps"], sa, sb, mode, gap_model)
+    tag = ("lin" if gap_model == "linear" else "") + ("L" if mode == "local" else "")
+    key = f"{name}_{tag + '_' if tag else ''}{tb}_{prec}_c{cut}_"
     assert np.array_equal(s, z[key + "scores"]), np.nonzero(s != z[key + "scores"])[0][:5]
     assert np.array_equal(g, z[key + "grads"])
     assert np.array_equal(gj, z[key + "guides"])
@@ -45,7 +48,8 @@ def test_reference_fixtures(name, prec, tb, cut, mode):
 @pytest.mark.parametrize("prec", [32, 64])
 @pytest.mark.parametrize("pmax", [False, True])
 @pytest.mark.parametrize("mode", ["global", "local"])
-def test_long_pairs_against_the_oracle(prec, pmax, mode):
+@pytest.mark.parametrize("gap_model", ["affine", "linear"])
+def test_long_pairs_against_the_oracle(prec, pmax, mode, gap_model):
     """Pairs of 1,000-6,000 residues (several recursion levels, multi-round pipelines) mixed
     with short pairs that run the Pointers path; Local: homologous cores inside unrelated
     flanks (a box well inside the pair), and unrelated pairs."""
@@ -58,9 +62,9 @@ def test_long_pairs_against_the_oracle(prec, pmax, mode):
         sb = [rand_seqs(rng, 1, 10, 400, AA)[0] + t + rand_seqs(rng, 1, 10, 400, AA)[0] if k % 3 else t
               for k, t in enumerate(sb)]
     cut = 256
-    s, g, gj, _ = _run(prec, "hirschberg_pmax" if pmax else "hirschberg", cut, mat, gaps, sa, sb, mode)
+    s, g, gj, _ = _run(prec, "hirschberg_pmax" if pmax else "hirschberg", cut, mat, gaps, sa, sb, mode, gap_model)
     o = oracle.hirschberg(prec, mat, gaps, oracle.Encoded(encode(AA, sa), encode(AA, sb)), cutoff=cut, pmax=pmax,
-                          local=mode == "local")
+                          local=mode == "local", linear=gap_model == "linear")
     assert np.array_equal(s, o["scores"]), np.nonzero(s != o["scores"])[0][:5]
     assert np.array_equal(g, o["grads"]), np.nonzero((g != o["grads"]).any(1))[0][:5]
     assert np.array_equal(gj, o["guides"])
@@ -98,12 +102,13 @@ def test_errors():
     b = nw.SeqPairBatch(sa, sb, neg, grad_mode="hard", traceback="hirschberg")
     with pytest.raises(ValueError, match="non-negative"):
         b.score_and_grad()
-    lin = nw.SeqPairBatch(sa, sb, nw.AlignParams.from_arrays(mat, [[11.0, 1.0, 11.0, 1.0]], alphabet=AA),
-                          gap_model="linear", grad_mode="hard", traceback="hirschberg")
+    tr = np.zeros(sum(len(s) for s in sa), np.uint16)
+    trk = nw.SeqPairBatch(sa, sb, nw.AlignParams.from_arrays(mat, [[11.0, 1.0, 11.0, 1.0]], alphabet=AA),
+                          grad_mode="hard", traceback="hirschberg", tracks=tr)
     with pytest.raises(NotImplementedError):
-        lin.score_and_grad()
+        trk.score_and_grad()
     nlocal = nw.SeqPairBatch(sa, sb, neg, mode="local", grad_mode="hard", traceback="hirschberg_pmax")
     with pytest.raises(ValueError, match="non-negative"):
         nlocal.score_and_grad()
     with pytest.raises(ValueError):
-        lin.hb_cutoff = 0
+        trk.hb_cutoff = 0
