@@ -225,8 +225,9 @@ double geo_cost(Geo g, int rows, int n, int extra_cols) {
     return stripes * GR * double(n + extra_cols + g.G - 1);
 }
 
-// The geometry for one pair: a lane per pair when the rows fit one lane (up to 32 rows),
-// else the warp geometry that pads the fewest cells (ties: more rows per lane).
+// The geometry for one pair: a lane per pair when the rows fit one lane (up to 32 rows);
+// else (soft) the geometry of least measured cost x padded cells, (hard) the warp geometry
+// that pads the fewest cells, weighing the shuffles of fewer rows per lane.
 // lanes / rpl > 0 force the lanes per pair / rows per lane (the tuner's measurements).
 Geo pick_geo(bool soft, int rows, int n, int lanes, int rpl, bool lane_ok) {
     if (lanes == 1 || (lanes == 0 && lane_ok && rows <= 32)) {
@@ -236,6 +237,21 @@ Geo pick_geo(bool soft, int rows, int n, int lanes, int rpl, bool lane_ok) {
     }
     const int G = lanes > 1 ? lanes : 32;
     if (rpl) return {G, rpl};
+    if (soft && lanes == 0) {
+        // soft, untuned: the geometry of least predicted time = a measured cost per padded cell
+        // (B200, float, the 100-500 residue batch; 32 x 4 = 1) x the pair's padded cells, so
+        // short pairs take narrower stripes and fewer lanes
+        struct C { int G, R; double cost; };
+        static const C costs[] = {{32, 4, 1.00}, {32, 8, 1.02}, {16, 8, 1.18}, {16, 4, 1.35},
+                                  {32, 2, 1.73}, {8, 4, 1.78}, {16, 2, 2.00}};
+        Geo bestc{32, 4};
+        double bt = 1e300;
+        for (const C& k : costs) {
+            const double t = k.cost * geo_cost(Geo{k.G, k.R}, rows, n, 1);
+            if (t < bt) { bt = t; bestc = Geo{k.G, k.R}; }
+        }
+        return bestc;
+    }
     Geo best{G, 4};
     double bc = 1e300;
     const int opts_h[] = {8, 4, 2, 1};
@@ -339,6 +355,10 @@ struct nwg_store {
     bool use_graphs = true;
     cudaStream_t gstream = nullptr;
     cudaEvent_t gev_in = nullptr, gev_out = nullptr;
+    // concurrent buckets: one private stream per bucket (up to kBucketStreams), fork / join events
+    static constexpr int kBucketStreams = 8;
+    cudaStream_t bstream[kBucketStreams] = {};
+    cudaEvent_t bev_fork = nullptr, bev_join[kBucketStreams] = {};
     int64_t graph_captures = 0, graph_replays = 0, graph_failures = 0;
     // timing
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -353,20 +373,54 @@ namespace {
 // CUDA graph on the store's private stream, which waits for `st` before and makes `st` wait
 // for it after: one graph launch in place of a launch per bucket, captured again only when
 // the sequence changes.
-void run_launches(nwg_store* s, GraphCache* gc, const std::vector<Launch>& L, cudaStream_t st) {
+void run_launches(nwg_store* s, GraphCache* gc, const std::vector<Launch>& L, cudaStream_t st,
+                  bool concurrent = false) {
     if (L.empty()) return;
     s->last_launches += int64_t(L.size());
-    auto launch_all = [&](cudaStream_t on) {
-        for (const Launch& l : L) {
-            void* args[] = {const_cast<unsigned char*>(l.arg.data())};
-            NWG_CUDA(cudaLaunchKernel(l.fn, dim3(l.grid), dim3(unsigned(l.block)), args, l.smem, on));
+    concurrent = concurrent && L.size() > 1;
+    if (concurrent && !s->bev_fork) {
+        NWG_CUDA(cudaEventCreateWithFlags(&s->bev_fork, cudaEventDisableTiming));
+        for (int k = 0; k < nwg_store::kBucketStreams; ++k) {
+            NWG_CUDA(cudaStreamCreateWithFlags(&s->bstream[k], cudaStreamNonBlocking));
+            NWG_CUDA(cudaEventCreateWithFlags(&s->bev_join[k], cudaEventDisableTiming));
         }
+    }
+    // the launches in order on `on`; concurrent: each on its own private stream, forked from and
+    // joined back into `on` (so a capture on `on` records them as parallel branches)
+    auto issue = [&](cudaStream_t on) -> cudaError_t {
+        if (!concurrent) {
+            for (const Launch& l : L) {
+                void* args[] = {const_cast<unsigned char*>(l.arg.data())};
+                const cudaError_t e = cudaLaunchKernel(l.fn, dim3(l.grid), dim3(unsigned(l.block)), args, l.smem, on);
+                if (e != cudaSuccess) return e;
+            }
+            return cudaSuccess;
+        }
+        cudaError_t e = cudaEventRecord(s->bev_fork, on);
+        if (e != cudaSuccess) return e;
+        const int ns = std::min<int>(int(L.size()), nwg_store::kBucketStreams);
+        for (int k = 0; k < ns; ++k)
+            if ((e = cudaStreamWaitEvent(s->bstream[k], s->bev_fork, 0)) != cudaSuccess) return e;
+        for (size_t i = 0; i < L.size(); ++i) {
+            const Launch& l = L[i];
+            void* args[] = {const_cast<unsigned char*>(l.arg.data())};
+            e = cudaLaunchKernel(l.fn, dim3(l.grid), dim3(unsigned(l.block)), args, l.smem,
+                                 s->bstream[i % size_t(nwg_store::kBucketStreams)]);
+            if (e != cudaSuccess) return e;
+        }
+        for (int k = 0; k < ns; ++k) {
+            if ((e = cudaEventRecord(s->bev_join[k], s->bstream[k])) != cudaSuccess) return e;
+            if ((e = cudaStreamWaitEvent(on, s->bev_join[k], 0)) != cudaSuccess) return e;
+        }
+        return cudaSuccess;
     };
+    auto launch_all = [&](cudaStream_t on) { NWG_CUDA(issue(on)); };
     if (!gc || !s->use_graphs) {
         launch_all(st);
         return;
     }
     std::vector<unsigned char> key;
+    key.push_back(concurrent ? 1 : 0);
     for (const Launch& l : L) {
         const unsigned char* f = reinterpret_cast<const unsigned char*>(&l.fn);
         key.insert(key.end(), f, f + sizeof(l.fn));
@@ -386,12 +440,7 @@ void run_launches(nwg_store* s, GraphCache* gc, const std::vector<Launch>& L, cu
         gc->reset();
         cudaGraph_t g = nullptr;
         NWG_CUDA(cudaStreamBeginCapture(s->gstream, cudaStreamCaptureModeThreadLocal));
-        cudaError_t le = cudaSuccess;
-        for (const Launch& l : L) {
-            void* args[] = {const_cast<unsigned char*>(l.arg.data())};
-            le = cudaLaunchKernel(l.fn, dim3(l.grid), dim3(unsigned(l.block)), args, l.smem, s->gstream);
-            if (le != cudaSuccess) break;
-        }
+        const cudaError_t le = issue(s->gstream);
         const cudaError_t ee = cudaStreamEndCapture(s->gstream, &g);
         cudaError_t ie = cudaErrorStreamCaptureInvalidated;
         if (le == cudaSuccess && ee == cudaSuccess && g) ie = cudaGraphInstantiate(&gc->exec, g, 0);
@@ -831,6 +880,7 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
     const int NV = aff ? 3 : 1;
     std::vector<Launch> launches;
     std::vector<nwg::SoftArgs> args;
+    std::vector<int64_t> need;   // scratch bytes of each launch
     int64_t scratch_total = 0;
     for (auto& B : P->buckets) {
         if (B.pairs.empty()) continue;
@@ -876,6 +926,7 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
         const int64_t slots = mw ? blocks : blocks * gpb;
         scratch_total = std::max<int64_t>(scratch_total, slots * stride);
         nwg::SoftArgs A{};
+        const int64_t bucket_need = (slots * stride + 255) & ~int64_t(255);
         A.a = s->a.as<uint8_t>(); A.oa = s->doa.as<int64_t>();
         A.b = s->b.as<uint8_t>(); A.ob = s->dob.as<int64_t>();
         A.tracks = tr ? s->tracks.as<uint16_t>() : nullptr;
@@ -900,16 +951,24 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
         }
         launches.push_back(make_launch(reinterpret_cast<const void*>(fn), unsigned(blocks), block, smem, A));
         args.push_back(A);
+        need.push_back(bucket_need);
     }
     if (launches.empty()) return;
-    // one scratch buffer for the sequence (the buckets run one after another)
-    s->scratch.need(size_t(scratch_total), st);
+    // the buckets run at once, each in its own part of the scratch, when their parts fit the
+    // budget together (a bucket of a few large pairs then shares the device with the others
+    // instead of running alone); else one after another in one shared part
+    int64_t sum = 0;
+    for (int64_t b : need) sum += b;
+    const bool concurrent = launches.size() > 1 && sum <= s->scratch_budget;
+    s->scratch.need(size_t(concurrent ? sum : scratch_total), st);
+    int64_t off = 0;
     for (size_t k = 0; k < launches.size(); ++k) {
-        args[k].scratch = s->scratch.p;
+        args[k].scratch = static_cast<unsigned char*>(s->scratch.p) + (concurrent ? off : 0);
+        off += need[k];
         std::memcpy(launches[k].arg.data(), &args[k], sizeof(nwg::SoftArgs));
     }
     GraphCache* gc = subset ? nullptr : J.band >= 0 ? &s->g_soft_band : &s->g_soft[sizeof(T) == 4 ? 0 : 1];
-    run_launches(s, gc, launches, st);
+    run_launches(s, gc, launches, st, concurrent);
 }
 
 void run_soft(nwg_store* s, const nwg_job& J, cudaStream_t st) {
@@ -1087,6 +1146,11 @@ int nwg_store_destroy(nwg_store* s) {
                               &s->g_hard_band})
             g->reset();
         if (s->gstream) cudaStreamDestroy(s->gstream);
+        for (int k = 0; k < nwg_store::kBucketStreams; ++k) {
+            if (s->bstream[k]) cudaStreamDestroy(s->bstream[k]);
+            if (s->bev_join[k]) cudaEventDestroy(s->bev_join[k]);
+        }
+        if (s->bev_fork) cudaEventDestroy(s->bev_fork);
         if (s->gev_in) cudaEventDestroy(s->gev_in);
         if (s->gev_out) cudaEventDestroy(s->gev_out);
         if (s->ev0) cudaEventDestroy(s->ev0);
