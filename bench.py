@@ -42,7 +42,7 @@ AA = "ACDEFGHIKLMNPQRSTVWY"
 OPS_PER_CELL_SOFT = 32.0          # soft affine: ~10 forward + ~22 backward/gradient FP32 ops
 OPS_PER_CELL_HARD = 22.0          # hard affine: 13 FP32 + 9 compare/select
 FP32_LANE_OPS_PEAK = 148 * 128 * 1.965e9   # ops/s at the maximum SM clock
-SOFT_DRAM_BYTES_PER_CELL = 31.1            # ncu, soft kernel 32x4 on 800+800 pairs of this workload
+SOFT_DRAM_BYTES_PER_CELL = 30.2            # ncu, soft kernel 32x4 on 800+800 pairs of this workload
 
 
 def measured_hbm_gbs():
