@@ -715,6 +715,7 @@ def bench_c1(args):
     cells = cells_of(oa, ob)
     params = nw.AlignParams.from_arrays(mat[None], [[11.0, 1.0, 11.0, 1.0]], alphabet=nw.AA20)
     bt = nw.SeqPairBatch.from_codes(a, oa, b, ob, params, grad_mode="hard")
+    table = {} if args.no_tune else bt.autotune()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     for _ in range(max(args.warmup, 3)):
         bt.score_and_grad(); bt.compute_grad()
@@ -729,7 +730,8 @@ def bench_c1(args):
     print(json.dumps({"metric": "hard-grad batch GCUPS", "value": cells * args.steps / (tot / 1e3) / 1e9,
                       "unit": "GCUPS", "n_gpus": 1, "steps": args.steps, "ms_per_step": tot / args.steps,
                       "kernel_ms_per_step": kms / args.steps, "config": {"workload": "c1 hard global affine float32, "
-                      "10k pairs L 50-300", "cells_per_step": cells}, "step_ms": ms}))
+                      "10k pairs L 50-300", "cells_per_step": cells},
+                      "autotune": {str(k): _tune_mod().describe(v) for k, v in table.items()}, "step_ms": ms}))
 
 
 def _trainer(pos, neg, mat, gaps0, steps, srv=None):

@@ -25,6 +25,15 @@
 #include "nwg_kernels.h"
 #include "nwg_walk.cuh"
 
+namespace nwg {
+// The traceback of pairs filled by several warps each: one thread per pair, after the fills.
+__global__ void walk_kernel(const WalkArgs A) {
+    const int64_t it = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (it >= A.n_items) return;
+    walk_pair(A, A.order[it]);
+}
+}  // namespace nwg
+
 namespace {
 
 thread_local std::string g_err;
@@ -84,6 +93,7 @@ void keep_pool(int dev) {
 // ── reductions ────────────────────────────────────────────────────────────────
 // The reference's blocked sum: block b sums w[p] * g[p][k] over its pairs in pair order from
 // 0.0 (a product, then an add: no fused multiply-add), then the blocks are added in order.
+template <bool W>
 __global__ void blocked_partial_kernel(const double* __restrict__ g, const double* __restrict__ w,
                                        int64_t n_pairs, int64_t gs, int64_t block, double* part) {
     const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -91,21 +101,35 @@ __global__ void blocked_partial_kernel(const double* __restrict__ g, const doubl
     if (k >= gs) return;
     const int64_t p0 = b * block, p1 = min(n_pairs, p0 + block);
     double acc = 0.0;
-    constexpr int U = 16;   // loads in flight; the adds stay in pair order
-    int64_t p = p0;
-    for (; p + U <= p1; p += U) {
-        double v[U];
+    // the adds stay in pair order; the loads run a batch ahead (two register batches), so
+    // 2U loads are in flight while U are added
+    constexpr int U = 16;
+    double va[U], vb[U], wa[W ? U : 1], wb[W ? U : 1];
+    auto load = [&](double (&v)[U], double (&ww)[W ? U : 1], int64_t q) {
 #pragma unroll
-        for (int u = 0; u < U; ++u) v[u] = g[(p + u) * gs + k];
-        if (w) {
+        for (int u = 0; u < U; ++u) {
+            v[u] = g[(q + u) * gs + k];
+            if constexpr (W) ww[u] = w[q + u];
+        }
+    };
+    const int64_t nfull = (p1 - p0) / U;
+    if (nfull > 0) load(va, wa, p0);
+    for (int64_t i = 0; i < nfull; ++i) {
+        const int64_t q = p0 + i * U;
+        if (i + 1 < nfull) load(vb, wb, q + U);
 #pragma unroll
-            for (int u = 0; u < U; ++u) acc = __dadd_rn(acc, __dmul_rn(w[p + u], v[u]));
-        } else {
+        for (int u = 0; u < U; ++u) {
+            if constexpr (W) acc = __dadd_rn(acc, __dmul_rn(wa[u], va[u]));
+            else acc = __dadd_rn(acc, va[u]);
+        }
 #pragma unroll
-            for (int u = 0; u < U; ++u) acc = __dadd_rn(acc, v[u]);
+        for (int u = 0; u < U; ++u) {
+            va[u] = vb[u];
+            if constexpr (W) wa[u] = wb[u];
         }
     }
-    for (; p < p1; ++p) acc = w ? __dadd_rn(acc, __dmul_rn(w[p], g[p * gs + k])) : __dadd_rn(acc, g[p * gs + k]);
+    for (int64_t p = p0 + nfull * U; p < p1; ++p)
+        acc = W ? __dadd_rn(acc, __dmul_rn(w[p], g[p * gs + k])) : __dadd_rn(acc, g[p * gs + k]);
     part[b * gs + k] = acc;
 }
 __global__ void blocked_total_kernel(const double* __restrict__ part, int64_t nblocks, int64_t gs,
@@ -254,15 +278,19 @@ Geo pick_geo(bool soft, int rows, int n, int lanes, int rpl, bool lane_ok) {
     }
     Geo best{G, 4};
     double bc = 1e300;
+    // hard: fewer rows per lane cost more shuffles and boundary moves per cell -- measured cost
+    // per padded cell (B200, float, the 50-300 residue batch; 8 rows = 1)
     const int opts_h[] = {8, 4, 2, 1};
+    const double cost_h[] = {1.00, 1.22, 1.35, 1.80};
     const int opts_s[] = {4, 2};
+    const double cost_s[] = {1.00, 1.73};
     const int* opts = soft ? opts_s : opts_h;
+    const double* cst = soft ? cost_s : cost_h;
     const int no = soft ? 2 : 4;
     for (int k = 0; k < no; ++k) {
         const Geo g{G, opts[k]};
         if (!geo_available(soft, g.G, g.R)) continue;
-        // fewer rows per lane costs more shuffles per cell: weigh them in
-        const double c = geo_cost(g, rows, n, soft ? 1 : 0) * (1.0 + 0.75 / g.R);
+        const double c = geo_cost(g, rows, n, soft ? 1 : 0) * cst[k];
         if (c < bc) { bc = c; best = g; }
     }
     return best;
@@ -343,7 +371,7 @@ struct nwg_store {
     struct GeoCost { int G, R; double ns_per_cell; };
     std::map<std::pair<int, int>, std::vector<GeoCost>> geo_costs;
     bool plain = false;
-    int64_t scratch_budget = int64_t(24) << 30;   // bytes of soft scratch one call may hold
+    int64_t scratch_budget = -1;   // bytes of soft scratch one call may hold (-1: from the device's memory)
     int64_t ck_threshold = int64_t(16) << 20;     // soft: forward tables above this are checkpointed
     DBuf stripe_tab;
     DBuf hb_pairs;                      // the pairs a Hirschberg run splits
@@ -374,7 +402,7 @@ namespace {
 // for it after: one graph launch in place of a launch per bucket, captured again only when
 // the sequence changes.
 void run_launches(nwg_store* s, GraphCache* gc, const std::vector<Launch>& L, cudaStream_t st,
-                  bool concurrent = false) {
+                  bool concurrent = false, const std::vector<int>* lanes = nullptr) {
     if (L.empty()) return;
     s->last_launches += int64_t(L.size());
     concurrent = concurrent && L.size() > 1;
@@ -398,14 +426,16 @@ void run_launches(nwg_store* s, GraphCache* gc, const std::vector<Launch>& L, cu
         }
         cudaError_t e = cudaEventRecord(s->bev_fork, on);
         if (e != cudaSuccess) return e;
-        const int ns = std::min<int>(int(L.size()), nwg_store::kBucketStreams);
+        // launches of one lane run in order on one stream; lanes run at once
+        auto lane_of = [&](size_t i) { return (lanes ? size_t((*lanes)[i]) : i) % size_t(nwg_store::kBucketStreams); };
+        int ns = 0;
+        for (size_t i = 0; i < L.size(); ++i) ns = std::max(ns, int(lane_of(i)) + 1);
         for (int k = 0; k < ns; ++k)
             if ((e = cudaStreamWaitEvent(s->bstream[k], s->bev_fork, 0)) != cudaSuccess) return e;
         for (size_t i = 0; i < L.size(); ++i) {
             const Launch& l = L[i];
             void* args[] = {const_cast<unsigned char*>(l.arg.data())};
-            e = cudaLaunchKernel(l.fn, dim3(l.grid), dim3(unsigned(l.block)), args, l.smem,
-                                 s->bstream[i % size_t(nwg_store::kBucketStreams)]);
+            e = cudaLaunchKernel(l.fn, dim3(l.grid), dim3(unsigned(l.block)), args, l.smem, s->bstream[lane_of(i)]);
             if (e != cudaSuccess) return e;
         }
         for (int k = 0; k < ns; ++k) {
@@ -421,6 +451,8 @@ void run_launches(nwg_store* s, GraphCache* gc, const std::vector<Launch>& L, cu
     }
     std::vector<unsigned char> key;
     key.push_back(concurrent ? 1 : 0);
+    if (concurrent && lanes)
+        for (int v : *lanes) key.push_back(static_cast<unsigned char>(v & 0xff));
     for (const Launch& l : L) {
         const unsigned char* f = reinterpret_cast<const unsigned char*>(&l.fn);
         key.insert(key.end(), f, f + sizeof(l.fn));
@@ -467,6 +499,15 @@ void run_launches(nwg_store* s, GraphCache* gc, const std::vector<Launch>& L, cu
     NWG_CUDA(cudaGraphLaunch(gc->exec, s->gstream));
     NWG_CUDA(cudaEventRecord(s->gev_out, s->gstream));
     NWG_CUDA(cudaStreamWaitEvent(st, s->gev_out, 0));
+}
+
+// The scratch budget of one call: as set, else 60 % of what the device could give it (its free
+// memory plus the scratch this store already holds), at least 24 GiB.
+int64_t scratch_budget_of(nwg_store* s) {
+    if (s->scratch_budget >= 0) return s->scratch_budget;
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    return std::max<int64_t>(int64_t(24) << 30, int64_t(0.6 * double(fr + s->scratch.bytes)));
 }
 
 void set_params_dev(nwg_store* s) {
@@ -660,15 +701,25 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
             stride = row;
         }
     };
-    int64_t max_total = 1;
+    int64_t max_total = 1, sum_total = 0;
+    bool any_mw = false;
+    int nbk = 0;
     for (auto& B : P.buckets) {
         if (B.pairs.empty()) continue;
         int64_t bl, sl, sd;
         bucket_shape(B, bl, sl, sd);
         max_total = std::max(max_total, sl * sd);
+        sum_total += (sl * sd * int64_t(sizeof(T)) + 255) & ~int64_t(255);
+        any_mw |= B.geo.mw > 1;
+        ++nbk;
     }
-    s->scratch.need(size_t(max_total) * sizeof(T), st);
+    // the buckets' fills and walks run at once (bucket k's walk after its fill, each bucket on
+    // its own stream and scratch part) when nothing needs a host check between fill and walk
+    const bool concurrent = !any_mw && nbk > 1 && sum_total <= scratch_budget_of(s);
+    s->scratch.need(concurrent ? size_t(sum_total) : size_t(max_total) * sizeof(T), st);
     std::vector<Launch> fills;
+    std::vector<nwg::HardArgs> fill_args;
+    int64_t soff_b = 0;
     for (auto& B : P.buckets) {
         if (B.pairs.empty()) continue;
         HardFn fn = hard_fn_rt<T>(aff, loc, tr, B.geo);
@@ -692,10 +743,13 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
         }
         int64_t blocks, slots, stride;
         bucket_shape(B, blocks, slots, stride);
-        A.scratch = s->scratch.p; A.scratch_stride = stride;
+        A.scratch = concurrent ? static_cast<void*>(static_cast<unsigned char*>(s->scratch.p) + soff_b) : s->scratch.p;
+        soff_b += (slots * stride * int64_t(sizeof(T)) + 255) & ~int64_t(255);
+        A.scratch_stride = stride;
         A.row_stride = 3 * (int64_t(B.maxn) + 1);
         A.score = s->score.as<double>(); A.end = s->end.as<int32_t>();
         fills.push_back(make_launch(reinterpret_cast<const void*>(fn), unsigned(blocks), hblock, smem, A));
+        fill_args.push_back(A);
     }
     // traceback buffers: gradient, guide, path
     if (want_grad) {
@@ -732,13 +786,38 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
     const Launch walk = make_launch(reinterpret_cast<const void*>(&nwg::walk_kernel),
                                     unsigned((P.n_planned + 127) / 128), 128, 0, W);
     // several warps per pair: a wait between warps that ran out fails the call (end state 3),
-    // which the host checks between the fills and the walk; otherwise the fills and the walk
-    // are one captured sequence
-    bool any_mw = false;
-    for (auto& B : P.buckets) any_mw |= (B.geo.mw > 1 && !B.pairs.empty());
+    // which the host checks between the fills and a separate walk; otherwise the fills walk
+    // their own pairs, one captured sequence
     GraphCache* gc = band ? &s->g_hard_band : &s->g_hard[sizeof(T) == 4 ? 0 : 1];
-    if (!any_mw && P.n_planned) fills.push_back(walk);
-    run_launches(s, gc, fills, st);
+    if (!any_mw) {
+        // a warp per pair: the fill walks its own pairs (the codes still in L2); a lane per pair
+        // (many short pairs): a walk launch over the bucket's pairs after its fill.  The buckets
+        // run at once when their scratch parts fit.
+        std::vector<Launch> seq;
+        std::vector<int> lanes;
+        size_t k = 0;
+        for (auto& B : P.buckets) {
+            if (B.pairs.empty()) continue;
+            const bool fuse = B.geo.G > 1;
+            fill_args[k].walk_fused = fuse ? 1 : 0;
+            fill_args[k].walk = W;
+            std::memcpy(fills[k].arg.data(), &fill_args[k], sizeof(nwg::HardArgs));
+            seq.push_back(fills[k]);
+            lanes.push_back(int(k));
+            if (!fuse) {
+                nwg::WalkArgs Wb = W;
+                Wb.order = P.order.as<int32_t>() + B.off;
+                Wb.n_items = int64_t(B.pairs.size());
+                seq.push_back(make_launch(reinterpret_cast<const void*>(&nwg::walk_kernel),
+                                          unsigned((Wb.n_items + 127) / 128), 128, 0, Wb));
+                lanes.push_back(int(k));
+            }
+            ++k;
+        }
+        run_launches(s, gc, seq, st, concurrent, &lanes);
+    } else {
+        run_launches(s, gc, fills, st);
+    }
     if (any_mw && s->n) {
         std::vector<int32_t> e(size_t(s->n) * 4);
         NWG_CUDA(cudaMemcpyAsync(e.data(), s->end.p, e.size() * 4, cudaMemcpyDeviceToHost, st));
@@ -878,6 +957,7 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
     }
     const int sms = sm_count(s->device);
     const int NV = aff ? 3 : 1;
+    const int64_t budget = scratch_budget_of(s);
     std::vector<Launch> launches;
     std::vector<nwg::SoftArgs> args;
     std::vector<int64_t> need;   // scratch bytes of each launch
@@ -922,7 +1002,7 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
         const int64_t per_block = mw ? stride : stride * gpb;
         // as many resident groups as fit the device (occupancy) and the scratch budget
         int64_t blocks = std::min<int64_t>(mw ? items : (items + gpb - 1) / gpb, int64_t(sms) * occ);
-        blocks = std::max<int64_t>(1, std::min<int64_t>(blocks, s->scratch_budget / std::max<int64_t>(1, per_block)));
+        blocks = std::max<int64_t>(1, std::min<int64_t>(blocks, budget / std::max<int64_t>(1, per_block)));
         const int64_t slots = mw ? blocks : blocks * gpb;
         scratch_total = std::max<int64_t>(scratch_total, slots * stride);
         nwg::SoftArgs A{};
@@ -959,7 +1039,7 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
     // instead of running alone); else one after another in one shared part
     int64_t sum = 0;
     for (int64_t b : need) sum += b;
-    const bool concurrent = launches.size() > 1 && sum <= s->scratch_budget;
+    const bool concurrent = launches.size() > 1 && sum <= budget;
     s->scratch.need(size_t(concurrent ? sum : scratch_total), st);
     int64_t off = 0;
     for (size_t k = 0; k < launches.size(); ++k) {
@@ -1323,7 +1403,8 @@ int nwg_reduce(nwg_store* s, const double* w, double* out) {
             NWG_CUDA(cudaMemcpy(dw, w, size_t(n) * 8, cudaMemcpyHostToDevice));
         }
         dim3 grid(unsigned((gs + 31) / 32), unsigned(nb));
-        blocked_partial_kernel<<<grid, 32>>>(s->grad.as<double>(), dw, n, gs, B, s->part.as<double>());
+        if (dw) blocked_partial_kernel<true><<<grid, 32>>>(s->grad.as<double>(), dw, n, gs, B, s->part.as<double>());
+        else blocked_partial_kernel<false><<<grid, 32>>>(s->grad.as<double>(), dw, n, gs, B, s->part.as<double>());
         NWG_CUDA(cudaGetLastError());
         blocked_total_kernel<<<unsigned((gs + 127) / 128), 128>>>(s->part.as<double>(), nb, gs, s->red.as<double>());
         NWG_CUDA(cudaGetLastError());
@@ -1347,7 +1428,8 @@ int nwg_reduce_range(nwg_store* s, int64_t start, int64_t end, const double* w, 
             NWG_CUDA(cudaMemcpy(dw, w, size_t(n) * 8, cudaMemcpyHostToDevice));
         }
         dim3 grid(unsigned((gs + 31) / 32), unsigned(nb));
-        blocked_partial_kernel<<<grid, 32>>>(s->grad.as<double>() + start * gs, dw, n, gs, B, s->part.as<double>());
+        if (dw) blocked_partial_kernel<true><<<grid, 32>>>(s->grad.as<double>() + start * gs, dw, n, gs, B, s->part.as<double>());
+        else blocked_partial_kernel<false><<<grid, 32>>>(s->grad.as<double>() + start * gs, dw, n, gs, B, s->part.as<double>());
         NWG_CUDA(cudaGetLastError());
         blocked_total_kernel<<<unsigned((gs + 127) / 128), 128>>>(s->part.as<double>(), nb, gs, s->red.as<double>());
         NWG_CUDA(cudaGetLastError());

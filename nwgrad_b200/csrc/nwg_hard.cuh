@@ -25,6 +25,7 @@
 // steps.  Border cells (row 0, column 0) are not stored: the walk knows them.
 #pragma once
 #include "nwg_common.cuh"
+#include "nwg_walk.cuh"
 
 namespace nwg {
 
@@ -49,6 +50,9 @@ struct HardArgs {
     int band;                                  // half-width
     const int64_t* stripe_base;                // per pair: first entry in stripe_tab
     int64_t* stripe_tab;                       // per stripe: code offset in the pair, first column
+    // one warp per pair: lane 0 walks the pair's codes as soon as its fill is done
+    int walk_fused;
+    WalkArgs walk;
 };
 
 // The band of DP row i around guide g (aligner.hpp:2644-2700): columns [jlo, jhi].
@@ -174,6 +178,8 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
                 A.score[p] = static_cast<double>(sc);
                 A.end[4 * p] = ei; A.end[4 * p + 1] = ej; A.end[4 * p + 2] = st;
                 A.end[4 * p + 3] = (G << 8) | R;
+                // an empty side: the walk runs the border (no codes read)
+                if (!MW && A.walk_fused) walk_pair(A.walk, p);
             }
             continue;
         }
@@ -491,6 +497,15 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
             A.score[p] = static_cast<double>(bestv);
             A.end[4 * p] = besti; A.end[4 * p + 1] = bestj; A.end[4 * p + 2] = bests;
             A.end[4 * p + 3] = (G << 8) | R;
+        }
+        if constexpr (!MW) {
+            // the traceback, while this pair's codes are still in L2: the group's codes and end
+            // cell are visible to its lane 0 after the warp barrier; its other lanes go on with
+            // their next pair's fill meanwhile
+            if (A.walk_fused) {
+                if constexpr (G > 1) __syncwarp(gmask);
+                if (lane == 0) walk_pair(A.walk, p);
+            }
         }
     }
 }

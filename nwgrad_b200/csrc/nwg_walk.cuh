@@ -1,7 +1,9 @@
-// Traceback kernel: one thread per pair walks the predecessor codes the fill stored
-// (nwg_hard.cuh) from the end cell back to the start.  Included by nwg_capi.cu only.
+// Traceback: one thread walks a pair's predecessor codes, which the fill stored
+// (nwg_hard.cuh), from the end cell back to the start.  walk_pair is called by the hard fill
+// itself right after it filled a pair (while the codes are fresh in L2), or by walk_kernel
+// (nwg_capi.cu) after the fills of pairs that several warps filled.
 #pragma once
-#include "nwg_hard.cuh"
+#include "nwg_common.cuh"
 
 namespace nwg {
 
@@ -40,10 +42,7 @@ __device__ __forceinline__ uint8_t code_at(const uint8_t* codes, int i, int j, i
     return codes[base + ((int64_t(t >> 3) * G + g) * 8 + (t & 7)) * R + r];
 }
 
-__global__ void walk_kernel(const WalkArgs A) {
-    const int64_t it = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (it >= A.n_items) return;
-    const int p = A.order[it];
+static __device__ __noinline__ void walk_pair(const WalkArgs& A, const int p) {
     const int64_t ao = A.oa[p], bo = A.ob[p];
     const int m = int(A.oa[p + 1] - ao), n = int(A.ob[p + 1] - bo);
     const uint8_t* ap = A.a + ao;
