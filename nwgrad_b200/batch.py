@@ -245,9 +245,7 @@ class SeqPairBatch:
         ob = np.ascontiguousarray(off_b, dtype=np.int64)
         if oa.shape != ob.shape or oa.ndim != 1 or oa.size < 1:
             raise ValueError("nwgrad: off_a / off_b need n_pairs + 1 entries each")
-        N = self._alpha.size
-        if a.size and int(a.max()) >= N or b.size and int(b.max()) >= N:
-            raise ValueError(f"nwgrad: a code is not in alphabet \"{self._alpha.symbols}\"")
+        N = self._alpha.size   # codes >= N: the store refuses them (ValueError)
         tk = kw.get("tracks")
         gk = kw.get("gap_tracks")
         self._n = oa.size - 1

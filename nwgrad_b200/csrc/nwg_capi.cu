@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -557,7 +558,15 @@ void build_plan(nwg_store* s, Plan& P, bool soft, int lanes, int rpl, int elem_b
     const int64_t n = s->n;
     // one lane per pair keeps a K*N*N histogram per lane in shared memory (soft)
     const bool lane_ok_soft = int64_t(s->K) * s->N * s->N * elem_bytes * 32 <= 48 * 1024;
-    std::map<std::tuple<int, int, int>, int> idx;
+    std::vector<std::array<int, 3>> bkeys;
+    // the tuner's choices per size class, looked up once
+    constexpr int kClasses = 64;
+    std::vector<const std::vector<nwg_store::GeoCost>*> cost_of(kClasses, nullptr);
+    std::vector<std::pair<int, int>> table_of(kClasses, {0, 0});
+    for (const auto& kv : s->geo_costs)
+        if (kv.first.first == int(soft) && kv.first.second >= 0 && kv.first.second < kClasses) cost_of[kv.first.second] = &kv.second;
+    for (const auto& kv : s->geo_table)
+        if (kv.first.first == int(soft) && kv.first.second >= 0 && kv.first.second < kClasses) table_of[kv.first.second] = kv.second;
     for (int64_t p = 0; p < n; ++p) {
         const int m = int(s->oa[p + 1] - s->oa[p]), nb = int(s->ob[p + 1] - s->ob[p]);
         if (hb_cut > 0 && m > hb_cut) continue;
@@ -569,36 +578,39 @@ void build_plan(nwg_store* s, Plan& P, bool soft, int lanes, int rpl, int elem_b
             if (s->plain) g = Geo{32, 4};
             else if (soft && !s->tracked() && rows >= kLongRows && nb >= 256) g = Geo{32, 4, false, long_warps(rows, 128)};
             else if (!soft && rows >= kLongRows && nb >= 256) g = Geo{32, 8, false, long_warps(rows, 256)};
-            else {
-                auto ic = s->geo_costs.find({int(soft), sc});
-                if (ic != s->geo_costs.end()) {
-                    double best = 1e300;
-                    for (const auto& gc : ic->second) {
-                        if (soft && gc.G == 1 && !lane_ok_soft) continue;
-                        const double t = gc.ns_per_cell * geo_cost(Geo{gc.G, gc.R}, std::max(rows, 1), nb, soft ? 1 : 0);
-                        if (t < best) { best = t; g = Geo{gc.G, gc.R}; }
-                    }
+            else if (sc < kClasses && cost_of[sc]) {
+                double best = 1e300;
+                for (const auto& gc : *cost_of[sc]) {
+                    if (soft && gc.G == 1 && !lane_ok_soft) continue;
+                    const double t = gc.ns_per_cell * geo_cost(Geo{gc.G, gc.R}, std::max(rows, 1), nb, soft ? 1 : 0);
+                    if (t < best) { best = t; g = Geo{gc.G, gc.R}; }
                 }
-                auto it = s->geo_table.find({int(soft), sc});
-                if (ic == s->geo_costs.end() && it != s->geo_table.end() && (!soft || it->second.first > 1 || lane_ok_soft))
-                    g = Geo{it->second.first, it->second.second};
+            } else if (sc < kClasses && table_of[sc].first > 0 && (!soft || table_of[sc].first > 1 || lane_ok_soft)) {
+                g = Geo{table_of[sc].first, table_of[sc].second};
             }
         }
-        auto key = std::make_tuple(g.G, g.R * 100 + g.mw, sc);
-        auto itb = idx.find(key);
-        int bi;
-        if (itb == idx.end()) { bi = int(P.buckets.size()); idx[key] = bi; P.buckets.push_back(Bucket{g, {}, 0, 0, 0}); }
-        else bi = itb->second;
+        // the bucket of (geometry, size class): few buckets, a linear search
+        const int k1 = g.G, k2 = g.R * 100 + g.mw, k3 = sc;
+        int bi = -1;
+        for (int q = 0; q < int(bkeys.size()); ++q)
+            if (bkeys[q][0] == k1 && bkeys[q][1] == k2 && bkeys[q][2] == k3) { bi = q; break; }
+        if (bi < 0) {
+            bi = int(P.buckets.size());
+            bkeys.push_back({k1, k2, k3});
+            P.buckets.push_back(Bucket{g, {}, 0, 0, 0});
+        }
         P.buckets[bi].pairs.push_back(int32_t(p));
     }
     std::vector<int32_t> order;
     order.reserve(n);
     if (!soft) P.code_off.assign(n + 1, 0);
+    std::vector<int64_t> cells_v(size_t(n) + 1);
+    int64_t* const pair_cells = cells_v.data();
+    for (int64_t q = 0; q < n; ++q) pair_cells[q] = (s->oa[q + 1] - s->oa[q]) * (s->ob[q + 1] - s->ob[q]);
     for (auto& B : P.buckets) {
         // longest first: the persistent groups then finish together
-        std::sort(B.pairs.begin(), B.pairs.end(), [&](int32_t x, int32_t y) {
-            const int64_t cx = (s->oa[x + 1] - s->oa[x]) * (s->ob[x + 1] - s->ob[x]);
-            const int64_t cy = (s->oa[y + 1] - s->oa[y]) * (s->ob[y + 1] - s->ob[y]);
+        std::sort(B.pairs.begin(), B.pairs.end(), [pair_cells](int32_t x, int32_t y) {
+            const int64_t cx = pair_cells[x], cy = pair_cells[y];
             return cx != cy ? cx > cy : x < y;
         });
         B.off = int64_t(order.size());
