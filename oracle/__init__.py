@@ -54,7 +54,8 @@ def lib():
                                                       _u16p, _u16p, C.c_double, _dp, _dp, _i32p, C.c_int]
         L.orc_soft_batch.restype = C.c_int
         L.orc_hb_batch.argtypes = [C.c_int] * 4 + [_dp, _dp, _u8p, _i64p, _u8p, _i64p, C.c_int64,
-                                                    _dp, _dp, _i32p, _u8p, C.c_int64, _i64p, C.c_int, _i32p, C.c_int]
+                                                    _dp, _dp, _i32p, _u8p, C.c_int64, _i64p, C.c_int, _i32p, C.c_int,
+                                                    C.c_int, _u16p, _u16p]
         L.orc_hb_batch.restype = C.c_int
         L.orc_blocked_sum.argtypes = [_dp, C.c_int64, C.c_int64, _dp, _dp]
         L.orc_blocked_sum.restype = C.c_int
@@ -118,25 +119,31 @@ def hard(prec, gm, am, mat, gaps, enc: Encoded, tracked=False, guides_in=None, b
 
 
 def hirschberg(prec, mat, gaps, enc: Encoded, cutoff=512, pmax=False, moves_cap=0, local=False, linear=False):
-    """Hirschberg, affine or linear gaps (untracked, one parameter set).  Pairs longer than
-    `cutoff` rows split, shorter ones run the Pointers path; Local: the endpoint scans give the
-    box that is solved as Global (pmax: the affine prefix-max carry; linear has one sweep).  Returns dict(scores, grads, guides, moves (n, moves_cap)
+    """Hirschberg, affine (untracked, one parameter set) or linear (tracked or not: enc's tracks,
+    K sets).  Pairs longer than `cutoff` rows split, shorter ones run the Pointers path; Local:
+    the endpoint scans give the box that is solved as Global (pmax: the affine prefix-max
+    carry; linear has one sweep).  Returns dict(scores, grads, guides, moves (n, moves_cap)
     path order start to end, nmoves, ends (n, 4): start i, start j, end i, end j)."""
     L = lib()
-    mat = np.ascontiguousarray(mat, np.float64).reshape(-1, np.shape(mat)[-1], np.shape(mat)[-1])[:1]
-    gaps = np.ascontiguousarray(gaps, np.float64).reshape(-1, 4)[:1]
-    N = mat.shape[1]
+    N = np.shape(mat)[-1]
+    mat = np.ascontiguousarray(mat, np.float64).reshape(-1, N, N)
+    gaps = np.ascontiguousarray(gaps, np.float64).reshape(-1, 4)
+    if not linear:
+        mat, gaps = mat[:1], gaps[:1]
+    K = mat.shape[0]
     n = enc.n
     scores = np.zeros(n, np.float64)
-    grads = np.zeros((n, N * N + 4), np.float64)
+    grads = np.zeros((n, K * N * N + 4 * K), np.float64)
     guides = np.zeros(int(enc.oa[-1]) + n, np.int32)
     nmoves = np.zeros(n, np.int64)
     moves = np.zeros((n, max(moves_cap, 1)), np.uint8) if moves_cap else None
     ends = np.zeros((n, 4), np.int32)
+    tk = enc.tracks if linear else None
+    gk = enc.gap_tracks if linear else None
     rc = L.orc_hb_batch(prec, int(bool(pmax)), int(cutoff), N, _p(mat, _dp), _p(gaps, _dp), _p(enc.a, _u8p),
                         _p(enc.oa, _i64p), _p(enc.b, _u8p), _p(enc.ob, _i64p), n, _p(scores, _dp),
                         _p(grads, _dp), _p(guides, _i32p), _p(moves, _u8p), int(moves_cap), _p(nmoves, _i64p),
-                        int(bool(local)), _p(ends, _i32p), int(bool(linear)))
+                        int(bool(local)), _p(ends, _i32p), int(bool(linear)), int(K), _p(tk, _u16p), _p(gk, _u16p))
     assert rc == 0
     return dict(scores=scores, grads=grads, guides=guides, moves=moves, nmoves=nmoves, ends=ends)
 

@@ -1058,23 +1058,29 @@ int hb_local_one(const Model& M, const uint8_t* a, int m, const uint8_t* b, int 
 // columns downward; strict >), then the box solved as Global.
 template <class T>
 struct Lhb {
-    int N; const T* blk; const uint8_t* a; const uint8_t* b; int cutoff;
-    T ge_a, ge_b;
+    int N; const T* blk; const uint8_t* b; int cutoff;
+    const Rows<T>* R;                           // per DP row: substitution row, extends
     std::vector<uint8_t> hops;
-    T sub(int r, int c) const { return blk[size_t(a[r - 1]) * N + b[c - 1]]; }   // 1-based
+    T sub(int i, int c) const { return blk[size_t(R->rs[i - 1]) * N + b[c - 1]]; }   // 1-based
+    T ga(int i) const { return R->gea[i]; }    // gaps in A within DP row i
+    T gb(int i) const { return R->geb[i]; }    // a gap in B into DP row i
+    // lhb_sweep: forward, DP rows i0+1..i1 (gaps in A on row i); reverse (the mirror), DP rows
+    // i1..i0+1 as the suffix from row i-1 (gaps in A on row i-1); row 0's chain on row i0 / i1
     void sweep(bool rev, int i0, int i1, int j0, int j1, std::vector<T>& row) const {
         const int W = j1 - j0;
         row.assign(size_t(W) + 1, T(0));
-        for (int cc = 1; cc <= W; ++cc) row[cc] = row[cc - 1] - ge_a;
+        const T g0 = ga(rev ? i1 : i0);
+        for (int cc = 1; cc <= W; ++cc) row[cc] = row[cc - 1] - g0;
         for (int r = 1; r <= i1 - i0; ++r) {
             const int i = rev ? i1 - r + 1 : i0 + r;
+            const T gea = ga(rev ? i - 1 : i), geb = gb(i);
             T diag = row[0];
-            row[0] = row[0] - ge_b;
+            row[0] = row[0] - geb;
             T left = row[0];
             for (int cc = 1; cc <= W; ++cc) {
                 const int bcol = rev ? j1 - cc : j0 + cc - 1;   // 0-based
-                T v = diag + blk[size_t(a[i - 1]) * N + b[bcol]];
-                const T u = row[cc] - ge_b, l = left - ge_a;
+                T v = diag + blk[size_t(R->rs[i - 1]) * N + b[bcol]];
+                const T u = row[cc] - geb, l = left - gea;
                 if (v < u) v = u;
                 if (v < l) v = l;
                 diag = row[cc];
@@ -1089,15 +1095,17 @@ struct Lhb {
         std::vector<uint8_t> D(size_t(H + 1) * st);
         std::vector<T> prev(st), cur(st);
         prev[0] = T(0);
-        for (int cc = 1; cc <= W; ++cc) { prev[cc] = prev[cc - 1] - ge_a; D[cc] = 2; }
+        const T g0 = ga(i0);
+        for (int cc = 1; cc <= W; ++cc) { prev[cc] = prev[cc - 1] - g0; D[cc] = 2; }
         for (int r = 1; r <= H; ++r) {
+            const T gea = ga(i0 + r), geb = gb(i0 + r);
             uint8_t* d = D.data() + size_t(r) * st;
-            cur[0] = prev[0] - ge_b; d[0] = 1;
+            cur[0] = prev[0] - geb; d[0] = 1;
             T left = cur[0];
             for (int cc = 1; cc <= W; ++cc) {
                 T v = prev[cc - 1] + sub(i0 + r, j0 + cc);
                 uint8_t k = 0;
-                const T u = prev[cc] - ge_b, l = left - ge_a;
+                const T u = prev[cc] - geb, l = left - gea;
                 if (v < u) { v = u; k = 1; }
                 if (v < l) { v = l; k = 2; }
                 cur[cc] = v; d[cc] = k; left = v;
@@ -1117,13 +1125,13 @@ struct Lhb {
         const int H = i1 - i0, W = j1 - j0;
         if (H <= cutoff) { base(i0, i1, j0, j1); return; }
         const int p = i0 + H / 2;
-        std::vector<T> F, R;
+        std::vector<T> F, Rr;
         sweep(false, i0, p, j0, j1, F);
-        sweep(true, p, i1, j0, j1, R);
+        sweep(true, p, i1, j0, j1, Rr);
         T best = ninf<T>();
         int cstar = 0;
         for (int cc = 0; cc <= W; ++cc) {
-            const T v = F[cc] + R[W - cc];
+            const T v = F[cc] + Rr[W - cc];
             if (v > best) { best = v; cstar = cc; }
         }
         solve(i0, p, j0, j0 + cstar);
@@ -1132,12 +1140,14 @@ struct Lhb {
 };
 
 template <class T>
-int lhb_one(const Model& M, const uint8_t* a, int m, const uint8_t* b, int n, int cutoff, HardOut& o) {
-    if (m <= cutoff) return hard_one<T>(M, a, m, b, n, nullptr, nullptr, false, nullptr, -1, o, 0);
-    std::vector<T> blk(size_t(M.N) * M.N);
+int lhb_one(const Model& M, const uint8_t* a, int m, const uint8_t* b, int n, const uint16_t* track,
+            const uint16_t* gtrack, bool tracked, int cutoff, HardOut& o) {
+    if (m <= cutoff) return hard_one<T>(M, a, m, b, n, track, gtrack, tracked, nullptr, -1, o, 0);
+    Rows<T> R;
+    setup_rows<T, true>(R, M, a, m, track, gtrack, tracked);
+    std::vector<T> blk(size_t(M.K) * M.N * M.N);
     for (size_t k = 0; k < blk.size(); ++k) blk[k] = static_cast<T>(M.mat[k]);
-    const T ge_a = static_cast<T>(M.gaps[kExtendA]), ge_b = static_cast<T>(M.gaps[kExtendB]);
-    Lhb<T> h{M.N, blk.data(), a, b, cutoff, ge_a, ge_b, {}};
+    Lhb<T> h{M.N, blk.data(), b, cutoff, &R, {}};
     int is = 0, js = 0, ie = m, je = n;
     bool empty = false;
     if (M.am == 1) {
@@ -1145,9 +1155,10 @@ int lhb_one(const Model& M, const uint8_t* a, int m, const uint8_t* b, int n, in
         T best = T(0); ie = 0; je = 0;
         for (int i = 1; i <= m; ++i) {
             T diag = row[0];
+            const T gea = h.ga(i), geb = h.gb(i);
             for (int j = 1; j <= n; ++j) {
-                T v = diag + blk[size_t(a[i - 1]) * M.N + b[j - 1]];
-                const T u = row[j] - ge_b, l = row[j - 1] - ge_a;
+                T v = diag + h.sub(i, j);
+                const T u = row[j] - geb, l = row[j - 1] - gea;
                 if (v < u) v = u;
                 if (v < l) v = l;
                 v = mx<T>(v, T(0));
@@ -1160,16 +1171,18 @@ int lhb_one(const Model& M, const uint8_t* a, int m, const uint8_t* b, int n, in
         else {
             std::vector<T> g(size_t(je) + 1);
             g[je] = T(0);
-            for (int q = je - 1; q >= 0; --q) g[q] = g[q + 1] - ge_a;
+            const T g0 = h.ga(ie);
+            for (int q = je - 1; q >= 0; --q) g[q] = g[q + 1] - g0;
             T sbest = g[0]; is = ie; js = 0;
             for (int q = 0; q <= je; ++q) if (g[q] > sbest) { sbest = g[q]; js = q; }
             for (int pi = ie - 1; pi >= 0; --pi) {
+                const T gea = h.ga(pi), geb = h.gb(pi + 1);
                 T diag = g[je];
-                g[je] = g[je] - ge_b;
+                g[je] = g[je] - geb;
                 if (g[je] > sbest) { sbest = g[je]; is = pi; js = je; }
                 for (int q = je - 1; q >= 0; --q) {
-                    T v = diag + blk[size_t(a[pi]) * M.N + b[q]];
-                    const T u = g[q] - ge_b, l = g[q + 1] - ge_a;
+                    T v = diag + h.sub(pi + 1, q + 1);
+                    const T u = g[q] - geb, l = g[q + 1] - gea;
                     if (v < u) v = u;
                     if (v < l) v = l;
                     diag = g[q];
@@ -1181,6 +1194,7 @@ int lhb_one(const Model& M, const uint8_t* a, int m, const uint8_t* b, int n, in
     }
     if (!empty) h.solve(is, ie, js, je);
     // replay: score in T, counts, guide (guide_j_affine_hb :5233-5249, gap-model free)
+    const size_t NN = size_t(M.K) * M.N * M.N;
     T s = T(0);
     int i = is, j = js;
     std::vector<int32_t> gj(size_t(m) + 1, -1);
@@ -1189,17 +1203,17 @@ int lhb_one(const Model& M, const uint8_t* a, int m, const uint8_t* b, int n, in
     for (uint8_t op : h.hops) {
         if (op == 0) {
             ++i; ++j;
-            s += blk[size_t(a[i - 1]) * M.N + b[j - 1]];
-            if (o.grad) o.grad[size_t(a[i - 1]) * M.N + b[j - 1]] += 1.0;
+            s += h.sub(i, j);
+            if (o.grad) o.grad[size_t(R.rs[i - 1]) * M.N + b[j - 1]] += 1.0;
             gj[i] = j;
         } else if (op == 1) {
             ++i;
-            s -= ge_b;
-            if (o.grad) o.grad[size_t(M.N) * M.N + kExtendB] -= 1.0;
+            s -= h.gb(i);
+            if (o.grad) o.grad[NN + 4 * size_t(R.trk[i - 1]) + kExtendB] -= 1.0;
             gj[i] = j;
         } else {
-            s -= ge_a;
-            if (o.grad) o.grad[size_t(M.N) * M.N + kExtendA] -= 1.0;
+            s -= h.ga(i);
+            if (o.grad) o.grad[NN + 4 * size_t(R.gtrk[i]) + kExtendA] -= 1.0;
             ++j;
         }
     }
@@ -1347,9 +1361,12 @@ int orc_soft_batch(int gm, int am, int N, int K, const double* mat, const double
 int orc_hb_batch(int prec, int pmax, int cutoff, int N, const double* mat, const double* gaps,
                  const uint8_t* a, const int64_t* oa, const uint8_t* b, const int64_t* ob, int64_t n_pairs,
                  double* scores, double* grads, int32_t* guides, uint8_t* moves, int64_t moves_cap,
-                 int64_t* nmoves, int local, int32_t* ends, int linear) {
-    Model M{linear ? 0 : 1, local ? 1 : 0, N, 1, mat, gaps};
-    const size_t gs = size_t(N) * N + 4;
+                 int64_t* nmoves, int local, int32_t* ends, int linear, int K, const uint16_t* tracks,
+                 const uint16_t* gtracks) {
+    K = std::max(K, 1);
+    Model M{linear ? 0 : 1, local ? 1 : 0, N, K, mat, gaps};
+    const bool tracked = tracks != nullptr || gtracks != nullptr || K > 1;
+    const size_t gs = size_t(K) * N * N + 4 * size_t(K);
     for (int64_t p = 0; p < n_pairs; ++p) {
         const int m = int(oa[p + 1] - oa[p]), n = int(ob[p + 1] - ob[p]);
         HardOut o;
@@ -1359,8 +1376,10 @@ int orc_hb_batch(int prec, int pmax, int cutoff, int N, const double* mat, const
         o.moves = moves ? moves + moves_cap * p : nullptr;
         o.moves_cap = moves_cap;
         if (linear) {
-            if (prec == 32) lhb_one<float>(M, a + oa[p], m, b + ob[p], n, cutoff, o);
-            else            lhb_one<double>(M, a + oa[p], m, b + ob[p], n, cutoff, o);
+            const uint16_t* tk = tracks ? tracks + oa[p] : nullptr;
+            const uint16_t* gk = gtracks ? gtracks + oa[p] + p : nullptr;
+            if (prec == 32) lhb_one<float>(M, a + oa[p], m, b + ob[p], n, tk, gk, tracked, cutoff, o);
+            else            lhb_one<double>(M, a + oa[p], m, b + ob[p], n, tk, gk, tracked, cutoff, o);
         } else if (local) {
             if (prec == 32) hb_local_one<float>(M, a + oa[p], m, b + ob[p], n, cutoff, pmax != 0, o);
             else            hb_local_one<double>(M, a + oa[p], m, b + ob[p], n, cutoff, pmax != 0, o);

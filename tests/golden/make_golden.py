@@ -173,6 +173,28 @@ def hb_fixtures():
                         out[key + "scores"] = r["scores"]
                         out[key + "grads"] = r["grads"]
                         out[key + "guides"] = r["guides"]
+    # tracked linear: three parameter sets picked per residue of A, gap sets per DP row
+    K = 3
+    mat = rng.integers(-4, 4, size=(K, 20, 20)).astype(np.float64)
+    for k in range(K):
+        mat[k][np.diag_indices(20)] = rng.integers(4, 12, size=20)
+    gaps = np.array([[11.0, 1.0, 11.0, 1.0], [9.0, 2.0, 10.0, 1.5], [12.0, 0.5, 8.0, 2.0]])
+    sa = ["".join(rng.choice(list(AA), size=int(rng.integers(1, 400)))) for _ in range(16)]
+    sb = ["".join(c if rng.random() > 0.25 else str(rng.choice(list(AA))) for c in s) if k % 2 else
+          "".join(rng.choice(list(AA), size=int(rng.integers(1, 400)))) for k, s in enumerate(sa)]
+    tr = np.concatenate([rng.integers(0, K, size=len(s)) for s in sa]).astype(np.uint16)
+    gt = np.concatenate([rng.integers(0, K, size=len(s) + 1) for s in sa]).astype(np.uint16)
+    out["trk_mat"], out["trk_gaps"], out["trk_sa"], out["trk_sb"] = mat, gaps, np.array(sa), np.array(sb)
+    out["trk_tracks"], out["trk_gap_tracks"] = tr, gt
+    for prec in (32, 64):
+        for cut in (8, 64):
+            for am, tag in ((0, "linT_"), (1, "linLT_")):
+                r = oracle.ref_run(prec, 0, am, 1, AA, mat, gaps, sa, sb, tracks=tr, gap_tracks=gt,
+                                   traceback="hirschberg", hb_cutoff=cut)
+                key = f"trk_{tag}hirschberg_{prec}_c{cut}_"
+                out[key + "scores"] = r["scores"]
+                out[key + "grads"] = r["grads"]
+                out[key + "guides"] = r["guides"]
     np.savez_compressed(os.path.join(HERE, "hirschberg.npz"), **out)
     print("hirschberg.npz:", len(out), "arrays")
 

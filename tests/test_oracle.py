@@ -126,6 +126,22 @@ def test_hirschberg_fixtures():
                         np.testing.assert_array_equal(o["guides"], z[key + "guides"])
 
 
+def test_hirschberg_tracked_linear_fixtures():
+    """Linear Hirschberg with three parameter sets (per-residue tracks, per-row gap tracks)
+    against the reference's own engine (tests/golden/hirschberg.npz, trk_*)."""
+    z = np.load(os.path.join(GOLD, "hirschberg.npz"))
+    sa, sb = [str(s) for s in z["trk_sa"]], [str(s) for s in z["trk_sb"]]
+    enc = oracle.Encoded(encode(AA, sa), encode(AA, sb), z["trk_tracks"], z["trk_gap_tracks"])
+    for prec in (32, 64):
+        for cut in (8, 64):
+            for local, tag in ((False, "linT_"), (True, "linLT_")):
+                key = f"trk_{tag}hirschberg_{prec}_c{cut}_"
+                o = oracle.hirschberg(prec, z["trk_mat"], z["trk_gaps"], enc, cutoff=cut, local=local, linear=True)
+                np.testing.assert_array_equal(o["scores"], z[key + "scores"])
+                np.testing.assert_array_equal(o["grads"], z[key + "grads"])
+                np.testing.assert_array_equal(o["guides"], z[key + "guides"])
+
+
 def test_soft_banded_fixtures():
     """The guide-banded soft restatement against the reference's own engine
     (tests/golden/soft_banded.npz): guides from the Viterbi pass under the first parameters,
