@@ -281,14 +281,15 @@ class SeqPairBatch:
 
     def _check_hirschberg(self):
         """Hirschberg splits pairs longer than hb_cutoff rows; this build implements the split
-        for untracked batches, affine or linear, Global or Local (the reference's
-        viterbi_affine_hirschberg, viterbi_affine_hirschberg_local, viterbi_linear_hirschberg)."""
-        if not self._tracked:
+        for untracked batches, affine or linear, and tracked linear ones, Global or Local (the
+        reference's viterbi_affine_hirschberg, viterbi_affine_hirschberg_local,
+        viterbi_linear_hirschberg); tracked affine splits are not built."""
+        if not self._tracked or self._gap_model == "linear":
             return
         if self._n and int(np.max(np.diff(self._oa))) > self._hb_cutoff:
             raise NotImplementedError(
                 f"nwgrad_b200: traceback=\"{self._traceback}\" splits pairs longer than hb_cutoff only for "
-                f"untracked batches in this build (this batch: {self._gap_model} {self._mode}"
+                f"untracked batches and tracked linear ones in this build (this batch: {self._gap_model} {self._mode}"
                 f"{', tracked' if self._tracked else ''}); use traceback=\"pointers\" or \"auto\"")
 
     @property

@@ -667,14 +667,17 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
     const bool band = J.band >= 0;
     // Hirschberg (untracked, full DP): pairs longer than the cutoff split (Local: by the
     // endpoint scans and their box)
-    const bool hb = !band && !tr && (J.traceback == 3 || J.traceback == 4);
+    const bool hb = !band && (!tr || !aff) && (J.traceback == 3 || J.traceback == 4);
     const int hb_cut = hb ? (J.hb_cutoff > 0 ? J.hb_cutoff : 512) : 0;
     std::vector<int32_t> hb_pairs;
     if (hb) {
         for (int64_t p = 0; p < s->n; ++p)
             if (s->oa[p + 1] - s->oa[p] > hb_cut) hb_pairs.push_back(int32_t(p));
         // non-negative penalties (hb_penalties_ok_, aligner.hpp:5747-5763): linear, the extends
-        const bool ok = s->gaps[1] >= 0.0 && s->gaps[3] >= 0.0 && (!aff || (s->gaps[0] >= 0.0 && s->gaps[2] >= 0.0));
+        bool ok = true;
+        for (int k = 0; k < s->K; ++k)
+            ok = ok && s->gaps[4 * k + 1] >= 0.0 && s->gaps[4 * k + 3] >= 0.0 &&
+                 (!aff || (s->gaps[4 * k] >= 0.0 && s->gaps[4 * k + 2] >= 0.0));
         if (!hb_pairs.empty() && !ok)
             throw Error(NWG_EINVAL, "nwgrad: traceback=\"hirschberg\" / \"hirschberg_pmax\" needs non-negative "
                                     "gap penalties (got a negative one); use traceback=\"pointers\" or \"auto\"");
@@ -860,6 +863,11 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
         H.h_pairs = hb_pairs.data(); H.n_pairs = int64_t(hb_pairs.size());
         H.h_oa = s->oa.data(); H.h_ob = s->ob.data();
         H.cutoff = hb_cut; H.pmax = J.traceback == 4; H.local = loc ? 1 : 0; H.linear = aff ? 0 : 1;
+        H.K = s->K; H.gaps_t = gapT.p;
+        if (tr) {   // linear, tracked (the fill's border set-up gave every tracked store its tracks)
+            H.tracks = s->tracks.as<uint16_t>();
+            H.gtracks = s->gtracks.p ? s->gtracks.as<uint16_t>() : nullptr;
+        }
         try {
             s->last_launches += nwg::hb_run(H, int(sizeof(T)), st, sms);
         } catch (const std::runtime_error& e) {

@@ -56,6 +56,8 @@ struct SweepJob {
 struct BaseJob {
     int64_t a_base, b_base;          // row t >= 1 reads a[a_base + t - 1]; column c >= 1 b[b_base + c - 1]
     int H, W, in_x, out_x;
+    int i0, pad;                     // linear, tracked: the DP row of the block's row 0
+    int64_t tk_off, gk_off;          // linear, tracked: the pair's track offsets (oa[p], oa[p] + p)
     int64_t codes;                   // byte offset of the (H + 1) x (W + 1) code table
     int64_t bnd;                     // T offset of the stripe boundary row (3 (W + 1))
     int64_t moves;                   // byte offset of the moves (walk order, H + W at most)
@@ -68,6 +70,17 @@ struct ScanJob {
 };
 
 template <class T> struct Gaps { T go_a, ge_a, go_b, ge_b; };
+
+// Per-row linear parameters of a tracked pair: the substitution row, the extend of a gap in B
+// into DP row i (its residue's set) and of a gap in A within DP row i (its gap set).
+template <class T>
+struct LinRows {
+    const uint16_t* tk; const uint16_t* gk; const T* gaps; int N;
+    __device__ __forceinline__ int tset(int i) const { return int(tk[i - 1]); }
+    __device__ __forceinline__ int gset(int i) const { return gk ? int(gk[i]) : (i == 0 ? int(tk[0]) : int(tk[i - 1])); }
+    __device__ __forceinline__ T ga(int i) const { return gaps[4 * gset(i) + 1]; }
+    __device__ __forceinline__ T gb(int i) const { return gaps[4 * tset(i) + 3]; }
+};
 
 template <class T>
 __device__ __forceinline__ T chain_y(T lm, T lx, T ly, const Gaps<T>& g) {
@@ -495,7 +508,11 @@ __global__ void hb_replay_kernel(const HbRun P, const BaseJob* __restrict__ jobs
     const T go_a = static_cast<T>(P.go_a), ge_a = static_cast<T>(P.ge_a);
     const T go_b = static_cast<T>(P.go_b), ge_b = static_cast<T>(P.ge_b);
     double* g = P.grad ? P.grad + P.gstride * p : nullptr;
-    const int64_t NN = int64_t(N) * N;
+    // tracked (linear): each row's substitution set and extends
+    const bool trk = P.linear && P.tracks != nullptr;
+    const LinRows<T> LR{P.tracks + (trk ? ao : 0), P.gtracks ? P.gtracks + ao + p : nullptr,
+                        static_cast<const T*>(P.gaps_t), N};
+    const int64_t NN = int64_t(trk ? P.K : 1) * N * N;
     int32_t* gj = P.guide ? P.guide + ao + p : nullptr;
     // Local: the path runs from its box's start (is, js) to its end (ie, je); Global: (0, 0)
     // to (m, n)
@@ -515,20 +532,22 @@ __global__ void hb_replay_kernel(const HbRun P, const BaseJob* __restrict__ jobs
             const int op = mv[e];
             if (op == 0) {
                 ++i; ++j;
-                const int64_t cell = int64_t(ap[i - 1]) * N + bp[j - 1];
+                const int64_t cell = (int64_t(trk ? LR.tset(i) : 0) * N + ap[i - 1]) * N + bp[j - 1];
                 s += mat[cell];
                 if (g) g[cell] += 1.0;
                 if (gj) gj[i] = j;
             } else if (op == 1) {
                 ++i;
                 if (!P.linear && prev != 1) { s -= go_b; if (g) g[NN + 2] -= 1.0; }
-                s -= ge_b;
-                if (g) g[NN + 3] -= 1.0;
+                const int64_t o = NN + 4 * int64_t(trk ? LR.tset(i) : 0);
+                s -= trk ? LR.gb(i) : ge_b;
+                if (g) g[o + 3] -= 1.0;
                 if (gj) gj[i] = j;
             } else {
                 if (!P.linear && prev != 2) { s -= go_a; if (g) g[NN + 0] -= 1.0; }
-                s -= ge_a;
-                if (g) g[NN + 1] -= 1.0;
+                const int64_t o = NN + 4 * int64_t(trk ? LR.gset(i) : 0);
+                s -= trk ? LR.ga(i) : ge_a;
+                if (g) g[o + 1] -= 1.0;
                 ++j;
             }
             if (keep) keep[total - 1 - idx] = uint8_t(op);   // walk order: end to start
@@ -569,17 +588,25 @@ struct LhbJob {
     int a_step, b_step;
     int H, W;
     int64_t out;                     // MODE 0: T offset of the last row (W + 1)
+    // tracked: row t >= 1 is DP row i = i_base + i_step t (its substitution set and the
+    // extend of a gap into it); its gaps in A lie in DP row i (forward) or i - 1 (reverse:
+    // the suffix from row i - 1), row 0's on row i_base (forward) or i_base - 1 (reverse)
+    int i_base, i_step;
+    int64_t tk_off, gk_off;
 };
+
 
 template <class T, int R, int MODE>
 __global__ void __launch_bounds__(128) lhb_kernel(const uint8_t* __restrict__ a, const uint8_t* __restrict__ b,
-                                                  const T* __restrict__ mat, int N, T ga, T gb,
+                                                  const T* __restrict__ mat, int N, int K, T ga_u, T gb_u,
+                                                  const uint16_t* __restrict__ tracks, const uint16_t* __restrict__ gtracks,
+                                                  const T* __restrict__ gaps_t,
                                                   const LhbJob* __restrict__ jobs, int n_jobs, T* rows,
                                                   int64_t row_stride, T* __restrict__ out,
                                                   int32_t* __restrict__ res) {
     extern __shared__ __align__(16) unsigned char hb_smem[];
     T* smat = reinterpret_cast<T*>(hb_smem);
-    for (int k = threadIdx.x; k < N * N; k += blockDim.x) smat[k] = mat[k];
+    for (int k = threadIdx.x; k < K * N * N; k += blockDim.x) smat[k] = mat[k];
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const int wpb = blockDim.x >> 5;
@@ -590,15 +617,19 @@ __global__ void __launch_bounds__(128) lhb_kernel(const uint8_t* __restrict__ a,
     for (int64_t jb = wg; jb < n_jobs; jb += nwarps) {
         const LhbJob J = jobs[jb];
         const int H = J.H, W = J.W;
+        const bool trk = tracks != nullptr;
+        const LinRows<T> LR{tracks + (trk ? J.tk_off : 0), gtracks ? gtracks + J.gk_off : nullptr, gaps_t, N};
+        const int gshift = J.i_step < 0 ? 1 : 0;   // reverse: row i's gaps in A on row i - 1
+        const T ga0 = trk ? LR.ga(J.i_base - gshift) : ga_u;
         T bv = T(0); int bi = 0, bj = 0;
         if constexpr (MODE == 2) {
             // row 0 (the end cell's row) seeds the best, its columns visited from W down: the
             // chain 0, -ga, -2ga, ... never rises (ga >= 0: Hirschberg needs non-negative
             // penalties), so the first largest is column 0, or column W when ga is 0
-            bv = T(0); bi = 0; bj = (ga > T(0)) ? 0 : W;
+            bv = T(0); bi = 0; bj = (ga0 > T(0)) ? 0 : W;
         }
         if (MODE == 0 && H == 0) {   // no rows: row 0 is the last
-            if (lane == 0) { T v = T(0); out[J.out] = v; for (int c = 1; c <= W; ++c) { v = v - ga; out[J.out + c] = v; } }
+            if (lane == 0) { T v = T(0); out[J.out] = v; for (int c = 1; c <= W; ++c) { v = v - ga0; out[J.out + c] = v; } }
         }
         if (H > 0) {
             const int nst = (H + 32 * R - 1) / (32 * R);
@@ -607,12 +638,19 @@ __global__ void __launch_bounds__(128) lhb_kernel(const uint8_t* __restrict__ a,
                 const int i0 = s * 32 * R + lane * R + 1;
                 int code[R];
                 bool valid[R];
-                T cur[R];
+                T cur[R], rga[R], rgb[R];
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
                     const int i = i0 + r;
                     valid[r] = i <= H;
-                    code[r] = valid[r] ? int(a[J.a_base + int64_t(J.a_step) * (i - 1)]) * N : 0;
+                    const int ac = valid[r] ? int(a[J.a_base + int64_t(J.a_step) * (i - 1)]) : 0;
+                    rga[r] = ga_u; rgb[r] = gb_u;
+                    code[r] = ac * N;
+                    if (trk && valid[r]) {
+                        const int di = J.i_base + J.i_step * i;   // the DP row
+                        code[r] = (LR.tset(di) * N + ac) * N;
+                        rga[r] = LR.ga(di - gshift); rgb[r] = LR.gb(di);
+                    }
                     cur[r] = T(0);
                 }
                 T dg = T(0), up = T(0);       // row above at column c - 1, c
@@ -625,7 +663,7 @@ __global__ void __launch_bounds__(128) lhb_kernel(const uint8_t* __restrict__ a,
                     if (lane == 0 && c <= W) {
                         if (s == 0) {
                             if (c == 0 || LOC) up = T(0);
-                            else up = r0 - ga;
+                            else up = r0 - ga0;
                             r0 = up;
                         } else {
                             up = nu;
@@ -639,10 +677,10 @@ __global__ void __launch_bounds__(128) lhb_kernel(const uint8_t* __restrict__ a,
                         for (int r = 0; r < R; ++r) {
                             T v;
                             if (c == 0) {
-                                v = LOC ? T(0) : q - gb;
+                                v = LOC ? T(0) : q - rgb[r];
                             } else {
                                 v = pd + smat[code[r] + bc];
-                                const T u = q - gb, l = cur[r] - ga;
+                                const T u = q - rgb[r], l = cur[r] - rga[r];
                                 if (v < u) v = u;
                                 if (v < l) v = l;
                                 if constexpr (LOC) v = (v < T(0)) ? T(0) : v;
@@ -719,13 +757,15 @@ __global__ void lhb_join_kernel(const LhbJob* __restrict__ jobs, int n_blocks, c
 // Global borders into a row-major code table, walked back from its corner by lane 0.
 template <class T, int R>
 __global__ void __launch_bounds__(128) lhb_base_kernel(const uint8_t* __restrict__ a, const uint8_t* __restrict__ b,
-                                                       const T* __restrict__ mat, int N, T ga, T gb,
+                                                       const T* __restrict__ mat, int N, int K, T ga_u, T gb_u,
+                                                       const uint16_t* __restrict__ tracks,
+                                                       const uint16_t* __restrict__ gtracks, const T* __restrict__ gaps_t,
                                                        const BaseJob* __restrict__ jobs, int n_jobs,
                                                        uint8_t* __restrict__ codes, T* __restrict__ bnds,
                                                        uint8_t* __restrict__ moves, int32_t* __restrict__ nmoves) {
     extern __shared__ __align__(16) unsigned char hb_smem[];
     T* smat = reinterpret_cast<T*>(hb_smem);
-    for (int k = threadIdx.x; k < N * N; k += blockDim.x) smat[k] = mat[k];
+    for (int k = threadIdx.x; k < K * N * N; k += blockDim.x) smat[k] = mat[k];
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const int wpb = blockDim.x >> 5;
@@ -733,6 +773,9 @@ __global__ void __launch_bounds__(128) lhb_base_kernel(const uint8_t* __restrict
         const BaseJob J = jobs[jb];
         const int H = J.H, W = J.W;
         const int64_t st = int64_t(W) + 1;
+        const bool trk = tracks != nullptr;
+        const LinRows<T> LR{tracks + (trk ? J.tk_off : 0), gtracks ? gtracks + J.gk_off : nullptr, gaps_t, N};
+        const T ga0 = trk ? LR.ga(J.i0) : ga_u;
         uint8_t* D = codes + J.codes;
         T* bnd = bnds + J.bnd;
         if (lane == 0) { D[0] = 3; for (int c = 1; c <= W; ++c) D[c] = 2; }
@@ -741,11 +784,18 @@ __global__ void __launch_bounds__(128) lhb_base_kernel(const uint8_t* __restrict
             for (int s = 0; s < nst; ++s) {
                 const int i0 = s * 32 * R + lane * R + 1;
                 int code[R];
-                T cur[R];
+                T cur[R], rga[R], rgb[R];
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
                     const int i = i0 + r;
-                    code[r] = i <= H ? int(a[J.a_base + i - 1]) * N : 0;
+                    const int ac = i <= H ? int(a[J.a_base + i - 1]) : 0;
+                    code[r] = ac * N;
+                    rga[r] = ga_u; rgb[r] = gb_u;
+                    if (trk && i <= H) {
+                        const int di = J.i0 + i;
+                        code[r] = (LR.tset(di) * N + ac) * N;
+                        rga[r] = LR.ga(di); rgb[r] = LR.gb(di);
+                    }
                     cur[r] = T(0);
                 }
                 T dg = T(0), up = T(0), r0 = T(0), nu = T(0);
@@ -754,7 +804,7 @@ __global__ void __launch_bounds__(128) lhb_base_kernel(const uint8_t* __restrict
                 for (int t = 0; t < S; ++t) {
                     const int c = t - lane;
                     if (lane == 0 && c <= W) {
-                        if (s == 0) { up = c == 0 ? T(0) : r0 - ga; r0 = up; }
+                        if (s == 0) { up = c == 0 ? T(0) : r0 - ga0; r0 = up; }
                         else { up = nu; if (c < W) nu = bnd[c + 1]; }
                     }
                     if (c >= 0 && c <= W) {
@@ -765,11 +815,11 @@ __global__ void __launch_bounds__(128) lhb_base_kernel(const uint8_t* __restrict
                             const int i = i0 + r;
                             T v;
                             uint8_t k;
-                            if (c == 0) { v = q - gb; k = 1; }
+                            if (c == 0) { v = q - rgb[r]; k = 1; }
                             else {
                                 v = pd + smat[code[r] + bc];
                                 k = 0;
-                                const T u = q - gb, l = cur[r] - ga;
+                                const T u = q - rgb[r], l = cur[r] - rga[r];
                                 if (v < u) { v = u; k = 1; }
                                 if (v < l) { v = l; k = 2; }
                             }
@@ -1022,8 +1072,15 @@ int64_t lhb_run_t(const HbRun& P, cudaStream_t st, int sms) {
     constexpr int R = 4;
     const T ga = static_cast<T>(P.ge_a), gb = static_cast<T>(P.ge_b);
     const T* mat = static_cast<const T*>(P.mat);
-    const size_t mat_bytes = size_t((P.N * P.N + 3) & ~3) * sizeof(T);
+    const bool trk = P.tracks != nullptr;
+    const int K = trk ? std::max(P.K, 1) : 1;
+    const T* gaps_t = static_cast<const T*>(P.gaps_t);
+    const size_t mat_bytes = size_t((K * P.N * P.N + 3) & ~3) * sizeof(T);
     Tmp djobs(st), dout(st), drows(st), dres(st), dboxes(st);
+    auto track_offs = [&](LhbJob& J, int p, int i_base, int i_step) {
+        J.i_base = i_base; J.i_step = i_step;
+        J.tk_off = P.h_oa[p]; J.gk_off = P.h_oa[p] + p;
+    };
     const int wpb = 4;
     // one launch of lhb_kernel<MODE> over jobs (MODE 0: rows out; else results back to the host)
     auto launch = [&](int mode, const std::vector<LhbJob>& jobs, T* o, std::vector<int32_t>* res) {
@@ -1038,7 +1095,8 @@ int64_t lhb_run_t(const HbRun& P, cudaStream_t st, int sms) {
         int32_t* rs = res ? static_cast<int32_t*>(dres.get(jobs.size() * 3 * sizeof(int32_t))) : nullptr;
         auto fn = mode == 0 ? lhb_kernel<T, R, 0> : mode == 1 ? lhb_kernel<T, R, 1> : lhb_kernel<T, R, 2>;
         HB_CUDA(allow_smem(reinterpret_cast<const void*>(fn), mat_bytes));
-        fn<<<grid, 32 * wpb, mat_bytes, st>>>(P.a, P.b, mat, P.N, ga, gb, dj, int(jobs.size()), rw, stride, o, rs);
+        fn<<<grid, 32 * wpb, mat_bytes, st>>>(P.a, P.b, mat, P.N, K, ga, gb, trk ? P.tracks : nullptr,
+                                              trk ? P.gtracks : nullptr, gaps_t, dj, int(jobs.size()), rw, stride, o, rs);
         HB_CUDA(cudaGetLastError());
         launches++;
         if (res) {
@@ -1062,6 +1120,7 @@ int64_t lhb_run_t(const HbRun& P, cudaStream_t st, int sms) {
             LhbJob J{};
             J.a_base = P.h_oa[p]; J.a_step = 1; J.b_base = P.h_ob[p]; J.b_step = 1;
             J.H = int(P.h_oa[p + 1] - P.h_oa[p]); J.W = int(P.h_ob[p + 1] - P.h_ob[p]);
+            track_offs(J, p, 0, 1);
             jf.push_back(J);
         }
         std::vector<int32_t> fr, rr;
@@ -1075,6 +1134,7 @@ int64_t lhb_run_t(const HbRun& P, cudaStream_t st, int sms) {
             LhbJob J{};
             J.a_base = P.h_oa[p] + ie - 1; J.a_step = -1; J.b_base = P.h_ob[p] + je - 1; J.b_step = -1;
             J.H = ie; J.W = je;
+            track_offs(J, p, ie + 1, -1);
             jr.push_back(J);
             rk.push_back(k);
         }
@@ -1102,9 +1162,11 @@ int64_t lhb_run_t(const HbRun& P, cudaStream_t st, int sms) {
             LhbJob& F = jobs[2 * s];
             F.a_base = P.h_oa[p] + B.i0; F.a_step = 1; F.b_base = P.h_ob[p] + B.j0; F.b_step = 1;
             F.H = mid - B.i0; F.W = W;
+            track_offs(F, p, B.i0, 1);
             LhbJob& Rv = jobs[2 * s + 1];
             Rv.a_base = P.h_oa[p] + B.i1 - 1; Rv.a_step = -1; Rv.b_base = P.h_ob[p] + B.j1 - 1; Rv.b_step = -1;
             Rv.H = B.i1 - mid; Rv.W = W;
+            track_offs(Rv, p, B.i1 + 1, -1);
             F.out = out_off; out_off += int64_t(W) + 1;
             Rv.out = out_off; out_off += int64_t(W) + 1;
         }
@@ -1145,6 +1207,7 @@ int64_t lhb_run_t(const HbRun& P, cudaStream_t st, int sms) {
         BaseJob& J = bj[q];
         J.a_base = P.h_oa[p] + B.i0; J.b_base = P.h_ob[p] + B.j0;
         J.H = B.i1 - B.i0; J.W = B.j1 - B.j0; J.in_x = 0; J.out_x = 0;
+        J.i0 = B.i0; J.pad = 0; J.tk_off = P.h_oa[p]; J.gk_off = P.h_oa[p] + p;
         J.codes = code_off; code_off += ((int64_t(J.H) + 1) * (int64_t(J.W) + 1) + 15) & ~int64_t(15);
         J.bnd = bnd_off; bnd_off += int64_t(J.W) + 1;
         J.moves = mv_off; mv_off += int64_t(J.H) + J.W + 1;
@@ -1163,8 +1226,9 @@ int64_t lhb_run_t(const HbRun& P, cudaStream_t st, int sms) {
     const int grid = int(std::min<int64_t>((int64_t(bj.size()) + wpb - 1) / wpb, int64_t(sms) * 8));
     if (grid > 0) {
         HB_CUDA(allow_smem(reinterpret_cast<const void*>(lhb_base_kernel<T, R>), mat_bytes));
-        lhb_base_kernel<T, R><<<grid, 32 * wpb, mat_bytes, st>>>(P.a, P.b, mat, P.N, ga, gb, dB, int(bj.size()), cd, bd,
-                                                                 mvd, nm);
+        lhb_base_kernel<T, R><<<grid, 32 * wpb, mat_bytes, st>>>(P.a, P.b, mat, P.N, K, ga, gb, trk ? P.tracks : nullptr,
+                                                                 trk ? P.gtracks : nullptr, gaps_t, dB, int(bj.size()),
+                                                                 cd, bd, mvd, nm);
         HB_CUDA(cudaGetLastError());
         launches++;
     }

@@ -26,6 +26,11 @@ struct HbRun {
     int pmax;                                  // the closed-form prefix-max horizontal carry
     int local;                                 // Local: endpoint scans, then the box's global solve
     int linear;                                // linear gaps (one state; pmax does not apply)
+    // linear, tracked: K sets (mat K x N x N, gaps_t K x 4 in T), per residue of A its set,
+    // per DP row its gap set (oa[p] + p offsets; null: the residue's set)
+    int K;
+    const void* gaps_t;
+    const uint16_t* tracks; const uint16_t* gtracks;
 };
 
 // Runs P on stream st (synchronising it); returns the number of kernel launches.  Throws

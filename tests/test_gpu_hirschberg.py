@@ -70,6 +70,51 @@ def test_long_pairs_against_the_oracle(prec, pmax, mode, gap_model):
     assert np.array_equal(gj, o["guides"])
 
 
+@pytest.mark.parametrize("prec", [32, 64])
+@pytest.mark.parametrize("cut", [8, 64])
+@pytest.mark.parametrize("mode", ["global", "local"])
+def test_tracked_linear_reference_fixtures(prec, cut, mode):
+    """Linear Hirschberg with three parameter sets (per-residue tracks, per-row gap tracks)
+    against the reference's own engine (tests/golden/hirschberg.npz, trk_*)."""
+    z = np.load(os.path.join(GOLD, "hirschberg.npz"))
+    sa, sb = [str(s) for s in z["trk_sa"]], [str(s) for s in z["trk_sb"]]
+    cls = nw.SeqPairBatch if prec == 32 else nw.SeqPairBatchDouble
+    b = cls(sa, sb, nw.AlignParams.from_arrays(z["trk_mat"], z["trk_gaps"], alphabet=AA), grad_mode="hard",
+            traceback="hirschberg", mode=mode, gap_model="linear", tracks=z["trk_tracks"],
+            gap_tracks=z["trk_gap_tracks"])
+    b.hb_cutoff = cut
+    b.score_and_grad()
+    gm, gg = b.grads()
+    flat = np.concatenate([gm.reshape(len(sa), -1), gg.reshape(len(sa), -1)], axis=1)
+    key = f"trk_{'linLT_' if mode == 'local' else 'linT_'}hirschberg_{prec}_c{cut}_"
+    assert np.array_equal(b.scores(), z[key + "scores"]), np.nonzero(b.scores() != z[key + "scores"])[0][:5]
+    assert np.array_equal(flat, z[key + "grads"])
+    assert np.array_equal(b.guides(), z[key + "guides"])
+
+
+@pytest.mark.parametrize("mode", ["global", "local"])
+def test_tracked_linear_long_pairs_against_the_oracle(mode):
+    rng = np.random.default_rng(2300 + (mode == "local"))
+    K = 3
+    mat = rand_matrix(rng, 20, K, integer=False)
+    gaps = rng.uniform(0.3, 3.0, size=(K, 4))
+    sa = rand_seqs(rng, 5, 1000, 4000, AA) + rand_seqs(rng, 6, 1, 300, AA)
+    sb = [mutate(rng, s, AA) if k % 3 else rand_seqs(rng, 1, 500, 3000, AA)[0] for k, s in enumerate(sa)]
+    tr = np.concatenate([rng.integers(0, K, size=len(s)) for s in sa]).astype(np.uint16)
+    gt = np.concatenate([rng.integers(0, K, size=len(s) + 1) for s in sa]).astype(np.uint16)
+    b = nw.SeqPairBatch(sa, sb, nw.AlignParams.from_arrays(mat, gaps, alphabet=AA), grad_mode="hard",
+                        traceback="hirschberg", mode=mode, gap_model="linear", tracks=tr, gap_tracks=gt)
+    b.hb_cutoff = 200
+    b.score_and_grad()
+    gm, gg = b.grads()
+    flat = np.concatenate([gm.reshape(len(sa), -1), gg.reshape(len(sa), -1)], axis=1)
+    o = oracle.hirschberg(32, mat, gaps, oracle.Encoded(encode(AA, sa), encode(AA, sb), tr, gt), cutoff=200,
+                          local=mode == "local", linear=True)
+    assert np.array_equal(b.scores(), o["scores"]), np.nonzero(b.scores() != o["scores"])[0][:5]
+    assert np.array_equal(flat, o["grads"]), np.nonzero((flat != o["grads"]).any(1))[0][:5]
+    assert np.array_equal(b.guides(), o["guides"])
+
+
 def test_score_matches_pointers_and_banded_follows():
     """Where the optimum is unique Hirschberg and Pointers agree; banded re-alignment then
     runs around the Hirschberg guide."""
