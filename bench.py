@@ -457,6 +457,7 @@ def main():
               for _ in range(args.steps)]
         kernel_ms = 0.0
         launches = 0
+        cap0 = pos.graph_stats()[0] + neg.graph_stats()[0]
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize()
@@ -483,6 +484,8 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
         step_ms = [e[0].elapsed_time(e[1]) for e in ev]
+        if clk:
+            clk.captures = pos.graph_stats()[0] + neg.graph_stats()[0] - cap0   # graphs captured while timed
         total_ms = float(np.sum(step_ms))
         if dist is not None:
             t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local}")
@@ -578,7 +581,7 @@ def main():
             "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
             "plain_fill": plain, "serve": serve,
             "autotune": {str(k): _tune_mod().describe(v) for k, v in tune_table.items()},
-            "step_ms": step_ms}))
+            "step_ms": step_ms, "graph_captures_timed": getattr(clk, "captures", None)}))
     if dist is not None:
         dist.destroy_process_group()
 

@@ -48,10 +48,10 @@ def lib():
         L = C.CDLL(path)
         L.orc_hard_batch.argtypes = [C.c_int] * 5 + [_dp, _dp, _u8p, _i64p, _u8p, _i64p, C.c_int64,
                                                       _u16p, _u16p, C.c_int, _i32p, C.c_int,
-                                                      _dp, _dp, _i32p, _u8p, C.c_int64, _i64p, _i32p]
+                                                      _dp, _dp, _i32p, _u8p, C.c_int64, _i64p, _i32p, C.c_int]
         L.orc_hard_batch.restype = C.c_int
         L.orc_soft_batch.argtypes = [C.c_int] * 4 + [_dp, _dp, _u8p, _i64p, _u8p, _i64p, C.c_int64,
-                                                      _u16p, _u16p, C.c_double, _dp, _dp, _i32p, C.c_int]
+                                                      _u16p, _u16p, C.c_double, _dp, _dp, _i32p, C.c_int, C.c_int]
         L.orc_soft_batch.restype = C.c_int
         L.orc_hb_batch.argtypes = [C.c_int] * 4 + [_dp, _dp, _u8p, _i64p, _u8p, _i64p, C.c_int64,
                                                     _dp, _dp, _i32p, _u8p, C.c_int64, _i64p, C.c_int, _i32p, C.c_int,
@@ -89,8 +89,9 @@ class Encoded:
 
 
 def hard(prec, gm, am, mat, gaps, enc: Encoded, tracked=False, guides_in=None, band=-1,
-         moves_cap=0):
-    """Viterbi (Pointers semantics) + traceback + hard gradient for every pair.
+         moves_cap=0, free_ends=12):
+    """Viterbi (Pointers semantics) + traceback + hard gradient for every pair.  am: 0 global,
+    1 local, 2 semi-global with `free_ends` (1 a_begin, 2 a_end, 4 b_begin, 8 b_end; 12 glocal).
 
     Returns dict(scores (n,), grads (n, K*N*N + 4K), guides (sum(m+1),), ends (n, 4)
     [end_i, end_j, start_i, start_j], moves (n, moves_cap) walk order, nmoves (n,)).
@@ -113,7 +114,7 @@ def hard(prec, gm, am, mat, gaps, enc: Encoded, tracked=False, guides_in=None, b
                           _p(enc.tracks, _u16p), _p(enc.gap_tracks, _u16p), int(bool(tracked)),
                           _p(gi, _i32p), int(band), _p(scores, _dp), _p(grads, _dp),
                           _p(guides, _i32p), _p(moves, _u8p), int(moves_cap), _p(nmoves, _i64p),
-                          _p(ends, _i32p))
+                          _p(ends, _i32p), int(free_ends))
     assert rc == 0
     return dict(scores=scores, grads=grads, guides=guides, ends=ends, moves=moves, nmoves=nmoves)
 
@@ -148,7 +149,7 @@ def hirschberg(prec, mat, gaps, enc: Encoded, cutoff=512, pmax=False, moves_cap=
     return dict(scores=scores, grads=grads, guides=guides, moves=moves, nmoves=nmoves, ends=ends)
 
 
-def soft(gm, am, mat, gaps, enc: Encoded, temperature=1.0, guides_in=None, band=-1):
+def soft(gm, am, mat, gaps, enc: Encoded, temperature=1.0, guides_in=None, band=-1, free_ends=12):
     """Log-space double forward-backward: (scores = T log Z, grads = expected counts); with
     guides_in and band >= 0 the guide-banded one."""
     L = lib()
@@ -163,7 +164,7 @@ def soft(gm, am, mat, gaps, enc: Encoded, temperature=1.0, guides_in=None, band=
                           _p(enc.tracks, _u16p), _p(enc.gap_tracks, _u16p), float(temperature),
                           _p(scores, _dp), _p(grads, _dp),
                           _p(None if guides_in is None else np.ascontiguousarray(guides_in, np.int32), _i32p),
-                          int(band))
+                          int(band), int(free_ends))
     assert rc == 0
     return scores, grads
 
@@ -187,7 +188,8 @@ class _Problem(C.Structure):
                 ("a", C.c_char_p), ("oa", _i64p), ("b", C.c_char_p), ("ob", _i64p),
                 ("tracks", _u16p), ("gtracks", _u16p), ("traceback", C.c_int), ("kernel", C.c_int),
                 ("n_threads", C.c_int), ("temperature", C.c_double), ("soft_impl", C.c_int),
-                ("soft_f32", C.c_int), ("hb_cutoff", C.c_int), ("inter_fill", C.c_int)]
+                ("soft_f32", C.c_int), ("hb_cutoff", C.c_int), ("inter_fill", C.c_int),
+                ("free_ends", C.c_int)]
 
 
 def ref_available(simd=False):
@@ -214,7 +216,8 @@ _TB = {"auto": 0, "pointers": 1, "scores": 2, "hirschberg": 3, "hirschberg_pmax"
 
 
 def _problem(prec, gm, am, grad_mode, alphabet, mat, gaps, seqs_a, seqs_b, tracks, gap_tracks,
-             traceback, kernel, n_threads, temperature, soft_impl, soft_f32, hb_cutoff, inter_fill):
+             traceback, kernel, n_threads, temperature, soft_impl, soft_f32, hb_cutoff, inter_fill,
+             free_ends=12):
     keep = []
     mat = np.ascontiguousarray(mat, np.float64)
     gaps = np.ascontiguousarray(gaps, np.float64)
@@ -232,21 +235,21 @@ def _problem(prec, gm, am, grad_mode, alphabet, mat, gaps, seqs_a, seqs_b, track
     P = _Problem(prec, gm, am, grad_mode, mat.shape[1], mat.shape[0], _p(mat, _dp), _p(gaps, _dp),
                  alpha, len(seqs_a), a, _p(oa, _i64p), b, _p(ob, _i64p), _p(tk, _u16p),
                  _p(gk, _u16p), _TB[traceback], kernel, n_threads, float(temperature),
-                 soft_impl, int(soft_f32), hb_cutoff, int(inter_fill))
+                 soft_impl, int(soft_f32), hb_cutoff, int(inter_fill), int(free_ends))
     return P, keep, oa
 
 
 def ref_run(prec, gm, am, grad_mode, alphabet, mat, gaps, seqs_a, seqs_b, tracks=None,
             gap_tracks=None, traceback="pointers", kernel=-1, n_threads=1, temperature=1.0,
             soft_impl=0, soft_f32=True, hb_cutoff=0, inter_fill=True, band=-1, mat2=None,
-            gaps2=None, simd=False):
+            gaps2=None, simd=False, free_ends=12):
     """Run the reference batch once; returns dict(scores, grads, guides, total)."""
     L = ref_lib(simd)
     if n_threads <= 0:
         n_threads = physical_cores()
     P, keep, oa = _problem(prec, gm, am, grad_mode, alphabet, mat, gaps, seqs_a, seqs_b, tracks,
                            gap_tracks, traceback, kernel, n_threads, temperature, soft_impl,
-                           soft_f32, hb_cutoff, inter_fill)
+                           soft_f32, hb_cutoff, inter_fill, free_ends)
     K, N = np.asarray(mat).shape[0], np.asarray(mat).shape[1]
     n = len(seqs_a)
     scores = np.zeros(n, np.float64)

@@ -8,6 +8,9 @@
 //   Viterbi, affine, Pointers codes ........ aligner.hpp:3955-4071 (viterbi_affine_ptr_impl)
 //   Viterbi, linear, Pointers codes ........ aligner.hpp:3756-3860 (viterbi_linear_ptr_impl)
 //   Local end cell (first row-major max) ... aligner.hpp:5975-5984 (local_row_best_)
+//   semi-global ends (glocal, overlap, free_ends): free row 0 / column 0 starts, end cells
+//   column n then row m, first strict max ..... aligner.hpp:3984-4071, 6100-6230 (SgEnd),
+//                                            soft borders / ends / gap targets 6362-6430, 6309-6319
 //   affine walk + hard gradient ............ aligner.hpp:2985-3056, 3177-3230
 //   linear walk + hard gradient ............ aligner.hpp:2852-2900 (walk_linear_impl), 3886-3925
 //   guide_j and its gap interpolation ...... aligner.hpp:3155-3160, 2734-2749
@@ -37,10 +40,30 @@ enum Tbl : uint8_t { TM = 0, TX = 1, TY = 2 };
 
 struct Model {
     int gm;            // 0 linear, 1 affine
-    int am;            // 0 global, 1 local
+    int am;            // 0 global, 1 local, 2 semi-global (free ends `sg`)
     int N, K;
     const double* mat;   // K*N*N
     const double* gaps;  // K*4
+    int sg = 12;         // am 2: free ends, 1 a_begin (column 0 a start), 2 a_end (column n ends),
+                         // 4 b_begin (row 0 a start), 8 b_end (row m ends); glocal is 12
+    bool semi() const { return am == 2; }
+    bool free_row0() const { return am == 1 || (am == 2 && (sg & 4)); }
+    bool free_col0() const { return am == 2 && (sg & 1); }
+    bool end_col() const { return am == 2 && (sg & 2); }
+    bool end_row() const { return am == 2 && (sg & 8); }
+};
+
+// The semi-global end (aligner.hpp:6160-6170, SgEnd): candidates offered in order, the
+// first of the maxima kept (strict >), its state by M > X > Y.
+template <class T>
+struct SgEnd {
+    T best = T(0); int i = -1, j = 0; Tbl t = TM;
+    void offer(int ci, int cj, T vm, T vx, T vy) {
+        const T v = (vm < vx ? vx : vm) < vy ? vy : (vm < vx ? vx : vm);
+        if (i >= 0 && !(v > best)) return;
+        best = v; i = ci; j = cj;
+        t = (vm >= vx && vm >= vy) ? TM : (vx >= vy ? TX : TY);
+    }
 };
 
 template <class T> inline T ninf() { return -std::numeric_limits<T>::infinity(); }
@@ -197,15 +220,18 @@ void affine_fill(const Model& M, const Rows<T>& R, const uint8_t* b, int m, int 
         return vm >= mx(vx, vy) ? uint8_t(0) : kxy;
     };
     const T go_a0 = R.goa[0], ge_a0 = R.gea[0];
+    const bool free0 = M.free_row0(), freec = M.free_col0();
     for (int j = 0; j <= n; ++j) {
-        if (local) { pM[j] = 0; pX[j] = ninf<T>(); pY[j] = ninf<T>(); }
+        if (free0) { pM[j] = 0; pX[j] = ninf<T>(); pY[j] = ninf<T>(); }
         else {
             pM[j] = (j == 0) ? T(0) : ninf<T>();
             pX[j] = ninf<T>();
             pY[j] = (j == 0) ? ninf<T>() : -(go_a0 + static_cast<T>(j) * ge_a0);
         }
-        D[j] = (j <= 1 || local) ? 3 : (3 | 2 << 4);
+        D[j] = (j <= 1 || free0) ? 3 : (3 | 2 << 4);
     }
+    SgEnd<T> sge;
+    if (M.end_col() && m > 0) sge.offer(0, n, pM[n], pX[n], pY[n]);
     bi = 0; bj = 0; bt = TM;
     T best_local = T(0);
     for (int i = 1; i <= m; ++i) {
@@ -216,6 +242,7 @@ void affine_fill(const Model& M, const Rows<T>& R, const uint8_t* b, int m, int 
         else { cM[0] = ninf<T>(); cX[0] = R.bx0[i]; }
         cY[0] = ninf<T>();
         d[0] = (i <= 1) ? 3 : (3 | 1 << 2);
+        if (freec) { cM[0] = 0; cX[0] = ninf<T>(); d[0] = 3; }
         T rowmax = T(0);
         for (int j = 1; j <= n; ++j) {
             const T dgM = pM[j - 1], dgX = pX[j - 1], dgY = pY[j - 1];
@@ -242,9 +269,14 @@ void affine_fill(const Model& M, const Rows<T>& R, const uint8_t* b, int m, int 
             const T vm = cM[j], vx = cX[j], vy = cY[j];
             bt = (vm >= vx && vm >= vy) ? TM : (vx >= vy ? TX : TY);
         }
+        if (M.end_col() && i < m) sge.offer(i, n, cM[n], cX[n], cY[n]);
         std::swap(pM, cM); std::swap(pX, cX); std::swap(pY, cY);
     }
-    if (!local) {
+    if (M.semi()) {   // row m (every column with a free B end, else (m, n)), after column n's
+        if (M.end_row()) { for (int j = 0; j <= n; ++j) sge.offer(m, j, pM[j], pX[j], pY[j]); }
+        else sge.offer(m, n, pM[n], pX[n], pY[n]);
+        score = sge.best; bi = sge.i; bj = sge.j; bt = sge.t;
+    } else if (!local) {
         const T vm = pM[n], vx = pX[n], vy = pY[n];
         score = mx3(vm, vx, vy);
         bi = m; bj = n;
@@ -269,8 +301,16 @@ void affine_walk(const Model& M, const std::vector<uint8_t>& D, int n, int bi, i
             c = D[size_t(i) * st + j];
             if (tbl == TM && (c & 3) == 3) break;
         } else {
-            if (i == 0) { for (; j > 0; --j) sink.emit(TY, 0, j, j == 1); break; }
-            if (j == 0) { for (; i > 0; --i) sink.emit(TX, i, 0, i == 1); break; }
+            if (i == 0) {
+                if (M.free_row0()) break;   // row 0: a free start
+                for (; j > 0; --j) sink.emit(TY, 0, j, j == 1);
+                break;
+            }
+            if (j == 0) {
+                if (M.free_col0()) break;   // column 0: a free start
+                for (; i > 0; --i) sink.emit(TX, i, 0, i == 1);
+                break;
+            }
             c = D[size_t(i) * st + j];
         }
         if (i == 0) tbl = TY;
@@ -304,19 +344,23 @@ void linear_fill(const Model& M, const Rows<T>& R, const uint8_t* b, int m, int 
     D.assign(size_t(m + 1) * st, 0);
     std::vector<T> prev(st), cur(st);
     const T ge_a0 = R.gea[0];
+    const bool free0 = M.free_row0(), freec = M.free_col0();
     prev[0] = T(0); D[0] = 3;
     for (int j = 1; j <= n; ++j) {
-        prev[j] = local ? T(0) : -static_cast<T>(j) * ge_a0;
-        D[j] = local ? 3 : 2;
+        prev[j] = free0 ? T(0) : -static_cast<T>(j) * ge_a0;
+        D[j] = free0 ? 3 : 2;
     }
+    const T NI = ninf<T>();
+    SgEnd<T> sge;
+    if (M.end_col() && m > 0) sge.offer(0, n, prev[n], NI, NI);
     bi = 0; bj = 0;
     T best_local = T(0);
     for (int i = 1; i <= m; ++i) {
         uint8_t* d = D.data() + size_t(i) * st;
         const T* prow = matT + size_t(R.rs[i - 1]) * M.N;
         const T ge_a = R.gea[i], ge_b = R.geb[i];
-        cur[0] = local ? T(0) : R.bx0[i];
-        d[0] = local ? 3 : 1;
+        cur[0] = (local || freec) ? T(0) : R.bx0[i];
+        d[0] = (local || freec) ? 3 : 1;
         for (int j = 1; j <= n; ++j) {
             const T d0 = prev[j - 1] + prow[b[j - 1]];
             const T u = prev[j] - ge_b;
@@ -337,7 +381,14 @@ void linear_fill(const Model& M, const Rows<T>& R, const uint8_t* b, int m, int 
             cur[j] = v; d[j] = c;
             left = v;
         }
+        if (M.end_col() && i < m) sge.offer(i, n, cur[n], NI, NI);
         std::swap(prev, cur);
+    }
+    if (M.semi()) {
+        if (M.end_row()) { for (int j = 0; j <= n; ++j) sge.offer(m, j, prev[j], NI, NI); }
+        else sge.offer(m, n, prev[n], NI, NI);
+        score = sge.best; bi = sge.i; bj = sge.j;
+        return;
     }
     score = local ? best_local : prev[n];
     if (!local) { bi = m; bj = n; }
@@ -606,6 +657,19 @@ void setup_drows(DRows& R, const Model& M, const uint8_t* a, int m, const uint16
 
 struct SoftOut { double logz = 0; double* grad = nullptr; };
 
+// Semi-global end cells, each once (aligner.hpp:6190-6196): row m's band (a free B end) or
+// (m, n), then column n of rows 0..m-1 (a free A end).
+template <class F>
+void for_end_cells(const Model& M, int m, int n, const Band& bd, F&& f) {
+    if (M.end_row()) { for (int j = bd.jlo0(m); j <= bd.jhi0(m); ++j) f(m, j); }
+    else f(m, n);
+    if (M.end_col()) for (int i = 0; i < m; ++i) f(i, n);
+}
+// The first row / column a gap move may target and be counted (aligner.hpp:6309-6319): a
+// free start's border cells are constants, not the targets of gap moves.
+int gap_min_j(const Model& M) { return M.am == 1 ? 1 : (M.free_col0() ? 1 : 0); }
+int gap_min_i(const Model& M) { return M.am == 0 ? 0 : (M.am == 1 ? 1 : ((M.sg & 4) ? 1 : 0)); }
+
 // Band bd (full when bd.band < 0): the guide-banded forward-backward (aligner.hpp:6362-6524
 // with AlignBand::GuideBanded): forward cells j in [jlo(i), jhi(i)], borders limited to
 // border_rows / border_cols (Global), Local log Z over [jlo0(i), jhi0(i)], backward sources
@@ -625,7 +689,9 @@ void soft_affine(const Model& M, const uint8_t* a, int m, const uint8_t* b, int 
         FM[I(0, 0)] = 0.0;
         const int bi = bd.border_rows(), bj = bd.border_cols();
         for (int i = 1; i <= bi; ++i) FX[I(i, 0)] = R.bx0[i];
-        for (int j = 1; j <= bj; ++j) FY[I(0, j)] = -(R.goa[0] + double(j) * R.gea[0]);
+        if (M.free_row0()) { for (int j = 0; j <= n; ++j) FM[I(0, j)] = 0.0; }   // a free start
+        else for (int j = 1; j <= bj; ++j) FY[I(0, j)] = -(R.goa[0] + double(j) * R.gea[0]);
+        if (M.free_col0()) for (int i = 1; i <= m; ++i) { FM[I(i, 0)] = 0.0; FX[I(i, 0)] = NI; }
     } else {
         for (int i = 0; i <= m; ++i) FM[I(i, 0)] = 0.0;
         for (int j = 0; j <= n; ++j) FM[I(0, j)] = 0.0;
@@ -641,14 +707,18 @@ void soft_affine(const Model& M, const uint8_t* a, int m, const uint8_t* b, int 
             FM[I(i, j)] = mv; FX[I(i, j)] = xv; FY[I(i, j)] = yv;
         }
     double lz;
-    if (!local) lz = lse3(FM[I(m, n)], FX[I(m, n)], FY[I(m, n)]);
+    if (M.semi()) {   // the end cells (sg_for_end_cells_, aligner.hpp:6190-6196)
+        lz = NI;
+        for_end_cells(M, m, n, bd, [&](int i, int j) { lz = lse2(lz, lse3(FM[I(i, j)], FX[I(i, j)], FY[I(i, j)])); });
+    } else if (!local) lz = lse3(FM[I(m, n)], FX[I(m, n)], FY[I(m, n)]);
     else {
         lz = NI;
         for (int i = 0; i <= m; ++i) for (int j = bd.jlo0(i); j <= bd.jhi0(i); ++j)
             lz = lse2(lz, lse3(FM[I(i, j)], FX[I(i, j)], FY[I(i, j)]));
     }
     std::vector<double> BM(cells, local ? 0.0 : NI), BX(BM), BY(BM);
-    if (!local) { BM[I(m, n)] = 0; BX[I(m, n)] = 0; BY[I(m, n)] = 0; }
+    if (M.semi()) for_end_cells(M, m, n, bd, [&](int i, int j) { BM[I(i, j)] = 0; BX[I(i, j)] = 0; BY[I(i, j)] = 0; });
+    else if (!local) { BM[I(m, n)] = 0; BX[I(m, n)] = 0; BY[I(m, n)] = 0; }
     for (int i = m; i >= 0; --i)
         for (int j = bd.jhi0(i); j >= bd.jlo0(i); --j) {
             const double bm = BM[I(i, j)], bx = BX[I(i, j)], by = BY[I(i, j)];
@@ -674,7 +744,7 @@ void soft_affine(const Model& M, const uint8_t* a, int m, const uint8_t* b, int 
     const size_t NN = size_t(M.K) * M.N * M.N;
     double* g = o.grad;
     auto gap = [&](int set, int f) -> double& { return g[NN + 4 * size_t(set) + f]; };
-    const int gmin_j = local ? 1 : 0, gmin_i = local ? 1 : 0;
+    const int gmin_j = gap_min_j(M), gmin_i = gap_min_i(M);
     for (int i = 1; i <= m; ++i)
         for (int j = bd.jlo(i); j <= bd.jhi(i); ++j) {
             const double bm = BM[I(i, j)];
@@ -725,7 +795,9 @@ void soft_linear(const Model& M, const uint8_t* a, int m, const uint8_t* b, int 
         F[I(0, 0)] = 0.0;
         const int bi = bd.border_rows(), bj = bd.border_cols();
         for (int i = 1; i <= bi; ++i) F[I(i, 0)] = R.bx0[i];
-        for (int j = 1; j <= bj; ++j) F[I(0, j)] = -double(j) * R.gea[0];
+        if (M.free_row0()) { for (int j = 0; j <= n; ++j) F[I(0, j)] = 0.0; }   // a free start
+        else for (int j = 1; j <= bj; ++j) F[I(0, j)] = -double(j) * R.gea[0];
+        if (M.free_col0()) for (int i = 1; i <= m; ++i) F[I(i, 0)] = 0.0;
     } else {
         for (int i = 0; i <= m; ++i) F[I(i, 0)] = 0.0;
         for (int j = 0; j <= n; ++j) F[I(0, j)] = 0.0;
@@ -737,12 +809,16 @@ void soft_linear(const Model& M, const uint8_t* a, int m, const uint8_t* b, int 
             F[I(i, j)] = v;
         }
     double lz;
-    if (!local) lz = F[I(m, n)];
+    if (M.semi()) {
+        lz = NI;
+        for_end_cells(M, m, n, bd, [&](int i, int j) { lz = lse2(lz, F[I(i, j)]); });
+    } else if (!local) lz = F[I(m, n)];
     else {
         lz = NI;
         for (int i = 0; i <= m; ++i) for (int j = bd.jlo0(i); j <= bd.jhi0(i); ++j) lz = lse2(lz, F[I(i, j)]);
     }
-    if (!local) B[I(m, n)] = 0.0;
+    if (M.semi()) for_end_cells(M, m, n, bd, [&](int i, int j) { B[I(i, j)] = 0.0; });
+    else if (!local) B[I(m, n)] = 0.0;
     for (int i = m; i >= 0; --i)
         for (int j = bd.jhi0(i); j >= bd.jlo0(i); --j) {
             const double bv = B[I(i, j)];
@@ -754,7 +830,7 @@ void soft_linear(const Model& M, const uint8_t* a, int m, const uint8_t* b, int 
     const size_t NN = size_t(M.K) * M.N * M.N;
     double* g = o.grad;
     auto gap = [&](int set, int f) -> double& { return g[NN + 4 * size_t(set) + f]; };
-    const int gmin_j = local ? 1 : 0, gmin_i = local ? 1 : 0;
+    const int gmin_j = gap_min_j(M), gmin_i = gap_min_i(M);
     for (int i = 1; i <= m; ++i)
         for (int j = bd.jlo(i); j <= bd.jhi(i); ++j) {
             const double bv = B[I(i, j)];
@@ -1303,8 +1379,8 @@ int orc_hard_batch(int prec, int gm, int am, int N, int K, const double* mat, co
                    int64_t n_pairs, const uint16_t* tracks, const uint16_t* gtracks, int tracked,
                    const int32_t* guides_in, int band,
                    double* scores, double* grads, int32_t* guides,
-                   uint8_t* moves, int64_t moves_cap, int64_t* nmoves, int32_t* ends) {
-    Model M{gm, am, N, K, mat, gaps};
+                   uint8_t* moves, int64_t moves_cap, int64_t* nmoves, int32_t* ends, int free_ends) {
+    Model M{gm, am, N, K, mat, gaps, free_ends};
     const size_t gs = size_t(K) * N * N + 4 * size_t(K);
     for (int64_t p = 0; p < n_pairs; ++p) {
         const int m = int(oa[p + 1] - oa[p]), n = int(ob[p + 1] - ob[p]);
@@ -1336,8 +1412,9 @@ int orc_hard_batch(int prec, int gm, int am, int N, int K, const double* mat, co
 int orc_soft_batch(int gm, int am, int N, int K, const double* mat, const double* gaps,
                    const uint8_t* a, const int64_t* oa, const uint8_t* b, const int64_t* ob,
                    int64_t n_pairs, const uint16_t* tracks, const uint16_t* gtracks,
-                   double temperature, double* scores, double* grads, const int32_t* guides_in, int band) {
-    Model M{gm, am, N, K, mat, gaps};
+                   double temperature, double* scores, double* grads, const int32_t* guides_in, int band,
+                   int free_ends) {
+    Model M{gm, am, N, K, mat, gaps, free_ends};
     const size_t gs = size_t(K) * N * N + 4 * size_t(K);
     for (int64_t p = 0; p < n_pairs; ++p) {
         const int m = int(oa[p + 1] - oa[p]), n = int(ob[p + 1] - ob[p]);
@@ -1346,7 +1423,7 @@ int orc_soft_batch(int gm, int am, int N, int K, const double* mat, const double
         std::fill(o.grad, o.grad + gs, 0.0);
         const uint16_t* tk = tracks ? tracks + oa[p] : nullptr;
         const uint16_t* gk = gtracks ? gtracks + oa[p] + p : nullptr;
-        Band bd; bd.m = m; bd.n = n; bd.global = am == 0;
+        Band bd; bd.m = m; bd.n = n; bd.global = am != 1;
         if (guides_in && band >= 0) { bd.band = band; bd.g = guides_in + oa[p] + p; }
         if (gm == 0) soft_linear(M, a + oa[p], m, b + ob[p], n, tk, gk, temperature, o, bd);
         else         soft_affine(M, a + oa[p], m, b + ob[p], n, tk, gk, temperature, o, bd);

@@ -38,6 +38,7 @@ struct Problem {
     int soft_f32;    // float32 batch: float32 soft pass first
     int hb_cutoff;
     int inter_fill;  // fill="interpair"
+    int free_ends;   // am 2 (semi-global): kSgFree* bits (1 a_begin, 2 a_end, 4 b_begin, 8 b_end)
 };
 
 TracebackMode tb_of(int t) {
@@ -83,7 +84,7 @@ struct Run {
         const GradMode gd = P.grad_mode == 0 ? GradMode::None : P.grad_mode == 1 ? GradMode::Hard : GradMode::Soft;
         batch = std::make_unique<SeqPairBatchT<T>>(
             sa, sb, make_params(P), P.gm == 0 ? GapModel::Linear : GapModel::Affine,
-            P.am == 0 ? AlignMode::Global : AlignMode::Local, gd, P.n_threads, tb_of(P.traceback),
+            P.am == 0 ? AlignMode::Global : P.am == 1 ? AlignMode::Local : AlignMode::Glocal, gd, P.n_threads, tb_of(P.traceback),
             P.kernel, tk, gk);
         if (P.grad_mode == 2) {
             batch->set_soft_temperature(P.temperature);
@@ -91,6 +92,7 @@ struct Run {
                                  : P.soft_impl == 1 ? SoftImpl::ScaledOrLog : SoftImpl::Scaled);
             batch->set_soft_f32(P.soft_f32 != 0);
         }
+        if (P.am == 2) batch->set_free_ends(P.free_ends);
         if (P.hb_cutoff > 0) batch->set_hb_cutoff(P.hb_cutoff);
         batch->set_fill(false, P.inter_fill != 0);
     }

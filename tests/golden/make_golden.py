@@ -18,6 +18,8 @@ Two sources, both the reference's own code run here:
   (affine Global, small hb_cutoff so pairs split several times), float32 and float64.
 * ``soft_banded.npz`` -- SeqPairBatchT<double> soft (log space): score_and_grad, set_params,
   banded_grad(bw) around the Viterbi guides, every gap model and mode, bw 1, 3, 8.
+* ``semiglobal.npz`` -- the batch engine with AlignMode::Glocal and free_ends sets (glocal,
+  overlap, mixed): hard float32 / float64 with guides, soft log space at T = 1.
 """
 from __future__ import annotations
 
@@ -144,6 +146,65 @@ def ref_fixtures():
     print("reference_batches.npz:", len(out), "arrays")
 
 
+def sg_fixtures():
+    """Semi-global ends (mode "glocal" = b_begin + b_end, "overlap" = all four, and other
+    free_ends sets): hard at float32 / float64 with guides, soft (log space) at T = 1."""
+    rng = np.random.default_rng(77)
+    AA = "ACDEFGHIKLMNPQRSTVWY"
+    out = {}
+    cases = []
+    for name, alpha, K, n, lo, hi, integer in (("prot", AA, 1, 24, 0, 60, True),
+                                                ("protf", AA, 1, 16, 1, 50, False),
+                                                ("rna3", "ACGTU", 3, 24, 1, 40, False)):
+        N = len(alpha)
+        if integer:
+            mat = rng.integers(-4, 4, size=(K, N, N)).astype(np.float64)
+            for k in range(K):
+                mat[k][np.diag_indices(N)] = rng.integers(4, 12, size=N)
+            gaps = np.tile([11.0, 1.0, 11.0, 1.0], (K, 1))
+        else:
+            mat = rng.normal(0, 2, size=(K, N, N)).round(3)
+            gaps = rng.uniform(0.3, 4.0, size=(K, 4)).round(3)
+        sa = ["".join(rng.choice(list(alpha), size=int(rng.integers(lo, hi + 1)))) for _ in range(n)]
+        sb = ["".join(rng.choice(list(alpha), size=int(rng.integers(lo, hi + 1)))) for _ in range(n)]
+        tr = gt = None
+        if K > 1:
+            tr = np.concatenate([rng.integers(0, K, size=len(s)) for s in sa]).astype(np.uint16)
+            gt = np.concatenate([rng.integers(0, K, size=len(s) + 1) for s in sa]).astype(np.uint16)
+        cases.append((name, alpha, mat, gaps, sa, sb, tr, gt))
+    for name, alpha, mat, gaps, sa, sb, tr, gt in cases:
+        pre = f"{name}_"
+        out[pre + "alpha"] = np.array(alpha)
+        out[pre + "mat"] = mat
+        out[pre + "gaps"] = gaps
+        out[pre + "sa"] = np.array(sa)
+        out[pre + "sb"] = np.array(sb)
+        if tr is not None:
+            out[pre + "tracks"] = tr
+            out[pre + "gap_tracks"] = gt
+        for fe in SG_SETS:
+            for gm in (0, 1):
+                for prec in (32, 64):
+                    r = oracle.ref_run(prec, gm, 2, 1, alpha, mat, gaps, sa, sb, tracks=tr, gap_tracks=gt,
+                                       free_ends=fe)
+                    key = f"{pre}hard{prec}_g{gm}_e{fe}_"
+                    out[key + "scores"] = r["scores"]
+                    out[key + "grads"] = r["grads"]
+                    out[key + "guides"] = r["guides"]
+                r = oracle.ref_run(64, gm, 2, 2, alpha, mat, gaps, sa, sb, tracks=tr, gap_tracks=gt,
+                                   soft_impl=2, temperature=1.0, free_ends=fe)
+                key = f"{pre}soft_g{gm}_e{fe}_"
+                out[key + "scores"] = r["scores"]
+                out[key + "grads"] = r["grads"]
+    np.savez_compressed(os.path.join(HERE, "semiglobal.npz"), **out)
+    print("semiglobal.npz:", len(out), "arrays")
+
+
+# free_ends bit sets of the semi-global fixtures: glocal, overlap, and mixed ones
+# (1 a_begin, 2 a_end, 4 b_begin, 8 b_end)
+SG_SETS = (12, 15, 9, 6, 3, 0)
+
+
 def hb_fixtures():
     rng = np.random.default_rng(123)
     AA = "ACDEFGHIKLMNPQRSTVWY"
@@ -224,7 +285,7 @@ def soft_banded_fixtures():
 
 
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["brute", "ref", "hb", "sb"]
+    which = sys.argv[1:] or ["brute", "ref", "hb", "sb", "sg"]
     if "brute" in which:
         brute_fixtures()
     if "ref" in which:
@@ -233,3 +294,5 @@ if __name__ == "__main__":
         hb_fixtures()
     if "sb" in which:
         soft_banded_fixtures()
+    if "sg" in which:
+        sg_fixtures()

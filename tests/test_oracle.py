@@ -72,6 +72,34 @@ def test_reference_batch_fixtures(name):
                 np.testing.assert_allclose(g, z[key + "grads"], rtol=1e-9, atol=1e-10)
 
 
+SG_SETS = (12, 15, 9, 6, 3, 0)   # free_ends bits: 1 a_begin, 2 a_end, 4 b_begin, 8 b_end
+
+
+@pytest.mark.parametrize("name", ["prot", "protf", "rna3"])
+def test_semiglobal_fixtures(name):
+    """Semi-global ends (glocal, overlap, mixed free_ends) against the reference engine."""
+    z = np.load(os.path.join(GOLD, "semiglobal.npz"))
+    pre = name + "_"
+    alpha = str(z[pre + "alpha"])
+    sa, sb = [str(s) for s in z[pre + "sa"]], [str(s) for s in z[pre + "sb"]]
+    tr = z[pre + "tracks"] if pre + "tracks" in z.files else None
+    gt = z[pre + "gap_tracks"] if pre + "gap_tracks" in z.files else None
+    enc = oracle.Encoded(encode(alpha, sa), encode(alpha, sb), tr, gt)
+    mat, gaps = z[pre + "mat"], z[pre + "gaps"]
+    for fe in SG_SETS:
+        for gm in (0, 1):
+            for prec in (32, 64):
+                key = f"{pre}hard{prec}_g{gm}_e{fe}_"
+                o = oracle.hard(prec, gm, 2, mat, gaps, enc, tracked=tr is not None, free_ends=fe)
+                np.testing.assert_array_equal(o["scores"], z[key + "scores"], err_msg=key)
+                np.testing.assert_array_equal(o["grads"], z[key + "grads"], err_msg=key)
+                np.testing.assert_array_equal(o["guides"], z[key + "guides"], err_msg=key)
+            key = f"{pre}soft_g{gm}_e{fe}_"
+            s, g = oracle.soft(gm, 2, mat, gaps, enc, 1.0, free_ends=fe)
+            np.testing.assert_allclose(s, z[key + "scores"], rtol=1e-11, atol=1e-11, err_msg=key)
+            np.testing.assert_allclose(g, z[key + "grads"], rtol=1e-9, atol=1e-10, err_msg=key)
+
+
 def test_blocked_sum_order():
     """Blocks of 4096 in pair order, then the blocks in order (batch_engine.hpp:1788-1827)."""
     rng = np.random.default_rng(3)
