@@ -30,7 +30,7 @@ typedef struct nwg_store nwg_store;
 
 typedef struct nwg_job {
     int gap_model;     /* 0 linear, 1 affine */
-    int mode;          /* 0 global, 1 local */
+    int mode;          /* 0 global, 1 local, 2 semi-global (free_ends) */
     int grad_mode;     /* 0 none (score only), 1 hard, 2 soft */
     int precision;     /* 32 float32 DP, 64 float64 DP */
     int band;          /* -1: full DP; >= 1: guide-banded re-alignment of this half-width */
@@ -42,6 +42,11 @@ typedef struct nwg_job {
     int traceback;     /* hard, affine Global, untracked: 3 hirschberg, 4 hirschberg_pmax (pairs
                           longer than hb_cutoff rows split); anything else the Pointers path */
     int hb_cutoff;     /* Hirschberg base-case rows (>= 1; 0: 512) */
+    int free_ends;     /* mode 2 (semi-global, the reference's AlignMode::Glocal with kSgFree*
+                          bits, simd_levels.hpp:170-182): 1 a_begin (column 0 a free start),
+                          2 a_end (column n's cells ends), 4 b_begin (row 0 a free start),
+                          8 b_end (row m's cells ends); "glocal" is 12, "overlap" 15.  Full DP,
+                          traceback Pointers; banded re-alignment refused */
 } nwg_job;
 
 /* Last error message of the calling thread ("" if none). */

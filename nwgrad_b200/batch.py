@@ -19,7 +19,57 @@ from ._capi import Job, check, ptr
 from .params import AlignParams, Alphabet
 
 _GAP = {"linear": 0, "affine": 1}
-_MODE = {"global": 0, "local": 1}
+_MODE = {"global": 0, "local": 1, "glocal": 2, "overlap": 2, "semiglobal": 2}
+# semi-global free ends (the reference's kSgFree* bits, simd_levels.hpp:170-182)
+_SG_NAMES = ("a_begin", "a_end", "b_begin", "b_end")
+_SG_BITS = (1, 2, 4, 8)
+SG_GLOCAL, SG_ALL = 12, 15
+
+
+def parse_mode(mode, free_ends=None):
+    """(mode, free_ends) -> (mode name, align mode 0 global / 1 local / 2 semi-global, free-end
+    bits), with the reference's rules and messages (py_exports.cpp:276-335): "semiglobal" takes
+    free_ends -- four truth values (a_begin, a_end, b_begin, b_end) or the names of the free
+    ones; "glocal" is (b_begin, b_end), "overlap" all four; other modes refuse free_ends."""
+    if mode == "semiglobal":
+        if free_ends is None:
+            raise ValueError("nwgrad: mode \"semiglobal\" needs free_ends=(a_begin, a_end, b_begin, b_end)")
+        return mode, 2, _parse_free_ends(free_ends)
+    if free_ends is not None:
+        raise ValueError(f"nwgrad: free_ends= goes with mode \"semiglobal\" (got mode \"{mode}\", "
+                         f"whose ends are fixed)")
+    if mode == "overlap":
+        return mode, 2, SG_ALL
+    if mode == "glocal":
+        return mode, 2, SG_GLOCAL
+    if mode in ("global", "local"):
+        return mode, _MODE[mode], SG_GLOCAL
+    raise ValueError(f"nwgrad: unknown mode \"{mode}\" (expected \"global\", \"local\", \"glocal\", "
+                     f"\"overlap\" or \"semiglobal\")")
+
+
+def _parse_free_ends(h):
+    msg = ("nwgrad: free_ends must be four booleans (a_begin, a_end, b_begin, b_end) or the names of "
+           "the free ends (\"a_begin\", \"a_end\", \"b_begin\", \"b_end\")")
+    if isinstance(h, str):
+        h = (h,)
+    try:
+        items = list(h)
+    except TypeError:
+        raise ValueError(msg) from None
+    if not items:
+        return 0
+    if all(isinstance(x, str) for x in items):
+        f = 0
+        for nm in items:
+            if nm not in _SG_NAMES:
+                raise ValueError(f"nwgrad: unknown free end \"{nm}\" (expected \"a_begin\", \"a_end\", "
+                                 f"\"b_begin\" or \"b_end\")")
+            f |= _SG_BITS[_SG_NAMES.index(nm)]
+        return f
+    if len(items) != 4 or any(isinstance(x, str) for x in items):
+        raise ValueError(msg)
+    return sum(b for b, x in zip(_SG_BITS, items) if bool(x))
 _GRAD = {"none": 0, "hard": 1, "soft": 2}
 _TB = ("auto", "pointers", "scores", "hirschberg", "hirschberg_pmax", "grid")
 _KERNELS = ("auto", "scalar_fallback", "sse2", "sse4", "avx2", "avx512", "neon")
@@ -140,18 +190,13 @@ class SeqPairBatch:
             raise ValueError(f"nwgrad: n_threads must be >= 0 (0: the default thread count), got {n_threads}")
         if gap_model not in _GAP:
             raise ValueError(f"nwgrad: gap_model must be \"linear\" or \"affine\", got \"{gap_model}\"")
-        if mode not in _MODE:
-            if mode in ("glocal", "semiglobal", "overlap"):
-                raise NotImplementedError(f"nwgrad_b200: mode \"{mode}\" is not available in this build")
-            raise ValueError(f"nwgrad: unknown mode \"{mode}\"")
+        mode, self._am, self._sg = parse_mode(mode, free_ends)
         if grad_mode not in _GRAD:
             raise ValueError(f"nwgrad: unknown grad_mode \"{grad_mode}\"")
         if traceback not in _TB:
             raise ValueError(f"nwgrad: unknown traceback \"{traceback}\"")
         if kernel not in _KERNELS:
             raise ValueError(f"nwgrad: unknown kernel \"{kernel}\"")
-        if free_ends is not None:
-            raise ValueError("nwgrad: free_ends needs mode=\"semiglobal\"")
         self._n_threads = int(n_threads)
         self._traceback = traceback
         self._gap_model = gap_model
@@ -275,15 +320,24 @@ class SeqPairBatch:
         tb = {"hirschberg": 3, "hirschberg_pmax": 4}.get(self._traceback, 0)
         if tb and grad_mode != 2 and band < 0:
             self._check_hirschberg()
-        return Job(_GAP[self._gap_model], _MODE[self._mode], grad_mode, self._precision, band,
+        if self._am == 2 and band >= 0:
+            raise NotImplementedError(f"nwgrad_b200: banded re-alignment with mode \"{self._mode}\" "
+                                      f"(semi-global ends) is not available in this build")
+        return Job(_GAP[self._gap_model], self._am, grad_mode, self._precision, band,
                    int(bool(keep_paths)), float(self.soft_temperature), soft_double, lanes, rows,
-                   tb, int(self._hb_cutoff))
+                   tb, int(self._hb_cutoff), int(self._sg))
 
     def _check_hirschberg(self):
         """Hirschberg splits pairs longer than hb_cutoff rows; this build implements the split
         for untracked batches, affine or linear, and tracked linear ones, Global or Local (the
         reference's viterbi_affine_hirschberg, viterbi_affine_hirschberg_local,
         viterbi_linear_hirschberg); tracked affine splits are not built."""
+        if self._am == 2:
+            if self._n and int(np.max(np.diff(self._oa))) > self._hb_cutoff:
+                raise NotImplementedError(
+                    f"nwgrad_b200: traceback=\"{self._traceback}\" with mode \"{self._mode}\" (semi-global "
+                    f"ends) splits no pair in this build; use traceback=\"pointers\" or \"auto\"")
+            return
         if not self._tracked or self._gap_model == "linear":
             return
         if self._n and int(np.max(np.diff(self._oa))) > self._hb_cutoff:
@@ -475,7 +529,8 @@ class SeqPairBatch:
             raise ValueError("nwgrad: aligned_a / aligned_b need one gapped string per pair")
         tmp = type(self)(seqs_a, seqs_b, params, gap_model=self._gap_model, mode=self._mode,
                          grad_mode=self._grad_mode, traceback=self._traceback, tracks=tracks,
-                         gap_tracks=gap_tracks, device=self._device)
+                         gap_tracks=gap_tracks, device=self._device,
+                         free_ends=self.free_ends if self._mode == "semiglobal" else None)
         tmp.soft_temperature = self.soft_temperature
         tmp.soft_precision = self.soft_precision
         tmp._hb_cutoff = self._hb_cutoff
@@ -653,6 +708,14 @@ class SeqPairBatch:
         return self._mode
 
     @property
+    def free_ends(self):
+        """(a_begin, a_end, b_begin, b_end): which flanks are free; None for local."""
+        if self._am == 1:
+            return None
+        sg = self._sg if self._am == 2 else 0
+        return tuple(bool(sg & b) for b in _SG_BITS)
+
+    @property
     def grad_mode(self):
         return self._grad_mode
 
@@ -788,10 +851,10 @@ class SeqPair:
     """One pair: a view of pair i of a batch, or a standalone pair (a one-pair batch)."""
 
     def __init__(self, seq_a, seq_b, params, gap_model="affine", mode="global", grad_mode="hard",
-                 kernel="auto", traceback="auto", *, track=None, gap_track=None, device=None):
+                 kernel="auto", traceback="auto", *, track=None, gap_track=None, free_ends=None, device=None):
         cls = SeqPairBatchDouble if getattr(self, "_double", False) else SeqPairBatch
         self._batch = cls([seq_a], [seq_b], params, traceback=traceback, gap_model=gap_model, mode=mode,
-                          grad_mode=grad_mode, kernel=kernel,
+                          grad_mode=grad_mode, kernel=kernel, free_ends=free_ends,
                           tracks=None if track is None else [track],
                           gap_tracks=None if gap_track is None else [gap_track], device=device)
         self._i = 0
@@ -903,6 +966,10 @@ class SeqPair:
     @property
     def mode(self):
         return self._batch.mode
+
+    @property
+    def free_ends(self):
+        return self._batch.free_ends
 
     @property
     def grad_mode(self):

@@ -328,7 +328,7 @@ struct Bucket {
 
 struct Plan {
     bool valid = false;
-    int key_soft = -1, key_lanes = -1, key_rows = -1, key_band = -1, key_hb = -1;
+    int key_soft = -1, key_lanes = -1, key_rows = -1, key_band = -1, key_hb = -1, key_one_warp = -1;
     int64_t n_planned = 0;           // pairs in the buckets (hard: those not split by Hirschberg)
     std::vector<Bucket> buckets;
     std::vector<int64_t> code_off;   // hard: per pair
@@ -549,12 +549,14 @@ const T* ensure_bx0(nwg_store* s, bool aff, cudaStream_t st, bool& ok, DBuf& buf
 }
 
 // hb_cut > 0 (hard, full DP): pairs longer than hb_cut rows are left out (Hirschberg runs them).
+// one_warp (hard): no pair runs with several warps (the semi-global ends are one warp's).
 void build_plan(nwg_store* s, Plan& P, bool soft, int lanes, int rpl, int elem_bytes, bool band = false,
-                int hb_cut = 0) {
+                int hb_cut = 0, bool one_warp = false) {
     if (P.valid && P.key_soft == int(soft) && P.key_lanes == lanes && P.key_rows == rpl && P.key_band == int(band) &&
-        P.key_hb == hb_cut) return;
+        P.key_hb == hb_cut && P.key_one_warp == int(one_warp)) return;
     P.reset();
     P.key_soft = soft; P.key_lanes = lanes; P.key_rows = rpl; P.key_band = band; P.key_hb = hb_cut;
+    P.key_one_warp = one_warp;
     const int64_t n = s->n;
     // one lane per pair keeps a K*N*N histogram per lane in shared memory (soft)
     const bool lane_ok_soft = int64_t(s->K) * s->N * s->N * elem_bytes * 32 <= 48 * 1024;
@@ -577,7 +579,7 @@ void build_plan(nwg_store* s, Plan& P, bool soft, int lanes, int rpl, int elem_b
         if (!band && !lanes && !rpl) {
             if (s->plain) g = Geo{32, 4};
             else if (soft && !s->tracked() && rows >= kLongRows && nb >= 256) g = Geo{32, 4, false, long_warps(rows, 128)};
-            else if (!soft && rows >= kLongRows && nb >= 256) g = Geo{32, 8, false, long_warps(rows, 256)};
+            else if (!soft && !one_warp && rows >= kLongRows && nb >= 256) g = Geo{32, 8, false, long_warps(rows, 256)};
             else if (sc < kClasses && cost_of[sc]) {
                 double best = 1e300;
                 for (const auto& gc : *cost_of[sc]) {
@@ -664,10 +666,11 @@ void build_plan(nwg_store* s, Plan& P, bool soft, int lanes, int rpl, int elem_b
 template <class T>
 void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, bool want_guide) {
     const bool aff = J.gap_model == 1, loc = J.mode == 1, tr = s->tracked();
+    const int ends = J.mode == 2 ? J.free_ends : 0;   // semi-global free ends (0: Global's)
     const bool band = J.band >= 0;
     // Hirschberg (untracked, full DP): pairs longer than the cutoff split (Local: by the
     // endpoint scans and their box)
-    const bool hb = !band && (!tr || !aff) && (J.traceback == 3 || J.traceback == 4);
+    const bool hb = !band && J.mode != 2 && (!tr || !aff) && (J.traceback == 3 || J.traceback == 4);
     const int hb_cut = hb ? (J.hb_cutoff > 0 ? J.hb_cutoff : 512) : 0;
     std::vector<int32_t> hb_pairs;
     if (hb) {
@@ -683,7 +686,7 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
                                     "gap penalties (got a negative one); use traceback=\"pointers\" or \"auto\"");
     }
     Plan& P = band ? s->band_plan : s->hard_plan;
-    build_plan(s, P, false, band ? 32 : J.lanes, band ? 2 : J.rows, sizeof(T), band, hb_cut);
+    build_plan(s, P, false, band ? 32 : J.lanes, band ? 2 : J.rows, sizeof(T), band, hb_cut, ends != 0);
     s->codes.need(size_t(P.code_bytes), st);
     if (band) s->stripe_tab.need(size_t(std::max<int64_t>(P.n_stripes, 1)) * 16, st);
     const DBuf& matT = sizeof(T) == 4 ? s->matf : s->matd;
@@ -763,6 +766,7 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
         A.scratch_stride = stride;
         A.row_stride = 3 * (int64_t(B.maxn) + 1);
         A.score = s->score.as<double>(); A.end = s->end.as<int32_t>();
+        A.ends = ends;
         fills.push_back(make_launch(reinterpret_cast<const void*>(fn), unsigned(blocks), hblock, smem, A));
         fill_args.push_back(A);
     }
@@ -790,7 +794,7 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
     W.order = P.order.as<int32_t>(); W.n_items = P.n_planned;
     W.stripe_base = band ? P.stripe_base.as<int64_t>() : nullptr;
     W.stripe_tab = band ? s->stripe_tab.as<int64_t>() : nullptr;
-    W.N = s->N; W.K = s->K; W.affine = aff; W.local = loc;
+    W.N = s->N; W.K = s->K; W.affine = aff; W.local = loc; W.ends = ends;
     W.codes = s->codes.as<uint8_t>(); W.code_off = P.dcode_off.as<int64_t>();
     W.end = s->end.as<int32_t>();
     W.grad = want_grad ? s->grad.as<double>() : nullptr; W.gstride = s->gstride;
@@ -1040,6 +1044,7 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
         A.guide = J.band >= 0 ? s->guide.as<int32_t>() : nullptr; A.band = J.band;
         A.bnd_off = (mw ? gpb : 1) * warp_bytes;
         A.renorm_mask = renorm - 1;
+        A.ends = J.mode == 2 ? J.free_ends : 0;
         A.score = s->score.as<double>(); A.grad = s->grad.as<double>(); A.gstride = s->gstride;
         A.status = s->status.as<int32_t>();
         if (ovf) {
@@ -1282,8 +1287,14 @@ int nwg_run(nwg_store* s, const nwg_job* job, void* stream, double* total) {
         if (!s || !job) throw Error(NWG_EINVAL, "null argument");
         if (!s->K) throw Error(NWG_ESTATE, "params not set");
         const nwg_job J = *job;
-        if (J.gap_model < 0 || J.gap_model > 1 || J.mode < 0 || J.mode > 1 || J.grad_mode < 0 || J.grad_mode > 2)
+        if (J.gap_model < 0 || J.gap_model > 1 || J.mode < 0 || J.mode > 2 || J.grad_mode < 0 || J.grad_mode > 2)
             throw Error(NWG_EINVAL, "bad job");
+        if (J.mode == 2) {
+            if (J.free_ends < 0 || J.free_ends > 15)
+                throw Error(NWG_EINVAL, "nwgrad: free_ends must be a 4-bit flag set (0..15), got " + std::to_string(J.free_ends));
+            if (J.band >= 0)
+                throw Error(NWG_EINVAL, "nwgrad_b200: banded re-alignment with semi-global ends is not available");
+        }
         if (J.precision != 32 && J.precision != 64) throw Error(NWG_EINVAL, "precision must be 32 or 64");
         if (J.band >= 0 && !s->have_guides) throw Error(NWG_ESTATE, "banded_grad() needs a guide; call score_and_grad() first");
         NWG_CUDA(cudaSetDevice(s->device));

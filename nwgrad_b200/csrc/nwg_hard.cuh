@@ -53,6 +53,10 @@ struct HardArgs {
     // one warp per pair: lane 0 walks the pair's codes as soon as its fill is done
     int walk_fused;
     WalkArgs walk;
+    // semi-global free ends (Global kernels, full DP, one warp or lane per pair): 1 a_begin
+    // (column 0 a free start), 2 a_end (column n's cells ends), 4 b_begin (row 0 a free start),
+    // 8 b_end (row m's cells ends); 0: Global's charged borders and end (m, n)
+    int ends;
 };
 
 // The band of DP row i around guide g (aligner.hpp:2644-2700): columns [jlo, jhi].
@@ -78,6 +82,19 @@ __device__ __forceinline__ T border_col0(const HardArgs& A, const T* bx0p, int i
         else return mul_rn(-static_cast<T>(i), geb);
     }
 }
+
+// The first of the maxima among end candidates offered in order (strict >), its state by
+// M > X > Y (aligner.hpp:6160-6170, SgEnd).
+template <class T> struct EndPick {
+    T v; int i, j, st; bool any;
+    __device__ __forceinline__ void init() { v = T(0); i = 0; j = 0; st = 0; any = false; }
+    __device__ __forceinline__ void offer(int ci, int cj, T vm, T vx, T vy) {
+        const T w = rmax3(vm, vx, vy);
+        if (any && !(w > v)) return;
+        v = w; i = ci; j = cj; any = true;
+        st = (vm >= vx && vm >= vy) ? 0 : (vx >= vy ? 1 : 2);
+    }
+};
 
 // Shared memory beyond the parameters that several warps per pair use: per warp a best value,
 // its cell and state, and a progress counter.
@@ -161,10 +178,33 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
         };
         const T goa0 = sgap[4 * gset(0) + 0], gea0 = sgap[4 * gset(0) + 1];
         const T ugob = sgap[2], ugeb = sgap[3], ugoa = sgap[0], ugea = sgap[1];
+        const bool sg_r0 = !LOC && (A.ends & 4), sg_c0 = !LOC && (A.ends & 1);
+        const bool sg_ec = !LOC && (A.ends & 2), sg_er = !LOC && (A.ends & 8);
         if (m == 0 || n == 0) {
             if (lane == 0 && (!MW || gib == 0)) {
                 T sc; int ei, ej, st;
                 if (LOC) { sc = T(0); ei = 0; ej = 0; st = 0; }
+                else if (A.ends) {
+                    // semi-global: the border cells in the reference's order (column n of rows
+                    // 0..m-1, then row m), each from its closed form
+                    auto cell = [&](int ci, int cj, T& vm, T& vx, T& vy) {
+                        vm = ninf<T>(); vx = ninf<T>(); vy = ninf<T>();
+                        if (ci == 0 && (cj == 0 || sg_r0)) vm = T(0);
+                        else if (ci == 0) {
+                            if constexpr (AFF) vy = -add_rn(goa0, mul_rn(static_cast<T>(cj), gea0));
+                            else vm = mul_rn(-static_cast<T>(cj), gea0);
+                        } else if (sg_c0) vm = T(0);
+                        else {
+                            const T bc = border_col0<T, AFF, TR>(A, bx0p, ci, ugob, ugeb);
+                            if constexpr (AFF) vx = bc; else vm = bc;
+                        }
+                    };
+                    EndPick<T> e; e.init();
+                    T vm, vx, vy;
+                    if (sg_ec) for (int ci = 0; ci < m; ++ci) { cell(ci, n, vm, vx, vy); e.offer(ci, n, vm, vx, vy); }
+                    for (int cj = sg_er ? 0 : n; cj <= n; ++cj) { cell(m, cj, vm, vx, vy); e.offer(m, cj, vm, vx, vy); }
+                    sc = e.v; ei = e.i; ej = e.j; st = e.st;
+                }
                 else if (m == 0 && n == 0) { sc = T(0); ei = 0; ej = 0; st = 0; }
                 else if (m == 0) {
                     sc = AFF ? -add_rn(goa0, mul_rn(static_cast<T>(n), gea0)) : mul_rn(-static_cast<T>(n), gea0);
@@ -198,6 +238,25 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
 
         T bestv = T(0); int besti = 0, bestj = 0, bests = 0;   // Local: the first row-major max
         T endM = ninf<T>(), endX = ninf<T>(), endY = ninf<T>();
+        // semi-global: the first max of row m (from column 0's border cell) and of column n's
+        // rows 0..m-1 (from row 0's cell); the lane holding row m tracks the former
+        EndPick<T> erow, ecol;
+        erow.init(); ecol.init();
+        if (!LOC && A.ends) {
+            T vm, vx, vy;
+            if (sg_c0) { vm = T(0); vx = ninf<T>(); vy = ninf<T>(); }
+            else {
+                const T bc = border_col0<T, AFF, TR>(A, bx0p, m, ugob, ugeb);
+                vm = AFF ? ninf<T>() : bc; vx = AFF ? bc : ninf<T>(); vy = ninf<T>();
+            }
+            erow.offer(m, 0, vm, vx, vy);
+            if (sg_ec) {
+                if (sg_r0) { vm = T(0); vy = ninf<T>(); }
+                else if constexpr (AFF) { vm = ninf<T>(); vy = -add_rn(goa0, mul_rn(static_cast<T>(n), gea0)); }
+                else { vm = mul_rn(-static_cast<T>(n), gea0); vy = ninf<T>(); }
+                ecol.offer(0, n, vm, ninf<T>(), vy);
+            }
+        }
 
         const int S_full = n + G - 1;          // MW: steps per stripe (full DP)
         const int SP = S_full + 1;             // MW: progress key per stripe
@@ -252,6 +311,8 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
                 if constexpr (LOC) {
                     cM[r] = cmin == 1 ? T(0) : ninf<T>(); cX[r] = ninf<T>();
                     rbest[r] = T(0); rbj[r] = 0; rbs[r] = 0;
+                } else if (sg_c0 && cmin == 1) {
+                    cM[r] = T(0); cX[r] = ninf<T>();   // column 0 a free start
                 } else {
                     cM[r] = ninf<T>();
                     cX[r] = (valid && cmin == 1 && i <= brows) ? border_col0<T, AFF, TR>(A, bx0p, i, ugob, ugeb) : ninf<T>();
@@ -263,7 +324,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
             auto row0 = [&](int j, T& vM, T& vX, T& vY) {
                 vX = ninf<T>();
                 if constexpr (LOC) { vM = T(0); vY = ninf<T>(); }
-                else if (j == 0) { vM = T(0); vY = ninf<T>(); }
+                else if (j == 0 || sg_r0) { vM = T(0); vY = ninf<T>(); }
                 else if constexpr (AFF) {
                     vM = ninf<T>();
                     vY = j <= bcols ? -add_rn(goa0, mul_rn(static_cast<T>(j), gea0)) : ninf<T>();
@@ -277,7 +338,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
                 const int i = i0 - 1;
                 if (cmin == 1) {
                     if (i == 0) { dgM = T(0); dgX = ninf<T>(); dgY = ninf<T>(); }
-                    else if (LOC) { dgM = T(0); dgX = ninf<T>(); dgY = ninf<T>(); }
+                    else if (LOC || sg_c0) { dgM = T(0); dgX = ninf<T>(); dgY = ninf<T>(); }
                     else {
                         dgX = i <= brows ? border_col0<T, AFF, TR>(A, bx0p, i, ugob, ugeb) : ninf<T>();
                         dgM = AFF ? ninf<T>() : dgX; dgY = ninf<T>();
@@ -390,6 +451,12 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
                         for (int r = 0; r < R; ++r) dst[r] = uint8_t(w[r >> 2] >> (8 * (r & 3)));
                     }
                     dgM = upM; dgX = upX; dgY = upY;
+                    if (!LOC && sg_er) {
+                        const int zr = m - i0;
+#pragma unroll
+                        for (int r = 0; r < R; ++r)
+                            if (r == zr) erow.offer(m, j, cM[r], AFF ? cX[r] : ninf<T>(), AFF ? cY[r] : ninf<T>());
+                    }
                 }
                 // hand the bottom row to the next lane (and, from the last lane, to the next stripe)
                 if constexpr (G > 1) {
@@ -416,6 +483,26 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
 #pragma unroll
                     for (int r = 0; r < R; ++r)
                         if (i0 + r == m) { endM = cM[r]; endX = cX[r]; endY = cY[r]; }
+                }
+                if (sg_ec) {
+                    // column n of this stripe's rows below m, first max in row order: this
+                    // lane's, then the group's (the lowest row among equal maxima)
+                    EndPick<T> lc; lc.init();
+#pragma unroll
+                    for (int r = 0; r < R; ++r)
+                        if (i0 + r < m) lc.offer(i0 + r, n, cM[r], AFF ? cX[r] : ninf<T>(), AFF ? cY[r] : ninf<T>());
+                    if constexpr (G > 1) {
+#pragma unroll
+                        for (int off = 1; off < G; off <<= 1) {
+                            const T ov = __shfl_down_sync(gmask, lc.v, off, G);
+                            const int oi = __shfl_down_sync(gmask, lc.i, off, G);
+                            const int os = __shfl_down_sync(gmask, lc.st, off, G);
+                            const bool oa = __shfl_down_sync(gmask, lc.any ? 1 : 0, off, G) != 0;
+                            const bool take = (lane + off < G) && oa && (!lc.any || ov > lc.v);
+                            if (take) { lc.v = ov; lc.i = oi; lc.st = os; lc.any = true; }
+                        }
+                    }
+                    if (lc.any && (!ecol.any || lc.v > ecol.v)) { ecol.v = lc.v; ecol.i = lc.i; ecol.j = n; ecol.st = lc.st; ecol.any = true; }
                 }
             } else {
                 // this lane's first row-major best of the stripe, then the group's
@@ -482,14 +569,28 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
                 endX = __shfl_sync(gmask, endX, src, G);
                 endY = __shfl_sync(gmask, endY, src, G);
             }
+            if (A.ends && sg_er) {
+                // row m's first max: held by the lane of row m
+                const int src = ((m - 1) % GR) / R;
+                if constexpr (G > 1) {
+                    erow.v = __shfl_sync(gmask, erow.v, src, G);
+                    erow.j = __shfl_sync(gmask, erow.j, src, G);
+                    erow.st = __shfl_sync(gmask, erow.st, src, G);
+                }
+            }
             if (lane == 0 && (!MW || gib == (nstripes - 1) % NWp)) {
-                T sc; int st;
+                T sc; int st, ei = m, ej = n;
                 if constexpr (AFF) {
                     sc = rmax3(endM, endX, endY);
                     st = (endM >= endX && endM >= endY) ? 0 : (endX >= endY ? 1 : 2);
                 } else { sc = endM; st = 0; }
+                if (A.ends) {
+                    // semi-global: column n's rows 0..m-1 were offered first, then row m
+                    if (sg_er) { sc = erow.v; ej = erow.j; st = erow.st; }
+                    if (sg_ec && ecol.any && !(sc > ecol.v)) { sc = ecol.v; ei = ecol.i; ej = n; st = ecol.st; }
+                }
                 A.score[p] = static_cast<double>(sc);
-                A.end[4 * p] = m; A.end[4 * p + 1] = n; A.end[4 * p + 2] = st;
+                A.end[4 * p] = ei; A.end[4 * p + 1] = ej; A.end[4 * p + 2] = st;
                 A.end[4 * p + 3] = (G << 8) | R;
             }
             if constexpr (MW) __syncthreads();

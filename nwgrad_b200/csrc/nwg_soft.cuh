@@ -7,7 +7,9 @@
 // Y(i,j) = (M + X)(i,j-1) o_a(i) + Y(i,j-1) e_a(i), M(i,j) = (M+X+Y)(i-1,j-1) w(a_i, b_j),
 // with o = exp(-(go+ge)/T), e = exp(-ge/T), w = exp(s/T); Local has no gap move into a border
 // cell.  Z = (M+X+Y)(m,n) (Global) or the sum over every cell (Local); backward B the mirror
-// recurrence seeded with 1 at (m,n) (Global) or at every cell (Local).  The expected count
+// recurrence seeded with 1 at (m,n) (Global) or at every cell (Local).  Semi-global ends
+// (`ends`, Global kernels): free starts of weight 1 on row 0 / column 0, and Z and the seeds
+// over the end cells.  The expected count
 // of a transition out of cell c into c' is F(c) trans B(c') / Z, so the backward pass, which
 // forms exactly the products trans * B(c') to build B(c), adds F(c) times them to the counts.
 // Linear gaps are the one-state case (o = e).
@@ -58,6 +60,10 @@ struct SoftArgs {
     const int32_t* guide;                    // banded: per pair m + 1 guide columns at oa[p] + p
     int band;                                // banded: half-width
     int renorm_mask;                         // renormalise when (step & renorm_mask) == 0
+    int ends;                                // Global kernels, full DP: semi-global free ends, 1 a_begin
+                                             // (column 0 a free start), 2 a_end (column n's cells
+                                             // ends), 4 b_begin (row 0 a free start), 8 b_end (row m's
+                                             // cells ends); 0: Global's borders and end (m, n)
     double temperature;
     double* score; double* grad; int64_t gstride;
     int32_t* status;                         // per pair: 0 ok, 1 refused (out of range)
@@ -324,6 +330,12 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
         const int S = n + G;                    // steps: columns 0..n plus the skew
         const int SP = S + 1;                   // MW: progress key per stripe
         bool bad = false;
+        // semi-global ends (aligner.hpp:6362-6430): free starts on row 0 / column 0, Z over the
+        // end cells (row m or (m, n), then column n of rows 0..m-1), the backward seeded with 1
+        // at each; gap moves into a free start's border cells are not moves (6309-6319)
+        const bool sg_r0 = !LOC && (A.ends & 4), sg_c0 = !LOC && (A.ends & 1);
+        const bool sg_ec = !LOC && (A.ends & 2), sg_er = !LOC && (A.ends & 8);
+        const bool zsg = !LOC && A.ends != 0;
         if constexpr (MW) {
             if (lane == 0) prog[gib] = -1;
             __syncthreads();
@@ -433,6 +445,8 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                     nbj = j < n ? int(bp[j]) : N;         // the next column's code, one step ahead
                     T pM = dgM, pX = dgX, pY = dgY;
                     T qM = upM, qX = upX, qY = upY;
+                    const bool c0free = sg_c0 && j == 0;      // column 0 a free start
+                    const bool jn = j == n, ecn = sg_ec && j == n;
 #pragma unroll
                     for (int r = 0; r < R; ++r) {
                         const int i = i0 + r;
@@ -450,7 +464,8 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                                 if (j == 0) fx = T(0);
                                 if (r == 0 && i == 0) fy = T(0);
                             } else {
-                                if (r == 0 && i == 0 && j == 0) fm = lone;
+                                if (r == 0 && i == 0 && (j == 0 || sg_r0)) { fm = lone; fy = T(0); }
+                                if (c0free && i >= 1 && i <= m) { fm = lone; fx = T(0); }
                             }
                         } else {
                             fm = fmaf_t(pM, wv, fmaf_t(qM, e_b, cM[r] * e_a));
@@ -458,7 +473,8 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                                 if ((r == 0 && i == 0) || j == 0) fm = T(0);
                                 fm += lone;
                             } else {
-                                if (r == 0 && i == 0 && j == 0) fm = lone;
+                                if (r == 0 && i == 0 && (j == 0 || sg_r0)) fm = lone;
+                                if (c0free && i >= 1 && i <= m) fm = lone;
                             }
                         }
                         if constexpr (BAND) {
@@ -477,6 +493,9 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                             T zm_ = vmask[r];
                             if constexpr (BAND) zm_ = (j >= blo0[r] && j <= bhi[r]) ? zm_ : T(0);
                             zpart = fmaf_t(zm_, (fm + fx) + fy, zpart);
+                        } else if (zsg) {
+                            const bool e = (i == m) ? (jn || sg_er) : (ecn && i < m);
+                            if (e) zpart += (fm + fx) + fy;
                         }
                     }
                     dgM = upM; dgX = upX; dgY = upY;
@@ -489,7 +508,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                         else if (mx > T(0)) {
                             int e = ilog2(mx);
                             if (e < -120) e = -120;
-                            if (LOC && pass1) zacc.add(static_cast<double>(zpart), E);
+                            if ((LOC || zsg) && pass1) zacc.add(static_cast<double>(zpart), E);
                             zpart = T(0);
                             if (e != 0) {
                                 const T f = pow2i<T>(-e);
@@ -564,7 +583,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
             }
             if (MW && pass1) publish(s * SP + S);
             if (pass1) {
-                if constexpr (LOC) { zacc.add(static_cast<double>(zpart), E); }
+                if (LOC || zsg) zacc.add(static_cast<double>(zpart), E);
                 if constexpr (!LOC) {
                     if (m >= i0 && m < i0 + R) {
 #pragma unroll
@@ -578,7 +597,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
         for (int s = MW ? gib : 0; s < nstripes; s += NWp) fwd_stripe(s, true);
         // Z = zhat * 2^EZ with zhat in [1, 2)
         double zm; int ze;
-        if constexpr (LOC) {
+        if (LOC || zsg) {
             if constexpr (G > 1) {
 #pragma unroll
                 for (int off = 1; off < G; off <<= 1) {
@@ -608,7 +627,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
             }
             __syncthreads();
             bool anybad = false, anystall = false;
-            if constexpr (LOC) {
+            if (LOC || zsg) {
                 XAcc za; za.init();
                 for (int w = 0; w < NWp; ++w) za.add(cpart[8 * w], int(cpart[8 * w + 1]));
                 zm = za.m; ze = za.e;
@@ -799,7 +818,8 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                     T xM = dnM, xX = dnX, xY = dnY;   // row below, column j
                     T so_b = T(0), sx_b = T(0), so_a = T(0), sx_a = T(0);
                     T mc[R];
-                    const bool noX = LOC && j == 0;   // Local: no gap move into column 0
+                    const bool noX = (LOC || sg_c0) && j == 0;   // Local / a free column 0: no gap move into it
+                    const bool ecn = sg_ec && j == n;
 #pragma unroll
                     for (int r = R - 1; r >= 0; --r) {
                         const int i = i0 + r;
@@ -812,7 +832,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                         if constexpr (AFF) {
                             const T fx = f[NV * r + 1], fy = f[NV * r + 2];
                             T dX = noX ? T(0) : xX;                    // BX(i+1, j)
-                            T rY = (LOC && r == 0 && i == 0) ? T(0) : bY[r];     // BY(i, j+1)
+                            T rY = ((LOC || sg_r0) && r == 0 && i == 0) ? T(0) : bY[r];     // BY(i, j+1)
                             nM = fmaf_t(o_a, rY, fmaf_t(o_b, dX, D));
                             nX = fmaf_t(o_a, rY, fmaf_t(e_b, dX, D));
                             nY = fmaf_t(e_a, rY, fmaf_t(o_b, dX, D));
@@ -820,6 +840,9 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                                 nM = fmaf_t(vmask[r], lone, nM);
                                 nX = fmaf_t(vmask[r], lone, nX);
                                 nY = fmaf_t(vmask[r], lone, nY);
+                            } else if (zsg) {   // the end cells besides (m, n), which the padding seeds
+                                const bool e = (i == m) ? (sg_er && j < n) : (ecn && i < m);
+                                if (e) { nM += lone; nX += lone; nY += lone; }
                             }
                             const T fmy = fm + fy, fmx = fm + fx;
                             mc[r] = (fmy + fx) * D;
@@ -838,10 +861,14 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                             }
                         } else {
                             T dX = noX ? T(0) : xM;
-                            T rY = (LOC && r == 0 && i == 0) ? T(0) : bM[r];
+                            T rY = ((LOC || sg_r0) && r == 0 && i == 0) ? T(0) : bM[r];
                             nM = fmaf_t(e_a, rY, fmaf_t(e_b, dX, D));
                             if constexpr (LOC) nM = fmaf_t(vmask[r], lone, nM);
                             else if (i == m && j == n) nM = lone;
+                            else if (zsg) {
+                                const bool e = (i == m) ? sg_er : (ecn && i < m);
+                                if (e) nM += lone;
+                            }
                             nX = nM; nY = nM;
                             mc[r] = fm * D;
                             if constexpr (TR) {

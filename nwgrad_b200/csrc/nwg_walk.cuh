@@ -23,6 +23,7 @@ struct WalkArgs {
     int32_t* path_info;                // per pair: n_moves, start_i, start_j (or null)
     const int64_t* stripe_base;        // banded: per pair first entry of stripe_tab (else null)
     const int64_t* stripe_tab;
+    int ends;                          // semi-global free ends: 1 column 0 a start, 4 row 0 a start
 };
 
 // Byte of cell (i, j) in the fill's tiled layout; banded fills record each stripe's code
@@ -102,8 +103,9 @@ static __device__ __noinline__ void walk_pair(const WalkArgs& A, const int p) {
                 c = (i == 0 || j == 0) ? 3u : code_at(codes, i, j, n, G, R, tab);
                 if (tbl == 0 && (c & 3u) == 3u) break;
             } else {
-                if (i == 0) { for (; j > 0; --j) emit(2, 0, j, j == 1); break; }
-                if (j == 0) { for (; i > 0; --i) emit(1, i, 0, i == 1); break; }
+                // a free start ends the walk on its border; a charged border is one gap run
+                if (i == 0) { if (!(A.ends & 4)) for (; j > 0; --j) emit(2, 0, j, j == 1); break; }
+                if (j == 0) { if (!(A.ends & 1)) for (; i > 0; --i) emit(1, i, 0, i == 1); break; }
                 c = code_at(codes, i, j, n, G, R, tab);
             }
             if (i == 0) tbl = 2;
@@ -119,8 +121,8 @@ static __device__ __noinline__ void walk_pair(const WalkArgs& A, const int p) {
         while (true) {
             if (i == 0 && j == 0) break;
             int k;
-            if (i == 0) k = A.local ? 3 : 2;
-            else if (j == 0) k = A.local ? 3 : 1;
+            if (i == 0) k = (A.local || (A.ends & 4)) ? 3 : 2;
+            else if (j == 0) k = (A.local || (A.ends & 1)) ? 3 : 1;
             else k = code_at(codes, i, j, n, G, R, tab);
             if (k == 3) break;
             if (k == 0) { emit(0, i, j, false); --i; --j; }

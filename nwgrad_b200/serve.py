@@ -16,7 +16,7 @@ import numpy as np
 
 from . import _capi
 from ._capi import Job, check, ptr
-from .batch import _GAP, _GRAD, _MODE, _device_index, _encode_all
+from .batch import _GAP, _GRAD, _device_index, _encode_all, parse_mode
 from .params import AlignParams
 
 
@@ -56,12 +56,13 @@ class Server:
 
     def __init__(self, params: AlignParams, *, gap_model="affine", mode="global", grad_mode="soft",
                  precision=32, temperature=1.0, workers=3, hbm_budget_gb=48.0, max_batch_pairs=65536,
-                 device=None):
+                 device=None, free_ends=None):
         self._L = _lib()
         self._params = params.copy()
         self._alpha = params.alphabet_obj
-        self._job = Job(_GAP[gap_model], _MODE[mode], _GRAD[grad_mode], int(precision), -1, 0,
-                        float(temperature), 0, 0, 0)
+        _, am, sg = parse_mode(mode, free_ends)
+        self._job = Job(_GAP[gap_model], am, _GRAD[grad_mode], int(precision), -1, 0,
+                        float(temperature), 0, 0, 0, 0, 0, sg)
         self._grad_mode = grad_mode
         m = np.ascontiguousarray(params._m, np.float64)
         g = np.ascontiguousarray(params._g, np.float64)

@@ -1,0 +1,186 @@
+"""Semi-global ends on the GPU: mode "glocal" (A within B: row 0 a free start, row m's cells
+ends), "overlap" (every flank free) and mode "semiglobal" with any free_ends set.
+
+Hard results (scores, per-pair gradients, guides, stored paths) bit for bit the reference's
+fixtures and the oracle's; soft within 1e-4 of the double log-space forward-backward.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import AA, encode, has_gpu, mutate, rand_matrix, rand_seqs
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not has_gpu(), reason="needs a CUDA GPU")]
+
+import nwgrad_b200 as nw  # noqa: E402
+
+SOFT_RTOL = 1e-4
+SG_SETS = (12, 15, 9, 6, 3, 0)    # free_ends bits: 1 a_begin, 2 a_end, 4 b_begin, 8 b_end
+NAMES = ("a_begin", "a_end", "b_begin", "b_end")
+
+
+def _mode_kw(fe):
+    """The API spelling of a free_ends bit set."""
+    if fe == 12:
+        return dict(mode="glocal")
+    if fe == 15:
+        return dict(mode="overlap")
+    return dict(mode="semiglobal", free_ends=tuple(bool(fe & (1 << k)) for k in range(4)))
+
+
+def _flat(b, n):
+    gmat, ggap = b.grads()
+    if gmat.ndim == 3:
+        gmat, ggap = gmat[:, None], ggap[:, None]
+    return np.concatenate([gmat.reshape(n, -1), ggap.reshape(n, -1)], axis=1)
+
+
+def _soft_close(flat, ref):
+    scale = np.maximum(np.abs(ref).max(axis=1, keepdims=True), 1.0)
+    err = np.abs(flat - ref) / scale
+    assert err.max() <= SOFT_RTOL, (err.max(), np.unravel_index(err.argmax(), err.shape))
+
+
+@pytest.mark.parametrize("name", ["prot", "protf", "rna3"])
+def test_semiglobal_reference_fixtures(name):
+    """The GPU path against the reference engine's own semi-global outputs."""
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "semiglobal.npz"))
+    pre = name + "_"
+    alpha = str(z[pre + "alpha"])
+    sa, sb = [str(s) for s in z[pre + "sa"]], [str(s) for s in z[pre + "sb"]]
+    tr = z[pre + "tracks"] if pre + "tracks" in z.files else None
+    gt = z[pre + "gap_tracks"] if pre + "gap_tracks" in z.files else None
+    p = nw.AlignParams.from_arrays(z[pre + "mat"], z[pre + "gaps"], alphabet=alpha)
+    for fe in SG_SETS:
+        for gm in (0, 1):
+            kw = dict(gap_model=("linear", "affine")[gm], tracks=tr, gap_tracks=gt, **_mode_kw(fe))
+            for prec in (32, 64):
+                cls = nw.SeqPairBatch if prec == 32 else nw.SeqPairBatchDouble
+                b = cls(sa, sb, p, grad_mode="hard", **kw)
+                b.score_and_grad()
+                key = f"{pre}hard{prec}_g{gm}_e{fe}_"
+                assert np.array_equal(b.scores(), z[key + "scores"]), key
+                assert np.array_equal(_flat(b, len(sa)), z[key + "grads"]), key
+                assert np.array_equal(b.guides(), z[key + "guides"]), key
+            b = nw.SeqPairBatch(sa, sb, p, grad_mode="soft", **kw)
+            b.score_and_grad()
+            key = f"{pre}soft_g{gm}_e{fe}_"
+            np.testing.assert_allclose(b.scores(), z[key + "scores"], rtol=SOFT_RTOL, atol=1e-5, err_msg=key)
+            _soft_close(_flat(b, len(sa)), z[key + "grads"])
+
+
+def _pairs(rng, long=False):
+    """Empty and one-residue sides, miRNA-like short A in long B, homologs in several stripes,
+    and (long) pairs of 1,600+ rows."""
+    sa = rand_seqs(rng, 30, 1, 40, AA) + ["", "A", "", "ACDEF"] + rand_seqs(rng, 6, 18, 26, AA)
+    sb = rand_seqs(rng, 30, 1, 40, AA) + ["KLM", "", "", "W"] + rand_seqs(rng, 6, 400, 1500, AA)
+    homo = rand_seqs(rng, 6, 150, 330, AA)
+    sa += homo
+    sb += [mutate(rng, s, AA) for s in homo]
+    if long:
+        lng = rand_seqs(rng, 2, 1600, 2100, AA)
+        sa += lng
+        sb += ["".join(rng.choice(list(AA), size=200)) + mutate(rng, s, AA) for s in lng]
+    return sa, sb
+
+
+@pytest.mark.parametrize("prec", [32, 64])
+@pytest.mark.parametrize("gm", [0, 1])
+@pytest.mark.parametrize("fe", [12, 15, 6, 9])
+def test_semiglobal_hard_oracle(prec, gm, fe):
+    rng = np.random.default_rng(3100 + prec + 7 * gm + fe)
+    mat = rand_matrix(rng, 20, 1, True)
+    gaps = np.array([[11.0, 1.0, 11.0, 1.0]]) if gm else np.array([[0.0, 3.0, 0.0, 2.0]])
+    sa, sb = _pairs(rng, long=(prec == 32))
+    cls = nw.SeqPairBatch if prec == 32 else nw.SeqPairBatchDouble
+    b = cls(sa, sb, nw.AlignParams.from_arrays(mat, gaps, alphabet=AA), gap_model=("linear", "affine")[gm],
+            grad_mode="hard", **_mode_kw(fe))
+    tot = b.score_and_grad(keep_paths=True)
+    cap = max(len(x) + len(y) for x, y in zip(sa, sb)) + 1
+    o = oracle.hard(prec, gm, 2, mat, gaps, oracle.Encoded(encode(AA, sa), encode(AA, sb)), moves_cap=cap,
+                    free_ends=fe)
+    s = b.scores()
+    assert np.array_equal(s, o["scores"]), np.nonzero(s != o["scores"])[0][:5]
+    assert tot == float(np.cumsum(o["scores"])[-1])
+    flat = _flat(b, len(sa))
+    assert np.array_equal(flat, o["grads"]), np.nonzero((flat != o["grads"]).any(1))[0][:5]
+    assert np.array_equal(b.guides(), o["guides"])
+    mo, mv, info = b._stored()
+    for i in range(len(sa)):
+        k = int(info[i, 0])
+        assert k == int(o["nmoves"][i])
+        assert np.array_equal(mv[mo[i]:mo[i] + k], o["moves"][i, :k])
+        assert (info[i, 1], info[i, 2]) == (o["ends"][i, 2], o["ends"][i, 3])
+        a_al, b_al = b[i].aligned()
+        si, sj, ei, ej = int(info[i, 1]), int(info[i, 2]), int(o["ends"][i, 0]), int(o["ends"][i, 1])
+        assert a_al.replace("-", "") == sa[i][si:ei] and b_al.replace("-", "") == sb[i][sj:ej]
+
+
+@pytest.mark.parametrize("prec", [32, 64])
+@pytest.mark.parametrize("gm", [0, 1])
+@pytest.mark.parametrize("fe", [12, 15, 6, 9])
+def test_semiglobal_soft_oracle(prec, gm, fe):
+    rng = np.random.default_rng(3200 + prec + 7 * gm + fe)
+    mat = rand_matrix(rng, 20, 1, True)
+    gaps = np.array([[11.0, 1.0, 11.0, 1.0]]) if gm else np.array([[0.0, 3.0, 0.0, 2.0]])
+    sa, sb = _pairs(rng, long=(prec == 32))
+    cls = nw.SeqPairBatch if prec == 32 else nw.SeqPairBatchDouble
+    b = cls(sa, sb, nw.AlignParams.from_arrays(mat, gaps, alphabet=AA), gap_model=("linear", "affine")[gm],
+            grad_mode="soft", **_mode_kw(fe))
+    b.score_and_grad()
+    so, go = oracle.soft(gm, 2, mat, gaps, oracle.Encoded(encode(AA, sa), encode(AA, sb)), free_ends=fe)
+    np.testing.assert_allclose(b.scores(), so, rtol=SOFT_RTOL, atol=1e-5)
+    _soft_close(_flat(b, len(sa)), go)
+
+
+@pytest.mark.parametrize("gm", [0, 1])
+def test_semiglobal_soft_geometries_agree(gm):
+    """Every soft geometry (a lane per pair, narrow and wide stripes, checkpointed) gives the
+    glocal result within tolerance of the oracle."""
+    rng = np.random.default_rng(3300 + gm)
+    mat = rand_matrix(rng, 20, 1, True)
+    gaps = np.array([[11.0, 1.0, 11.0, 1.0]])
+    sa = rand_seqs(rng, 24, 5, 30, AA) + rand_seqs(rng, 8, 100, 260, AA)
+    sb = [mutate(rng, s, AA) for s in sa]
+    p = nw.AlignParams.from_arrays(mat, gaps, alphabet=AA)
+    so, go = oracle.soft(gm, 2, mat, gaps, oracle.Encoded(encode(AA, sa), encode(AA, sb)), free_ends=12)
+    for geo in ((1, 16), (16, 4), (32, 2), (32, 8)):
+        b = nw.SeqPairBatch(sa, sb, p, gap_model=("linear", "affine")[gm], mode="glocal", grad_mode="soft")
+        b._tune = geo
+        b.score_and_grad()
+        np.testing.assert_allclose(b.scores(), so, rtol=SOFT_RTOL, atol=1e-5, err_msg=str(geo))
+        _soft_close(_flat(b, len(sa)), go)
+
+
+def test_semiglobal_refusals_and_api():
+    rng = np.random.default_rng(3400)
+    mat = rand_matrix(rng, 20, 1, True)
+    p = nw.AlignParams.from_arrays(mat, [[11.0, 1.0, 11.0, 1.0]], alphabet=AA)
+    sa = rand_seqs(rng, 4, 600, 700, AA)
+    sb = [mutate(rng, s, AA) for s in sa]
+    b = nw.SeqPairBatch(sa, sb, p, mode="glocal", grad_mode="hard")
+    assert b.mode == "glocal" and b.free_ends == (False, False, True, True)
+    b.score_and_grad()
+    with pytest.raises(NotImplementedError):
+        b.banded_grad(8)
+    h = nw.SeqPairBatch(sa, sb, p, mode="glocal", grad_mode="hard", traceback="hirschberg")
+    with pytest.raises(NotImplementedError):
+        h.score_and_grad()
+    # pairs within the Hirschberg cutoff run the Pointers path, as the reference's do
+    short = nw.SeqPairBatch(sa[:2], sb[:2], p, mode="glocal", grad_mode="hard", traceback="hirschberg")
+    short.hb_cutoff = 1000
+    short.score_and_grad()
+    assert np.array_equal(short.scores(), b.scores()[:2])
+    o = nw.SeqPairBatch(sa, sb, p, mode="semiglobal", free_ends=("a_begin", "b_end"), grad_mode="soft")
+    assert o.free_ends == (True, False, False, True)
+    assert nw.SeqPairBatch(sa, sb, p, mode="overlap").free_ends == (True, True, True, True)
+    assert nw.SeqPairBatch(sa, sb, p, mode="global").free_ends == (False, False, False, False)
+    assert nw.SeqPairBatch(sa, sb, p, mode="local").free_ends is None
+    # semiglobal with no free end is Global's DP
+    g0 = nw.SeqPairBatch(sa, sb, p, mode="semiglobal", free_ends=(), grad_mode="hard")
+    g1 = nw.SeqPairBatch(sa, sb, p, mode="global", grad_mode="hard")
+    g0.score_and_grad()
+    g1.score_and_grad()
+    assert np.array_equal(g0.scores(), g1.scores())

@@ -55,3 +55,27 @@ def test_subst_matrix_score():
     assert sm.score("C", "G") == 6.0
     with pytest.raises(ValueError):
         sm.score("C", "N")
+
+
+def test_mode_parsing():
+    """Mode names and free_ends onto (align mode, free-end bits), with the reference's rules
+    (py_exports.cpp:276-335)."""
+    from nwgrad_b200.batch import parse_mode
+    assert parse_mode("global") == ("global", 0, 12)
+    assert parse_mode("local") == ("local", 1, 12)
+    assert parse_mode("glocal") == ("glocal", 2, 12)
+    assert parse_mode("overlap") == ("overlap", 2, 15)
+    assert parse_mode("semiglobal", (True, False, False, True)) == ("semiglobal", 2, 9)
+    assert parse_mode("semiglobal", ("a_end", "b_begin")) == ("semiglobal", 2, 6)
+    assert parse_mode("semiglobal", "b_end") == ("semiglobal", 2, 8)
+    assert parse_mode("semiglobal", ()) == ("semiglobal", 2, 0)
+    with pytest.raises(ValueError, match="needs free_ends"):
+        parse_mode("semiglobal")
+    with pytest.raises(ValueError, match="goes with mode"):
+        parse_mode("glocal", ("a_begin",))
+    with pytest.raises(ValueError, match="unknown free end"):
+        parse_mode("semiglobal", ("a_start",))
+    with pytest.raises(ValueError, match="four booleans"):
+        parse_mode("semiglobal", (True, False))
+    with pytest.raises(ValueError, match="unknown mode"):
+        parse_mode("fitting")
