@@ -360,11 +360,13 @@ def main():
                     help="soft: per-pair forward tables above this many MiB are checkpointed (-1: default)")
     ap.add_argument("--geometry", default=None, help="LANESxROWS for every pair (no tuning), e.g. 32x4")
     ap.add_argument("--workload", default="c2-soft",
-                    choices=["c2-soft", "c1-hard", "c4-long", "c3-short", "c5-serve-train"],
+                    choices=["c2-soft", "c1-hard", "c4-long", "c3-short", "c5-serve-train", "c6-glocal"],
                     help="c2-soft (default): the soft-gradient batch; side measurements: c1-hard (plain hard "
                          "batch), c4-long (64 long pairs: Pointers, Hirschberg, soft, banded), c3-short "
                          "(many short local linear tracked pairs, hard and soft), c5-serve-train (the "
-                         "server under a Poisson stream while an autograd loop trains the parameters)")
+                         "server under a Poisson stream while an autograd loop trains the parameters), "
+                         "c6-glocal (miRNA-like A within longer B, glocal ends, hard and soft)")
+    ap.add_argument("--glocal-pairs", type=int, default=200_000)
     ap.add_argument("--long-pairs", type=int, default=64)
     ap.add_argument("--short-pairs", type=int, default=2_000_000)
     ap.add_argument("--train-pairs", type=int, default=2000, help="c5-serve-train: homolog pairs (as many decoys)")
@@ -378,6 +380,8 @@ def main():
         return bench_c3(args)
     if args.workload == "c5-serve-train":
         return bench_c5(args)
+    if args.workload == "c6-glocal":
+        return bench_c6(args)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -680,6 +684,61 @@ def c3_workload(n_pairs, seed=3):
             mat[k, x, y] = 5.0
     gaps = np.tile([6.0, 6.0, 6.0, 6.0], (3, 1))
     return mat, gaps, a.reshape(-1), oa, b, ob, tr.reshape(-1)
+
+
+def c6_workload(n_pairs, seed=6):
+    """miRNA-like A (22 nt RNA, ACGU) against B of 200-1000 nt (ACGT) holding the reverse
+    complement of A[1:8] at a random offset: the "A within B" problem of glocal ends."""
+    rng = np.random.default_rng(seed)
+    A = np.array([0, 1, 2, 4], np.uint8)
+    a = A[rng.integers(0, 4, size=(n_pairs, 22))]
+    lb = rng.integers(200, 1001, size=n_pairs)
+    ob = np.zeros(n_pairs + 1, np.int64); np.cumsum(lb, out=ob[1:])
+    b = rng.integers(0, 4, size=int(ob[-1])).astype(np.uint8)
+    lut = np.array([3, 2, 1, 0, 0], np.uint8)
+    for p in range(n_pairs):
+        off = int(rng.integers(0, lb[p] - 8))
+        b[ob[p] + off: ob[p] + off + 7] = lut[a[p, 1:8][::-1]]
+    oa = np.arange(n_pairs + 1, dtype=np.int64) * 22
+    mat = np.full((1, 5, 5), -4.0)
+    for x, y in ((0, 3), (1, 2), (2, 1), (3, 0), (4, 0), (2, 4)):
+        mat[0, x, y] = 5.0
+    gaps = np.array([[5.0, 2.0, 5.0, 2.0]])
+    return mat, gaps, a.reshape(-1), oa, b, ob
+
+
+def bench_c6(args):
+    """Side measurement: glocal ends (A within B), affine, hard and soft, autotuned; the same
+    batch with Global ends beside it, and the reference's CPU path on a bounded sample."""
+    import nwgrad_b200 as nw
+    import oracle
+    mat, gaps, a, oa, b, ob = c6_workload(args.glocal_pairs)
+    cells = cells_of(oa, ob)
+    p = nw.AlignParams.from_arrays(mat, gaps, alphabet="ACGTU")
+    out = {"metric": "glocal GCUPS", "unit": "GCUPS", "n_gpus": 1,
+           "config": {"workload": f"{args.glocal_pairs} pairs, A 22 nt RNA, B 200-1000 nt DNA with a seed site, "
+                                  f"affine (5, 2), glocal ends", "cells": cells}, "modes": {}}
+    for grad in ("hard", "soft"):
+        res = {}
+        for mode in ("glocal", "global"):
+            bt = nw.SeqPairBatch.from_codes(a, oa, b, ob, p, grad_mode=grad, mode=mode)
+            table = bt.autotune()
+            bt.score_and_grad()
+            t = _timed_run(lambda: (bt.score_and_grad(), bt.compute_grad()), reps=3)
+            ms, launches = bt.last_timing()
+            res[mode] = {"gcups": cells / t / 1e9, "seconds": t, "device_ms": ms, "launches": launches,
+                         "autotune": {str(k): _tune_mod().describe(v) for k, v in table.items()}}
+            del bt
+        if oracle.ref_bench_available() and not args.no_cpu_baseline:
+            k = min(args.glocal_pairs, 20000)
+            secs, _, threads, isa = oracle.ref_time_codes(32, 1, 2, 2 if grad == "soft" else 1, "ACGTU", mat, gaps,
+                                                          a, oa[:k + 1], b, ob[:k + 1], warmup=1, reps=2,
+                                                          free_ends=12)
+            ck = cells_of(oa[:k + 1], ob[:k + 1])
+            res["cpu_reference"] = {"gcups": ck / float(np.min(secs)) / 1e9, "pairs": k, "cores": threads,
+                                    "isa": isa, "sample": f"first {k} pairs, best of {len(secs)}"}
+        out["modes"][grad] = res
+    print(json.dumps(out))
 
 
 def bench_c3(args):

@@ -303,7 +303,7 @@ def ref_bench_available() -> bool:
 
 
 def ref_time_codes(prec, gm, am, grad_mode, alphabet, mat, gaps, a, oa, b, ob, n_threads=0,
-                   warmup=1, reps=3, kernel=-2):
+                   warmup=1, reps=3, kernel=-2, free_ends=12):
     """Time the reference's SIMD batch path (score_and_grad + compute_grad per pass) in its
     own process (_ref/nwref_bench) on pairs given as codes: returns (seconds per pass,
     total, threads, isa)."""
@@ -316,7 +316,8 @@ def ref_time_codes(prec, gm, am, grad_mode, alphabet, mat, gaps, a, oa, b, ob, n
     K, N = mat.shape[0], mat.shape[1]
     sym = np.frombuffer(alphabet.encode(), dtype=np.uint8)
     with tempfile.NamedTemporaryFile(suffix=".bin", delete=False) as f:
-        f.write(np.array([prec, gm, am, grad_mode, N, K, n_threads, warmup, reps, kernel], np.int32).tobytes())
+        f.write(np.array([prec, gm, am, grad_mode, N, K, n_threads, warmup, reps, kernel, free_ends],
+                         np.int32).tobytes())
         f.write(np.array([len(oa) - 1], np.int64).tobytes())
         f.write(np.array([len(alphabet)], np.int32).tobytes())
         f.write(alphabet.encode())

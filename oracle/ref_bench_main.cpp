@@ -6,7 +6,7 @@
 //   nwref_bench <problem file>
 //
 // Problem file (little-endian): int32 prec, gm, am, grad_mode, N, K, n_threads, warmup, reps,
-// kernel; int64 n_pairs; int32 alphabet length, alphabet bytes; K*N*N doubles; K*4 doubles;
+// kernel, free_ends; int64 n_pairs; int32 alphabet length, alphabet bytes; K*N*N doubles; K*4 doubles;
 // (n_pairs + 1) int64 offsets of A, then the A characters; the same for B.
 // Prints one JSON line: {"secs": [...], "total": T, "threads": n, "isa": "..."}.
 #include <cstdint>
@@ -21,6 +21,7 @@ struct Problem {
     const char* a; const int64_t* oa; const char* b; const int64_t* ob;
     const uint16_t* tracks; const uint16_t* gtracks;
     int traceback, kernel, n_threads; double temperature; int soft_impl, soft_f32, hb_cutoff, inter_fill;
+    int free_ends;
 };
 extern "C" int ref_time(const Problem* P, int warmup, int reps, double* secs, double* total);
 extern "C" int ref_info(int n_threads, int* resolved, char* isa, int isa_cap);
@@ -32,7 +33,7 @@ int main(int argc, char** argv) {
     if (argc < 2) { std::fprintf(stderr, "usage: nwref_bench <problem file>\n"); return 2; }
     std::ifstream f(argv[1], std::ios::binary);
     if (!f) { std::fprintf(stderr, "cannot open %s\n", argv[1]); return 2; }
-    int h[10];
+    int h[11];
     for (int& x : h) x = rd<int32_t>(f);
     const int64_t n = rd<int64_t>(f);
     const int al = rd<int32_t>(f);
@@ -52,7 +53,7 @@ int main(int argc, char** argv) {
     if (!f) { std::fprintf(stderr, "truncated problem file\n"); return 2; }
     Problem P{h[0], h[1], h[2], h[3], N, K, mat.data(), gaps.data(), alpha.c_str(), n,
               A.c_str(), oa.data(), B.c_str(), ob.data(), nullptr, nullptr,
-              0, h[9], h[6], 1.0, 0, 1, 0, 1};
+              0, h[9], h[6], 1.0, 0, 1, 0, 1, h[10]};
     const int reps = h[8];
     std::vector<double> secs(static_cast<size_t>(reps));
     double total = 0;
