@@ -229,8 +229,8 @@ struct GraphCache {
 using HardFn = nwg::HardFn;
 using SoftFn = nwg::SoftFn;
 using Geo = nwg::Geo;
-template <class T> HardFn hard_fn_rt(bool aff, bool loc, bool tr, Geo g) {
-    return sizeof(T) == 4 ? nwg::hard_fn_f32(aff, loc, tr, g) : nwg::hard_fn_f64(aff, loc, tr, g);
+template <class T> HardFn hard_fn_rt(bool aff, int am, bool tr, Geo g) {
+    return sizeof(T) == 4 ? nwg::hard_fn_f32(aff, am, tr, g) : nwg::hard_fn_f64(aff, am, tr, g);
 }
 template <class T> SoftFn soft_fn_rt(bool aff, bool loc, bool tr, Geo g) {
     return sizeof(T) == 4 ? nwg::soft_fn_f32(aff, loc, tr, g) : nwg::soft_fn_f64(aff, loc, tr, g);
@@ -740,7 +740,7 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
     int64_t soff_b = 0;
     for (auto& B : P.buckets) {
         if (B.pairs.empty()) continue;
-        HardFn fn = hard_fn_rt<T>(aff, loc, tr, B.geo);
+        HardFn fn = hard_fn_rt<T>(aff, ends ? 2 : (loc ? 1 : 0), tr, B.geo);
         if (!fn) throw Error(NWG_EINVAL, "no kernel for this geometry");
         const int hblock = B.geo.mw > 1 ? 32 * B.geo.mw : 128;
         const size_t smem = smem_base + (B.geo.mw > 1 ? nwg::hard_mw_smem_bytes(B.geo.mw, int(sizeof(T))) : 0);

@@ -108,9 +108,11 @@ __host__ __device__ inline size_t hard_mw_smem_bytes(int warps, int tsize) {
 // (nwg_soft.cuh).  A wait that runs out marks the pair's end state 3 and the host fails the call.
 constexpr int kHardSpinLimit = 1 << 22;
 
-template <class T, bool AFF, bool LOC, bool TR, int G, int R, bool BAND = false, bool MW = false>
+// SG: the semi-global ends of A.ends (Global fills only, full DP, a warp or lane per pair)
+template <class T, bool AFF, bool LOC, bool TR, int G, int R, bool BAND = false, bool MW = false, bool SG = false>
 __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArgs A) {
     static_assert(!MW || (G == 32 && !BAND), "several warps per pair: 32 lanes, full DP");
+    static_assert(!SG || (!LOC && !BAND && !MW), "semi-global ends: Global fills, full DP, one warp per pair");
     constexpr int GR = G * R;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* smat = reinterpret_cast<T*>(smem_raw);
@@ -178,13 +180,13 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
         };
         const T goa0 = sgap[4 * gset(0) + 0], gea0 = sgap[4 * gset(0) + 1];
         const T ugob = sgap[2], ugeb = sgap[3], ugoa = sgap[0], ugea = sgap[1];
-        const bool sg_r0 = !LOC && (A.ends & 4), sg_c0 = !LOC && (A.ends & 1);
-        const bool sg_ec = !LOC && (A.ends & 2), sg_er = !LOC && (A.ends & 8);
+        const bool sg_r0 = SG && (A.ends & 4), sg_c0 = SG && (A.ends & 1);
+        const bool sg_ec = SG && (A.ends & 2), sg_er = SG && (A.ends & 8);
         if (m == 0 || n == 0) {
             if (lane == 0 && (!MW || gib == 0)) {
                 T sc; int ei, ej, st;
                 if (LOC) { sc = T(0); ei = 0; ej = 0; st = 0; }
-                else if (A.ends) {
+                else if (SG) {
                     // semi-global: the border cells in the reference's order (column n of rows
                     // 0..m-1, then row m), each from its closed form
                     auto cell = [&](int ci, int cj, T& vm, T& vx, T& vy) {
@@ -242,7 +244,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
         // rows 0..m-1 (from row 0's cell); the lane holding row m tracks the former
         EndPick<T> erow, ecol;
         erow.init(); ecol.init();
-        if (!LOC && A.ends) {
+        if constexpr (SG) {
             T vm, vx, vy;
             if (sg_c0) { vm = T(0); vx = ninf<T>(); vy = ninf<T>(); }
             else {
@@ -451,7 +453,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
                         for (int r = 0; r < R; ++r) dst[r] = uint8_t(w[r >> 2] >> (8 * (r & 3)));
                     }
                     dgM = upM; dgX = upX; dgY = upY;
-                    if (!LOC && sg_er) {
+                    if (SG && sg_er) {
                         const int zr = m - i0;
 #pragma unroll
                         for (int r = 0; r < R; ++r)
@@ -484,7 +486,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
                     for (int r = 0; r < R; ++r)
                         if (i0 + r == m) { endM = cM[r]; endX = cX[r]; endY = cY[r]; }
                 }
-                if (sg_ec) {
+                if (SG && sg_ec) {
                     // column n of this stripe's rows below m, first max in row order: this
                     // lane's, then the group's (the lowest row among equal maxima)
                     EndPick<T> lc; lc.init();
@@ -569,7 +571,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
                 endX = __shfl_sync(gmask, endX, src, G);
                 endY = __shfl_sync(gmask, endY, src, G);
             }
-            if (A.ends && sg_er) {
+            if (SG && sg_er) {
                 // row m's first max: held by the lane of row m
                 const int src = ((m - 1) % GR) / R;
                 if constexpr (G > 1) {
@@ -584,7 +586,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
                     sc = rmax3(endM, endX, endY);
                     st = (endM >= endX && endM >= endY) ? 0 : (endX >= endY ? 1 : 2);
                 } else { sc = endM; st = 0; }
-                if (A.ends) {
+                if constexpr (SG) {
                     // semi-global: column n's rows 0..m-1 were offered first, then row m
                     if (sg_er) { sc = erow.v; ej = erow.j; st = erow.st; }
                     if (sg_ec && ecol.any && !(sc > ecol.v)) { sc = ecol.v; ei = ecol.i; ej = n; st = ecol.st; }
