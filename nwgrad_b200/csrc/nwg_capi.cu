@@ -232,8 +232,8 @@ using Geo = nwg::Geo;
 template <class T> HardFn hard_fn_rt(bool aff, int am, bool tr, Geo g) {
     return sizeof(T) == 4 ? nwg::hard_fn_f32(aff, am, tr, g) : nwg::hard_fn_f64(aff, am, tr, g);
 }
-template <class T> SoftFn soft_fn_rt(bool aff, bool loc, bool tr, Geo g) {
-    return sizeof(T) == 4 ? nwg::soft_fn_f32(aff, loc, tr, g) : nwg::soft_fn_f64(aff, loc, tr, g);
+template <class T> SoftFn soft_fn_rt(bool aff, int am, bool tr, Geo g) {
+    return sizeof(T) == 4 ? nwg::soft_fn_f32(aff, am, tr, g) : nwg::soft_fn_f64(aff, am, tr, g);
 }
 
 // The kernel geometries (lanes per pair G, rows per lane R) each path is instantiated for.
@@ -988,7 +988,7 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
     int64_t scratch_total = 0;
     for (auto& B : P->buckets) {
         if (B.pairs.empty()) continue;
-        SoftFn fn = soft_fn_rt<T>(aff, loc, tr, B.geo);
+        SoftFn fn = soft_fn_rt<T>(aff, (J.mode == 2 && J.free_ends) ? 2 : (loc ? 1 : 0), tr, B.geo);
         if (!fn) throw Error(NWG_EINVAL, "no soft kernel for this geometry");
         const int G = B.geo.G;
         const bool mw = B.geo.mw > 1;            // several warps per pair (long pairs)

@@ -13,6 +13,6 @@ struct Geo { int G, R; bool band = false; int mw = 0; };   // mw > 1: that many 
 // am: 0 Global, 1 Local, 2 semi-global ends (full DP, one warp or lane per pair)
 HardFn hard_fn_f32(bool aff, int am, bool tr, Geo g);
 HardFn hard_fn_f64(bool aff, int am, bool tr, Geo g);
-SoftFn soft_fn_f32(bool aff, bool loc, bool tr, Geo g);
-SoftFn soft_fn_f64(bool aff, bool loc, bool tr, Geo g);
+SoftFn soft_fn_f32(bool aff, int am, bool tr, Geo g);
+SoftFn soft_fn_f64(bool aff, int am, bool tr, Geo g);
 }  // namespace nwg

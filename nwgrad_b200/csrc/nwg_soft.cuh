@@ -206,10 +206,11 @@ constexpr int kPrefetchSteps = NWG_SOFT_PREFETCH_STEPS;
 // outside [jlo(i), jhi(i)], Global border cells past border_rows / border_cols, backward cells
 // outside [jlo0(i), jhi0(i)]; Local log Z sums the band only.  Zero cells neither receive nor
 // pass on probability, which is what the reference's band-limited tables compute.
-template <class T, bool AFF, bool LOC, bool TR, int G, int R, bool MW = false, bool BAND = false>
+template <class T, bool AFF, bool LOC, bool TR, int G, int R, bool MW = false, bool BAND = false, bool SG = false>
 __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2 : 4) : 1))) soft_kernel(const SoftArgs A) {
     static_assert(!MW || (G == 32 && !TR), "several warps per pair: 32 lanes, untracked");
     static_assert(!BAND || (G == 32 && !MW), "banded: 32 lanes, one warp per pair");
+    static_assert(!SG || (!LOC && !BAND), "semi-global ends: Global kernels, full DP");
     constexpr int GR = G * R;
     constexpr int NV = AFF ? 3 : 1;          // values per cell
     constexpr int CV = NV * R;               // values per lane column
@@ -333,9 +334,9 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
         // semi-global ends (aligner.hpp:6362-6430): free starts on row 0 / column 0, Z over the
         // end cells (row m or (m, n), then column n of rows 0..m-1), the backward seeded with 1
         // at each; gap moves into a free start's border cells are not moves (6309-6319)
-        const bool sg_r0 = !LOC && (A.ends & 4), sg_c0 = !LOC && (A.ends & 1);
-        const bool sg_ec = !LOC && (A.ends & 2), sg_er = !LOC && (A.ends & 8);
-        const bool zsg = !LOC && A.ends != 0;
+        const bool sg_r0 = SG && (A.ends & 4), sg_c0 = SG && (A.ends & 1);
+        const bool sg_ec = SG && (A.ends & 2), sg_er = SG && (A.ends & 8);
+        const bool zsg = SG && A.ends != 0;
         if constexpr (MW) {
             if (lane == 0) prog[gib] = -1;
             __syncthreads();

@@ -3,15 +3,17 @@
 
 namespace nwg {
 namespace {
-template <class T, bool AFF, bool LOC, bool TR>
+// SG: the semi-global ends (Global kernels, full DP), their own instantiations so the Global
+// kernels test no end flag per cell
+template <class T, bool AFF, bool LOC, bool TR, bool SG = false>
 SoftFn pick(Geo g) {
-    if (g.band) return (g.G == 32 && g.R == 4 && g.mw <= 1) ? &soft_kernel<T, AFF, LOC, TR, 32, 4, false, true> : nullptr;
+    if (g.band) return (!SG && g.G == 32 && g.R == 4 && g.mw <= 1) ? &soft_kernel<T, AFF, LOC, TR, 32, 4, false, true> : nullptr;
     if constexpr (!TR) {
-        if (g.mw > 1) return (g.G == 32 && g.R == 4) ? &soft_kernel<T, AFF, LOC, false, 32, 4, true> : nullptr;
+        if (g.mw > 1) return (g.G == 32 && g.R == 4) ? &soft_kernel<T, AFF, LOC, false, 32, 4, true, false, SG> : nullptr;
     } else {
         if (g.mw > 1) return nullptr;
     }
-#define NWG_S(GG, RR) if (g.G == GG && g.R == RR) return &soft_kernel<T, AFF, LOC, TR, GG, RR>;
+#define NWG_S(GG, RR) if (g.G == GG && g.R == RR) return &soft_kernel<T, AFF, LOC, TR, GG, RR, false, false, SG>;
     NWG_S(1, 8) NWG_S(1, 16) NWG_S(1, 24) NWG_S(1, 32) NWG_S(32, 2) NWG_S(32, 4)
     NWG_S(16, 2) NWG_S(16, 4) NWG_S(8, 4) NWG_S(16, 8) NWG_S(32, 8)
 #undef NWG_S
@@ -19,8 +21,13 @@ SoftFn pick(Geo g) {
 }
 }  // namespace
 
-SoftFn NWG_SOFT_FN(bool aff, bool loc, bool tr, Geo g) {
+SoftFn NWG_SOFT_FN(bool aff, int am, bool tr, Geo g) {
     using T = NWG_T;
+    const bool loc = am == 1;
+    if (am == 2) {
+        if (aff) return tr ? pick<T, true, false, true, true>(g) : pick<T, true, false, false, true>(g);
+        return tr ? pick<T, false, false, true, true>(g) : pick<T, false, false, false, true>(g);
+    }
     if (aff) {
         if (loc) return tr ? pick<T, true, true, true>(g) : pick<T, true, true, false>(g);
         return tr ? pick<T, true, false, true>(g) : pick<T, true, false, false>(g);
