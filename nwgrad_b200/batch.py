@@ -24,6 +24,7 @@ _MODE = {"global": 0, "local": 1, "glocal": 2, "overlap": 2, "semiglobal": 2}
 _SG_NAMES = ("a_begin", "a_end", "b_begin", "b_end")
 _SG_BITS = (1, 2, 4, 8)
 SG_GLOCAL, SG_ALL = 12, 15
+_CURRENT = object()   # a deferred soft guide due under the params current at its first use
 
 
 def parse_mode(mode, free_ends=None):
@@ -208,7 +209,7 @@ class SeqPairBatch:
         self.soft_temperature = 1.0
         self.soft_impl = "scaled"
         self.soft_precision = "float32" if self._precision == 32 else "double"
-        self.soft_guide = "eager"
+        self._soft_guide = "eager"
         self.fill = "interpair"
         self.schedule = "dynamic"
         self.track_storage = "paths"
@@ -403,7 +404,8 @@ class SeqPairBatch:
         if gm == 2:
             tot = self._run(2)
             # the guide is deferred: computed on first use under the params scored now
-            self._guides_pending = self._params.copy()
+            # ("eager") or under those current at that use ("lazy")
+            self._guides_pending = self._params.copy() if self._soft_guide == "eager" else _CURRENT
             self._have_guides = False
             self._guides = None
             self._paths = False
@@ -438,7 +440,7 @@ class SeqPairBatch:
         batch's params and results are untouched (batch_soft_defer.inl)."""
         if self._guides_pending is None or self._store is None:
             return
-        snap = self._guides_pending
+        snap = self._params if self._guides_pending is _CURRENT else self._guides_pending
         m = np.ascontiguousarray(snap._m, dtype=np.float64)
         g = np.ascontiguousarray(snap._g, dtype=np.float64)
         job = self._job(0)
@@ -706,6 +708,24 @@ class SeqPairBatch:
     @property
     def mode(self):
         return self._mode
+
+    @property
+    def soft_guide(self):
+        """When soft pairs compute their guide path (the Viterbi path banded_grad() bands
+        around): "eager" (default) under the params score_and_grad() ran with, computed on
+        first use from a snapshot of them; "lazy" under the params current at first use
+        (after set_params() it follows the new params).  "posterior" (the forward-backward's
+        per-row column of greatest posterior mass) is not built here."""
+        return self._soft_guide
+
+    @soft_guide.setter
+    def soft_guide(self, v):
+        if v not in ("eager", "lazy", "posterior"):
+            raise ValueError(f"nwgrad: unknown soft_guide \"{v}\" (expected \"eager\", \"lazy\" or \"posterior\")")
+        if v == "posterior":
+            raise NotImplementedError("nwgrad_b200: soft_guide=\"posterior\" is not available in this build; "
+                                      "use \"eager\" or \"lazy\"")
+        self._soft_guide = v
 
     @property
     def free_ends(self):
