@@ -100,8 +100,9 @@ int nwg_set_geometry_costs(nwg_store* s, int soft, int size_class, int n, const 
  * (fewer pairs run at once when they are large); a pair whose whole forward table would be
  * above checkpoint_bytes keeps only its stripe boundaries and recomputes each stripe just
  * before that stripe's backward (results are bit-identical either way).  A value < 0 keeps the
- * current setting (defaults: 60 % of the device memory free at the call, at least 24 GiB; and
- * 16 MiB).  No counterpart in the reference (its CPU
+ * current setting (defaults: 60 % of the device memory free at the call -- the device's free
+ * memory, the blocks the memory pool keeps idle and the store's own scratch -- at least 24 GiB;
+ * and 16 MiB).  No counterpart in the reference (its CPU
  * path keeps a whole table per thread). */
 int nwg_set_memory(nwg_store* s, int64_t scratch_budget_bytes, int64_t checkpoint_bytes);
 

@@ -508,7 +508,17 @@ int64_t scratch_budget_of(nwg_store* s) {
     if (s->scratch_budget >= 0) return s->scratch_budget;
     size_t fr = 0, tot = 0;
     cudaMemGetInfo(&fr, &tot);
-    return std::max<int64_t>(int64_t(24) << 30, int64_t(0.6 * double(fr + s->scratch.bytes)));
+    // blocks the pool keeps from earlier batches are free for this one too (the device's free
+    // memory does not count them)
+    uint64_t reserved = 0, used = 0;
+    cudaMemPool_t pool;
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used);
+    }
+    const double idle = reserved > used ? double(reserved - used) : 0.0;
+    return std::max<int64_t>(int64_t(24) << 30, int64_t(0.6 * (double(fr) + idle + double(s->scratch.bytes))));
 }
 
 void set_params_dev(nwg_store* s) {
