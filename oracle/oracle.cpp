@@ -433,7 +433,8 @@ void banded_affine(const Model& M, const Rows<T>& R, const uint8_t* b, int m, in
         at(VM, 0, 0) = T(0);
         const int bi = B.border_rows(), bj = B.border_cols();
         for (int i = 1; i <= bi; ++i) at(VX, i, 0) = R.bx0[i];
-        for (int j = 1; j <= bj; ++j) at(VY, 0, j) = -(R.goa[0] + static_cast<T>(j) * R.gea[0]);
+        if (M.free_row0()) { for (int j = 0; j <= n; ++j) at(VM, 0, j) = T(0); }   // glocal: a free start
+        else for (int j = 1; j <= bj; ++j) at(VY, 0, j) = -(R.goa[0] + static_cast<T>(j) * R.gea[0]);
     } else {
         for (int i = 0; i <= m; ++i) at(VM, i, 0) = T(0);
         for (int j = 0; j <= n; ++j) at(VM, 0, j) = T(0);
@@ -464,7 +465,11 @@ void banded_affine(const Model& M, const Rows<T>& R, const uint8_t* b, int m, in
             bt = (vm >= vx && vm >= vy) ? TM : (vx >= vy ? TX : TY);
         }
     }
-    if (!local) {
+    if (M.semi()) {   // glocal: row m's first best column over its band (glocal_end_affine_)
+        SgEnd<T> e;
+        for (int j = B.jlo0(m); j <= B.jhi0(m); ++j) e.offer(m, j, at(VM, m, j), at(VX, m, j), at(VY, m, j));
+        score = e.best; bi = e.i; bj = e.j; bt = e.t;
+    } else if (!local) {
         const T vm = at(VM, m, n), vx = at(VX, m, n), vy = at(VY, m, n);
         score = mx3(vm, vx, vy);
         bi = m; bj = n;
@@ -481,6 +486,7 @@ void banded_affine(const Model& M, const Rows<T>& R, const uint8_t* b, int m, in
         if (local) {
             if (tbl == TM && at(VM, i, j) <= T(0)) break;
         } else {
+            if (i == 0 && M.free_row0()) break;
             if (i == 0) { for (; j > 0; --j) sink.emit(TY, 0, j, j == 1); break; }
             if (j == 0) { for (; i > 0; --i) sink.emit(TX, i, 0, i == 1); break; }
         }
@@ -516,7 +522,8 @@ void banded_linear(const Model& M, const Rows<T>& R, const uint8_t* b, int m, in
         at(0, 0) = T(0);
         const int bi = B.border_rows(), bj = B.border_cols();
         for (int i = 1; i <= bi; ++i) at(i, 0) = R.bx0[i];
-        for (int j = 1; j <= bj; ++j) at(0, j) = -static_cast<T>(j) * R.gea[0];
+        if (M.free_row0()) { for (int j = 0; j <= n; ++j) at(0, j) = T(0); }   // glocal: a free start
+        else for (int j = 1; j <= bj; ++j) at(0, j) = -static_cast<T>(j) * R.gea[0];
     } else {
         for (int i = 0; i <= m; ++i) at(i, 0) = T(0);
         for (int j = 0; j <= n; ++j) at(0, j) = T(0);
@@ -539,17 +546,24 @@ void banded_linear(const Model& M, const Rows<T>& R, const uint8_t* b, int m, in
             best_local = rowmax; bi = i; bj = j;
         }
     }
-    score = local ? best_local : at(m, n);
-    if (!local) { bi = m; bj = n; }
+    if (M.semi()) {   // glocal: row m's first best column over its band (glocal_end_linear_)
+        SgEnd<T> e;
+        for (int j = B.jlo0(m); j <= B.jhi0(m); ++j) e.offer(m, j, at(m, j), ninf<T>(), ninf<T>());
+        score = e.best; bi = e.i; bj = e.j;
+    } else {
+        score = local ? best_local : at(m, n);
+        if (!local) { bi = m; bj = n; }
+    }
     sink.o.end_i = bi; sink.o.end_j = bj;
     if (sink.gj) {
         auto& gj = *sink.gj; gj.assign(m + 1, -1); gj[0] = 0; gj[m] = n;
-        gj[local ? bi : m] = local ? bj : n;
+        gj[M.am == 0 ? m : bi] = M.am == 0 ? n : bj;
     }
     int i = bi, j = bj;
     while (true) {
         if (i == 0 && j == 0) break;
         if (local && at(i, j) <= T(0)) break;
+        if (i == 0 && M.free_row0()) break;
         int k;
         if (i > 0 && j > 0 && at(i, j) == at(i - 1, j - 1) + matT[size_t(R.rs[i - 1]) * M.N + b[j - 1]]) k = 0;
         else if (i > 0 && (j == 0 || at(i, j) == at(i - 1, j) - R.geb[i])) k = 1;
@@ -1423,7 +1437,7 @@ int orc_soft_batch(int gm, int am, int N, int K, const double* mat, const double
         std::fill(o.grad, o.grad + gs, 0.0);
         const uint16_t* tk = tracks ? tracks + oa[p] : nullptr;
         const uint16_t* gk = gtracks ? gtracks + oa[p] + p : nullptr;
-        Band bd; bd.m = m; bd.n = n; bd.global = am != 1;
+        Band bd; bd.m = m; bd.n = n; bd.global = am == 0;
         if (guides_in && band >= 0) { bd.band = band; bd.g = guides_in + oa[p] + p; }
         if (gm == 0) soft_linear(M, a + oa[p], m, b + ob[p], n, tk, gk, temperature, o, bd);
         else         soft_affine(M, a + oa[p], m, b + ob[p], n, tk, gk, temperature, o, bd);

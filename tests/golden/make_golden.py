@@ -171,9 +171,13 @@ def sg_fixtures():
         if K > 1:
             tr = np.concatenate([rng.integers(0, K, size=len(s)) for s in sa]).astype(np.uint16)
             gt = np.concatenate([rng.integers(0, K, size=len(s) + 1) for s in sa]).astype(np.uint16)
-        cases.append((name, alpha, mat, gaps, sa, sb, tr, gt))
-    for name, alpha, mat, gaps, sa, sb, tr, gt in cases:
+        mat2 = (mat + rng.normal(0, 0.3, size=mat.shape)).round(3)
+        gaps2 = (gaps + rng.uniform(0, 0.2, size=gaps.shape)).round(3)
+        cases.append((name, alpha, mat, gaps, sa, sb, tr, gt, mat2, gaps2))
+    for name, alpha, mat, gaps, sa, sb, tr, gt, mat2, gaps2 in cases:
         pre = f"{name}_"
+        out[pre + "mat2"] = mat2
+        out[pre + "gaps2"] = gaps2
         out[pre + "alpha"] = np.array(alpha)
         out[pre + "mat"] = mat
         out[pre + "gaps"] = gaps
@@ -196,6 +200,21 @@ def sg_fixtures():
                 key = f"{pre}soft_g{gm}_e{fe}_"
                 out[key + "scores"] = r["scores"]
                 out[key + "grads"] = r["grads"]
+                if fe == 12 and tr is None:
+                    # banded re-alignment (glocal only; the reference refuses other ends banded),
+                    # around the guides of the params scored, after a parameter step
+                    for prec in (32, 64):
+                        rb = oracle.ref_run(prec, gm, 2, 1, alpha, mat, gaps, sa, sb, band=4, mat2=mat2,
+                                            gaps2=gaps2, free_ends=fe)
+                        key = f"{pre}band{prec}_g{gm}_e{fe}_"
+                        out[key + "scores"] = rb["scores"]
+                        out[key + "grads"] = rb["grads"]
+                        out[key + "guides"] = rb["guides"]
+                    rb = oracle.ref_run(64, gm, 2, 2, alpha, mat, gaps, sa, sb, soft_impl=2, temperature=1.0,
+                                        band=4, mat2=mat2, gaps2=gaps2, free_ends=fe)
+                    key = f"{pre}softband_g{gm}_e{fe}_"
+                    out[key + "scores"] = rb["scores"]
+                    out[key + "grads"] = rb["grads"]
     np.savez_compressed(os.path.join(HERE, "semiglobal.npz"), **out)
     print("semiglobal.npz:", len(out), "arrays")
 

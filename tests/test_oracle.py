@@ -98,6 +98,20 @@ def test_semiglobal_fixtures(name):
             s, g = oracle.soft(gm, 2, mat, gaps, enc, 1.0, free_ends=fe)
             np.testing.assert_allclose(s, z[key + "scores"], rtol=1e-11, atol=1e-11, err_msg=key)
             np.testing.assert_allclose(g, z[key + "grads"], rtol=1e-9, atol=1e-10, err_msg=key)
+            if fe == 12 and tr is None:
+                mat2, gaps2 = z[pre + "mat2"], z[pre + "gaps2"]
+                for prec in (32, 64):
+                    o = oracle.hard(prec, gm, 2, mat, gaps, enc, free_ends=fe)
+                    key = f"{pre}band{prec}_g{gm}_e{fe}_"
+                    ob = oracle.hard(prec, gm, 2, mat2, gaps2, enc, guides_in=o["guides"], band=4, free_ends=fe)
+                    np.testing.assert_array_equal(ob["scores"], z[key + "scores"], err_msg=key)
+                    np.testing.assert_array_equal(ob["grads"], z[key + "grads"], err_msg=key)
+                    np.testing.assert_array_equal(ob["guides"], z[key + "guides"], err_msg=key)
+                o = oracle.hard(64, gm, 2, mat, gaps, enc, free_ends=fe)
+                key = f"{pre}softband_g{gm}_e{fe}_"
+                s, g = oracle.soft(gm, 2, mat2, gaps2, enc, 1.0, guides_in=o["guides"], band=4, free_ends=fe)
+                np.testing.assert_allclose(s, z[key + "scores"], rtol=1e-11, atol=1e-11, err_msg=key)
+                np.testing.assert_allclose(g, z[key + "grads"], rtol=1e-9, atol=1e-10, err_msg=key)
 
 
 def test_blocked_sum_order():
