@@ -45,8 +45,8 @@ typedef struct nwg_job {
     int free_ends;     /* mode 2 (semi-global, the reference's AlignMode::Glocal with kSgFree*
                           bits, simd_levels.hpp:170-182): 1 a_begin (column 0 a free start),
                           2 a_end (column n's cells ends), 4 b_begin (row 0 a free start),
-                          8 b_end (row m's cells ends); "glocal" is 12, "overlap" 15.  Full DP,
-                          traceback Pointers; banded re-alignment refused */
+                          8 b_end (row m's cells ends); "glocal" is 12, "overlap" 15.  Traceback
+                          Pointers; banded re-alignment with 12 only (aligner.hpp:2222-2231) */
 } nwg_job;
 
 /* Last error message of the calling thread ("" if none). */

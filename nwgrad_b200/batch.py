@@ -321,9 +321,10 @@ class SeqPairBatch:
         tb = {"hirschberg": 3, "hirschberg_pmax": 4}.get(self._traceback, 0)
         if tb and grad_mode != 2 and band < 0:
             self._check_hirschberg()
-        if self._am == 2 and band >= 0:
-            raise NotImplementedError(f"nwgrad_b200: banded re-alignment with mode \"{self._mode}\" "
-                                      f"(semi-global ends) is not available in this build")
+        if self._am == 2 and band >= 0 and self._sg != SG_GLOCAL:
+            # aligner.hpp:2222-2231 (check_problem)
+            raise ValueError("nwgrad: guide-banded alignment supports the semi-global ends of \"glocal\" "
+                             "only; align these free ends with the full DP")
         return Job(_GAP[self._gap_model], self._am, grad_mode, self._precision, band,
                    int(bool(keep_paths)), float(self.soft_temperature), soft_double, lanes, rows,
                    tb, int(self._hb_cutoff), int(self._sg))

@@ -1302,8 +1302,9 @@ int nwg_run(nwg_store* s, const nwg_job* job, void* stream, double* total) {
         if (J.mode == 2) {
             if (J.free_ends < 0 || J.free_ends > 15)
                 throw Error(NWG_EINVAL, "nwgrad: free_ends must be a 4-bit flag set (0..15), got " + std::to_string(J.free_ends));
-            if (J.band >= 0)
-                throw Error(NWG_EINVAL, "nwgrad_b200: banded re-alignment with semi-global ends is not available");
+            if (J.band >= 0 && J.free_ends != 12)
+                throw Error(NWG_EINVAL, "nwgrad: guide-banded alignment supports the semi-global ends of \"glocal\" "
+                                        "only; align these free ends with the full DP");
         }
         if (J.precision != 32 && J.precision != 64) throw Error(NWG_EINVAL, "precision must be 32 or 64");
         if (J.band >= 0 && !s->have_guides) throw Error(NWG_ESTATE, "banded_grad() needs a guide; call score_and_grad() first");

@@ -112,7 +112,7 @@ constexpr int kHardSpinLimit = 1 << 22;
 template <class T, bool AFF, bool LOC, bool TR, int G, int R, bool BAND = false, bool MW = false, bool SG = false>
 __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArgs A) {
     static_assert(!MW || (G == 32 && !BAND), "several warps per pair: 32 lanes, full DP");
-    static_assert(!SG || (!LOC && !BAND && !MW), "semi-global ends: Global fills, full DP, one warp per pair");
+    static_assert(!SG || (!LOC && !MW), "semi-global ends: Global fills, one warp per pair");
     constexpr int GR = G * R;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* smat = reinterpret_cast<T*>(smem_raw);
@@ -228,7 +228,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
         uint8_t* __restrict__ codes = A.codes + A.code_off[p];
         const int nstripes = (m + GR - 1) / GR;
         // the band (full DP: every column of every row; borders reach every row / column)
-        BandRows bw{BAND ? A.guide + ao + p : nullptr, A.band, m, n, !LOC};
+        BandRows bw{BAND ? A.guide + ao + p : nullptr, A.band, m, n, !LOC && !SG};   // glocal: row m's own band
         int brows = m, bcols = n;            // rows / columns whose border cells are charged
         if constexpr (BAND) {
             brows = 0;
@@ -248,7 +248,8 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
             T vm, vx, vy;
             if (sg_c0) { vm = T(0); vx = ninf<T>(); vy = ninf<T>(); }
             else {
-                const T bc = border_col0<T, AFF, TR>(A, bx0p, m, ugob, ugeb);
+                // banded: column 0's cell of row m is charged only within the border rows
+                const T bc = (!BAND || m <= brows) ? border_col0<T, AFF, TR>(A, bx0p, m, ugob, ugeb) : ninf<T>();
                 vm = AFF ? ninf<T>() : bc; vx = AFF ? bc : ninf<T>(); vy = ninf<T>();
             }
             erow.offer(m, 0, vm, vx, vy);

@@ -12,7 +12,12 @@ HardFn pick_band(Geo g) {
 // semi-global ends: their own instantiations, so the Global fills carry none of their state
 template <class T, bool AFF, bool TR>
 HardFn pick_sg(Geo g) {
-    if (g.band || g.mw > 1) return nullptr;
+    if (g.band) {   // glocal ends, banded re-alignment
+        if (g.G == 32 && g.R == 1) return &hard_fill_kernel<T, AFF, false, TR, 32, 1, true, false, true>;
+        if (g.G == 32 && g.R == 2) return &hard_fill_kernel<T, AFF, false, TR, 32, 2, true, false, true>;
+        return nullptr;
+    }
+    if (g.mw > 1) return nullptr;
 #define NWG_H(GG, RR) if (g.G == GG && g.R == RR) return &hard_fill_kernel<T, AFF, false, TR, GG, RR, false, false, true>;
     NWG_H(1, 8) NWG_H(1, 16) NWG_H(1, 24) NWG_H(1, 32) NWG_H(32, 1) NWG_H(32, 2) NWG_H(32, 4) NWG_H(32, 8)
 #undef NWG_H

@@ -210,7 +210,7 @@ template <class T, bool AFF, bool LOC, bool TR, int G, int R, bool MW = false, b
 __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2 : 4) : 1))) soft_kernel(const SoftArgs A) {
     static_assert(!MW || (G == 32 && !TR), "several warps per pair: 32 lanes, untracked");
     static_assert(!BAND || (G == 32 && !MW), "banded: 32 lanes, one warp per pair");
-    static_assert(!SG || (!LOC && !BAND), "semi-global ends: Global kernels, full DP");
+    static_assert(!SG || !LOC, "semi-global ends: Global kernels");
     constexpr int GR = G * R;
     constexpr int NV = AFF ? 3 : 1;          // values per cell
     constexpr int CV = NV * R;               // values per lane column
@@ -312,7 +312,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
         auto jlo_of = [&](int i) { return max(1, gd[i] - bw); };
         auto jlo0_of = [&](int i) { return max(0, gd[i] - bw); };
         auto jhi_of = [&](int i) {
-            if (!LOC && i == m) return n;
+            if (!LOC && !SG && i == m) return n;   // glocal: row m's own band
             int hi = gd[i] + bw;
             if (i < m) hi = max(hi, gd[i + 1] - 1 + bw);
             return min(n, hi);
@@ -483,7 +483,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                                 if (j < blo[r] || j > bhi[r]) { fm = T(0); fx = T(0); fy = T(0); }
                             } else if constexpr (!LOC) {
                                 // the charged borders (linear keeps them in M)
-                                if (i == 0 && j > bcols) { fy = T(0); if constexpr (!AFF) fm = T(0); }
+                                if (i == 0 && j > bcols && !sg_r0) { fy = T(0); if constexpr (!AFF) fm = T(0); }
                                 if (j == 0 && i > brows) { fx = T(0); if constexpr (!AFF) fm = T(0); }
                             }
                         }

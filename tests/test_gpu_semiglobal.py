@@ -69,6 +69,27 @@ def test_semiglobal_reference_fixtures(name):
             key = f"{pre}soft_g{gm}_e{fe}_"
             np.testing.assert_allclose(b.scores(), z[key + "scores"], rtol=SOFT_RTOL, atol=1e-5, err_msg=key)
             _soft_close(_flat(b, len(sa)), z[key + "grads"])
+            if fe == 12 and tr is None:
+                # banded re-alignment around the guides of the params scored, after a step
+                p2 = nw.AlignParams.from_arrays(z[pre + "mat2"], z[pre + "gaps2"], alphabet=alpha)
+                for prec in (32, 64):
+                    cls = nw.SeqPairBatch if prec == 32 else nw.SeqPairBatchDouble
+                    hb = cls(sa, sb, p, grad_mode="hard", **kw)
+                    hb.score_and_grad()
+                    hb.set_params(p2)
+                    hb.banded_grad(4)
+                    key = f"{pre}band{prec}_g{gm}_e{fe}_"
+                    assert np.array_equal(hb.scores(), z[key + "scores"]), key
+                    assert np.array_equal(_flat(hb, len(sa)), z[key + "grads"]), key
+                    assert np.array_equal(hb.guides(), z[key + "guides"]), key
+                # the reference's soft fixtures ran in double: its guides are the float64 Viterbi's
+                b = nw.SeqPairBatchDouble(sa, sb, p, grad_mode="soft", **kw)
+                b.score_and_grad()
+                b.set_params(p2)
+                b.banded_grad(4)
+                key = f"{pre}softband_g{gm}_e{fe}_"
+                np.testing.assert_allclose(b.scores(), z[key + "scores"], rtol=SOFT_RTOL, atol=1e-5, err_msg=key)
+                _soft_close(_flat(b, len(sa)), z[key + "grads"])
 
 
 def _pairs(rng, long=False):
@@ -163,8 +184,12 @@ def test_semiglobal_refusals_and_api():
     b = nw.SeqPairBatch(sa, sb, p, mode="glocal", grad_mode="hard")
     assert b.mode == "glocal" and b.free_ends == (False, False, True, True)
     b.score_and_grad()
-    with pytest.raises(NotImplementedError):
-        b.banded_grad(8)
+    full = b.scores().copy()
+    b.banded_grad(8)                          # glocal ends band (the reference's guide band)
+    ov = nw.SeqPairBatch(sa, sb, p, mode="overlap", grad_mode="hard")
+    ov.score_and_grad()
+    with pytest.raises(ValueError, match="glocal"):
+        ov.banded_grad(8)
     h = nw.SeqPairBatch(sa, sb, p, mode="glocal", grad_mode="hard", traceback="hirschberg")
     with pytest.raises(NotImplementedError):
         h.score_and_grad()
@@ -172,7 +197,7 @@ def test_semiglobal_refusals_and_api():
     short = nw.SeqPairBatch(sa[:2], sb[:2], p, mode="glocal", grad_mode="hard", traceback="hirschberg")
     short.hb_cutoff = 1000
     short.score_and_grad()
-    assert np.array_equal(short.scores(), b.scores()[:2])
+    assert np.array_equal(short.scores(), full[:2])
     o = nw.SeqPairBatch(sa, sb, p, mode="semiglobal", free_ends=("a_begin", "b_end"), grad_mode="soft")
     assert o.free_ends == (True, False, False, True)
     assert nw.SeqPairBatch(sa, sb, p, mode="overlap").free_ends == (True, True, True, True)
@@ -184,3 +209,34 @@ def test_semiglobal_refusals_and_api():
     g0.score_and_grad()
     g1.score_and_grad()
     assert np.array_equal(g0.scores(), g1.scores())
+
+
+@pytest.mark.parametrize("gm", [0, 1])
+def test_glocal_banded_oracle(gm):
+    """Banded re-alignment with glocal ends on multi-stripe pairs (miRNA-like A in long B and
+    homologs): hard bit for bit, soft within tolerance of the oracle's banded forward-backward."""
+    rng = np.random.default_rng(3500 + gm)
+    mat = rand_matrix(rng, 20, 1, True)
+    gaps = np.array([[11.0, 1.0, 11.0, 1.0]]) if gm else np.array([[0.0, 3.0, 0.0, 2.0]])
+    sa = rand_seqs(rng, 8, 18, 26, AA) + rand_seqs(rng, 10, 60, 300, AA)
+    sb = rand_seqs(rng, 8, 200, 600, AA) + [mutate(rng, s, AA) for s in sa[8:]]
+    p = nw.AlignParams.from_arrays(mat, gaps, alphabet=AA)
+    q = nw.AlignParams.from_arrays(mat + 0.5, gaps + 0.25, alphabet=AA)
+    enc = oracle.Encoded(encode(AA, sa), encode(AA, sb))
+    kw = dict(gap_model=("linear", "affine")[gm], mode="glocal")
+    o = oracle.hard(32, gm, 2, mat, gaps, enc, free_ends=12)
+    ob = oracle.hard(32, gm, 2, mat + 0.5, gaps + 0.25, enc, guides_in=o["guides"], band=6, free_ends=12)
+    b = nw.SeqPairBatch(sa, sb, p, grad_mode="hard", **kw)
+    b.score_and_grad()
+    b.set_params(q)
+    b.banded_grad(6)
+    assert np.array_equal(b.scores(), ob["scores"])
+    assert np.array_equal(_flat(b, len(sa)), ob["grads"])
+    assert np.array_equal(b.guides(), ob["guides"])
+    so, go = oracle.soft(gm, 2, mat + 0.5, gaps + 0.25, enc, 1.0, guides_in=o["guides"], band=6, free_ends=12)
+    s = nw.SeqPairBatch(sa, sb, p, grad_mode="soft", **kw)
+    s.score_and_grad()
+    s.set_params(q)
+    s.banded_grad(6)
+    np.testing.assert_allclose(s.scores(), so, rtol=SOFT_RTOL, atol=1e-5)
+    _soft_close(_flat(s, len(sa)), go)
