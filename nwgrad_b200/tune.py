@@ -154,7 +154,8 @@ def describe(entry) -> str:
 def _key(batch, sc: int) -> str:
     return "|".join(str(x) for x in (_device_name(batch._device), "soft" if _soft(batch) else "hard",
                                      batch._gap_model, batch._mode, batch._precision, batch._alpha.size,
-                                     batch._params.num_sets, int(batch._tracked), sc))
+                                     batch._params.num_sets, int(batch._tracked), sc)) + \
+        (f"|ends{batch._sg}" if getattr(batch, "_am", 0) == 2 else "")   # semiglobal: its free ends
 
 
 def tune(batch, sample_pairs: int = 65536, force: bool = False, verbose: bool = False, reps: int = 2,
