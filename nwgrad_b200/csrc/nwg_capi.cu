@@ -917,9 +917,11 @@ void soft_weights(const nwg_store* s, const nwg_job& J, std::vector<T>& w, std::
     }
 }
 
-// One soft pass (precision T) over `pairs` (all pairs when null).
+// One soft pass (precision T) over `pairs` (all pairs when null).  one_lane (a rerun): every
+// pair at one lane per pair.
 template <class T>
-void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vector<int32_t>* subset) {
+void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vector<int32_t>* subset,
+               bool one_lane = false) {
     const bool aff = J.gap_model == 1, loc = J.mode == 1, tr = s->tracked();
     std::vector<T> w, gw;
     bool ovf;
@@ -954,7 +956,8 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
         const bool lane_ok = int64_t(s->K) * s->N * s->N * sizeof(T) * 32 <= 48 * 1024;
         for (int32_t p : *subset) {
             const int m = int(s->oa[p + 1] - s->oa[p]), nb = int(s->ob[p + 1] - s->ob[p]);
-            const Geo g = J.band >= 0 ? Geo{32, 4, true} : pick_geo(true, m + 1, nb, J.lanes, J.rows, lane_ok);
+            const Geo g = J.band >= 0 ? Geo{32, 4, true}
+                        : one_lane ? Geo{1, 8} : pick_geo(true, m + 1, nb, J.lanes, J.rows, lane_ok);
             auto key = std::make_tuple(g.G, g.R, size_class(m + 1, nb));
             auto itb = idx.find(key);
             int bi;
@@ -1108,15 +1111,24 @@ void run_soft(nwg_store* s, const nwg_job& J, cudaStream_t st) {
         if (s->h_status[p]) refused.push_back(int32_t(p));
     }
     if (!refused.empty()) {
-        if (f32) {
-            soft_pass<double>(s, J, st, &refused);
-            std::vector<int32_t> hs(size_t(s->n));
+        // refused pairs rerun in double; those still refused (seen: a short A against a long B
+        // under global ends, at several lanes per pair) rerun in double at one lane per pair,
+        // where the shared-memory histograms of that geometry fit
+        std::vector<int32_t> hs(size_t(s->n));
+        auto rerun = [&](std::vector<int32_t>& ps, bool one_lane) {
+            soft_pass<double>(s, J, st, &ps, one_lane);
             NWG_CUDA(cudaMemcpyAsync(hs.data(), s->status.p, size_t(s->n) * 4, cudaMemcpyDeviceToHost, st));
             NWG_CUDA(cudaStreamSynchronize(st));
-            for (int32_t p : refused) s->h_status[p] = hs[p] ? 2 : 1;
-        } else {
-            for (int32_t p : refused) s->h_status[p] = 2;
-        }
+            std::vector<int32_t> left;
+            for (int32_t p : ps) if (hs[p]) left.push_back(p);
+            ps.swap(left);
+        };
+        std::vector<int32_t> left = refused;
+        if (f32) rerun(left, false);
+        const bool lane_fits = int64_t(s->K) * s->N * s->N * 8 * 32 <= 48 * 1024;
+        if (!left.empty() && J.band < 0 && lane_fits) rerun(left, true);
+        for (int32_t p : refused) s->h_status[p] = f32 ? 1 : 0;   // 1: the float32 pass refused it
+        for (int32_t p : left) s->h_status[p] = 2;
         for (int32_t p : refused)
             if (s->h_status[p] == 2) {
                 char buf[256];

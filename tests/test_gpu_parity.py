@@ -382,3 +382,30 @@ def test_soft_banded(prec, gm, am, bw):
     flat = np.concatenate([gmat.reshape(len(sa), -1), ggap.reshape(len(sa), -1)], axis=1)
     scale = np.maximum(np.abs(go).max(axis=1, keepdims=True), 1.0)
     assert (np.abs(flat - go) / scale).max() <= SOFT_RTOL
+
+
+@pytest.mark.parametrize("prec", [32, 64])
+@pytest.mark.parametrize("geo", [(8, 4), (32, 4)])
+def test_soft_long_gap_chains_rerun_one_lane(prec, geo):
+    """A short A against a long B under global ends, forced to several lanes per pair: those
+    lanes refuse the pair in float and double, which then reruns at one lane per pair in double
+    and matches the oracle."""
+    rng = np.random.default_rng(5100 + prec + geo[0] + geo[1])
+    alpha = "ACGTU"
+    mat = np.full((1, 5, 5), -4.0)
+    for x, y in ((0, 3), (1, 2), (2, 1), (3, 0), (4, 0), (2, 4)):
+        mat[0, x, y] = 5.0
+    gaps = np.array([[5.0, 2.0, 5.0, 2.0]])
+    sa = ["".join(rng.choice(list("ACGU"), size=22)) for _ in range(6)]
+    sb = ["".join(rng.choice(list("ACGT"), size=int(rng.integers(500, 900)))) for _ in range(6)]
+    cls = nw.SeqPairBatch if prec == 32 else nw.SeqPairBatchDouble
+    b = cls(sa, sb, _params(alpha, mat, gaps), grad_mode="soft")
+    b._tune = geo
+    b.score_and_grad()
+    enc = oracle.Encoded(encode(alpha, sa), encode(alpha, sb))
+    so, go = oracle.soft(1, 0, mat, gaps, enc)
+    np.testing.assert_allclose(b.scores(), so, rtol=SOFT_RTOL, atol=1e-5)
+    gmat, ggap = b.grads()
+    flat = np.concatenate([gmat.reshape(len(sa), -1), ggap.reshape(len(sa), -1)], axis=1)
+    scale = np.maximum(np.abs(go).max(axis=1, keepdims=True), 1.0)
+    assert (np.abs(flat - go) / scale).max() <= SOFT_RTOL
