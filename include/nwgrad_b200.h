@@ -106,6 +106,14 @@ int nwg_set_geometry_costs(nwg_store* s, int soft, int size_class, int n, const 
  * path keeps a whole table per thread). */
 int nwg_set_memory(nwg_store* s, int64_t scratch_budget_bytes, int64_t checkpoint_bytes);
 
+/* Long pairs run with several warps per pair that wait on one another's progress; each wait
+ * polls at most `polls` times (default 4194304, about a quarter second at the poll interval),
+ * then the kernel marks the pair, finishes without waiting further and the call fails with
+ * NWG_ECUDA ("a wait ... ran out") instead of hanging.  The store stays usable.  polls < 1 is
+ * refused.  No counterpart in the reference (its CPU threads never wait on one another inside a
+ * pair). */
+int nwg_set_spin_limit(nwg_store* s, int polls);
+
 /* Per-pair scores (n_pairs doubles).  Replaces BatchEngine::scores (batch_engine.hpp:689). */
 int nwg_scores(nwg_store* s, double* out);
 
@@ -190,7 +198,10 @@ const char* nwg_server_last_error(void);
  * the output.  mat (nalpha x nalpha, nalpha <= 32) and gaps (4) are host doubles.  The
  * float32 score-only fill of nwg_run (bit-identical scores), one parameter set, untracked.
  * Scratch comes from a 24 MiB array every GPU that loads the library reserves until exit;
- * limit: B at most 2047 residues (max_len_b states the batch's longest B; larger: NWG_EINVAL).
+ * limits: B at most 2047 residues (max_len_b states the batch's longest B; larger: NWG_EINVAL)
+ * and A at most 2^31 - 256.  The offsets live on the device, so the call cannot check each
+ * pair: a pair over either limit (max_len_b understated) gets a NaN score and the call still
+ * returns NWG_OK.  The parameters travel by value in the kernel launch (no host copy).
  * The first call on a device looks the array up (cudaGetSymbolAddress) -- make it before any
  * stream capture.  Calls share that array: calls whose kernels overlap on the GPU race.
  * Errors: nwg_noalloc_last_error(). */

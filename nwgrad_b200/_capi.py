@@ -55,13 +55,14 @@ def lib():
     L.nwg_status.argtypes = [C.c_void_p, _i32p]
     L.nwg_last_timing.argtypes = [C.c_void_p, _dp, _i64p]
     L.nwg_set_memory.argtypes = [C.c_void_p, C.c_int64, C.c_int64]
+    L.nwg_set_spin_limit.argtypes = [C.c_void_p, C.c_int]
     L.nwg_set_geometry.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int]
     L.nwg_set_graphs.argtypes = [C.c_void_p, C.c_int]
     L.nwg_set_geometry_costs.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, _i32p, _i32p, _dp]
     L.nwg_graph_stats.argtypes = [C.c_void_p, _i64p, _i64p]
     for name in ("nwg_store_create", "nwg_store_destroy", "nwg_params_set", "nwg_run", "nwg_scores",
                  "nwg_grads", "nwg_reduce", "nwg_guides", "nwg_set_guides", "nwg_resolve_guides", "nwg_paths", "nwg_status",
-                 "nwg_last_timing", "nwg_set_memory", "nwg_set_geometry", "nwg_set_graphs", "nwg_graph_stats", "nwg_set_geometry_costs"):
+                 "nwg_last_timing", "nwg_set_memory", "nwg_set_spin_limit", "nwg_set_geometry", "nwg_set_graphs", "nwg_graph_stats", "nwg_set_geometry_costs"):
         getattr(L, name).restype = C.c_int
     _lib = L
     return L

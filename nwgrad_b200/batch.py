@@ -492,6 +492,17 @@ class SeqPairBatch:
             check(self._store._L.nwg_scores(self._store.h, ptr(out, _capi._dp)))
         return out
 
+    def soft_status(self) -> np.ndarray:
+        """Per pair, how the last soft pass computed it (low 8 bits): 0 in the batch's precision,
+        1 refused by the float32 pass and computed in double -- the reference's kF32Refused flag
+        (batch_engine.hpp:1285).  Bits 8 and up give the float32 pass's reasons: 1 a value out
+        of range, 2 Z out of range, 4 a count's scale factor out of range, 8 a count out of
+        range, 16 the lost-mass bound above 2^-24, 32 a weight out of range."""
+        out = np.zeros(self._n, np.int32)
+        if self._n:
+            check(self._store._L.nwg_status(self._store.h, ptr(out, _capi._i32p)))
+        return out
+
     def grads(self):
         """Per-pair gradients: (N, n, n) matrices and (N, 4) gaps; tracked: (N, K, n, n), (N, K, 4)."""
         if self._n == 0:
@@ -781,6 +792,11 @@ class SeqPairBatch:
         table size above which only stripe boundaries are kept and each stripe is recomputed
         before its backward (bit-identical results).  -1 keeps the current value."""
         check(self._store._L.nwg_set_memory(self._store.h, int(scratch_budget_bytes), int(checkpoint_bytes)))
+
+    def set_spin_limit(self, polls: int = 1 << 22) -> None:
+        """Polls a wait between the warps of one long pair makes before it gives up: the call
+        then raises RuntimeError instead of hanging, and the batch stays usable."""
+        check(self._store._L.nwg_set_spin_limit(self._store.h, int(polls)))
 
     def use_graphs(self, enable: bool = True) -> None:
         """Run each plan's per-bucket launches as one captured CUDA graph (the default), replayed

@@ -21,11 +21,12 @@ LIB = os.path.join(OUT_DIR, "libnwgrad_b200.so")
 INCLUDE = os.path.join(HERE, "..", "include")
 # (object name, source, extra defines)
 UNITS = [
-    ("capi", "nwg_capi.cu", []),
+    (f"soft_{t}_am{am}", "nwg_soft_inst.cu", [f"-DNWG_T={ty}", f"-DNWG_SOFT_AM={am}", f"-DNWG_SOFT_FN=soft_fn_{t}_am{am}"])
+    for t, ty in (("f32", "float"), ("f64", "double")) for am in (0, 1, 2)
+] + [
     ("hard_f32", "nwg_hard_inst.cu", ["-DNWG_T=float", "-DNWG_HARD_FN=hard_fn_f32"]),
     ("hard_f64", "nwg_hard_inst.cu", ["-DNWG_T=double", "-DNWG_HARD_FN=hard_fn_f64"]),
-    ("soft_f32", "nwg_soft_inst.cu", ["-DNWG_T=float", "-DNWG_SOFT_FN=soft_fn_f32"]),
-    ("soft_f64", "nwg_soft_inst.cu", ["-DNWG_T=double", "-DNWG_SOFT_FN=soft_fn_f64"]),
+    ("capi", "nwg_capi.cu", []),
     ("noalloc", "nwg_noalloc.cu", []),
     ("server", "nwg_server.cu", []),
     ("hb", "nwg_hb.cu", []),

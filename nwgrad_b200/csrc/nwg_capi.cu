@@ -233,7 +233,11 @@ template <class T> HardFn hard_fn_rt(bool aff, int am, bool tr, Geo g) {
     return sizeof(T) == 4 ? nwg::hard_fn_f32(aff, am, tr, g) : nwg::hard_fn_f64(aff, am, tr, g);
 }
 template <class T> SoftFn soft_fn_rt(bool aff, int am, bool tr, Geo g) {
-    return sizeof(T) == 4 ? nwg::soft_fn_f32(aff, am, tr, g) : nwg::soft_fn_f64(aff, am, tr, g);
+    if (sizeof(T) == 4)
+        return am == 2 ? nwg::soft_fn_f32_am2(aff, tr, g) : am == 1 ? nwg::soft_fn_f32_am1(aff, tr, g)
+                                                          : nwg::soft_fn_f32_am0(aff, tr, g);
+    return am == 2 ? nwg::soft_fn_f64_am2(aff, tr, g) : am == 1 ? nwg::soft_fn_f64_am1(aff, tr, g)
+                                                      : nwg::soft_fn_f64_am0(aff, tr, g);
 }
 
 // The kernel geometries (lanes per pair G, rows per lane R) each path is instantiated for.
@@ -374,6 +378,7 @@ struct nwg_store {
     bool plain = false;
     int64_t scratch_budget = -1;   // bytes of soft scratch one call may hold (-1: from the device's memory)
     int64_t ck_threshold = int64_t(16) << 20;     // soft: forward tables above this are checkpointed
+    int spin_limit = nwg::kSpinLimit;             // several warps per pair: polls before a wait gives up
     DBuf stripe_tab;
     DBuf hb_pairs;                      // the pairs a Hirschberg run splits
     std::vector<int32_t> h_status;
@@ -777,6 +782,7 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
         A.row_stride = 3 * (int64_t(B.maxn) + 1);
         A.score = s->score.as<double>(); A.end = s->end.as<int32_t>();
         A.ends = ends;
+        A.spin_limit = s->spin_limit;
         fills.push_back(make_launch(reinterpret_cast<const void*>(fn), unsigned(blocks), hblock, smem, A));
         fill_args.push_back(A);
     }
@@ -917,11 +923,9 @@ void soft_weights(const nwg_store* s, const nwg_job& J, std::vector<T>& w, std::
     }
 }
 
-// One soft pass (precision T) over `pairs` (all pairs when null).  one_lane (a rerun): every
-// pair at one lane per pair.
+// One soft pass (precision T) over `subset` (all pairs when null).
 template <class T>
-void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vector<int32_t>* subset,
-               bool one_lane = false) {
+void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vector<int32_t>* subset) {
     const bool aff = J.gap_model == 1, loc = J.mode == 1, tr = s->tracked();
     std::vector<T> w, gw;
     bool ovf;
@@ -939,6 +943,8 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
     int pw = 1;
     while (pw * 2 <= std::min(renorm, sizeof(T) == 4 ? 8 : 16)) pw *= 2;
     renorm = pw;
+    // after the gap weights: the float32 lost-mass charge per unit of F^ + B^ (nwg_soft.cuh)
+    gw.push_back(static_cast<T>(16.0 + 16.0 * std::min(wmax, 1e30)));
     // the weights go to buffers the store keeps (one per precision), so a captured sequence
     // reads this call's weights at the same address
     DBuf& dw = sizeof(T) == 4 ? s->swf : s->swd;
@@ -957,7 +963,7 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
         for (int32_t p : *subset) {
             const int m = int(s->oa[p + 1] - s->oa[p]), nb = int(s->ob[p + 1] - s->ob[p]);
             const Geo g = J.band >= 0 ? Geo{32, 4, true}
-                        : one_lane ? Geo{1, 8} : pick_geo(true, m + 1, nb, J.lanes, J.rows, lane_ok);
+                        : pick_geo(true, m + 1, nb, J.lanes, J.rows, lane_ok);
             auto key = std::make_tuple(g.G, g.R, size_class(m + 1, nb));
             auto itb = idx.find(key);
             int bi;
@@ -1060,9 +1066,11 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
         A.ends = J.mode == 2 ? J.free_ends : 0;
         A.score = s->score.as<double>(); A.grad = s->grad.as<double>(); A.gstride = s->gstride;
         A.status = s->status.as<int32_t>();
+        A.spin_limit = s->spin_limit;
         if (ovf) {
             // a weight overflows T: every pair of this bucket is out of range in T
-            mark_status_kernel<<<unsigned((items + 255) / 256), 256, 0, st>>>(A.order, items, A.status, 1);
+            mark_status_kernel<<<unsigned((items + 255) / 256), 256, 0, st>>>(A.order, items, A.status,
+                                                                                nwg::kSoftWeights);
             NWG_CUDA(cudaGetLastError());
             s->last_launches++;
             continue;
@@ -1089,56 +1097,69 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
     run_launches(s, gc, launches, st, concurrent);
 }
 
+// The reason a soft pass refused a pair, from its status bits (the first that applies).
+std::string soft_refusal_reason(int32_t why) {
+    if (why & nwg::kSoftWeights) return "a substitution or gap weight exp(score / T) overflows";
+    if (why & nwg::kSoftRange) return "a forward or backward value overflows";
+    if (why & nwg::kSoftZ) return "the partition function Z is zero or out of range";
+    if (why & nwg::kSoftScale) return "the forward and backward mass of a cell sit too far apart for the count scale";
+    if (why & nwg::kSoftCounts) return "an expected count overflows";
+    if (why & nwg::kSoftLoss) return "mass lost to underflow could move a posterior by more than 2^-24";
+    return "out of range";
+}
+
 void run_soft(nwg_store* s, const nwg_job& J, cudaStream_t st) {
     s->score.need(size_t(std::max<int64_t>(s->n, 1)) * 8, st);
     s->grad.need(size_t(s->n) * s->gstride * 8 + 8, st);
     s->status.need(size_t(std::max<int64_t>(s->n, 1)) * 4, st);
     NWG_CUDA(cudaMemsetAsync(s->status.p, 0, size_t(std::max<int64_t>(s->n, 1)) * 4, st));
-    // Banded: the band masks leave whole lane-columns at zero, and a lane whose values are all
-    // zero keeps a stale power-of-two exponent; over a narrow band that can misalign values in
-    // float's range.  The double pass's range makes it harmless, so banded runs go to double.
-    const bool f32 = J.precision == 32 && !J.soft_double && J.band < 0;
+    const bool f32 = J.precision == 32 && !J.soft_double;
     if (f32) soft_pass<float>(s, J, st, nullptr);
     else soft_pass<double>(s, J, st, nullptr);
     s->h_status.assign(size_t(s->n), 0);
     if (s->n) NWG_CUDA(cudaMemcpyAsync(s->h_status.data(), s->status.p, size_t(s->n) * 4, cudaMemcpyDeviceToHost, st));
     NWG_CUDA(cudaStreamSynchronize(st));
+    auto stall_check = [&](const std::vector<int32_t>& hs) {
+        for (int64_t p = 0; p < s->n; ++p)
+            if (hs[size_t(p)] & nwg::kSoftStall)
+                throw Error(NWG_ECUDA, "nwgrad_b200: soft pass: a wait between the warps of pair " + std::to_string(p) +
+                                       " ran out (the kernel gave up instead of hanging)");
+    };
+    stall_check(s->h_status);
     std::vector<int32_t> refused;
-    for (int64_t p = 0; p < s->n; ++p) {
-        if (s->h_status[p] == 3)
-            throw Error(NWG_ECUDA, "nwgrad_b200: soft pass: a wait between the warps of pair " + std::to_string(p) +
-                                   " ran out (the kernel gave up instead of hanging)");
+    for (int64_t p = 0; p < s->n; ++p)
         if (s->h_status[p]) refused.push_back(int32_t(p));
-    }
-    if (!refused.empty()) {
-        // refused pairs rerun in double; those still refused (seen: a short A against a long B
-        // under global ends, at several lanes per pair) rerun in double at one lane per pair,
-        // where the shared-memory histograms of that geometry fit
+    if (refused.empty()) return;
+    // pairs the float32 pass refused (out of range, or a lost-mass bound above tolerance) rerun
+    // in double, as the reference's run_fwdbwd does (aligner.hpp:6554-6626); a pair the double
+    // pass refuses too is an error naming the reason
+    std::vector<int32_t> why(s->h_status.begin(), s->h_status.end());
+    std::vector<int32_t> left = refused;
+    if (f32) {
+        soft_pass<double>(s, J, st, &left);
         std::vector<int32_t> hs(size_t(s->n));
-        auto rerun = [&](std::vector<int32_t>& ps, bool one_lane) {
-            soft_pass<double>(s, J, st, &ps, one_lane);
-            NWG_CUDA(cudaMemcpyAsync(hs.data(), s->status.p, size_t(s->n) * 4, cudaMemcpyDeviceToHost, st));
-            NWG_CUDA(cudaStreamSynchronize(st));
-            std::vector<int32_t> left;
-            for (int32_t p : ps) if (hs[p]) left.push_back(p);
-            ps.swap(left);
-        };
-        std::vector<int32_t> left = refused;
-        if (f32) rerun(left, false);
-        const bool lane_fits = int64_t(s->K) * s->N * s->N * 8 * 32 <= 48 * 1024;
-        if (!left.empty() && J.band < 0 && lane_fits) rerun(left, true);
-        for (int32_t p : refused) s->h_status[p] = f32 ? 1 : 0;   // 1: the float32 pass refused it
-        for (int32_t p : left) s->h_status[p] = 2;
-        for (int32_t p : refused)
-            if (s->h_status[p] == 2) {
-                char buf[256];
-                std::snprintf(buf, sizeof buf,
-                              "nwgrad: soft path: pair %d (lengths %lld x %lld) does not fit the scaled "
-                              "probability-space forward-backward (a weight or a row overflows, typically a "
-                              "very low temperature or extreme scores)",
-                              p, (long long)(s->oa[p + 1] - s->oa[p]), (long long)(s->ob[p + 1] - s->ob[p]));
-                throw Error(NWG_ERANGE, buf);
-            }
+        NWG_CUDA(cudaMemcpyAsync(hs.data(), s->status.p, size_t(s->n) * 4, cudaMemcpyDeviceToHost, st));
+        NWG_CUDA(cudaStreamSynchronize(st));
+        stall_check(hs);
+        std::vector<int32_t> still;
+        for (int32_t p : left)
+            if (hs[size_t(p)]) { still.push_back(p); why[size_t(p)] = hs[size_t(p)]; }
+        left.swap(still);
+    }
+    // per pair: 1 the float32 pass refused it (reran in double), 2 every pass refused it; the
+    // first pass's kSoft* reason bits above bit 8
+    for (int32_t p : refused) s->h_status[p] = (f32 ? 1 : 0) | (s->h_status[p] << 8);
+    for (int32_t p : left) s->h_status[p] = 2 | (why[size_t(p)] << 8);
+    if (!left.empty()) {
+        const int32_t p = left.front();
+        char buf[512];
+        std::snprintf(buf, sizeof buf,
+                      "nwgrad: soft path: pair %d (lengths %lld x %lld) does not fit the scaled "
+                      "probability-space forward-backward in double precision: %s (typically a very low "
+                      "temperature or extreme scores)",
+                      p, (long long)(s->oa[p + 1] - s->oa[p]), (long long)(s->ob[p + 1] - s->ob[p]),
+                      soft_refusal_reason(why[size_t(p)]).c_str());
+        throw Error(NWG_ERANGE, buf);
     }
 }
 
@@ -1425,6 +1446,14 @@ int nwg_set_memory(nwg_store* s, int64_t scratch_budget_bytes, int64_t checkpoin
         if (!s) throw Error(NWG_EINVAL, "null store");
         if (scratch_budget_bytes >= 0) s->scratch_budget = std::max<int64_t>(scratch_budget_bytes, 1);
         if (checkpoint_bytes >= 0) s->ck_threshold = checkpoint_bytes;
+    });
+}
+
+int nwg_set_spin_limit(nwg_store* s, int polls) {
+    return guarded([&] {
+        if (!s) throw Error(NWG_EINVAL, "null store");
+        if (polls < 1) throw Error(NWG_EINVAL, "spin limit must be at least 1 poll");
+        s->spin_limit = polls;
     });
 }
 

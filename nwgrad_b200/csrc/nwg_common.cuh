@@ -70,6 +70,28 @@ template <> __device__ __forceinline__ double pow2i<double>(int e) {
     if (e > 1023) return __longlong_as_double(0x7ff0000000000000ll);
     return __longlong_as_double(static_cast<long long>(e + 1023) << 52);
 }
+// 2^e with gradual underflow: subnormal for float e in [-149, -127] (double: [-1074, -1023]),
+// 0 below, so a value scaled by it loses at most half the smallest subnormal.
+template <class T> __device__ __forceinline__ T pow2s(int e);
+template <> __device__ __forceinline__ float pow2s<float>(int e) {
+    if (e >= -126) return pow2i<float>(e);
+    if (e < -149) return 0.0f;
+    return __int_as_float(1 << (e + 149));
+}
+template <> __device__ __forceinline__ double pow2s<double>(int e) {
+    if (e >= -1022) return pow2i<double>(e);
+    if (e < -1074) return 0.0;
+    return __longlong_as_double(1ll << (e + 1074));
+}
+// v * 2^d for d <= 0 with gradual underflow: the result is v * 2^d rounded once into the
+// subnormal range (or 0 when below half the smallest subnormal for v < 2), never a
+// flush of a value that float could still hold.
+template <class T> __device__ __forceinline__ T scale_down(T v, int d) {
+    constexpr int lo = sizeof(T) == 4 ? -126 : -1022;
+    if (d >= lo) return v * pow2i<T>(d);
+    v *= pow2i<T>(lo);
+    return v * pow2s<T>(d - lo);
+}
 // floor(log2(x)) for a finite x > 0 (normal or subnormal handled via the bits).
 template <class T> __device__ __forceinline__ int ilog2(T x);
 template <> __device__ __forceinline__ int ilog2<float>(float x) {

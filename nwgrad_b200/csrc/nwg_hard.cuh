@@ -57,6 +57,7 @@ struct HardArgs {
     // (column 0 a free start), 2 a_end (column n's cells ends), 4 b_begin (row 0 a free start),
     // 8 b_end (row m's cells ends); 0: Global's charged borders and end (m, n)
     int ends;
+    int spin_limit;                            // several warps per pair: polls before a wait gives up
 };
 
 // The band of DP row i around guide g (aligner.hpp:2644-2700): columns [jlo, jhi].
@@ -105,8 +106,8 @@ __host__ __device__ inline size_t hard_mw_smem_bytes(int warps, int tsize) {
 // Several warps per pair (MW, long pairs): warp w fills stripes w, w + NW, ..., each stripe's
 // bottom row in its own scratch row, and waits (every 32 steps, bounded) until the warp filling
 // the stripe above has published enough steps -- the protocol of the soft kernel
-// (nwg_soft.cuh).  A wait that runs out marks the pair's end state 3 and the host fails the call.
-constexpr int kHardSpinLimit = 1 << 22;
+// (nwg_soft.cuh).  A wait that runs out (HardArgs::spin_limit polls) marks the pair's end
+// state 3 and the host fails the call.
 
 // SG: the semi-global ends of A.ends (Global fills only, full DP, a warp or lane per pair)
 template <class T, bool AFF, bool LOC, bool TR, int G, int R, bool BAND = false, bool MW = false, bool SG = false>
@@ -143,7 +144,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
         if constexpr (MW) {
             int k = 0;
             while (!stalled && prog[pw] < target) {
-                if (++k > kHardSpinLimit) stalled = true;
+                if (++k > A.spin_limit) stalled = true;
                 else __nanosleep(64);
             }
             __syncwarp();

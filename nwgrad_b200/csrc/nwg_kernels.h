@@ -13,6 +13,11 @@ struct Geo { int G, R; bool band = false; int mw = 0; };   // mw > 1: that many 
 // am: 0 Global, 1 Local, 2 semi-global ends (full DP, one warp or lane per pair)
 HardFn hard_fn_f32(bool aff, int am, bool tr, Geo g);
 HardFn hard_fn_f64(bool aff, int am, bool tr, Geo g);
-SoftFn soft_fn_f32(bool aff, int am, bool tr, Geo g);
-SoftFn soft_fn_f64(bool aff, int am, bool tr, Geo g);
+// soft: one table per end mode (0 Global, 1 Local, 2 semi-global ends)
+SoftFn soft_fn_f32_am0(bool aff, bool tr, Geo g);
+SoftFn soft_fn_f32_am1(bool aff, bool tr, Geo g);
+SoftFn soft_fn_f32_am2(bool aff, bool tr, Geo g);
+SoftFn soft_fn_f64_am0(bool aff, bool tr, Geo g);
+SoftFn soft_fn_f64_am1(bool aff, bool tr, Geo g);
+SoftFn soft_fn_f64_am2(bool aff, bool tr, Geo g);
 }  // namespace nwg

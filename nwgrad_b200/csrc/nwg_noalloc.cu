@@ -11,11 +11,13 @@
 // linear or affine.  Pairs longer than one stripe (128 rows of A) hand each stripe's bottom
 // row to the next through a scratch row per warp; those rows are carved out of one
 // file-scope device array of kScratchBytes (24 MiB), which every GPU that loads the library
-// holds until the process exits.  Limit: sequence B of at most kMaxColumns (2047) residues;
-// A is unbounded.  The scores are bit-identical to nwg_run's (same expressions, same order).
+// holds until the process exits.  Limits: sequence B of at most kMaxColumns (2047) residues,
+// A of at most kMaxRows.  The scores are bit-identical to nwg_run's (same expressions, same
+// order).  The substitution matrix and gap costs travel in the kernel's argument block (by
+// value), so a call copies nothing from host memory.
 //
-// Calls share the scratch array and the parameter block: calls whose kernels overlap on the
-// GPU (other streams, other host threads) race and give wrong scores; serialise them.
+// Calls share the scratch array: calls whose kernels overlap on the GPU (other streams, other
+// host threads) race and give wrong scores; serialise them.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -35,12 +37,18 @@ constexpr int kMaxColumns = 2047;                             // columns of B a 
 constexpr size_t kRowFloats = 3 * (size_t(kMaxColumns) + 1);  // M, X, Y per column 0..n
 constexpr size_t kScratchBytes = size_t(kSlots) * kRowFloats * sizeof(float);   // 24 MiB
 constexpr int kMaxAlpha = 32;
+constexpr int64_t kMaxRows = (int64_t(1) << 31) - 256;        // A: rows stay in int with the stripe padding
 constexpr int R = 4;     // rows per lane
 constexpr int G = 32;    // lanes per pair
 
 static __device__ __align__(256) float g_noalloc_scratch[kSlots * kRowFloats];
-// parameters of the current call: N*N matrix then the four gap costs, float
-static __device__ __align__(16) float g_noalloc_params[kMaxAlpha * kMaxAlpha + 4];
+
+// The call's parameters, passed by value in the launch's argument block (4112 bytes; kernels
+// take up to 32 KB of arguments on sm_70 and later with CUDA 12.1+): the N*N matrix, then the
+// four gap costs (open_a, extend_a, open_b, extend_b), float.
+struct NoallocParams {
+    float v[kMaxAlpha * kMaxAlpha + 4];
+};
 
 thread_local std::string g_err_na;
 std::mutex g_mu;
@@ -50,26 +58,30 @@ template <bool AFF, bool LOC>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32)
 score_fill_noalloc_kernel(const uint8_t* __restrict__ ca, const int64_t* __restrict__ oa,
                           const uint8_t* __restrict__ cb, const int64_t* __restrict__ ob,
-                          int64_t n_pairs, int N, float* scratch, double* scores) {
+                          int64_t n_pairs, int N, float* scratch, double* scores, const NoallocParams P) {
     using T = float;
     constexpr int GR = G * R;
     __shared__ T smat[kMaxAlpha * kMaxAlpha];
-    for (int k = threadIdx.x; k < N * N; k += blockDim.x) smat[k] = g_noalloc_params[k];
+    for (int k = threadIdx.x; k < N * N; k += blockDim.x) smat[k] = P.v[k];
     __syncthreads();
-    const T go_a = g_noalloc_params[N * N + 0], ge_a = g_noalloc_params[N * N + 1];
-    const T go_b = g_noalloc_params[N * N + 2], ge_b = g_noalloc_params[N * N + 3];
+    const T go_a = P.v[N * N + 0], ge_a = P.v[N * N + 1];
+    const T go_b = P.v[N * N + 2], ge_b = P.v[N * N + 3];
     const int lane = threadIdx.x & 31;
     const int64_t slot = int64_t(blockIdx.x) * kWarpsPerBlock + threadIdx.x / 32;
     T* bnd = scratch + slot * kRowFloats;
     for (int64_t p = slot; p < n_pairs; p += int64_t(gridDim.x) * kWarpsPerBlock) {
         const int64_t ao = oa[p], bo = ob[p];
-        const int m = int(oa[p + 1] - ao), n = int(ob[p + 1] - bo);
+        const int64_t m64 = oa[p + 1] - ao, n64 = ob[p + 1] - bo;
+        // a pair over the limits (the caller understated max_len_b, or A is over kMaxRows)
+        // is not computed: its score is NaN
+        const bool over = n64 > kMaxColumns || m64 > kMaxRows || m64 < 0 || n64 < 0;
+        const int m = over ? 0 : int(m64), n = over ? 0 : int(n64);
         const uint8_t* ap = ca + ao;
         const uint8_t* bp = cb + bo;
-        if (m == 0 || n == 0 || n > kMaxColumns) {
+        if (m == 0 || n == 0) {
             if (lane == 0) {
                 double sc = 0.0;
-                if (n > kMaxColumns) sc = __longlong_as_double(0x7ff8000000000000ll);   // NaN: over the limit
+                if (over) sc = __longlong_as_double(0x7ff8000000000000ll);   // NaN: over the limits
                 else if (!LOC && m == 0 && n > 0)
                     sc = AFF ? -nwg::add_rn(go_a, nwg::mul_rn(T(n), ge_a)) : nwg::mul_rn(-T(n), ge_a);
                 else if (!LOC && n == 0 && m > 0)
@@ -214,21 +226,18 @@ int nwg_scores_noalloc(const uint8_t* codes_a, const int64_t* off_a, const uint8
         }
         scratch = g_scratch_ptr[dev];
     }
-    float host_params[kMaxAlpha * kMaxAlpha + 4];
-    for (int k = 0; k < nalpha * nalpha; ++k) host_params[k] = static_cast<float>(mat[k]);
-    for (int k = 0; k < 4; ++k) host_params[nalpha * nalpha + k] = static_cast<float>(gaps[k]);
+    NoallocParams P{};
+    for (int k = 0; k < nalpha * nalpha; ++k) P.v[k] = static_cast<float>(mat[k]);
+    for (int k = 0; k < 4; ++k) P.v[nalpha * nalpha + k] = static_cast<float>(gaps[k]);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    e = cudaMemcpyToSymbolAsync(g_noalloc_params, host_params, sizeof(float) * size_t(nalpha * nalpha + 4), 0,
-                                cudaMemcpyHostToDevice, st);
-    if (e != cudaSuccess) return fail(NWG_ECUDA, std::string("nwg_scores_noalloc: ") + cudaGetErrorString(e));
     if (n_pairs == 0) return NWG_OK;
     const dim3 grid(kBlocks), block(kWarpsPerBlock * 32);
     if (gap_model == 1) {
-        if (mode == 1) score_fill_noalloc_kernel<true, true><<<grid, block, 0, st>>>(codes_a, off_a, codes_b, off_b, n_pairs, nalpha, scratch, scores);
-        else score_fill_noalloc_kernel<true, false><<<grid, block, 0, st>>>(codes_a, off_a, codes_b, off_b, n_pairs, nalpha, scratch, scores);
+        if (mode == 1) score_fill_noalloc_kernel<true, true><<<grid, block, 0, st>>>(codes_a, off_a, codes_b, off_b, n_pairs, nalpha, scratch, scores, P);
+        else score_fill_noalloc_kernel<true, false><<<grid, block, 0, st>>>(codes_a, off_a, codes_b, off_b, n_pairs, nalpha, scratch, scores, P);
     } else {
-        if (mode == 1) score_fill_noalloc_kernel<false, true><<<grid, block, 0, st>>>(codes_a, off_a, codes_b, off_b, n_pairs, nalpha, scratch, scores);
-        else score_fill_noalloc_kernel<false, false><<<grid, block, 0, st>>>(codes_a, off_a, codes_b, off_b, n_pairs, nalpha, scratch, scores);
+        if (mode == 1) score_fill_noalloc_kernel<false, true><<<grid, block, 0, st>>>(codes_a, off_a, codes_b, off_b, n_pairs, nalpha, scratch, scores, P);
+        else score_fill_noalloc_kernel<false, false><<<grid, block, 0, st>>>(codes_a, off_a, codes_b, off_b, n_pairs, nalpha, scratch, scores, P);
     }
     e = cudaGetLastError();
     if (e != cudaSuccess) return fail(NWG_ECUDA, std::string("nwg_scores_noalloc: launch: ") + cudaGetErrorString(e));

@@ -45,7 +45,8 @@ struct SoftArgs {
     const int32_t* order; int64_t n_items;
     const void* w;       // weights, (K*N + 1) rows x (N + 1) columns in T; row K*N and column N
                          // are 0 but for w[K*N][N] = 1, which carries the Global corner seed
-    const void* gw;      // per set: o_a, e_a, o_b, e_b in T
+    const void* gw;      // per set: o_a, e_a, o_b, e_b in T; then the float32 lost-mass charge per
+                         // unit of F^ + B^ (16 + 16 wmax), so a parameter step changes no argument
     int N, K;
     void* scratch; int64_t scratch_stride;   // bytes per group slot
     int64_t fwd_bytes;                       // bytes of the forward table within a slot
@@ -66,13 +67,41 @@ struct SoftArgs {
                                              // cells ends); 0: Global's borders and end (m, n)
     double temperature;
     double* score; double* grad; int64_t gstride;
-    int32_t* status;                         // per pair: 0 ok, 1 refused (out of range)
+    int32_t* status;                         // per pair: 0 ok, else kSoft* bits (why it was refused)
+    int spin_limit;                          // several warps per pair: polls before a wait gives up
 };
 
-// A value handed to a lane whose exponent is more than 2^kLift below the sender's moves the
-// receiver's own state down instead of being scaled up: incoming values then grow by at most
-// 2^kLift, which bounds the renormalisation period the host picks (nwg_capi.cu).
+// Per-pair status bits of a soft pass: a refused pair's score and counts are not written and
+// the host reruns it (float32 -> double).
+constexpr int32_t kSoftRange = 1;    // a forward or backward value left T's range
+constexpr int32_t kSoftZ = 2;        // Z is zero or out of range
+constexpr int32_t kSoftScale = 4;    // a count's scale factor 2^(E_F + E_B - E_Z) / Z overflowed T
+constexpr int32_t kSoftCounts = 8;   // a count left T's range
+constexpr int32_t kSoftLoss = 16;    // float32: mass lost to underflow could move a posterior by > 2^-24
+constexpr int32_t kSoftWeights = 32; // (host) a weight overflows T
+constexpr int32_t kSoftStall = 64;   // several warps per pair: a wait ran out (the call fails)
+
+// A lane receiving values whose largest lies more than 2^kLift above its own scale moves its
+// own state down instead: incoming values then land below 2^(kLift + 1), which bounds the
+// renormalisation period the host picks (nwg_capi.cu).
 constexpr int kLift = 32;
+
+// The exponent of a lane whose values are all zero: it carries no scale, so a neighbour
+// receiving its zeros keeps its own exponent, and the lane itself takes the scale of the
+// first non-zero values it receives (a zero lane with a stale exponent once pulled the
+// neighbouring lane's state down to zero, or flushed the values it received).
+constexpr int kEmpty = -(1 << 28);
+
+// Float32 lost-mass bound.  With subnormals kept (no FTZ), a rounding whose result falls
+// below FLT_MIN errs by at most 2^-150 in the lane's units; an error in a value that a weight
+// then multiplies grows by that weight (at most wmax, the largest of the exp'd scores and gap
+// weights), and mass lost at a cell moves a posterior (and Z) by at most that mass times
+// B(c) / Z.  So, with fac = 2^(E_F + E_B - E_Z) / Z, the backward pass charges per lane and
+// step fac * (loss_w * (sum F^ + sum B^) + 16 R) -- loss_w = 16 + 16 wmax roundings per state
+// and cell, transfers and rescales included, 16 per row for the count products -- and where
+// fac itself underflows the products it drops (each at most F^ B^ 2^(E_F + E_B - E_Z)), all in
+// units of 2^-150.  A pair whose charge exceeds kLossMax (damage 2^-24) is refused.
+constexpr float kLossMax = 0x1p126f;
 
 // Double accumulator with its own binary exponent: value = m * 2^e.
 struct XAcc {
@@ -189,8 +218,9 @@ __host__ __device__ inline size_t soft_smem_bytes(int K, int N, int G, int R, in
 
 // Several warps per pair (long pairs): warp w fills stripes w, w + NW, ... and waits, every 32
 // steps, until the warp filling the stripe above (below, in the backward pass) has published
-// enough progress.  The wait is bounded: past kSpinLimit polls the pair is marked failed
-// (status 3) and every warp finishes the pass without waiting further.
+// enough progress.  The wait is bounded: past SoftArgs::spin_limit polls (kSpinLimit unless
+// the store sets another) the pair is marked failed (kSoftStall) and every warp finishes the
+// pass without waiting further.
 constexpr int kSpinLimit = 1 << 22;
 
 // The backward pass reads the forward table one lane-step row (G lanes x R rows x 3 values)
@@ -212,6 +242,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
     static_assert(!BAND || (G == 32 && !MW), "banded: 32 lanes, one warp per pair");
     static_assert(!SG || !LOC, "semi-global ends: Global kernels");
     constexpr int GR = G * R;
+    constexpr bool kCount = sizeof(T) == 4;  // float32 charges its lost mass (double's is ~2^-900)
     constexpr int NV = AFF ? 3 : 1;          // values per cell
     constexpr int CV = NV * R;               // values per lane column
     constexpr int BW = AFF ? 4 : 2;          // boundary-row values per column: M (X, Y), exponent
@@ -273,7 +304,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
         if constexpr (MW) {
             int k = 0;
             while (!stalled && prog[pw] < target) {
-                if (++k > kSpinLimit) stalled = true;
+                if (++k > A.spin_limit) stalled = true;
                 else __nanosleep(64);
             }
             __syncwarp();
@@ -289,6 +320,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
     };
     // untracked: the one set's gap weights
     const T oa0 = sgw[0], ea0 = sgw[1], ob0 = sgw[2], eb0 = sgw[3];
+    const T loss_w = static_cast<const T*>(A.gw)[4 * K];
 
     for (int64_t it = slot; it < A.n_items; it += MW ? int64_t(gridDim.x) : int64_t(gridDim.x) * gpb) {
         const int p = A.order[it];
@@ -330,7 +362,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
         }
         const int S = n + G;                    // steps: columns 0..n plus the skew
         const int SP = S + 1;                   // MW: progress key per stripe
-        bool bad = false;
+        int why = 0;                            // kSoft* bits: why this pair is refused
         // semi-global ends (aligner.hpp:6362-6430): free starts on row 0 / column 0, Z over the
         // end cells (row m or (m, n), then column n of rows 0..m-1), the backward seeded with 1
         // at each; gap moves into a free start's border cells are not moves (6309-6319)
@@ -379,8 +411,13 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                 }
                 cM[r] = T(0); cX[r] = T(0); cY[r] = T(0);
             }
-            int E = 0;
-            T lone = T(1);                        // 2^-E: a free start's weight in lane units
+            // a lane holding a start cell begins at exponent 0 (its start weight is 1); the
+            // others begin empty and take the scale of the first values they receive.
+            // Lanes that add a start weight at every step (Local; row 0 a free start) keep
+            // their exponent when their values vanish (band masks), so that weight stays finite.
+            const bool keep_e = LOC || (sg_r0 && s == 0 && lane == 0);
+            int E = (LOC || sg_c0 || (s == 0 && lane == 0)) ? 0 : kEmpty;
+            T lone = pow2s<T>(-E);                // 2^-E: a free start's weight in lane units
             T zpart = T(0);                       // Local: the cells' sum since the last renorm
             T dgM = T(0), dgX = T(0), dgY = T(0); // row above, column j-1
             T upM = T(0), upX = T(0), upY = T(0); // row above, column j
@@ -410,15 +447,34 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
             auto take_up = [&](const T iM, const T iX, const T iY, const int iE) {
                 int d = iE - E;
                 if (d > kLift) {   // keep the incoming values in range: move own state down
-                    const T f = pow2i<T>(kLift - d);
+                    const T mi = AFF ? tmax(iM, tmax(iX, iY)) : iM;
+                    if (!(mi > T(0))) {   // zeros: nothing to align to
+                        upM = T(0); upX = T(0); upY = T(0);
+                        return;
+                    }
+                    // the incoming largest value lands at 2^kLift (an empty lane: at 1), by
+                    // its own magnitude, not its sender's exponent -- a sender between its
+                    // rescales can hold values far above 1, and lifts down a chain of empty
+                    // lanes would compound
+                    const int de = d + ilog2(mi);
+                    const int tgt = E == kEmpty ? 0 : kLift;
+                    if (de > tgt) {
+                        const int sh = tgt - de;
 #pragma unroll
-                    for (int r = 0; r < R; ++r) { cM[r] *= f; cX[r] *= f; cY[r] *= f; }
-                    dgM *= f; dgX *= f; dgY *= f; zpart *= f;
-                    E = iE - kLift; lone = pow2i<T>(-E); d = kLift;
+                        for (int r = 0; r < R; ++r) { cM[r] = scale_down(cM[r], sh); cX[r] = scale_down(cX[r], sh); cY[r] = scale_down(cY[r], sh); }
+                        dgM = scale_down(dgM, sh); dgX = scale_down(dgX, sh); dgY = scale_down(dgY, sh);
+                        zpart = scale_down(zpart, sh);
+                        E -= sh; lone = pow2s<T>(-E); d += sh;
+                    }
                 }
-                const T f = pow2i<T>(d);
-                upM = iM * f;
-                if constexpr (AFF) { upX = iX * f; upY = iY * f; }
+                if (d >= (sizeof(T) == 4 ? -126 : -1022)) {
+                    const T f = pow2i<T>(d);
+                    upM = iM * f;
+                    if constexpr (AFF) { upX = iX * f; upY = iY * f; }
+                } else {
+                    upM = scale_down(iM, d);
+                    if constexpr (AFF) { upX = scale_down(iX, d); upY = scale_down(iY, d); }
+                }
             };
             if (s > 0) {
                 if constexpr (G == 1) {
@@ -505,7 +561,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                         T mx = T(0);
 #pragma unroll
                         for (int r = 0; r < R; ++r) mx = tmax(mx, tmax(cM[r], tmax(cX[r], cY[r])));
-                        if (!is_finite(mx)) bad = true;
+                        if (!is_finite(mx)) why |= kSoftRange;
                         else if (mx > T(0)) {
                             int e = ilog2(mx);
                             if (e < -120) e = -120;
@@ -516,8 +572,13 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
 #pragma unroll
                                 for (int r = 0; r < R; ++r) { cM[r] *= f; cX[r] *= f; cY[r] *= f; }
                                 dgM *= f; dgX *= f; dgY *= f;
-                                E += e; lone = pow2i<T>(-E);
+                                E += e; lone = pow2s<T>(-E);
                             }
+                        } else if (!keep_e && !(dgM > T(0) || dgX > T(0) || dgY > T(0))) {
+                            // nothing left to scale: the next values set the exponent
+                            if ((LOC || zsg) && pass1) zacc.add(static_cast<double>(zpart), E);
+                            zpart = T(0);
+                            E = kEmpty;
                         }
                     }
                     // store the column for the backward pass
@@ -572,7 +633,10 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                     const bool top = lane == 0;
                     T v[BW];
                     vload<T, BW>(v, str + (cn & (G - 1)) * 4);
-                    if (!top || (s > 0 && cn <= n))
+                    // only for a column this lane still computes: a finished lane keeps its
+                    // state (row m's values are Z), an idle one its empty exponent
+                    const int jn1 = t + 1 - lane;
+                    if (jn1 >= 0 && jn1 <= n && (!top || s > 0))
                         take_up(top ? v[0] : sM, top ? (AFF ? v[1] : T(0)) : sX, top ? (AFF ? v[2] : T(0)) : sY,
                                 top ? bits_exp(v[BW - 1]) : sE);
                 } else {
@@ -618,16 +682,16 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                 ze = __shfl_sync(gmask, ze, src, G);
             }
         }
-        if constexpr (G > 1) bad = __any_sync(gmask, bad);
+        if constexpr (G > 1) why = __reduce_or_sync(gmask, why);
         if constexpr (MW) {
             // every warp's part of Z: Global, the warp holding row m; Local, the sum in warp order
             stalled = __any_sync(gmask, stalled);
             if (lane == 0) {
                 cpart[8 * gib + 0] = zm; cpart[8 * gib + 1] = double(ze);
-                cpart[8 * gib + 2] = bad ? 1.0 : 0.0; cpart[8 * gib + 3] = stalled ? 1.0 : 0.0;
+                cpart[8 * gib + 2] = double(why); cpart[8 * gib + 3] = stalled ? 1.0 : 0.0;
             }
             __syncthreads();
-            bool anybad = false, anystall = false;
+            bool anystall = false;
             if (LOC || zsg) {
                 XAcc za; za.init();
                 for (int w = 0; w < NWp; ++w) za.add(cpart[8 * w], int(cpart[8 * w + 1]));
@@ -636,18 +700,19 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                 const int ow = (nstripes - 1) % NWp;
                 zm = cpart[8 * ow]; ze = int(cpart[8 * ow + 1]);
             }
-            for (int w = 0; w < NWp; ++w) { anybad |= cpart[8 * w + 2] != 0.0; anystall |= cpart[8 * w + 3] != 0.0; }
-            bad = anybad; stalled = anystall;
+            for (int w = 0; w < NWp; ++w) { why |= int(cpart[8 * w + 2]); anystall |= cpart[8 * w + 3] != 0.0; }
+            stalled = anystall;
             if (lane == 0) prog[gib] = -1;
             __syncthreads();
             if (stalled) {
-                if (threadIdx.x == 0) { A.status[p] = 3; A.score[p] = 0.0; }
+                if (threadIdx.x == 0) { A.status[p] = kSoftStall; A.score[p] = 0.0; }
                 stalled = false;
                 continue;
             }
         }
-        if (!(zm > 0.0) || !(zm < 1e300) || bad) {
-            if (lane == 0 && (!MW || gib == 0)) { A.status[p] = 1; A.score[p] = 0.0; }
+        if (!(zm > 0.0) || !(zm < 1e300)) why |= kSoftZ;
+        if (why) {
+            if (lane == 0 && (!MW || gib == 0)) { A.status[p] = why; A.score[p] = 0.0; }
             continue;
         }
         const int EZ = ze + ilog2(zm);
@@ -657,6 +722,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
 
         // ── backward, fused with the expected counts ─────────────────────────
         double ga_o = 0, ga_x = 0, gb_o = 0, gb_x = 0;   // untracked: opens and extend-only moves
+        T lacc = T(0);                                   // float32: this lane's lost-mass charge
         bool cnt_nf = false;                             // one lane per pair: a count not finite
         if constexpr (G == 1) {
             double* g1 = A.grad + A.gstride * p;
@@ -696,8 +762,12 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                 }
                 bM[r] = T(0); bX[r] = T(0); bY[r] = T(0);
             }
-            int EB = 0;
-            T lone = T(1);
+            // a lane holding an end cell at its first column (row m's lane; Local every lane;
+            // column n ends every lane with rows) begins at exponent 0, the others empty
+            const bool holds_m = i0 <= m && m < i0 + R;
+            const bool keep_b = LOC || (sg_er && holds_m);
+            int EB = (LOC || holds_m || (sg_ec && i0 <= m)) ? 0 : kEmpty;
+            T lone = pow2s<T>(-EB);
             T sgb_o = T(0), sga_o = T(0), sgb_x = T(0), sga_x = T(0);   // untracked: this stripe's gap sums
             T dgM = T(0);                             // row below, column j+1 (BM only)
             // Global affine: the seed B = 1 at (m, n) enters every state through the diagonal
@@ -745,16 +815,30 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
             auto take_dn = [&](const T iM, const T iX, const T iY, const int iE) {
                 int d = iE - EB;
                 if (d > kLift) {
-                    const T f = pow2i<T>(kLift - d);
+                    const T mi = AFF ? tmax(iM, tmax(iX, iY)) : iM;
+                    if (!(mi > T(0))) {   // zeros: nothing to align to
+                        dnM = T(0); dnX = T(0); dnY = T(0);
+                        return;
+                    }
+                    const int de = d + ilog2(mi);   // as in the forward pass
+                    const int tgt = EB == kEmpty ? 0 : kLift;
+                    if (de > tgt) {
+                        const int sh = tgt - de;
 #pragma unroll
-                    for (int r = 0; r < R; ++r) { bM[r] *= f; bX[r] *= f; bY[r] *= f; }
-                    dgM *= f;
-                    EB = iE - kLift; lone = pow2i<T>(-EB); d = kLift;
+                        for (int r = 0; r < R; ++r) { bM[r] = scale_down(bM[r], sh); bX[r] = scale_down(bX[r], sh); bY[r] = scale_down(bY[r], sh); }
+                        dgM = scale_down(dgM, sh);
+                        EB -= sh; lone = pow2s<T>(-EB); d += sh;
+                    }
                 }
-                const T f = pow2i<T>(d);
-                dnM = iM * f;
-                if constexpr (AFF) { dnX = iX * f; dnY = iY * f; }
-                else { dnX = dnM; dnY = dnM; }
+                if (d >= (sizeof(T) == 4 ? -126 : -1022)) {
+                    const T f = pow2i<T>(d);
+                    dnM = iM * f;
+                    if constexpr (AFF) { dnX = iX * f; dnY = iY * f; }
+                } else {
+                    dnM = scale_down(iM, d);
+                    if constexpr (AFF) { dnX = scale_down(iX, d); dnY = scale_down(iY, d); }
+                }
+                if constexpr (!AFF) { dnX = dnM; dnY = dnM; }
             };
             if (s < nstripes - 1) {
                 if constexpr (G == 1) {
@@ -812,9 +896,11 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                     }
                     // scale of this step's products: 2^(E_F + E_B - E_Z) / zhat (an exact power of
                     // two times 1 / zhat rounded to T)
-                    const double facd = (TR && lane_rows) ? pow2i<double>(EF + EB - EZ) * invz : 0.0;
-                    const T fac = TR ? static_cast<T>(facd) : lane_rows ? pow2i<T>(EF + EB - EZ) * invzT : T(0);
-                    if (!is_finite(fac)) bad = true;
+                    const int efac = EF + EB - EZ;
+                    const double facd = (TR && lane_rows) ? pow2i<double>(efac) * invz : 0.0;
+                    const T fac = TR ? static_cast<T>(facd) : lane_rows ? pow2i<T>(efac) * invzT : T(0);
+                    if (!is_finite(fac)) why |= kSoftScale;
+                    T SF = T(0), SB = T(0);           // float32: this step's F^ and B^ sums (lost mass)
                     T dM = dgM;                       // row below, column j+1
                     T xM = dnM, xX = dnX, xY = dnY;   // row below, column j
                     T so_b = T(0), sx_b = T(0), so_a = T(0), sx_a = T(0);
@@ -846,7 +932,9 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                                 if (e) { nM += lone; nX += lone; nY += lone; }
                             }
                             const T fmy = fm + fy, fmx = fm + fx;
-                            mc[r] = (fmy + fx) * D;
+                            const T fsum = fmy + fx;
+                            mc[r] = fsum * D;
+                            if constexpr (kCount) SF = fmaf_t(vmask[r], fsum, SF);
                             if constexpr (TR) {
                                 const double ob_c = static_cast<double>(fmy * o_b * dX) * facd;
                                 const double eb_c = static_cast<double>(fx * e_b * dX) * facd;
@@ -872,6 +960,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                             }
                             nX = nM; nY = nM;
                             mc[r] = fm * D;
+                            if constexpr (kCount) SF = fmaf_t(vmask[r], fm, SF);
                             if constexpr (TR) {
                                 tg[4 * tsd[r] + 3] += static_cast<double>(fm * e_b * dX) * facd;
                                 tg[4 * gsr[r] + 1] += static_cast<double>(fm * e_a * rY) * facd;
@@ -883,6 +972,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                         if constexpr (BAND) {
                             if (j < bblo0[r] || j > bbhi[r]) { nM = T(0); nX = T(0); nY = T(0); }
                         }
+                        if constexpr (kCount) SB += AFF ? (nM + nX) + nY : nM;
                         dM = bM[r];
                         bM[r] = nM; bX[r] = nX; bY[r] = nY;
                         xM = nM; xX = nX; xY = nY;
@@ -904,12 +994,21 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                         sgb_x = fmaf_t(sx_b, fac, sgb_x);
                         sga_x = fmaf_t(sx_a, fac, sga_x);
                     }
+                    if constexpr (kCount) {
+                        // the lost-mass charge of this lane-step (scale factor in range), or the
+                        // products an underflowed scale factor dropped (each <= F^ B^ 2^efac),
+                        // in units of 2^-150
+                        if (lane_rows) {
+                            if (efac >= -126) lacc = fmaf_t(fac, fmaf_t(SF + SB, loss_w, T(16 * R)), lacc);
+                            else lacc = fmaf_t((SF + T(1)) * (SB + T(1)), T(5 * R) * pow2s<T>(efac + 150), lacc);
+                        }
+                    }
                     dgM = dnM;
                     if ((t & rmask) == 0 || j == 0) {
                         T mx = T(0);
 #pragma unroll
                         for (int r = 0; r < R; ++r) mx = tmax(mx, tmax(bM[r], tmax(bX[r], bY[r])));
-                        if (!is_finite(mx)) bad = true;
+                        if (!is_finite(mx)) why |= kSoftRange;
                         else if (mx > T(0)) {
                             int e = ilog2(mx);
                             if (e < -120) e = -120;
@@ -918,8 +1017,10 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
 #pragma unroll
                                 for (int r = 0; r < R; ++r) { bM[r] *= fsc; bX[r] *= fsc; bY[r] *= fsc; }
                                 dgM *= fsc;
-                                EB += e; lone = pow2i<T>(-EB);
+                                EB += e; lone = pow2s<T>(-EB);
                             }
+                        } else if (!keep_b && !(dgM > T(0))) {
+                            EB = kEmpty;   // nothing left to scale: the next values set the exponent
                         }
                     }
                 }
@@ -963,7 +1064,8 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                     const bool bot = lane == G - 1;
                     T v[BW];
                     vload<T, BW>(v, str + (dn & (G - 1)) * 4);
-                    if (!bot || (s < nstripes - 1 && dn <= n))
+                    const int jn1 = n - (t + 1) + (G - 1 - lane);   // this lane's next column
+                    if (jn1 >= 0 && jn1 <= n && (!bot || s < nstripes - 1))
                         take_dn(bot ? v[0] : sM, bot ? (AFF ? v[1] : T(0)) : sX, bot ? (AFF ? v[2] : T(0)) : sY,
                                 bot ? bits_exp(v[BW - 1]) : sE);
                 } else {
@@ -1013,7 +1115,13 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                 __syncwarp(gmask);
             }
         }
-        if constexpr (G > 1) bad = __any_sync(gmask, bad);
+        if constexpr (kCount) {
+            // the group's lost-mass charge (every lane's, in any order: a bound, not a result)
+            if constexpr (G > 1) {
+#pragma unroll
+                for (int off = G / 2; off > 0; off >>= 1) lacc += __shfl_xor_sync(gmask, lacc, off, G);
+            }
+        }
         if constexpr (!TR && G > 1) {
 #pragma unroll
             for (int off = G / 2; off > 0; off >>= 1) {
@@ -1027,14 +1135,14 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
         const int64_t NN = int64_t(K) * N * N;
         // counts that left the range of T (a scale factor that overflowed where a product with
         // it was zero) refuse the pair like any other overflow: the host reruns it in double
-        if (!bad) {
+        {
             bool nf = false;
             if constexpr (G > 1) { for (int k = lane; k < K * N * N; k += G) nf |= !is_finite(hist[k]); }
             else nf |= cnt_nf;
             if constexpr (!TR) nf |= !(is_finite(ga_o) && is_finite(ga_x) && is_finite(gb_o) && is_finite(gb_x));
             else { for (int k = 0; k < 4 * K; ++k) nf |= !is_finite(tg[k]); }
-            if constexpr (G > 1) nf = __any_sync(gmask, nf);
-            bad = nf;
+            if (nf) why |= kSoftCounts;
+            if constexpr (G > 1) why = __reduce_or_sync(gmask, why);
         }
         if constexpr (MW) {
             // the pair's totals: every warp's histogram and gap sums, added in warp order
@@ -1042,18 +1150,21 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
             if (lane == 0) {
                 cpart[8 * gib + 0] = ga_o; cpart[8 * gib + 1] = ga_x;
                 cpart[8 * gib + 2] = gb_o; cpart[8 * gib + 3] = gb_x;
-                cpart[8 * gib + 4] = bad ? 1.0 : 0.0; cpart[8 * gib + 5] = stalled ? 1.0 : 0.0;
+                cpart[8 * gib + 4] = double(why); cpart[8 * gib + 5] = stalled ? 1.0 : 0.0;
+                cpart[8 * gib + 6] = kCount ? static_cast<double>(lacc) : 0.0;
             }
             __syncthreads();
-            double to_a = 0, tx_a = 0, to_b = 0, tx_b = 0;
-            bool anybad = false, anystall = false;
+            double to_a = 0, tx_a = 0, to_b = 0, tx_b = 0, tl = 0;
+            bool anystall = false;
             for (int w = 0; w < NWp; ++w) {
                 to_a += cpart[8 * w + 0]; tx_a += cpart[8 * w + 1];
                 to_b += cpart[8 * w + 2]; tx_b += cpart[8 * w + 3];
-                anybad |= cpart[8 * w + 4] != 0.0; anystall |= cpart[8 * w + 5] != 0.0;
+                why |= int(cpart[8 * w + 4]); anystall |= cpart[8 * w + 5] != 0.0;
+                tl += cpart[8 * w + 6];
             }
-            if (anystall || anybad) {
-                if (threadIdx.x == 0) { A.status[p] = anystall ? 3 : 1; A.score[p] = 0.0; }
+            if (kCount && !(tl <= double(kLossMax))) why |= kSoftLoss;
+            if (anystall || why) {
+                if (threadIdx.x == 0) { A.status[p] = anystall ? kSoftStall : why; A.score[p] = 0.0; }
             } else {
                 for (int k = threadIdx.x; k < K * N * N; k += blockDim.x) {
                     double v = 0.0;
@@ -1073,8 +1184,8 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
             }
             stalled = false;
             __syncthreads();
-        } else if (bad) {
-            if (lane == 0) { A.status[p] = 1; A.score[p] = 0.0; }
+        } else if (why || (kCount && !(lacc <= kLossMax))) {
+            if (lane == 0) { A.status[p] = why | ((kCount && !(lacc <= kLossMax)) ? kSoftLoss : 0); A.score[p] = 0.0; }
         } else {
             if constexpr (G > 1)
                 for (int k = lane; k < K * N * N; k += G) g[k] = static_cast<double>(hist[k]);

@@ -1,4 +1,6 @@
-// Soft-path kernels for one precision (NWG_T: float or double), every compiled geometry.
+// Soft-path kernels for one precision (NWG_T: float or double) and one end mode (NWG_SOFT_AM:
+// 0 Global, 1 Local, 2 semi-global ends), every compiled geometry.  One translation unit per
+// (precision, mode) so the units compile in parallel.
 #include "nwg_kernels.h"
 
 namespace nwg {
@@ -21,18 +23,15 @@ SoftFn pick(Geo g) {
 }
 }  // namespace
 
-SoftFn NWG_SOFT_FN(bool aff, int am, bool tr, Geo g) {
+SoftFn NWG_SOFT_FN(bool aff, bool tr, Geo g) {
     using T = NWG_T;
-    const bool loc = am == 1;
-    if (am == 2) {
-        if (aff) return tr ? pick<T, true, false, true, true>(g) : pick<T, true, false, false, true>(g);
-        return tr ? pick<T, false, false, true, true>(g) : pick<T, false, false, false, true>(g);
-    }
-    if (aff) {
-        if (loc) return tr ? pick<T, true, true, true>(g) : pick<T, true, true, false>(g);
-        return tr ? pick<T, true, false, true>(g) : pick<T, true, false, false>(g);
-    }
-    if (loc) return tr ? pick<T, false, true, true>(g) : pick<T, false, true, false>(g);
-    return tr ? pick<T, false, false, true>(g) : pick<T, false, false, false>(g);
+#if NWG_SOFT_AM == 2
+    if (aff) return tr ? pick<T, true, false, true, true>(g) : pick<T, true, false, false, true>(g);
+    return tr ? pick<T, false, false, true, true>(g) : pick<T, false, false, false, true>(g);
+#else
+    constexpr bool loc = NWG_SOFT_AM == 1;
+    if (aff) return tr ? pick<T, true, loc, true>(g) : pick<T, true, loc, false>(g);
+    return tr ? pick<T, false, loc, true>(g) : pick<T, false, loc, false>(g);
+#endif
 }
 }  // namespace nwg

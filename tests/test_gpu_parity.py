@@ -385,27 +385,21 @@ def test_soft_banded(prec, gm, am, bw):
 
 
 @pytest.mark.parametrize("prec", [32, 64])
-@pytest.mark.parametrize("geo", [(8, 4), (32, 4)])
-def test_soft_long_gap_chains_rerun_one_lane(prec, geo):
-    """A short A against a long B under global ends, forced to several lanes per pair: those
-    lanes refuse the pair in float and double, which then reruns at one lane per pair in double
-    and matches the oracle."""
-    rng = np.random.default_rng(5100 + prec + geo[0] + geo[1])
-    alpha = "ACGTU"
-    mat = np.full((1, 5, 5), -4.0)
-    for x, y in ((0, 3), (1, 2), (2, 1), (3, 0), (4, 0), (2, 4)):
-        mat[0, x, y] = 5.0
-    gaps = np.array([[5.0, 2.0, 5.0, 2.0]])
-    sa = ["".join(rng.choice(list("ACGU"), size=22)) for _ in range(6)]
-    sb = ["".join(rng.choice(list("ACGT"), size=int(rng.integers(500, 900)))) for _ in range(6)]
+@pytest.mark.parametrize("gm", [0, 1])
+@pytest.mark.parametrize("am", [0, 1])
+def test_score_only_bit_exact(prec, gm, am):
+    """grad_mode="none" (the score-only fill: no codes, no walk) against the oracle's Viterbi
+    scores bit for bit: short pairs at a lane per pair, medium at a warp, and long pairs at
+    several warps per pair."""
+    rng = np.random.default_rng(1300 + prec + 10 * gm + 20 * am)
+    mat, gaps, sa, sb, tr, gt = _problem(rng, AA, 60, 0, 40, integer=False)
+    sa += ["", "ACD", "W" * 70] + rand_seqs(rng, 6, 200, 400, AA) + rand_seqs(rng, 2, 1600, 2200, AA)
+    sb += ["KLM", "", "W" * 3] + rand_seqs(rng, 6, 150, 420, AA) + rand_seqs(rng, 2, 1500, 2300, AA)
     cls = nw.SeqPairBatch if prec == 32 else nw.SeqPairBatchDouble
-    b = cls(sa, sb, _params(alpha, mat, gaps), grad_mode="soft")
-    b._tune = geo
-    b.score_and_grad()
-    enc = oracle.Encoded(encode(alpha, sa), encode(alpha, sb))
-    so, go = oracle.soft(1, 0, mat, gaps, enc)
-    np.testing.assert_allclose(b.scores(), so, rtol=SOFT_RTOL, atol=1e-5)
-    gmat, ggap = b.grads()
-    flat = np.concatenate([gmat.reshape(len(sa), -1), ggap.reshape(len(sa), -1)], axis=1)
-    scale = np.maximum(np.abs(go).max(axis=1, keepdims=True), 1.0)
-    assert (np.abs(flat - go) / scale).max() <= SOFT_RTOL
+    b = cls(sa, sb, _params(AA, mat, gaps), gap_model=("linear", "affine")[gm],
+            mode=("global", "local")[am], grad_mode="none")
+    tot = b.score_and_grad()
+    o = oracle.hard(prec, gm, am, mat, gaps, oracle.Encoded(encode(AA, sa), encode(AA, sb)))
+    s = b.scores()
+    assert np.array_equal(s, o["scores"]), np.nonzero(s != o["scores"])[0][:5]
+    assert tot == float(np.cumsum(o["scores"])[-1])

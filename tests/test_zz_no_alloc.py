@@ -1,14 +1,17 @@
 """nwg_scores_noalloc: the scores entry point that allocates no device memory, for callers
 whose host framework owns every device allocation and forbids cudaMalloc.  Checked through
-the C ABI against the store path's scores (nwg_run, score only), bit for bit as every hard
-result, on two calls in a row (the second reuses the reserved scratch the first left dirty).
-Collected last on purpose: it must also pass after every other test in the same process."""
+the C ABI against the store path's scores (nwg_run, score only) and the CPU oracle's Viterbi
+scores, bit for bit as every hard result, on two calls in a row (the second reuses the
+reserved scratch the first left dirty), and that the second call changes neither the device's
+free memory nor torch's allocated bytes.  Collected last on purpose: it must also pass after
+every other test in the same process."""
 import ctypes as C
 
 import numpy as np
 import pytest
 
-from conftest import AA, has_gpu, rand_matrix, rand_seqs
+import oracle
+from conftest import AA, encode, has_gpu, rand_matrix, rand_seqs
 
 pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not has_gpu(), reason="needs a CUDA GPU")]
 
@@ -49,6 +52,9 @@ def test_noalloc_scores_match_store_path(gap_model, mode):
     b = nw.SeqPairBatch(sa, sb, params, gap_model=gap_model, mode=mode, grad_mode="none")
     b.score_and_grad()
     ref = b.scores()
+    o = oracle.hard(32, int(gap_model == "affine"), int(mode == "local"), mat, gaps,
+                    oracle.Encoded(encode(AA, sa), encode(AA, sb)))
+    assert np.array_equal(ref, o["scores"])
     ca, oa = _encode(AA, sa)
     cb, ob = _encode(AA, sb)
     dev = torch.device("cuda", torch.cuda.current_device())
@@ -62,12 +68,16 @@ def test_noalloc_scores_match_store_path(gap_model, mode):
     for call in range(2):
         out.fill_(-1.0)
         torch.cuda.synchronize()
+        free0, alloc0 = torch.cuda.mem_get_info()[0], torch.cuda.memory_allocated()
         rc = L.nwg_scores_noalloc(t_ca.data_ptr(), t_oa.data_ptr(), t_cb.data_ptr(), t_ob.data_ptr(), len(sa),
                                   max_b, 20, m.ctypes.data_as(C.POINTER(C.c_double)),
                                   g.ctypes.data_as(C.POINTER(C.c_double)), int(gap_model == "affine"),
                                   int(mode == "local"), out.data_ptr(), None)
         assert rc == 0, L.nwg_noalloc_last_error()
         torch.cuda.synchronize()
+        if call == 1:   # after the first call's one-time set-up, a call allocates nothing
+            assert torch.cuda.mem_get_info()[0] == free0
+            assert torch.cuda.memory_allocated() == alloc0
         got = out.cpu().numpy()
         assert np.array_equal(got, ref), (call, np.nonzero(got != ref)[0][:5])
 
