@@ -237,6 +237,49 @@ def cpu_reference(mat, a, oa, bp, obp, bn, obn, sample_pairs, steps, warmup):
             "value": cells / float(np.min(per_step)) / 1e9}
 
 
+def parity_sample(batches, a, oa, mat, per_bin=250, seed=11):
+    """Checker of the timed workload's own results: a stratified sample of pairs of each batch
+    (per_bin pairs with A in each of 100-199, 200-299, 300-399, 400-500) recomputed by the CPU
+    oracle (double, log space, several host threads), against the per-pair scores and expected
+    counts the GPU left in the batches.  Returns the largest relative errors: scores against
+    max(|log Z|, 1), counts against each pair's largest count (the parity tests' convention)."""
+    import concurrent.futures as cf
+    import oracle
+    rng = np.random.default_rng(seed)
+    la = np.diff(oa)
+    gaps = np.array([[11.0, 1.0, 11.0, 1.0]])
+    err_s = err_g = 0.0
+    n_checked = refused = 0
+    for b, bcodes, ob in batches:
+        idx = []
+        for lo, hi in ((100, 200), (200, 300), (300, 400), (400, 501)):
+            cand = np.nonzero((la >= lo) & (la < hi))[0]
+            idx.extend(rng.choice(cand, size=min(per_bin, cand.size), replace=False).tolist())
+        idx = np.sort(np.asarray(idx, np.int64))
+        s_gpu = b.scores()[idx]
+        gm, gg = b.grads()
+        g_gpu = np.concatenate([gm[idx].reshape(idx.size, -1), gg[idx].reshape(idx.size, -1)], axis=1)
+        refused += int(np.count_nonzero(b.soft_status()[idx] & 0xff))
+        A = [a[oa[i]:oa[i + 1]].tolist() for i in idx]
+        B = [bcodes[ob[i]:ob[i + 1]].tolist() for i in idx]
+
+        def run(lo):
+            enc = oracle.Encoded(A[lo:lo + 25], B[lo:lo + 25])
+            return oracle.soft(1, 0, mat[None], gaps, enc)
+        with cf.ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as ex:
+            parts = list(ex.map(run, range(0, idx.size, 25)))
+        so = np.concatenate([p[0] for p in parts])
+        go = np.concatenate([p[1] for p in parts])
+        err_s = max(err_s, float(np.max(np.abs(s_gpu - so) / np.maximum(np.abs(so), 1.0))))
+        scale = np.maximum(np.abs(go).max(axis=1, keepdims=True), 1.0)
+        err_g = max(err_g, float(np.max(np.abs(g_gpu - go) / scale)))
+        n_checked += idx.size
+    return {"pairs": n_checked, "max_rel_err_scores": err_s, "max_rel_err_counts": err_g, "tol": 1e-4,
+            "ok": bool(err_s <= 1e-4 and err_g <= 1e-4), "float32_refused_to_double": refused,
+            "oracle": "CPU oracle, double log-space forward-backward",
+            "sample": f"{per_bin} pairs per A-length bin (100-199 .. 400-500) of each batch, seeded"}
+
+
 def _tune_mod():
     from nwgrad_b200 import tune
     return tune
@@ -567,7 +610,13 @@ def main():
                              "sum-product: no tensor-core contraction)",
                 "ops_per_cell": OPS_PER_CELL_SOFT, "kernel_ms_per_step": kernel_ms / args.steps}
     cpu = None
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # the CPU leg: the oracle checks the timed batches' own results on a stratified sample,
+        # then the reference's CPU path is timed on a sample of the same workload
+        pos.score_and_grad()          # the tuned geometries' results (the plain arm ran last)
+        neg.score_and_grad()
+        parity = parity_sample([(pos, bp, obp), (neg, bn, obn)], a, oa, mat)
         r = cpu_reference(mat, a, oa, bp, obp, bn, obn, args.cpu_sample, 2, 1)
         if r is not None:
             cpu = {"value": r["value"], "unit": "GCUPS", "cores": r["threads"], "kind": "reference",
@@ -582,7 +631,7 @@ def main():
             "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": total_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded)", "config": config, "e2e": e2e, "roofline": roofline,
-            "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
+            "cpu_baseline": cpu, "parity": parity, "clocks": clocks, "gpu_launches": launches,
             "plain_fill": plain, "serve": serve,
             "autotune": {str(k): _tune_mod().describe(v) for k, v in tune_table.items()},
             "step_ms": step_ms, "graph_captures_timed": getattr(clk, "captures", None)}))
