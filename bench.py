@@ -88,16 +88,17 @@ def _mutate_codes(rng, a, freqs, sub=0.30, indel=0.05):
     return np.concatenate(parts).astype(np.uint8)
 
 
-def c2_workload(n_pairs, seed=1):
-    """(mat, codes_a, off_a, codes_b_pos, off_b_pos, codes_b_neg, off_b_neg)."""
-    cache = os.path.join("/tmp", f"nwgrad_b200_c2_{n_pairs}_{seed}.npz")
+def c2_workload(n_pairs, seed=1, lmax=500):
+    """(mat, codes_a, off_a, codes_b_pos, off_b_pos, codes_b_neg, off_b_neg); lmax < 500 caps A's
+    length (profiling cases of the same distribution that still fill the device)."""
+    cache = os.path.join("/tmp", f"nwgrad_b200_c2_{n_pairs}_{seed}_{lmax}.npz")
     if os.path.exists(cache):
         z = np.load(cache)
         return tuple(z[k] for k in ("mat", "a", "oa", "bp", "obp", "bn", "obn"))
     rng = np.random.default_rng(seed)
     freqs = rng.dirichlet(np.full(20, 5.0))
     mat = c2_matrix(rng)
-    la = rng.integers(100, 501, size=n_pairs)
+    la = rng.integers(100, lmax + 1, size=n_pairs)
     oa = np.zeros(n_pairs + 1, np.int64)
     oa[1:] = np.cumsum(la)
     a = rng.choice(20, size=int(oa[-1]), p=freqs).astype(np.uint8)
@@ -393,6 +394,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--pairs", type=int, default=100000, help="pairs per batch (positives; as many decoys)")
     ap.add_argument("--cpu-sample", type=int, default=4000, help="pairs per batch in the CPU-baseline sample")
+    ap.add_argument("--lmax", type=int, default=500, help="longest A (profiling cases; the workload is 100-500)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-fill arm")
@@ -429,7 +431,7 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    mat, a, oa, bp, obp, bn, obn = c2_workload(args.pairs, seed=1)
+    mat, a, oa, bp, obp, bn, obn = c2_workload(args.pairs, seed=1, lmax=args.lmax)
     cells = cells_of(oa, obp) + cells_of(oa, obn)
     config = {"workload": "soft-gradient global affine batch, float32 DP: 100k homologous protein pairs "
                           "(L 100-500, 30% subs, indels 0.05) + 100k shuffled decoys, margin gradient",

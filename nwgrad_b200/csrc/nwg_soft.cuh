@@ -321,6 +321,9 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
     // untracked: the one set's gap weights
     const T oa0 = sgw[0], ea0 = sgw[1], ob0 = sgw[2], eb0 = sgw[3];
     const T loss_w = static_cast<const T*>(A.gw)[4 * K];
+    // the largest exact power of two one factor of a transfer may take (incoming values can
+    // lie more than that above a lane's scale only when they are at most 2^kLift in its units)
+    constexpr int kExpHi = sizeof(T) == 4 ? 126 : 1022;
 
     for (int64_t it = slot; it < A.n_items; it += MW ? int64_t(gridDim.x) : int64_t(gridDim.x) * gpb) {
         const int p = A.order[it];
@@ -465,6 +468,12 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                         dgM = scale_down(dgM, sh); dgX = scale_down(dgX, sh); dgY = scale_down(dgY, sh);
                         zpart = scale_down(zpart, sh);
                         E -= sh; lone = pow2s<T>(-E); d += sh;
+                    }
+                    if (d > kExpHi) {   // small values far above this lane's scale: 2^d in two factors
+                        const T f1 = pow2i<T>(d - kExpHi), f2 = pow2i<T>(kExpHi);
+                        upM = (iM * f1) * f2;
+                        if constexpr (AFF) { upX = (iX * f1) * f2; upY = (iY * f1) * f2; }
+                        return;
                     }
                 }
                 if (d >= (sizeof(T) == 4 ? -126 : -1022)) {
@@ -828,6 +837,13 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                         for (int r = 0; r < R; ++r) { bM[r] = scale_down(bM[r], sh); bX[r] = scale_down(bX[r], sh); bY[r] = scale_down(bY[r], sh); }
                         dgM = scale_down(dgM, sh);
                         EB -= sh; lone = pow2s<T>(-EB); d += sh;
+                    }
+                    if (d > kExpHi) {   // as in the forward pass
+                        const T f1 = pow2i<T>(d - kExpHi), f2 = pow2i<T>(kExpHi);
+                        dnM = (iM * f1) * f2;
+                        if constexpr (AFF) { dnX = (iX * f1) * f2; dnY = (iY * f1) * f2; }
+                        else { dnX = dnM; dnY = dnM; }
+                        return;
                     }
                 }
                 if (d >= (sizeof(T) == 4 ? -126 : -1022)) {
