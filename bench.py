@@ -546,19 +546,31 @@ def main():
     value = world * cells * args.steps / (total_ms / 1e3) / 1e9
     plain = None
     if not args.no_plain:
+        # plain and tuned interleaved, three runs of K steps each (the headline is the first
+        # tuned run above): the tuner's gain against run-to-run spread
         saved = pos._tune
-        pos._tune = neg._tune = (0, 0)
-        pos.use_plain_fill()
-        neg.use_plain_fill()
-        p_total, p_steps, p_kms, p_launch, _ = timed(False)
-        plain = {"value": world * cells * args.steps / (p_total / 1e3) / 1e9, "unit": "GCUPS",
-                 "ms_per_step": p_total / args.steps, "kernel_ms_per_step": p_kms / args.steps,
+        gc = lambda ms: world * cells * args.steps / (ms / 1e3) / 1e9   # noqa: E731
+        runs = {"plain": [], "tuned": [value]}
+        p_kms = 0.0
+        for rep in range(3):
+            pos._tune = neg._tune = (0, 0)
+            pos.use_plain_fill()
+            neg.use_plain_fill()
+            p_total, _, p_kms_r, _, _ = timed(False)
+            runs["plain"].append(gc(p_total))
+            p_kms += p_kms_r
+            pos._tune = neg._tune = saved
+            if not args.no_tune:
+                pos.autotune()
+                neg.autotune()
+            if rep < 2:
+                runs["tuned"].append(gc(timed(False)[0]))
+        med = {k: float(np.median(v)) for k, v in runs.items()}
+        plain = {"value": med["plain"], "unit": "GCUPS", "kernel_ms_per_step": p_kms / (3 * args.steps),
                  "geometry": "32 lanes x 4 rows for every pair, one launch per size bucket",
-                 "tuned_over_plain": (value / (world * cells * args.steps / (p_total / 1e3) / 1e9))}
-        pos._tune = neg._tune = saved
-        if not args.no_tune:
-            pos.autotune()
-            neg.autotune()
+                 "runs": runs, "median": med,
+                 "range": {k: [float(min(v)), float(max(v))] for k, v in runs.items()},
+                 "tuned_over_plain": med["tuned"] / med["plain"]}
 
     # end to end through the public API: host codes uploaded, aligned, gradient read back
     e2e = None

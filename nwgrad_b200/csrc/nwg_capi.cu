@@ -311,12 +311,11 @@ int long_warps(int rows, int GR) {
 }
 
 // Pairs are bucketed by geometry and by size class: the binary order of magnitude of the DP
-// (rows x columns), with everything up to 2^20 cells in one class.  Small pairs share a
-// launch (their scratch strides are small anyway); large pairs get a bucket per doubling, so
-// a bucket's scratch stride is sized close to its own pairs.
+// (rows x columns).  A bucket per doubling sizes its scratch stride close to its own pairs and
+// lets the autotuner pick a geometry per class.
 int size_class(int rows, int n) {
     const double cells = double(std::max(rows, 1)) * double(std::max(n, 1));
-    return std::max(20, int(std::ceil(std::log2(cells))));
+    return std::max(0, int(std::ceil(std::log2(cells))));
 }
 
 

@@ -5,8 +5,8 @@ quarter, half or whole warp per pair, with 2 to 32 rows per lane.  Every geometr
 the same cells, so results do not change; speed does, through padding (rows rounded up to
 whole stripes), skew (the wavefront's ramp), parallelism and shared memory per group.
 
-Pairs are grouped in size classes: max(20, ceil(log2(rows * columns))), the same rule as the
-library's planner (so every pair up to 2^20 cells is one class).  For each class in a batch
+Pairs are grouped in size classes: ceil(log2(rows * columns)), the same rule as the library's
+planner, so a batch of pairs of 100 to 500 residues spans five classes, each tuned apart.  For each class in a batch
 the tuner aligns a sample of the class's own pairs with every candidate geometry, times the
 device work (``SeqPairBatch.last_timing``), keeps the fastest and stores the choice in a JSON
 cache keyed by device, problem type and class.
@@ -32,7 +32,7 @@ SOFT_GEOS = [(32, 4), (32, 2), (32, 8), (16, 4), (16, 2), (16, 8), (8, 4), (1, 8
 
 
 def size_class(rows: int, cols: int) -> int:
-    return max(20, int(math.ceil(math.log2(max(rows, 1) * max(cols, 1)))))
+    return max(0, int(math.ceil(math.log2(max(rows, 1) * max(cols, 1)))))
 
 
 def _cache_path() -> str:
@@ -80,7 +80,7 @@ def _classes(batch) -> dict:
     n = np.diff(batch._ob).astype(np.int64)
     rows = m + 1 if _soft(batch) else m
     cells = np.maximum(rows, 1).astype(np.float64) * np.maximum(n, 1).astype(np.float64)
-    sc = np.maximum(20, np.ceil(np.log2(cells))).astype(np.int64)
+    sc = np.maximum(0, np.ceil(np.log2(cells))).astype(np.int64)
     return {int(c): np.nonzero(sc == c)[0] for c in np.unique(sc)}
 
 
