@@ -378,6 +378,18 @@ struct nwg_store {
     int64_t scratch_budget = -1;   // bytes of soft scratch one call may hold (-1: from the device's memory)
     int64_t ck_threshold = int64_t(16) << 20;     // soft: forward tables above this are checkpointed
     int spin_limit = nwg::kSpinLimit;             // several warps per pair: polls before a wait gives up
+    // work-queue counters, two ints per launch of a call (soft launches from 0, hard fills from
+    // kQueueHard); each launch leaves its pair at zero, so they are zeroed once
+    static constexpr int kQueues = 4096, kQueueHard = 2048;
+    DBuf wq;
+    int* queue(int k, cudaStream_t st) {
+        if (!wq.p) {
+            wq.need(size_t(kQueues) * 2 * sizeof(int), st);
+            NWG_CUDA(cudaMemsetAsync(wq.p, 0, wq.bytes, st));
+        }
+        if (k < 0 || k >= kQueues) throw Error(NWG_EINVAL, "too many launches in one call");
+        return wq.as<int>() + 2 * k;
+    }
     DBuf stripe_tab;
     DBuf hb_pairs;                      // the pairs a Hirschberg run splits
     std::vector<int32_t> h_status;
@@ -782,6 +794,7 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
         A.score = s->score.as<double>(); A.end = s->end.as<int32_t>();
         A.ends = ends;
         A.spin_limit = s->spin_limit;
+        A.queue = s->queue(nwg_store::kQueueHard + int(fills.size()), st);
         fills.push_back(make_launch(reinterpret_cast<const void*>(fn), unsigned(blocks), hblock, smem, A));
         fill_args.push_back(A);
     }
@@ -1066,6 +1079,7 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
         A.score = s->score.as<double>(); A.grad = s->grad.as<double>(); A.gstride = s->gstride;
         A.status = s->status.as<int32_t>();
         A.spin_limit = s->spin_limit;
+        A.queue = s->queue(int(launches.size()), st);
         if (ovf) {
             // a weight overflows T: every pair of this bucket is out of range in T
             mark_status_kernel<<<unsigned((items + 255) / 256), 256, 0, st>>>(A.order, items, A.status,

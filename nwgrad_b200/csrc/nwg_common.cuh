@@ -114,6 +114,18 @@ __device__ __forceinline__ void prefetch_l2_bulk(const void* p, unsigned bytes) 
 __device__ __forceinline__ void prefetch_l2(const void* p) {
     asm volatile("prefetch.global.L2 [%0];" ::"l"(p) : "memory");
 }
+// Work queue of one persistent launch: q[0] the next item of the launch's order (longest
+// first), q[1] the groups that have found it empty.  A group's leader draws items until one is
+// past the end; the last of the launch's ngroups groups to do so resets both counters, so the
+// next launch (or graph replay) on the same counters starts at zero without a memset.
+__device__ __forceinline__ int64_t wq_next(int* q, int ngroups, int64_t n_items) {
+    const int64_t it = atomicAdd(q, 1);
+    if (it >= n_items && atomicAdd(q + 1, 1) == ngroups - 1) {
+        atomicExch(q, 0);
+        atomicExch(q + 1, 0);
+    }
+    return it;
+}
 __device__ __forceinline__ bool is_finite(float x) { return (__float_as_uint(x) & 0x7f800000u) != 0x7f800000u; }
 __device__ __forceinline__ bool is_finite(double x) {
     return (static_cast<unsigned long long>(__double_as_longlong(x)) & 0x7ff0000000000000ull) != 0x7ff0000000000000ull;

@@ -58,6 +58,7 @@ struct HardArgs {
     // 8 b_end (row m's cells ends); 0: Global's charged borders and end (m, n)
     int ends;
     int spin_limit;                            // several warps per pair: polls before a wait gives up
+    int* queue;                                // this launch's work-queue counters (2 ints, zero at launch)
 };
 
 // The band of DP row i around guide g (aligner.hpp:2644-2700): columns [jlo, jhi].
@@ -159,7 +160,23 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
         }
     };
 
-    for (int64_t it = MW ? int64_t(blockIdx.x) : slot; it < A.n_items; it += MW ? int64_t(gridDim.x) : int64_t(gridDim.x) * gpb) {
+    // the next pair of this group (a block, for several warps per pair) from the launch's work
+    // queue, in the longest-first order: a group that finishes early takes the next pair
+    __shared__ long long s_next;
+    auto next_item = [&]() -> int64_t {
+        if constexpr (MW) {
+            __syncthreads();
+            if (threadIdx.x == 0) s_next = wq_next(A.queue, int(gridDim.x), A.n_items);
+            __syncthreads();
+            return s_next;
+        } else {
+            long long v = 0;
+            if (lane == 0) v = wq_next(A.queue, int(gridDim.x) * gpb, A.n_items);
+            if constexpr (G > 1) v = __shfl_sync(gmask, v, 0, G);
+            return v;
+        }
+    };
+    for (int64_t it = next_item(); it < A.n_items; it = next_item()) {
         if constexpr (MW) {
             if (lane == 0) prog[gib] = -1;
             __syncthreads();

@@ -69,6 +69,7 @@ struct SoftArgs {
     double* score; double* grad; int64_t gstride;
     int32_t* status;                         // per pair: 0 ok, else kSoft* bits (why it was refused)
     int spin_limit;                          // several warps per pair: polls before a wait gives up
+    int* queue;                              // this launch's work-queue counters (2 ints, zero at launch)
 };
 
 // Per-pair status bits of a soft pass: a refused pair's score and counts are not written and
@@ -325,7 +326,23 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
     // lie more than that above a lane's scale only when they are at most 2^kLift in its units)
     constexpr int kExpHi = sizeof(T) == 4 ? 126 : 1022;
 
-    for (int64_t it = slot; it < A.n_items; it += MW ? int64_t(gridDim.x) : int64_t(gridDim.x) * gpb) {
+    // the next pair of this group (a block, for several warps per pair) from the launch's work
+    // queue, in the longest-first order: a group that finishes early takes the next pair
+    __shared__ long long s_next;
+    auto next_item = [&]() -> int64_t {
+        if constexpr (MW) {
+            __syncthreads();
+            if (threadIdx.x == 0) s_next = wq_next(A.queue, int(gridDim.x), A.n_items);
+            __syncthreads();
+            return s_next;
+        } else {
+            long long v = 0;
+            if (lane == 0) v = wq_next(A.queue, int(gridDim.x) * gpb, A.n_items);
+            if constexpr (G > 1) v = __shfl_sync(gmask, v, 0, G);
+            return v;
+        }
+    };
+    for (int64_t it = next_item(); it < A.n_items; it = next_item()) {
         const int p = A.order[it];
         const int64_t ao = A.oa[p], bo = A.ob[p];
         const int m = int(A.oa[p + 1] - ao), n = int(A.ob[p + 1] - bo);
