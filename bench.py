@@ -129,15 +129,15 @@ def c1_workload(n_pairs=10000, seed=0):
     return mat, a, oa, b, ob
 
 
-def c5_requests(n_req, seed=5, max_batch=4096):
-    """Serving requests: batch size log-uniform 1..max_batch, A lengths log-uniform 20-5000,
+def c5_requests(n_req, seed=5, max_batch=4096, lmin=20, lmax=5000):
+    """Serving requests: batch size log-uniform 1..max_batch, A lengths log-uniform lmin-lmax,
     B = A with 30 % substitutions and single-residue insertions / deletions at 2.5 % each."""
     rng = np.random.default_rng(seed)
     freqs = rng.dirichlet(np.full(20, 5.0))
     out = []
     for _ in range(n_req):
         k = min(max_batch, int(np.exp(rng.uniform(0.0, np.log(max_batch + 1)))))
-        la = np.exp(rng.uniform(np.log(20), np.log(5000), size=k)).astype(np.int64)
+        la = np.exp(rng.uniform(np.log(lmin), np.log(lmax), size=k)).astype(np.int64)
         oa = np.zeros(k + 1, np.int64)
         np.cumsum(la, out=oa[1:])
         a = rng.choice(20, size=int(oa[-1]), p=freqs).astype(np.uint8)
@@ -336,7 +336,9 @@ def serve_server(params, reqs, arrivals, device, workers=3):
         st = srv.stats()
     p50, p99 = _quantiles(lat)
     return {"p50_ms": p50, "p99_ms": p99, "gcups": cells / span / 1e9, "seconds": span,
-            "batches": int(st["batches"]), "requests": len(reqs)}
+            "batches": int(st["batches"]), "requests": len(reqs),
+            "device_overlap": st["device_overlap"], "device_busy_ms": st["device_busy_ms"],
+            "device_sum_ms": st["device_sum_ms"]}
 
 
 def serve_plain(params, reqs, arrivals, device):
@@ -362,7 +364,7 @@ def serve_plain(params, reqs, arrivals, device):
     return {"p50_ms": p50, "p99_ms": p99, "gcups": cells / span / 1e9, "seconds": span, "requests": len(reqs)}
 
 
-def serve_bench(params, n_req, device, seed=5):
+def serve_bench(params, n_req, device, seed=5, n_lat=10000):
     reqs = c5_requests(n_req, seed=seed)
     cells = sum(cells_of(oa, ob) for _, oa, _, ob in reqs)
     burst = [0.0] * len(reqs)
@@ -382,7 +384,31 @@ def serve_bench(params, n_req, device, seed=5):
                         "(30% subs, 2.5% ins, 2.5% del), soft global affine f32",
             "offered_rate_per_s": rate,
             "server": {"burst": srv_burst, "poisson": srv_poisson, "workers": 3},
-            "plain_fill_one_at_a_time": {"burst": plain_burst, "poisson": plain_poisson}}
+            "plain_fill_one_at_a_time": {"burst": plain_burst, "poisson": plain_poisson},
+            "latency": serve_latency(params, n_lat, device, seed=seed + 7)}
+
+
+def serve_latency(params, n_req, device, seed=12, load=0.8, n_plain=2000):
+    """Latency arm at the small end of the serving distribution (lengths log-uniform 20-300,
+    batch sizes log-uniform 1-64): the server's capacity from a burst of all n_req requests,
+    then Poisson arrivals at `load` of that capacity through the server (p50 / p99 over n_req
+    requests) and, for comparison, the first n_plain of the same arrivals through plain-fill
+    batches one request at a time."""
+    reqs = c5_requests(n_req, seed=seed, max_batch=64, lmin=20, lmax=300)
+    burst = [0.0] * len(reqs)
+    serve_server(params, reqs[:64], burst[:64], device)
+    serve_plain(params, reqs[:16], burst[:16], device)
+    cap = serve_server(params, reqs, burst, device)
+    rate = load * len(reqs) / cap["seconds"]
+    rng = np.random.default_rng(seed + 1000)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(reqs))).tolist()
+    srv = serve_server(params, reqs, arrivals, device)
+    plain = serve_plain(params, reqs[:n_plain], arrivals[:n_plain], device)
+    return {"requests": len(reqs), "workload": "lengths log-uniform 20-300, batch sizes log-uniform 1-64, "
+                                               "B = A mutated, soft global affine f32",
+            "capacity_req_per_s": len(reqs) / cap["seconds"], "offered_rate_per_s": rate, "load": load,
+            "server_burst": cap, "server_poisson": srv,
+            "plain_fill_one_at_a_time_poisson": dict(plain, note=f"first {n_plain} arrivals")}
 
 
 # ── main ─────────────────────────────────────────────────────────────────────

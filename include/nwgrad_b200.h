@@ -187,6 +187,10 @@ int nwg_server_wait(nwg_server* s, int64_t ticket, double* scores, double* grad,
 /* Latency p50 / p99 (ms) of completed requests, throughput since the first submit. */
 int nwg_server_stats(nwg_server* s, double* p50_ms, double* p99_ms, double* gcups, int64_t* done,
                      int64_t* batches);
+/* Device time of the completed batches (CUDA events around each batch's run, on its worker's
+ * stream): busy_ms the union of the intervals, sum_ms the sum of their lengths -- sum / busy > 1
+ * means batches of different workers were on the device at the same time. */
+int nwg_server_device_stats(nwg_server* s, double* busy_ms, double* sum_ms, int64_t* batches);
 int nwg_server_destroy(nwg_server* s);
 const char* nwg_server_last_error(void);
 

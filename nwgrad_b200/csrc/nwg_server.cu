@@ -77,6 +77,9 @@ struct nwg_server {
     std::vector<double> latencies_ms;
     double cells_done = 0;
     int64_t batches = 0;
+    // device intervals of the batches (ms from ev_ref): how much the workers' batches overlap
+    cudaEvent_t ev_ref = nullptr;
+    std::vector<std::pair<double, double>> dev_iv;
     Clock::time_point t0;
     bool started = false;
 };
@@ -98,7 +101,8 @@ double request_bytes(const nwg_job& J, const std::vector<int64_t>& oa, const std
     return b;
 }
 
-void run_batch(nwg_server* S, nwg_store*& store, cudaStream_t st, std::vector<std::shared_ptr<Request>>& reqs) {
+void run_batch(nwg_server* S, nwg_store*& store, cudaStream_t st, cudaEvent_t e0, cudaEvent_t e1,
+               std::vector<std::shared_ptr<Request>>& reqs) {
     // concatenate the requests' pairs
     std::vector<uint8_t> a, b;
     std::vector<int64_t> oa{0}, ob{0};
@@ -134,7 +138,9 @@ void run_batch(nwg_server* S, nwg_store*& store, cudaStream_t st, std::vector<st
     }
     double total = 0;
     if (rc == NWG_OK) ck(nwg_params_set(store, P.mats.data(), P.gaps.data(), P.K, P.N));
+    cudaEventRecord(e0, st);
     if (rc == NWG_OK) ck(nwg_run(store, &S->job, st, &total));
+    cudaEventRecord(e1, st);
     const int64_t gs = int64_t(P.K) * P.N * P.N + 4 * P.K;
     for (size_t k = 0; k < reqs.size(); ++k) {
         auto& r = reqs[k];
@@ -144,8 +150,13 @@ void run_batch(nwg_server* S, nwg_store*& store, cudaStream_t st, std::vector<st
         if (rc == NWG_OK && S->job.grad_mode && r->n_pairs)
             ck(nwg_reduce_range(store, first[k], first[k + 1], nullptr, r->grad.data()));
     }
+    float ms0 = 0, ms1 = 0;
+    const bool timed = cudaEventSynchronize(e1) == cudaSuccess && S->ev_ref &&
+                       cudaEventElapsedTime(&ms0, S->ev_ref, e0) == cudaSuccess &&
+                       cudaEventElapsedTime(&ms1, S->ev_ref, e1) == cudaSuccess;
     const auto now = Clock::now();
     std::lock_guard<std::mutex> lk(S->mu);
+    if (timed) S->dev_iv.emplace_back(double(ms0), double(ms1));
     for (auto& r : reqs) {
         r->status = rc;
         r->err = err;
@@ -162,6 +173,9 @@ void worker_main(nwg_server* S) {
     cudaSetDevice(S->device);
     cudaStream_t st = nullptr;
     cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
     nwg_store* store = nullptr;
     while (true) {
         std::vector<std::shared_ptr<Request>> take;
@@ -191,7 +205,7 @@ void worker_main(nwg_server* S) {
             }
             S->in_flight_bytes += int64_t(bytes);
         }
-        run_batch(S, store, st, take);
+        run_batch(S, store, st, e0, e1, take);
         {
             std::lock_guard<std::mutex> lk(S->mu);
             S->in_flight_bytes -= int64_t(bytes);
@@ -199,6 +213,8 @@ void worker_main(nwg_server* S) {
         S->cv_work.notify_all();
     }
     if (store) nwg_store_destroy(store);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
     if (st) cudaStreamDestroy(st);
 }
 
@@ -235,6 +251,13 @@ int nwg_server_create(int device, const nwg_job* job, int nalpha, const double* 
         P->gaps.assign(gaps, gaps + size_t(4) * K);
         S->params = P;
         S->t0 = Clock::now();
+        cudaSetDevice(device);
+        if (cudaEventCreate(&S->ev_ref) == cudaSuccess) {
+            cudaEventRecord(S->ev_ref, nullptr);
+            cudaEventSynchronize(S->ev_ref);
+        } else {
+            S->ev_ref = nullptr;
+        }
         nwg_server* raw = S.get();
         for (int w = 0; w < workers; ++w) S->workers.emplace_back(worker_main, raw);
         *out = S.release();
@@ -328,6 +351,31 @@ int nwg_server_stats(nwg_server* S, double* p50_ms, double* p99_ms, double* gcup
     });
 }
 
+// Device time of the completed batches: the union of their intervals (the device was busy
+// with at least one batch) and the sum of their lengths; sum / union > 1 means batches of
+// different workers ran on the device at the same time.
+int nwg_server_device_stats(nwg_server* S, double* busy_ms, double* sum_ms, int64_t* batches) {
+    return sguard([&]() -> int {
+        std::vector<std::pair<double, double>> iv;
+        {
+            std::lock_guard<std::mutex> lk(S->mu);
+            iv = S->dev_iv;
+        }
+        std::sort(iv.begin(), iv.end());
+        double uni = 0, sum = 0, cs = 0, ce = -1;
+        for (auto& x : iv) {
+            sum += x.second - x.first;
+            if (x.first > ce) { if (ce > cs) uni += ce - cs; cs = x.first; ce = x.second; }
+            else ce = std::max(ce, x.second);
+        }
+        if (ce > cs) uni += ce - cs;
+        if (busy_ms) *busy_ms = uni;
+        if (sum_ms) *sum_ms = sum;
+        if (batches) *batches = int64_t(iv.size());
+        return NWG_OK;
+    });
+}
+
 int nwg_server_destroy(nwg_server* S) {
     return sguard([&]() -> int {
         if (!S) return NWG_OK;
@@ -337,6 +385,7 @@ int nwg_server_destroy(nwg_server* S) {
         }
         S->cv_work.notify_all();
         for (auto& t : S->workers) t.join();
+        if (S->ev_ref) cudaEventDestroy(S->ev_ref);
         delete S;
         return NWG_OK;
     });

@@ -32,9 +32,11 @@ def _lib():
         L.nwg_server_stats.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                        C.POINTER(C.c_double), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
         L.nwg_server_destroy.argtypes = [C.c_void_p]
+        L.nwg_server_device_stats.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                              C.POINTER(C.c_int64)]
         L.nwg_server_last_error.restype = C.c_char_p
         for f in ("nwg_server_create", "nwg_server_set_params", "nwg_server_submit", "nwg_server_wait",
-                  "nwg_server_stats", "nwg_server_destroy"):
+                  "nwg_server_stats", "nwg_server_destroy", "nwg_server_device_stats"):
             getattr(L, f).restype = C.c_int
         L._server_bound = True
     return L
@@ -122,8 +124,11 @@ class Server:
         done, batches = C.c_int64(), C.c_int64()
         _check(self._L, self._L.nwg_server_stats(self._h, C.byref(p50), C.byref(p99), C.byref(gc),
                                                  C.byref(done), C.byref(batches)))
+        busy, total, nb = C.c_double(), C.c_double(), C.c_int64()
+        _check(self._L, self._L.nwg_server_device_stats(self._h, C.byref(busy), C.byref(total), C.byref(nb)))
         return {"p50_ms": p50.value, "p99_ms": p99.value, "gcups": gc.value, "done": done.value,
-                "batches": batches.value}
+                "batches": batches.value, "device_busy_ms": busy.value, "device_sum_ms": total.value,
+                "device_overlap": (total.value / busy.value) if busy.value > 0 else None}
 
     def close(self):
         if getattr(self, "_h", None):

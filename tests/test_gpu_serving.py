@@ -61,3 +61,23 @@ def test_set_params_applies_to_later_requests():
         b = nw.SeqPairBatch(sa, sb, p)
         b.score_and_grad()
         assert np.array_equal(b.scores(), s)
+
+
+def test_concurrent_batches_overlap_on_the_device():
+    """A burst of requests larger than one worker's batch: the workers' batches are in flight
+    on the device at the same time -- the sum of their device intervals (CUDA events around
+    each batch's run) exceeds the time the device had any batch in flight."""
+    rng = np.random.default_rng(9)
+    mat = rand_matrix(rng, 20)
+    params = nw.AlignParams.from_arrays(mat, [[11.0, 1.0, 11.0, 1.0]], alphabet=AA)
+    reqs = []
+    for _ in range(12):
+        sa = rand_seqs(rng, 150, 200, 400, AA)
+        reqs.append((sa, [mutate(rng, s, AA) for s in sa]))
+    with Server(params, grad_mode="soft", workers=3, max_batch_pairs=300) as srv:
+        tickets = [srv.submit(sa, sb) for sa, sb in reqs]
+        for t, (sa, _) in zip(tickets, reqs):
+            srv.wait(t, len(sa))
+        st = srv.stats()
+    assert st["batches"] >= 6
+    assert st["device_sum_ms"] > st["device_busy_ms"] > 0, st
