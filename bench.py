@@ -439,20 +439,18 @@ def main():
                          "c6-glocal (miRNA-like A within longer B, glocal ends, hard and soft)")
     ap.add_argument("--glocal-pairs", type=int, default=200_000)
     ap.add_argument("--long-pairs", type=int, default=64)
-    ap.add_argument("--short-pairs", type=int, default=2_000_000)
+    ap.add_argument("--short-pairs", type=int, default=10_000_000)
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the other configurations' measurements (hard batch, short pairs, long pairs, "
+                         "serve + train) in the default run")
     ap.add_argument("--train-pairs", type=int, default=2000, help="c5-serve-train: homolog pairs (as many decoys)")
     ap.add_argument("--train-steps", type=int, default=200)
     args = ap.parse_args()
-    if args.workload == "c1-hard":
-        return bench_c1(args)
-    if args.workload == "c4-long":
-        return bench_c4(args)
-    if args.workload == "c3-short":
-        return bench_c3(args)
-    if args.workload == "c5-serve-train":
-        return bench_c5(args)
-    if args.workload == "c6-glocal":
-        return bench_c6(args)
+    side = {"c1-hard": bench_c1, "c4-long": bench_c4, "c3-short": bench_c3, "c5-serve-train": bench_c5,
+            "c6-glocal": bench_c6}
+    if args.workload in side:
+        print(json.dumps(side[args.workload](args)))
+        return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -665,13 +663,26 @@ def main():
     serve = None
     if rank == 0 and world == 1 and not args.no_serve and args.serve_requests > 0:
         serve = serve_bench(params, args.serve_requests, local)
+    extras = None
+    if rank == 0 and world == 1 and not args.no_extras:
+        # the other configurations, each measured on its own inputs after the headline's
+        import copy
+        extras = {}
+        for name, fn, over in (("c1_hard_batch", bench_c1, {}), ("c3_short_pairs", bench_c3, {}),
+                               ("c4_long_pairs", bench_c4, {}), ("c5_serve_train", bench_c5, {"serve_requests": 60})):
+            a2 = copy.copy(args)
+            for k, v in over.items():
+                setattr(a2, k, v)
+            t0 = time.perf_counter()
+            extras[name] = fn(a2)
+            extras[name]["wall_s"] = time.perf_counter() - t0
     if rank == 0:
         print(json.dumps({
             "metric": "soft-grad batch GCUPS", "value": value, "unit": "GCUPS", "n_gpus": world,
             "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": total_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded)", "config": config, "e2e": e2e, "roofline": roofline,
-            "cpu_baseline": cpu, "parity": parity, "clocks": clocks, "gpu_launches": launches,
+            "cpu_baseline": cpu, "parity": parity, "clocks": clocks, "gpu_launches": launches, "extras": extras,
             "plain_fill": plain, "serve": serve,
             "autotune": {str(k): _tune_mod().describe(v) for k, v in tune_table.items()},
             "step_ms": step_ms, "graph_captures_timed": getattr(clk, "captures", None)}))
@@ -745,7 +756,7 @@ def bench_c4(args):
     bt.score_and_grad()
     t = _timed_run(lambda: (bt.score_and_grad(), bt.compute_grad()))
     out["stages"]["soft_f32"] = {"seconds": t, "gcups": cells / t / 1e9}
-    print(json.dumps(out))
+    return out
 
 
 def c3_workload(n_pairs, seed=3):
@@ -827,7 +838,7 @@ def bench_c6(args):
             res["cpu_reference"] = {"gcups": ck / float(np.min(secs)) / 1e9, "pairs": k, "cores": threads,
                                     "isa": isa, "sample": f"first {k} pairs, best of {len(secs)}"}
         out["modes"][grad] = res
-    print(json.dumps(out))
+    return out
 
 
 def bench_c3(args):
@@ -854,7 +865,7 @@ def bench_c3(args):
                               "plain_fill_gcups": cells / tp / 1e9,
                               "autotune": {str(k): _tune_mod().describe(v) for k, v in table.items()}}
         del bt
-    print(json.dumps(out))
+    return out
 
 
 def bench_c1(args):
@@ -878,11 +889,11 @@ def bench_c1(args):
         e0.record(); bt.score_and_grad(); bt.compute_grad(); e1.record(); torch.cuda.synchronize()
         ms.append(e0.elapsed_time(e1)); kms += bt.last_timing()[0]
     tot = float(np.sum(ms))
-    print(json.dumps({"metric": "hard-grad batch GCUPS", "value": cells * args.steps / (tot / 1e3) / 1e9,
+    return ({"metric": "hard-grad batch GCUPS", "value": cells * args.steps / (tot / 1e3) / 1e9,
                       "unit": "GCUPS", "n_gpus": 1, "steps": args.steps, "ms_per_step": tot / args.steps,
                       "kernel_ms_per_step": kms / args.steps, "config": {"workload": "c1 hard global affine float32, "
                       "10k pairs L 50-300", "cells_per_step": cells},
-                      "autotune": {str(k): _tune_mod().describe(v) for k, v in table.items()}, "step_ms": ms}))
+                      "autotune": {str(k): _tune_mod().describe(v) for k, v in table.items()}, "step_ms": ms})
 
 
 def _trainer(pos, neg, mat, gaps0, steps, srv=None):
@@ -965,7 +976,7 @@ def bench_c5(args):
         tt.join()
     p50, p99 = _quantiles(lat)
     train_mixed, margins_mixed = out["train"]
-    print(json.dumps({
+    return ({
         "metric": "serve p50/p99 latency and training GCUPS, both at once", "n_gpus": 1,
         "config": {"workload": "Poisson request stream (lengths log-uniform 20-5000, batch sizes log-uniform "
                                "1-4096, B mutated) through the server, offered at 70% of its burst capacity, "
@@ -982,7 +993,7 @@ def bench_c5(args):
         "mixed": {"serve_p50_ms": p50, "serve_p99_ms": p99, "serve_gcups": req_cells / serve_span / 1e9,
                   "train_seconds": train_mixed, "train_gcups": train_cells * steps / train_mixed / 1e9,
                   "margin_last": margins_mixed[-1]},
-    }))
+    })
 
 
 if __name__ == "__main__":
