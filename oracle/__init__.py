@@ -51,7 +51,8 @@ def lib():
                                                       _dp, _dp, _i32p, _u8p, C.c_int64, _i64p, _i32p, C.c_int]
         L.orc_hard_batch.restype = C.c_int
         L.orc_soft_batch.argtypes = [C.c_int] * 4 + [_dp, _dp, _u8p, _i64p, _u8p, _i64p, C.c_int64,
-                                                      _u16p, _u16p, C.c_double, _dp, _dp, _i32p, C.c_int, C.c_int]
+                                                      _u16p, _u16p, C.c_double, _dp, _dp, _i32p, C.c_int, C.c_int,
+                                                      _i32p]
         L.orc_soft_batch.restype = C.c_int
         L.orc_hb_batch.argtypes = [C.c_int] * 4 + [_dp, _dp, _u8p, _i64p, _u8p, _i64p, C.c_int64,
                                                     _dp, _dp, _i32p, _u8p, C.c_int64, _i64p, C.c_int, _i32p, C.c_int,
@@ -149,9 +150,11 @@ def hirschberg(prec, mat, gaps, enc: Encoded, cutoff=512, pmax=False, moves_cap=
     return dict(scores=scores, grads=grads, guides=guides, moves=moves, nmoves=nmoves, ends=ends)
 
 
-def soft(gm, am, mat, gaps, enc: Encoded, temperature=1.0, guides_in=None, band=-1, free_ends=12):
+def soft(gm, am, mat, gaps, enc: Encoded, temperature=1.0, guides_in=None, band=-1, free_ends=12,
+         posterior=False):
     """Log-space double forward-backward: (scores = T log Z, grads = expected counts); with
-    guides_in and band >= 0 the guide-banded one."""
+    guides_in and band >= 0 the guide-banded one; posterior=True adds the posterior guides
+    (m + 1 columns per pair at off_a[p] + p, the reference's posterior_rows_log)."""
     L = lib()
     mat = np.ascontiguousarray(mat, np.float64)
     gaps = np.ascontiguousarray(gaps, np.float64)
@@ -159,14 +162,15 @@ def soft(gm, am, mat, gaps, enc: Encoded, temperature=1.0, guides_in=None, band=
     gs = K * N * N + 4 * K
     scores = np.zeros(enc.n, np.float64)
     grads = np.zeros((enc.n, gs), np.float64)
+    post = np.zeros(int(enc.oa[-1]) + enc.n + 1, np.int32) if posterior else None
     rc = L.orc_soft_batch(gm, am, N, K, _p(mat, _dp), _p(gaps, _dp), _p(enc.a, _u8p),
                           _p(enc.oa, _i64p), _p(enc.b, _u8p), _p(enc.ob, _i64p), enc.n,
                           _p(enc.tracks, _u16p), _p(enc.gap_tracks, _u16p), float(temperature),
                           _p(scores, _dp), _p(grads, _dp),
                           _p(None if guides_in is None else np.ascontiguousarray(guides_in, np.int32), _i32p),
-                          int(band), int(free_ends))
+                          int(band), int(free_ends), _p(post, _i32p))
     assert rc == 0
-    return scores, grads
+    return (scores, grads, post) if posterior else (scores, grads)
 
 
 def blocked_sum(grads, weights=None):
@@ -189,7 +193,7 @@ class _Problem(C.Structure):
                 ("tracks", _u16p), ("gtracks", _u16p), ("traceback", C.c_int), ("kernel", C.c_int),
                 ("n_threads", C.c_int), ("temperature", C.c_double), ("soft_impl", C.c_int),
                 ("soft_f32", C.c_int), ("hb_cutoff", C.c_int), ("inter_fill", C.c_int),
-                ("free_ends", C.c_int)]
+                ("free_ends", C.c_int), ("soft_guide", C.c_int)]
 
 
 def ref_available(simd=False):
@@ -217,7 +221,7 @@ _TB = {"auto": 0, "pointers": 1, "scores": 2, "hirschberg": 3, "hirschberg_pmax"
 
 def _problem(prec, gm, am, grad_mode, alphabet, mat, gaps, seqs_a, seqs_b, tracks, gap_tracks,
              traceback, kernel, n_threads, temperature, soft_impl, soft_f32, hb_cutoff, inter_fill,
-             free_ends=12):
+             free_ends=12, soft_guide=0):
     keep = []
     mat = np.ascontiguousarray(mat, np.float64)
     gaps = np.ascontiguousarray(gaps, np.float64)
@@ -235,21 +239,22 @@ def _problem(prec, gm, am, grad_mode, alphabet, mat, gaps, seqs_a, seqs_b, track
     P = _Problem(prec, gm, am, grad_mode, mat.shape[1], mat.shape[0], _p(mat, _dp), _p(gaps, _dp),
                  alpha, len(seqs_a), a, _p(oa, _i64p), b, _p(ob, _i64p), _p(tk, _u16p),
                  _p(gk, _u16p), _TB[traceback], kernel, n_threads, float(temperature),
-                 soft_impl, int(soft_f32), hb_cutoff, int(inter_fill), int(free_ends))
+                 soft_impl, int(soft_f32), hb_cutoff, int(inter_fill), int(free_ends), int(soft_guide))
     return P, keep, oa
 
 
 def ref_run(prec, gm, am, grad_mode, alphabet, mat, gaps, seqs_a, seqs_b, tracks=None,
             gap_tracks=None, traceback="pointers", kernel=-1, n_threads=1, temperature=1.0,
             soft_impl=0, soft_f32=True, hb_cutoff=0, inter_fill=True, band=-1, mat2=None,
-            gaps2=None, simd=False, free_ends=12):
-    """Run the reference batch once; returns dict(scores, grads, guides, total)."""
+            gaps2=None, simd=False, free_ends=12, soft_guide=0):
+    """Run the reference batch once; returns dict(scores, grads, guides, total).  soft_guide: 0
+    eager, 1 lazy, 2 posterior (the guides a soft run leaves)."""
     L = ref_lib(simd)
     if n_threads <= 0:
         n_threads = physical_cores()
     P, keep, oa = _problem(prec, gm, am, grad_mode, alphabet, mat, gaps, seqs_a, seqs_b, tracks,
                            gap_tracks, traceback, kernel, n_threads, temperature, soft_impl,
-                           soft_f32, hb_cutoff, inter_fill, free_ends)
+                           soft_f32, hb_cutoff, inter_fill, free_ends, soft_guide)
     K, N = np.asarray(mat).shape[0], np.asarray(mat).shape[1]
     n = len(seqs_a)
     scores = np.zeros(n, np.float64)

@@ -669,7 +669,34 @@ void setup_drows(DRows& R, const Model& M, const uint8_t* a, int m, const uint16
     }
 }
 
-struct SoftOut { double logz = 0; double* grad = nullptr; };
+struct SoftOut { double logz = 0; double* grad = nullptr; int32_t* post = nullptr; };
+
+// soft_guide="posterior" (aligner.hpp:6776-6808, posterior_rows_log): per row i, the column of
+// greatest EXIT mass over the row's band -- the cell's posterior less the mass moving on to
+// (i, j+1) in row i (affine: the Y posterior at (i, j+1); linear: F(i,j) e_a B(i,j+1)) -- the
+// first such column on ties; both in units of the row's largest cell posterior.  v(j) and y(j)
+// are the two log-space terms at column j.  The rows then become a monotone guide.
+template <class V, class Y>
+void posterior_rows(int m, const Band& bd, int32_t* post, V&& v, Y&& y) {
+    const double NI = -std::numeric_limits<double>::infinity();
+    for (int i = 0; i <= m; ++i) {
+        post[i] = 0;
+        const int lo = bd.jlo0(i), hi = bd.jhi0(i);
+        if (lo > hi) continue;
+        double rmax = NI;
+        for (int j = lo; j <= hi; ++j) rmax = std::max(rmax, v(i, j));
+        double bv = -1.0;
+        int bj = lo;
+        for (int j = lo; j <= hi; ++j) {
+            const double e = std::exp(v(i, j) - rmax) - std::exp((j < hi ? y(i, j) : NI) - rmax);
+            if (e > bv) { bv = e; bj = j; }
+        }
+        post[i] = bj;
+    }
+    // posterior_guide (aligner.hpp:1466-1475): the rows as a guide, non-decreasing in [0, n]
+    int run = 0;
+    for (int i = 0; i <= m; ++i) { run = std::max(run, std::min(std::max(post[i], 0), bd.n)); post[i] = run; }
+}
 
 // Semi-global end cells, each once (aligner.hpp:6190-6196): row m's band (a free B end) or
 // (m, n), then column n of rows 0..m-1 (a free A end).
@@ -792,6 +819,10 @@ void soft_affine(const Model& M, const uint8_t* a, int m, const uint8_t* b, int 
             const double lo = lse2(FM[I(i, j - 1)], FX[I(i, j - 1)]) - R.goa[i] - R.gea[i] + by - lz;
             if (lo > -700) gap(R.gtrk[i], kOpenA) -= std::exp(lo);
         }
+    if (o.post)
+        posterior_rows(m, bd, o.post,
+                       [&](int i, int j) { return lse3(FM[I(i, j)] + BM[I(i, j)], FX[I(i, j)] + BX[I(i, j)], FY[I(i, j)] + BY[I(i, j)]); },
+                       [&](int i, int j) { return FY[I(i, j + 1)] + BY[I(i, j + 1)]; });
     o.logz = lz * T;
 }
 
@@ -863,6 +894,9 @@ void soft_linear(const Model& M, const uint8_t* a, int m, const uint8_t* b, int 
             if (bv == NI || fv == NI) continue;
             gap(R.gtrk[i], kExtendA) -= std::exp(fv - R.gea[i] + bv - lz);
         }
+    if (o.post)
+        posterior_rows(m, bd, o.post, [&](int i, int j) { return F[I(i, j)] + B[I(i, j)]; },
+                       [&](int i, int j) { return F[I(i, j)] - R.gea[i] + B[I(i, j + 1)]; });
     o.logz = lz * T;
 }
 
@@ -1427,7 +1461,7 @@ int orc_soft_batch(int gm, int am, int N, int K, const double* mat, const double
                    const uint8_t* a, const int64_t* oa, const uint8_t* b, const int64_t* ob,
                    int64_t n_pairs, const uint16_t* tracks, const uint16_t* gtracks,
                    double temperature, double* scores, double* grads, const int32_t* guides_in, int band,
-                   int free_ends) {
+                   int free_ends, int32_t* post_out) {
     Model M{gm, am, N, K, mat, gaps, free_ends};
     const size_t gs = size_t(K) * N * N + 4 * size_t(K);
     for (int64_t p = 0; p < n_pairs; ++p) {
@@ -1435,6 +1469,7 @@ int orc_soft_batch(int gm, int am, int N, int K, const double* mat, const double
         SoftOut o;
         o.grad = grads + gs * p;
         std::fill(o.grad, o.grad + gs, 0.0);
+        o.post = post_out ? post_out + oa[p] + p : nullptr;
         const uint16_t* tk = tracks ? tracks + oa[p] : nullptr;
         const uint16_t* gk = gtracks ? gtracks + oa[p] + p : nullptr;
         Band bd; bd.m = m; bd.n = n; bd.global = am == 0;

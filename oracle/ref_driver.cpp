@@ -39,6 +39,7 @@ struct Problem {
     int hb_cutoff;
     int inter_fill;  // fill="interpair"
     int free_ends;   // am 2 (semi-global): kSgFree* bits (1 a_begin, 2 a_end, 4 b_begin, 8 b_end)
+    int soft_guide;  // 0 eager, 1 lazy, 2 posterior
 };
 
 TracebackMode tb_of(int t) {
@@ -91,6 +92,7 @@ struct Run {
             batch->set_soft_impl(P.soft_impl == 2 ? SoftImpl::Log
                                  : P.soft_impl == 1 ? SoftImpl::ScaledOrLog : SoftImpl::Scaled);
             batch->set_soft_f32(P.soft_f32 != 0);
+            batch->set_soft_guide(P.soft_guide == 1, P.soft_guide == 2);
         }
         if (P.am == 2) batch->set_free_ends(P.free_ends);
         if (P.hb_cutoff > 0) batch->set_hb_cutoff(P.hb_cutoff);

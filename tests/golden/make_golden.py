@@ -303,8 +303,38 @@ def soft_banded_fixtures():
     print("soft_banded.npz:", len(out), "arrays")
 
 
+def posterior_fixtures():
+    """soft_guide="posterior": the reference engine's guides after a double soft pass, every gap
+    model and end mode (global, local, glocal, overlap), DNA and protein, T 1 and 0.5."""
+    rng = np.random.default_rng(654)
+    out = {}
+    for alpha in ("ACGT", "ACDEFGHIKLMNPQRSTVWY"):
+        N = len(alpha)
+        mat = rng.normal(0, 1.5, size=(1, N, N)).round(3)
+        gaps = rng.uniform(0.5, 3.0, size=(1, 4)).round(3)
+        sa = ["".join(rng.choice(list(alpha), size=int(rng.integers(1, 110)))) for _ in range(24)]
+        sb = []
+        for s in sa:
+            t = [c if rng.random() > 0.25 else str(rng.choice(list(alpha))) for c in s]
+            sb.append("".join(t) if rng.random() > 0.2 else "".join(rng.choice(list(alpha), size=int(rng.integers(1, 110)))))
+        key = f"N{N}_"
+        out.update({key + "mat": mat, key + "gaps": gaps, key + "sa": np.array(sa), key + "sb": np.array(sb),
+                    key + "alpha": np.array(alpha)})
+        for gm in (0, 1):
+            for am, fe in ((0, 12), (1, 12), (2, 12), (2, 15)):
+                for T in (1.0, 0.5):
+                    r = oracle.ref_run(64, gm, am, 2, alpha, mat, gaps, sa, sb, soft_guide=2, free_ends=fe,
+                                       temperature=T)
+                    out[f"{key}g{gm}_m{am}_e{fe}_T{T}_guides"] = r["guides"]
+                    out[f"{key}g{gm}_m{am}_e{fe}_T{T}_scores"] = r["scores"]
+    np.savez_compressed(os.path.join(HERE, "posterior.npz"), **out)
+    print("posterior.npz:", len(out), "arrays")
+
+
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["brute", "ref", "hb", "sb", "sg"]
+    which = sys.argv[1:] or ["brute", "ref", "hb", "sb", "sg", "post"]
+    if "post" in which:
+        posterior_fixtures()
     if "brute" in which:
         brute_fixtures()
     if "ref" in which:

@@ -198,3 +198,26 @@ def test_soft_banded_fixtures():
                 s, g = oracle.soft(gm, am, z["mat2"], z["gaps2"], enc, guides_in=g0, band=bw)
                 np.testing.assert_allclose(s, z[f"g{gm}_m{am}_b{bw}_scores"], rtol=1e-12, atol=1e-12)
                 np.testing.assert_allclose(g, z[f"g{gm}_m{am}_b{bw}_grads"], rtol=1e-10, atol=1e-12)
+
+
+def test_posterior_guides_pinned_to_the_reference():
+    """The oracle's soft_guide="posterior" (per-row argmax of exit mass, made monotone) against
+    the reference engine's guides (tests/golden/posterior.npz, make_golden.py post): every gap
+    model and end mode, DNA and protein, T 1 and 0.5; the scores to 1e-9."""
+    import os
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "posterior.npz"))
+    for N in (4, 20):
+        key = f"N{N}_"
+        alpha = str(z[key + "alpha"])
+        sa, sb = [str(s) for s in z[key + "sa"]], [str(s) for s in z[key + "sb"]]
+        lut = {c: i for i, c in enumerate(alpha)}
+        enc = oracle.Encoded([[lut[c] for c in s] for s in sa], [[lut[c] for c in s] for s in sb])
+        n = sum(len(s) + 1 for s in sa)
+        for gm in (0, 1):
+            for am, fe in ((0, 12), (1, 12), (2, 12), (2, 15)):
+                for T in (1.0, 0.5):
+                    pre = f"{key}g{gm}_m{am}_e{fe}_T{T}_"
+                    s, _, post = oracle.soft(gm, am, z[key + "mat"], z[key + "gaps"], enc, T, free_ends=fe,
+                                             posterior=True)
+                    np.testing.assert_allclose(s, z[pre + "scores"], rtol=1e-9, atol=1e-9)
+                    assert np.array_equal(post[:n], z[pre + "guides"][:n]), pre
