@@ -47,6 +47,9 @@ typedef struct nwg_job {
                           2 a_end (column n's cells ends), 4 b_begin (row 0 a free start),
                           8 b_end (row m's cells ends); "glocal" is 12, "overlap" 15.  Traceback
                           Pointers; banded re-alignment with 12 only (aligner.hpp:2222-2231) */
+    int soft_post;     /* soft, full DP, untracked: 1 also leave every pair's posterior guide
+                          (soft_guide="posterior", aligner.hpp:6776-6808, 1466-1475) for
+                          nwg_guides and a later banded run */
 } nwg_job;
 
 /* Last error message of the calling thread ("" if none). */

@@ -24,7 +24,7 @@ class Job(C.Structure):
                 ("precision", C.c_int), ("band", C.c_int), ("keep_paths", C.c_int),
                 ("temperature", C.c_double), ("soft_double", C.c_int), ("lanes", C.c_int),
                 ("rows", C.c_int), ("traceback", C.c_int), ("hb_cutoff", C.c_int),
-                ("free_ends", C.c_int)]
+                ("free_ends", C.c_int), ("soft_post", C.c_int)]
 
 
 _lib = None

@@ -327,7 +327,8 @@ class SeqPairBatch:
                              "only; align these free ends with the full DP")
         return Job(_GAP[self._gap_model], self._am, grad_mode, self._precision, band,
                    int(bool(keep_paths)), float(self.soft_temperature), soft_double, lanes, rows,
-                   tb, int(self._hb_cutoff), int(self._sg))
+                   tb, int(self._hb_cutoff), int(self._sg),
+                   int(grad_mode == 2 and band < 0 and self._soft_guide == "posterior"))
 
     def _check_hirschberg(self):
         """Hirschberg splits pairs longer than hb_cutoff rows; this build implements the split
@@ -404,10 +405,15 @@ class SeqPairBatch:
         gm = _GRAD[self._grad_mode]
         if gm == 2:
             tot = self._run(2)
-            # the guide is deferred: computed on first use under the params scored now
-            # ("eager") or under those current at that use ("lazy")
-            self._guides_pending = self._params.copy() if self._soft_guide == "eager" else _CURRENT
-            self._have_guides = False
+            if self._soft_guide == "posterior":
+                # the forward-backward left every pair's posterior guide
+                self._guides_pending = None
+                self._have_guides = True
+            else:
+                # the guide is deferred: computed on first use under the params scored now
+                # ("eager") or under those current at that use ("lazy")
+                self._guides_pending = self._params.copy() if self._soft_guide == "eager" else _CURRENT
+                self._have_guides = False
             self._guides = None
             self._paths = False
         else:
@@ -726,17 +732,18 @@ class SeqPairBatch:
         """When soft pairs compute their guide path (the Viterbi path banded_grad() bands
         around): "eager" (default) under the params score_and_grad() ran with, computed on
         first use from a snapshot of them; "lazy" under the params current at first use
-        (after set_params() it follows the new params).  "posterior" (the forward-backward's
-        per-row column of greatest posterior mass) is not built here."""
+        (after set_params() it follows the new params).  "posterior": the forward-backward's own
+        guide -- per row the column of greatest exit mass, made non-decreasing -- left by
+        score_and_grad() itself (full DP, untracked batches)."""
         return self._soft_guide
 
     @soft_guide.setter
     def soft_guide(self, v):
         if v not in ("eager", "lazy", "posterior"):
             raise ValueError(f"nwgrad: unknown soft_guide \"{v}\" (expected \"eager\", \"lazy\" or \"posterior\")")
-        if v == "posterior":
-            raise NotImplementedError("nwgrad_b200: soft_guide=\"posterior\" is not available in this build; "
-                                      "use \"eager\" or \"lazy\"")
+        if v == "posterior" and self._tracked:
+            raise NotImplementedError("nwgrad_b200: soft_guide=\"posterior\" is built for untracked batches; "
+                                      "use \"eager\" or \"lazy\" with tracks")
         self._soft_guide = v
 
     @property

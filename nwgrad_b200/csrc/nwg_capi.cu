@@ -975,6 +975,7 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
         for (int32_t p : *subset) {
             const int m = int(s->oa[p + 1] - s->oa[p]), nb = int(s->ob[p + 1] - s->ob[p]);
             const Geo g = J.band >= 0 ? Geo{32, 4, true}
+                        : J.soft_post ? Geo{32, 4}
                         : pick_geo(true, m + 1, nb, J.lanes, J.rows, lane_ok);
             auto key = std::make_tuple(g.G, g.R, size_class(m + 1, nb));
             auto itb = idx.find(key);
@@ -1000,7 +1001,8 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
         build_plan(s, *P, true, 32, 4, sizeof(T), true);
     } else {
         P = &s->soft_plan;
-        build_plan(s, *P, true, J.lanes, J.rows, sizeof(T));
+        // posterior guides: every pair at 32 x 4, one warp (the POST kernels)
+        build_plan(s, *P, true, J.soft_post ? 32 : J.lanes, J.soft_post ? 4 : J.rows, sizeof(T));
     }
     DBuf sub_order;
     struct Free1 { DBuf& a; cudaStream_t st; ~Free1() { a.release(st); } } fr1{sub_order, st};
@@ -1019,7 +1021,9 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
     int64_t scratch_total = 0;
     for (auto& B : P->buckets) {
         if (B.pairs.empty()) continue;
-        SoftFn fn = soft_fn_rt<T>(aff, (J.mode == 2 && J.free_ends) ? 2 : (loc ? 1 : 0), tr, B.geo);
+        Geo gk = B.geo;
+        gk.post = J.soft_post != 0;
+        SoftFn fn = soft_fn_rt<T>(aff, (J.mode == 2 && J.free_ends) ? 2 : (loc ? 1 : 0), tr, gk);
         if (!fn) throw Error(NWG_EINVAL, "no soft kernel for this geometry");
         const int G = B.geo.G;
         const bool mw = B.geo.mw > 1;            // several warps per pair (long pairs)
@@ -1080,6 +1084,7 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
         A.status = s->status.as<int32_t>();
         A.spin_limit = s->spin_limit;
         A.queue = s->queue(int(launches.size()), st);
+        A.post = J.soft_post ? s->guide.as<int32_t>() : nullptr;
         if (ovf) {
             // a weight overflows T: every pair of this bucket is out of range in T
             mark_status_kernel<<<unsigned((items + 255) / 256), 256, 0, st>>>(A.order, items, A.status,
@@ -1360,7 +1365,11 @@ int nwg_run(nwg_store* s, const nwg_job* job, void* stream, double* total) {
         NWG_CUDA(cudaEventRecord(s->ev0, st));
         s->have_scores = s->have_grads = s->have_paths = false;
         if (J.grad_mode == 2) {
+            if (J.soft_post && (J.band >= 0 || s->tracked()))
+                throw Error(NWG_EINVAL, "posterior guides: full DP, untracked batches");
+            if (J.soft_post) s->guide.need(size_t(s->total_a + s->n) * 4 + 4, st);
             run_soft(s, J, st);
+            if (J.soft_post) s->have_guides = true;
         } else {
             const bool grad = J.grad_mode == 1;
             if (J.precision == 32) run_hard<float>(s, J, st, grad, true);

@@ -70,6 +70,7 @@ struct SoftArgs {
     int32_t* status;                         // per pair: 0 ok, else kSoft* bits (why it was refused)
     int spin_limit;                          // several warps per pair: polls before a wait gives up
     int* queue;                              // this launch's work-queue counters (2 ints, zero at launch)
+    int32_t* post;                           // POST kernels: per pair m + 1 posterior guide columns at oa[p] + p
 };
 
 // Per-pair status bits of a soft pass: a refused pair's score and counts are not written and
@@ -237,8 +238,15 @@ constexpr int kPrefetchSteps = NWG_SOFT_PREFETCH_STEPS;
 // outside [jlo(i), jhi(i)], Global border cells past border_rows / border_cols, backward cells
 // outside [jlo0(i), jhi0(i)]; Local log Z sums the band only.  Zero cells neither receive nor
 // pass on probability, which is what the reference's band-limited tables compute.
-template <class T, bool AFF, bool LOC, bool TR, int G, int R, bool MW = false, bool BAND = false, bool SG = false>
-__global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2 : 4) : 1))) soft_kernel(const SoftArgs A) {
+// POST: soft_guide="posterior" (aligner.hpp:6776-6808, 1466-1475): the backward pass also keeps,
+// per row, the column of greatest exit mass -- the cell's posterior less the posterior of moving
+// on to (i, j+1) within the row (affine: the Y posterior there; linear: F e_a B(i, j+1)), the
+// first such column on ties -- and the pair's guide is their running maximum over the rows.
+template <class T, bool AFF, bool LOC, bool TR, int G, int R, bool MW = false, bool BAND = false, bool SG = false,
+          bool POST = false>
+__global__ void __launch_bounds__(MW ? 512 : 128, (POST ? 3 : MW ? 1 : (G > 1 ? (R >= 8 ? 2 : 4) : 1)))
+soft_kernel(const SoftArgs A) {
+    static_assert(!POST || (G == 32 && R == 4 && !MW && !BAND && !TR), "posterior guides: 32 x 4, untracked, full DP");
     static_assert(!MW || (G == 32 && !TR), "several warps per pair: 32 lanes, untracked");
     static_assert(!BAND || (G == 32 && !MW), "banded: 32 lanes, one warp per pair");
     static_assert(!SG || !LOC, "semi-global ends: Global kernels");
@@ -795,6 +803,12 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
             int EB = (LOC || holds_m || (sg_ec && i0 <= m)) ? 0 : kEmpty;
             T lone = pow2s<T>(-EB);
             T sgb_o = T(0), sga_o = T(0), sgb_x = T(0), sga_x = T(0);   // untracked: this stripe's gap sums
+            // POST: per row the best exit mass so far (columns n down to j), its column, and the
+            // Y posterior of the column to the right
+            T pbest[POST ? R : 1], pyr[POST ? R : 1];
+            int pcol[POST ? R : 1];
+#pragma unroll
+            for (int r = 0; r < (POST ? R : 1); ++r) { pbest[r] = T(-1); pyr[r] = T(0); pcol[r] = 0; }
             T dgM = T(0);                             // row below, column j+1 (BM only)
             // Global affine: the seed B = 1 at (m, n) enters every state through the diagonal
             // term, as B_M(m+1, n+1) = 1 with the padding weight w[K*N][N] = 1 (the cell and
@@ -951,11 +965,16 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                         T nM, nX, nY;
                         if constexpr (AFF) {
                             const T fx = f[NV * r + 1], fy = f[NV * r + 2];
-                            T dX = noX ? T(0) : xX;                    // BX(i+1, j)
-                            T rY = ((LOC || sg_r0) && r == 0 && i == 0) ? T(0) : bY[r];     // BY(i, j+1)
-                            nM = fmaf_t(o_a, rY, fmaf_t(o_b, dX, D));
-                            nX = fmaf_t(o_a, rY, fmaf_t(e_b, dX, D));
-                            nY = fmaf_t(e_a, rY, fmaf_t(o_b, dX, D));
+                            // B keeps the gap moves into a free start's border cells (down column
+                            // 0, along row 0) that the forward pass never takes, as the reference's
+                            // backward does (they carry no forward mass, but the posterior guide
+                            // reads those cells' B); the counts leave them out (aligner.hpp:6309-6319)
+                            const T dXb = xX, rYb = bY[r];              // BX(i+1, j), BY(i, j+1)
+                            const T dX = noX ? T(0) : dXb;
+                            const T rY = ((LOC || sg_r0) && r == 0 && i == 0) ? T(0) : rYb;
+                            nM = fmaf_t(o_a, rYb, fmaf_t(o_b, dXb, D));
+                            nX = fmaf_t(o_a, rYb, fmaf_t(e_b, dXb, D));
+                            nY = fmaf_t(e_a, rYb, fmaf_t(o_b, dXb, D));
                             if constexpr (LOC) {
                                 nM = fmaf_t(vmask[r], lone, nM);
                                 nX = fmaf_t(vmask[r], lone, nX);
@@ -982,9 +1001,10 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                                 so_a = fmaf_t(fmx, rY, so_a); sx_a = fmaf_t(fy, rY, sx_a);
                             }
                         } else {
-                            T dX = noX ? T(0) : xM;
-                            T rY = ((LOC || sg_r0) && r == 0 && i == 0) ? T(0) : bM[r];
-                            nM = fmaf_t(e_a, rY, fmaf_t(e_b, dX, D));
+                            const T dXb = xM, rYb = bM[r];              // as in the affine case
+                            const T dX = noX ? T(0) : dXb;
+                            const T rY = ((LOC || sg_r0) && r == 0 && i == 0) ? T(0) : rYb;
+                            nM = fmaf_t(e_a, rYb, fmaf_t(e_b, dXb, D));
                             if constexpr (LOC) nM = fmaf_t(vmask[r], lone, nM);
                             else if (i == m && j == n) nM = lone;
                             else if (zsg) {
@@ -1006,6 +1026,19 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                             if (j < bblo0[r] || j > bbhi[r]) { nM = T(0); nX = T(0); nY = T(0); }
                         }
                         if constexpr (kCount) SB += AFF ? (nM + nX) + nY : nM;
+                        if constexpr (POST) {
+                            // scanning columns downwards, >= keeps the first (smallest) column of the max
+                            T ex;
+                            if constexpr (AFF) {
+                                const T cp = fmaf_t(f[NV * r], nM, fmaf_t(f[NV * r + 1], nX, f[NV * r + 2] * nY)) * fac;
+                                ex = cp - pyr[r];
+                                pyr[r] = f[NV * r + 2] * nY * fac;
+                            } else {
+                                const T e_a = ea0;
+                                ex = f[NV * r] * (nM - e_a * bM[r]) * fac;
+                            }
+                            if (ex >= pbest[r]) { pbest[r] = ex; pcol[r] = j; }
+                        }
                         dM = bM[r];
                         bM[r] = nM; bX[r] = nX; bY[r] = nY;
                         xM = nM; xX = nX; xY = nY;
@@ -1109,6 +1142,11 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                 }
             }
             if constexpr (MW) publish(bkey * SP + S);
+            if constexpr (POST) {   // this stripe's rows are complete: their columns
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    if (i0 + r <= m) A.post[ao + p + i0 + r] = pcol[r];
+            }
             if constexpr (!TR) {   // the stripe's gap sums into the pair's (double)
                 gb_o += static_cast<double>(sgb_o); ga_o += static_cast<double>(sga_o);
                 gb_x += static_cast<double>(sgb_x); ga_x += static_cast<double>(sga_x);
@@ -1147,6 +1185,15 @@ __global__ void __launch_bounds__(MW ? 512 : 128, (MW ? 1 : (G > 1 ? (R >= 8 ? 2
                 }
                 __syncwarp(gmask);
             }
+        }
+        if constexpr (POST) {   // the rows' columns as a guide: non-decreasing, in [0, n]
+            __syncwarp(gmask);
+            if (lane == 0) {
+                int32_t* gp = A.post + ao + p;
+                int run = 0;
+                for (int i = 0; i <= m; ++i) { run = max(run, min(max(gp[i], 0), n)); gp[i] = run; }
+            }
+            __syncwarp(gmask);
         }
         if constexpr (kCount) {
             // the group's lost-mass charge (every lane's, in any order: a bound, not a result)

@@ -9,6 +9,13 @@ namespace {
 // kernels test no end flag per cell
 template <class T, bool AFF, bool LOC, bool TR, bool SG = false>
 SoftFn pick(Geo g) {
+    if (g.post) {
+        if constexpr (!TR) {
+            if (g.G == 32 && g.R == 4 && !g.band && g.mw <= 1)
+                return &soft_kernel<T, AFF, LOC, false, 32, 4, false, false, SG, true>;
+        }
+        return nullptr;
+    }
     if (g.band) return (g.G == 32 && g.R == 4 && g.mw <= 1) ? &soft_kernel<T, AFF, LOC, TR, 32, 4, false, true, SG> : nullptr;
     if constexpr (!TR) {
         if (g.mw > 1) return (g.G == 32 && g.R == 4) ? &soft_kernel<T, AFF, LOC, false, 32, 4, true, false, SG> : nullptr;

@@ -1,9 +1,11 @@
 """soft_guide: when a soft batch computes the guide that banded_grad() bands around.
-"eager" takes the params score_and_grad() ran with, "lazy" those current at first use."""
+"eager" takes the params score_and_grad() ran with, "lazy" those current at first use,
+"posterior" the forward-backward's own per-row guide."""
 import numpy as np
 import pytest
 
-from conftest import AA, has_gpu, mutate, rand_matrix, rand_seqs
+import oracle
+from conftest import AA, encode, has_gpu, mutate, rand_matrix, rand_seqs
 
 pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not has_gpu(), reason="needs a CUDA GPU")]
 
@@ -37,8 +39,57 @@ def test_eager_and_lazy_guides():
     assert np.array_equal(out["eager"], gp)
     assert np.array_equal(out["lazy"], gq)
     b = nw.SeqPairBatch(sa, sb, p, grad_mode="soft")
-    with pytest.raises(NotImplementedError):
-        b.soft_guide = "posterior"
     with pytest.raises(ValueError, match="unknown soft_guide"):
         b.soft_guide = "viterbi"
     assert b.soft_guide == "eager"
+
+
+@pytest.mark.parametrize("gm", [0, 1])
+@pytest.mark.parametrize("mode", ["global", "local", "glocal", "overlap"])
+def test_posterior_guides_match_the_reference(gm, mode):
+    """soft_guide="posterior": the guides score_and_grad() leaves (per row the column of
+    greatest exit mass, made non-decreasing; aligner.hpp:6776-6808, 1466-1475) against the
+    reference engine's (tests/golden/posterior.npz).  Near-ties of exit mass can break either
+    way in a different arithmetic: double agrees on >= 99 % of rows, float32 on >= 95 % (the
+    reference's own float32-vs-double bar, test_soft_float32.py); the scores to 1e-4 / 1e-9."""
+    import os
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "posterior.npz"))
+    am, fe = {"global": (0, 12), "local": (1, 12), "glocal": (2, 12), "overlap": (2, 15)}[mode]
+    for N in (4, 20):
+        key = f"N{N}_"
+        alpha = str(z[key + "alpha"])
+        sa, sb = [str(s) for s in z[key + "sa"]], [str(s) for s in z[key + "sb"]]
+        params = nw.AlignParams.from_arrays(z[key + "mat"], z[key + "gaps"], alphabet=alpha)
+        for T in (1.0, 0.5):
+            pre = f"{key}g{gm}_m{am}_e{fe}_T{T}_"
+            want = z[pre + "guides"]
+            for cls, bar, tol in ((nw.SeqPairBatchDouble, 0.99, 1e-9), (nw.SeqPairBatch, 0.95, 1e-4)):
+                b = cls(sa, sb, params, gap_model=("linear", "affine")[gm], mode=mode, grad_mode="soft")
+                b.soft_guide = "posterior"
+                b.soft_temperature = T
+                b.score_and_grad()
+                np.testing.assert_allclose(b.scores(), z[pre + "scores"], rtol=tol, atol=tol)
+                got = np.asarray(b.guides())
+                n = got.size
+                assert (got == want[:n]).mean() >= bar, (cls.__name__, T, (got == want[:n]).mean())
+
+
+def test_banded_after_posterior_guide():
+    """banded_grad() around the posterior guides a soft pass left (no Viterbi run), against the
+    oracle's banded forward-backward around the same guides."""
+    rng = np.random.default_rng(61)
+    mat = rng.normal(0, 1.5, size=(1, 20, 20))
+    gaps = np.array([[2.0, 0.5, 2.5, 0.5]])
+    sa = rand_seqs(rng, 20, 40, 200, AA)
+    sb = [mutate(rng, s, AA) for s in sa]
+    b = nw.SeqPairBatchDouble(sa, sb, nw.AlignParams.from_arrays(mat, gaps, alphabet=AA), grad_mode="soft")
+    b.soft_guide = "posterior"
+    b.score_and_grad()
+    guides = np.asarray(b.guides()).astype(np.int32)
+    b.banded_grad(8)
+    enc = oracle.Encoded(encode(AA, sa), encode(AA, sb))
+    so, go = oracle.soft(1, 0, mat, gaps, enc, guides_in=guides, band=8)
+    np.testing.assert_allclose(b.scores(), so, rtol=1e-9, atol=1e-9)
+    gmat, ggap = b.grads()
+    flat = np.concatenate([gmat.reshape(len(sa), -1), ggap.reshape(len(sa), -1)], axis=1)
+    np.testing.assert_allclose(flat, go, rtol=1e-8, atol=1e-8)
