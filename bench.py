@@ -421,6 +421,8 @@ def main():
     ap.add_argument("--pairs", type=int, default=100000, help="pairs per batch (positives; as many decoys)")
     ap.add_argument("--cpu-sample", type=int, default=4000, help="pairs per batch in the CPU-baseline sample")
     ap.add_argument("--lmax", type=int, default=500, help="longest A (profiling cases; the workload is 100-500)")
+    ap.add_argument("--scratch-gb", type=float, default=-1,
+                    help="soft scratch budget per batch in GiB (default: the library's, from free memory)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-fill arm")
@@ -500,6 +502,9 @@ def main():
     if args.checkpoint_mb >= 0:
         for b in (pos, neg):
             b.set_memory(checkpoint_bytes=int(args.checkpoint_mb * (1 << 20)))
+    if args.scratch_gb > 0:
+        for b in (pos, neg):
+            b.set_memory(scratch_budget_bytes=int(args.scratch_gb * (1 << 30)))
     tune_table = {}
     if args.geometry:
         geo = tuple(int(x) for x in args.geometry.lower().split("x"))

@@ -376,6 +376,8 @@ struct nwg_store {
     std::map<std::pair<int, int>, std::vector<GeoCost>> geo_costs;
     bool plain = false;
     int64_t scratch_budget = -1;   // bytes of soft scratch one call may hold (-1: from the device's memory)
+    int64_t auto_budget = -1;      // that budget as first computed for this store, kept so later calls
+                                   // decide concurrency (and scratch size) the same way
     int64_t ck_threshold = int64_t(16) << 20;     // soft: forward tables above this are checkpointed
     int spin_limit = nwg::kSpinLimit;             // several warps per pair: polls before a wait gives up
     // work-queue counters, two ints per launch of a call (soft launches from 0, hard fills from
@@ -522,6 +524,7 @@ void run_launches(nwg_store* s, GraphCache* gc, const std::vector<Launch>& L, cu
 // memory plus the scratch this store already holds), at least 24 GiB.
 int64_t scratch_budget_of(nwg_store* s) {
     if (s->scratch_budget >= 0) return s->scratch_budget;
+    if (s->auto_budget >= 0) return s->auto_budget;
     size_t fr = 0, tot = 0;
     cudaMemGetInfo(&fr, &tot);
     // blocks the pool keeps from earlier batches are free for this one too (the device's free
@@ -534,7 +537,8 @@ int64_t scratch_budget_of(nwg_store* s) {
         cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used);
     }
     const double idle = reserved > used ? double(reserved - used) : 0.0;
-    return std::max<int64_t>(int64_t(24) << 30, int64_t(0.6 * (double(fr) + idle + double(s->scratch.bytes))));
+    s->auto_budget = std::max<int64_t>(int64_t(24) << 30, int64_t(0.6 * (double(fr) + idle + double(s->scratch.bytes))));
+    return s->auto_budget;
 }
 
 void set_params_dev(nwg_store* s) {
@@ -1301,6 +1305,7 @@ int nwg_store_destroy(nwg_store* s) {
         if (!s) return;
         cudaSetDevice(s->device);
         s->hard_plan.reset(); s->soft_plan.reset(); s->band_plan.reset(); s->soft_band_plan.reset();
+        s->auto_budget = -1;   // a new batch: the budget from the memory free now
         for (DBuf* b : {&s->a, &s->b, &s->doa, &s->dob, &s->tracks, &s->gtracks, &s->matf, &s->gapf, &s->matd,
                         &s->gapd, &s->bx0f, &s->bx0d, &s->score, &s->end, &s->grad, &s->guide, &s->status,
                         &s->stripe_tab, &s->codes, &s->scratch, &s->part, &s->red, &s->moves,
