@@ -731,8 +731,8 @@ def _timed_run(fn, reps=1):
 
 
 def bench_c4(args):
-    """Side measurement: long pairs (log-uniform 5k-36k).  Hard gradient by Pointers (several
-    warps per pair) and by Hirschberg (float32 prefix-max carry and float64 exact carry), soft
+    """Side measurement: long pairs (log-uniform 5k-36k).  Hard gradient by Pointers (tiles of
+    256 x 256 cells, a launch per anti-diagonal of tiles) and by Hirschberg (float32 prefix-max carry and float64 exact carry), soft
     gradient (several warps per pair, stripe checkpoints), then banded re-alignment (bandwidth
     64) after a 1e-3 parameter step.  GCUPS per stage from wall time around each call."""
     import nwgrad_b200 as nw

@@ -305,6 +305,7 @@ Geo pick_geo(bool soft, int rows, int n, int lanes, int rpl, bool lane_ok) {
 // pair's stripes) instead of one: a long pair is then not a single warp's serial work.  The
 // warps per pair grow with the pair's stripes (each warp keeps at least 3 stripes).
 constexpr int kLongRows = 1536;
+constexpr int kTileW = 256;   // columns per tile of a tiled long pair (a multiple of 8)
 int long_warps(int rows, int GR) {
     const int ns = (rows + GR - 1) / GR;
     return ns >= 64 ? 16 : ns >= 24 ? 8 : 4;
@@ -338,9 +339,19 @@ struct Plan {
     int64_t code_bytes = 0;
     int64_t n_stripes = 0;           // banded: stripes over all pairs
     DBuf order, dcode_off, stripe_base;
+    // hard, tiled long pairs: the tiles (p, s, c) of every tiled pair grouped by anti-diagonal
+    // s + c (diagonal d: items diag_off[d] .. diag_off[d + 1] - 1); per pair (by index) its row
+    // and column buffer offsets and first tile slot, in elements
+    std::vector<int32_t> tile_pairs;
+    std::vector<int64_t> diag_off;
+    int64_t tile_row_elems = 0, tile_col_elems = 0, n_tiles = 0;
+    DBuf tile_items, tile_rowoff, tile_coloff, tile_slot, tile_plist, tile_count;
     void reset() {
         order.release(); dcode_off.release(); stripe_base.release();
+        tile_items.release(); tile_rowoff.release(); tile_coloff.release(); tile_slot.release();
+        tile_plist.release(); tile_count.release();
         valid = false; buckets.clear(); code_off.clear(); code_bytes = 0; n_stripes = 0;
+        tile_pairs.clear(); diag_off.clear(); tile_row_elems = tile_col_elems = n_tiles = 0;
     }
 };
 
@@ -364,6 +375,7 @@ struct nwg_store {
     bool bx0f_ok = false, bx0d_ok = false;
     // results
     DBuf score, end, grad, guide, status, codes, scratch, part, red, moves, moves_off, path_info;
+    DBuf trow, tcol, tbest, tcell;      // tiled long pairs: stripe rows, tile columns, Local tile bests
     int64_t gstride = 0;
     bool have_scores = false, have_grads = false, have_guides = false, have_paths = false;
     int last_grad_mode = 0, last_gm = -1, last_am = -1, last_prec = 0;
@@ -609,7 +621,10 @@ void build_plan(nwg_store* s, Plan& P, bool soft, int lanes, int rpl, int elem_b
         if (!band && !lanes && !rpl) {
             if (s->plain) g = Geo{32, 4};
             else if (soft && !s->tracked() && rows >= kLongRows && nb >= 256) g = Geo{32, 4, false, long_warps(rows, 128)};
-            else if (!soft && !one_warp && rows >= kLongRows && nb >= 256) g = Geo{32, 8, false, long_warps(rows, 256)};
+            else if (!soft && !one_warp && rows >= kLongRows && nb >= 256)
+                // long pairs: untracked ones as tiles over the whole device, tracked ones with
+                // several warps per pair
+                g = s->tracked() ? Geo{32, 8, false, long_warps(rows, 256)} : Geo{32, 8, false, 0, false, true};
             else if (sc < kClasses && cost_of[sc]) {
                 double best = 1e300;
                 for (const auto& gc : *cost_of[sc]) {
@@ -622,7 +637,7 @@ void build_plan(nwg_store* s, Plan& P, bool soft, int lanes, int rpl, int elem_b
             }
         }
         // the bucket of (geometry, size class): few buckets, a linear search
-        const int k1 = g.G, k2 = g.R * 100 + g.mw, k3 = sc;
+        const int k1 = g.G, k2 = g.R * 100 + g.mw + (g.tile ? 50 : 0), k3 = sc;
         int bi = -1;
         for (int q = 0; q < int(bkeys.size()); ++q)
             if (bkeys[q][0] == k1 && bkeys[q][1] == k2 && bkeys[q][2] == k3) { bi = q; break; }
@@ -671,6 +686,49 @@ void build_plan(nwg_store* s, Plan& P, bool soft, int lanes, int rpl, int elem_b
                 off += (bytes + 15) & ~int64_t(15);
             }
         P.code_bytes = std::max<int64_t>(off, 16);
+        // tiled pairs: stripes of G R rows x tiles of kTileW columns; the tile (s, c) needs
+        // (s - 1, c) and (s, c - 1), both on the diagonal before its own
+        std::vector<int64_t> roff(size_t(n) + 1, 0), coff(size_t(n) + 1, 0), toff(size_t(n) + 1, 0);
+        std::vector<int32_t> tcount;
+        std::vector<std::vector<int32_t>> diags;
+        for (auto& B : P.buckets) {
+            if (!B.geo.tile) continue;
+            const int GR = B.geo.G * B.geo.R;
+            for (int32_t p : B.pairs) {
+                const int m = int(s->oa[p + 1] - s->oa[p]), nb = int(s->ob[p + 1] - s->ob[p]);
+                const int ns = (m + GR - 1) / GR, nt = (nb + kTileW - 1) / kTileW;
+                roff[p] = P.tile_row_elems; P.tile_row_elems += int64_t(ns) * 3 * (nb + 1);
+                coff[p] = P.tile_col_elems; P.tile_col_elems += int64_t(ns) * nt * 3 * GR;
+                toff[p] = P.n_tiles; P.n_tiles += int64_t(ns) * nt;
+                P.tile_pairs.push_back(p);
+                tcount.push_back(ns * nt);
+                if (int(diags.size()) < ns + nt - 1) diags.resize(size_t(ns + nt - 1));
+                for (int st = 0; st < ns; ++st)
+                    for (int c = 0; c < nt; ++c) {
+                        auto& dv = diags[size_t(st + c)];
+                        dv.push_back(p); dv.push_back(st); dv.push_back(c);
+                    }
+            }
+        }
+        if (!P.tile_pairs.empty()) {
+            std::vector<int32_t> items;
+            items.reserve(size_t(P.n_tiles) * 3);
+            P.diag_off.assign(1, 0);
+            for (auto& dv : diags) {
+                items.insert(items.end(), dv.begin(), dv.end());
+                P.diag_off.push_back(int64_t(items.size() / 3));
+            }
+            auto up = [](DBuf& d, const void* h, size_t bytes) {
+                d.need(bytes);
+                NWG_CUDA(cudaMemcpy(d.p, h, bytes, cudaMemcpyHostToDevice));
+            };
+            up(P.tile_items, items.data(), items.size() * 4);
+            up(P.tile_rowoff, roff.data(), roff.size() * 8);
+            up(P.tile_coloff, coff.data(), coff.size() * 8);
+            up(P.tile_slot, toff.data(), toff.size() * 8);
+            up(P.tile_plist, P.tile_pairs.data(), P.tile_pairs.size() * 4);
+            up(P.tile_count, tcount.data(), tcount.size() * 4);
+        }
     }
     P.n_planned = int64_t(order.size());
     P.order.need(size_t(std::max<int64_t>(n, 1)) * 4);
@@ -736,7 +794,9 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
         const int gpb = 128 / B.geo.G;
         const int64_t items = int64_t(B.pairs.size());
         const int64_t row = 3 * (int64_t(B.maxn) + 1);
-        if (B.geo.mw > 1) {
+        if (B.geo.tile) {   // tiles: per-pair row and column buffers instead of scratch
+            blocks = 0; slots = 0; stride = 0;
+        } else if (B.geo.mw > 1) {
             const int GR = B.geo.G * B.geo.R;
             int64_t ns = 0;
             for (int32_t p : B.pairs) ns = std::max<int64_t>(ns, (s->oa[p + 1] - s->oa[p] + GR - 1) / GR);
@@ -750,7 +810,7 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
         }
     };
     int64_t max_total = 1, sum_total = 0;
-    bool any_mw = false;
+    bool any_mw = false, any_tile = false;
     int nbk = 0;
     for (auto& B : P.buckets) {
         if (B.pairs.empty()) continue;
@@ -759,17 +819,21 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
         max_total = std::max(max_total, sl * sd);
         sum_total += (sl * sd * int64_t(sizeof(T)) + 255) & ~int64_t(255);
         any_mw |= B.geo.mw > 1;
+        any_tile |= B.geo.tile;
         ++nbk;
     }
+    // several warps per pair and tiles: the fills first, then one walk over every pair
+    const bool sep_walk = any_mw || any_tile;
     // the buckets' fills and walks run at once (bucket k's walk after its fill, each bucket on
     // its own stream and scratch part) when nothing needs a host check between fill and walk
-    const bool concurrent = !any_mw && nbk > 1 && sum_total <= scratch_budget_of(s);
+    const bool concurrent = !sep_walk && nbk > 1 && sum_total <= scratch_budget_of(s);
     s->scratch.need(concurrent ? size_t(sum_total) : size_t(max_total) * sizeof(T), st);
     std::vector<Launch> fills;
     std::vector<nwg::HardArgs> fill_args;
     int64_t soff_b = 0;
+    int nq = 0;   // work-queue counters used
     for (auto& B : P.buckets) {
-        if (B.pairs.empty()) continue;
+        if (B.pairs.empty() || B.geo.tile) continue;
         HardFn fn = hard_fn_rt<T>(aff, ends ? 2 : (loc ? 1 : 0), tr, B.geo);
         if (!fn) throw Error(NWG_EINVAL, "no kernel for this geometry");
         const int hblock = B.geo.mw > 1 ? 32 * B.geo.mw : 128;
@@ -798,9 +862,57 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
         A.score = s->score.as<double>(); A.end = s->end.as<int32_t>();
         A.ends = ends;
         A.spin_limit = s->spin_limit;
-        A.queue = s->queue(nwg_store::kQueueHard + int(fills.size()), st);
+        A.queue = s->queue(nwg_store::kQueueHard + nq++, st);
         fills.push_back(make_launch(reinterpret_cast<const void*>(fn), unsigned(blocks), hblock, smem, A));
         fill_args.push_back(A);
+    }
+    if (any_tile) {
+        // tiled long pairs: a launch per anti-diagonal of tiles over every tiled pair, each tile
+        // one warp's item from the launch's work queue; the launches run in order on one stream,
+        // so they share one queue (each leaves it at zero)
+        const Geo tg{32, 8, false, 0, false, true};
+        HardFn fn = hard_fn_rt<T>(aff, loc ? 1 : 0, tr, tg);
+        if (!fn) throw Error(NWG_EINVAL, "no kernel for this geometry");
+        NWG_CUDA(nwg::allow_smem(reinterpret_cast<const void*>(fn), smem_base));
+        s->trow.need(size_t(std::max<int64_t>(P.tile_row_elems, 1)) * sizeof(T), st);
+        s->tcol.need(size_t(std::max<int64_t>(P.tile_col_elems, 1)) * sizeof(T), st);
+        if (loc) {
+            s->tbest.need(size_t(std::max<int64_t>(P.n_tiles, 1)) * sizeof(T), st);
+            s->tcell.need(size_t(std::max<int64_t>(P.n_tiles, 1)) * 12, st);
+        }
+        nwg::HardArgs A{};
+        A.a = s->a.as<uint8_t>(); A.oa = s->doa.as<int64_t>();
+        A.b = s->b.as<uint8_t>(); A.ob = s->dob.as<int64_t>();
+        A.tracks = tr ? s->tracks.as<uint16_t>() : nullptr;
+        A.gtracks = tr ? s->gtracks.as<uint16_t>() : nullptr;
+        A.bx0 = bx0;
+        A.mat = matT.p; A.gaps = gapT.p; A.N = s->N; A.K = s->K;
+        A.codes = s->codes.as<uint8_t>(); A.code_off = P.dcode_off.as<int64_t>();
+        A.scratch = s->trow.p; A.scratch_stride = 0;
+        A.score = s->score.as<double>(); A.end = s->end.as<int32_t>();
+        A.spin_limit = s->spin_limit;
+        A.queue = s->queue(nwg_store::kQueueHard + nq++, st);
+        A.tile_w = kTileW;
+        A.rowbuf = s->trow.p; A.rowbuf_off = P.tile_rowoff.as<int64_t>();
+        A.colbuf = s->tcol.p; A.colbuf_off = P.tile_coloff.as<int64_t>();
+        A.tbest = loc ? s->tbest.p : nullptr; A.tcell = loc ? s->tcell.as<int32_t>() : nullptr;
+        A.tile_off = P.tile_slot.as<int64_t>();
+        for (size_t d = 0; d + 1 < P.diag_off.size(); ++d) {
+            const int64_t cnt = P.diag_off[d + 1] - P.diag_off[d];
+            A.tiles = P.tile_items.as<int32_t>() + 3 * P.diag_off[d];
+            A.n_items = cnt;
+            const int64_t blocks = std::min<int64_t>((cnt + 3) / 4, int64_t(sms) * 16);
+            fills.push_back(make_launch(reinterpret_cast<const void*>(fn), unsigned(blocks), 128, smem_base, A));
+        }
+        if (loc) {
+            nwg::TileBestArgs TB{};
+            TB.pairs = P.tile_plist.as<int32_t>(); TB.n_pairs = int64_t(P.tile_pairs.size());
+            TB.tile_off = P.tile_slot.as<int64_t>(); TB.tiles_of = P.tile_count.as<int32_t>();
+            TB.tbest = s->tbest.p; TB.tcell = s->tcell.as<int32_t>();
+            TB.score = s->score.as<double>(); TB.end = s->end.as<int32_t>(); TB.layout = (32 << 8) | 8;
+            fills.push_back(make_launch(reinterpret_cast<const void*>(&nwg::tile_best_kernel<T>),
+                                        unsigned((TB.n_pairs + 127) / 128), 128, 0, TB));
+        }
     }
     // traceback buffers: gradient, guide, path
     if (want_grad) {
@@ -840,7 +952,7 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
     // which the host checks between the fills and a separate walk; otherwise the fills walk
     // their own pairs, one captured sequence
     GraphCache* gc = band ? &s->g_hard_band : &s->g_hard[sizeof(T) == 4 ? 0 : 1];
-    if (!any_mw) {
+    if (!sep_walk) {
         // a warp per pair: the fill walks its own pairs (the codes still in L2); a lane per pair
         // (many short pairs): a walk launch over the bucket's pairs after its fill.  The buckets
         // run at once when their scratch parts fit.
@@ -880,7 +992,7 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
                         throw Error(NWG_ECUDA, "nwgrad_b200: hard fill: a wait between the warps of pair " +
                                                    std::to_string(p) + " ran out (the kernel gave up instead of hanging)");
     }
-    if (any_mw && P.n_planned) run_launches(s, nullptr, std::vector<Launch>{walk}, st);
+    if (sep_walk && P.n_planned) run_launches(s, nullptr, std::vector<Launch>{walk}, st);
     if (!hb_pairs.empty()) {
         s->hb_pairs.need(hb_pairs.size() * 4, st);
         NWG_CUDA(cudaMemcpyAsync(s->hb_pairs.p, hb_pairs.data(), hb_pairs.size() * 4, cudaMemcpyHostToDevice, st));

@@ -59,6 +59,14 @@ struct HardArgs {
     int ends;
     int spin_limit;                            // several warps per pair: polls before a wait gives up
     int* queue;                                // this launch's work-queue counters (2 ints, zero at launch)
+    // tiled long pairs (TL kernels): an item is one tile -- stripe s of pair p over columns
+    // c W + 1 .. (c + 1) W -- and a launch holds one anti-diagonal (s + c) of every pair's tiles
+    const int32_t* tiles;                      // per item: p, s, c
+    int tile_w;                                // W, a multiple of 8
+    void* rowbuf; const int64_t* rowbuf_off;   // per pair, per stripe its bottom row: (n + 1) x 3 T
+    void* colbuf; const int64_t* colbuf_off;   // per pair, per stripe and tile its last column: G R x 3 T
+    void* tbest; int32_t* tcell;               // Local: per tile its first row-major best and cell (i, j, state)
+    const int64_t* tile_off;                   // per pair: its first tile's slot in tbest / tcell
 };
 
 // The band of DP row i around guide g (aligner.hpp:2644-2700): columns [jlo, jhi].
@@ -111,9 +119,14 @@ __host__ __device__ inline size_t hard_mw_smem_bytes(int warps, int tsize) {
 // state 3 and the host fails the call.
 
 // SG: the semi-global ends of A.ends (Global fills only, full DP, a warp or lane per pair)
-template <class T, bool AFF, bool LOC, bool TR, int G, int R, bool BAND = false, bool MW = false, bool SG = false>
+// TL: tiled long pairs (A.tiles): each item one stripe of one pair over one tile of columns; the
+// tile's top row comes from the stripe above (rowbuf), its left column from the tile to its left
+// (colbuf), and its codes go where the full fill would put them, so the walk reads them as usual
+template <class T, bool AFF, bool LOC, bool TR, int G, int R, bool BAND = false, bool MW = false, bool SG = false,
+          bool TL = false>
 __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArgs A) {
     static_assert(!MW || (G == 32 && !BAND), "several warps per pair: 32 lanes, full DP");
+    static_assert(!TL || (G == 32 && !BAND && !MW && !SG), "tiles: 32 lanes, full DP, Global or Local");
     static_assert(!SG || (!LOC && !MW), "semi-global ends: Global fills, one warp per pair");
     constexpr int GR = G * R;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -181,7 +194,8 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
             if (lane == 0) prog[gib] = -1;
             __syncthreads();
         }
-        const int p = A.order[it];
+        const int p = TL ? A.tiles[3 * it] : A.order[it];
+        const int ts = TL ? A.tiles[3 * it + 1] : 0, tc = TL ? A.tiles[3 * it + 2] : 0;   // TL: stripe, tile
         const int64_t ao = A.oa[p], bo = A.ob[p];
         const int m = int(A.oa[p + 1] - ao), n = int(A.ob[p + 1] - bo);
         const uint8_t* __restrict__ ap = A.a + ao;
@@ -239,7 +253,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
                 A.end[4 * p] = ei; A.end[4 * p + 1] = ej; A.end[4 * p + 2] = st;
                 A.end[4 * p + 3] = (G << 8) | R;
                 // an empty side: the walk runs the border (no codes read)
-                if (!MW && A.walk_fused) walk_pair(A.walk, p);
+                if (!MW && !TL && A.walk_fused) walk_pair(A.walk, p);
             }
             continue;
         }
@@ -254,7 +268,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
             bcols = bw.jhi(0);
         }
         int64_t soff = 0;                     // this stripe's code offset within the pair
-        int pmin = 1, pmax = 0;               // the previous stripe's columns
+        int pmin = 1, pmax = TL ? n : 0;      // the previous stripe's columns (TL: all of them)
 
         T bestv = T(0); int besti = 0, bestj = 0, bests = 0;   // Local: the first row-major max
         T endM = ninf<T>(), endX = ninf<T>(), endY = ninf<T>();
@@ -281,13 +295,19 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
 
         const int S_full = n + G - 1;          // MW: steps per stripe (full DP)
         const int SP = S_full + 1;             // MW: progress key per stripe
-        for (int s = MW ? gib : 0; s < nstripes; s += NWp) {
+        T* const rows_p = TL ? static_cast<T*>(A.rowbuf) + A.rowbuf_off[p] : nullptr;
+        T* const cols_p = TL ? static_cast<T*>(A.colbuf) + A.colbuf_off[p] : nullptr;
+        const int ntc = TL ? (n + A.tile_w - 1) / A.tile_w : 1;   // TL: tiles per stripe
+        for (int s = TL ? ts : (MW ? gib : 0); s < (TL ? ts + 1 : nstripes); s += NWp) {
             // the previous stripe's bottom row (read) and this stripe's (written)
-            T* const bnd = bnd0 + (MW ? int64_t(s - 1) * A.row_stride : 0);
-            T* const bnd_out = bnd0 + (MW ? int64_t(s) * A.row_stride : 0);
+            T* const bnd = TL ? rows_p + int64_t(s - 1) * 3 * (n + 1) : bnd0 + (MW ? int64_t(s - 1) * A.row_stride : 0);
+            T* const bnd_out = TL ? rows_p + int64_t(s) * 3 * (n + 1) : bnd0 + (MW ? int64_t(s) * A.row_stride : 0);
             const int i0 = s * GR + lane * R + 1;   // this lane's first DP row
-            // the stripe's columns [cmin, cmax]: the union of its rows' bands
-            int cmin = 1, cmax = n;
+            // the stripe's columns [cmin, cmax]: the union of its rows' bands (TL: the tile's)
+            int cmin = TL ? tc * A.tile_w + 1 : 1, cmax = TL ? min(n, (tc + 1) * A.tile_w) : n;
+            // TL: the column left of the tile, GR rows x 3 values, and this tile's last column
+            const T* const lcol = TL && tc > 0 ? cols_p + (int64_t(s) * ntc + tc - 1) * 3 * GR : nullptr;
+            T* const rcol = TL ? cols_p + (int64_t(s) * ntc + tc) * 3 * GR : nullptr;
             int rlo[BAND ? R : 1], rhi[BAND ? R : 1];
             if constexpr (BAND) {
                 int lo = n + 1, hi = 0;
@@ -329,9 +349,15 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
                     rp[r].gob = sgap[4 * ts + 2]; rp[r].geb = sgap[4 * ts + 3];
                 }
                 // the cell left of the stripe's first column: column 0's border, or out of band
+                // (TL: the tile to the left's last column, its own rows)
+                if constexpr (LOC) { rbest[r] = T(0); rbj[r] = 0; rbs[r] = 0; }
+                if (TL && cmin > 1) {
+                    const int q = lane * R + r;
+                    cM[r] = lcol[3 * q]; cX[r] = lcol[3 * q + 1]; cY[r] = lcol[3 * q + 2];
+                    continue;
+                }
                 if constexpr (LOC) {
                     cM[r] = cmin == 1 ? T(0) : ninf<T>(); cX[r] = ninf<T>();
-                    rbest[r] = T(0); rbj[r] = 0; rbs[r] = 0;
                 } else if (sg_c0 && cmin == 1) {
                     cM[r] = T(0); cX[r] = ninf<T>();   // column 0 a free start
                 } else {
@@ -368,10 +394,15 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
                     row0(cmin - 1, dgM, dgX, dgY);
                 } else if (lane == 0 && cmin - 1 >= pmin && cmin - 1 <= pmax) {
                     dgM = bnd[3 * (cmin - 1)]; dgX = bnd[3 * (cmin - 1) + 1]; dgY = bnd[3 * (cmin - 1) + 2];
+                } else if (TL && lane > 0) {   // the lane above's last row in the tile to the left
+                    const int q = lane * R - 1;
+                    dgM = lcol[3 * q]; dgX = lcol[3 * q + 1]; dgY = lcol[3 * q + 2];
                 } else { dgM = ninf<T>(); dgX = ninf<T>(); dgY = ninf<T>(); }
             }
             T upM = ninf<T>(), upX = ninf<T>(), upY = ninf<T>();
-            uint8_t* cs = codes + (BAND ? soff : int64_t(s) * S8 * GR);
+            // TL: the tile's steps start (cmin - 1) steps into the stripe's full-width codes
+            uint8_t* cs = TL ? codes + int64_t(s) * ((n + G - 1 + 7) & ~7) * GR + int64_t((cmin - 1) >> 3) * G * 8 * R
+                             : codes + (BAND ? soff : int64_t(s) * S8 * GR);
             // lane 0: the row above one column ahead, so the load is in flight meanwhile
             T nuM = ninf<T>(), nuX = ninf<T>(), nuY = ninf<T>();
             auto fetch_up = [&](int jj) {
@@ -495,12 +526,21 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
                 }
             }
             if constexpr (MW) publish(s * SP + S_full);
+            if constexpr (TL) {   // the tile's last column, for the tile to its right
+                if (tc + 1 < ntc) {
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        const int q = lane * R + r;
+                        rcol[3 * q] = cM[r]; rcol[3 * q + 1] = cX[r]; rcol[3 * q + 2] = cY[r];
+                    }
+                }
+            }
             pmin = cmin; pmax = cmax;
             soff += int64_t(S8) * GR;
             // the end cell (m, n): after the stripe each register holds column n (a banded
             // Global stripe holding row m always reaches column n)
             if constexpr (!LOC) {
-                if (m >= i0 && m < i0 + R) {
+                if (m >= i0 && m < i0 + R && (!TL || cmax == n)) {
 #pragma unroll
                     for (int r = 0; r < R; ++r)
                         if (i0 + r == m) { endM = cM[r]; endX = cX[r]; endY = cY[r]; }
@@ -599,7 +639,9 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
                     erow.st = __shfl_sync(gmask, erow.st, src, G);
                 }
             }
-            if (lane == 0 && (!MW || gib == (nstripes - 1) % NWp)) {
+            // TL: the tile holding (m, n) writes the pair's result
+            const bool tl_end = !TL || (ts == nstripes - 1 && min(n, (tc + 1) * A.tile_w) == n);
+            if (lane == 0 && tl_end && (!MW || gib == (nstripes - 1) % NWp)) {
                 T sc; int st, ei = m, ej = n;
                 if constexpr (AFF) {
                     sc = rmax3(endM, endX, endY);
@@ -616,11 +658,17 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
             }
             if constexpr (MW) __syncthreads();
         } else if (lane == 0) {
-            A.score[p] = static_cast<double>(bestv);
-            A.end[4 * p] = besti; A.end[4 * p + 1] = bestj; A.end[4 * p + 2] = bests;
-            A.end[4 * p + 3] = (G << 8) | R;
+            if constexpr (TL) {   // this tile's first row-major best; a later pass picks the pair's
+                const int64_t slot = A.tile_off[p] + int64_t(ts) * ntc + tc;
+                static_cast<T*>(A.tbest)[slot] = bestv;
+                A.tcell[3 * slot] = besti; A.tcell[3 * slot + 1] = bestj; A.tcell[3 * slot + 2] = bests;
+            } else {
+                A.score[p] = static_cast<double>(bestv);
+                A.end[4 * p] = besti; A.end[4 * p + 1] = bestj; A.end[4 * p + 2] = bests;
+                A.end[4 * p + 3] = (G << 8) | R;
+            }
         }
-        if constexpr (!MW) {
+        if constexpr (!MW && !TL) {
             // the traceback, while this pair's codes are still in L2: the group's codes and end
             // cell are visible to its lane 0 after the warp barrier; its other lanes go on with
             // their next pair's fill meanwhile
@@ -630,6 +678,35 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
             }
         }
     }
+}
+
+// TL, Local: each pair's best over its tiles -- the first row-major maximum (the largest value,
+// then the lowest row, then the lowest column; a tile's own best is its first) -- as the
+// pair's score and end cell.  One thread per pair.
+struct TileBestArgs {
+    const int32_t* pairs; int64_t n_pairs;   // the tiled pairs
+    const int64_t* tile_off;                 // per pair: its first tile's slot
+    const int32_t* tiles_of;                 // per listed pair: its tiles
+    const void* tbest; const int32_t* tcell;
+    double* score; int32_t* end; int layout;
+};
+template <class T>
+__global__ void tile_best_kernel(const TileBestArgs A) {
+    const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= A.n_pairs) return;
+    const int p = A.pairs[k];
+    const T* tbest = static_cast<const T*>(A.tbest);
+    T bv = T(0); int bi = 0, bj = 0, bs = 0;
+    for (int t = 0; t < A.tiles_of[k]; ++t) {
+        const int64_t q = A.tile_off[p] + t;
+        const T v = tbest[q];
+        const int vi = A.tcell[3 * q], vj = A.tcell[3 * q + 1];
+        if (v > bv || (v == bv && v > T(0) && (vi < bi || (vi == bi && vj < bj)))) {
+            bv = v; bi = vi; bj = vj; bs = A.tcell[3 * q + 2];
+        }
+    }
+    A.score[p] = static_cast<double>(bv);
+    A.end[4 * p] = bi; A.end[4 * p + 1] = bj; A.end[4 * p + 2] = bs; A.end[4 * p + 3] = A.layout;
 }
 
 }  // namespace nwg

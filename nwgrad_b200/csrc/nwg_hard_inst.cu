@@ -26,6 +26,7 @@ HardFn pick_sg(Geo g) {
 template <class T, bool AFF, bool LOC, bool TR>
 HardFn pick(Geo g) {
     if (g.band) return pick_band<T, AFF, LOC, TR>(g);
+    if (g.tile) return (g.G == 32 && g.R == 8) ? &hard_fill_kernel<T, AFF, LOC, TR, 32, 8, false, false, false, true> : nullptr;
     if (g.mw > 1) {   // several warps per pair
         if (g.G == 32 && g.R == 4) return &hard_fill_kernel<T, AFF, LOC, TR, 32, 4, false, true>;
         if (g.G == 32 && g.R == 8) return &hard_fill_kernel<T, AFF, LOC, TR, 32, 8, false, true>;

@@ -338,14 +338,49 @@ def test_soft_long_pairs_several_warps_per_pair(gm, am):
 @pytest.mark.parametrize("prec", [32, 64])
 @pytest.mark.parametrize("gm", [0, 1])
 @pytest.mark.parametrize("am", [0, 1])
-def test_hard_long_pairs_several_warps_per_pair(prec, gm, am):
-    """Pairs of 1,600+ rows fill with four warps per pair: bit for bit the oracle's
-    (scores, per-pair gradients, guides), with short pairs in the same batch."""
+def test_hard_long_pairs_tiles(prec, gm, am):
+    """Untracked pairs of 1,536+ rows and 256+ columns fill as tiles (256 rows x 256 columns,
+    a launch per anti-diagonal of tiles): bit for bit the oracle's (scores, per-pair
+    gradients, guides), with short pairs in the same batch and ragged last tiles (B of 256,
+    257, 511, 513 and 1,000+ residues; A of 1,536 rows exactly, one stripe of 256 rows more
+    than a multiple, and longer)."""
     rng = np.random.default_rng(1700 + prec + gm + 2 * am)
     mat, gaps, sa, sb, tr, gt = _problem(rng, AA, 8, 1, 150, integer=(gm == 1), homolog=True)
     sa += rand_seqs(rng, 3, 1600, 2600, AA)
     sb += [mutate(rng, s, AA) for s in sa[-3:]]
+    for la, lb in ((1536, 256), (1537, 257), (1800, 511), (2049, 513), (1600, 2900)):
+        sa += rand_seqs(rng, 1, la, la, AA)
+        sb += rand_seqs(rng, 1, lb, lb, AA)
     _hard_check(prec, gm, am, AA, mat, gaps, sa, sb, None, None, False)
+
+
+@pytest.mark.parametrize("gm", [0, 1])
+def test_hard_local_tiles_tied_best(gm):
+    """Local, tiled: one segment twice in A (rows 100-199 and 1700-1799) and twice in B
+    (columns 600-699 and 1000-1099) on backgrounds that score -5 against everything, so
+    four end cells in different stripes and tiles tie for the best; the pair's end is the
+    first in row-major order (200, 700), as the oracle's."""
+    alpha = AA
+    N = len(alpha)
+    mat = np.full((1, N, N), -5.0)
+    seg_letters = alpha[2:]
+    for k in range(2, N):
+        mat[0, k, k] = 5.0
+    gaps = np.array([[11.0, 3.0, 11.0, 3.0]])
+    rng = np.random.default_rng(1750 + gm)
+    seg = "".join(rng.choice(list(seg_letters), 100))
+    a = list(alpha[0] * 2000)
+    b = list(alpha[1] * 1400)
+    for o in (100, 1700):
+        a[o:o + 100] = seg
+    for o in (600, 1000):
+        b[o:o + 100] = seg
+    sa, sb = ["".join(a)], ["".join(b)]
+    _hard_check(32, gm, 1, alpha, mat, gaps, sa, sb, None, None, False)
+    bt = nw.SeqPairBatch(sa, sb, _params(alpha, mat, gaps), gap_model=("linear", "affine")[gm], mode="local",
+                         grad_mode="hard")
+    bt.score_and_grad()
+    assert bt.scores()[0] == 500.0
 
 
 def test_hard_long_tracked_several_warps_per_pair():

@@ -215,8 +215,9 @@ def test_float32_out_of_range_reruns_in_double():
 
 @pytest.mark.parametrize("grad_mode", ["soft", "hard"])
 def test_wait_limit_fails_cleanly(grad_mode):
-    """Several warps per pair wait on one another with bounded polls.  With the limit at one
-    poll the waits run out: the kernel marks the pair and returns, the call raises
+    """Several warps per pair wait on one another with bounded polls (soft long pairs; hard long
+    pairs with tracks -- untracked ones fill as tiles, which never wait).  With the limit at
+    one poll the waits run out: the kernel marks the pair and returns, the call raises
     RuntimeError, and the same batch then runs to the oracle's result at the default limit."""
     rng = np.random.default_rng(31)
     mat = rng.integers(-4, 4, size=(1, 20, 20)).astype(np.float64)
@@ -225,7 +226,9 @@ def test_wait_limit_fails_cleanly(grad_mode):
     gaps = np.array([[11.0, 1.0, 11.0, 1.0]])
     sa = ["".join(rng.choice(list(AA), 2600)) for _ in range(2)]
     sb = ["".join(c if rng.random() > 0.2 else rng.choice(list(AA)) for c in a) for a in sa]
-    b = nw.SeqPairBatch(sa, sb, nw.AlignParams.from_arrays(mat, gaps, alphabet=AA), grad_mode=grad_mode)
+    tracks = np.zeros(sum(len(s) for s in sa), np.uint16) if grad_mode == "hard" else None
+    b = nw.SeqPairBatch(sa, sb, nw.AlignParams.from_arrays(mat, gaps, alphabet=AA), grad_mode=grad_mode,
+                        tracks=tracks)
     b.set_spin_limit(1)
     with pytest.raises(RuntimeError, match="ran out"):
         b.score_and_grad()
