@@ -109,7 +109,7 @@ int nwg_set_geometry_costs(nwg_store* s, int soft, int size_class, int n, const 
  * path keeps a whole table per thread). */
 int nwg_set_memory(nwg_store* s, int64_t scratch_budget_bytes, int64_t checkpoint_bytes);
 
-/* Long pairs run with several warps per pair that wait on one another's progress; each wait
+/* Soft long pairs run with several warps per pair that wait on one another's progress; each wait
  * polls at most `polls` times (default 4194304, about a quarter second at the poll interval),
  * then the kernel marks the pair, finishes without waiting further and the call fails with
  * NWG_ECUDA ("a wait ... ran out") instead of hanging.  The store stays usable.  polls < 1 is

@@ -801,8 +801,8 @@ class SeqPairBatch:
         check(self._store._L.nwg_set_memory(self._store.h, int(scratch_budget_bytes), int(checkpoint_bytes)))
 
     def set_spin_limit(self, polls: int = 1 << 22) -> None:
-        """Polls a wait between the warps of one long pair makes before it gives up: the call
-        then raises RuntimeError instead of hanging, and the batch stays usable."""
+        """Polls a wait between the warps of one long pair (soft gradient) makes before it gives
+        up: the call then raises RuntimeError instead of hanging, and the batch stays usable."""
         check(self._store._L.nwg_set_spin_limit(self._store.h, int(polls)))
 
     def use_graphs(self, enable: bool = True) -> None:

@@ -622,9 +622,7 @@ void build_plan(nwg_store* s, Plan& P, bool soft, int lanes, int rpl, int elem_b
             if (s->plain) g = Geo{32, 4};
             else if (soft && !s->tracked() && rows >= kLongRows && nb >= 256) g = Geo{32, 4, false, long_warps(rows, 128)};
             else if (!soft && !one_warp && rows >= kLongRows && nb >= 256)
-                // long pairs: untracked ones as tiles over the whole device, tracked ones with
-                // several warps per pair
-                g = s->tracked() ? Geo{32, 8, false, long_warps(rows, 256)} : Geo{32, 8, false, 0, false, true};
+                g = Geo{32, 8, false, 0, false, true};   // long pairs: tiles over the whole device
             else if (sc < kClasses && cost_of[sc]) {
                 double best = 1e300;
                 for (const auto& gc : *cost_of[sc]) {
@@ -788,21 +786,13 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
     s->end.need(size_t(std::max<int64_t>(s->n, 1)) * 16, st);
     const int sms = sm_count(s->device);
     const size_t smem_base = (size_t(s->K) * s->N * s->N + 4 * size_t(s->K)) * sizeof(T);
-    // scratch per slot: the stripe boundary row (one group per pair), or one row per stripe
-    // (several warps per pair: a slot is a block)
+    // scratch per slot: the stripe boundary row (one group per pair)
     auto bucket_shape = [&](const Bucket& B, int64_t& blocks, int64_t& slots, int64_t& stride) {
         const int gpb = 128 / B.geo.G;
         const int64_t items = int64_t(B.pairs.size());
         const int64_t row = 3 * (int64_t(B.maxn) + 1);
         if (B.geo.tile) {   // tiles: per-pair row and column buffers instead of scratch
             blocks = 0; slots = 0; stride = 0;
-        } else if (B.geo.mw > 1) {
-            const int GR = B.geo.G * B.geo.R;
-            int64_t ns = 0;
-            for (int32_t p : B.pairs) ns = std::max<int64_t>(ns, (s->oa[p + 1] - s->oa[p] + GR - 1) / GR);
-            blocks = std::min<int64_t>(items, int64_t(sms) * std::max(1, 16 / B.geo.mw));
-            slots = blocks;
-            stride = std::max<int64_t>(ns, 1) * row;
         } else {
             blocks = std::min<int64_t>((items + gpb - 1) / gpb, int64_t(sms) * 16);
             slots = blocks * gpb;
@@ -810,7 +800,7 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
         }
     };
     int64_t max_total = 1, sum_total = 0;
-    bool any_mw = false, any_tile = false;
+    bool any_tile = false;
     int nbk = 0;
     for (auto& B : P.buckets) {
         if (B.pairs.empty()) continue;
@@ -818,14 +808,13 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
         bucket_shape(B, bl, sl, sd);
         max_total = std::max(max_total, sl * sd);
         sum_total += (sl * sd * int64_t(sizeof(T)) + 255) & ~int64_t(255);
-        any_mw |= B.geo.mw > 1;
         any_tile |= B.geo.tile;
         ++nbk;
     }
-    // several warps per pair and tiles: the fills first, then one walk over every pair
-    const bool sep_walk = any_mw || any_tile;
-    // the buckets' fills and walks run at once (bucket k's walk after its fill, each bucket on
-    // its own stream and scratch part) when nothing needs a host check between fill and walk
+    // tiles: the fills first, then one walk over every pair
+    const bool sep_walk = any_tile;
+    // otherwise the buckets' fills and walks run at once (bucket k's walk after its fill, each
+    // bucket on its own stream and scratch part) when their scratch parts fit
     const bool concurrent = !sep_walk && nbk > 1 && sum_total <= scratch_budget_of(s);
     s->scratch.need(concurrent ? size_t(sum_total) : size_t(max_total) * sizeof(T), st);
     std::vector<Launch> fills;
@@ -836,8 +825,8 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
         if (B.pairs.empty() || B.geo.tile) continue;
         HardFn fn = hard_fn_rt<T>(aff, ends ? 2 : (loc ? 1 : 0), tr, B.geo);
         if (!fn) throw Error(NWG_EINVAL, "no kernel for this geometry");
-        const int hblock = B.geo.mw > 1 ? 32 * B.geo.mw : 128;
-        const size_t smem = smem_base + (B.geo.mw > 1 ? nwg::hard_mw_smem_bytes(B.geo.mw, int(sizeof(T))) : 0);
+        const int hblock = 128;
+        const size_t smem = smem_base;
         NWG_CUDA(nwg::allow_smem(reinterpret_cast<const void*>(fn), smem));
         nwg::HardArgs A{};
         A.a = s->a.as<uint8_t>(); A.oa = s->doa.as<int64_t>();
@@ -858,10 +847,8 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
         A.scratch = concurrent ? static_cast<void*>(static_cast<unsigned char*>(s->scratch.p) + soff_b) : s->scratch.p;
         soff_b += (slots * stride * int64_t(sizeof(T)) + 255) & ~int64_t(255);
         A.scratch_stride = stride;
-        A.row_stride = 3 * (int64_t(B.maxn) + 1);
         A.score = s->score.as<double>(); A.end = s->end.as<int32_t>();
         A.ends = ends;
-        A.spin_limit = s->spin_limit;
         A.queue = s->queue(nwg_store::kQueueHard + nq++, st);
         fills.push_back(make_launch(reinterpret_cast<const void*>(fn), unsigned(blocks), hblock, smem, A));
         fill_args.push_back(A);
@@ -890,7 +877,6 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
         A.codes = s->codes.as<uint8_t>(); A.code_off = P.dcode_off.as<int64_t>();
         A.scratch = s->trow.p; A.scratch_stride = 0;
         A.score = s->score.as<double>(); A.end = s->end.as<int32_t>();
-        A.spin_limit = s->spin_limit;
         A.queue = s->queue(nwg_store::kQueueHard + nq++, st);
         A.tile_w = kTileW;
         A.rowbuf = s->trow.p; A.rowbuf_off = P.tile_rowoff.as<int64_t>();
@@ -948,9 +934,8 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
     W.path_info = keep ? s->path_info.as<int32_t>() : nullptr;
     const Launch walk = make_launch(reinterpret_cast<const void*>(&nwg::walk_kernel),
                                     unsigned((P.n_planned + 127) / 128), 128, 0, W);
-    // several warps per pair: a wait between warps that ran out fails the call (end state 3),
-    // which the host checks between the fills and a separate walk; otherwise the fills walk
-    // their own pairs, one captured sequence
+    // one captured sequence: the fills walk their own pairs, or (tiles) one walk launch over
+    // every pair follows all the fills
     GraphCache* gc = band ? &s->g_hard_band : &s->g_hard[sizeof(T) == 4 ? 0 : 1];
     if (!sep_walk) {
         // a warp per pair: the fill walks its own pairs (the codes still in L2); a lane per pair
@@ -979,20 +964,9 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
         }
         run_launches(s, gc, seq, st, concurrent, &lanes);
     } else {
+        if (P.n_planned) fills.push_back(walk);
         run_launches(s, gc, fills, st);
     }
-    if (any_mw && s->n) {
-        std::vector<int32_t> e(size_t(s->n) * 4);
-        NWG_CUDA(cudaMemcpyAsync(e.data(), s->end.p, e.size() * 4, cudaMemcpyDeviceToHost, st));
-        NWG_CUDA(cudaStreamSynchronize(st));
-        for (auto& B : P.buckets)
-            if (B.geo.mw > 1)
-                for (int32_t p : B.pairs)
-                    if (e[4 * size_t(p) + 2] == 3)
-                        throw Error(NWG_ECUDA, "nwgrad_b200: hard fill: a wait between the warps of pair " +
-                                                   std::to_string(p) + " ran out (the kernel gave up instead of hanging)");
-    }
-    if (sep_walk && P.n_planned) run_launches(s, nullptr, std::vector<Launch>{walk}, st);
     if (!hb_pairs.empty()) {
         s->hb_pairs.need(hb_pairs.size() * 4, st);
         NWG_CUDA(cudaMemcpyAsync(s->hb_pairs.p, hb_pairs.data(), hb_pairs.size() * 4, cudaMemcpyHostToDevice, st));

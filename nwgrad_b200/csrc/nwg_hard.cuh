@@ -42,7 +42,6 @@ struct HardArgs {
     int N, K;
     uint8_t* codes; const int64_t* code_off;   // per pair code table
     void* scratch; int64_t scratch_stride;     // per group slot: the stripe boundary row, 3*(n+1) T
-    int64_t row_stride;                        // several warps per pair: T per boundary row (one per stripe)
     double* score;                             // per pair
     int32_t* end;                              // per pair: end_i, end_j, state, layout (G<<8|R)
     // guide-banded re-alignment (BAND kernels only)
@@ -57,7 +56,6 @@ struct HardArgs {
     // (column 0 a free start), 2 a_end (column n's cells ends), 4 b_begin (row 0 a free start),
     // 8 b_end (row m's cells ends); 0: Global's charged borders and end (m, n)
     int ends;
-    int spin_limit;                            // several warps per pair: polls before a wait gives up
     int* queue;                                // this launch's work-queue counters (2 ints, zero at launch)
     // tiled long pairs (TL kernels): an item is one tile -- stripe s of pair p over columns
     // c W + 1 .. (c + 1) W -- and a launch holds one anti-diagonal (s + c) of every pair's tiles
@@ -106,38 +104,19 @@ template <class T> struct EndPick {
     }
 };
 
-// Shared memory beyond the parameters that several warps per pair use: per warp a best value,
-// its cell and state, and a progress counter.
-__host__ __device__ inline size_t hard_mw_smem_bytes(int warps, int tsize) {
-    return size_t(warps) * (tsize + 4 * 4) + size_t(warps) * 4 + 64;
-}
-
-// Several warps per pair (MW, long pairs): warp w fills stripes w, w + NW, ..., each stripe's
-// bottom row in its own scratch row, and waits (every 32 steps, bounded) until the warp filling
-// the stripe above has published enough steps -- the protocol of the soft kernel
-// (nwg_soft.cuh).  A wait that runs out (HardArgs::spin_limit polls) marks the pair's end
-// state 3 and the host fails the call.
-
 // SG: the semi-global ends of A.ends (Global fills only, full DP, a warp or lane per pair)
 // TL: tiled long pairs (A.tiles): each item one stripe of one pair over one tile of columns; the
 // tile's top row comes from the stripe above (rowbuf), its left column from the tile to its left
 // (colbuf), and its codes go where the full fill would put them, so the walk reads them as usual
-template <class T, bool AFF, bool LOC, bool TR, int G, int R, bool BAND = false, bool MW = false, bool SG = false,
-          bool TL = false>
-__global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArgs A) {
-    static_assert(!MW || (G == 32 && !BAND), "several warps per pair: 32 lanes, full DP");
-    static_assert(!TL || (G == 32 && !BAND && !MW && !SG), "tiles: 32 lanes, full DP, Global or Local");
-    static_assert(!SG || (!LOC && !MW), "semi-global ends: Global fills, one warp per pair");
+template <class T, bool AFF, bool LOC, bool TR, int G, int R, bool BAND = false, bool SG = false, bool TL = false>
+__global__ void __launch_bounds__(128) hard_fill_kernel(const HardArgs A) {
+    static_assert(!TL || (G == 32 && !BAND && !SG), "tiles: 32 lanes, full DP, Global or Local");
+    static_assert(!SG || !LOC, "semi-global ends: Global fills, one warp or lane per pair");
     constexpr int GR = G * R;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* smat = reinterpret_cast<T*>(smem_raw);
     const int nmat = A.K * A.N * A.N;
     T* sgap = smat + nmat;
-    unsigned char* mw_raw = reinterpret_cast<unsigned char*>(
-        (reinterpret_cast<uintptr_t>(sgap + 4 * A.K) + 15) & ~uintptr_t(15));
-    T* wbest = reinterpret_cast<T*>(mw_raw);                                   // MW: [warp]
-    int* wcell = reinterpret_cast<int*>(wbest + (blockDim.x / G));             // MW: [warp][4]
-    volatile int* prog = wcell + 4 * (blockDim.x / G);                         // MW: [warp]
     for (int k = threadIdx.x; k < nmat; k += blockDim.x) smat[k] = static_cast<const T*>(A.mat)[k];
     for (int k = threadIdx.x; k < 4 * A.K; k += blockDim.x) sgap[k] = static_cast<const T*>(A.gaps)[k];
     __syncthreads();
@@ -145,55 +124,21 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
     const int lane = threadIdx.x % G;
     const int gpb = blockDim.x / G;
     const int gib = threadIdx.x / G;
-    const int NWp = MW ? gpb : 1;
-    const int pw = (gib + NWp - 1) % NWp;                   // MW: the warp of the stripe above
-    const int64_t slot = MW ? int64_t(blockIdx.x) : int64_t(blockIdx.x) * gpb + gib;
+    const int64_t slot = int64_t(blockIdx.x) * gpb + gib;
     unsigned gmask;
     if constexpr (G == 32) gmask = 0xffffffffu;
     else gmask = ((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1));
     T* const bnd0 = static_cast<T*>(A.scratch) + slot * A.scratch_stride;
     const int N = A.N;
-    bool stalled = false;
-    auto wait_for = [&](int target) {
-        if constexpr (MW) {
-            int k = 0;
-            while (!stalled && prog[pw] < target) {
-                if (++k > A.spin_limit) stalled = true;
-                else __nanosleep(64);
-            }
-            __syncwarp();
-            __threadfence_block();
-        }
-    };
-    auto publish = [&](int v) {
-        if constexpr (MW) {
-            __syncwarp();
-            __threadfence_block();
-            if (lane == 0) prog[gib] = v;
-        }
-    };
-
-    // the next pair of this group (a block, for several warps per pair) from the launch's work
-    // queue, in the longest-first order: a group that finishes early takes the next pair
-    __shared__ long long s_next;
+    // the next item (pair, or tile) of this group from the launch's work queue, in the
+    // longest-first order: a group that finishes early takes the next one
     auto next_item = [&]() -> int64_t {
-        if constexpr (MW) {
-            __syncthreads();
-            if (threadIdx.x == 0) s_next = wq_next(A.queue, int(gridDim.x), A.n_items);
-            __syncthreads();
-            return s_next;
-        } else {
-            long long v = 0;
-            if (lane == 0) v = wq_next(A.queue, int(gridDim.x) * gpb, A.n_items);
-            if constexpr (G > 1) v = __shfl_sync(gmask, v, 0, G);
-            return v;
-        }
+        long long v = 0;
+        if (lane == 0) v = wq_next(A.queue, int(gridDim.x) * gpb, A.n_items);
+        if constexpr (G > 1) v = __shfl_sync(gmask, v, 0, G);
+        return v;
     };
     for (int64_t it = next_item(); it < A.n_items; it = next_item()) {
-        if constexpr (MW) {
-            if (lane == 0) prog[gib] = -1;
-            __syncthreads();
-        }
         const int p = TL ? A.tiles[3 * it] : A.order[it];
         const int ts = TL ? A.tiles[3 * it + 1] : 0, tc = TL ? A.tiles[3 * it + 2] : 0;   // TL: stripe, tile
         const int64_t ao = A.oa[p], bo = A.ob[p];
@@ -215,7 +160,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
         const bool sg_r0 = SG && (A.ends & 4), sg_c0 = SG && (A.ends & 1);
         const bool sg_ec = SG && (A.ends & 2), sg_er = SG && (A.ends & 8);
         if (m == 0 || n == 0) {
-            if (lane == 0 && (!MW || gib == 0)) {
+            if (lane == 0) {
                 T sc; int ei, ej, st;
                 if (LOC) { sc = T(0); ei = 0; ej = 0; st = 0; }
                 else if (SG) {
@@ -253,7 +198,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
                 A.end[4 * p] = ei; A.end[4 * p + 1] = ej; A.end[4 * p + 2] = st;
                 A.end[4 * p + 3] = (G << 8) | R;
                 // an empty side: the walk runs the border (no codes read)
-                if (!MW && !TL && A.walk_fused) walk_pair(A.walk, p);
+                if (!TL && A.walk_fused) walk_pair(A.walk, p);
             }
             continue;
         }
@@ -293,15 +238,14 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
             }
         }
 
-        const int S_full = n + G - 1;          // MW: steps per stripe (full DP)
-        const int SP = S_full + 1;             // MW: progress key per stripe
         T* const rows_p = TL ? static_cast<T*>(A.rowbuf) + A.rowbuf_off[p] : nullptr;
         T* const cols_p = TL ? static_cast<T*>(A.colbuf) + A.colbuf_off[p] : nullptr;
         const int ntc = TL ? (n + A.tile_w - 1) / A.tile_w : 1;   // TL: tiles per stripe
-        for (int s = TL ? ts : (MW ? gib : 0); s < (TL ? ts + 1 : nstripes); s += NWp) {
-            // the previous stripe's bottom row (read) and this stripe's (written)
-            T* const bnd = TL ? rows_p + int64_t(s - 1) * 3 * (n + 1) : bnd0 + (MW ? int64_t(s - 1) * A.row_stride : 0);
-            T* const bnd_out = TL ? rows_p + int64_t(s) * 3 * (n + 1) : bnd0 + (MW ? int64_t(s) * A.row_stride : 0);
+        for (int s = TL ? ts : 0; s < (TL ? ts + 1 : nstripes); ++s) {
+            // the previous stripe's bottom row (read) and this stripe's (written; one row in
+            // place, except for tiles: a row per stripe)
+            T* const bnd = TL ? rows_p + int64_t(s - 1) * 3 * (n + 1) : bnd0;
+            T* const bnd_out = TL ? rows_p + int64_t(s) * 3 * (n + 1) : bnd0;
             const int i0 = s * GR + lane * R + 1;   // this lane's first DP row
             // the stripe's columns [cmin, cmax]: the union of its rows' bands (TL: the tile's)
             int cmin = TL ? tc * A.tile_w + 1 : 1, cmax = TL ? min(n, (tc + 1) * A.tile_w) : n;
@@ -411,14 +355,10 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
                     else { nuM = ninf<T>(); nuX = ninf<T>(); nuY = ninf<T>(); }
                 }
             };
-            const bool waits = MW && s > 0;
-            if (waits) wait_for((s - 1) * SP + min(S_full, 2 * G + 1));
             fetch_up(cmin);
 
             for (int t = 0; t < S; ++t) {
                 const int j = cmin + t - lane;
-                if (waits && t > 0 && (t & 31) == 0) wait_for((s - 1) * SP + min(S_full, t + 2 * G + 1));
-                if (MW && t > 0 && (t & 7) == 0) publish(s * SP + t);
                 if (lane == 0 && j <= cmax) {
                     if (s == 0) row0(j, upM, upX, upY);
                     else { upM = nuM; upX = nuX; upY = nuY; fetch_up(j + 1); }
@@ -525,7 +465,6 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
                     if constexpr (AFF) { bnd_out[3 * j + 1] = cX[R - 1]; bnd_out[3 * j + 2] = cY[R - 1]; }
                 }
             }
-            if constexpr (MW) publish(s * SP + S_full);
             if constexpr (TL) {   // the tile's last column, for the tile to its right
                 if (tc + 1 < ntc) {
 #pragma unroll
@@ -586,42 +525,6 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
             }
             if constexpr (G > 1) __syncwarp(gmask);
         }
-        if constexpr (MW) {
-            // a wait that ran out fails the pair; Local: the warps' bests, first row-major max
-            stalled = __any_sync(gmask, stalled);
-            if (lane == 0) {
-                wbest[gib] = bestv;
-                wcell[4 * gib] = besti; wcell[4 * gib + 1] = bestj; wcell[4 * gib + 2] = bests;
-                wcell[4 * gib + 3] = stalled ? 1 : 0;
-            }
-            __syncthreads();
-            bool anystall = false;
-            for (int w = 0; w < NWp; ++w) anystall |= wcell[4 * w + 3] != 0;
-            if (anystall) {
-                if (threadIdx.x == 0) {
-                    A.score[p] = 0.0;
-                    A.end[4 * p] = 0; A.end[4 * p + 1] = 0; A.end[4 * p + 2] = 3; A.end[4 * p + 3] = (G << 8) | R;
-                }
-                __syncthreads();
-                stalled = false;
-                continue;
-            }
-            if constexpr (LOC) {
-                if (threadIdx.x == 0) {
-                    T bv = T(0); int bi = 0, bj = 0, bs = 0;
-                    for (int w = 0; w < NWp; ++w) {
-                        const T v = wbest[w];
-                        const int wi = wcell[4 * w];
-                        if (v > bv || (v == bv && v > T(0) && wi < bi)) { bv = v; bi = wi; bj = wcell[4 * w + 1]; bs = wcell[4 * w + 2]; }
-                    }
-                    A.score[p] = static_cast<double>(bv);
-                    A.end[4 * p] = bi; A.end[4 * p + 1] = bj; A.end[4 * p + 2] = bs;
-                    A.end[4 * p + 3] = (G << 8) | R;
-                }
-                __syncthreads();
-                continue;
-            }
-        }
         if constexpr (!LOC) {
             if constexpr (G > 1) {
                 // the lane holding row m broadcasts its end values
@@ -641,7 +544,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
             }
             // TL: the tile holding (m, n) writes the pair's result
             const bool tl_end = !TL || (ts == nstripes - 1 && min(n, (tc + 1) * A.tile_w) == n);
-            if (lane == 0 && tl_end && (!MW || gib == (nstripes - 1) % NWp)) {
+            if (lane == 0 && tl_end) {
                 T sc; int st, ei = m, ej = n;
                 if constexpr (AFF) {
                     sc = rmax3(endM, endX, endY);
@@ -656,7 +559,6 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
                 A.end[4 * p] = ei; A.end[4 * p + 1] = ej; A.end[4 * p + 2] = st;
                 A.end[4 * p + 3] = (G << 8) | R;
             }
-            if constexpr (MW) __syncthreads();
         } else if (lane == 0) {
             if constexpr (TL) {   // this tile's first row-major best; a later pass picks the pair's
                 const int64_t slot = A.tile_off[p] + int64_t(ts) * ntc + tc;
@@ -668,7 +570,7 @@ __global__ void __launch_bounds__(MW ? 512 : 128) hard_fill_kernel(const HardArg
                 A.end[4 * p + 3] = (G << 8) | R;
             }
         }
-        if constexpr (!MW && !TL) {
+        if constexpr (!TL) {
             // the traceback, while this pair's codes are still in L2: the group's codes and end
             // cell are visible to its lane 0 after the warp barrier; its other lanes go on with
             // their next pair's fill meanwhile

@@ -13,12 +13,12 @@ HardFn pick_band(Geo g) {
 template <class T, bool AFF, bool TR>
 HardFn pick_sg(Geo g) {
     if (g.band) {   // glocal ends, banded re-alignment
-        if (g.G == 32 && g.R == 1) return &hard_fill_kernel<T, AFF, false, TR, 32, 1, true, false, true>;
-        if (g.G == 32 && g.R == 2) return &hard_fill_kernel<T, AFF, false, TR, 32, 2, true, false, true>;
+        if (g.G == 32 && g.R == 1) return &hard_fill_kernel<T, AFF, false, TR, 32, 1, true, true>;
+        if (g.G == 32 && g.R == 2) return &hard_fill_kernel<T, AFF, false, TR, 32, 2, true, true>;
         return nullptr;
     }
-    if (g.mw > 1) return nullptr;
-#define NWG_H(GG, RR) if (g.G == GG && g.R == RR) return &hard_fill_kernel<T, AFF, false, TR, GG, RR, false, false, true>;
+    if (g.mw > 1 || g.tile) return nullptr;
+#define NWG_H(GG, RR) if (g.G == GG && g.R == RR) return &hard_fill_kernel<T, AFF, false, TR, GG, RR, false, true>;
     NWG_H(1, 8) NWG_H(1, 16) NWG_H(1, 24) NWG_H(1, 32) NWG_H(32, 1) NWG_H(32, 2) NWG_H(32, 4) NWG_H(32, 8)
 #undef NWG_H
     return nullptr;
@@ -26,12 +26,8 @@ HardFn pick_sg(Geo g) {
 template <class T, bool AFF, bool LOC, bool TR>
 HardFn pick(Geo g) {
     if (g.band) return pick_band<T, AFF, LOC, TR>(g);
-    if (g.tile) return (g.G == 32 && g.R == 8) ? &hard_fill_kernel<T, AFF, LOC, TR, 32, 8, false, false, false, true> : nullptr;
-    if (g.mw > 1) {   // several warps per pair
-        if (g.G == 32 && g.R == 4) return &hard_fill_kernel<T, AFF, LOC, TR, 32, 4, false, true>;
-        if (g.G == 32 && g.R == 8) return &hard_fill_kernel<T, AFF, LOC, TR, 32, 8, false, true>;
-        return nullptr;
-    }
+    if (g.tile) return (g.G == 32 && g.R == 8) ? &hard_fill_kernel<T, AFF, LOC, TR, 32, 8, false, false, true> : nullptr;
+    if (g.mw > 1) return nullptr;
 #define NWG_H(GG, RR) if (g.G == GG && g.R == RR) return &hard_fill_kernel<T, AFF, LOC, TR, GG, RR>;
     NWG_H(1, 8) NWG_H(1, 16) NWG_H(1, 24) NWG_H(1, 32) NWG_H(32, 1) NWG_H(32, 2) NWG_H(32, 4) NWG_H(32, 8)
 #undef NWG_H

@@ -9,8 +9,8 @@
 namespace nwg {
 using HardFn = void (*)(const HardArgs);
 using SoftFn = void (*)(const SoftArgs);
-// mw > 1: that many warps per pair; post: the posterior-guide kernels (32 x 4, full DP, untracked);
-// tile: the hard fill over tiles of long pairs (32 x 8, one launch per anti-diagonal of tiles)
+// mw > 1: that many warps per pair (soft); post: the posterior-guide kernels (32 x 4, full DP,
+// untracked); tile: the hard fill over tiles of long pairs (32 x 8, a launch per anti-diagonal)
 struct Geo { int G, R; bool band = false; int mw = 0; bool post = false; bool tile = false; };
 // am: 0 Global, 1 Local, 2 semi-global ends (full DP, one warp or lane per pair)
 HardFn hard_fn_f32(bool aff, int am, bool tr, Geo g);

@@ -383,7 +383,8 @@ def test_hard_local_tiles_tied_best(gm):
     assert bt.scores()[0] == 500.0
 
 
-def test_hard_long_tracked_several_warps_per_pair():
+def test_hard_long_tracked_tiles():
+    """Tracked long pairs (three parameter sets, gap tracks) fill as tiles too: bit for bit."""
     rng = np.random.default_rng(1800)
     alpha = "ACGTU"
     mat, gaps, sa, sb, tr, gt = _problem(rng, alpha, 3, 1600, 2200, K=3, tracked=True, gap_tracks=True)
@@ -423,9 +424,9 @@ def test_soft_banded(prec, gm, am, bw):
 @pytest.mark.parametrize("gm", [0, 1])
 @pytest.mark.parametrize("am", [0, 1])
 def test_score_only_bit_exact(prec, gm, am):
-    """grad_mode="none" (the score-only fill: no codes, no walk) against the oracle's Viterbi
-    scores bit for bit: short pairs at a lane per pair, medium at a warp, and long pairs at
-    several warps per pair."""
+    """grad_mode="none" (the Viterbi fill and the walk for the guides, no gradient) against the
+    oracle's Viterbi scores bit for bit: short pairs at a lane per pair, medium at a warp, and
+    long pairs as tiles."""
     rng = np.random.default_rng(1300 + prec + 10 * gm + 20 * am)
     mat, gaps, sa, sb, tr, gt = _problem(rng, AA, 60, 0, 40, integer=False)
     sa += ["", "ACD", "W" * 70] + rand_seqs(rng, 6, 200, 400, AA) + rand_seqs(rng, 2, 1600, 2200, AA)
