@@ -40,7 +40,10 @@ typedef struct nwg_job {
     int lanes;         /* 0 auto; else lanes per pair (1 or 32) for every pair (tuning) */
     int rows;          /* 0 auto; else rows per lane (tuning) */
     int traceback;     /* hard, affine Global, untracked: 3 hirschberg, 4 hirschberg_pmax (pairs
-                          longer than hb_cutoff rows split); anything else the Pointers path */
+                          longer than hb_cutoff rows split); 5 grid (full DP, Global or Local:
+                          pairs of 1536+ rows and 256+ columns keep a grid of rows and columns
+                          and refill the tiles their path crosses, the Pointers result bit for
+                          bit); anything else the Pointers path */
     int hb_cutoff;     /* Hirschberg base-case rows (>= 1; 0: 512) */
     int free_ends;     /* mode 2 (semi-global, the reference's AlignMode::Glocal with kSgFree*
                           bits, simd_levels.hpp:170-182): 1 a_begin (column 0 a free start),

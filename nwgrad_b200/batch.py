@@ -318,8 +318,8 @@ class SeqPairBatch:
     def _job(self, grad_mode, band=-1, keep_paths=False):
         lanes, rows = self._tune
         soft_double = 1 if (self._precision == 64 or self.soft_precision == "double") else 0
-        tb = {"hirschberg": 3, "hirschberg_pmax": 4}.get(self._traceback, 0)
-        if tb and grad_mode != 2 and band < 0:
+        tb = {"hirschberg": 3, "hirschberg_pmax": 4, "grid": 5}.get(self._traceback, 0)
+        if tb in (3, 4) and grad_mode != 2 and band < 0:
             self._check_hirschberg()
         if self._am == 2 and band >= 0 and self._sg != SG_GLOCAL:
             # aligner.hpp:2222-2231 (check_problem)

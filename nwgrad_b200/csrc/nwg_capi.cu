@@ -332,7 +332,7 @@ struct Bucket {
 
 struct Plan {
     bool valid = false;
-    int key_soft = -1, key_lanes = -1, key_rows = -1, key_band = -1, key_hb = -1, key_one_warp = -1;
+    int key_soft = -1, key_lanes = -1, key_rows = -1, key_band = -1, key_hb = -1, key_one_warp = -1, key_grid = -1;
     int64_t n_planned = 0;           // pairs in the buckets (hard: those not split by Hirschberg)
     std::vector<Bucket> buckets;
     std::vector<int64_t> code_off;   // hard: per pair
@@ -376,6 +376,7 @@ struct nwg_store {
     // results
     DBuf score, end, grad, guide, status, codes, scratch, part, red, moves, moves_off, path_info;
     DBuf trow, tcol, tbest, tcell;      // tiled long pairs: stripe rows, tile columns, Local tile bests
+    DBuf tgrid;                         // grid traceback: one tile's codes per walking warp
     int64_t gstride = 0;
     bool have_scores = false, have_grads = false, have_guides = false, have_paths = false;
     int last_grad_mode = 0, last_gm = -1, last_am = -1, last_prec = 0;
@@ -592,13 +593,14 @@ const T* ensure_bx0(nwg_store* s, bool aff, cudaStream_t st, bool& ok, DBuf& buf
 
 // hb_cut > 0 (hard, full DP): pairs longer than hb_cut rows are left out (Hirschberg runs them).
 // one_warp (hard): no pair runs with several warps (the semi-global ends are one warp's).
+// grid: the grid traceback for tiled pairs (no code table for them)
 void build_plan(nwg_store* s, Plan& P, bool soft, int lanes, int rpl, int elem_bytes, bool band = false,
-                int hb_cut = 0, bool one_warp = false) {
+                int hb_cut = 0, bool one_warp = false, bool grid = false) {
     if (P.valid && P.key_soft == int(soft) && P.key_lanes == lanes && P.key_rows == rpl && P.key_band == int(band) &&
-        P.key_hb == hb_cut && P.key_one_warp == int(one_warp)) return;
+        P.key_hb == hb_cut && P.key_one_warp == int(one_warp) && P.key_grid == int(grid)) return;
     P.reset();
     P.key_soft = soft; P.key_lanes = lanes; P.key_rows = rpl; P.key_band = band; P.key_hb = hb_cut;
-    P.key_one_warp = one_warp;
+    P.key_one_warp = one_warp; P.key_grid = grid;
     const int64_t n = s->n;
     // one lane per pair keeps a K*N*N histogram per lane in shared memory (soft)
     const bool lane_ok_soft = int64_t(s->K) * s->N * s->N * elem_bytes * 32 <= 48 * 1024;
@@ -646,6 +648,8 @@ void build_plan(nwg_store* s, Plan& P, bool soft, int lanes, int rpl, int elem_b
         }
         P.buckets[bi].pairs.push_back(int32_t(p));
     }
+    // tiled buckets last: the pairs walked from a code table are then a prefix of the order
+    std::stable_partition(P.buckets.begin(), P.buckets.end(), [](const Bucket& B) { return !B.geo.tile; });
     std::vector<int32_t> order;
     order.reserve(n);
     if (!soft) P.code_off.assign(n + 1, 0);
@@ -680,7 +684,8 @@ void build_plan(nwg_store* s, Plan& P, bool soft, int lanes, int rpl, int elem_b
                 const int GR = B.geo.G * B.geo.R;
                 const int64_t st = (m + GR - 1) / GR;
                 P.code_off[p] = off;
-                const int64_t bytes = (m && nb) ? st * (((nb + B.geo.G - 1) + 7) & ~int64_t(7)) * GR : 0;
+                const bool table = m && nb && !(grid && B.geo.tile);
+                const int64_t bytes = table ? st * (((nb + B.geo.G - 1) + 7) & ~int64_t(7)) * GR : 0;
                 off += (bytes + 15) & ~int64_t(15);
             }
         P.code_bytes = std::max<int64_t>(off, 16);
@@ -771,8 +776,10 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
             throw Error(NWG_EINVAL, "nwgrad: traceback=\"hirschberg\" / \"hirschberg_pmax\" needs non-negative "
                                     "gap penalties (got a negative one); use traceback=\"pointers\" or \"auto\"");
     }
+    // the grid traceback (aligner.hpp:89-100): tiled pairs keep rows and columns, not codes
+    const bool grid = !band && ends == 0 && J.traceback == 5;
     Plan& P = band ? s->band_plan : s->hard_plan;
-    build_plan(s, P, false, band ? 32 : J.lanes, band ? 2 : J.rows, sizeof(T), band, hb_cut, ends != 0);
+    build_plan(s, P, false, band ? 32 : J.lanes, band ? 2 : J.rows, sizeof(T), band, hb_cut, ends != 0, grid);
     s->codes.need(size_t(P.code_bytes), st);
     if (band) s->stripe_tab.need(size_t(std::max<int64_t>(P.n_stripes, 1)) * 16, st);
     const DBuf& matT = sizeof(T) == 4 ? s->matf : s->matd;
@@ -874,7 +881,7 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
         A.gtracks = tr ? s->gtracks.as<uint16_t>() : nullptr;
         A.bx0 = bx0;
         A.mat = matT.p; A.gaps = gapT.p; A.N = s->N; A.K = s->K;
-        A.codes = s->codes.as<uint8_t>(); A.code_off = P.dcode_off.as<int64_t>();
+        A.codes = grid ? nullptr : s->codes.as<uint8_t>(); A.code_off = P.dcode_off.as<int64_t>();
         A.scratch = s->trow.p; A.scratch_stride = 0;
         A.score = s->score.as<double>(); A.end = s->end.as<int32_t>();
         A.queue = s->queue(nwg_store::kQueueHard + nq++, st);
@@ -964,7 +971,43 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
         }
         run_launches(s, gc, seq, st, concurrent, &lanes);
     } else {
-        if (P.n_planned) fills.push_back(walk);
+        const int64_t n_tiled = int64_t(P.tile_pairs.size());
+        if (grid && n_tiled) {
+            // a warp per tiled pair walks back, refilling the tiles its path crosses into its
+            // own tile buffer; the pairs before them in the order walk their code tables
+            const Geo gg{32, 8, false, 0, false, true, true};
+            HardFn fn = hard_fn_rt<T>(aff, loc ? 1 : 0, tr, gg);
+            if (!fn) throw Error(NWG_EINVAL, "no kernel for this geometry");
+            NWG_CUDA(nwg::allow_smem(reinterpret_cast<const void*>(fn), smem_base));
+            const int64_t blocks = std::min<int64_t>((n_tiled + 3) / 4, int64_t(sms) * 16);
+            const int64_t stride = int64_t((kTileW + 32 - 1 + 7) & ~7) * 32 * 8;   // steps x lanes x rows
+            s->tgrid.need(size_t(blocks * 4 * stride), st);
+            nwg::HardArgs A{};
+            A.a = s->a.as<uint8_t>(); A.oa = s->doa.as<int64_t>();
+            A.b = s->b.as<uint8_t>(); A.ob = s->dob.as<int64_t>();
+            A.tracks = tr ? s->tracks.as<uint16_t>() : nullptr;
+            A.gtracks = tr ? s->gtracks.as<uint16_t>() : nullptr;
+            A.bx0 = bx0;
+            A.order = P.tile_plist.as<int32_t>(); A.n_items = n_tiled;
+            A.mat = matT.p; A.gaps = gapT.p; A.N = s->N; A.K = s->K;
+            A.codes = nullptr; A.code_off = P.dcode_off.as<int64_t>();
+            A.scratch = s->tgrid.p; A.scratch_stride = stride;
+            A.score = s->score.as<double>(); A.end = s->end.as<int32_t>();
+            A.queue = s->queue(nwg_store::kQueueHard + nq++, st);
+            A.tile_w = kTileW;
+            A.rowbuf = s->trow.p; A.rowbuf_off = P.tile_rowoff.as<int64_t>();
+            A.colbuf = s->tcol.p; A.colbuf_off = P.tile_coloff.as<int64_t>();
+            A.walk = W;
+            fills.push_back(make_launch(reinterpret_cast<const void*>(fn), unsigned(blocks), 128, smem_base, A));
+            if (P.n_planned > n_tiled) {
+                nwg::WalkArgs Wp = W;
+                Wp.n_items = P.n_planned - n_tiled;
+                fills.push_back(make_launch(reinterpret_cast<const void*>(&nwg::walk_kernel),
+                                            unsigned((Wp.n_items + 127) / 128), 128, 0, Wp));
+            }
+        } else if (P.n_planned) {
+            fills.push_back(walk);
+        }
         run_launches(s, gc, fills, st);
     }
     if (!hb_pairs.empty()) {

@@ -108,9 +108,18 @@ template <class T> struct EndPick {
 // TL: tiled long pairs (A.tiles): each item one stripe of one pair over one tile of columns; the
 // tile's top row comes from the stripe above (rowbuf), its left column from the tile to its left
 // (colbuf), and its codes go where the full fill would put them, so the walk reads them as usual
-template <class T, bool AFF, bool LOC, bool TR, int G, int R, bool BAND = false, bool SG = false, bool TL = false>
+// (A.codes null: no codes -- the grid traceback's score-only pass, which keeps only the rows and
+// columns).
+// GW: the grid traceback (aligner.hpp:89-100, viterbi_affine_grid :5327) over those rows and
+// columns: a warp per pair (A.order) walks back from the end cell, and each time the path enters
+// a tile the warp fills that tile again, with codes, into its own tile buffer (A.scratch).  The
+// refill starts from the same row and column values as the first pass, so its codes are the
+// Pointers fill's, bit for bit; memory is the grid of rows and columns, not a code per cell.
+template <class T, bool AFF, bool LOC, bool TR, int G, int R, bool BAND = false, bool SG = false, bool TL = false,
+          bool GW = false>
 __global__ void __launch_bounds__(128) hard_fill_kernel(const HardArgs A) {
     static_assert(!TL || (G == 32 && !BAND && !SG), "tiles: 32 lanes, full DP, Global or Local");
+    static_assert(!GW || TL, "the grid walk refills tiles");
     static_assert(!SG || !LOC, "semi-global ends: Global fills, one warp or lane per pair");
     constexpr int GR = G * R;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -139,8 +148,9 @@ __global__ void __launch_bounds__(128) hard_fill_kernel(const HardArgs A) {
         return v;
     };
     for (int64_t it = next_item(); it < A.n_items; it = next_item()) {
-        const int p = TL ? A.tiles[3 * it] : A.order[it];
-        const int ts = TL ? A.tiles[3 * it + 1] : 0, tc = TL ? A.tiles[3 * it + 2] : 0;   // TL: stripe, tile
+        const int p = (TL && !GW) ? A.tiles[3 * it] : A.order[it];
+        // TL: the item's stripe and tile (GW: those of the tile being refilled)
+        int ts = (TL && !GW) ? A.tiles[3 * it + 1] : 0, tc = (TL && !GW) ? A.tiles[3 * it + 2] : 0;
         const int64_t ao = A.oa[p], bo = A.ob[p];
         const int m = int(A.oa[p + 1] - ao), n = int(A.ob[p + 1] - bo);
         const uint8_t* __restrict__ ap = A.a + ao;
@@ -202,7 +212,7 @@ __global__ void __launch_bounds__(128) hard_fill_kernel(const HardArgs A) {
             }
             continue;
         }
-        uint8_t* __restrict__ codes = A.codes + A.code_off[p];
+        uint8_t* __restrict__ codes = (TL && !A.codes) ? nullptr : A.codes + A.code_off[p];
         const int nstripes = (m + GR - 1) / GR;
         // the band (full DP: every column of every row; borders reach every row / column)
         BandRows bw{BAND ? A.guide + ao + p : nullptr, A.band, m, n, !LOC && !SG};   // glocal: row m's own band
@@ -241,6 +251,30 @@ __global__ void __launch_bounds__(128) hard_fill_kernel(const HardArgs A) {
         T* const rows_p = TL ? static_cast<T*>(A.rowbuf) + A.rowbuf_off[p] : nullptr;
         T* const cols_p = TL ? static_cast<T*>(A.colbuf) + A.colbuf_off[p] : nullptr;
         const int ntc = TL ? (n + A.tile_w - 1) / A.tile_w : 1;   // TL: tiles per stripe
+        // GW: the walker lives in lane 0; each pass of the loop below refills the tile holding the
+        // next code the walk needs, then walks on until the path leaves it (other fills: one pass)
+        Walker wk;
+        uint8_t* const tilebuf = GW ? static_cast<uint8_t*>(A.scratch) + slot * A.scratch_stride : nullptr;
+        auto tile_code = [&](int ci, int cj) -> uint32_t {
+            const int w = ci - 1 - ts * GR, gg = w / R, rr = w - gg * R;
+            const int t = cj - tc * A.tile_w - 1 + gg;
+            return tilebuf[((int64_t(t >> 3) * G + gg) * 8 + (t & 7)) * R + rr];
+        };
+        if constexpr (GW) { if (lane == 0) wk.init(A.walk, p); }
+        // a monotone path crosses at most nstripes + ntc - 1 tiles: the bound only guards the loop
+        for (int pass = 0, more = 1; more && pass <= nstripes + ntc; ++pass) {
+            more = 0;
+            if constexpr (GW) {
+                const int wi = __shfl_sync(gmask, wk.i, 0), wj = __shfl_sync(gmask, wk.j, 0);
+                if (__shfl_sync(gmask, wk.done ? 1 : 0, 0)) break;
+                more = 1;
+                if (wi == 0 || wj == 0) {   // the rest is border moves: no codes
+                    if (lane == 0) wk.run(tile_code, 1, 1);
+                    continue;
+                }
+                ts = (wi - 1) / GR;
+                tc = (wj - 1) / A.tile_w;
+            }
         for (int s = TL ? ts : 0; s < (TL ? ts + 1 : nstripes); ++s) {
             // the previous stripe's bottom row (read) and this stripe's (written; one row in
             // place, except for tiles: a row per stripe)
@@ -345,7 +379,9 @@ __global__ void __launch_bounds__(128) hard_fill_kernel(const HardArgs A) {
             }
             T upM = ninf<T>(), upX = ninf<T>(), upY = ninf<T>();
             // TL: the tile's steps start (cmin - 1) steps into the stripe's full-width codes
-            uint8_t* cs = TL ? codes + int64_t(s) * ((n + G - 1 + 7) & ~7) * GR + int64_t((cmin - 1) >> 3) * G * 8 * R
+            uint8_t* cs = GW ? tilebuf
+                        : TL ? (codes ? codes + int64_t(s) * ((n + G - 1 + 7) & ~7) * GR + int64_t((cmin - 1) >> 3) * G * 8 * R
+                                      : nullptr)
                              : codes + (BAND ? soff : int64_t(s) * S8 * GR);
             // lane 0: the row above one column ahead, so the load is in flight meanwhile
             T nuM = ninf<T>(), nuX = ninf<T>(), nuY = ninf<T>();
@@ -428,7 +464,8 @@ __global__ void __launch_bounds__(128) hard_fill_kernel(const HardArgs A) {
                     }
                     // one coalesced store of this lane's R codes
                     uint8_t* dst = cs + ((int64_t(t >> 3) * G + lane) * 8 + (t & 7)) * R;
-                    if constexpr (R % 16 == 0) {
+                    if (TL && !cs) {
+                    } else if constexpr (R % 16 == 0) {
 #pragma unroll
                         for (int k = 0; k < R / 16; ++k)
                             reinterpret_cast<uint4*>(dst)[k] = make_uint4(w[4 * k], w[4 * k + 1], w[4 * k + 2], w[4 * k + 3]);
@@ -460,13 +497,13 @@ __global__ void __launch_bounds__(128) hard_fill_kernel(const HardArgs A) {
                     }
                     if (lane > 0) { upM = sM; upX = sX; upY = sY; }
                 }
-                if (lane == G - 1 && active && s + 1 < nstripes) {
+                if (!GW && lane == G - 1 && active && s + 1 < nstripes) {
                     bnd_out[3 * j] = cM[R - 1];
                     if constexpr (AFF) { bnd_out[3 * j + 1] = cX[R - 1]; bnd_out[3 * j + 2] = cY[R - 1]; }
                 }
             }
             if constexpr (TL) {   // the tile's last column, for the tile to its right
-                if (tc + 1 < ntc) {
+                if (!GW && tc + 1 < ntc) {
 #pragma unroll
                     for (int r = 0; r < R; ++r) {
                         const int q = lane * R + r;
@@ -474,7 +511,7 @@ __global__ void __launch_bounds__(128) hard_fill_kernel(const HardArgs A) {
                     }
                 }
             }
-            pmin = cmin; pmax = cmax;
+            if constexpr (!TL) { pmin = cmin; pmax = cmax; }   // tiles: the row above is whole
             soff += int64_t(S8) * GR;
             // the end cell (m, n): after the stripe each register holds column n (a banded
             // Global stripe holding row m always reaches column n)
@@ -524,6 +561,15 @@ __global__ void __launch_bounds__(128) hard_fill_kernel(const HardArgs A) {
                 if (lv > bestv) { bestv = lv; besti = li; bestj = lj; bests = ls; }
             }
             if constexpr (G > 1) __syncwarp(gmask);
+        }
+            if constexpr (GW) {   // walk on through the refilled tile
+                if (lane == 0) wk.run(tile_code, ts * GR + 1, tc * A.tile_w + 1);
+                __syncwarp(gmask);
+            }
+        }
+        if constexpr (GW) {
+            if (lane == 0) wk.finish();
+            continue;
         }
         if constexpr (!LOC) {
             if constexpr (G > 1) {

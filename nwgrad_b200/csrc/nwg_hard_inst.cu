@@ -26,7 +26,11 @@ HardFn pick_sg(Geo g) {
 template <class T, bool AFF, bool LOC, bool TR>
 HardFn pick(Geo g) {
     if (g.band) return pick_band<T, AFF, LOC, TR>(g);
-    if (g.tile) return (g.G == 32 && g.R == 8) ? &hard_fill_kernel<T, AFF, LOC, TR, 32, 8, false, false, true> : nullptr;
+    if (g.tile) {
+        if (g.G != 32 || g.R != 8) return nullptr;
+        if (g.grid) return &hard_fill_kernel<T, AFF, LOC, TR, 32, 8, false, false, true, true>;
+        return &hard_fill_kernel<T, AFF, LOC, TR, 32, 8, false, false, true>;
+    }
     if (g.mw > 1) return nullptr;
 #define NWG_H(GG, RR) if (g.G == GG && g.R == RR) return &hard_fill_kernel<T, AFF, LOC, TR, GG, RR>;
     NWG_H(1, 8) NWG_H(1, 16) NWG_H(1, 24) NWG_H(1, 32) NWG_H(32, 1) NWG_H(32, 2) NWG_H(32, 4) NWG_H(32, 8)

@@ -10,8 +10,9 @@ namespace nwg {
 using HardFn = void (*)(const HardArgs);
 using SoftFn = void (*)(const SoftArgs);
 // mw > 1: that many warps per pair (soft); post: the posterior-guide kernels (32 x 4, full DP,
-// untracked); tile: the hard fill over tiles of long pairs (32 x 8, a launch per anti-diagonal)
-struct Geo { int G, R; bool band = false; int mw = 0; bool post = false; bool tile = false; };
+// untracked); tile: the hard fill over tiles of long pairs (32 x 8, a launch per anti-diagonal);
+// grid (with tile): the grid traceback's walk, which refills the tiles its path crosses
+struct Geo { int G, R; bool band = false; int mw = 0; bool post = false; bool tile = false; bool grid = false; };
 // am: 0 Global, 1 Local, 2 semi-global ends (full DP, one warp or lane per pair)
 HardFn hard_fn_f32(bool aff, int am, bool tr, Geo g);
 HardFn hard_fn_f64(bool aff, int am, bool tr, Geo g);

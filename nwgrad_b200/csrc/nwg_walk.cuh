@@ -43,38 +43,54 @@ __device__ __forceinline__ uint8_t code_at(const uint8_t* codes, int i, int j, i
     return codes[base + ((int64_t(t >> 3) * G + g) * 8 + (t & 7)) * R + r];
 }
 
-static __device__ __noinline__ void walk_pair(const WalkArgs& A, const int p) {
-    const int64_t ao = A.oa[p], bo = A.ob[p];
-    const int m = int(A.oa[p + 1] - ao), n = int(A.ob[p + 1] - bo);
-    const uint8_t* ap = A.a + ao;
-    const uint8_t* bp = A.b + bo;
-    const uint16_t* tk = A.tracks ? A.tracks + ao : nullptr;
-    const uint16_t* gk = A.gtracks ? A.gtracks + ao + p : nullptr;
-    const int N = A.N;
-    const int64_t NN = int64_t(A.K) * N * N;
-    double* g = A.grad ? A.grad + A.gstride * p : nullptr;   // zeroed by the host
-    const uint8_t* codes = A.codes + A.code_off[p];
-    const int64_t* tab = A.stripe_tab ? A.stripe_tab + 2 * A.stripe_base[p] : nullptr;
-    const int lay = A.end[4 * p + 3];
-    const int G = lay >> 8, R = lay & 0xff;
-    auto tset = [&](int i) -> int { return tk ? int(tk[i - 1]) : 0; };
-    auto gset = [&](int i) -> int {
+// The walk of one pair as a resumable state: `run` walks from the current cell while the codes
+// it needs lie at rows >= ilo and columns >= jlo (the whole table: 1, 1), and stops where the
+// next code lies outside (the grid walk then refills the tile holding it) or at the path's start.
+struct Walker {
+    const WalkArgs* A;
+    int p, m, n, N, G, R;
+    int64_t NN;
+    const uint8_t* ap; const uint8_t* bp;
+    const uint16_t* tk; const uint16_t* gk;
+    double* g;
+    int32_t* gj;
+    uint8_t* mv;
+    int64_t nm;
+    int i, j, tbl;
+    bool done;
+
+    __device__ int tset(int ii) const { return tk ? int(tk[ii - 1]) : 0; }
+    __device__ int gset(int ii) const {
         if (!tk) return 0;
-        if (gk) return int(gk[i]);
-        return i == 0 ? (m ? int(tk[0]) : 0) : int(tk[i - 1]);
-    };
-    int32_t* gj = A.guide ? A.guide + ao + p : nullptr;
-    if (gj) {
-        for (int k = 0; k <= m; ++k) gj[k] = -1;
-        gj[0] = 0; gj[m] = n;
+        if (gk) return int(gk[ii]);
+        return ii == 0 ? (m ? int(tk[0]) : 0) : int(tk[ii - 1]);
     }
-    int i = A.end[4 * p], j = A.end[4 * p + 1];
-    int tbl = A.end[4 * p + 2];
-    if (gj) gj[i] = j;
-    uint8_t* mv = A.moves ? A.moves + A.moves_off[p] : nullptr;
-    int64_t nm = 0;
-    // emit one move out of (i, j): 0 M, 1 X (gap in B), 2 Y (gap in A)
-    auto emit = [&](int s, int ii, int jj, bool open) {
+    __device__ void init(const WalkArgs& W, int pair) {
+        A = &W; p = pair;
+        const int64_t ao = W.oa[p], bo = W.ob[p];
+        m = int(W.oa[p + 1] - ao); n = int(W.ob[p + 1] - bo);
+        ap = W.a + ao; bp = W.b + bo;
+        tk = W.tracks ? W.tracks + ao : nullptr;
+        gk = W.gtracks ? W.gtracks + ao + p : nullptr;
+        N = W.N;
+        NN = int64_t(W.K) * N * N;
+        g = W.grad ? W.grad + W.gstride * p : nullptr;   // zeroed by the host
+        const int lay = W.end[4 * p + 3];
+        G = lay >> 8; R = lay & 0xff;
+        gj = W.guide ? W.guide + ao + p : nullptr;
+        if (gj) {
+            for (int k = 0; k <= m; ++k) gj[k] = -1;
+            gj[0] = 0; gj[m] = n;
+        }
+        i = W.end[4 * p]; j = W.end[4 * p + 1];
+        tbl = W.end[4 * p + 2];
+        if (gj) gj[i] = j;
+        mv = W.moves ? W.moves + W.moves_off[p] : nullptr;
+        nm = 0;
+        done = false;
+    }
+    // one move out of (ii, jj): 0 M, 1 X (gap in B), 2 Y (gap in A)
+    __device__ void emit(int s, int ii, int jj, bool open) {
         if (mv) mv[nm] = uint8_t(s);
         ++nm;
         if (s == 0) {
@@ -94,66 +110,88 @@ static __device__ __noinline__ void walk_pair(const WalkArgs& A, const int p) {
                 if (open) g[o + 0] -= 1.0;
             }
         }
-    };
-    if (A.affine) {
-        while (true) {
-            if (i == 0 && j == 0) break;
-            uint32_t c;
-            if (A.local) {
-                c = (i == 0 || j == 0) ? 3u : code_at(codes, i, j, n, G, R, tab);
-                if (tbl == 0 && (c & 3u) == 3u) break;
-            } else {
-                // a free start ends the walk on its border; a charged border is one gap run
-                if (i == 0) { if (!(A.ends & 4)) for (; j > 0; --j) emit(2, 0, j, j == 1); break; }
-                if (j == 0) { if (!(A.ends & 1)) for (; i > 0; --i) emit(1, i, 0, i == 1); break; }
-                c = code_at(codes, i, j, n, G, R, tab);
+    }
+    template <class CodeFn>
+    __device__ void run(CodeFn code, int ilo, int jlo) {
+        const bool local = A->local != 0;
+        const int ends = A->ends;
+        if (A->affine) {
+            while (!done) {
+                if (i == 0 && j == 0) { done = true; break; }
+                uint32_t c;
+                if (local) {
+                    if (i > 0 && j > 0 && (i < ilo || j < jlo)) return;
+                    c = (i == 0 || j == 0) ? 3u : code(i, j);
+                    if (tbl == 0 && (c & 3u) == 3u) { done = true; break; }
+                } else {
+                    // a free start ends the walk on its border; a charged border is one gap run
+                    if (i == 0) { if (!(ends & 4)) for (; j > 0; --j) emit(2, 0, j, j == 1); done = true; break; }
+                    if (j == 0) { if (!(ends & 1)) for (; i > 0; --i) emit(1, i, 0, i == 1); done = true; break; }
+                    if (i < ilo || j < jlo) return;
+                    c = code(i, j);
+                }
+                if (i == 0) tbl = 2;
+                else if (j == 0) tbl = 1;
+                int prev;
+                auto from_code = [](uint32_t cc) { return cc == 1u ? 1 : (cc == 2u ? 2 : 0); };
+                if (tbl == 0) { prev = from_code(c & 3u); emit(0, i, j, false); --i; --j; }
+                else if (tbl == 1) { prev = from_code((c >> 2) & 3u); emit(1, i, j, prev != 1); --i; }
+                else { prev = from_code(c >> 4); emit(2, i, j, prev != 2); --j; }
+                tbl = prev;
             }
-            if (i == 0) tbl = 2;
-            else if (j == 0) tbl = 1;
-            int prev;
-            auto from_code = [](uint32_t cc) { return cc == 1u ? 1 : (cc == 2u ? 2 : 0); };
-            if (tbl == 0) { prev = from_code(c & 3u); emit(0, i, j, false); --i; --j; }
-            else if (tbl == 1) { prev = from_code((c >> 2) & 3u); emit(1, i, j, prev != 1); --i; }
-            else { prev = from_code(c >> 4); emit(2, i, j, prev != 2); --j; }
-            tbl = prev;
-        }
-    } else {
-        while (true) {
-            if (i == 0 && j == 0) break;
-            int k;
-            if (i == 0) k = (A.local || (A.ends & 4)) ? 3 : 2;
-            else if (j == 0) k = (A.local || (A.ends & 1)) ? 3 : 1;
-            else k = code_at(codes, i, j, n, G, R, tab);
-            if (k == 3) break;
-            if (k == 0) { emit(0, i, j, false); --i; --j; }
-            else if (k == 1) {
-                if (mv) mv[nm] = 1;
-                ++nm;
-                if (g) g[NN + 4 * tset(i) + 3] -= 1.0;
-                if (gj) gj[i - 1] = j;
-                --i;
-            } else {
-                if (mv) mv[nm] = 2;
-                ++nm;
-                if (g) g[NN + 4 * gset(i) + 1] -= 1.0;
-                --j;
+        } else {
+            while (!done) {
+                if (i == 0 && j == 0) { done = true; break; }
+                int k;
+                if (i == 0) k = (local || (ends & 4)) ? 3 : 2;
+                else if (j == 0) k = (local || (ends & 1)) ? 3 : 1;
+                else {
+                    if (i < ilo || j < jlo) return;
+                    k = code(i, j);
+                }
+                if (k == 3) { done = true; break; }
+                if (k == 0) { emit(0, i, j, false); --i; --j; }
+                else if (k == 1) {
+                    if (mv) mv[nm] = 1;
+                    ++nm;
+                    if (g) g[NN + 4 * tset(i) + 3] -= 1.0;
+                    if (gj) gj[i - 1] = j;
+                    --i;
+                } else {
+                    if (mv) mv[nm] = 2;
+                    ++nm;
+                    if (g) g[NN + 4 * gset(i) + 1] -= 1.0;
+                    --j;
+                }
             }
         }
     }
-    if (A.path_info) { A.path_info[3 * p] = int32_t(nm); A.path_info[3 * p + 1] = i; A.path_info[3 * p + 2] = j; }
-    if (gj) {
-        // interpolate the rows the path does not fix (aligner.hpp:2734-2749)
-        const int L = m + 1;
-        int lo = 0;
-        while (lo < L) {
-            if (gj[lo] < 0) { ++lo; continue; }
-            int hi = lo + 1;
-            while (hi < L && gj[hi] < 0) ++hi;
-            if (hi == L) { for (int k = lo + 1; k < L; ++k) gj[k] = gj[lo]; break; }
-            for (int k = lo + 1; k < hi; ++k) gj[k] = gj[lo] + (gj[hi] - gj[lo]) * (k - lo) / (hi - lo);
-            lo = hi;
+    __device__ void finish() {
+        if (A->path_info) { A->path_info[3 * p] = int32_t(nm); A->path_info[3 * p + 1] = i; A->path_info[3 * p + 2] = j; }
+        if (gj) {
+            // interpolate the rows the path does not fix (aligner.hpp:2734-2749)
+            const int L = m + 1;
+            int lo = 0;
+            while (lo < L) {
+                if (gj[lo] < 0) { ++lo; continue; }
+                int hi = lo + 1;
+                while (hi < L && gj[hi] < 0) ++hi;
+                if (hi == L) { for (int k = lo + 1; k < L; ++k) gj[k] = gj[lo]; break; }
+                for (int k = lo + 1; k < hi; ++k) gj[k] = gj[lo] + (gj[hi] - gj[lo]) * (k - lo) / (hi - lo);
+                lo = hi;
+            }
         }
     }
+};
+
+static __device__ __noinline__ void walk_pair(const WalkArgs& A, const int p) {
+    Walker w;
+    w.init(A, p);
+    const uint8_t* codes = A.codes + A.code_off[p];
+    const int64_t* tab = A.stripe_tab ? A.stripe_tab + 2 * A.stripe_base[p] : nullptr;
+    const int n = w.n, G = w.G, R = w.R;
+    w.run([&](int i, int j) -> uint32_t { return code_at(codes, i, j, n, G, R, tab); }, 1, 1);
+    w.finish();
 }
 
 }  // namespace nwg
