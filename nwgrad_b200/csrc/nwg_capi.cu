@@ -305,7 +305,7 @@ Geo pick_geo(bool soft, int rows, int n, int lanes, int rpl, bool lane_ok) {
 // pair's stripes) instead of one: a long pair is then not a single warp's serial work.  The
 // warps per pair grow with the pair's stripes (each warp keeps at least 3 stripes).
 constexpr int kLongRows = 1536;
-constexpr int kTileW = 256;   // columns per tile of a tiled long pair (a multiple of 8)
+constexpr int kTileW = 256;   // columns per tile of a tiled long pair (a multiple of 8; soft: of 32)
 int long_warps(int rows, int GR) {
     const int ns = (rows + GR - 1) / GR;
     return ns >= 64 ? 16 : ns >= 24 ? 8 : 4;
@@ -342,16 +342,17 @@ struct Plan {
     // hard, tiled long pairs: the tiles (p, s, c) of every tiled pair grouped by anti-diagonal
     // s + c (diagonal d: items diag_off[d] .. diag_off[d + 1] - 1); per pair (by index) its row
     // and column buffer offsets and first tile slot, in elements
+    // (soft: rows in columns, lane states, tiles and stripes; every stripe's partial too)
     std::vector<int32_t> tile_pairs;
     std::vector<int64_t> diag_off;
-    int64_t tile_row_elems = 0, tile_col_elems = 0, n_tiles = 0;
-    DBuf tile_items, tile_rowoff, tile_coloff, tile_slot, tile_plist, tile_count;
+    int64_t tile_row_elems = 0, tile_col_elems = 0, n_tiles = 0, n_tile_stripes = 0;
+    DBuf tile_items, tile_rowoff, tile_coloff, tile_slot, tile_plist, tile_count, tile_stripeoff, tile_nstripes;
     void reset() {
         order.release(); dcode_off.release(); stripe_base.release();
         tile_items.release(); tile_rowoff.release(); tile_coloff.release(); tile_slot.release();
-        tile_plist.release(); tile_count.release();
+        tile_plist.release(); tile_count.release(); tile_stripeoff.release(); tile_nstripes.release();
         valid = false; buckets.clear(); code_off.clear(); code_bytes = 0; n_stripes = 0;
-        tile_pairs.clear(); diag_off.clear(); tile_row_elems = tile_col_elems = n_tiles = 0;
+        tile_pairs.clear(); diag_off.clear(); tile_row_elems = tile_col_elems = n_tiles = n_tile_stripes = 0;
     }
 };
 
@@ -377,6 +378,8 @@ struct nwg_store {
     DBuf score, end, grad, guide, status, codes, scratch, part, red, moves, moves_off, path_info;
     DBuf trow, tcol, tbest, tcell;      // tiled long pairs: stripe rows, tile columns, Local tile bests
     DBuf tgrid;                         // grid traceback: one tile's codes per walking warp
+    // soft tiles: per-warp tables, rows, lane states, Z parts and per-pair Z, stripe partials
+    DBuf tl_table, tl_rowf, tl_rowb, tl_colf, tl_colb, tl_zpart, tl_zpair, tl_spart;
     int64_t gstride = 0;
     bool have_scores = false, have_grads = false, have_guides = false, have_paths = false;
     int last_grad_mode = 0, last_gm = -1, last_am = -1, last_prec = 0;
@@ -411,7 +414,7 @@ struct nwg_store {
     // soft weights per precision (kept: a captured graph reads them at a fixed address)
     DBuf swf, sgwf, swd, sgwd;
     // captured bucket sequences, replayed on a private stream ordered after the caller's
-    GraphCache g_soft[2], g_soft_band, g_hard[2], g_hard_band;
+    GraphCache g_soft[2], g_soft_band, g_hard[2], g_hard_band, g_soft_tile[2];
     bool use_graphs = true;
     cudaStream_t gstream = nullptr;
     cudaEvent_t gev_in = nullptr, gev_out = nullptr;
@@ -622,7 +625,9 @@ void build_plan(nwg_store* s, Plan& P, bool soft, int lanes, int rpl, int elem_b
                      : pick_geo(soft, std::max(rows, 1), nb, lanes, rpl, soft ? lane_ok_soft : true);
         if (!band && !lanes && !rpl) {
             if (s->plain) g = Geo{32, 4};
-            else if (soft && !s->tracked() && rows >= kLongRows && nb >= 256) g = Geo{32, 4, false, long_warps(rows, 128)};
+            else if (soft && !s->tracked() && rows >= kLongRows && nb >= 256)
+                // long pairs: tiles over the whole device; with semi-global ends, several warps
+                g = one_warp ? Geo{32, 4, false, long_warps(rows, 128)} : Geo{32, 4, false, 0, false, true};
             else if (!soft && !one_warp && rows >= kLongRows && nb >= 256)
                 g = Geo{32, 8, false, 0, false, true};   // long pairs: tiles over the whole device
             else if (sc < kClasses && cost_of[sc]) {
@@ -689,49 +694,57 @@ void build_plan(nwg_store* s, Plan& P, bool soft, int lanes, int rpl, int elem_b
                 off += (bytes + 15) & ~int64_t(15);
             }
         P.code_bytes = std::max<int64_t>(off, 16);
-        // tiled pairs: stripes of G R rows x tiles of kTileW columns; the tile (s, c) needs
-        // (s - 1, c) and (s, c - 1), both on the diagonal before its own
-        std::vector<int64_t> roff(size_t(n) + 1, 0), coff(size_t(n) + 1, 0), toff(size_t(n) + 1, 0);
-        std::vector<int32_t> tcount;
-        std::vector<std::vector<int32_t>> diags;
-        for (auto& B : P.buckets) {
-            if (!B.geo.tile) continue;
-            const int GR = B.geo.G * B.geo.R;
-            for (int32_t p : B.pairs) {
-                const int m = int(s->oa[p + 1] - s->oa[p]), nb = int(s->ob[p + 1] - s->ob[p]);
-                const int ns = (m + GR - 1) / GR, nt = (nb + kTileW - 1) / kTileW;
-                roff[p] = P.tile_row_elems; P.tile_row_elems += int64_t(ns) * 3 * (nb + 1);
-                coff[p] = P.tile_col_elems; P.tile_col_elems += int64_t(ns) * nt * 3 * GR;
-                toff[p] = P.n_tiles; P.n_tiles += int64_t(ns) * nt;
-                P.tile_pairs.push_back(p);
-                tcount.push_back(ns * nt);
-                if (int(diags.size()) < ns + nt - 1) diags.resize(size_t(ns + nt - 1));
-                for (int st = 0; st < ns; ++st)
-                    for (int c = 0; c < nt; ++c) {
-                        auto& dv = diags[size_t(st + c)];
-                        dv.push_back(p); dv.push_back(st); dv.push_back(c);
-                    }
-            }
+    }
+    // tiled pairs: stripes of G R rows x tiles of kTileW columns; the tile (s, c) needs
+    // (s - 1, c) and (s, c - 1), both on the diagonal before its own.  Hard: rows 1..m and
+    // columns 1..n, offsets in T; soft: rows 0..m and columns 0..n, offsets in columns, lane
+    // states, tiles and stripes (the kernel scales them by its own state sizes)
+    std::vector<int64_t> roff(size_t(n) + 1, 0), coff(size_t(n) + 1, 0), toff(size_t(n) + 1, 0);
+    std::vector<int64_t> soff(size_t(n) + 1, 0);
+    std::vector<int32_t> tcount, scount;
+    std::vector<std::vector<int32_t>> diags;
+    for (auto& B : P.buckets) {
+        if (!B.geo.tile) continue;
+        const int GR = B.geo.G * B.geo.R;
+        for (int32_t p : B.pairs) {
+            const int m = int(s->oa[p + 1] - s->oa[p]), nb = int(s->ob[p + 1] - s->ob[p]);
+            const int ns = soft ? (m + 1 + GR - 1) / GR : (m + GR - 1) / GR;
+            const int nt = soft ? nb / kTileW + 1 : (nb + kTileW - 1) / kTileW;
+            roff[p] = P.tile_row_elems; P.tile_row_elems += int64_t(ns) * (soft ? 1 : 3) * (nb + 1);
+            coff[p] = P.tile_col_elems; P.tile_col_elems += int64_t(ns) * nt * (soft ? B.geo.G : 3 * GR);
+            toff[p] = P.n_tiles; P.n_tiles += int64_t(ns) * nt;
+            soff[p] = P.n_tile_stripes; P.n_tile_stripes += ns;
+            P.tile_pairs.push_back(p);
+            tcount.push_back(ns * nt);
+            scount.push_back(ns);
+            if (int(diags.size()) < ns + nt - 1) diags.resize(size_t(ns + nt - 1));
+            for (int st = 0; st < ns; ++st)
+                for (int c = 0; c < nt; ++c) {
+                    auto& dv = diags[size_t(st + c)];
+                    dv.push_back(p); dv.push_back(st); dv.push_back(c);
+                }
         }
-        if (!P.tile_pairs.empty()) {
-            std::vector<int32_t> items;
-            items.reserve(size_t(P.n_tiles) * 3);
-            P.diag_off.assign(1, 0);
-            for (auto& dv : diags) {
-                items.insert(items.end(), dv.begin(), dv.end());
-                P.diag_off.push_back(int64_t(items.size() / 3));
-            }
-            auto up = [](DBuf& d, const void* h, size_t bytes) {
-                d.need(bytes);
-                NWG_CUDA(cudaMemcpy(d.p, h, bytes, cudaMemcpyHostToDevice));
-            };
-            up(P.tile_items, items.data(), items.size() * 4);
-            up(P.tile_rowoff, roff.data(), roff.size() * 8);
-            up(P.tile_coloff, coff.data(), coff.size() * 8);
-            up(P.tile_slot, toff.data(), toff.size() * 8);
-            up(P.tile_plist, P.tile_pairs.data(), P.tile_pairs.size() * 4);
-            up(P.tile_count, tcount.data(), tcount.size() * 4);
+    }
+    if (!P.tile_pairs.empty()) {
+        std::vector<int32_t> items;
+        items.reserve(size_t(P.n_tiles) * 3);
+        P.diag_off.assign(1, 0);
+        for (auto& dv : diags) {
+            items.insert(items.end(), dv.begin(), dv.end());
+            P.diag_off.push_back(int64_t(items.size() / 3));
         }
+        auto up = [](DBuf& d, const void* h, size_t bytes) {
+            d.need(bytes);
+            NWG_CUDA(cudaMemcpy(d.p, h, bytes, cudaMemcpyHostToDevice));
+        };
+        up(P.tile_items, items.data(), items.size() * 4);
+        up(P.tile_rowoff, roff.data(), roff.size() * 8);
+        up(P.tile_coloff, coff.data(), coff.size() * 8);
+        up(P.tile_slot, toff.data(), toff.size() * 8);
+        up(P.tile_plist, P.tile_pairs.data(), P.tile_pairs.size() * 4);
+        up(P.tile_count, tcount.data(), tcount.size() * 4);
+        up(P.tile_stripeoff, soff.data(), soff.size() * 8);
+        up(P.tile_nstripes, scount.data(), scount.size() * 4);
     }
     P.n_planned = int64_t(order.size());
     P.order.need(size_t(std::max<int64_t>(n, 1)) * 4);
@@ -1069,6 +1082,86 @@ void soft_weights(const nwg_store* s, const nwg_job& J, std::vector<T>& w, std::
 }
 
 // One soft pass (precision T) over `subset` (all pairs when null).
+// The soft pass over tiled long pairs (soft_kernel<..., TL>): a launch per anti-diagonal of
+// tiles in the forward phase, Z per pair, a launch per anti-diagonal in reverse order in the
+// backward phase (each tile recomputes its own forward table), then every pair's totals; one
+// captured sequence, replayed while the plan and buffers stay.
+template <class T>
+void soft_tile_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const Plan& P, const DBuf& dw, const DBuf& dgw,
+                    int renorm, bool loc, bool aff) {
+    const Geo tg{32, 4, false, 0, false, true};
+    SoftFn fn = soft_fn_rt<T>(aff, loc ? 1 : 0, false, tg);
+    if (!fn) throw Error(NWG_EINVAL, "no soft kernel for this geometry");
+    const int K = s->K, N = s->N, G = 32, R = 4, NV = aff ? 3 : 1, BW = aff ? 4 : 2, LS = NV * R + 1;
+    const int block = 128, gpb = block / G;
+    const size_t smem = nwg::soft_smem_bytes(K, N, G, R, block, int(sizeof(T)), false, false);
+    if (smem > 227 * 1024) throw Error(NWG_EINVAL, "soft: the alphabet / parameter sets do not fit shared memory");
+    NWG_CUDA(nwg::allow_smem(reinterpret_cast<const void*>(fn), smem));
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, block, smem);
+    occ = std::max(occ, 1);
+    const int sms = sm_count(s->device);
+    // per warp: one tile's forward table (its steps x G lanes x NV R values) and exponents
+    const int64_t steps = kTileW + G;
+    const int64_t fwd_bytes = (steps * G * NV * R * int64_t(sizeof(T)) + 255) & ~int64_t(255);
+    const int64_t exp_bytes = (steps * G * 4 + 255) & ~int64_t(255);
+    const int64_t stride = fwd_bytes + exp_bytes;
+    const int64_t max_blocks = int64_t(sms) * occ;
+    const int64_t nt = int64_t(P.tile_pairs.size());
+    s->tl_table.need(size_t(max_blocks * gpb * stride), st);
+    s->tl_rowf.need(size_t(std::max<int64_t>(P.tile_row_elems, 1)) * BW * sizeof(T), st);
+    s->tl_rowb.need(size_t(std::max<int64_t>(P.tile_row_elems, 1)) * BW * sizeof(T), st);
+    s->tl_colf.need(size_t(std::max<int64_t>(P.tile_col_elems, 1)) * LS * sizeof(T), st);
+    s->tl_colb.need(size_t(std::max<int64_t>(P.tile_col_elems, 1)) * LS * sizeof(T), st);
+    s->tl_zpart.need(size_t(std::max<int64_t>(P.n_tiles, 1)) * 16, st);
+    s->tl_zpair.need(size_t(std::max<int64_t>(s->n, 1)) * 16, st);
+    const int64_t part_bytes = P.n_tile_stripes * (s->gstride + 1) * 8;
+    s->tl_spart.need(size_t(std::max<int64_t>(part_bytes, 8)), st);
+    NWG_CUDA(cudaMemsetAsync(s->tl_spart.p, 0, size_t(part_bytes), st));
+    nwg::SoftArgs A{};
+    A.a = s->a.as<uint8_t>(); A.oa = s->doa.as<int64_t>();
+    A.b = s->b.as<uint8_t>(); A.ob = s->dob.as<int64_t>();
+    A.w = dw.p; A.gw = dgw.p; A.N = N; A.K = K;
+    A.scratch = s->tl_table.p; A.scratch_stride = stride; A.fwd_bytes = fwd_bytes;
+    A.maxn = 0; A.ck = 1; A.max_stripes = 1; A.bnd_off = 0; A.warp_stride = 0;
+    A.renorm_mask = renorm - 1;
+    A.temperature = J.temperature;
+    A.score = s->score.as<double>(); A.grad = s->grad.as<double>(); A.gstride = s->gstride;
+    A.status = s->status.as<int32_t>();
+    A.spin_limit = s->spin_limit;
+    A.queue = s->queue(nwg_store::kQueueHard - 1, st);   // the tile launches run in order: one queue
+    A.tile_w = kTileW;
+    A.rowf = s->tl_rowf.p; A.rowb = s->tl_rowb.p; A.row_off = P.tile_rowoff.as<int64_t>();
+    A.colf = s->tl_colf.p; A.colb = s->tl_colb.p; A.col_off = P.tile_coloff.as<int64_t>();
+    A.zpart = s->tl_zpart.as<double>(); A.tile_off = P.tile_slot.as<int64_t>();
+    A.zpair = s->tl_zpair.as<double>();
+    A.spart = s->tl_spart.as<double>(); A.stripe_off = P.tile_stripeoff.as<int64_t>();
+    std::vector<Launch> L;
+    const size_t nd = P.diag_off.size() - 1;
+    auto diag = [&](size_t d, int phase) {
+        const int64_t cnt = P.diag_off[d + 1] - P.diag_off[d];
+        A.tiles = P.tile_items.as<int32_t>() + 3 * P.diag_off[d];
+        A.n_items = cnt;
+        A.tl_phase = phase;
+        const int64_t blocks = std::min<int64_t>((cnt + gpb - 1) / gpb, max_blocks);
+        L.push_back(make_launch(reinterpret_cast<const void*>(fn), unsigned(blocks), block, smem, A));
+    };
+    for (size_t d = 0; d < nd; ++d) diag(d, 0);
+    nwg::TileSoftArgs Z{};
+    Z.pairs = P.tile_plist.as<int32_t>(); Z.n_pairs = nt;
+    Z.tile_off = P.tile_slot.as<int64_t>(); Z.tiles_of = P.tile_count.as<int32_t>();
+    Z.zpart = s->tl_zpart.as<double>(); Z.zpair = s->tl_zpair.as<double>();
+    Z.stripe_off = P.tile_stripeoff.as<int64_t>(); Z.stripes_of = P.tile_nstripes.as<int32_t>();
+    Z.spart = s->tl_spart.as<double>(); Z.gw = dgw.p;
+    Z.status = s->status.as<int32_t>(); Z.score = s->score.as<double>(); Z.grad = s->grad.as<double>();
+    Z.gstride = s->gstride; Z.K = K; Z.N = N; Z.local = loc ? 1 : 0; Z.affine = aff ? 1 : 0;
+    Z.temperature = J.temperature;
+    L.push_back(make_launch(reinterpret_cast<const void*>(&nwg::tile_z_kernel<T>), unsigned((nt + 127) / 128), 128, 0, Z));
+    for (size_t d = nd; d-- > 0;) diag(d, 1);
+    L.push_back(make_launch(reinterpret_cast<const void*>(&nwg::tile_finish_kernel<T>), unsigned(nt), 128, 0, Z));
+    run_launches(s, &s->g_soft_tile[sizeof(T) == 4 ? 0 : 1], L, st);
+}
+
 template <class T>
 void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vector<int32_t>* subset) {
     const bool aff = J.gap_model == 1, loc = J.mode == 1, tr = s->tracked();
@@ -1135,7 +1228,8 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
     } else {
         P = &s->soft_plan;
         // posterior guides: every pair at 32 x 4, one warp (the POST kernels)
-        build_plan(s, *P, true, J.soft_post ? 32 : J.lanes, J.soft_post ? 4 : J.rows, sizeof(T));
+        build_plan(s, *P, true, J.soft_post ? 32 : J.lanes, J.soft_post ? 4 : J.rows, sizeof(T), false, 0,
+                   J.mode == 2 && J.free_ends != 0);
     }
     DBuf sub_order;
     struct Free1 { DBuf& a; cudaStream_t st; ~Free1() { a.release(st); } } fr1{sub_order, st};
@@ -1153,7 +1247,7 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
     std::vector<int64_t> need;   // scratch bytes of each launch
     int64_t scratch_total = 0;
     for (auto& B : P->buckets) {
-        if (B.pairs.empty()) continue;
+        if (B.pairs.empty() || B.geo.tile) continue;
         Geo gk = B.geo;
         gk.post = J.soft_post != 0;
         SoftFn fn = soft_fn_rt<T>(aff, (J.mode == 2 && J.free_ends) ? 2 : (loc ? 1 : 0), tr, gk);
@@ -1230,22 +1324,30 @@ void soft_pass(nwg_store* s, const nwg_job& J, cudaStream_t st, const std::vecto
         args.push_back(A);
         need.push_back(bucket_need);
     }
-    if (launches.empty()) return;
-    // the buckets run at once, each in its own part of the scratch, when their parts fit the
-    // budget together (a bucket of a few large pairs then shares the device with the others
-    // instead of running alone); else one after another in one shared part
-    int64_t sum = 0;
-    for (int64_t b : need) sum += b;
-    const bool concurrent = launches.size() > 1 && sum <= budget;
-    s->scratch.need(size_t(concurrent ? sum : scratch_total), st);
-    int64_t off = 0;
-    for (size_t k = 0; k < launches.size(); ++k) {
-        args[k].scratch = static_cast<unsigned char*>(s->scratch.p) + (concurrent ? off : 0);
-        off += need[k];
-        std::memcpy(launches[k].arg.data(), &args[k], sizeof(nwg::SoftArgs));
+    if (!launches.empty()) {
+        // the buckets run at once, each in its own part of the scratch, when their parts fit the
+        // budget together (a bucket of a few large pairs then shares the device with the others
+        // instead of running alone); else one after another in one shared part
+        int64_t sum = 0;
+        for (int64_t b : need) sum += b;
+        const bool concurrent = launches.size() > 1 && sum <= budget;
+        s->scratch.need(size_t(concurrent ? sum : scratch_total), st);
+        int64_t off = 0;
+        for (size_t k = 0; k < launches.size(); ++k) {
+            args[k].scratch = static_cast<unsigned char*>(s->scratch.p) + (concurrent ? off : 0);
+            off += need[k];
+            std::memcpy(launches[k].arg.data(), &args[k], sizeof(nwg::SoftArgs));
+        }
+        GraphCache* gc = subset ? nullptr : J.band >= 0 ? &s->g_soft_band : &s->g_soft[sizeof(T) == 4 ? 0 : 1];
+        run_launches(s, gc, launches, st, concurrent);
     }
-    GraphCache* gc = subset ? nullptr : J.band >= 0 ? &s->g_soft_band : &s->g_soft[sizeof(T) == 4 ? 0 : 1];
-    run_launches(s, gc, launches, st, concurrent);
+    if (!subset && !P->tile_pairs.empty() && !ovf)
+        soft_tile_pass<T>(s, J, st, *P, dw, dgw, renorm, loc, aff);
+    else if (!subset && !P->tile_pairs.empty()) {
+        mark_status_kernel<<<unsigned((P->tile_pairs.size() + 255) / 256), 256, 0, st>>>(
+            P->tile_plist.as<int32_t>(), int64_t(P->tile_pairs.size()), s->status.as<int32_t>(), nwg::kSoftWeights);
+        NWG_CUDA(cudaGetLastError());
+    }
 }
 
 // The reason a soft pass refused a pair, from its status bits (the first that applies).
@@ -1440,10 +1542,12 @@ int nwg_store_destroy(nwg_store* s) {
                         &s->stripe_tab, &s->codes, &s->scratch, &s->part, &s->red, &s->moves,
                         &s->moves_off, &s->path_info, &s->tmatf, &s->tgapf, &s->tmatd, &s->tgapd,
                         &s->tbx0f, &s->tbx0d, &s->tscore, &s->tend, &s->hb_pairs, &s->swf, &s->sgwf,
-                        &s->swd, &s->sgwd})
+                        &s->swd, &s->sgwd, &s->wq, &s->trow, &s->tcol, &s->tbest, &s->tcell, &s->tgrid,
+                        &s->tl_table, &s->tl_rowf, &s->tl_rowb, &s->tl_colf, &s->tl_colb, &s->tl_zpart,
+                        &s->tl_zpair, &s->tl_spart})
             b->release();
         for (GraphCache* g : {&s->g_soft[0], &s->g_soft[1], &s->g_soft_band, &s->g_hard[0], &s->g_hard[1],
-                              &s->g_hard_band})
+                              &s->g_hard_band, &s->g_soft_tile[0], &s->g_soft_tile[1]})
             g->reset();
         if (s->gstream) cudaStreamDestroy(s->gstream);
         for (int k = 0; k < nwg_store::kBucketStreams; ++k) {

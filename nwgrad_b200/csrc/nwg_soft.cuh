@@ -71,6 +71,24 @@ struct SoftArgs {
     int spin_limit;                          // several warps per pair: polls before a wait gives up
     int* queue;                              // this launch's work-queue counters (2 ints, zero at launch)
     int32_t* post;                           // POST kernels: per pair m + 1 posterior guide columns at oa[p] + p
+    // tiled long pairs (TL kernels): an item is one tile -- stripe s of pair p over columns
+    // c W .. c W + W - 1 -- and a launch holds one anti-diagonal s + c of every pair's tiles, in
+    // the forward phase (0) or, in reverse diagonal order, the backward phase (1)
+    const int32_t* tiles;                    // per item: p, s, c
+    int tile_w;                              // W, a multiple of 32
+    int tl_phase;
+    void* rowf; void* rowb;                  // per pair, per stripe: the forward bottom row and the
+    const int64_t* row_off;                  // backward top row, (n + 1) x BW T; offset per pair in
+                                             // columns (x BW: T)
+    void* colf; void* colb;                  // per pair, per (stripe, tile): every lane's forward state
+    const int64_t* col_off;                  // at the tile's last column / backward state at its first
+                                             // (G x (NV R + 1) T, the exponent as T's bits); offset per
+                                             // pair in lane states (x (NV R + 1): T)
+    double* zpart; const int64_t* tile_off;  // Local: per tile its part of Z (m, e); offset per pair in tiles
+    double* zpair;                           // per pair: Z as (m, e) once the forward phase is done
+    double* spart; const int64_t* stripe_off;   // per pair, per stripe: its counts (gstride doubles)
+                                                // and lost-mass charge (1 more), added tile by tile;
+                                                // offset per pair in stripes
 };
 
 // Per-pair status bits of a soft pass: a refused pair's score and counts are not written and
@@ -242,11 +260,19 @@ constexpr int kPrefetchSteps = NWG_SOFT_PREFETCH_STEPS;
 // per row, the column of greatest exit mass -- the cell's posterior less the posterior of moving
 // on to (i, j+1) within the row (affine: the Y posterior there; linear: F e_a B(i, j+1)), the
 // first such column on ties -- and the pair's guide is their running maximum over the rows.
+// TL: tiled long pairs (SoftArgs::tiles, one phase per launch).  Forward: the tile's lanes start
+// from the tile to the left's saved last column and the row above from the stripe above's bottom
+// row; the tile leaves its own bottom row and last column, and its part of Z.  Backward (tiles in
+// reverse diagonal order): the tile recomputes its forward table from the same inputs (the same
+// bits), starts from the tile to the right's saved first column and the row below from the
+// stripe below's top row, and adds its counts into its stripe's partial; tile_z_kernel and
+// tile_finish_kernel form Z and each pair's totals between and after the phases.
 template <class T, bool AFF, bool LOC, bool TR, int G, int R, bool MW = false, bool BAND = false, bool SG = false,
-          bool POST = false>
+          bool POST = false, bool TL = false>
 __global__ void __launch_bounds__(MW ? 512 : 128, (POST ? 3 : MW ? 1 : (G > 1 ? (R >= 8 ? 2 : 4) : 1)))
 soft_kernel(const SoftArgs A) {
     static_assert(!POST || (G == 32 && R == 4 && !MW && !BAND && !TR), "posterior guides: 32 x 4, untracked, full DP");
+    static_assert(!TL || (G == 32 && !MW && !BAND && !SG && !TR && !POST), "tiles: 32 lanes, untracked, full DP, Global or Local");
     static_assert(!MW || (G == 32 && !TR), "several warps per pair: 32 lanes, untracked");
     static_assert(!BAND || (G == 32 && !MW), "banded: 32 lanes, one warp per pair");
     static_assert(!SG || !LOC, "semi-global ends: Global kernels");
@@ -300,7 +326,7 @@ soft_kernel(const SoftArgs A) {
     T* fwd = reinterpret_cast<T*>(sbase + (MW ? gib * A.warp_stride : 0));
     int* fexp = reinterpret_cast<int*>(reinterpret_cast<unsigned char*>(fwd) + A.fwd_bytes);
     const int64_t nb = int64_t(A.maxn) + 1;
-    const bool ck = MW || A.ck != 0;
+    const bool ck = MW || TL || A.ck != 0;
     const int nbrows = ck ? A.max_stripes : 1;              // forward boundary rows kept
     const int nbrows_b = MW ? A.max_stripes : 1;            // backward boundary rows kept
     unsigned char* bb = sbase + A.bnd_off;
@@ -351,7 +377,8 @@ soft_kernel(const SoftArgs A) {
         }
     };
     for (int64_t it = next_item(); it < A.n_items; it = next_item()) {
-        const int p = A.order[it];
+        const int p = TL ? A.tiles[3 * it] : A.order[it];
+        const int ts = TL ? A.tiles[3 * it + 1] : 0, tc = TL ? A.tiles[3 * it + 2] : 0;   // TL: stripe, tile
         const int64_t ao = A.oa[p], bo = A.ob[p];
         const int m = int(A.oa[p + 1] - ao), n = int(A.ob[p + 1] - bo);
         const uint8_t* __restrict__ ap = A.a + ao;
@@ -388,8 +415,17 @@ soft_kernel(const SoftArgs A) {
             }
             bcols = jhi_of(0);
         }
-        const int S = n + G;                    // steps: columns 0..n plus the skew
+        // the stripe's columns [tc0, tc1] (TL: the tile's) and steps: its columns plus the skew
+        const int tc0 = TL ? tc * A.tile_w : 0, tc1 = TL ? min(n, tc0 + A.tile_w - 1) : n;
+        const int ntc = TL ? n / A.tile_w + 1 : 1;   // TL: tiles per stripe (columns 0..n)
+        const int S = tc1 - tc0 + G;
         const int SP = S + 1;                   // MW: progress key per stripe
+        // TL: this pair's rows (stride n + 1), per-tile lane states and per-stripe partials
+        T* const rowf_p = TL ? static_cast<T*>(A.rowf) + A.row_off[p] * BW : nullptr;
+        T* const rowb_p = TL ? static_cast<T*>(A.rowb) + A.row_off[p] * BW : nullptr;
+        constexpr int LS = NV * R + 1;          // TL: one lane's saved state (values, exponent)
+        T* const colf_p = TL ? static_cast<T*>(A.colf) + A.col_off[p] * LS : nullptr;
+        T* const colb_p = TL ? static_cast<T*>(A.colb) + A.col_off[p] * LS : nullptr;
         int why = 0;                            // kSoft* bits: why this pair is refused
         // semi-global ends (aligner.hpp:6362-6430): free starts on row 0 / column 0, Z over the
         // end cells (row m or (m, n), then column n of rows 0..m-1), the backward seeded with 1
@@ -413,8 +449,8 @@ soft_kernel(const SoftArgs A) {
             // a lane wholly below row m (the last stripe's padding) keeps no table: its backward
             // values are zero, so its forward values are never needed
             const bool store_table = (!ck || !pass1) && i0 <= m;
-            T* const fb_in = fbnd + (ck ? int64_t(s - 1) * BW * nb : 0);
-            T* const fb_out = fbnd + (ck ? int64_t(s) * BW * nb : 0);
+            T* const fb_in = TL ? rowf_p + int64_t(s - 1) * BW * (n + 1) : fbnd + (ck ? int64_t(s - 1) * BW * nb : 0);
+            T* const fb_out = TL ? rowf_p + int64_t(s) * BW * (n + 1) : fbnd + (ck ? int64_t(s) * BW * nb : 0);
             int key[R];
             T roa[TR ? R : 1], rea[TR ? R : 1], rob[TR ? R : 1], reb[TR ? R : 1];
             T vmask[R];
@@ -451,7 +487,18 @@ soft_kernel(const SoftArgs A) {
             T upM = T(0), upX = T(0), upY = T(0); // row above, column j
             T* fs = fwd + (ck ? 0 : int64_t(s) * S * G * CV);
             int* fe = fexp + (ck ? 0 : int64_t(s) * S * G);
-            int nbj = N;
+            int nbj = tc0 > 0 ? int(bp[tc0 - 1]) : N;   // the first column's b code (column 0: none)
+            // TL: this lane's state at the column left of the tile, as the tile to the left left it
+            const T* const lst = (TL && tc > 0) ? colf_p + (int64_t(s) * ntc + tc - 1) * G * LS : nullptr;
+            if (TL && tc > 0) {
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    cM[r] = lst[lane * LS + NV * r];
+                    if constexpr (AFF) { cX[r] = lst[lane * LS + NV * r + 1]; cY[r] = lst[lane * LS + NV * r + 2]; }
+                }
+                E = bits_exp(lst[lane * LS + LS - 1]);
+                lone = pow2s<T>(-E);
+            }
             // the row above (the previous stripe's bottom row): one lane per pair reads it one
             // column ahead; a group loads it G columns at a time, one segment ahead (rb), into
             // the staging row lane 0 reads
@@ -459,7 +506,7 @@ soft_kernel(const SoftArgs A) {
 #pragma unroll
             for (int k = 0; k < BW; ++k) rb[k] = T(0);
             auto load_seg = [&](int c0) {   // group: columns c0 .. c0 + G - 1 into rb
-                if (c0 + lane <= n) vload<T, BW>(rb, fb_in + int64_t(c0 + lane) * BW);
+                if (c0 + lane <= tc1) vload<T, BW>(rb, fb_in + int64_t(c0 + lane) * BW);
             };
             auto stage_seg = [&]() {        // group: rb into the staging row
                 __syncwarp(gmask);
@@ -510,15 +557,32 @@ soft_kernel(const SoftArgs A) {
                     if constexpr (AFF) { upX = scale_down(iX, d); upY = scale_down(iY, d); }
                 }
             };
+            if (TL && tc > 0) {
+                // the row above at the column left of the tile, into this lane's units: lane 0 from
+                // the stripe above's bottom row, the others from the lane above's saved last row
+                T v[BW];
+                if (lane == 0) {
+                    if (s > 0) vload<T, BW>(v, fb_in + int64_t(tc0 - 1) * BW);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < NV; ++k) v[k] = lst[(lane - 1) * LS + NV * (R - 1) + k];
+                    v[BW - 1] = lst[(lane - 1) * LS + LS - 1];
+                }
+                if (lane > 0 || s > 0) {
+                    take_up(v[0], AFF ? v[1] : T(0), AFF ? v[2] : T(0), bits_exp(v[BW - 1]));
+                    dgM = upM; dgX = upX; dgY = upY;
+                    upM = T(0); upX = T(0); upY = T(0);
+                }
+            }
             if (s > 0) {
                 if constexpr (G == 1) {
                     load_seg(0);
                     take_up(rb[0], AFF ? rb[1] : T(0), AFF ? rb[2] : T(0), bits_exp(rb[BW - 1]));
                     load_seg(1);
                 } else {
-                    load_seg(0);
+                    load_seg(tc0);
                     stage_seg();
-                    load_seg(G);
+                    load_seg(tc0 + G);
                     if (lane == 0) {
                         T v[BW];
                         vload<T, BW>(v, str);
@@ -527,10 +591,10 @@ soft_kernel(const SoftArgs A) {
                 }
             }
             for (int t = 0; t < S; ++t) {
-                const int j = t - lane;           // column 0..n
+                const int j = tc0 + t - lane;     // column tc0..tc1 (the full DP: 0..n)
                 if (waits && t > 0 && (t & 31) == 0) wait_for((s - 1) * SP + min(S, t + 4 * G + 1));
                 if (MW && pass1 && t > 0 && (t & 7) == 0) publish(s * SP + t);   // steps 0 .. t-1 done
-                const bool active = (j >= 0) && (j <= n);
+                const bool active = (j >= tc0) && (j <= tc1);
                 if (active) {
                     const int bj = nbj;                   // column 0: the zero column
                     nbj = j < n ? int(bp[j]) : N;         // the next column's code, one step ahead
@@ -590,7 +654,7 @@ soft_kernel(const SoftArgs A) {
                         }
                     }
                     dgM = upM; dgX = upX; dgY = upY;
-                    if ((t & rmask) == 0 || j == n) {
+                    if ((t & rmask) == 0 || j == tc1) {
                         // renormalise: the lane's largest value into [1, 2)
                         T mx = T(0);
 #pragma unroll
@@ -629,7 +693,7 @@ soft_kernel(const SoftArgs A) {
                 }
                 // this stripe's bottom row (lane G-1's column t - G + 1) for the stripe below
                 if (pass1 && s + 1 < nstripes) {
-                    const int c = t - (G - 1);
+                    const int c = tc0 + t - (G - 1);
                     T v[BW];
                     v[0] = cM[R - 1];
                     if constexpr (AFF) { v[1] = cX[R - 1]; v[2] = cY[R - 1]; }
@@ -637,8 +701,8 @@ soft_kernel(const SoftArgs A) {
                     if constexpr (G == 1) {
                         if (c >= 0) vstore<T, BW>(fb_out + int64_t(c) * BW, v);
                     } else {
-                        if (lane == G - 1 && c >= 0) vstore<T, BW>(stw + (c & (G - 1)) * 4, v);
-                        if (c >= 0 && ((c & (G - 1)) == G - 1 || c == n)) {   // a full segment (or the last)
+                        if (lane == G - 1 && c >= tc0) vstore<T, BW>(stw + (c & (G - 1)) * 4, v);
+                        if (c >= tc0 && ((c & (G - 1)) == G - 1 || c == tc1)) {   // a full segment (or the last)
                             __syncwarp(gmask);
                             const int cc = c - (c & (G - 1)) + lane;
                             if (cc <= c) {
@@ -659,8 +723,8 @@ soft_kernel(const SoftArgs A) {
                         sY = __shfl_up_sync(gmask, cY[R - 1], 1, G);
                     }
                     const int sE = __shfl_up_sync(gmask, E, 1, G);
-                    const int cn = t + 1;                 // lane 0's next column
-                    if (s > 0 && cn <= n && (cn & (G - 1)) == 0) {   // a new segment: stage it, load the next
+                    const int cn = tc0 + t + 1;           // lane 0's next column
+                    if (s > 0 && cn <= tc1 && (cn & (G - 1)) == 0) {   // a new segment: stage it, load the next
                         stage_seg();
                         load_seg(cn + G);
                     }
@@ -669,8 +733,8 @@ soft_kernel(const SoftArgs A) {
                     vload<T, BW>(v, str + (cn & (G - 1)) * 4);
                     // only for a column this lane still computes: a finished lane keeps its
                     // state (row m's values are Z), an idle one its empty exponent
-                    const int jn1 = t + 1 - lane;
-                    if (jn1 >= 0 && jn1 <= n && (!top || s > 0))
+                    const int jn1 = tc0 + t + 1 - lane;
+                    if (jn1 >= tc0 && jn1 <= tc1 && (!top || s > 0))
                         take_up(top ? v[0] : sM, top ? (AFF ? v[1] : T(0)) : sX, top ? (AFF ? v[2] : T(0)) : sY,
                                 top ? bits_exp(v[BW - 1]) : sE);
                 } else {
@@ -681,10 +745,19 @@ soft_kernel(const SoftArgs A) {
                 }
             }
             if (MW && pass1) publish(s * SP + S);
+            if (TL && pass1 && tc + 1 < ntc) {   // this lane's state at the tile's last column
+                T* const dst = colf_p + (int64_t(s) * ntc + tc) * G * LS + lane * LS;
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    dst[NV * r] = cM[r];
+                    if constexpr (AFF) { dst[NV * r + 1] = cX[r]; dst[NV * r + 2] = cY[r]; }
+                }
+                dst[LS - 1] = exp_bits(E, T(0));
+            }
             if (pass1) {
                 if (LOC || zsg) zacc.add(static_cast<double>(zpart), E);
                 if constexpr (!LOC) {
-                    if (m >= i0 && m < i0 + R) {
+                    if (m >= i0 && m < i0 + R && tc1 == n) {
 #pragma unroll
                         for (int r = 0; r < R; ++r)
                             if (i0 + r == m) { zM = cM[r]; zX = cX[r]; zY = cY[r]; zE = E; }
@@ -693,7 +766,8 @@ soft_kernel(const SoftArgs A) {
             }
             if constexpr (G > 1) __syncwarp(gmask);
         };
-        for (int s = MW ? gib : 0; s < nstripes; s += NWp) fwd_stripe(s, true);
+        if constexpr (TL) { if (A.tl_phase == 0) fwd_stripe(ts, true); }
+        else for (int s = MW ? gib : 0; s < nstripes; s += NWp) fwd_stripe(s, true);
         // Z = zhat * 2^EZ with zhat in [1, 2)
         double zm; int ze;
         if (LOC || zsg) {
@@ -717,6 +791,24 @@ soft_kernel(const SoftArgs A) {
             }
         }
         if constexpr (G > 1) why = __reduce_or_sync(gmask, why);
+        if constexpr (TL) {
+            if (A.tl_phase == 0) {
+                // the tile's part of Z (Local), or Z itself from the tile holding (m, n)
+                if (lane == 0) {
+                    if (LOC) {
+                        const int64_t q = A.tile_off[p] + int64_t(ts) * ntc + tc;
+                        A.zpart[2 * q] = zm; A.zpart[2 * q + 1] = double(ze);
+                    } else if (ts == nstripes - 1 && tc1 == n) {
+                        A.zpair[2 * p] = zm; A.zpair[2 * p + 1] = double(ze);
+                    }
+                    if (why) atomicOr(A.status + p, why);
+                }
+                continue;
+            }
+            // backward: the pair's Z (tile_z_kernel); a refused pair's tiles do nothing
+            zm = A.zpair[2 * p]; ze = int(A.zpair[2 * p + 1]);
+            if (A.status[p] != 0) continue;
+        }
         if constexpr (MW) {
             // every warp's part of Z: Global, the warp holding row m; Local, the sum in warp order
             stalled = __any_sync(gmask, stalled);
@@ -762,11 +854,11 @@ soft_kernel(const SoftArgs A) {
             double* g1 = A.grad + A.gstride * p;
             for (int k = 0; k < K * N * N; ++k) g1[k] = 0.0;
         }
-        for (int s = nstripes - 1 - (MW ? gib : 0); s >= 0; s -= NWp) {
+        for (int s = TL ? ts : nstripes - 1 - (MW ? gib : 0); s >= (TL ? ts : 0); s -= NWp) {
             if (ck) fwd_stripe(s, false);       // this stripe's forward table, from its checkpoint
             // this stripe's row below (read) and its own top row (written): MW keeps one per stripe
-            T* const bb_in = bbnd + (MW ? int64_t(s + 1) * BW * nb : 0);
-            T* const bb_out = bbnd + (MW ? int64_t(s) * BW * nb : 0);
+            T* const bb_in = TL ? rowb_p + int64_t(s + 1) * BW * (n + 1) : bbnd + (MW ? int64_t(s + 1) * BW * nb : 0);
+            T* const bb_out = TL ? rowb_p + int64_t(s) * BW * (n + 1) : bbnd + (MW ? int64_t(s) * BW * nb : 0);
             const int bkey = nstripes - 1 - s;   // MW: progress keys grow as the pass goes up
             const int i0 = s * GR + lane * R;
             int keyd[R], krow[R];
@@ -814,7 +906,7 @@ soft_kernel(const SoftArgs A) {
             // term, as B_M(m+1, n+1) = 1 with the padding weight w[K*N][N] = 1 (the cell and
             // everything else it reaches in the padding are zero), so no cell tests for it
             if constexpr (AFF && !LOC) {
-                if (s == nstripes - 1) {
+                if (s == nstripes - 1 && tc1 == n) {
                     const int rc = m - i0;
 #pragma unroll
                     for (int r = 1; r < R; ++r) bM[r] = (r == rc + 1) ? T(1) : bM[r];
@@ -822,6 +914,18 @@ soft_kernel(const SoftArgs A) {
                 }
             }
             T dnM = T(0), dnX = T(0), dnY = T(0);     // row below, column j
+            // TL: this lane's state at the column right of the tile, as the tile to the right left it
+            const T* const rst = (TL && tc1 < n) ? colb_p + (int64_t(s) * ntc + tc + 1) * G * LS : nullptr;
+            if (TL && tc1 < n) {
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    bM[r] = rst[lane * LS + NV * r];
+                    if constexpr (AFF) { bX[r] = rst[lane * LS + NV * r + 1]; bY[r] = rst[lane * LS + NV * r + 2]; }
+                    else { bX[r] = bM[r]; bY[r] = bM[r]; }
+                }
+                EB = bits_exp(rst[lane * LS + LS - 1]);
+                lone = pow2s<T>(-EB);
+            }
             const T* fs = fwd + (ck ? 0 : int64_t(s) * S * G * CV);
             const int* fe = fexp + (ck ? 0 : int64_t(s) * S * G);
             // a lane wholly below row m has no table (its backward values are zero): it reads
@@ -839,7 +943,7 @@ soft_kernel(const SoftArgs A) {
 #pragma unroll
             for (int k = 0; k < BW; ++k) rb[k] = T(0);
             auto load_seg = [&](int d0) {   // group: distances d0 .. d0 + G - 1 into rb
-                if (d0 + lane <= n) vload<T, BW>(rb, bb_in + int64_t(n - d0 - lane) * BW);
+                if (d0 + lane <= tc1 - tc0) vload<T, BW>(rb, bb_in + int64_t(tc1 - d0 - lane) * BW);
             };
             auto stage_seg = [&]() {
                 __syncwarp(gmask);
@@ -887,6 +991,24 @@ soft_kernel(const SoftArgs A) {
                 }
                 if constexpr (!AFF) { dnX = dnM; dnY = dnM; }
             };
+            if (TL && tc1 < n) {
+                // the row below at the column right of the tile (its M enters the diagonal term),
+                // into this lane's units: lane G-1 from the stripe below's top row, the others from
+                // the lane below's saved first row
+                T v[BW];
+                if (lane == G - 1) {
+                    if (s < nstripes - 1) vload<T, BW>(v, bb_in + int64_t(tc1 + 1) * BW);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < NV; ++k) v[k] = rst[(lane + 1) * LS + k];
+                    v[BW - 1] = rst[(lane + 1) * LS + LS - 1];
+                }
+                if (lane < G - 1 || s < nstripes - 1) {
+                    take_dn(v[0], AFF ? v[1] : T(0), AFF ? v[2] : T(0), bits_exp(v[BW - 1]));
+                    dgM = dnM;
+                    dnM = T(0); dnX = T(0); dnY = T(0);
+                }
+            }
             if (s < nstripes - 1) {
                 if constexpr (G == 1) {
                     load_seg(0);
@@ -904,11 +1026,11 @@ soft_kernel(const SoftArgs A) {
                 }
             }
             for (int t = 0; t < S; ++t) {
-                const int j = n - t + (G - 1 - lane);     // column n..0
+                const int j = tc1 - t + (G - 1 - lane);   // column tc1..tc0 (the full DP: n..0)
                 if constexpr (kPrefetchSteps > 0) {
-                    // every lane reads table row n + G - 1 - t at step t (its column j plus its
-                    // lane index): the row kPrefetchSteps ahead goes to L2 now
-                    const int u = n + G - 1 - t - kPrefetchSteps;
+                    // every lane reads table row j - tc0 + lane at step t: the row kPrefetchSteps
+                    // steps ahead goes to L2 now
+                    const int u = tc1 - tc0 + G - 1 - t - kPrefetchSteps;
                     if (lane == 0 && u >= 0) {
                         prefetch_l2_bulk(fs + int64_t(u) * G * CV, unsigned(G * CV * sizeof(T)));
                         if constexpr ((G * sizeof(int)) % 16 == 0) prefetch_l2_bulk(fe + int64_t(u) * G, unsigned(G * sizeof(int)));
@@ -917,14 +1039,14 @@ soft_kernel(const SoftArgs A) {
                 }
                 if (bwaits && t > 0 && (t & 31) == 0) wait_for((bkey - 1) * SP + min(S, t + 4 * G + 1));
                 if (MW && t > 0 && (t & 7) == 0) publish(bkey * SP + t);
-                const bool active = (j >= 0) && (j <= n);
+                const bool active = (j >= tc0) && (j <= tc1);
                 if (active) {
                     // this column's forward values were loaded one step ahead (or now, on
                     // the lane's first step); issue the next column's loads before the math
                     if (!have_next) {
                         if (lane_rows) {
-                            vload_ro<T, CV>(nf, fs + (int64_t(j + lane) * G + lane) * CV);
-                            nEF = __ldg(fe + int64_t(j + lane) * G + lane);
+                            vload_ro<T, CV>(nf, fs + (int64_t(j - tc0 + lane) * G + lane) * CV);
+                            nEF = __ldg(fe + int64_t(j - tc0 + lane) * G + lane);
                         }
                         nbj = j < n ? int(bp[j]) : N;
                     }
@@ -933,11 +1055,11 @@ soft_kernel(const SoftArgs A) {
                     for (int k = 0; k < CV; ++k) f[k] = nf[k];
                     const int EF = nEF;
                     const int bj1 = nbj;              // b code of column j+1 (N: none)
-                    have_next = j > 0;
+                    have_next = j > tc0;
                     if (have_next) {
                         if (lane_rows) {
-                            vload_ro<T, CV>(nf, fs + (int64_t(j - 1 + lane) * G + lane) * CV);
-                            nEF = __ldg(fe + int64_t(j - 1 + lane) * G + lane);
+                            vload_ro<T, CV>(nf, fs + (int64_t(j - 1 - tc0 + lane) * G + lane) * CV);
+                            nEF = __ldg(fe + int64_t(j - 1 - tc0 + lane) * G + lane);
                         }
                         nbj = int(bp[j - 1]);
                     }
@@ -1070,7 +1192,7 @@ soft_kernel(const SoftArgs A) {
                         }
                     }
                     dgM = dnM;
-                    if ((t & rmask) == 0 || j == 0) {
+                    if ((t & rmask) == 0 || j == tc0) {
                         T mx = T(0);
 #pragma unroll
                         for (int r = 0; r < R; ++r) mx = tmax(mx, tmax(bM[r], tmax(bX[r], bY[r])));
@@ -1101,13 +1223,13 @@ soft_kernel(const SoftArgs A) {
                         if (d >= 0) vstore<T, BW>(bb_out + int64_t(n - d) * BW, v);
                     } else {
                         if (lane == 0 && d >= 0) vstore<T, BW>(stw + (d & (G - 1)) * 4, v);
-                        if (d >= 0 && ((d & (G - 1)) == G - 1 || d == n)) {   // a full segment (or the last)
+                        if (d >= 0 && ((d & (G - 1)) == G - 1 || d == tc1 - tc0)) {   // a full segment (or the last)
                             __syncwarp(gmask);
                             const int dd = d - (d & (G - 1)) + lane;
                             if (dd <= d) {
                                 T w[BW];
                                 vload<T, BW>(w, stw + lane * 4);
-                                vstore<T, BW>(bb_out + int64_t(n - dd) * BW, w);
+                                vstore<T, BW>(bb_out + int64_t(tc1 - dd) * BW, w);
                             }
                             __syncwarp(gmask);
                         }
@@ -1123,15 +1245,15 @@ soft_kernel(const SoftArgs A) {
                     }
                     const int sE = __shfl_down_sync(gmask, EB, 1, G);
                     const int dn = t + 1;                 // lane G-1's next distance
-                    if (s < nstripes - 1 && dn <= n && (dn & (G - 1)) == 0) {   // a new segment
+                    if (s < nstripes - 1 && dn <= tc1 - tc0 && (dn & (G - 1)) == 0) {   // a new segment
                         stage_seg();
                         load_seg(dn + G);
                     }
                     const bool bot = lane == G - 1;
                     T v[BW];
                     vload<T, BW>(v, str + (dn & (G - 1)) * 4);
-                    const int jn1 = n - (t + 1) + (G - 1 - lane);   // this lane's next column
-                    if (jn1 >= 0 && jn1 <= n && (!bot || s < nstripes - 1))
+                    const int jn1 = tc1 - (t + 1) + (G - 1 - lane);   // this lane's next column
+                    if (jn1 >= tc0 && jn1 <= tc1 && (!bot || s < nstripes - 1))
                         take_dn(bot ? v[0] : sM, bot ? (AFF ? v[1] : T(0)) : sX, bot ? (AFF ? v[2] : T(0)) : sY,
                                 bot ? bits_exp(v[BW - 1]) : sE);
                 } else {
@@ -1142,6 +1264,15 @@ soft_kernel(const SoftArgs A) {
                 }
             }
             if constexpr (MW) publish(bkey * SP + S);
+            if (TL && tc > 0) {   // this lane's state at the tile's first column, for the tile to its left
+                T* const dst = colb_p + (int64_t(s) * ntc + tc) * G * LS + lane * LS;
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    dst[NV * r] = bM[r];
+                    if constexpr (AFF) { dst[NV * r + 1] = bX[r]; dst[NV * r + 2] = bY[r]; }
+                }
+                dst[LS - 1] = exp_bits(EB, T(0));
+            }
             if constexpr (POST) {   // this stripe's rows are complete: their columns
 #pragma unroll
                 for (int r = 0; r < R; ++r)
@@ -1210,6 +1341,22 @@ soft_kernel(const SoftArgs A) {
                 gb_o += __shfl_xor_sync(gmask, gb_o, off, G);
                 gb_x += __shfl_xor_sync(gmask, gb_x, off, G);
             }
+        }
+        if constexpr (TL) {
+            // the tile's counts into its stripe's partial (the stripe's tiles run one launch after
+            // another, right to left: a fixed order), its gap sums and lost-mass charge after them
+            const int64_t NNt = int64_t(K) * N * N;
+            double* sp = A.spart + (A.stripe_off[p] + ts) * (A.gstride + 1);
+            __syncwarp(gmask);
+            for (int k = lane; k < K * N * N; k += G) { sp[k] += static_cast<double>(hist[k]); hist[k] = T(0); }
+            if (lane == 0) {
+                sp[NNt + 0] += ga_o; sp[NNt + 1] += ga_x; sp[NNt + 2] += gb_o; sp[NNt + 3] += gb_x;
+                if constexpr (kCount) sp[A.gstride] += static_cast<double>(lacc);
+            }
+            why = __reduce_or_sync(gmask, why);
+            if (why && lane == 0) atomicOr(A.status + p, why);
+            __syncwarp(gmask);
+            continue;
         }
         double* g = A.grad + A.gstride * p;
         const int64_t NN = int64_t(K) * N * N;
@@ -1305,6 +1452,92 @@ soft_kernel(const SoftArgs A) {
         if constexpr (TR) for (int k = 0; k < 4 * K; ++k) tg[k] = 0.0;
         if constexpr (G > 1) __syncwarp(gmask);
     }
+}
+
+// TL: per tiled pair, between the phases, Z (Local: the tiles' parts in tile order) and its
+// range check; after the backward phase, the pair's counts (its stripes' partials in stripe
+// order), score and status -- what the untiled kernel writes at the end of a pair.
+struct TileSoftArgs {
+    const int32_t* pairs; int64_t n_pairs;   // the tiled pairs
+    const int64_t* tile_off; const int32_t* tiles_of;      // per pair / per listed pair
+    const double* zpart; double* zpair;
+    const int64_t* stripe_off; const int32_t* stripes_of;  // per pair / per listed pair
+    const double* spart;
+    const void* gw;                          // the pass's gap weights o_a, e_a, o_b, e_b in T
+    int32_t* status; double* score; double* grad; int64_t gstride;
+    int K, N, local, affine;
+    double temperature;
+};
+template <class T>
+__global__ void tile_z_kernel(const TileSoftArgs A) {   // one thread per pair
+    const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= A.n_pairs) return;
+    const int p = A.pairs[k];
+    if (A.local) {
+        XAcc za; za.init();
+        for (int t = 0; t < A.tiles_of[k]; ++t) {
+            const int64_t q = A.tile_off[p] + t;
+            za.add(A.zpart[2 * q], int(A.zpart[2 * q + 1]));
+        }
+        A.zpair[2 * p] = za.m; A.zpair[2 * p + 1] = double(za.e);
+    }
+    const double zm = A.zpair[2 * p];
+    if (!(zm > 0.0) || !(zm < 1e300)) A.status[p] |= kSoftZ;
+}
+template <class T>
+__global__ void tile_finish_kernel(const TileSoftArgs A) {   // one block per pair
+    const int64_t k = blockIdx.x;
+    if (k >= A.n_pairs) return;
+    const int p = A.pairs[k];
+    const int ns = A.stripes_of[k];
+    const int64_t NN = int64_t(A.K) * A.N * A.N;
+    const int64_t rs = A.gstride + 1;
+    const double* sp = A.spart + A.stripe_off[p] * rs;
+    double* g = A.grad + A.gstride * p;
+    const int32_t st0 = A.status[p];
+    __shared__ int s_bad;
+    if (threadIdx.x == 0) s_bad = 0;
+    __syncthreads();
+    if (st0 == 0) {
+        for (int64_t q = threadIdx.x; q < NN; q += blockDim.x) {
+            double v = 0.0;
+            for (int s = 0; s < ns; ++s) v += sp[s * rs + q];
+            if (!is_finite(v)) s_bad = 1;
+            g[q] = v;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    int32_t why = st0;
+    if (why == 0) {
+        double ga_o = 0, ga_x = 0, gb_o = 0, gb_x = 0, tl = 0;
+        for (int s = 0; s < ns; ++s) {
+            const double* q = sp + s * rs + NN;
+            ga_o += q[0]; ga_x += q[1]; gb_o += q[2]; gb_x += q[3];
+            tl += sp[s * rs + A.gstride];
+        }
+        if (s_bad || !(is_finite(ga_o) && is_finite(ga_x) && is_finite(gb_o) && is_finite(gb_x))) why |= kSoftCounts;
+        if (sizeof(T) == 4 && !(tl <= double(kLossMax))) why |= kSoftLoss;
+        if (why == 0) {
+            const T* gw = static_cast<const T*>(A.gw);
+            // opens carry o = exp(-(go+ge)/T); an opening move also extends
+            const double cga_o = A.affine ? static_cast<double>(gw[0]) * ga_o : 0.0;
+            const double cgb_o = A.affine ? static_cast<double>(gw[2]) * gb_o : 0.0;
+            g[NN + 0] = 0.0 - cga_o;
+            g[NN + 1] = 0.0 - (cga_o + static_cast<double>(gw[1]) * ga_x);
+            g[NN + 2] = 0.0 - cgb_o;
+            g[NN + 3] = 0.0 - (cgb_o + static_cast<double>(gw[3]) * gb_x);
+            const double zm = A.zpair[2 * p];
+            const int ze = int(A.zpair[2 * p + 1]);
+            const int EZ = ze + ilog2(zm);
+            const double zhat = zm * pow2i<double>(ze - EZ);
+            A.status[p] = 0;
+            A.score[p] = A.temperature * (log(zhat) + double(EZ) * 0.69314718055994530942);
+            return;
+        }
+    }
+    A.status[p] = why;
+    A.score[p] = 0.0;
 }
 
 }  // namespace nwg

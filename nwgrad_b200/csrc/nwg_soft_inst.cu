@@ -17,6 +17,12 @@ SoftFn pick(Geo g) {
         return nullptr;
     }
     if (g.band) return (g.G == 32 && g.R == 4 && g.mw <= 1) ? &soft_kernel<T, AFF, LOC, TR, 32, 4, false, true, SG> : nullptr;
+    if (g.tile) {   // tiled long pairs: untracked, Global or Local
+        if constexpr (!TR && !SG) {
+            if (g.G == 32 && g.R == 4) return &soft_kernel<T, AFF, LOC, false, 32, 4, false, false, false, false, true>;
+        }
+        return nullptr;
+    }
     if constexpr (!TR) {
         if (g.mw > 1) return (g.G == 32 && g.R == 4) ? &soft_kernel<T, AFF, LOC, false, 32, 4, true, false, SG> : nullptr;
     } else {

@@ -309,9 +309,10 @@ def test_autotuned_and_plain_fill_same_results(grad_mode, tmp_path, monkeypatch)
 
 @pytest.mark.parametrize("gm", [0, 1])
 @pytest.mark.parametrize("am", [0, 1])
-def test_soft_long_pairs_several_warps_per_pair(gm, am):
-    """Pairs of 1,600+ rows run with four warps per pair (a pipeline over their stripes):
-    within tolerance of the oracle and of the one-warp kernel on the same pairs."""
+def test_soft_long_pairs_tiles(gm, am):
+    """Pairs of 1,600+ rows run as tiles (128 rows x 256 columns; forward and backward a launch
+    per anti-diagonal): within tolerance of the oracle and of the one-warp kernel on the same
+    pairs."""
     rng = np.random.default_rng(1600 + gm + 2 * am)
     mat, gaps, sa, sb, tr, gt = _problem(rng, AA, 6, 5, 200, homolog=True)
     sa += rand_seqs(rng, 3, 1600, 2400, AA)

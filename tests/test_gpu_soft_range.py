@@ -214,11 +214,11 @@ def test_float32_out_of_range_reruns_in_double():
 
 
 def test_wait_limit_fails_cleanly():
-    """Soft long pairs fill with several warps per pair that wait on one another with bounded
-    polls.  With the limit at one poll the waits run out: the kernel marks the pair and
-    returns, the call raises RuntimeError, and the same batch then runs to the oracle's result
-    at the default limit.  (Hard long pairs fill as tiles, a launch per anti-diagonal: no
-    waits.)"""
+    """Soft long pairs with semi-global ends fill with several warps per pair that wait on one
+    another with bounded polls.  With the limit at one poll the waits run out: the kernel
+    marks the pair and returns, the call raises RuntimeError, and the same batch then runs to
+    the oracle's result at the default limit.  (Other long pairs fill as tiles, a launch per
+    anti-diagonal: no waits.)"""
     rng = np.random.default_rng(31)
     mat = rng.integers(-4, 4, size=(1, 20, 20)).astype(np.float64)
     mat[0] = np.triu(mat[0]) + np.triu(mat[0], 1).T
@@ -226,12 +226,13 @@ def test_wait_limit_fails_cleanly():
     gaps = np.array([[11.0, 1.0, 11.0, 1.0]])
     sa = ["".join(rng.choice(list(AA), 2600)) for _ in range(2)]
     sb = ["".join(c if rng.random() > 0.2 else rng.choice(list(AA)) for c in a) for a in sa]
-    b = nw.SeqPairBatch(sa, sb, nw.AlignParams.from_arrays(mat, gaps, alphabet=AA), grad_mode="soft")
+    b = nw.SeqPairBatch(sa, sb, nw.AlignParams.from_arrays(mat, gaps, alphabet=AA), grad_mode="soft",
+                        mode="glocal")
     b.set_spin_limit(1)
     with pytest.raises(RuntimeError, match="ran out"):
         b.score_and_grad()
     b.set_spin_limit()
     b.score_and_grad()
     enc = oracle.Encoded(encode(AA, sa), encode(AA, sb))
-    so, go = oracle.soft(1, 0, mat, gaps, enc)
+    so, go = oracle.soft(1, 2, mat, gaps, enc, free_ends=12)
     np.testing.assert_allclose(b.scores(), so, rtol=SOFT_RTOL)
