@@ -336,10 +336,15 @@ class SeqPairBatch:
         reference's viterbi_affine_hirschberg, viterbi_affine_hirschberg_local,
         viterbi_linear_hirschberg); tracked affine splits are not built."""
         if self._am == 2:
+            # glocal ends split untracked pairs (viterbi_affine_hirschberg_glocal, the linear
+            # glocal branch of viterbi_linear_hirschberg); other free-end sets run Pointers, as in
+            # the reference (aligner.hpp:2323-2330)
+            if self._sg != SG_GLOCAL or not self._tracked:
+                return
             if self._n and int(np.max(np.diff(self._oa))) > self._hb_cutoff:
                 raise NotImplementedError(
-                    f"nwgrad_b200: traceback=\"{self._traceback}\" with mode \"{self._mode}\" (semi-global "
-                    f"ends) splits no pair in this build; use traceback=\"pointers\" or \"auto\"")
+                    f"nwgrad_b200: traceback=\"{self._traceback}\" with mode \"{self._mode}\" splits pairs "
+                    f"in this build only for untracked batches; use traceback=\"pointers\" or \"auto\"")
             return
         if not self._tracked or self._gap_model == "linear":
             return

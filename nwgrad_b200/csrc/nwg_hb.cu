@@ -66,7 +66,8 @@ struct BaseJob {
 struct ScanJob {
     int64_t a_base, b_base;          // row t >= 1 reads a[a_base + a_step (t - 1)]; column c >= 1 b[b_base + b_step (c - 1)]
     int a_step, b_step;
-    int H, W, local, pad;
+    int H, W, local;
+    int glocal;                      // 1: the glocal end scan, 2: the glocal start scan (see hb_scan_kernel)
 };
 
 template <class T> struct Gaps { T go_a, ge_a, go_b, ge_b; };
@@ -96,7 +97,12 @@ __device__ __forceinline__ T chain_x(T um, T ux, T uy, const Gaps<T>& g) {
 // free starts on row 0 and column 0; else the global borders (row 0 the charged Y chain,
 // column 0 the X chain).  The best cell is the first strictly larger max(M, X, Y) in
 // row-major order from 0: each lane keeps the lexicographically least (row, column) among its
-// largest cells, then the warp reduces with the same order.  One warp per block: lanes own R
+// largest cells, then the warp reduces with the same order.  Glocal (`glocal` 1 / 2, the
+// unclamped recurrence): only the block's last row is a candidate, column 0 included, the
+// first column of its maximum; 1 (the end scan) has row 0 a free start (M = 0, no Y) and
+// the candidate max(M, X, Y); 2 (the start scan from the end cell, Global's borders) has as
+// its last row DP row 0, which a path leaves by a diagonal or a vertical move only, so the
+// candidate is max(M, X).  One warp per block: lanes own R
 // rows of a 32R-row stripe, skewed by one column; the row above arrives by shuffle, lane 0's
 // from the previous stripe's bottom row (a per-warp row in global memory) or row 0.
 template <class T, bool PMAX, int R>
@@ -119,7 +125,8 @@ __global__ void __launch_bounds__(128) hb_scan_kernel(const uint8_t* __restrict_
         const ScanJob J = jobs[jb];
         const int H = J.H, W = J.W;
         const bool loc = J.local != 0;
-        T bv = T(0); int bi = 0, bj = 0;
+        const int gl = J.glocal;
+        T bv = gl ? NI : T(0); int bi = 0, bj = 0;
         if (H > 0 && W > 0) {
             const int nst = (H + 32 * R - 1) / (32 * R);
             for (int s = 0; s < nst; ++s) {
@@ -145,7 +152,7 @@ __global__ void __launch_bounds__(128) hb_scan_kernel(const uint8_t* __restrict_
                     const int c = t - lane;
                     if (lane == 0 && c <= W) {
                         if (s == 0) {
-                            if (c == 0 || loc) { upM = T(0); upX = NI; upY = NI; }
+                            if (c == 0 || loc || gl == 1) { upM = T(0); upX = NI; upY = NI; }
                             else {
                                 upM = NI; upX = NI;
                                 upY = hmax((hmax(r0M, r0X) - go_a) - ge_a, r0Y - ge_a);
@@ -169,6 +176,10 @@ __global__ void __launch_bounds__(128) hb_scan_kernel(const uint8_t* __restrict_
                                 m = loc ? T(0) : NI;
                                 y = NI;
                                 if constexpr (PMAX) P[r] = y - ge_a;
+                                if (gl && i0 + r == H) {   // glocal: row H's column 0 is a candidate
+                                    const T here = gl == 2 ? hmax(m, x) : hmax3(m, x, y);
+                                    if (here > bv) { bv = here; bi = H; bj = 0; }
+                                }
                             } else {
                                 m = hmax3(pM, pX, pY) + smat[code[r] + bc];
                                 if (loc) m = hmax(m, T(0));
@@ -179,7 +190,12 @@ __global__ void __launch_bounds__(128) hb_scan_kernel(const uint8_t* __restrict_
                                 } else {
                                     y = hmax3((cM[r] - go_a) - ge_a, (cX[r] - go_a) - ge_a, cY[r] - ge_a);
                                 }
-                                if (valid[r]) {
+                                if (gl) {
+                                    if (i0 + r == H) {
+                                        const T here = gl == 2 ? hmax(m, x) : hmax3(m, x, y);
+                                        if (here > bv) { bv = here; bi = H; bj = c; }
+                                    }
+                                } else if (valid[r]) {
                                     const T here = hmax3(m, x, y);
                                     const int i = i0 + r;
                                     if (here > bv || (here == bv && i < bi)) { bv = here; bi = i; bj = c; }
@@ -210,7 +226,7 @@ __global__ void __launch_bounds__(128) hb_scan_kernel(const uint8_t* __restrict_
             const int oj = __shfl_xor_sync(0xffffffffu, bj, off);
             if (ov > bv || (ov == bv && (oi < bi || (oi == bi && oj < bj)))) { bv = ov; bi = oi; bj = oj; }
         }
-        if (lane == 0) { res[3 * jb] = bv > T(0) ? 1 : 0; res[3 * jb + 1] = bi; res[3 * jb + 2] = bj; }
+        if (lane == 0) { res[3 * jb] = (gl || bv > T(0)) ? 1 : 0; res[3 * jb + 1] = bi; res[3 * jb + 2] = bj; }
         __syncwarp();
     }
 }
@@ -514,22 +530,39 @@ __global__ void hb_replay_kernel(const HbRun P, const BaseJob* __restrict__ jobs
                         static_cast<const T*>(P.gaps_t), N};
     const int64_t NN = int64_t(trk ? P.K : 1) * N * N;
     int32_t* gj = P.guide ? P.guide + ao + p : nullptr;
-    // Local: the path runs from its box's start (is, js) to its end (ie, je); Global: (0, 0)
-    // to (m, n)
-    const int is = boxes ? boxes[4 * k] : 0, js = boxes ? boxes[4 * k + 1] : 0;
+    // Local and glocal: the path runs from its box's start (is, js) to its end (ie, je); Global:
+    // (0, 0) to (m, n)
+    const int is = boxes ? boxes[4 * k] : 0;
+    int js = boxes ? boxes[4 * k + 1] : 0;
     const int ie = boxes ? boxes[4 * k + 2] : m, je = boxes ? boxes[4 * k + 3] : nb;
-    if (gj) { for (int q = 0; q <= m; ++q) gj[q] = -1; gj[0] = 0; gj[is] = js; }
-    uint8_t* keep = P.moves ? P.moves + P.moves_off[p] : nullptr;
     int64_t total = 0;
     for (int64_t q = first[k]; q < first[k + 1]; ++q) total += nmoves[q];
+    // glocal: the box's leading moves along row 0 are free, not glocal moves -- dropped, the
+    // start moving right past them (aligner.hpp:4716-4718)
+    int64_t lead = 0;
+    if (P.glocal) {
+        bool on = true;
+        for (int64_t q = first[k]; q < first[k + 1] && on; ++q) {
+            const uint8_t* mv = moves + jobs[q].moves;
+            for (int e = nmoves[q] - 1; e >= 0; --e) {
+                if (mv[e] != 2) { on = false; break; }
+                ++lead;
+            }
+        }
+        js += int(lead);
+        total -= lead;
+    }
+    if (gj) { for (int q = 0; q <= m; ++q) gj[q] = -1; gj[0] = 0; gj[is] = js; }
+    uint8_t* keep = P.moves ? P.moves + P.moves_off[p] : nullptr;
     T s = T(0);
     int i = is, j = js;
     int prev = 3;
-    int64_t idx = 0;
+    int64_t idx = 0, skip = lead;
     for (int64_t q = first[k]; q < first[k + 1]; ++q) {
         const uint8_t* mv = moves + jobs[q].moves;
         for (int e = nmoves[q] - 1; e >= 0; --e) {
             const int op = mv[e];
+            if (skip > 0) { --skip; continue; }
             if (op == 0) {
                 ++i; ++j;
                 const int64_t cell = (int64_t(trk ? LR.tset(i) : 0) * N + ap[i - 1]) * N + bp[j - 1];
@@ -593,6 +626,7 @@ struct LhbJob {
     // the suffix from row i - 1), row 0's on row i_base (forward) or i_base - 1 (reverse)
     int i_base, i_step;
     int64_t tk_off, gk_off;
+    int free0, pad;                  // MODE 0: row 0 a free start (0 at every column; glocal's end sweep)
 };
 
 
@@ -629,7 +663,11 @@ __global__ void __launch_bounds__(128) lhb_kernel(const uint8_t* __restrict__ a,
             bv = T(0); bi = 0; bj = (ga0 > T(0)) ? 0 : W;
         }
         if (MODE == 0 && H == 0) {   // no rows: row 0 is the last
-            if (lane == 0) { T v = T(0); out[J.out] = v; for (int c = 1; c <= W; ++c) { v = v - ga0; out[J.out + c] = v; } }
+            if (lane == 0) {
+                T v = T(0);
+                out[J.out] = v;
+                for (int c = 1; c <= W; ++c) { if (!J.free0) v = v - ga0; out[J.out + c] = v; }
+            }
         }
         if (H > 0) {
             const int nst = (H + 32 * R - 1) / (32 * R);
@@ -662,7 +700,7 @@ __global__ void __launch_bounds__(128) lhb_kernel(const uint8_t* __restrict__ a,
                     const int c = t - lane;
                     if (lane == 0 && c <= W) {
                         if (s == 0) {
-                            if (c == 0 || LOC) up = T(0);
+                            if (c == 0 || LOC || J.free0) up = T(0);
                             else up = r0 - ga0;
                             r0 = up;
                         } else {
@@ -719,6 +757,42 @@ __global__ void __launch_bounds__(128) lhb_kernel(const uint8_t* __restrict__ a,
         }
         __syncwarp();
     }
+}
+
+// Linear glocal endpoints (viterbi_linear_hirschberg, aligner.hpp:5132-5158), one thread per
+// pair.  phase 0: the end column je, the first of the largest values of the free-row-0 sweep's
+// row m (F, W + 1 values).  phase 1: the start column js -- the best path from (0, q) to
+// (m, je) whose first move is a diagonal or a vertical one, R[d] being the reverse sweep's row
+// 1 (from (1, je - d)); q = je first (down only), then q = je - 1 down to 0, strict >.
+template <class T>
+__global__ void lhb_glocal_pick_kernel(int phase, const LhbJob* __restrict__ jobs, int n_jobs, const T* __restrict__ out,
+                                       const uint8_t* __restrict__ a, const uint8_t* __restrict__ b,
+                                       const T* __restrict__ mat, int N, T gb1, int32_t* __restrict__ res) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n_jobs) return;
+    const LhbJob J = jobs[k];
+    const T* F = out + J.out;
+    if (phase == 0) {
+        int je = 0;
+        for (int c = 1; c <= J.W; ++c) if (F[c] > F[je]) je = c;
+        res[k] = je;
+        return;
+    }
+    // phase 1: J.a_base points at A's last residue (the reverse sweep), J.b_base at B[je - 1];
+    // row 1's residue is A[0], column q + 1's is B[q]
+    const int je = J.W;
+    const int64_t a0 = J.a_base - (J.H);         // A[0]: the reverse sweep ran over A[1 .. m - 1]
+    const int64_t b0 = J.b_base - (je - 1);      // B[0]
+    const int ar = int(a[a0]) * N;
+    T sbest = F[0] - gb1;
+    int js = je;
+    for (int q = je - 1; q >= 0; --q) {
+        T v = F[je - q - 1] + mat[ar + int(b[b0 + q])];
+        const T u = F[je - q] - gb1;
+        if (v < u) v = u;
+        if (v > sbest) { sbest = v; js = q; }
+    }
+    res[k] = js;
 }
 
 // The join of a linear split (lhb_solve :4999-5017): the first column of the strictly largest
@@ -884,14 +958,18 @@ int64_t hb_run_t(const HbRun& P, cudaStream_t st, int sms) {
     constexpr int R = 4;
     Tmp djobs(st), dout(st), dwrap(st), dres(st), dboxes(st);
     std::vector<int32_t> boxes;
-    if (!P.local) {
+    if (!P.local && !P.glocal) {
         for (int k = 0; k < n; ++k) {
             const int p = P.h_pairs[k];
             cur.push_back(Blk{k, 0, int(P.h_oa[p + 1] - P.h_oa[p]), 0, int(P.h_ob[p + 1] - P.h_ob[p]), 0, 0});
         }
     } else {
         // Local: the forward clamped scan of every pair, then the reverse global-suffix scan of
-        // the pairs with a positive best, give each pair's box
+        // the pairs with a positive best, give each pair's box.  Glocal
+        // (viterbi_affine_hirschberg_glocal, aligner.hpp:4709-4745): the end scan's first best
+        // column je of row m, then the start scan from (m, je) for the start column js of row
+        // 0; the box A x B[js, je) (a pair without B: column 0).  Either box then runs as a
+        // Global pair.
         boxes.assign(size_t(n) * 4, 0);
         const size_t mat_b = size_t((P.N * P.N + 3) & ~3) * sizeof(T);
         auto run_scans = [&](const std::vector<ScanJob>& sj, std::vector<int32_t>& out) {
@@ -916,33 +994,58 @@ int64_t hb_run_t(const HbRun& P, cudaStream_t st, int sms) {
             HB_CUDA(cudaStreamSynchronize(st));
         };
         std::vector<ScanJob> scan_f;
+        std::vector<int> fk;                      // the pair of each forward scan
         scan_f.reserve(size_t(n));
         for (int k = 0; k < n; ++k) {
             const int p = P.h_pairs[k];
             ScanJob J{};
             J.a_base = P.h_oa[p]; J.a_step = 1; J.b_base = P.h_ob[p]; J.b_step = 1;
-            J.H = int(P.h_oa[p + 1] - P.h_oa[p]); J.W = int(P.h_ob[p + 1] - P.h_ob[p]); J.local = 1; J.pad = 0;
+            J.H = int(P.h_oa[p + 1] - P.h_oa[p]); J.W = int(P.h_ob[p + 1] - P.h_ob[p]);
+            J.local = P.glocal ? 0 : 1; J.glocal = P.glocal ? 1 : 0;
+            if (P.glocal && J.W == 0) continue;   // no B: the end is column 0
             scan_f.push_back(J);
+            fk.push_back(k);
         }
         std::vector<int32_t> fr, rr;
         run_scans(scan_f, fr);
         std::vector<ScanJob> rev;
         std::vector<int> rk;
-        for (int k = 0; k < n; ++k) {
-            if (!fr[3 * k] || fr[3 * k + 1] <= 0 || fr[3 * k + 2] <= 0) continue;   // no positive cell: empty
+        std::vector<int> ends(size_t(n) * 2, 0);  // per pair: ie, je
+        for (size_t q = 0; q < fk.size(); ++q) {
+            const int k = fk[q];
             const int p = P.h_pairs[k];
-            const int ie = fr[3 * k + 1], je = fr[3 * k + 2];
+            const int ie = fr[3 * q + 1], je = fr[3 * q + 2];
+            ends[2 * size_t(k)] = ie; ends[2 * size_t(k) + 1] = je;
             ScanJob J{};
+            if (P.glocal) {
+                if (je == 0) continue;            // the end on column 0: the box is column 0
+                J.H = ie; J.glocal = 2;
+            } else {
+                if (!fr[3 * q] || ie <= 0 || je <= 0) continue;   // no positive cell: empty
+                J.H = ie;
+            }
             J.a_base = P.h_oa[p] + ie - 1; J.a_step = -1; J.b_base = P.h_ob[p] + je - 1; J.b_step = -1;
-            J.H = ie; J.W = je; J.local = 0;
+            J.W = je; J.local = 0;
             rev.push_back(J);
             rk.push_back(k);
         }
         run_scans(rev, rr);
+        std::vector<int> starts(size_t(n) * 2, -1);   // per pair: is, js (-1: no box)
         for (size_t q = 0; q < rk.size(); ++q) {
             const int k = rk[q];
-            const int ie = fr[3 * k + 1], je = fr[3 * k + 2];
-            const int is = ie - rr[3 * q + 1], js = je - rr[3 * q + 2];
+            starts[2 * size_t(k)] = ends[2 * size_t(k)] - rr[3 * q + 1];
+            starts[2 * size_t(k) + 1] = ends[2 * size_t(k) + 1] - rr[3 * q + 2];
+        }
+        for (int k = 0; k < n; ++k) {
+            const int p = P.h_pairs[k];
+            int is = starts[2 * size_t(k)], js = starts[2 * size_t(k) + 1];
+            int ie = ends[2 * size_t(k)], je = ends[2 * size_t(k) + 1];
+            if (P.glocal) {
+                ie = int(P.h_oa[p + 1] - P.h_oa[p]);   // the end row is m (also without B)
+                if (is < 0) { is = 0; js = je; }      // the end on column 0
+            } else if (is < 0) {
+                continue;                              // Local, nothing positive: the empty alignment
+            }
             boxes[4 * size_t(k)] = is; boxes[4 * size_t(k) + 1] = js;
             boxes[4 * size_t(k) + 2] = ie; boxes[4 * size_t(k) + 3] = je;
             cur.push_back(Blk{k, is, ie, js, je, 0, 0});
@@ -1050,7 +1153,7 @@ int64_t hb_run_t(const HbRun& P, cudaStream_t st, int sms) {
             HB_CUDA(cudaGetLastError());
         }
         int32_t* bx = nullptr;
-        if (P.local) {
+        if (P.local || P.glocal) {
             bx = static_cast<int32_t*>(dboxes.get(boxes.size() * sizeof(int32_t)));
             HB_CUDA(cudaMemcpyAsync(bx, boxes.data(), boxes.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
         }
@@ -1107,7 +1210,67 @@ int64_t lhb_run_t(const HbRun& P, cudaStream_t st, int sms) {
     };
     std::vector<Blk> cur;
     std::vector<int32_t> boxes;
-    if (!P.local) {
+    if (P.glocal) {
+        // glocal (aligner.hpp:5132-5158): the end column je from row m of a sweep with row 0 a
+        // free start, the start column js from the reverse sweep over rows 2..m to row 1 and a
+        // pick over row 0's columns; the box A x B[js, je) then runs as a Global pair
+        boxes.assign(size_t(n) * 4, 0);
+        auto pick = [&](int phase, const std::vector<LhbJob>& jobs, std::vector<int32_t>& res) {
+            res.assign(jobs.size(), 0);
+            if (jobs.empty()) return;
+            int64_t out_off = 0;
+            for (const LhbJob& x : jobs) out_off += int64_t(x.W) + 1;
+            T* o = static_cast<T*>(dout.get(size_t(out_off) * sizeof(T)));
+            launch(0, jobs, o, nullptr);
+            int32_t* rs = static_cast<int32_t*>(dres.get(jobs.size() * sizeof(int32_t)));
+            lhb_glocal_pick_kernel<T><<<unsigned((jobs.size() + 127) / 128), 128, 0, st>>>(
+                phase, static_cast<const LhbJob*>(djobs.p), int(jobs.size()), o, P.a, P.b, mat, P.N, gb, rs);
+            HB_CUDA(cudaGetLastError());
+            launches++;
+            HB_CUDA(cudaMemcpyAsync(res.data(), rs, res.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+            HB_CUDA(cudaStreamSynchronize(st));
+        };
+        std::vector<LhbJob> jf;
+        int64_t off = 0;
+        for (int k = 0; k < n; ++k) {
+            const int p = P.h_pairs[k];
+            LhbJob J{};
+            J.a_base = P.h_oa[p]; J.a_step = 1; J.b_base = P.h_ob[p]; J.b_step = 1;
+            J.H = int(P.h_oa[p + 1] - P.h_oa[p]); J.W = int(P.h_ob[p + 1] - P.h_ob[p]);
+            J.free0 = 1;
+            track_offs(J, p, 0, 1);
+            J.out = off; off += int64_t(J.W) + 1;
+            jf.push_back(J);
+        }
+        std::vector<int32_t> je_of, js_of;
+        pick(0, jf, je_of);
+        std::vector<LhbJob> jr;
+        std::vector<int> rk;
+        off = 0;
+        for (int k = 0; k < n; ++k) {
+            const int p = P.h_pairs[k];
+            const int m = int(P.h_oa[p + 1] - P.h_oa[p]), je = je_of[size_t(k)];
+            if (je == 0 || m < 2) continue;   // js = je: the box is one column (or one row: the pick is the end's)
+            LhbJob J{};
+            J.a_base = P.h_oa[p] + m - 1; J.a_step = -1; J.b_base = P.h_ob[p] + je - 1; J.b_step = -1;
+            J.H = m - 1; J.W = je;
+            track_offs(J, p, m + 1, -1);
+            J.out = off; off += int64_t(je) + 1;
+            jr.push_back(J);
+            rk.push_back(k);
+        }
+        pick(1, jr, js_of);
+        std::vector<int> js_k(size_t(n), -1);
+        for (size_t q = 0; q < rk.size(); ++q) js_k[size_t(rk[q])] = js_of[q];
+        for (int k = 0; k < n; ++k) {
+            const int p = P.h_pairs[k];
+            const int m = int(P.h_oa[p + 1] - P.h_oa[p]), je = je_of[size_t(k)];
+            const int js = js_k[size_t(k)] >= 0 ? js_k[size_t(k)] : je;
+            boxes[4 * size_t(k)] = 0; boxes[4 * size_t(k) + 1] = js;
+            boxes[4 * size_t(k) + 2] = m; boxes[4 * size_t(k) + 3] = je;
+            cur.push_back(Blk{k, 0, m, js, je, 0, 0});
+        }
+    } else if (!P.local) {
         for (int k = 0; k < n; ++k) {
             const int p = P.h_pairs[k];
             cur.push_back(Blk{k, 0, int(P.h_oa[p + 1] - P.h_oa[p]), 0, int(P.h_ob[p + 1] - P.h_ob[p]), 0, 0});
@@ -1233,7 +1396,7 @@ int64_t lhb_run_t(const HbRun& P, cudaStream_t st, int sms) {
         launches++;
     }
     int32_t* bx = nullptr;
-    if (P.local) {
+    if (P.local || P.glocal) {
         bx = static_cast<int32_t*>(dboxes.get(boxes.size() * sizeof(int32_t)));
         HB_CUDA(cudaMemcpyAsync(bx, boxes.data(), boxes.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
     }

@@ -25,6 +25,8 @@ struct HbRun {
     int cutoff;                                // rows at which blocks stop splitting (>= 1)
     int pmax;                                  // the closed-form prefix-max horizontal carry
     int local;                                 // Local: endpoint scans, then the box's global solve
+    int glocal;                                // glocal ends (row 0 a free start, row m's cells ends):
+                                               // the glocal endpoint scans, then the box's global solve
     int linear;                                // linear gaps (one state; pmax does not apply)
     // linear, tracked: K sets (mat K x N x N, gaps_t K x 4 in T), per residue of A its set,
     // per DP row its gap set (oa[p] + p offsets; null: the residue's set)

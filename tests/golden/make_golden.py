@@ -20,6 +20,9 @@ Two sources, both the reference's own code run here:
   banded_grad(bw) around the Viterbi guides, every gap model and mode, bw 1, 3, 8.
 * ``semiglobal.npz`` -- the batch engine with AlignMode::Glocal and free_ends sets (glocal,
   overlap, mixed): hard float32 / float64 with guides, soft log space at T = 1.
+* ``hirschberg_glocal.npz`` -- the batch engine with glocal ends and traceback "hirschberg" /
+  "hirschberg_pmax" (affine and linear, small hb_cutoff): A within a longer B, float32 and
+  float64.
 """
 from __future__ import annotations
 
@@ -331,8 +334,48 @@ def posterior_fixtures():
     print("posterior.npz:", len(out), "arrays")
 
 
+def hb_glocal_fixtures():
+    """Glocal Hirschberg (viterbi_affine_hirschberg_glocal): A (a mutated stretch of B, or
+    random) within B with random flanks, so the end and start scans pick columns inside B."""
+    rng = np.random.default_rng(321)
+    AA = "ACDEFGHIKLMNPQRSTVWY"
+    out = {}
+    for name, integer in (("int", True), ("flt", False)):
+        mat = rng.integers(-4, 4, size=(1, 20, 20)).astype(np.float64) if integer else \
+            rng.normal(0, 2, size=(1, 20, 20)).round(3)
+        if integer:
+            mat[0][np.diag_indices(20)] = rng.integers(4, 12, size=20)
+        gaps = np.array([[11.0, 1.0, 11.0, 1.0]]) if integer else rng.uniform(0.3, 4.0, size=(1, 4)).round(3)
+        sa, sb = [], []
+        for k in range(16):
+            core = "".join(rng.choice(list(AA), size=int(rng.integers(1, 300))))
+            a = "".join(c if rng.random() > 0.25 else str(rng.choice(list(AA))) for c in core) if k % 3 else core
+            if k % 4 == 0:
+                a = "".join(rng.choice(list(AA), size=int(rng.integers(1, 300))))
+            left = "".join(rng.choice(list(AA), size=int(rng.integers(0, 120))))
+            right = "".join(rng.choice(list(AA), size=int(rng.integers(0, 120))))
+            sa.append(a)
+            sb.append(left + core + right if k % 5 else "")   # every fifth pair: no B
+        out[f"{name}_mat"], out[f"{name}_gaps"] = mat, gaps
+        out[f"{name}_sa"], out[f"{name}_sb"] = np.array(sa), np.array(sb)
+        for prec in (32, 64):
+            for tb in ("hirschberg", "hirschberg_pmax"):
+                for cut in (8, 64):
+                    for gm, tag in ((1, ""), (0, "lin_")):
+                        r = oracle.ref_run(prec, gm, 2, 1, AA, mat, gaps, sa, sb, traceback=tb, hb_cutoff=cut,
+                                           free_ends=12)
+                        key = f"{name}_{tag}{tb}_{prec}_c{cut}_"
+                        out[key + "scores"] = r["scores"]
+                        out[key + "grads"] = r["grads"]
+                        out[key + "guides"] = r["guides"]
+    np.savez_compressed(os.path.join(HERE, "hirschberg_glocal.npz"), **out)
+    print("hirschberg_glocal.npz:", len(out), "arrays")
+
+
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["brute", "ref", "hb", "sb", "sg", "post"]
+    which = sys.argv[1:] or ["brute", "ref", "hb", "sb", "sg", "post", "hbg"]
+    if "hbg" in which:
+        hb_glocal_fixtures()
     if "post" in which:
         posterior_fixtures()
     if "brute" in which:

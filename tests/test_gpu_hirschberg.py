@@ -1,5 +1,5 @@
 """Hirschberg re-alignment on the GPU (traceback "hirschberg" / "hirschberg_pmax"; affine and
-linear gaps, Global and Local): scores, gradients and guides bit for bit against the reference's own engine
+linear gaps, Global and Local, affine glocal ends): scores, gradients and guides bit for bit against the reference's own engine
 (tests/golden/hirschberg.npz) and against the oracle's restatement on longer pairs."""
 import os
 
@@ -43,6 +43,59 @@ def test_reference_fixtures(name, prec, tb, cut, mode, gap_model):
     assert np.array_equal(g, z[key + "grads"])
     assert np.array_equal(gj, z[key + "guides"])
     assert tot == float(np.cumsum(z[key + "scores"])[-1])
+
+
+@pytest.mark.parametrize("name", ["int", "flt"])
+@pytest.mark.parametrize("prec", [32, 64])
+@pytest.mark.parametrize("tb", ["hirschberg", "hirschberg_pmax"])
+@pytest.mark.parametrize("cut", [8, 64])
+@pytest.mark.parametrize("gap_model", ["affine", "linear"])
+def test_glocal_reference_fixtures(name, prec, tb, cut, gap_model):
+    """Glocal ends (affine: viterbi_affine_hirschberg_glocal, aligner.hpp:4709; linear: the
+    glocal branch of viterbi_linear_hirschberg, :5132): the end and start scans, the box's
+    global solve with its free leading moves dropped -- scores, gradients and guides bit for
+    bit the reference engine's (tests/golden/hirschberg_glocal.npz: A within a longer B,
+    pairs without B)."""
+    z = np.load(os.path.join(GOLD, "hirschberg_glocal.npz"))
+    sa, sb = [str(s) for s in z[f"{name}_sa"]], [str(s) for s in z[f"{name}_sb"]]
+    s, g, gj, tot = _run(prec, tb, cut, z[f"{name}_mat"], z[f"{name}_gaps"], sa, sb, "glocal", gap_model)
+    key = f"{name}_{'lin_' if gap_model == 'linear' else ''}{tb}_{prec}_c{cut}_"
+    assert np.array_equal(s, z[key + "scores"]), np.nonzero(s != z[key + "scores"])[0][:5]
+    assert np.array_equal(g, z[key + "grads"]), np.nonzero((g != z[key + "grads"]).any(1))[0][:5]
+    assert np.array_equal(gj, z[key + "guides"])
+
+
+@pytest.mark.parametrize("prec", [32, 64])
+@pytest.mark.parametrize("pmax", [False, True])
+@pytest.mark.parametrize("gap_model", ["affine", "linear"])
+def test_glocal_long_pairs_against_the_oracle(prec, pmax, gap_model):
+    """Glocal pairs of 1,000-4,000 residues within longer B: the same score as the oracle's
+    glocal Pointers (any optimal path), a path that scores it (the replayed gradient's
+    substitution and gap counts give the score back), and keep_paths moves that start on
+    row 0 and end on row m."""
+    rng = np.random.default_rng(2600 + prec + pmax + 7 * (gap_model == "linear"))
+    mat = rand_matrix(rng, 20, integer=True)
+    gm = 1 if gap_model == "affine" else 0
+    gaps = np.array([[11.0, 1.0, 11.0, 1.0]]) if gm else np.array([[0.0, 3.0, 0.0, 3.0]])
+    sa = rand_seqs(rng, 5, 1000, 4000, AA) + rand_seqs(rng, 6, 1, 300, AA)
+    sb = []
+    for k, a in enumerate(sa):
+        core = mutate(rng, a, AA) if k % 3 else rand_seqs(rng, 1, 200, 3000, AA)[0]
+        sb.append(rand_seqs(rng, 1, 0, 500, AA)[0] + core + rand_seqs(rng, 1, 0, 500, AA)[0])
+    tb = "hirschberg_pmax" if pmax else "hirschberg"
+    cls = nw.SeqPairBatch if prec == 32 else nw.SeqPairBatchDouble
+    p = nw.AlignParams.from_arrays(mat, gaps, alphabet=AA)
+    b = cls(sa, sb, p, grad_mode="hard", traceback=tb, mode="glocal", gap_model=gap_model)
+    b.score_and_grad(keep_paths=True)
+    o = oracle.hard(prec, gm, 2, mat, gaps, oracle.Encoded(encode(AA, sa), encode(AA, sb)), free_ends=12)
+    np.testing.assert_array_equal(b.scores(), o["scores"])
+    gm, gg = b.grads()
+    flat = np.concatenate([gm.reshape(len(sa), -1), gg.reshape(len(sa), -1)], axis=1)
+    w = np.concatenate([mat.reshape(-1), gaps.reshape(-1)])
+    np.testing.assert_allclose(flat @ w, o["scores"], rtol=1e-6)
+    for i in range(len(sa)):
+        a_al, b_al = b[i].aligned()
+        assert a_al.replace("-", "") == sa[i]
 
 
 @pytest.mark.parametrize("prec", [32, 64])
