@@ -48,7 +48,8 @@ constexpr int kHbRing = 4 * kHbC;    // ring slots per warp boundary
 struct SweepJob {
     int64_t a_base; int64_t b_base;  // row t >= 1 reads a[a_base + a_step (t - 1)]; column c >= 1 b[b_base + b_step (c - 1)]
     int a_step, b_step;
-    int H, W, flag, pad;
+    int H, W, flag;
+    int tiled;                       // swept by hb_tile_kernel (hb_sweep_kernel skips it)
     int64_t out;                     // T offset of the last row: M, X, Y arrays of W + 1
     int64_t wrap;                    // T offset of the wrap row buffer (3 (W + 1))
 };
@@ -251,6 +252,7 @@ __global__ void __launch_bounds__(512) hb_sweep_kernel(const uint8_t* __restrict
 
     for (int jb = blockIdx.x; jb < n_jobs; jb += gridDim.x) {
         const SweepJob J = jobs[jb];
+        if (J.tiled) continue;
         const int H = J.H, W = J.W;
         const int ns = (H + 1 + GR - 1) / GR;              // stripes over rows 0..H
         const int rounds = (ns + NW - 1) / NW;
@@ -345,6 +347,132 @@ __global__ void __launch_bounds__(512) hb_sweep_kernel(const uint8_t* __restrict
             }
             __syncthreads();
         }
+    }
+}
+
+// ── tiled half-sweeps ─────────────────────────────────────────────────────────
+// The large half-sweeps of a level (a top level of long pairs: one block of warps would hold
+// one SM for most of the level) as tiles: stripe s (rows s GR .. s GR + GR - 1 of 0..H) over
+// columns c Wt .. c Wt + Wt - 1 of 0..W, one warp per tile, a launch per anti-diagonal s + c
+// of every tiled job's tiles.  The cells are hb_sweep_kernel's -- the same expressions, borders
+// and flags -- so the last row is the same bits; the row above comes from the stripe above's
+// bottom row (one row per stripe), the lanes' state at the column left of the tile (M, X, Y and
+// the prefix-max carry of each row) from the tile to the left.
+struct HbTileArgs {
+    const SweepJob* jobs;
+    const int32_t* tiles;            // per item: job, stripe, tile
+    int64_t n_items;
+    int tile_w;                      // a multiple of 32
+    const int64_t* row_off;          // per job: T offset of its rows (ns x 3 (W + 1))
+    const int64_t* col_off;          // per job: T offset of its lane states (ns x nt x 32 x 4R)
+    int* queue;                      // the work queue shared by the level's tile launches
+};
+template <class T, bool PMAX, int R>
+__global__ void __launch_bounds__(128) hb_tile_kernel(const uint8_t* __restrict__ a, const uint8_t* __restrict__ b,
+                                                      const T* __restrict__ mat, int N, Gaps<T> gp, HbTileArgs A,
+                                                      T* __restrict__ out, T* __restrict__ rows, T* __restrict__ cols) {
+    constexpr int G = 32, GR = G * R, LSZ = 4 * R;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* smat = reinterpret_cast<T*>(smem_raw);
+    for (int k = threadIdx.x; k < N * N; k += blockDim.x) smat[k] = mat[k];
+    __syncthreads();
+    const int lane = threadIdx.x % G, gpb = blockDim.x / G;
+    const T NI = ninf<T>();
+    auto next_item = [&]() -> int64_t {
+        long long v = 0;
+        if (lane == 0) v = wq_next(A.queue, int(gridDim.x) * gpb, A.n_items);
+        return __shfl_sync(0xffffffffu, v, 0);
+    };
+    for (int64_t it = next_item(); it < A.n_items; it = next_item()) {
+        const int jb = A.tiles[3 * it], s = A.tiles[3 * it + 1], tc = A.tiles[3 * it + 2];
+        const SweepJob J = A.jobs[jb];
+        const int H = J.H, W = J.W;
+        const int ns = (H + 1 + GR - 1) / GR, nt = W / A.tile_w + 1;
+        const int c0 = tc * A.tile_w, c1 = min(W, c0 + A.tile_w - 1);
+        T* oM = out + J.out; T* oX = oM + (W + 1); T* oY = oX + (W + 1);
+        T* const rowp = rows + A.row_off[jb];
+        T* const colp = cols + A.col_off[jb];
+        const T* const above = rowp + int64_t(s - 1) * 3 * (W + 1);   // s > 0
+        T* const below = rowp + int64_t(s) * 3 * (W + 1);
+        const int i0 = s * GR + lane * R;
+        int key[R];
+        T cM[R], cX[R], cY[R], P[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int t = i0 + r;
+            key[r] = (t >= 1 && t <= H) ? int(a[J.a_base + int64_t(J.a_step) * (t - 1)]) * N : 0;
+            cM[r] = NI; cX[r] = NI; cY[r] = NI; P[r] = NI;
+        }
+        T dgM = NI, dgX = NI, dgY = NI, upM = NI, upX = NI, upY = NI;
+        if (tc > 0) {   // the state the tile to the left left at column c0 - 1
+            const T* ls = colp + (int64_t(s) * nt + tc - 1) * G * LSZ;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                cM[r] = ls[lane * LSZ + 4 * r]; cX[r] = ls[lane * LSZ + 4 * r + 1];
+                cY[r] = ls[lane * LSZ + 4 * r + 2]; P[r] = ls[lane * LSZ + 4 * r + 3];
+            }
+            if (lane > 0) {
+                const T* q = ls + (lane - 1) * LSZ + 4 * (R - 1);
+                dgM = q[0]; dgX = q[1]; dgY = q[2];
+            } else if (s > 0) {
+                dgM = above[3 * (c0 - 1)]; dgX = above[3 * (c0 - 1) + 1]; dgY = above[3 * (c0 - 1) + 2];
+            }
+        }
+        T nuM = NI, nuX = NI, nuY = NI;   // lane 0: the row above one column ahead
+        if (lane == 0 && s > 0) { nuM = above[3 * c0]; nuX = above[3 * c0 + 1]; nuY = above[3 * c0 + 2]; }
+        const int S = (c1 - c0 + 1) + G - 1;
+        for (int t = 0; t < S; ++t) {
+            const int c = c0 + t - lane;
+            if (lane == 0 && s > 0 && c <= c1) {
+                upM = nuM; upX = nuX; upY = nuY;
+                if (c < c1) { nuM = above[3 * (c + 1)]; nuX = above[3 * (c + 1) + 1]; nuY = above[3 * (c + 1) + 2]; }
+            }
+            const bool active = c >= c0 && c <= c1;
+            if (active) {
+                const int bj = c >= 1 ? int(b[J.b_base + int64_t(J.b_step) * (c - 1)]) : 0;
+                T pM = dgM, pX = dgX, pY = dgY;      // row above, column c - 1
+                T qM = upM, qX = upX, qY = upY;      // row above, column c
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const int t2 = i0 + r;
+                    T mv, xv, yv;
+                    if (t2 == 0) {
+                        if (c == 0) { mv = J.flag ? NI : T(0); xv = NI; yv = NI; }
+                        else { mv = NI; xv = NI; yv = chain_y(cM[r], cX[r], cY[r], gp); }
+                    } else if (c == 0) {
+                        mv = NI; yv = NI;
+                        xv = (t2 == 1 && J.flag) ? T(0) - gp.ge_b : chain_x(qM, qX, qY, gp);
+                    } else {
+                        mv = hmax3(pM, pX, pY) + smat[key[r] + bj];
+                        xv = chain_x(qM, qX, qY, gp);
+                        if constexpr (PMAX) {
+                            const T g = (hmax(cM[r], cX[r]) - gp.go_a) - gp.ge_a;
+                            const T rm = mul_rn(static_cast<T>(c - 1), gp.ge_a);
+                            P[r] = hmax(add_rn(g, rm), P[r]);
+                            yv = P[r] - rm;
+                        } else {
+                            yv = chain_y(cM[r], cX[r], cY[r], gp);
+                        }
+                    }
+                    pM = cM[r]; pX = cX[r]; pY = cY[r];
+                    cM[r] = mv; cX[r] = xv; cY[r] = yv;
+                    qM = mv; qX = xv; qY = yv;
+                    if (t2 == H) { oM[c] = mv; oX[c] = xv; oY[c] = yv; }
+                }
+                dgM = upM; dgX = upX; dgY = upY;
+            }
+            const T sM = __shfl_up_sync(0xffffffffu, cM[R - 1], 1);
+            const T sX = __shfl_up_sync(0xffffffffu, cX[R - 1], 1);
+            const T sY = __shfl_up_sync(0xffffffffu, cY[R - 1], 1);
+            if (lane > 0) { upM = sM; upX = sX; upY = sY; }
+            if (lane == G - 1 && active && s + 1 < ns) { below[3 * c] = cM[R - 1]; below[3 * c + 1] = cX[R - 1]; below[3 * c + 2] = cY[R - 1]; }
+        }
+        if (tc + 1 < nt) {   // this lane's state at the tile's last column
+            T* ls = colp + (int64_t(s) * nt + tc) * G * LSZ + lane * LSZ;
+#pragma unroll
+            for (int r = 0; r < R; ++r) { ls[4 * r] = cM[r]; ls[4 * r + 1] = cX[r]; ls[4 * r + 2] = cY[r]; ls[4 * r + 3] = P[r]; }
+        }
+        __syncwarp();
     }
 }
 
@@ -957,6 +1085,7 @@ int64_t hb_run_t(const HbRun& P, cudaStream_t st, int sms) {
     cur.reserve(size_t(n));
     constexpr int R = 4;
     Tmp djobs(st), dout(st), dwrap(st), dres(st), dboxes(st);
+    Tmp dtiles(st), droff(st), dcoff(st), dtrows(st), dtcols(st), dq(st);   // tiled half-sweeps
     std::vector<int32_t> boxes;
     if (!P.local && !P.glocal) {
         for (int k = 0; k < n; ++k) {
@@ -1069,14 +1198,45 @@ int64_t hb_run_t(const HbRun& P, cudaStream_t st, int sms) {
             const int mid = B.i0 + (B.i1 - B.i0) / 2, W = B.j1 - B.j0;
             SweepJob& F = jobs[2 * s];
             F.a_base = P.h_oa[p] + B.i0; F.a_step = 1; F.b_base = P.h_ob[p] + B.j0; F.b_step = 1;
-            F.H = mid - B.i0; F.W = W; F.flag = B.in_x; F.pad = 0;
+            F.H = mid - B.i0; F.W = W; F.flag = B.in_x; F.tiled = 0;
             SweepJob& Rv = jobs[2 * s + 1];
             Rv.a_base = P.h_oa[p] + B.i1 - 1; Rv.a_step = -1; Rv.b_base = P.h_ob[p] + B.j1 - 1; Rv.b_step = -1;
-            Rv.H = B.i1 - mid; Rv.W = W; Rv.flag = B.out_x; Rv.pad = 0;
+            Rv.H = B.i1 - mid; Rv.W = W; Rv.flag = B.out_x; Rv.tiled = 0;
             for (SweepJob* x : {&F, &Rv}) {
                 x->out = out_off; out_off += 3 * (int64_t(W) + 1);
                 x->wrap = wrap_off; wrap_off += 3 * (int64_t(W) + 1);
                 max_ns = std::max(max_ns, (x->H + 1 + 32 * R - 1) / (32 * R));
+            }
+        }
+        // half-sweeps of at least kHbTileCells cells run as tiles over the whole device (a
+        // block of warps would hold one SM for most of the level), within a memory budget
+        // for their rows and lane states; the rest as one block each
+        constexpr int64_t kHbTileCells = int64_t(8) << 20;
+        constexpr int kHbTileW = 256;
+        const int GRt = 32 * R;
+        std::vector<int64_t> roff(jobs.size(), 0), coff(jobs.size(), 0);
+        std::vector<std::vector<int32_t>> diags;
+        int64_t row_elems = 0, col_elems = 0, n_tiles = 0;
+        {
+            size_t free_b = 0, total_b = 0;
+            cudaMemGetInfo(&free_b, &total_b);
+            const int64_t budget = int64_t(free_b / 4);
+            for (size_t q = 0; q < jobs.size(); ++q) {
+                SweepJob& x = jobs[q];
+                if ((int64_t(x.H) + 1) * (int64_t(x.W) + 1) < kHbTileCells) continue;
+                const int nsj = (x.H + 1 + GRt - 1) / GRt, ntj = x.W / kHbTileW + 1;
+                const int64_t re = int64_t(nsj) * 3 * (x.W + 1), ce = int64_t(nsj) * ntj * 32 * 4 * R;
+                if ((row_elems + re + col_elems + ce) * int64_t(sizeof(T)) > budget) continue;
+                x.tiled = 1;
+                roff[q] = row_elems; row_elems += re;
+                coff[q] = col_elems; col_elems += ce;
+                if (int(diags.size()) < nsj + ntj - 1) diags.resize(size_t(nsj + ntj - 1));
+                for (int sj = 0; sj < nsj; ++sj)
+                    for (int cj = 0; cj < ntj; ++cj) {
+                        auto& dv = diags[size_t(sj + cj)];
+                        dv.push_back(int32_t(q)); dv.push_back(sj); dv.push_back(cj);
+                    }
+                n_tiles += int64_t(nsj) * ntj;
             }
         }
         int NW = 1;
@@ -1090,14 +1250,49 @@ int64_t hb_run_t(const HbRun& P, cudaStream_t st, int sms) {
         HB_CUDA(allow_smem(reinterpret_cast<const void*>(fn), smem));
         int occ = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 32 * NW, smem);
-        const int grid = int(std::min<int64_t>(int64_t(jobs.size()), int64_t(sms) * std::max(occ, 1)));
-        fn<<<grid, 32 * NW, smem, st>>>(P.a, P.b, static_cast<const T*>(P.mat), P.N, gp, dj, int(jobs.size()), o, wr);
-        HB_CUDA(cudaGetLastError());
+        int64_t n_block = 0;
+        for (const SweepJob& x : jobs) n_block += x.tiled ? 0 : 1;
+        if (n_block) {
+            const int grid = int(std::min<int64_t>(n_block, int64_t(sms) * std::max(occ, 1)));
+            fn<<<grid, 32 * NW, smem, st>>>(P.a, P.b, static_cast<const T*>(P.mat), P.N, gp, dj, int(jobs.size()), o, wr);
+            HB_CUDA(cudaGetLastError());
+        }
+        if (n_tiles) {
+            std::vector<int32_t> items;
+            items.reserve(size_t(n_tiles) * 3);
+            std::vector<int64_t> doff(1, 0);
+            for (auto& dv : diags) { items.insert(items.end(), dv.begin(), dv.end()); doff.push_back(int64_t(items.size() / 3)); }
+            int32_t* ti = static_cast<int32_t*>(dtiles.get(items.size() * 4));
+            HB_CUDA(cudaMemcpyAsync(ti, items.data(), items.size() * 4, cudaMemcpyHostToDevice, st));
+            int64_t* ro = static_cast<int64_t*>(droff.get(roff.size() * 8));
+            int64_t* co = static_cast<int64_t*>(dcoff.get(coff.size() * 8));
+            HB_CUDA(cudaMemcpyAsync(ro, roff.data(), roff.size() * 8, cudaMemcpyHostToDevice, st));
+            HB_CUDA(cudaMemcpyAsync(co, coff.data(), coff.size() * 8, cudaMemcpyHostToDevice, st));
+            T* tr_rows = static_cast<T*>(dtrows.get(size_t(row_elems) * sizeof(T)));
+            T* tr_cols = static_cast<T*>(dtcols.get(size_t(col_elems) * sizeof(T)));
+            int* q2 = static_cast<int*>(dq.get(2 * sizeof(int)));
+            HB_CUDA(cudaMemsetAsync(q2, 0, 2 * sizeof(int), st));
+            auto tfn = P.pmax ? hb_tile_kernel<T, true, R> : hb_tile_kernel<T, false, R>;
+            HB_CUDA(allow_smem(reinterpret_cast<const void*>(tfn), mat_bytes));
+            int tocc = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tocc, tfn, 128, mat_bytes);
+            const int64_t tmax = int64_t(sms) * std::max(tocc, 1);
+            HbTileArgs TA{};
+            TA.jobs = dj; TA.tile_w = kHbTileW; TA.row_off = ro; TA.col_off = co; TA.queue = q2;
+            for (size_t d = 0; d + 1 < doff.size(); ++d) {
+                TA.tiles = ti + 3 * doff[d];
+                TA.n_items = doff[d + 1] - doff[d];
+                const unsigned tg = unsigned(std::min<int64_t>((TA.n_items + 3) / 4, tmax));
+                tfn<<<tg, 128, mat_bytes, st>>>(P.a, P.b, static_cast<const T*>(P.mat), P.N, gp, TA, o, tr_rows, tr_cols);
+                HB_CUDA(cudaGetLastError());
+                launches++;
+            }
+        }
         int32_t* res = static_cast<int32_t*>(dres.get(split.size() * 2 * sizeof(int32_t)));
         const int jgrid = int(std::min<int64_t>(int64_t(split.size()), int64_t(sms) * 8));
         hb_join_kernel<T><<<jgrid, 256, 0, st>>>(dj, int(split.size()), o, gp.go_b, res);
         HB_CUDA(cudaGetLastError());
-        launches += 2;
+        launches += (n_block ? 1 : 0) + 1;   // the block sweep, the join
         std::vector<int32_t> h(split.size() * 2);
         HB_CUDA(cudaMemcpyAsync(h.data(), res, h.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
         HB_CUDA(cudaStreamSynchronize(st));

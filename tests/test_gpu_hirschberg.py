@@ -45,6 +45,26 @@ def test_reference_fixtures(name, prec, tb, cut, mode, gap_model):
     assert tot == float(np.cumsum(z[key + "scores"])[-1])
 
 
+@pytest.mark.parametrize("pmax", [False, True])
+@pytest.mark.parametrize("mode", ["global", "local"])
+def test_tiled_half_sweeps_against_the_oracle(pmax, mode):
+    """Pairs of 7,000-9,000 residues: the half-sweeps of the top levels (8M cells and more) run
+    as tiles over the whole device (hb_tile_kernel), the rest as one block each; scores,
+    gradients and guides bit for bit the oracle's restatement of the reference's recursion."""
+    rng = np.random.default_rng(2500 + pmax + 2 * (mode == "local"))
+    mat = rand_matrix(rng, 20, integer=False)
+    gaps = np.array([[3.1, 0.7, 2.9, 0.8]])
+    sa = rand_seqs(rng, 3, 7000, 9000, AA) + rand_seqs(rng, 4, 600, 2000, AA)
+    sb = [mutate(rng, s, AA) for s in sa]
+    tb = "hirschberg_pmax" if pmax else "hirschberg"
+    s, g, gj, tot = _run(32, tb, 512, mat, gaps, sa, sb, mode)
+    enc = oracle.Encoded(encode(AA, sa), encode(AA, sb))
+    o = oracle.hirschberg(32, mat, gaps, enc, cutoff=512, pmax=pmax, local=(mode == "local"))
+    assert np.array_equal(s, o["scores"]), np.nonzero(s != o["scores"])[0][:5]
+    assert np.array_equal(g, o["grads"])
+    assert np.array_equal(gj, o["guides"])
+
+
 @pytest.mark.parametrize("name", ["int", "flt"])
 @pytest.mark.parametrize("prec", [32, 64])
 @pytest.mark.parametrize("tb", ["hirschberg", "hirschberg_pmax"])
