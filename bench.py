@@ -18,7 +18,7 @@ runs the same steps with the plain fill (one fixed geometry, 32 lanes x 4 rows, 
 per size bucket).  The serving arm streams requests (lengths log-uniform 20-5000, batch sizes
 log-uniform 1-4096, B a mutated copy of A) through the continuous-batching server and, for
 comparison, through plain-fill batches one request at a time, first as a burst (throughput)
-then as Poisson arrivals at 70 % of the plain arm's capacity (p50/p99 latency).
+then as Poisson arrivals at 70 % of the server's burst capacity (p50/p99 latency).
 
 Prints one JSON line (rank 0).  Under torchrun every rank aligns its own copy of the
 workload (weak scaling) and the margin gradients are summed over ranks (NCCL all-reduce).
@@ -373,8 +373,9 @@ def serve_bench(params, n_req, device, seed=5, n_lat=10000):
     serve_plain(params, reqs[:8], burst[:8], device)
     srv_burst = serve_server(params, reqs, burst, device)
     plain_burst = serve_plain(params, reqs, burst, device)
-    # Poisson arrivals at 70 % of the plain arm's capacity
-    rate = 0.7 * len(reqs) / plain_burst["seconds"]
+    # Poisson arrivals at 70 % of the server's own capacity (its burst throughput); the plain
+    # one-at-a-time arm gets the same arrivals, which it cannot keep up with
+    rate = 0.7 * len(reqs) / srv_burst["seconds"]
     rng = np.random.default_rng(seed + 1000)
     arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(reqs))).tolist()
     srv_poisson = serve_server(params, reqs, arrivals, device)

@@ -1044,6 +1044,7 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
         H.h_oa = s->oa.data(); H.h_ob = s->ob.data();
         H.cutoff = hb_cut; H.pmax = J.traceback == 4; H.local = loc ? 1 : 0; H.linear = aff ? 0 : 1;
         H.glocal = J.mode == 2 ? 1 : 0;
+        H.tile_budget = scratch_budget_of(s) / 2;
         H.K = s->K; H.gaps_t = gapT.p;
         if (tr) {   // linear, tracked (the fill's border set-up gave every tracked store its tracks)
             H.tracks = s->tracks.as<uint16_t>();

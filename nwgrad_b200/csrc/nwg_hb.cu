@@ -1218,9 +1218,7 @@ int64_t hb_run_t(const HbRun& P, cudaStream_t st, int sms) {
         std::vector<std::vector<int32_t>> diags;
         int64_t row_elems = 0, col_elems = 0, n_tiles = 0;
         {
-            size_t free_b = 0, total_b = 0;
-            cudaMemGetInfo(&free_b, &total_b);
-            const int64_t budget = int64_t(free_b / 4);
+            const int64_t budget = P.tile_budget;
             for (size_t q = 0; q < jobs.size(); ++q) {
                 SweepJob& x = jobs[q];
                 if ((int64_t(x.H) + 1) * (int64_t(x.W) + 1) < kHbTileCells) continue;

@@ -33,6 +33,7 @@ struct HbRun {
     int K;
     const void* gaps_t;
     const uint16_t* tracks; const uint16_t* gtracks;
+    int64_t tile_budget;                       // bytes the tiled half-sweeps' rows and lane states may hold
 };
 
 // Runs P on stream st (synchronising it); returns the number of kernel launches.  Throws
