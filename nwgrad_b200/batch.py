@@ -811,9 +811,10 @@ class SeqPairBatch:
         check(self._store._L.nwg_set_spin_limit(self._store.h, int(polls)))
 
     def use_graphs(self, enable: bool = True) -> None:
-        """Run each plan's per-bucket launches as one captured CUDA graph (the default), replayed
-        while the launches are unchanged (set_params steps keep them); False launches every
-        bucket directly.  Results are the same either way."""
+        """Run each plan's per-bucket launches as one captured CUDA graph (the default): captured
+        the second time the same launches run (a batch run once launches directly), replayed
+        while they are unchanged (set_params steps keep them); False launches every bucket
+        directly.  Results are the same either way."""
         check(self._store._L.nwg_set_graphs(self._store.h, 1 if enable else 0))
 
     def graph_stats(self):

@@ -19,6 +19,7 @@
 #include <numeric>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/nwgrad_b200.h"
@@ -217,11 +218,13 @@ Launch make_launch(const void* fn, unsigned grid, int block, size_t smem, const 
 // keep their address), a new batch or a grown scratch buffer does (a new capture).
 struct GraphCache {
     std::vector<unsigned char> key;
+    std::vector<unsigned char> seen;   // the last sequence launched directly (not yet captured)
     cudaGraphExec_t exec = nullptr;
     void reset() {
         if (exec) cudaGraphExecDestroy(exec);
         exec = nullptr;
         key.clear();
+        seen.clear();
     }
 };
 
@@ -250,8 +253,8 @@ bool geo_available(bool soft, int G, int R) {
 // Padded cells a geometry computes for an (m, n) problem over `rows` DP rows.
 double geo_cost(Geo g, int rows, int n, int extra_cols) {
     const int GR = g.G * g.R;
-    const double stripes = std::ceil(double(rows) / GR);
-    return stripes * GR * double(n + extra_cols + g.G - 1);
+    const int64_t stripes = (int64_t(rows) + GR - 1) / GR;
+    return double(stripes * GR) * double(n + extra_cols + g.G - 1);
 }
 
 // The geometry for one pair: a lane per pair when the rows fit one lane (up to 32 rows);
@@ -315,8 +318,8 @@ int long_warps(int rows, int GR) {
 // (rows x columns).  A bucket per doubling sizes its scratch stride close to its own pairs and
 // lets the autotuner pick a geometry per class.
 int size_class(int rows, int n) {
-    const double cells = double(std::max(rows, 1)) * double(std::max(n, 1));
-    return std::max(0, int(std::ceil(std::log2(cells))));
+    const uint64_t cells = uint64_t(std::max(rows, 1)) * uint64_t(std::max(n, 1));
+    return cells <= 1 ? 0 : 64 - __builtin_clzll(cells - 1);   // ceil(log2(cells))
 }
 
 
@@ -501,6 +504,13 @@ void run_launches(nwg_store* s, GraphCache* gc, const std::vector<Launch>& L, cu
         NWG_CUDA(cudaEventCreateWithFlags(&s->gev_in, cudaEventDisableTiming));
         NWG_CUDA(cudaEventCreateWithFlags(&s->gev_out, cudaEventDisableTiming));
     }
+    // a sequence seen for the first time launches directly (a batch run once -- a new store
+    // per batch -- never pays for a capture); the second time it is captured, then replayed
+    if ((!gc->exec || key != gc->key) && key != gc->seen) {
+        gc->seen = std::move(key);
+        launch_all(st);
+        return;
+    }
     NWG_CUDA(cudaEventRecord(s->gev_in, st));
     NWG_CUDA(cudaStreamWaitEvent(s->gstream, s->gev_in, 0));
     if (!gc->exec || key != gc->key) {
@@ -607,7 +617,8 @@ void build_plan(nwg_store* s, Plan& P, bool soft, int lanes, int rpl, int elem_b
     const int64_t n = s->n;
     // one lane per pair keeps a K*N*N histogram per lane in shared memory (soft)
     const bool lane_ok_soft = int64_t(s->K) * s->N * s->N * elem_bytes * 32 <= 48 * 1024;
-    std::vector<std::array<int, 3>> bkeys;
+    std::vector<std::array<int, 3>> bkeys;   // the distinct geometries
+    std::vector<int> btab;                   // per geometry and size class: its bucket (-1: none)
     // the tuner's choices per size class, looked up once
     constexpr int kClasses = 64;
     std::vector<const std::vector<nwg_store::GeoCost>*> cost_of(kClasses, nullptr);
@@ -641,14 +652,22 @@ void build_plan(nwg_store* s, Plan& P, bool soft, int lanes, int rpl, int elem_b
                 g = Geo{table_of[sc].first, table_of[sc].second};
             }
         }
-        // the bucket of (geometry, size class): few buckets, a linear search
-        const int k1 = g.G, k2 = g.R * 100 + g.mw + (g.tile ? 50 : 0), k3 = sc;
-        int bi = -1;
+        // the bucket of (geometry, size class): the geometry's index among the few distinct ones
+        // seen (a short search), then a table over size classes
+        const int k1 = g.G, k2 = g.R * 100 + g.mw + (g.tile ? 50 : 0);
+        int gi = -1;
         for (int q = 0; q < int(bkeys.size()); ++q)
-            if (bkeys[q][0] == k1 && bkeys[q][1] == k2 && bkeys[q][2] == k3) { bi = q; break; }
+            if (bkeys[q][0] == k1 && bkeys[q][1] == k2) { gi = q; break; }
+        if (gi < 0) {
+            gi = int(bkeys.size());
+            bkeys.push_back({k1, k2, 0});
+            btab.resize(bkeys.size() * kClasses, -1);
+        }
+        const int sci = std::min(sc, kClasses - 1);
+        int bi = btab[size_t(gi) * kClasses + sci];
         if (bi < 0) {
             bi = int(P.buckets.size());
-            bkeys.push_back({k1, k2, k3});
+            btab[size_t(gi) * kClasses + sci] = bi;
             P.buckets.push_back(Bucket{g, {}, 0, 0, 0});
         }
         P.buckets[bi].pairs.push_back(int32_t(p));
@@ -661,12 +680,28 @@ void build_plan(nwg_store* s, Plan& P, bool soft, int lanes, int rpl, int elem_b
     std::vector<int64_t> cells_v(size_t(n) + 1);
     int64_t* const pair_cells = cells_v.data();
     for (int64_t q = 0; q < n; ++q) pair_cells[q] = (s->oa[q + 1] - s->oa[q]) * (s->ob[q + 1] - s->ob[q]);
+    // longest first, to 1/64 of a doubling of the cells (a counting sort, stable: pair order
+    // within a bin): the persistent groups, which take pairs in this order from their work
+    // queue, then finish together
+    constexpr int kSortBins = 64 * 64;
+    auto sort_key = [](int64_t cells) -> int {
+        if (cells <= 1) return 0;
+        const uint64_t c = uint64_t(cells);
+        const int e = 63 - __builtin_clzll(c);                       // floor(log2)
+        const int frac = e >= 6 ? int((c >> (e - 6)) & 63) : int((c << (6 - e)) & 63);
+        return std::min(kSortBins - 1, e * 64 + frac);
+    };
+    std::vector<int32_t> bin_count(kSortBins + 1), sorted;
+    std::vector<int> keys;
     for (auto& B : P.buckets) {
-        // longest first: the persistent groups then finish together
-        std::sort(B.pairs.begin(), B.pairs.end(), [pair_cells](int32_t x, int32_t y) {
-            const int64_t cx = pair_cells[x], cy = pair_cells[y];
-            return cx != cy ? cx > cy : x < y;
-        });
+        const size_t np = B.pairs.size();
+        keys.resize(np);
+        std::fill(bin_count.begin(), bin_count.end(), 0);
+        for (size_t q = 0; q < np; ++q) { keys[q] = kSortBins - 1 - sort_key(pair_cells[B.pairs[q]]); ++bin_count[keys[q] + 1]; }
+        for (int k = 0; k < kSortBins; ++k) bin_count[k + 1] += bin_count[k];
+        sorted.resize(np);
+        for (size_t q = 0; q < np; ++q) sorted[size_t(bin_count[keys[q]]++)] = B.pairs[q];
+        B.pairs.swap(sorted);
         B.off = int64_t(order.size());
         for (int32_t p : B.pairs) {
             order.push_back(p);
@@ -699,8 +734,10 @@ void build_plan(nwg_store* s, Plan& P, bool soft, int lanes, int rpl, int elem_b
     // (s - 1, c) and (s, c - 1), both on the diagonal before its own.  Hard: rows 1..m and
     // columns 1..n, offsets in T; soft: rows 0..m and columns 0..n, offsets in columns, lane
     // states, tiles and stripes (the kernel scales them by its own state sizes)
-    std::vector<int64_t> roff(size_t(n) + 1, 0), coff(size_t(n) + 1, 0), toff(size_t(n) + 1, 0);
-    std::vector<int64_t> soff(size_t(n) + 1, 0);
+    bool any_tile = false;
+    for (auto& B : P.buckets) any_tile |= B.geo.tile && !B.pairs.empty();
+    const size_t tn = any_tile ? size_t(n) + 1 : 0;   // per-pair tile offsets only when tiles exist
+    std::vector<int64_t> roff(tn, 0), coff(tn, 0), toff(tn, 0), soff(tn, 0);
     std::vector<int32_t> tcount, scount;
     std::vector<std::vector<int32_t>> diags;
     for (auto& B : P.buckets) {
@@ -1457,11 +1494,26 @@ void load_pairs(nwg_store* s, const uint8_t* codes_a, const int64_t* off_a, cons
     const int64_t a0 = s->oa[0], b0 = s->ob[0];
     for (auto& v : s->oa) v -= a0;
     for (auto& v : s->ob) v -= b0;
-    // the largest code of each side (a branch-free loop the compiler vectorises)
+    // the largest code of each side (a branch-free loop the compiler vectorises; large inputs
+    // in parallel chunks on host threads)
     auto max_code = [](const uint8_t* x, int64_t len) {
-        uint8_t mx = 0;
-        for (int64_t k = 0; k < len; ++k) mx = x[k] > mx ? x[k] : mx;
-        return int(mx);
+        auto run = [](const uint8_t* y, int64_t l) {
+            uint8_t mx = 0;
+            for (int64_t k = 0; k < l; ++k) mx = y[k] > mx ? y[k] : mx;
+            return mx;
+        };
+        const int64_t kChunk = int64_t(4) << 20;
+        const int nth = int(std::min<int64_t>(8, (len + kChunk - 1) / kChunk));
+        if (nth <= 1) return int(run(x, len));
+        std::vector<uint8_t> part(size_t(nth), 0);
+        std::vector<std::thread> th;
+        const int64_t step = (len + nth - 1) / nth;
+        for (int t = 0; t < nth; ++t) {
+            const int64_t lo = t * step, hi = std::min(len, lo + step);
+            th.emplace_back([&, t, lo, hi] { part[size_t(t)] = lo < hi ? run(x + lo, hi - lo) : 0; });
+        }
+        for (auto& h : th) h.join();
+        return int(*std::max_element(part.begin(), part.end()));
     };
     if (s->total_a && max_code(codes_a + a0, s->total_a) >= nalpha) throw Error(NWG_EINVAL, "code out of range in sequence A");
     if (s->total_b && max_code(codes_b + b0, s->total_b) >= nalpha) throw Error(NWG_EINVAL, "code out of range in sequence B");

@@ -22,7 +22,6 @@ instead (one fixed geometry, 32 lanes x 4 rows, for every pair).
 from __future__ import annotations
 
 import json
-import math
 import os
 
 import numpy as np
@@ -32,7 +31,9 @@ SOFT_GEOS = [(32, 4), (32, 2), (32, 8), (16, 4), (16, 2), (16, 8), (8, 4), (1, 8
 
 
 def size_class(rows: int, cols: int) -> int:
-    return max(0, int(math.ceil(math.log2(max(rows, 1) * max(cols, 1)))))
+    """ceil(log2(rows x cols)), in integers (the store's own size_class)."""
+    c = max(rows, 1) * max(cols, 1)
+    return 0 if c <= 1 else (c - 1).bit_length()
 
 
 def _cache_path() -> str:
