@@ -80,9 +80,12 @@ def _classes(batch) -> dict:
     m = np.diff(batch._oa).astype(np.int64)
     n = np.diff(batch._ob).astype(np.int64)
     rows = m + 1 if _soft(batch) else m
-    cells = np.maximum(rows, 1).astype(np.float64) * np.maximum(n, 1).astype(np.float64)
-    sc = np.maximum(0, np.ceil(np.log2(cells))).astype(np.int64)
-    return {int(c): np.nonzero(sc == c)[0] for c in np.unique(sc)}
+    cells = np.maximum(rows, 1) * np.maximum(n, 1)
+    # ceil(log2(cells)) in integers, as the store computes it: the binary exponent of cells - 1
+    sc = np.where(cells <= 1, 0, np.frexp(np.maximum(cells - 1, 1).astype(np.float64))[1]).astype(np.int64)
+    order = np.argsort(sc, kind="stable")
+    bounds = np.flatnonzero(np.diff(sc[order])) + 1
+    return {int(sc[g[0]]): g for g in np.split(order, bounds) if g.size}   # each in pair order (stable)
 
 
 def _codes(batch):
