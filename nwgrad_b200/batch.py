@@ -332,27 +332,17 @@ class SeqPairBatch:
 
     def _check_hirschberg(self):
         """Hirschberg splits pairs longer than hb_cutoff rows; this build implements the split
-        for untracked batches, affine or linear, and tracked linear ones, Global or Local (the
-        reference's viterbi_affine_hirschberg, viterbi_affine_hirschberg_local,
-        viterbi_linear_hirschberg); tracked affine splits are not built."""
-        if self._am == 2:
-            # glocal ends split untracked pairs (viterbi_affine_hirschberg_glocal, the linear
-            # glocal branch of viterbi_linear_hirschberg); other free-end sets run Pointers, as in
-            # the reference (aligner.hpp:2323-2330)
-            if self._sg != SG_GLOCAL or not self._tracked:
-                return
-            if self._n and int(np.max(np.diff(self._oa))) > self._hb_cutoff:
-                raise NotImplementedError(
-                    f"nwgrad_b200: traceback=\"{self._traceback}\" with mode \"{self._mode}\" splits pairs "
-                    f"in this build only for untracked batches; use traceback=\"pointers\" or \"auto\"")
+        for affine and linear gaps, Global, Local and glocal, tracked or not (the reference's
+        viterbi_affine_hirschberg / _local / _glocal with hb_reverse_rows_ for tracks, and
+        viterbi_linear_hirschberg) -- except linear glocal with tracks.  Other semi-global
+        free-end sets run Pointers, as in the reference (aligner.hpp:2323-2330)."""
+        if self._am != 2 or self._sg != SG_GLOCAL:
             return
-        if not self._tracked or self._gap_model == "linear":
-            return
-        if self._n and int(np.max(np.diff(self._oa))) > self._hb_cutoff:
+        if self._tracked and self._gap_model == "linear" and self._n and \
+                int(np.max(np.diff(self._oa))) > self._hb_cutoff:
             raise NotImplementedError(
-                f"nwgrad_b200: traceback=\"{self._traceback}\" splits pairs longer than hb_cutoff only for "
-                f"untracked batches and tracked linear ones in this build (this batch: {self._gap_model} {self._mode}"
-                f"{', tracked' if self._tracked else ''}); use traceback=\"pointers\" or \"auto\"")
+                f"nwgrad_b200: traceback=\"{self._traceback}\" with mode \"{self._mode}\" splits tracked pairs "
+                f"in this build only with affine gaps; use traceback=\"pointers\" or \"auto\"")
 
     @property
     def hb_cutoff(self) -> int:

@@ -811,9 +811,9 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
     const bool band = J.band >= 0;
     // Hirschberg (untracked, full DP): pairs longer than the cutoff split (Local: by the
     // endpoint scans and their box)
-    // (semi-global ends: glocal's only, untracked -- aligner.hpp:2323-2330, 4709, 5132)
-    const bool glocal_hb = J.mode == 2 && J.free_ends == 12 && !tr;
-    const bool hb = !band && (J.mode != 2 || glocal_hb) && (!tr || !aff) && (J.traceback == 3 || J.traceback == 4);
+    // (semi-global ends: glocal's only -- aligner.hpp:2323-2330, 4709, 5132; tracked, affine)
+    const bool glocal_hb = J.mode == 2 && J.free_ends == 12 && (!tr || aff);
+    const bool hb = !band && (J.mode != 2 || glocal_hb) && (J.traceback == 3 || J.traceback == 4);
     const int hb_cut = hb ? (J.hb_cutoff > 0 ? J.hb_cutoff : 512) : 0;
     std::vector<int32_t> hb_pairs;
     if (hb) {
@@ -1083,7 +1083,7 @@ void run_hard(nwg_store* s, const nwg_job& J, cudaStream_t st, bool want_grad, b
         H.glocal = J.mode == 2 ? 1 : 0;
         H.tile_budget = scratch_budget_of(s) / 2;
         H.K = s->K; H.gaps_t = gapT.p;
-        if (tr) {   // linear, tracked (the fill's border set-up gave every tracked store its tracks)
+        if (tr) {   // tracked (the fill's border set-up gave every tracked store its tracks)
             H.tracks = s->tracks.as<uint16_t>();
             H.gtracks = s->gtracks.p ? s->gtracks.as<uint16_t>() : nullptr;
         }

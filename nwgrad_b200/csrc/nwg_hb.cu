@@ -50,6 +50,10 @@ struct SweepJob {
     int a_step, b_step;
     int H, W, flag;
     int tiled;                       // swept by hb_tile_kernel (hb_sweep_kernel skips it)
+    // tracked: row t >= 0 consumes DP row di = i_base + i_step t (its set; a reverse sweep's
+    // gaps in A lie in row di - 1); the pair's m and track offsets (oa[p], oa[p] + p)
+    int i_base, i_step, pm, pad2;
+    int64_t tk_off, gk_off;
     int64_t out;                     // T offset of the last row: M, X, Y arrays of W + 1
     int64_t wrap;                    // T offset of the wrap row buffer (3 (W + 1))
 };
@@ -57,8 +61,8 @@ struct SweepJob {
 struct BaseJob {
     int64_t a_base, b_base;          // row t >= 1 reads a[a_base + t - 1]; column c >= 1 b[b_base + c - 1]
     int H, W, in_x, out_x;
-    int i0, pad;                     // linear, tracked: the DP row of the block's row 0
-    int64_t tk_off, gk_off;          // linear, tracked: the pair's track offsets (oa[p], oa[p] + p)
+    int i0, pm;                      // tracked: the DP row of the block's row 0, the pair's m
+    int64_t tk_off, gk_off;          // tracked: the pair's track offsets (oa[p], oa[p] + p)
     int64_t codes;                   // byte offset of the (H + 1) x (W + 1) code table
     int64_t bnd;                     // T offset of the stripe boundary row (3 (W + 1))
     int64_t moves;                   // byte offset of the moves (walk order, H + W at most)
@@ -69,9 +73,49 @@ struct ScanJob {
     int a_step, b_step;
     int H, W, local;
     int glocal;                      // 1: the glocal end scan, 2: the glocal start scan (see hb_scan_kernel)
+    int i_base, i_step, pm, pad2;    // tracked: as SweepJob's
+    int64_t tk_off, gk_off;
 };
 
 template <class T> struct Gaps { T go_a, ge_a, go_b, ge_b; };
+
+// Per-row affine parameters of a tracked pair (aligner.hpp:1848-1871, 1907-1910): DP row i's
+// substitution set and the gap moves into it (a gap in B, its residue's set) and within it (a
+// gap in A, its gap set); a reverse sweep's vertical move into row i is rewritten
+// (hb_reverse_rows_): the open of row i + 1 (row m: its own) and its own extend plus the
+// difference of the two opens.  tk null: untracked, the one set `u`.
+template <class T>
+struct AffRows {
+    const uint16_t* tk; const uint16_t* gk; const T* gaps; Gaps<T> u;
+    __device__ __forceinline__ int tset(int i) const { return int(tk[i - 1]); }
+    __device__ __forceinline__ int gset(int i) const { return gk ? int(gk[i]) : (i == 0 ? int(tk[0]) : int(tk[i - 1])); }
+    // the parameters of sweep row t consuming DP row di (rev: a reverse sweep), as one Gaps
+    __device__ __forceinline__ Gaps<T> row(int di, bool rev, int m) const {
+        if (!tk) return u;
+        Gaps<T> g;
+        const int ga = gset(rev ? di - 1 : di);
+        g.go_a = gaps[4 * ga]; g.ge_a = gaps[4 * ga + 1];
+        if (di >= 1 && di <= m) {
+            const int tb = tset(di);
+            const T ob = gaps[4 * tb + 2], eb = gaps[4 * tb + 3];
+            if (rev) {
+                const T on = di < m ? gaps[4 * tset(di + 1) + 2] : ob;
+                g.go_b = on; g.ge_b = eb + (ob - on);
+            } else {
+                g.go_b = ob; g.ge_b = eb;
+            }
+        } else {
+            g.go_b = u.go_b; g.ge_b = u.ge_b;
+        }
+        return g;
+    }
+    __device__ __forceinline__ int key(int di, int ac, int N) const { return tk ? (tset(di) * N + ac) * N : ac * N; }
+    __device__ __forceinline__ AffRows at(int64_t tk_off, int64_t gk_off) const {
+        AffRows r = *this;
+        if (tk) { r.tk = tk + tk_off; r.gk = gk ? gk + gk_off : nullptr; }
+        return r;
+    }
+};
 
 // Per-row linear parameters of a tracked pair: the substitution row, the extend of a gap in B
 // into DP row i (its residue's set) and of a gap in A within DP row i (its gap set).
@@ -108,12 +152,12 @@ __device__ __forceinline__ T chain_x(T um, T ux, T uy, const Gaps<T>& g) {
 // from the previous stripe's bottom row (a per-warp row in global memory) or row 0.
 template <class T, bool PMAX, int R>
 __global__ void __launch_bounds__(128) hb_scan_kernel(const uint8_t* __restrict__ a, const uint8_t* __restrict__ b,
-                                                      const T* __restrict__ mat, int N, Gaps<T> gp,
+                                                      const T* __restrict__ mat, int N, AffRows<T> AR, int K,
                                                       const ScanJob* __restrict__ jobs, int n_jobs, T* rows,
                                                       int64_t row_stride, int32_t* __restrict__ res) {
     extern __shared__ __align__(16) unsigned char hb_smem[];
     T* smat = reinterpret_cast<T*>(hb_smem);
-    for (int k = threadIdx.x; k < N * N; k += blockDim.x) smat[k] = mat[k];
+    for (int k = threadIdx.x; k < K * N * N; k += blockDim.x) smat[k] = mat[k];
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const int wpb = blockDim.x >> 5;
@@ -121,12 +165,14 @@ __global__ void __launch_bounds__(128) hb_scan_kernel(const uint8_t* __restrict_
     const int64_t nwarps = int64_t(gridDim.x) * wpb;
     T* bnd = rows + wg * row_stride;
     const T NI = ninf<T>();
-    const T go_a = gp.go_a, ge_a = gp.ge_a, go_b = gp.go_b, ge_b = gp.ge_b;
     for (int64_t jb = wg; jb < n_jobs; jb += nwarps) {
         const ScanJob J = jobs[jb];
         const int H = J.H, W = J.W;
         const bool loc = J.local != 0;
         const int gl = J.glocal;
+        const bool rev = J.a_step < 0;
+        const AffRows<T> AJ = AR.at(J.tk_off, J.gk_off);
+        const Gaps<T> g0 = AJ.row(J.i_base, rev, J.pm);   // the block's row 0 (its gaps in A)
         T bv = gl ? NI : T(0); int bi = 0, bj = 0;
         if (H > 0 && W > 0) {
             const int nst = (H + 32 * R - 1) / (32 * R);
@@ -134,12 +180,15 @@ __global__ void __launch_bounds__(128) hb_scan_kernel(const uint8_t* __restrict_
                 const int i0 = s * 32 * R + lane * R + 1;   // block row of this lane's first row
                 int code[R];
                 bool valid[R];
+                Gaps<T> rg[R];
                 T cM[R], cX[R], cY[R], P[R];
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
                     const int i = i0 + r;
+                    const int di = J.i_base + J.i_step * i;
                     valid[r] = i <= H;
-                    code[r] = valid[r] ? int(a[J.a_base + int64_t(J.a_step) * (i - 1)]) * N : 0;
+                    code[r] = valid[r] ? AJ.key(di, int(a[J.a_base + int64_t(J.a_step) * (i - 1)]), N) : 0;
+                    rg[r] = AJ.row(di, rev, J.pm);
                     cM[r] = NI; cX[r] = NI; cY[r] = NI; P[r] = NI;
                 }
                 T dgM = NI, dgX = NI, dgY = NI;       // row above, column c - 1
@@ -156,7 +205,7 @@ __global__ void __launch_bounds__(128) hb_scan_kernel(const uint8_t* __restrict_
                             if (c == 0 || loc || gl == 1) { upM = T(0); upX = NI; upY = NI; }
                             else {
                                 upM = NI; upX = NI;
-                                upY = hmax((hmax(r0M, r0X) - go_a) - ge_a, r0Y - ge_a);
+                                upY = hmax((hmax(r0M, r0X) - g0.go_a) - g0.ge_a, r0Y - g0.ge_a);
                             }
                             r0M = upM; r0X = upX; r0Y = upY;
                         } else {
@@ -168,15 +217,16 @@ __global__ void __launch_bounds__(128) hb_scan_kernel(const uint8_t* __restrict_
                         T qM = upM, qX = upX, qY = upY;
                         T pM = dgM, pX = dgX, pY = dgY;
                         const int bc = c >= 1 ? int(b[J.b_base + int64_t(J.b_step) * (c - 1)]) : 0;
-                        const T rmpc = (PMAX && c >= 1) ? static_cast<T>(c - 1) * ge_a : T(0);
 #pragma unroll
                         for (int r = 0; r < R; ++r) {
+                            const Gaps<T>& q = rg[r];
+                            const T rmpc = (PMAX && c >= 1) ? mul_rn(static_cast<T>(c - 1), q.ge_a) : T(0);
                             T m, x, y;
-                            x = hmax3((qM - go_b) - ge_b, qX - ge_b, (qY - go_b) - ge_b);
+                            x = hmax3((qM - q.go_b) - q.ge_b, qX - q.ge_b, (qY - q.go_b) - q.ge_b);
                             if (c == 0) {
                                 m = loc ? T(0) : NI;
                                 y = NI;
-                                if constexpr (PMAX) P[r] = y - ge_a;
+                                if constexpr (PMAX) P[r] = y - q.ge_a;
                                 if (gl && i0 + r == H) {   // glocal: row H's column 0 is a candidate
                                     const T here = gl == 2 ? hmax(m, x) : hmax3(m, x, y);
                                     if (here > bv) { bv = here; bi = H; bj = 0; }
@@ -185,11 +235,11 @@ __global__ void __launch_bounds__(128) hb_scan_kernel(const uint8_t* __restrict_
                                 m = hmax3(pM, pX, pY) + smat[code[r] + bc];
                                 if (loc) m = hmax(m, T(0));
                                 if constexpr (PMAX) {
-                                    const T gg = (hmax(cM[r], cX[r]) - go_a) - ge_a;
-                                    P[r] = hmax(gg + rmpc, P[r]);
+                                    const T gg = (hmax(cM[r], cX[r]) - q.go_a) - q.ge_a;
+                                    P[r] = hmax(add_rn(gg, rmpc), P[r]);
                                     y = P[r] - rmpc;
                                 } else {
-                                    y = hmax3((cM[r] - go_a) - ge_a, (cX[r] - go_a) - ge_a, cY[r] - ge_a);
+                                    y = hmax3((cM[r] - q.go_a) - q.ge_a, (cX[r] - q.go_a) - q.ge_a, cY[r] - q.ge_a);
                                 }
                                 if (gl) {
                                     if (i0 + r == H) {
@@ -235,14 +285,14 @@ __global__ void __launch_bounds__(128) hb_scan_kernel(const uint8_t* __restrict_
 // ── sweep ─────────────────────────────────────────────────────────────────────
 template <class T, bool PMAX, int R>
 __global__ void __launch_bounds__(512) hb_sweep_kernel(const uint8_t* __restrict__ a, const uint8_t* __restrict__ b,
-                                                       const T* __restrict__ mat, int N, Gaps<T> gp,
+                                                       const T* __restrict__ mat, int N, AffRows<T> AR, int K,
                                                        const SweepJob* __restrict__ jobs, int n_jobs,
                                                        T* __restrict__ out, T* __restrict__ wrapbuf) {
     constexpr int G = 32, GR = G * R;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* smat = reinterpret_cast<T*>(smem_raw);
-    T* ring = smat + ((N * N + 3) & ~3);                   // [NW][3][kHbRing]
-    for (int k = threadIdx.x; k < N * N; k += blockDim.x) smat[k] = mat[k];
+    T* ring = smat + ((K * N * N + 3) & ~3);               // [NW][3][kHbRing]
+    for (int k = threadIdx.x; k < K * N * N; k += blockDim.x) smat[k] = mat[k];
     __syncthreads();
     const int NW = blockDim.x / G;
     const int w = threadIdx.x / G, lane = threadIdx.x % G;
@@ -266,8 +316,10 @@ __global__ void __launch_bounds__(512) hb_sweep_kernel(const uint8_t* __restrict
 
         int sn = 0, i0 = 0;
         int key[R];
+        Gaps<T> rg[R];                                     // each row's gap parameters
         T cM[R], cX[R], cY[R], P[R];
         T dgM = NI, dgX = NI, dgY = NI, upM = NI, upX = NI, upY = NI;
+        const AffRows<T> AJ = AR.at(J.tk_off, J.gk_off);
         for (int64_t K = 0; K < supers; ++K) {
             const int64_t v = K - 2 * w;
             if (v >= 0 && v < chunks) {
@@ -278,7 +330,9 @@ __global__ void __launch_bounds__(512) hb_sweep_kernel(const uint8_t* __restrict
 #pragma unroll
                     for (int r = 0; r < R; ++r) {
                         const int t = i0 + r;
-                        key[r] = (t >= 1 && t <= H) ? int(a[J.a_base + int64_t(J.a_step) * (t - 1)]) * N : 0;
+                        const int di = J.i_base + J.i_step * t;
+                        key[r] = (t >= 1 && t <= H) ? AJ.key(di, int(a[J.a_base + int64_t(J.a_step) * (t - 1)]), N) : 0;
+                        rg[r] = AJ.row(di, J.a_step < 0, J.pm);
                         cM[r] = NI; cX[r] = NI; cY[r] = NI; P[r] = NI;
                     }
                     dgM = dgX = dgY = NI; upM = upX = upY = NI;
@@ -307,20 +361,20 @@ __global__ void __launch_bounds__(512) hb_sweep_kernel(const uint8_t* __restrict
                                 T mv, xv, yv;
                                 if (t == 0) {
                                     if (c == 0) { mv = J.flag ? NI : T(0); xv = NI; yv = NI; }
-                                    else { mv = NI; xv = NI; yv = chain_y(cM[r], cX[r], cY[r], gp); }
+                                    else { mv = NI; xv = NI; yv = chain_y(cM[r], cX[r], cY[r], rg[r]); }
                                 } else if (c == 0) {
                                     mv = NI; yv = NI;
-                                    xv = (t == 1 && J.flag) ? T(0) - gp.ge_b : chain_x(qM, qX, qY, gp);
+                                    xv = (t == 1 && J.flag) ? T(0) - rg[r].ge_b : chain_x(qM, qX, qY, rg[r]);
                                 } else {
                                     mv = hmax3(pM, pX, pY) + smat[key[r] + bj];
-                                    xv = chain_x(qM, qX, qY, gp);
+                                    xv = chain_x(qM, qX, qY, rg[r]);
                                     if constexpr (PMAX) {
-                                        const T g = (hmax(cM[r], cX[r]) - gp.go_a) - gp.ge_a;
-                                        const T rm = mul_rn(static_cast<T>(c - 1), gp.ge_a);
+                                        const T g = (hmax(cM[r], cX[r]) - rg[r].go_a) - rg[r].ge_a;
+                                        const T rm = mul_rn(static_cast<T>(c - 1), rg[r].ge_a);
                                         P[r] = hmax(add_rn(g, rm), P[r]);
                                         yv = P[r] - rm;
                                     } else {
-                                        yv = chain_y(cM[r], cX[r], cY[r], gp);
+                                        yv = chain_y(cM[r], cX[r], cY[r], rg[r]);
                                     }
                                 }
                                 pM = cM[r]; pX = cX[r]; pY = cY[r];
@@ -369,12 +423,13 @@ struct HbTileArgs {
 };
 template <class T, bool PMAX, int R>
 __global__ void __launch_bounds__(128) hb_tile_kernel(const uint8_t* __restrict__ a, const uint8_t* __restrict__ b,
-                                                      const T* __restrict__ mat, int N, Gaps<T> gp, HbTileArgs A,
-                                                      T* __restrict__ out, T* __restrict__ rows, T* __restrict__ cols) {
+                                                      const T* __restrict__ mat, int N, AffRows<T> AR, int K,
+                                                      HbTileArgs A, T* __restrict__ out, T* __restrict__ rows,
+                                                      T* __restrict__ cols) {
     constexpr int G = 32, GR = G * R, LSZ = 4 * R;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* smat = reinterpret_cast<T*>(smem_raw);
-    for (int k = threadIdx.x; k < N * N; k += blockDim.x) smat[k] = mat[k];
+    for (int k = threadIdx.x; k < K * N * N; k += blockDim.x) smat[k] = mat[k];
     __syncthreads();
     const int lane = threadIdx.x % G, gpb = blockDim.x / G;
     const T NI = ninf<T>();
@@ -395,12 +450,16 @@ __global__ void __launch_bounds__(128) hb_tile_kernel(const uint8_t* __restrict_
         const T* const above = rowp + int64_t(s - 1) * 3 * (W + 1);   // s > 0
         T* const below = rowp + int64_t(s) * 3 * (W + 1);
         const int i0 = s * GR + lane * R;
+        const AffRows<T> AJ = AR.at(J.tk_off, J.gk_off);
         int key[R];
+        Gaps<T> rg[R];
         T cM[R], cX[R], cY[R], P[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const int t = i0 + r;
-            key[r] = (t >= 1 && t <= H) ? int(a[J.a_base + int64_t(J.a_step) * (t - 1)]) * N : 0;
+            const int di = J.i_base + J.i_step * t;
+            key[r] = (t >= 1 && t <= H) ? AJ.key(di, int(a[J.a_base + int64_t(J.a_step) * (t - 1)]), N) : 0;
+            rg[r] = AJ.row(di, J.a_step < 0, J.pm);
             cM[r] = NI; cX[r] = NI; cY[r] = NI; P[r] = NI;
         }
         T dgM = NI, dgX = NI, dgY = NI, upM = NI, upX = NI, upY = NI;
@@ -438,20 +497,20 @@ __global__ void __launch_bounds__(128) hb_tile_kernel(const uint8_t* __restrict_
                     T mv, xv, yv;
                     if (t2 == 0) {
                         if (c == 0) { mv = J.flag ? NI : T(0); xv = NI; yv = NI; }
-                        else { mv = NI; xv = NI; yv = chain_y(cM[r], cX[r], cY[r], gp); }
+                        else { mv = NI; xv = NI; yv = chain_y(cM[r], cX[r], cY[r], rg[r]); }
                     } else if (c == 0) {
                         mv = NI; yv = NI;
-                        xv = (t2 == 1 && J.flag) ? T(0) - gp.ge_b : chain_x(qM, qX, qY, gp);
+                        xv = (t2 == 1 && J.flag) ? T(0) - rg[r].ge_b : chain_x(qM, qX, qY, rg[r]);
                     } else {
                         mv = hmax3(pM, pX, pY) + smat[key[r] + bj];
-                        xv = chain_x(qM, qX, qY, gp);
+                        xv = chain_x(qM, qX, qY, rg[r]);
                         if constexpr (PMAX) {
-                            const T g = (hmax(cM[r], cX[r]) - gp.go_a) - gp.ge_a;
-                            const T rm = mul_rn(static_cast<T>(c - 1), gp.ge_a);
+                            const T g = (hmax(cM[r], cX[r]) - rg[r].go_a) - rg[r].ge_a;
+                            const T rm = mul_rn(static_cast<T>(c - 1), rg[r].ge_a);
                             P[r] = hmax(add_rn(g, rm), P[r]);
                             yv = P[r] - rm;
                         } else {
-                            yv = chain_y(cM[r], cX[r], cY[r], gp);
+                            yv = chain_y(cM[r], cX[r], cY[r], rg[r]);
                         }
                     }
                     pM = cM[r]; pX = cX[r]; pY = cY[r];
@@ -480,13 +539,17 @@ __global__ void __launch_bounds__(128) hb_tile_kernel(const uint8_t* __restrict_
 // Split block k: forward sweep 2k, reverse sweep 2k + 1.  res[2k] = column, res[2k+1] = span.
 template <class T>
 __global__ void hb_join_kernel(const SweepJob* __restrict__ jobs, int n_blocks, const T* __restrict__ out,
-                               T go_b, int32_t* __restrict__ res) {
+                               AffRows<T> AR, int32_t* __restrict__ res) {
     __shared__ T sv[256];
     __shared__ int sc[256], ss[256];
     const T NI = ninf<T>();
     for (int k = blockIdx.x; k < n_blocks; k += gridDim.x) {
         const SweepJob F = jobs[2 * k], Rv = jobs[2 * k + 1];
         const int W = F.W;
+        // the open refunded to an X run straddling the cut: tracked, that of the first row
+        // below it, DP row p + 1 (aligner.hpp:4497)
+        const int p = F.i_base + F.H;
+        const T go_b = AR.tk ? AR.at(F.tk_off, F.gk_off).row(p + 1, false, F.pm).go_b : AR.u.go_b;
         const T* FM = out + F.out; const T* FX = FM + (W + 1); const T* FY = FX + (W + 1);
         const T* rM = out + Rv.out; const T* rX = rM + (W + 1); const T* rY = rX + (W + 1);
         T best = NI; int bc = 0x7fffffff, bs = 0;
@@ -532,14 +595,14 @@ __device__ __forceinline__ uint32_t pick_hb(T vm, T vx, T vy) {
 
 template <class T, int R>
 __global__ void __launch_bounds__(128) hb_base_kernel(const uint8_t* __restrict__ a, const uint8_t* __restrict__ b,
-                                                      const T* __restrict__ mat, int N, Gaps<T> gp,
+                                                      const T* __restrict__ mat, int N, AffRows<T> AR, int K,
                                                       const BaseJob* __restrict__ jobs, int n_jobs,
                                                       uint8_t* __restrict__ codes, T* __restrict__ bndbuf,
                                                       uint8_t* __restrict__ moves, int32_t* __restrict__ nmoves) {
     constexpr int G = 32, GR = G * R;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* smat = reinterpret_cast<T*>(smem_raw);
-    for (int k = threadIdx.x; k < N * N; k += blockDim.x) smat[k] = mat[k];
+    for (int k = threadIdx.x; k < K * N * N; k += blockDim.x) smat[k] = mat[k];
     __syncthreads();
     const int lane = threadIdx.x % G;
     const int wpb = blockDim.x / G;
@@ -552,14 +615,17 @@ __global__ void __launch_bounds__(128) hb_base_kernel(const uint8_t* __restrict_
         T* bM = bndbuf + J.bnd; T* bX = bM + st; T* bY = bX + st;
         const int ns = (H + 1 + GR - 1) / GR;
         T eM = NI, eX = NI, eY = NI;                       // row H, column W (its owner lane)
+        const AffRows<T> AJ = AR.at(J.tk_off, J.gk_off);
         for (int s = 0; s < ns; ++s) {
             const int i0 = s * GR + lane * R;
             int key[R];
+            Gaps<T> rg[R];                                 // row t is DP row J.i0 + t
             T cM[R], cX[R], cY[R];
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 const int t = i0 + r;
-                key[r] = (t >= 1 && t <= H) ? int(a[J.a_base + t - 1]) * N : 0;
+                key[r] = (t >= 1 && t <= H) ? AJ.key(J.i0 + t, int(a[J.a_base + t - 1]), N) : 0;
+                rg[r] = AJ.row(J.i0 + t, false, J.pm);
                 cM[r] = NI; cX[r] = NI; cY[r] = NI;
             }
             T dgM = NI, dgX = NI, dgY = NI, upM = NI, upX = NI, upY = NI;
@@ -579,18 +645,21 @@ __global__ void __launch_bounds__(128) hb_base_kernel(const uint8_t* __restrict_
                         if (t == 0) {
                             if (c == 0) { mv = J.in_x ? NI : T(0); xv = NI; yv = NI; code = 3u | (3u << 2) | (3u << 4); }
                             else {
-                                const T uy = (cM[r] - gp.go_a) - gp.ge_a, vy = (cX[r] - gp.go_a) - gp.ge_a, wy = cY[r] - gp.ge_a;
+                                const Gaps<T>& q = rg[r];
+                                const T uy = (cM[r] - q.go_a) - q.ge_a, vy = (cX[r] - q.go_a) - q.ge_a, wy = cY[r] - q.ge_a;
                                 mv = NI; xv = NI; yv = hmax3(uy, vy, wy);
                                 code = 3u | (3u << 2) | (pick_hb(uy, vy, wy) << 4);
                             }
                         } else if (c == 0) {
-                            const T ux = (qM - gp.go_b) - gp.ge_b, vx = qX - gp.ge_b, wx = (qY - gp.go_b) - gp.ge_b;
+                            const Gaps<T>& q = rg[r];
+                            const T ux = (qM - q.go_b) - q.ge_b, vx = qX - q.ge_b, wx = (qY - q.go_b) - q.ge_b;
                             mv = NI; yv = NI; xv = hmax3(ux, vx, wx);
                             code = 3u | (pick_hb(ux, vx, wx) << 2) | (3u << 4);
-                            if (J.in_x && t == 1) { xv = T(0) - gp.ge_b; code = 3u | (1u << 2) | (3u << 4); }
+                            if (J.in_x && t == 1) { xv = T(0) - q.ge_b; code = 3u | (1u << 2) | (3u << 4); }
                         } else {
-                            const T ux = (qM - gp.go_b) - gp.ge_b, vx = qX - gp.ge_b, wx = (qY - gp.go_b) - gp.ge_b;
-                            const T uy = (cM[r] - gp.go_a) - gp.ge_a, vy = (cX[r] - gp.go_a) - gp.ge_a, wy = cY[r] - gp.ge_a;
+                            const Gaps<T>& q = rg[r];
+                            const T ux = (qM - q.go_b) - q.ge_b, vx = qX - q.ge_b, wx = (qY - q.go_b) - q.ge_b;
+                            const T uy = (cM[r] - q.go_a) - q.ge_a, vy = (cX[r] - q.go_a) - q.ge_a, wy = cY[r] - q.ge_a;
                             mv = hmax3(pM, pX, pY) + smat[key[r] + bj];
                             xv = hmax3(ux, vx, wx);
                             yv = hmax3(uy, vy, wy);
@@ -652,8 +721,8 @@ __global__ void hb_replay_kernel(const HbRun P, const BaseJob* __restrict__ jobs
     const T go_a = static_cast<T>(P.go_a), ge_a = static_cast<T>(P.ge_a);
     const T go_b = static_cast<T>(P.go_b), ge_b = static_cast<T>(P.ge_b);
     double* g = P.grad ? P.grad + P.gstride * p : nullptr;
-    // tracked (linear): each row's substitution set and extends
-    const bool trk = P.linear && P.tracks != nullptr;
+    // tracked: each row's substitution set and gap costs (opens too, affine)
+    const bool trk = P.tracks != nullptr;
     const LinRows<T> LR{P.tracks + (trk ? ao : 0), P.gtracks ? P.gtracks + ao + p : nullptr,
                         static_cast<const T*>(P.gaps_t), N};
     const int64_t NN = int64_t(trk ? P.K : 1) * N * N;
@@ -699,14 +768,14 @@ __global__ void hb_replay_kernel(const HbRun P, const BaseJob* __restrict__ jobs
                 if (gj) gj[i] = j;
             } else if (op == 1) {
                 ++i;
-                if (!P.linear && prev != 1) { s -= go_b; if (g) g[NN + 2] -= 1.0; }
                 const int64_t o = NN + 4 * int64_t(trk ? LR.tset(i) : 0);
+                if (!P.linear && prev != 1) { s -= trk ? LR.gaps[o - NN + 2] : go_b; if (g) g[o + 2] -= 1.0; }
                 s -= trk ? LR.gb(i) : ge_b;
                 if (g) g[o + 3] -= 1.0;
                 if (gj) gj[i] = j;
             } else {
-                if (!P.linear && prev != 2) { s -= go_a; if (g) g[NN + 0] -= 1.0; }
                 const int64_t o = NN + 4 * int64_t(trk ? LR.gset(i) : 0);
+                if (!P.linear && prev != 2) { s -= trk ? LR.gaps[o - NN] : go_a; if (g) g[o + 0] -= 1.0; }
                 s -= trk ? LR.ga(i) : ge_a;
                 if (g) g[o + 1] -= 1.0;
                 ++j;
@@ -1081,6 +1150,15 @@ int64_t hb_run_t(const HbRun& P, cudaStream_t st, int sms) {
     if (n == 0) return 0;
     int64_t launches = 0;
     const Gaps<T> gp{static_cast<T>(P.go_a), static_cast<T>(P.ge_a), static_cast<T>(P.go_b), static_cast<T>(P.ge_b)};
+    // tracked: every row's parameters from the tracks (K sets of K x N x N and K x 4 in T)
+    const bool trk = P.tracks != nullptr;
+    const int K = trk ? std::max(P.K, 1) : 1;
+    const AffRows<T> AR{trk ? P.tracks : nullptr, trk ? P.gtracks : nullptr, static_cast<const T*>(P.gaps_t), gp};
+    // a job's tracked fields: row t consumes DP row i_base + i_step t
+    auto track = [&](auto& J, int p, int i_base, int i_step) {
+        J.i_base = i_base; J.i_step = i_step; J.pm = int(P.h_oa[p + 1] - P.h_oa[p]);
+        J.tk_off = P.h_oa[p]; J.gk_off = P.h_oa[p] + p;
+    };
     std::vector<Blk> cur;
     cur.reserve(size_t(n));
     constexpr int R = 4;
@@ -1100,7 +1178,7 @@ int64_t hb_run_t(const HbRun& P, cudaStream_t st, int sms) {
         // 0; the box A x B[js, je) (a pair without B: column 0).  Either box then runs as a
         // Global pair.
         boxes.assign(size_t(n) * 4, 0);
-        const size_t mat_b = size_t((P.N * P.N + 3) & ~3) * sizeof(T);
+        const size_t mat_b = size_t((K * P.N * P.N + 3) & ~3) * sizeof(T);
         auto run_scans = [&](const std::vector<ScanJob>& sj, std::vector<int32_t>& out) {
             out.assign(sj.size() * 3, 0);
             if (sj.empty()) return;
@@ -1115,7 +1193,7 @@ int64_t hb_run_t(const HbRun& P, cudaStream_t st, int sms) {
             int32_t* rs = static_cast<int32_t*>(dres.get(out.size() * sizeof(int32_t)));
             auto fn = P.pmax ? hb_scan_kernel<T, true, R> : hb_scan_kernel<T, false, R>;
             HB_CUDA(allow_smem(reinterpret_cast<const void*>(fn), mat_b));
-            fn<<<grid, 32 * wpb, mat_b, st>>>(P.a, P.b, static_cast<const T*>(P.mat), P.N, gp, dj, int(sj.size()), rw,
+            fn<<<grid, 32 * wpb, mat_b, st>>>(P.a, P.b, static_cast<const T*>(P.mat), P.N, AR, K, dj, int(sj.size()), rw,
                                               stride, rs);
             HB_CUDA(cudaGetLastError());
             launches++;
@@ -1130,6 +1208,7 @@ int64_t hb_run_t(const HbRun& P, cudaStream_t st, int sms) {
             ScanJob J{};
             J.a_base = P.h_oa[p]; J.a_step = 1; J.b_base = P.h_ob[p]; J.b_step = 1;
             J.H = int(P.h_oa[p + 1] - P.h_oa[p]); J.W = int(P.h_ob[p + 1] - P.h_ob[p]);
+            track(J, p, 0, 1);
             J.local = P.glocal ? 0 : 1; J.glocal = P.glocal ? 1 : 0;
             if (P.glocal && J.W == 0) continue;   // no B: the end is column 0
             scan_f.push_back(J);
@@ -1154,6 +1233,7 @@ int64_t hb_run_t(const HbRun& P, cudaStream_t st, int sms) {
                 J.H = ie;
             }
             J.a_base = P.h_oa[p] + ie - 1; J.a_step = -1; J.b_base = P.h_ob[p] + je - 1; J.b_step = -1;
+            track(J, p, ie + 1, -1);
             J.W = je; J.local = 0;
             rev.push_back(J);
             rk.push_back(k);
@@ -1182,7 +1262,7 @@ int64_t hb_run_t(const HbRun& P, cudaStream_t st, int sms) {
     }
     const int NWmax = 16;
     const size_t ring_bytes_per_warp = size_t(3) * kHbRing * sizeof(T);
-    const size_t mat_bytes = size_t((P.N * P.N + 3) & ~3) * sizeof(T);
+    const size_t mat_bytes = size_t((K * P.N * P.N + 3) & ~3) * sizeof(T);
     while (true) {
         std::vector<int> split;
         for (int q = 0; q < int(cur.size()); ++q)
@@ -1199,9 +1279,11 @@ int64_t hb_run_t(const HbRun& P, cudaStream_t st, int sms) {
             SweepJob& F = jobs[2 * s];
             F.a_base = P.h_oa[p] + B.i0; F.a_step = 1; F.b_base = P.h_ob[p] + B.j0; F.b_step = 1;
             F.H = mid - B.i0; F.W = W; F.flag = B.in_x; F.tiled = 0;
+            track(F, p, B.i0, 1);
             SweepJob& Rv = jobs[2 * s + 1];
             Rv.a_base = P.h_oa[p] + B.i1 - 1; Rv.a_step = -1; Rv.b_base = P.h_ob[p] + B.j1 - 1; Rv.b_step = -1;
             Rv.H = B.i1 - mid; Rv.W = W; Rv.flag = B.out_x; Rv.tiled = 0;
+            track(Rv, p, B.i1 + 1, -1);
             for (SweepJob* x : {&F, &Rv}) {
                 x->out = out_off; out_off += 3 * (int64_t(W) + 1);
                 x->wrap = wrap_off; wrap_off += 3 * (int64_t(W) + 1);
@@ -1252,7 +1334,7 @@ int64_t hb_run_t(const HbRun& P, cudaStream_t st, int sms) {
         for (const SweepJob& x : jobs) n_block += x.tiled ? 0 : 1;
         if (n_block) {
             const int grid = int(std::min<int64_t>(n_block, int64_t(sms) * std::max(occ, 1)));
-            fn<<<grid, 32 * NW, smem, st>>>(P.a, P.b, static_cast<const T*>(P.mat), P.N, gp, dj, int(jobs.size()), o, wr);
+            fn<<<grid, 32 * NW, smem, st>>>(P.a, P.b, static_cast<const T*>(P.mat), P.N, AR, K, dj, int(jobs.size()), o, wr);
             HB_CUDA(cudaGetLastError());
         }
         if (n_tiles) {
@@ -1281,14 +1363,14 @@ int64_t hb_run_t(const HbRun& P, cudaStream_t st, int sms) {
                 TA.tiles = ti + 3 * doff[d];
                 TA.n_items = doff[d + 1] - doff[d];
                 const unsigned tg = unsigned(std::min<int64_t>((TA.n_items + 3) / 4, tmax));
-                tfn<<<tg, 128, mat_bytes, st>>>(P.a, P.b, static_cast<const T*>(P.mat), P.N, gp, TA, o, tr_rows, tr_cols);
+                tfn<<<tg, 128, mat_bytes, st>>>(P.a, P.b, static_cast<const T*>(P.mat), P.N, AR, K, TA, o, tr_rows, tr_cols);
                 HB_CUDA(cudaGetLastError());
                 launches++;
             }
         }
         int32_t* res = static_cast<int32_t*>(dres.get(split.size() * 2 * sizeof(int32_t)));
         const int jgrid = int(std::min<int64_t>(int64_t(split.size()), int64_t(sms) * 8));
-        hb_join_kernel<T><<<jgrid, 256, 0, st>>>(dj, int(split.size()), o, gp.go_b, res);
+        hb_join_kernel<T><<<jgrid, 256, 0, st>>>(dj, int(split.size()), o, AR, res);
         HB_CUDA(cudaGetLastError());
         launches += (n_block ? 1 : 0) + 1;   // the block sweep, the join
         std::vector<int32_t> h(split.size() * 2);
@@ -1322,6 +1404,8 @@ int64_t hb_run_t(const HbRun& P, cudaStream_t st, int sms) {
         BaseJob& J = bj[q];
         J.a_base = P.h_oa[p] + B.i0; J.b_base = P.h_ob[p] + B.j0;
         J.H = B.i1 - B.i0; J.W = B.j1 - B.j0; J.in_x = B.in_x; J.out_x = B.out_x;
+        J.i0 = B.i0; J.pm = int(P.h_oa[p + 1] - P.h_oa[p]);
+        J.tk_off = P.h_oa[p]; J.gk_off = P.h_oa[p] + p;
         J.codes = code_off; code_off += ((int64_t(J.H) + 1) * (int64_t(J.W) + 1) + 15) & ~int64_t(15);
         J.bnd = bnd_off; bnd_off += 3 * (int64_t(J.W) + 1);
         J.moves = mv_off; mv_off += int64_t(J.H) + J.W + 1;
@@ -1341,7 +1425,7 @@ int64_t hb_run_t(const HbRun& P, cudaStream_t st, int sms) {
         const int wpb = 4;
         const int grid = int(std::min<int64_t>((int64_t(bj.size()) + wpb - 1) / wpb, int64_t(sms) * 8));
         if (grid > 0) {
-            hb_base_kernel<T, R><<<grid, 32 * wpb, mat_bytes, st>>>(P.a, P.b, static_cast<const T*>(P.mat), P.N, gp,
+            hb_base_kernel<T, R><<<grid, 32 * wpb, mat_bytes, st>>>(P.a, P.b, static_cast<const T*>(P.mat), P.N, AR, K,
                                                                    dB, int(bj.size()), cd, bd, mvd, nm);
             HB_CUDA(cudaGetLastError());
         }
@@ -1563,7 +1647,7 @@ int64_t lhb_run_t(const HbRun& P, cudaStream_t st, int sms) {
         BaseJob& J = bj[q];
         J.a_base = P.h_oa[p] + B.i0; J.b_base = P.h_ob[p] + B.j0;
         J.H = B.i1 - B.i0; J.W = B.j1 - B.j0; J.in_x = 0; J.out_x = 0;
-        J.i0 = B.i0; J.pad = 0; J.tk_off = P.h_oa[p]; J.gk_off = P.h_oa[p] + p;
+        J.i0 = B.i0; J.pm = int(P.h_oa[p + 1] - P.h_oa[p]); J.tk_off = P.h_oa[p]; J.gk_off = P.h_oa[p] + p;
         J.codes = code_off; code_off += ((int64_t(J.H) + 1) * (int64_t(J.W) + 1) + 15) & ~int64_t(15);
         J.bnd = bnd_off; bnd_off += int64_t(J.W) + 1;
         J.moves = mv_off; mv_off += int64_t(J.H) + J.W + 1;

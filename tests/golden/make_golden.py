@@ -20,6 +20,8 @@ Two sources, both the reference's own code run here:
   banded_grad(bw) around the Viterbi guides, every gap model and mode, bw 1, 3, 8.
 * ``semiglobal.npz`` -- the batch engine with AlignMode::Glocal and free_ends sets (glocal,
   overlap, mixed): hard float32 / float64 with guides, soft log space at T = 1.
+* ``hirschberg_tracked.npz`` -- tracked affine Hirschberg (three parameter sets, with and without
+  gap tracks), Global, Local and glocal, both carries, float32 and float64.
 * ``hirschberg_glocal.npz`` -- the batch engine with glocal ends and traceback "hirschberg" /
   "hirschberg_pmax" (affine and linear, small hb_cutoff): A within a longer B, float32 and
   float64.
@@ -334,6 +336,40 @@ def posterior_fixtures():
     print("posterior.npz:", len(out), "arrays")
 
 
+def hb_tracked_fixtures():
+    """Tracked affine Hirschberg (hb_reverse_rows_, aligner.hpp:1848-1871): three parameter
+    sets picked per residue of A and gap sets per DP row, Global, Local and glocal, both carries."""
+    rng = np.random.default_rng(456)
+    AA = "ACDEFGHIKLMNPQRSTVWY"
+    K = 3
+    out = {}
+    mat = rng.integers(-4, 4, size=(K, 20, 20)).astype(np.float64)
+    for k in range(K):
+        mat[k][np.diag_indices(20)] = rng.integers(4, 12, size=20)
+    gaps = np.array([[11.0, 1.0, 11.0, 1.0], [9.0, 2.0, 10.0, 1.5], [12.0, 0.5, 8.0, 2.0]])
+    sa = ["".join(rng.choice(list(AA), size=int(rng.integers(1, 400)))) for _ in range(16)]
+    sb = ["".join(c if rng.random() > 0.25 else str(rng.choice(list(AA))) for c in s) if k % 2 else
+          "".join(rng.choice(list(AA), size=int(rng.integers(1, 400)))) for k, s in enumerate(sa)]
+    tr = np.concatenate([rng.integers(0, K, size=len(s)) for s in sa]).astype(np.uint16)
+    gt = np.concatenate([rng.integers(0, K, size=len(s) + 1) for s in sa]).astype(np.uint16)
+    out["mat"], out["gaps"], out["sa"], out["sb"] = mat, gaps, np.array(sa), np.array(sb)
+    out["tracks"], out["gap_tracks"] = tr, gt
+    for prec in (32, 64):
+        for tb in ("hirschberg", "hirschberg_pmax"):
+            for cut in (8, 64):
+                for am, tag in ((0, "G_"), (1, "L_"), (2, "g_")):
+                    for use_gt in (False, True):
+                        r = oracle.ref_run(prec, 1, am, 1, AA, mat, gaps, sa, sb, tracks=tr,
+                                           gap_tracks=gt if use_gt else None, traceback=tb, hb_cutoff=cut,
+                                           free_ends=12)
+                        key = f"{tag}{'gt_' if use_gt else ''}{tb}_{prec}_c{cut}_"
+                        out[key + "scores"] = r["scores"]
+                        out[key + "grads"] = r["grads"]
+                        out[key + "guides"] = r["guides"]
+    np.savez_compressed(os.path.join(HERE, "hirschberg_tracked.npz"), **out)
+    print("hirschberg_tracked.npz:", len(out), "arrays")
+
+
 def hb_glocal_fixtures():
     """Glocal Hirschberg (viterbi_affine_hirschberg_glocal): A (a mutated stretch of B, or
     random) within B with random flanks, so the end and start scans pick columns inside B."""
@@ -373,9 +409,11 @@ def hb_glocal_fixtures():
 
 
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["brute", "ref", "hb", "sb", "sg", "post", "hbg"]
+    which = sys.argv[1:] or ["brute", "ref", "hb", "sb", "sg", "post", "hbg", "hbt"]
     if "hbg" in which:
         hb_glocal_fixtures()
+    if "hbt" in which:
+        hb_tracked_fixtures()
     if "post" in which:
         posterior_fixtures()
     if "brute" in which:

@@ -45,6 +45,32 @@ def test_reference_fixtures(name, prec, tb, cut, mode, gap_model):
     assert tot == float(np.cumsum(z[key + "scores"])[-1])
 
 
+@pytest.mark.parametrize("prec", [32, 64])
+@pytest.mark.parametrize("tb", ["hirschberg", "hirschberg_pmax"])
+@pytest.mark.parametrize("cut", [8, 64])
+@pytest.mark.parametrize("mode", ["global", "local", "glocal"])
+@pytest.mark.parametrize("use_gt", [False, True])
+def test_tracked_affine_reference_fixtures(prec, tb, cut, mode, use_gt):
+    """Tracked affine Hirschberg (three parameter sets per residue of A, gap sets per DP row
+    or from the residues): every row's own substitution set and gap costs, the reverse sweep's
+    rewritten vertical moves (hb_reverse_rows_, aligner.hpp:1848-1871), the open refunded at
+    the cut from row p + 1 -- scores, gradients and guides bit for bit the reference engine's
+    (tests/golden/hirschberg_tracked.npz)."""
+    z = np.load(os.path.join(GOLD, "hirschberg_tracked.npz"))
+    sa, sb = [str(s) for s in z["sa"]], [str(s) for s in z["sb"]]
+    cls = nw.SeqPairBatch if prec == 32 else nw.SeqPairBatchDouble
+    b = cls(sa, sb, nw.AlignParams.from_arrays(z["mat"], z["gaps"], alphabet=AA), grad_mode="hard", traceback=tb,
+            mode=mode, tracks=z["tracks"], gap_tracks=z["gap_tracks"] if use_gt else None)
+    b.hb_cutoff = cut
+    b.score_and_grad()
+    gm, gg = b.grads()
+    flat = np.concatenate([gm.reshape(len(sa), -1), gg.reshape(len(sa), -1)], axis=1)
+    key = f"{dict(global_='G_', local_='L_', glocal_='g_')[mode + '_']}{'gt_' if use_gt else ''}{tb}_{prec}_c{cut}_"
+    assert np.array_equal(b.scores(), z[key + "scores"]), np.nonzero(b.scores() != z[key + "scores"])[0][:5]
+    assert np.array_equal(flat, z[key + "grads"]), np.nonzero((flat != z[key + "grads"]).any(1))[0][:5]
+    assert np.array_equal(b.guides(), z[key + "guides"])
+
+
 @pytest.mark.parametrize("pmax", [False, True])
 @pytest.mark.parametrize("mode", ["global", "local"])
 def test_tiled_half_sweeps_against_the_oracle(pmax, mode):
@@ -220,9 +246,10 @@ def test_errors():
     b = nw.SeqPairBatch(sa, sb, neg, grad_mode="hard", traceback="hirschberg")
     with pytest.raises(ValueError, match="non-negative"):
         b.score_and_grad()
+    # tracked linear glocal splits are not built (tracked affine ones are)
     tr = np.zeros(sum(len(s) for s in sa), np.uint16)
-    trk = nw.SeqPairBatch(sa, sb, nw.AlignParams.from_arrays(mat, [[11.0, 1.0, 11.0, 1.0]], alphabet=AA),
-                          grad_mode="hard", traceback="hirschberg", tracks=tr)
+    trk = nw.SeqPairBatch(sa, sb, nw.AlignParams.from_arrays(mat, [[0.0, 1.0, 0.0, 1.0]], alphabet=AA),
+                          grad_mode="hard", traceback="hirschberg", tracks=tr, mode="glocal", gap_model="linear")
     with pytest.raises(NotImplementedError):
         trk.score_and_grad()
     nlocal = nw.SeqPairBatch(sa, sb, neg, mode="local", grad_mode="hard", traceback="hirschberg_pmax")

@@ -190,15 +190,15 @@ def test_semiglobal_refusals_and_api():
     ov.score_and_grad()
     with pytest.raises(ValueError, match="glocal"):
         ov.banded_grad(8)
-    # glocal ends split untracked pairs (the reference's glocal Hirschberg): the same optimal
-    # scores; tracked glocal splits are not built; other end sets run Pointers
+    # glocal ends split pairs (the reference's glocal Hirschberg): the same optimal scores,
+    # tracked affine too (tracked linear glocal splits are not built); other end sets run Pointers
     h = nw.SeqPairBatch(sa, sb, p, mode="glocal", grad_mode="hard", traceback="hirschberg")
     h.score_and_grad()
     assert np.array_equal(h.scores(), full)
     trk = np.zeros(sum(len(x) for x in sa), np.uint16)
     ht = nw.SeqPairBatch(sa, sb, p, mode="glocal", grad_mode="hard", traceback="hirschberg", tracks=trk)
-    with pytest.raises(NotImplementedError):
-        ht.score_and_grad()
+    ht.score_and_grad()
+    assert np.array_equal(ht.scores(), full)
     hov = nw.SeqPairBatch(sa, sb, p, mode="overlap", grad_mode="hard", traceback="hirschberg")
     hov.score_and_grad()
     assert np.array_equal(hov.scores(), ov.scores())
