@@ -734,9 +734,11 @@ def _timed_run(fn, reps=1):
 def bench_c4(args):
     """Side measurement: long pairs (log-uniform 5k-36k).  Hard gradient by Pointers (tiles of
     256 x 256 cells, a launch per anti-diagonal of tiles), by the grid traceback (the same tiles
-    score-only, then a walk that refills the tiles its path crosses) and by Hirschberg (float32 prefix-max carry and float64 exact carry), soft
-    gradient (several warps per pair, stripe checkpoints), then banded re-alignment (bandwidth
-    64) after a 1e-3 parameter step.  GCUPS per stage from wall time around each call."""
+    score-only, then a walk that refills the tiles its path crosses) and by Hirschberg (float32
+    prefix-max carry and float64 exact carry; the large half-sweeps as tiles), each hard run
+    then re-aligned banded (bandwidth 64) after a 1e-3 parameter step; soft gradient (tiles:
+    forward and backward a launch per anti-diagonal), then soft banded re-alignment after a
+    step.  GCUPS per stage from wall time around each call (after a warm call)."""
     import nwgrad_b200 as nw
     mat, a, oa, b, ob = c4_workload(args.long_pairs)
     cells = cells_of(oa, ob)
@@ -765,6 +767,16 @@ def bench_c4(args):
     bt.score_and_grad()
     t = _timed_run(lambda: (bt.score_and_grad(), bt.compute_grad()))
     out["stages"]["soft_f32"] = {"seconds": t, "gcups": cells / t / 1e9}
+    # soft banded re-alignment (bandwidth 64) around the Viterbi guides after a parameter step,
+    # in float32 (the batch's precision)
+    g = bt.compute_grad()
+    bt.set_params(p + g * 1e-3)
+    bt.banded_grad(64)                                      # warm: the band plan
+    t = _timed_run(lambda: (bt.banded_grad(64), bt.compute_grad()))
+    band_cells = float(np.sum(np.diff(oa) * 129))
+    out["stages"]["soft_banded64_after_step_f32"] = {"seconds": t, "gcups_full_equivalent": cells / t / 1e9,
+                                                     "band_cells": band_cells,
+                                                     "refused_to_double": int(np.count_nonzero(bt.soft_status() & 0xFF))}
     return out
 
 
