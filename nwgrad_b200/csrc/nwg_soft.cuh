@@ -118,9 +118,10 @@ constexpr int kEmpty = -(1 << 28);
 // weights), and mass lost at a cell moves a posterior (and Z) by at most that mass times
 // B(c) / Z.  So, with fac = 2^(E_F + E_B - E_Z) / Z, the backward pass charges per lane and
 // step fac * (loss_w * (sum F^ + sum B^) + 16 R) -- loss_w = 16 + 16 wmax roundings per state
-// and cell, transfers and rescales included, 16 per row for the count products -- and where
-// fac itself underflows the products it drops (each at most F^ B^ 2^(E_F + E_B - E_Z)), all in
-// units of 2^-150.  A pair whose charge exceeds kLossMax (damage 2^-24) is refused.
+// and cell, transfers and rescales included, 16 per row for the count products -- in units of
+// 2^-150.  Where 2^(E_F + E_B - E_Z) falls below the normal range, the step's F^ move down
+// into it (fac stays normal) and the step charges its B^ once more for the F^ that rounded on
+// the way.  A pair whose charge exceeds kLossMax (damage 2^-24) is refused.
 constexpr float kLossMax = 0x1p126f;
 
 // Double accumulator with its own binary exponent: value = m * 2^e.
@@ -1064,8 +1065,23 @@ soft_kernel(const SoftArgs A) {
                         nbj = int(bp[j - 1]);
                     }
                     // scale of this step's products: 2^(E_F + E_B - E_Z) / zhat (an exact power of
-                    // two times 1 / zhat rounded to T)
-                    const int efac = EF + EB - EZ;
+                    // two times 1 / zhat rounded to T).  Both lanes may hold values far above 1
+                    // between renormalisations, so where that power falls below T's normal range
+                    // F^ B^ itself can leave it (a posterior of 1 at 2^-130: F^ 2^63, B^ 2^67);
+                    // this step's F^ then move down by the difference and the factor stays
+                    // normal, so that no product overflows and none is dropped
+                    int efac = EF + EB - EZ;
+                    constexpr int kFacLo = sizeof(T) == 4 ? -126 : -1022;
+                    const bool fdown = efac < kFacLo;
+                    if (__builtin_expect(fdown, 0)) {
+                        // 2^(efac - kFacLo) in two factors: a normal one, then the rest with
+                        // gradual underflow (each F^ rounds at most twice, by 2^-150 each)
+                        const int a = efac - kFacLo, h1 = max(a, kFacLo);
+                        const T s1 = pow2i<T>(h1), s2 = pow2s<T>(a - h1);
+#pragma unroll
+                        for (int k = 0; k < CV; ++k) f[k] = (f[k] * s1) * s2;
+                        efac = kFacLo;
+                    }
                     const double facd = (TR && lane_rows) ? pow2i<double>(efac) * invz : 0.0;
                     const T fac = TR ? static_cast<T>(facd) : lane_rows ? pow2i<T>(efac) * invzT : T(0);
                     if (!is_finite(fac)) why |= kSoftScale;
@@ -1183,12 +1199,13 @@ soft_kernel(const SoftArgs A) {
                         sga_x = fmaf_t(sx_a, fac, sga_x);
                     }
                     if constexpr (kCount) {
-                        // the lost-mass charge of this lane-step (scale factor in range), or the
-                        // products an underflowed scale factor dropped (each <= F^ B^ 2^efac),
-                        // in units of 2^-150
+                        // the lost-mass charge of this lane-step in units of 2^-150 (the factor is
+                        // normal: a step whose F^ moved down charges its B^ twice, for the F^ that
+                        // rounded into the subnormal range on the way); fac scales the sums first,
+                        // so that a large F^ + B^ times loss_w stays in range
                         if (lane_rows) {
-                            if (efac >= -126) lacc = fmaf_t(fac, fmaf_t(SF + SB, loss_w, T(16 * R)), lacc);
-                            else lacc = fmaf_t((SF + T(1)) * (SB + T(1)), T(5 * R) * pow2s<T>(efac + 150), lacc);
+                            const T sb = fdown ? SB + SB : SB;
+                            lacc = fmaf_t(fac * (SF + sb), loss_w, fmaf_t(fac, T(16 * R), lacc));
                         }
                     }
                     dgM = dnM;

@@ -183,6 +183,46 @@ def test_banded_soft_both_precisions(gm, mode, prec):
     _close(s, g, so, go, rtol=SOFT_RTOL if prec == 32 else 1e-9, atol=1e-5 if prec == 32 else 1e-9)
 
 
+def _long_homologs(rng, L, n):
+    """Integer matrix with diagonal scores 4-11 (steps of up to e^11 per cell at T = 1); B is A
+    with 20 % substitutions and single-residue insertions and deletions (2.5 % each)."""
+    m = rng.integers(-4, 4, size=(20, 20)).astype(np.float64)
+    m = np.triu(m) + np.triu(m, 1).T
+    m[np.diag_indices(20)] = rng.integers(4, 12, size=20)
+    sa, sb = [], []
+    for _ in range(n):
+        a = rng.integers(0, 20, L)
+        b = a.copy()
+        sub = rng.random(L) < 0.2
+        b[sub] = rng.integers(0, 20, int(sub.sum()))
+        out = []
+        for x, u in zip(b, rng.random(L)):
+            if u < 0.025:
+                continue                                  # deletion
+            out.append(x)
+            if u > 0.975:
+                out.append(int(rng.integers(0, 20)))      # insertion
+        sa.append("".join(AA[i] for i in a))
+        sb.append("".join(AA[i] for i in out))
+    return m[None], sa, sb
+
+
+@pytest.mark.parametrize("mode", ["global", "local"])
+def test_banded_long_pairs_stay_float32(mode):
+    """Banded re-alignment (bandwidth 64) of 3,000-residue related pairs after a parameter step.
+    Between renormalisations both lanes hold values far above 1, so a count's scale
+    2^(E_F + E_B - E_Z) falls below float32's normal range while F^ B^ nears 2^130; the step's
+    F^ move into the scale, so float32 keeps every pair (no refusal to double) and matches the
+    double batch."""
+    rng = np.random.default_rng(31)
+    mat, sa, sb = _long_homologs(rng, 3000, 3)
+    gaps = np.array([[11.0, 1.0, 11.0, 1.0]])
+    s32, g32, st = _run(nw.SeqPairBatch, AA, mat, gaps, sa, sb, "affine", mode, band=64)
+    s64, g64, _ = _run(nw.SeqPairBatchDouble, AA, mat, gaps, sa, sb, "affine", mode, band=64)
+    assert (st == 0).all(), st
+    _close(s32, g32, s64, g64)
+
+
 def test_out_of_range_raises():
     """A step score of 800 nats overflows exp() in double too: ValueError naming the reason
     (test_soft_denormal.py: test_out_of_range_still_raises)."""
