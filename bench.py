@@ -696,6 +696,14 @@ def main():
         dist.destroy_process_group()
 
 
+def _small_step(p, g, size=0.05):
+    """A gradient step whose largest move is `size` (scores in nats).  The summed gradient of
+    64 long pairs runs to tens of thousands per entry, so a fixed learning rate on it would move
+    the scores by tens of nats: weights near e^60, far outside a training step."""
+    big = max(float(np.abs(g.matrices).max()), float(np.abs(g.gaps).max()), 1e-30)
+    return p + g * (size / big)
+
+
 def c4_workload(n_pairs=64, seed=4):
     """Long pairs: A of length log-uniform 5,000-36,000, B = A with 20 % substitutions and
     single-residue indels (2.5 % each)."""
@@ -755,8 +763,7 @@ def bench_c4(args):
         t = _timed_run(lambda: (bt.score_and_grad(), bt.compute_grad()))
         out["stages"][name] = {"seconds": t, "gcups": cells / t / 1e9}
         if name == "hard_hirschberg_pmax_f32":
-            g = bt.compute_grad()
-            bt.set_params(p + g * 1e-3)
+            bt.set_params(_small_step(p, bt.compute_grad()))
             bt.banded_grad(64)                                  # warm: the band plan and its graph
             t = _timed_run(lambda: (bt.banded_grad(64), bt.compute_grad()))
             band_cells = float(np.sum(np.diff(oa) * 129))
@@ -769,8 +776,7 @@ def bench_c4(args):
     out["stages"]["soft_f32"] = {"seconds": t, "gcups": cells / t / 1e9}
     # soft banded re-alignment (bandwidth 64) around the Viterbi guides after a parameter step,
     # in float32 (the batch's precision)
-    g = bt.compute_grad()
-    bt.set_params(p + g * 1e-3)
+    bt.set_params(_small_step(p, bt.compute_grad()))
     bt.banded_grad(64)                                      # warm: the band plan
     t = _timed_run(lambda: (bt.banded_grad(64), bt.compute_grad()))
     band_cells = float(np.sum(np.diff(oa) * 129))

@@ -416,11 +416,30 @@ soft_kernel(const SoftArgs A) {
             }
             bcols = jhi_of(0);
         }
-        // the stripe's columns [tc0, tc1] (TL: the tile's) and steps: its columns plus the skew
-        const int tc0 = TL ? tc * A.tile_w : 0, tc1 = TL ? min(n, tc0 + A.tile_w - 1) : n;
+        // the columns [tc0f, tc1f] a stripe sweeps (TL: the tile's) and its steps, its columns
+        // plus the skew; a banded stripe sweeps fewer (band_cols), within the same table stride
+        const int tc0f = TL ? tc * A.tile_w : 0, tc1f = TL ? min(n, tc0f + A.tile_w - 1) : n;
         const int ntc = TL ? n / A.tile_w + 1 : 1;   // TL: tiles per stripe (columns 0..n)
-        const int S = tc1 - tc0 + G;
-        const int SP = S + 1;                   // MW: progress key per stripe
+        const int Sf = tc1f - tc0f + G;
+        const int SP = Sf + 1;                  // MW: progress key per stripe
+        // banded: the columns of stripe s, the union of its rows' bands with the first rounded
+        // down to a multiple of G (the forward pass stages the row above in G-aligned
+        // segments).  Both passes' cells outside a row's band are zero, so the sweep skips them;
+        // a column left of the union is out of band for all of the stripe's rows, and where the
+        // union starts at column 1 the rounding takes in column 0 (its Local start weights feed
+        // column 1).  A neighbouring stripe's row outside its own columns reads as zero.
+        auto band_cols = [&](const int s, int& lo, int& hi) {
+            int l = n + 1, h = -1;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int i = s * GR + lane * R + r;
+                if (i <= m) { l = min(l, jlo0_of(i)); h = max(h, jhi_of(i)); }
+            }
+            l = __reduce_min_sync(gmask, l);
+            h = __reduce_max_sync(gmask, h);
+            lo = l & ~(G - 1);
+            hi = h;
+        };
         // TL: this pair's rows (stride n + 1), per-tile lane states and per-stripe partials
         T* const rowf_p = TL ? static_cast<T*>(A.rowf) + A.row_off[p] * BW : nullptr;
         T* const rowb_p = TL ? static_cast<T*>(A.rowb) + A.row_off[p] * BW : nullptr;
@@ -450,6 +469,13 @@ soft_kernel(const SoftArgs A) {
             // a lane wholly below row m (the last stripe's padding) keeps no table: its backward
             // values are zero, so its forward values are never needed
             const bool store_table = (!ck || !pass1) && i0 <= m;
+            int tc0 = tc0f, tc1 = tc1f;
+            int plo = 0, phi = -1;              // banded: the columns the stripe above swept
+            if constexpr (BAND) {
+                band_cols(s, tc0, tc1);
+                if (s > 0) band_cols(s - 1, plo, phi);
+            }
+            const int S = tc1 - tc0 + G;
             T* const fb_in = TL ? rowf_p + int64_t(s - 1) * BW * (n + 1) : fbnd + (ck ? int64_t(s - 1) * BW * nb : 0);
             T* const fb_out = TL ? rowf_p + int64_t(s) * BW * (n + 1) : fbnd + (ck ? int64_t(s) * BW * nb : 0);
             int key[R];
@@ -486,8 +512,8 @@ soft_kernel(const SoftArgs A) {
             T zpart = T(0);                       // Local: the cells' sum since the last renorm
             T dgM = T(0), dgX = T(0), dgY = T(0); // row above, column j-1
             T upM = T(0), upX = T(0), upY = T(0); // row above, column j
-            T* fs = fwd + (ck ? 0 : int64_t(s) * S * G * CV);
-            int* fe = fexp + (ck ? 0 : int64_t(s) * S * G);
+            T* fs = fwd + (ck ? 0 : int64_t(s) * Sf * G * CV);
+            int* fe = fexp + (ck ? 0 : int64_t(s) * Sf * G);
             int nbj = tc0 > 0 ? int(bp[tc0 - 1]) : N;   // the first column's b code (column 0: none)
             // TL: this lane's state at the column left of the tile, as the tile to the left left it
             const T* const lst = (TL && tc > 0) ? colf_p + (int64_t(s) * ntc + tc - 1) * G * LS : nullptr;
@@ -507,7 +533,14 @@ soft_kernel(const SoftArgs A) {
 #pragma unroll
             for (int k = 0; k < BW; ++k) rb[k] = T(0);
             auto load_seg = [&](int c0) {   // group: columns c0 .. c0 + G - 1 into rb
-                if (c0 + lane <= tc1) vload<T, BW>(rb, fb_in + int64_t(c0 + lane) * BW);
+                const int c = c0 + lane;
+                if (BAND && (c < plo || c > phi)) {   // not swept above: zero, no scale
+#pragma unroll
+                    for (int k = 0; k < BW - 1; ++k) rb[k] = T(0);
+                    rb[BW - 1] = exp_bits(kEmpty, T(0));
+                } else if (c <= tc1) {
+                    vload<T, BW>(rb, fb_in + int64_t(c) * BW);
+                }
             };
             auto stage_seg = [&]() {        // group: rb into the staging row
                 __syncwarp(gmask);
@@ -570,6 +603,17 @@ soft_kernel(const SoftArgs A) {
                     v[BW - 1] = lst[(lane - 1) * LS + LS - 1];
                 }
                 if (lane > 0 || s > 0) {
+                    take_up(v[0], AFF ? v[1] : T(0), AFF ? v[2] : T(0), bits_exp(v[BW - 1]));
+                    dgM = upM; dgX = upX; dgY = upY;
+                    upM = T(0); upX = T(0); upY = T(0);
+                }
+            }
+            if constexpr (BAND) {
+                // the row above at the column left of the stripe's first: lane 0 from the stripe
+                // above's bottom row (the other lanes' rows above are out of band there)
+                if (s > 0 && tc0 > 0 && lane == 0 && tc0 - 1 >= plo && tc0 - 1 <= phi) {
+                    T v[BW];
+                    vload<T, BW>(v, fb_in + int64_t(tc0 - 1) * BW);
                     take_up(v[0], AFF ? v[1] : T(0), AFF ? v[2] : T(0), bits_exp(v[BW - 1]));
                     dgM = upM; dgX = upX; dgY = upY;
                     upM = T(0); upX = T(0); upY = T(0);
@@ -799,7 +843,7 @@ soft_kernel(const SoftArgs A) {
                     if (LOC) {
                         const int64_t q = A.tile_off[p] + int64_t(ts) * ntc + tc;
                         A.zpart[2 * q] = zm; A.zpart[2 * q + 1] = double(ze);
-                    } else if (ts == nstripes - 1 && tc1 == n) {
+                    } else if (ts == nstripes - 1 && tc1f == n) {
                         A.zpair[2 * p] = zm; A.zpair[2 * p + 1] = double(ze);
                     }
                     if (why) atomicOr(A.status + p, why);
@@ -857,6 +901,13 @@ soft_kernel(const SoftArgs A) {
         }
         for (int s = TL ? ts : nstripes - 1 - (MW ? gib : 0); s >= (TL ? ts : 0); s -= NWp) {
             if (ck) fwd_stripe(s, false);       // this stripe's forward table, from its checkpoint
+            int tc0 = tc0f, tc1 = tc1f;
+            int nlo = 0, nhi = -1;              // banded: the columns the stripe below swept
+            if constexpr (BAND) {
+                band_cols(s, tc0, tc1);
+                if (s < nstripes - 1) band_cols(s + 1, nlo, nhi);
+            }
+            const int S = tc1 - tc0 + G;
             // this stripe's row below (read) and its own top row (written): MW keeps one per stripe
             T* const bb_in = TL ? rowb_p + int64_t(s + 1) * BW * (n + 1) : bbnd + (MW ? int64_t(s + 1) * BW * nb : 0);
             T* const bb_out = TL ? rowb_p + int64_t(s) * BW * (n + 1) : bbnd + (MW ? int64_t(s) * BW * nb : 0);
@@ -927,8 +978,8 @@ soft_kernel(const SoftArgs A) {
                 EB = bits_exp(rst[lane * LS + LS - 1]);
                 lone = pow2s<T>(-EB);
             }
-            const T* fs = fwd + (ck ? 0 : int64_t(s) * S * G * CV);
-            const int* fe = fexp + (ck ? 0 : int64_t(s) * S * G);
+            const T* fs = fwd + (ck ? 0 : int64_t(s) * Sf * G * CV);
+            const int* fe = fexp + (ck ? 0 : int64_t(s) * Sf * G);
             // a lane wholly below row m has no table (its backward values are zero): it reads
             // zeros and scales by zero
             const bool lane_rows = i0 <= m;
@@ -944,7 +995,14 @@ soft_kernel(const SoftArgs A) {
 #pragma unroll
             for (int k = 0; k < BW; ++k) rb[k] = T(0);
             auto load_seg = [&](int d0) {   // group: distances d0 .. d0 + G - 1 into rb
-                if (d0 + lane <= tc1 - tc0) vload<T, BW>(rb, bb_in + int64_t(tc1 - d0 - lane) * BW);
+                const int c = tc1 - d0 - lane;
+                if (BAND && (c < nlo || c > nhi)) {   // not swept below: zero, no scale
+#pragma unroll
+                    for (int k = 0; k < BW - 1; ++k) rb[k] = T(0);
+                    rb[BW - 1] = exp_bits(kEmpty, T(0));
+                } else if (d0 + lane <= tc1 - tc0) {
+                    vload<T, BW>(rb, bb_in + int64_t(c) * BW);
+                }
             };
             auto stage_seg = [&]() {
                 __syncwarp(gmask);
@@ -1005,6 +1063,17 @@ soft_kernel(const SoftArgs A) {
                     v[BW - 1] = rst[(lane + 1) * LS + LS - 1];
                 }
                 if (lane < G - 1 || s < nstripes - 1) {
+                    take_dn(v[0], AFF ? v[1] : T(0), AFF ? v[2] : T(0), bits_exp(v[BW - 1]));
+                    dgM = dnM;
+                    dnM = T(0); dnX = T(0); dnY = T(0);
+                }
+            }
+            if constexpr (BAND) {
+                // the row below at the column right of the stripe's last: lane G-1 from the
+                // stripe below's top row (the other lanes' rows below are out of band there)
+                if (s < nstripes - 1 && tc1 < n && lane == G - 1 && tc1 + 1 >= nlo && tc1 + 1 <= nhi) {
+                    T v[BW];
+                    vload<T, BW>(v, bb_in + int64_t(tc1 + 1) * BW);
                     take_dn(v[0], AFF ? v[1] : T(0), AFF ? v[2] : T(0), bits_exp(v[BW - 1]));
                     dgM = dnM;
                     dnM = T(0); dnX = T(0); dnY = T(0);

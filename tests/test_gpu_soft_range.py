@@ -207,6 +207,27 @@ def _long_homologs(rng, L, n):
     return m[None], sa, sb
 
 
+@pytest.mark.parametrize("gm", ["linear", "affine"])
+@pytest.mark.parametrize("mode", ["global", "local"])
+def test_banded_soft_long_against_oracle(gm, mode):
+    """Banded re-alignment (bandwidth 20) of 1,500-residue related pairs with insertions and
+    deletions.  A stripe sweeps only the union of its rows' bands, so most stripes start far
+    right of column 0 and read the stripe above (or below) outside its own columns as zero.
+    Float32 and double against the oracle's banded pass around the same guides."""
+    rng = np.random.default_rng(37)
+    _, sa, sb = _long_homologs(rng, 1500, 3)
+    mat = rng.normal(-0.6, 0.6, (1, 20, 20)) + 2.0 * np.eye(20)
+    gaps = np.array([[3.3, 0.3, 3.3, 0.3]])
+    enc = oracle.Encoded(encode(AA, sa), encode(AA, sb))
+    gi, ai = ("linear", "affine").index(gm), _am(mode)
+    for prec, cls in ((32, nw.SeqPairBatch), (64, nw.SeqPairBatchDouble)):
+        s, g, st = _run(cls, AA, mat, gaps, sa, sb, gm, mode, band=20)
+        assert (st == 0).all(), st
+        g0 = oracle.hard(prec, gi, ai, mat, gaps, enc)["guides"]
+        so, go = oracle.soft(gi, ai, mat + 0.25, gaps + 0.1, enc, guides_in=g0, band=20)
+        _close(s, g, so, go, rtol=SOFT_RTOL if prec == 32 else 1e-9, atol=1e-5 if prec == 32 else 1e-9)
+
+
 @pytest.mark.parametrize("mode", ["global", "local"])
 def test_banded_long_pairs_stay_float32(mode):
     """Banded re-alignment (bandwidth 64) of 3,000-residue related pairs after a parameter step.
