@@ -253,10 +253,11 @@ constexpr int kSpinLimit = 1 << 22;
 constexpr int kPrefetchSteps = NWG_SOFT_PREFETCH_STEPS;
 
 // BAND: the guide-banded forward-backward (aligner.hpp:6231-6524 with AlignBand::GuideBanded):
-// the full DP is swept, and cells outside the band are zero -- forward cells of row i >= 1
-// outside [jlo(i), jhi(i)], Global border cells past border_rows / border_cols, backward cells
-// outside [jlo0(i), jhi0(i)]; Local log Z sums the band only.  Zero cells neither receive nor
-// pass on probability, which is what the reference's band-limited tables compute.
+// cells outside the band are zero -- forward cells of row i >= 1 outside [jlo(i), jhi(i)],
+// Global border cells past border_rows / border_cols, backward cells outside [jlo0(i), jhi0(i)];
+// Local log Z sums the band only.  Zero cells neither receive nor pass on probability, which is
+// what the reference's band-limited tables compute.  Each stripe sweeps only the union of its
+// rows' bands (band_cols), so a pass costs about (128 + 2 x bandwidth) columns per stripe.
 // POST: soft_guide="posterior" (aligner.hpp:6776-6808, 1466-1475): the backward pass also keeps,
 // per row, the column of greatest exit mass -- the cell's posterior less the posterior of moving
 // on to (i, j+1) within the row (affine: the Y posterior there; linear: F e_a B(i, j+1)), the
