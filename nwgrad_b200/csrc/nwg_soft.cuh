@@ -425,10 +425,13 @@ soft_kernel(const SoftArgs A) {
         const int SP = Sf + 1;                  // MW: progress key per stripe
         // banded: the columns of stripe s, the union of its rows' bands with the first rounded
         // down to a multiple of G (the forward pass stages the row above in G-aligned
-        // segments).  Both passes' cells outside a row's band are zero, so the sweep skips them;
-        // a column left of the union is out of band for all of the stripe's rows, and where the
-        // union starts at column 1 the rounding takes in column 0 (its Local start weights feed
-        // column 1).  A neighbouring stripe's row outside its own columns reads as zero.
+        // segments).  Both passes' cells of rows >= 1 outside a row's band are zero, so the
+        // sweep skips them; a column left of the union is out of band for all of the stripe's
+        // rows, and where the union starts at column 1 the rounding takes in column 0 (its Local
+        // start weights feed column 1).  Stripe 0 starts at column 0: row 0's cells are the
+        // origin and its gap run (Global) or start weights at every column (Local, glocal), and
+        // row 1 reads them left of its band.  A neighbouring stripe's row outside its own
+        // columns reads as zero.
         auto band_cols = [&](const int s, int& lo, int& hi) {
             int l = n + 1, h = -1;
 #pragma unroll
@@ -438,7 +441,7 @@ soft_kernel(const SoftArgs A) {
             }
             l = __reduce_min_sync(gmask, l);
             h = __reduce_max_sync(gmask, h);
-            lo = l & ~(G - 1);
+            lo = s == 0 ? 0 : l & ~(G - 1);
             hi = h;
         };
         // TL: this pair's rows (stride n + 1), per-tile lane states and per-stripe partials

@@ -228,6 +228,35 @@ def test_banded_soft_long_against_oracle(gm, mode):
         _close(s, g, so, go, rtol=SOFT_RTOL if prec == 32 else 1e-9, atol=1e-5 if prec == 32 else 1e-9)
 
 
+@pytest.mark.parametrize("gm", ["linear", "affine"])
+@pytest.mark.parametrize("mode", ["global", "local", "glocal"])
+def test_banded_soft_late_starts_against_oracle(gm, mode):
+    """B is a random prefix of 88-133 residues followed by a mutated copy of a 300-residue A,
+    so the paths start far along row 0: Global through the origin and a long gap run on row 0,
+    Local and glocal from row 0's start weights left of row 1's band.  Banded stripes below
+    the first start right of column 0; the prefix lengths put band edges on multiples of 32.
+    Float32 against the oracle's banded pass (bandwidth 6)."""
+    rng = np.random.default_rng(41)
+    mat = rng.normal(-0.6, 0.6, (1, 20, 20)) + 2.0 * np.eye(20)
+    gaps = np.array([[3.3, 0.3, 3.3, 0.3]])
+    sa, sb = [], []
+    for P in range(88, 136, 3):
+        a = rng.integers(0, 20, 300)
+        b = a.copy()
+        sub = rng.random(300) < 0.15
+        b[sub] = rng.integers(0, 20, int(sub.sum()))
+        sa.append("".join(AA[i] for i in a))
+        sb.append("".join(AA[i] for i in np.concatenate([rng.integers(0, 20, P), b])))
+    enc = oracle.Encoded(encode(AA, sa), encode(AA, sb))
+    gi, ai = ("linear", "affine").index(gm), _am(mode)
+    fe = dict(free_ends=12) if mode == "glocal" else {}
+    s, g, st = _run(nw.SeqPairBatch, AA, mat, gaps, sa, sb, gm, mode, band=6)
+    assert (st == 0).all(), st
+    g0 = oracle.hard(32, gi, ai, mat, gaps, enc, **fe)["guides"]
+    so, go = oracle.soft(gi, ai, mat + 0.25, gaps + 0.1, enc, 1.0, guides_in=g0, band=6, **fe)
+    _close(s, g, so, go)
+
+
 @pytest.mark.parametrize("mode", ["global", "local"])
 def test_banded_long_pairs_stay_float32(mode):
     """Banded re-alignment (bandwidth 64) of 3,000-residue related pairs after a parameter step.
