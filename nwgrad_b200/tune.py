@@ -21,6 +21,7 @@ instead (one fixed geometry, 32 lanes x 4 rows, for every pair).
 """
 from __future__ import annotations
 
+import functools
 import json
 import os
 
@@ -63,6 +64,7 @@ def _save_cache(c: dict) -> None:
         pass
 
 
+@functools.lru_cache(maxsize=None)
 def _device_name(dev: int) -> str:
     try:
         import torch
@@ -75,14 +77,20 @@ def _soft(batch) -> bool:
     return batch._grad_mode == "soft"
 
 
-def _classes(batch) -> dict:
-    """size class -> indices of the batch's pairs in it."""
+def _class_of(batch) -> np.ndarray:
+    """Every pair's size class: ceil(log2(cells)) in integers, as the store computes it (the
+    binary exponent of cells - 1)."""
     m = np.diff(batch._oa).astype(np.int64)
     n = np.diff(batch._ob).astype(np.int64)
     rows = m + 1 if _soft(batch) else m
     cells = np.maximum(rows, 1) * np.maximum(n, 1)
-    # ceil(log2(cells)) in integers, as the store computes it: the binary exponent of cells - 1
-    sc = np.where(cells <= 1, 0, np.frexp(np.maximum(cells - 1, 1).astype(np.float64))[1]).astype(np.int64)
+    return np.where(cells <= 1, 0, np.frexp(np.maximum(cells - 1, 1).astype(np.float64))[1]).astype(np.int64)
+
+
+def _classes(batch, sc=None) -> dict:
+    """size class -> indices of the batch's pairs in it."""
+    if sc is None:
+        sc = _class_of(batch)
     order = np.argsort(sc, kind="stable")
     bounds = np.flatnonzero(np.diff(sc[order])) + 1
     return {int(sc[g[0]]): g for g in np.split(order, bounds) if g.size}   # each in pair order (stable)
@@ -175,8 +183,15 @@ def tune(batch, sample_pairs: int = 65536, force: bool = False, verbose: bool = 
     table = {}
     codes = None
     dirty = False
-    for sc, idx in sorted(_classes(batch).items()):
-        key = _key(batch, sc)
+    csc = _class_of(batch)
+    present = np.flatnonzero(np.bincount(csc))
+    keys = {int(sc): _key(batch, int(sc)) for sc in present}
+    if not force and all(k in cache for k in keys.values()):
+        groups = {sc: None for sc in keys}           # every class cached: no pair lists needed
+    else:
+        groups = _classes(batch, csc)
+    for sc, idx in sorted(groups.items()):
+        key = keys[sc]
         if not force and key in cache:
             ent = cache[key]
             table[sc] = {"costs": [tuple(x) for x in ent["costs"]]} if "costs" in ent else tuple(ent["geo"])
