@@ -608,12 +608,23 @@ def main():
         h2d = int(a.nbytes + bp.nbytes + bn.nbytes + 3 * oa.nbytes)
         gs = params.num_sets * (20 * 20 + 4)
         d2h = int(2 * gs * 8 + 8)
+        # the step's inputs in pinned host memory (a loader's staging buffers): the library
+        # copies them to HBM inside the timed region at DMA speed
+        keep = []
+
+        def pinned(x):
+            t = torch.empty(x.shape, dtype=torch.from_numpy(x[:0]).dtype, pin_memory=True)
+            v = t.numpy()
+            v[...] = x
+            keep.append(t)
+            return v
+        ha, hoa, hbp, hobp, hbn, hobn = (pinned(x) for x in (a, oa, bp, obp, bn, obn))
         e2e_ms = []
         for k in range(max(1, min(args.steps, 3))):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            p_ = nw.SeqPairBatch.from_codes(a, oa, bp, obp, params, grad_mode="soft", device=local)
-            n_ = nw.SeqPairBatch.from_codes(a, oa, bn, obn, params, grad_mode="soft", device=local)
+            p_ = nw.SeqPairBatch.from_codes(ha, hoa, hbp, hobp, params, grad_mode="soft", device=local)
+            n_ = nw.SeqPairBatch.from_codes(ha, hoa, hbn, hobn, params, grad_mode="soft", device=local)
             if args.geometry:
                 p_._tune = n_._tune = pos._tune
             elif not args.no_tune:
@@ -632,7 +643,7 @@ def main():
             em = float(t.item())
         e2e = {"value": world * cells / (em / 1e3) / 1e9, "unit": "GCUPS", "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "ms_per_step": em,
-               "path": "SeqPairBatch.from_codes (host codes -> HBM) + autotune (cached table) + "
+               "path": "SeqPairBatch.from_codes (pinned host codes -> HBM) + autotune (cached table) + "
                        "score_and_grad + compute_grad"}
 
     clocks = clk.summary()
