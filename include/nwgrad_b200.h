@@ -60,7 +60,11 @@ const char* nwg_last_error(void);
 
 /* Build a store: upload n_pairs pairs (codes of A and B, concatenated, with n_pairs + 1
  * int64 offsets each), every code < nalpha.  tracks: per residue of A (off_a offsets) or
- * NULL; gap_tracks: per DP row, m + 1 per pair at off_a[p] + p, or NULL.
+ * NULL; gap_tracks: per DP row, m + 1 per pair at off_a[p] + p, or NULL.  The host buffers
+ * may be reused once the call returns.  Codes in pinned host memory (cudaHostAlloc, a torch
+ * pin_memory tensor) upload at DMA speed; pageable ones go through the driver's staging (a
+ * store of 60 MB of codes: about 9.5 ms from pageable buffers, about 6 ms from pinned ones on
+ * a B200 host, the rest being the code check and the offsets).
  * Replaces BatchEngine's constructor (batch_engine.hpp:284-350). */
 int nwg_store_create(const uint8_t* codes_a, const int64_t* off_a, const uint8_t* codes_b,
                      const int64_t* off_b, int64_t n_pairs, int nalpha, const uint16_t* tracks,
