@@ -79,3 +79,32 @@ def test_mode_parsing():
         parse_mode("semiglobal", (True, False))
     with pytest.raises(ValueError, match="unknown mode"):
         parse_mode("fitting")
+
+
+def test_tuner_size_classes():
+    """The tuner's size classes: ceil(log2(rows x cols)) in integers (soft rows count row 0),
+    the class set it keys the cache by equals the classes of the per-pair split, and every
+    pair lands in exactly one class, in pair order."""
+    from nwgrad_b200 import tune
+
+    class FakeBatch:
+        pass
+
+    rng = np.random.default_rng(3)
+    la = rng.integers(0, 700, 5000)
+    lb = rng.integers(0, 700, 5000)
+    for grad_mode in ("soft", "hard"):
+        b = FakeBatch()
+        b._oa = np.concatenate([[0], np.cumsum(la)]).astype(np.int64)
+        b._ob = np.concatenate([[0], np.cumsum(lb)]).astype(np.int64)
+        b._grad_mode = grad_mode
+        sc = tune._class_of(b)
+        rows = la + 1 if grad_mode == "soft" else la
+        want = [tune.size_class(int(r), int(c)) for r, c in zip(rows, lb)]
+        np.testing.assert_array_equal(sc, want)
+        groups = tune._classes(b, sc)
+        assert sorted(groups) == np.flatnonzero(np.bincount(sc)).tolist()
+        idx = np.concatenate([groups[k] for k in sorted(groups)])
+        assert np.array_equal(np.sort(idx), np.arange(la.size))
+        for k, g in groups.items():
+            assert np.all(sc[g] == k) and np.all(np.diff(g) > 0)
